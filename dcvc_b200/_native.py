@@ -1,0 +1,66 @@
+"""ctypes binding of libdcvc_b200.so (the C ABI declared in include/dcvc_b200.h).
+
+The library is required: there is no CPU or PyTorch fallback for any operator of this package.
+If it is missing, importing this module raises.
+"""
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libdcvc_b200.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(
+        f"{LIB_PATH} is missing: build it with `python -m dcvc_b200.build` (nvcc, sm_100a)")
+
+lib = ctypes.CDLL(LIB_PATH)
+
+c_int = ctypes.c_int
+c_vp = ctypes.c_void_p
+c_float_p = ctypes.POINTER(ctypes.c_float)
+
+# status codes (include/dcvc_b200.h)
+DCVC_OK = 0
+STATUS_NAMES = {
+    1: "invalid argument", 2: "CUDA error", 3: "device timeout", 4: "out of memory",
+    5: "corrupt stream", 6: "not ready", 7: "host timeout", 8: "internal error",
+}
+
+F16, BF16 = 0, 1
+EPI_BIAS, EPI_BIAS_WSILU, EPI_BIAS_RES, EPI_BIAS_RES_Q, EPI_BIAS_RES2, EPI_QUAD, EPI_SUBPEL, \
+    EPI_BIAS_Q = range(8)
+
+
+class DcvcError(RuntimeError):
+    """Raised when a C-ABI call returns a non-zero status."""
+
+    def __init__(self, status, where):
+        msg = lib.dcvc_last_error().decode(errors="replace")
+        super().__init__(f"{where}: {STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+def check(status, where):
+    if status != DCVC_OK:
+        raise DcvcError(status, where)
+
+
+def _proto(name, restype, argtypes):
+    f = getattr(lib, name)
+    f.restype = restype
+    f.argtypes = argtypes
+    return f
+
+
+_proto("dcvc_last_error", ctypes.c_char_p, [])
+_proto("dcvc_abi_version", c_int, [])
+_proto("dcvc_device_error", c_int, [ctypes.POINTER(c_int), c_int])
+_proto("dcvc_conv1x1", c_int,
+       [c_int, c_int, c_int, c_int, c_int, c_vp, c_int, c_vp, c_vp, c_vp, c_int, c_vp, c_int,
+        c_vp, c_vp, c_int, c_int, c_int, c_int, c_vp])
+
+
+def device_error(clear=True):
+    code = c_int(0)
+    check(lib.dcvc_device_error(ctypes.byref(code), 1 if clear else 0), "dcvc_device_error")
+    return code.value

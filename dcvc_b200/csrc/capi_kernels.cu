@@ -1,0 +1,71 @@
+// extern "C" kernel-level entry points (declared in include/dcvc_b200.h).
+#include "errors.h"
+#include "gemm_sm100.cuh"
+
+#include "../../include/dcvc_b200.h"
+
+namespace dcvc {
+cudaError_t gemm_sm100(int dtype, const void* A, int lda, const void* W, const GemmParams& p,
+                       int epi, int bn, cudaStream_t stream);
+}
+
+using namespace dcvc;
+
+extern "C" {
+
+const char* dcvc_last_error(void) { return last_error(); }
+
+int dcvc_abi_version(void) { return DCVC_ABI_VERSION; }
+
+int dcvc_device_error(int* code, int clear)
+{
+    if (code == nullptr) {
+        set_last_error("dcvc_device_error: null code pointer");
+        return kInvalidArgument;
+    }
+    int* w = device_error_word();
+    if (w == nullptr) {
+        set_last_error("dcvc_device_error: no device error word");
+        return kCudaError;
+    }
+    int st = cuda_status(cudaMemcpy(code, w, sizeof(int), cudaMemcpyDeviceToHost), "dcvc_device_error");
+    if (st == kOk && clear) {
+        st = cuda_status(cudaMemset(w, 0, sizeof(int)), "dcvc_device_error");
+    }
+    return st;
+}
+
+int dcvc_conv1x1(int dtype, int epilogue, int M, int N, int K, const void* a, int lda,
+                 const void* w, const float* bias, const void* res, int ldr, const void* res2,
+                 int ldr2, const void* qscale, void* out, int ldo, int sub_w, int sub_cout,
+                 int block_n, void* stream)
+{
+    if (dtype != DCVC_F16 && dtype != DCVC_BF16) {
+        set_last_error("dcvc_conv1x1: dtype must be f16 or bf16");
+        return kInvalidArgument;
+    }
+    GemmParams p{};
+    p.M = M;
+    p.N = N;
+    p.K = K;
+    p.bias = bias;
+    p.res = res;
+    p.ldr = ldr;
+    p.res2 = res2;
+    p.ldr2 = ldr2;
+    p.qscale = qscale;
+    p.out = out;
+    p.ldo = ldo;
+    p.sub_w = sub_w;
+    p.sub_cout = sub_cout;
+    p.err = device_error_word();
+    cudaError_t e = gemm_sm100(dtype, a, lda, w, p, epilogue, block_n,
+                               static_cast<cudaStream_t>(stream));
+    if (e == cudaErrorInvalidValue) {
+        set_last_error("dcvc_conv1x1: unsupported shape, pitch, alignment or epilogue");
+        return kInvalidArgument;
+    }
+    return cuda_status(e, "dcvc_conv1x1");
+}
+
+}  // extern "C"

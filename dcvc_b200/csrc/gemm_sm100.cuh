@@ -1,0 +1,47 @@
+// 1x1-convolution GEMM family for sm_100a: D[M,N] = epilogue(A[M,K] . W[N,K]^T).
+//
+// A is an NHWC activation (rows = pixels, K = input channels, row pitch lda), W the conv weight
+// [C_out, C_in] (K-major).  Both operands are staged by TMA (128-byte swizzle) into a multi-stage
+// shared-memory ring; one thread issues tcgen05.mma (M=128, N=BN, K=16) into a double-buffered
+// FP32 accumulator in tensor memory; four epilogue warps drain it with tcgen05.ld, apply the
+// fused epilogue and store FP16/BF16.  The kernel is persistent (one CTA per SM, static tile
+// striding) so the epilogue of one tile overlaps the main loop of the next.
+//
+// Reference operators covered (src/layers/extensions/inference/def_cutlass.h:10-34):
+//   conv1x1_bias, conv1x1_bias_wsilu, conv1x1_bias_shortcut, conv1x1_bias_shortcut2,
+//   conv1x1_bias_shortcut_with_quant, conv1x1_bias_with_quant, conv1x1_bias_wsilu_chunk_add
+//   (the "quad GEMM"), and the 2x2 stride-2 transposed conv (transposed_conv.cu) as a GEMM with
+//   a pixel-shuffle store.
+#pragma once
+
+#include "common.cuh"
+
+namespace dcvc {
+
+enum GemmEpilogue : int {
+    kEpiBias = 0,         // out = acc + b
+    kEpiBiasWsilu = 1,    // out = wsilu(acc + b)
+    kEpiBiasRes = 2,      // out = acc + b + r
+    kEpiBiasResQ = 3,     // out = (acc + b + r) * q[n]
+    kEpiBiasRes2 = 4,     // out = acc + b + r + r2
+    kEpiQuad = 5,         // out[n/4] = sum_{k<4} wsilu(acc[n+k] + b[n+k])
+    kEpiSubpel = 6,       // out[(2h+dy, 2w+dx), c] = acc  (columns ordered (dy, dx, c))
+    kEpiBiasQ = 7,        // out = (acc + b) * q[n]
+};
+
+struct GemmParams {
+    int M, N, K;
+    const float* bias;   // [N] fp32 (may be null for kEpiSubpel)
+    const void* res;     // residual rows, pitch ldr (elements)
+    int ldr;
+    const void* res2;
+    int ldr2;
+    const void* qscale;  // [N] per-output-channel multiplier (same dtype as the activations)
+    void* out;           // output rows, pitch ldo (elements)
+    int ldo;
+    int sub_w;           // kEpiSubpel: width of the input grid (rows are h * sub_w + w)
+    int sub_cout;        // kEpiSubpel: output channels per sub-pixel position
+    int* err;            // device error word
+};
+
+}  // namespace dcvc

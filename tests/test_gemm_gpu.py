@@ -1,0 +1,94 @@
+"""tcgen05 1x1-conv GEMM family vs a plain PyTorch fp32 reference of the same op.
+
+Tolerance: FP16/BF16 operands with FP32 accumulation, output rounded once to the activation
+type; we allow |err| <= atol + rtol*|ref| with (atol, rtol) = (2e-2, 1e-2) for f16 and
+(6e-2, 2e-2) for bf16.
+"""
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+TOL = {torch.float16: (2e-2, 1e-2), torch.bfloat16: (6e-2, 2e-2)}
+
+
+def _wsilu(x):
+    return x * torch.sigmoid(4.0 * x)
+
+
+def _ref(epi, a, w, b, res=None, res2=None, q=None, sub_w=0, sub_cout=0):
+    from dcvc_b200 import _native as N
+    acc = a.float() @ w.float().t()
+    if epi == N.EPI_SUBPEL:
+        M = a.shape[0]
+        H = M // sub_w
+        t = acc.view(H, sub_w, 2, 2, sub_cout)  # (h, w, dy, dx, c)
+        return t.permute(0, 2, 1, 3, 4).reshape(4 * M, sub_cout)
+    acc = acc + b
+    if epi == N.EPI_BIAS_WSILU:
+        acc = _wsilu(acc)
+    if epi in (N.EPI_BIAS_RES, N.EPI_BIAS_RES_Q, N.EPI_BIAS_RES2):
+        acc = acc + res.float()
+    if epi == N.EPI_BIAS_RES2:
+        acc = acc + res2.float()
+    if epi in (N.EPI_BIAS_RES_Q, N.EPI_BIAS_Q):
+        acc = acc * q.float()
+    if epi == N.EPI_QUAD:
+        acc = _wsilu(acc).view(acc.shape[0], -1, 4).sum(-1)
+    return acc
+
+
+CASES = [
+    # (epilogue name, M, N, K, dtype, block_n)
+    ("EPI_BIAS", 1000, 256, 512, torch.float16, 0),
+    ("EPI_BIAS", 32640, 512, 512, torch.float16, 0),
+    ("EPI_BIAS", 8160, 768, 768, torch.float16, 0),
+    ("EPI_BIAS", 510, 192, 256, torch.float16, 0),
+    ("EPI_BIAS", 777, 128, 64, torch.float16, 128),
+    ("EPI_BIAS", 4000, 256, 1024, torch.float16, 64),
+    ("EPI_BIAS_WSILU", 32640, 256, 512, torch.float16, 0),
+    ("EPI_BIAS_RES", 8160, 512, 256, torch.float16, 0),
+    ("EPI_BIAS_RES_Q", 3000, 512, 256, torch.float16, 0),
+    ("EPI_BIAS_RES2", 3000, 256, 256, torch.float16, 0),
+    ("EPI_QUAD", 32640, 1024, 512, torch.float16, 0),
+    ("EPI_QUAD", 2040, 1024, 256, torch.float16, 128),
+    ("EPI_BIAS_Q", 1500, 512, 512, torch.float16, 0),
+    ("EPI_BIAS", 5000, 512, 512, torch.bfloat16, 0),
+    ("EPI_QUAD", 5000, 1024, 512, torch.bfloat16, 0),
+]
+
+
+@pytest.mark.parametrize("name,M,Nn,K,dtype,bn", CASES)
+def test_conv1x1(name, M, Nn, K, dtype, bn):
+    from dcvc_b200 import _native as N, ops
+    epi = getattr(N, name)
+    g = torch.Generator(device="cuda").manual_seed(M * 7 + Nn * 3 + K)
+    dev = "cuda"
+    # strided A (a channel slice of a wider buffer) to exercise the row pitch
+    abuf = torch.randn(M, K + 64, device=dev, generator=g).to(dtype)
+    a = abuf[:, 32:32 + K]
+    w = (torch.randn(Nn, K, device=dev, generator=g) / K ** 0.5).to(dtype)
+    b = torch.randn(Nn, device=dev, generator=g) * 0.1
+    res = torch.randn(M, Nn, device=dev, generator=g).to(dtype)
+    res2 = torch.randn(M, Nn, device=dev, generator=g).to(dtype)
+    q = (torch.rand(Nn, device=dev, generator=g) + 0.5).to(dtype)
+    out = ops.conv1x1(a, w, b, epi, res=res, res2=res2, qscale=q, block_n=bn)
+    torch.cuda.synchronize()
+    assert N.device_error() == 0
+    ref = _ref(epi, a, w, b, res, res2, q)
+    atol, rtol = TOL[dtype]
+    err = (out.float() - ref).abs()
+    assert bool((err <= atol + rtol * ref.abs()).all()), float(err.max())
+
+
+@pytest.mark.parametrize("H,W,Cin,Cout", [(17, 30, 128, 256), (34, 60, 256, 256), (68, 120, 256, 512)])
+def test_subpel(H, W, Cin, Cout):
+    from dcvc_b200 import _native as N, ops
+    g = torch.Generator(device="cuda").manual_seed(H * W)
+    x = torch.randn(H * W, Cin, device="cuda", generator=g).half()
+    w = (torch.randn(4 * Cout, Cin, device="cuda", generator=g) / Cin ** 0.5).half()
+    out = ops.conv1x1(x, w, None, N.EPI_SUBPEL, sub_w=W, sub_cout=Cout)
+    torch.cuda.synchronize()
+    ref = _ref(N.EPI_SUBPEL, x, w, None, sub_w=W, sub_cout=Cout)
+    err = (out.float() - ref).abs()
+    assert bool((err <= 2e-2 + 1e-2 * ref.abs()).all()), float(err.max())
