@@ -1,0 +1,802 @@
+#include "elementwise.cuh"
+#include "host_util.h"
+
+namespace dcvc {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+inline int grid_for(long long work, int threads = kThreads)
+{
+    long long g = (work + threads - 1) / threads;
+    long long cap = static_cast<long long>(num_sms()) * 16;
+    if (g > cap) {
+        g = cap;
+    }
+    return g < 1 ? 1 : static_cast<int>(g);
+}
+
+// FP16 ops as at::Half does them: FP32 op, one rounding to FP16.
+__device__ __forceinline__ float h2f(__half h) { return __half2float(h); }
+__device__ __forceinline__ __half f2h(float f) { return __float2half_rn(f); }
+__device__ __forceinline__ __half hadd(__half a, __half b) { return f2h(__fadd_rn(h2f(a), h2f(b))); }
+__device__ __forceinline__ __half hsub(__half a, __half b) { return f2h(__fsub_rn(h2f(a), h2f(b))); }
+__device__ __forceinline__ __half hmul(__half a, __half b) { return f2h(__fmul_rn(h2f(a), h2f(b))); }
+__device__ __forceinline__ __half hzero() { return __ushort_as_half(0); }
+
+struct alignas(16) Vec8h {
+    __half v[8];
+};
+
+__device__ __forceinline__ Vec8h ld8(const __half* p) { return *reinterpret_cast<const Vec8h*>(p); }
+__device__ __forceinline__ void st8(__half* p, const Vec8h& v) { *reinterpret_cast<Vec8h*>(p) = v; }
+
+// ------------------------------------------------------------------------------ layout
+
+__global__ void pad_unshuffle8_kernel(const __half* __restrict__ x, int H, int W, int C, int ldx,
+                                      int H8, int W8, __half* __restrict__ out, int ldo)
+{
+    // one thread = 8 output channels c*64 + dy*8 + [0, 8) of one output pixel
+    const long long vec_per_pix = static_cast<long long>(C) * 8;
+    const long long total = static_cast<long long>(H8) * W8 * vec_per_pix;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const long long pix = i / vec_per_pix;
+        const int v = static_cast<int>(i - pix * vec_per_pix);
+        const int c = v >> 3;
+        const int dy = v & 7;
+        const int h8 = static_cast<int>(pix / W8);
+        const int w8 = static_cast<int>(pix - static_cast<long long>(h8) * W8);
+        const int sh = min(h8 * 8 + dy, H - 1);
+        Vec8h o;
+#pragma unroll
+        for (int dx = 0; dx < 8; ++dx) {
+            const int sw = min(w8 * 8 + dx, W - 1);
+            o.v[dx] = x[(static_cast<long long>(sh) * W + sw) * ldx + c];
+        }
+        st8(out + pix * ldo + c * 64 + dy * 8, o);
+    }
+}
+
+__global__ void shuffle8_clamp_kernel(const __half* __restrict__ in, int H8, int W8, int C, int ldi,
+                                      __half* __restrict__ out)
+{
+    const int Wp = W8 * 8;
+    const long long total = static_cast<long long>(H8) * 8 * Wp;
+    const __half lo = __float2half_rn(-0.5f);
+    const __half hi = __float2half_rn(0.5f);
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const int y = static_cast<int>(i / Wp);
+        const int xx = static_cast<int>(i - static_cast<long long>(y) * Wp);
+        const __half* src = in + (static_cast<long long>(y >> 3) * W8 + (xx >> 3)) * ldi +
+                            (y & 7) * 8 + (xx & 7);
+        for (int c = 0; c < C; ++c) {
+            __half v = src[c * 64];
+            v = __hmax(v, lo);
+            v = __hmin(v, hi);
+            out[i * C + c] = v;
+        }
+    }
+}
+
+__global__ void space_to_depth2_kernel(const __half* __restrict__ x, int H, int W, int C, int ldx,
+                                       __half* __restrict__ out)
+{
+    const int Ho = H / 2, Wo = W / 2;
+    const int vecs = C / 8;
+    const long long total = static_cast<long long>(Ho) * Wo * 4 * vecs;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const long long pix = i / (4 * vecs);
+        const int r = static_cast<int>(i - pix * 4 * vecs);
+        const int sub = r / vecs;
+        const int v = r - sub * vecs;
+        const int ho = static_cast<int>(pix / Wo);
+        const int wo = static_cast<int>(pix - static_cast<long long>(ho) * Wo);
+        const int h = 2 * ho + (sub >> 1);
+        const int w = 2 * wo + (sub & 1);
+        st8(out + pix * (4LL * C) + sub * C + v * 8,
+            ld8(x + (static_cast<long long>(h) * W + w) * ldx + v * 8));
+    }
+}
+
+__global__ void im2col3x3s2_kernel(const __half* __restrict__ x, int H, int W, int C, int ldx,
+                                   __half* __restrict__ out)
+{
+    const int Ho = H / 2, Wo = W / 2;
+    const int vecs = C / 8;
+    const long long total = static_cast<long long>(Ho) * Wo * 9 * vecs;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const long long pix = i / (9 * vecs);
+        const int r = static_cast<int>(i - pix * 9 * vecs);
+        const int tap = r / vecs;
+        const int v = r - tap * vecs;
+        const int ho = static_cast<int>(pix / Wo);
+        const int wo = static_cast<int>(pix - static_cast<long long>(ho) * Wo);
+        const int h = 2 * ho + tap / 3 - 1;
+        const int w = 2 * wo + tap % 3 - 1;
+        Vec8h o;
+        if (h >= 0 && h < H && w >= 0 && w < W) {
+            o = ld8(x + (static_cast<long long>(h) * W + w) * ldx + v * 8);
+        } else {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                o.v[j] = hzero();
+            }
+        }
+        st8(out + pix * (9LL * C) + tap * C + v * 8, o);
+    }
+}
+
+__global__ void replicate_pad_kernel(const __half* __restrict__ x, int H, int W, int C, int ldx,
+                                     int Hp, int Wp, __half* __restrict__ out)
+{
+    const int vecs = C / 8;
+    const long long total = static_cast<long long>(Hp) * Wp * vecs;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const long long pix = i / vecs;
+        const int v = static_cast<int>(i - pix * vecs);
+        const int h = static_cast<int>(pix / Wp);
+        const int w = static_cast<int>(pix - static_cast<long long>(h) * Wp);
+        const int sh = min(h, H - 1), sw = min(w, W - 1);
+        st8(out + pix * C + v * 8, ld8(x + (static_cast<long long>(sh) * W + sw) * ldx + v * 8));
+    }
+}
+
+__global__ void crop_kernel(const __half* __restrict__ x, int Wx, int ldx, int H, int W, int C,
+                            __half* __restrict__ out, int ldo)
+{
+    const int vecs = C / 8;
+    const long long total = static_cast<long long>(H) * W * vecs;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const long long pix = i / vecs;
+        const int v = static_cast<int>(i - pix * vecs);
+        const int h = static_cast<int>(pix / W);
+        const int w = static_cast<int>(pix - static_cast<long long>(h) * W);
+        st8(out + pix * ldo + v * 8, ld8(x + (static_cast<long long>(h) * Wx + w) * ldx + v * 8));
+    }
+}
+
+// ------------------------------------------------------------------------------ latents
+
+__global__ void round_z_kernel(const __half* __restrict__ z, int n, __half* __restrict__ z_hat,
+                               int8_t* __restrict__ z_i8)
+{
+    const __half lo = __float2half_rn(-64.f), hi = __float2half_rn(63.f);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        __half v = f2h(roundf(h2f(z[i])));
+        v = __hmax(v, lo);
+        v = __hmin(v, hi);
+        z_hat[i] = v;
+        z_i8[i] = static_cast<int8_t>(static_cast<int>(h2f(v)));
+    }
+}
+
+__global__ void int8_to_half_kernel(const int8_t* __restrict__ x, int n, __half* __restrict__ out)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        out[i] = f2h(static_cast<float>(x[i]));
+    }
+}
+
+__global__ void mul_channel_kernel(const __half* __restrict__ x, int M, int C, int ldx,
+                                   const __half* __restrict__ q, __half* __restrict__ out, int ldo)
+{
+    const int vecs = C / 8;
+    const long long total = static_cast<long long>(M) * vecs;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const long long m = i / vecs;
+        const int v = static_cast<int>(i - m * vecs);
+        Vec8h a = ld8(x + m * ldx + v * 8);
+        const Vec8h b = ld8(q + v * 8);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            a.v[j] = hmul(a.v[j], b.v[j]);
+        }
+        st8(out + m * ldo + v * 8, a);
+    }
+}
+
+__global__ void div_clamp_kernel(__half* __restrict__ y, int M, int C, int ldy,
+                                 const __half* __restrict__ q, int ldq)
+{
+    const int vecs = C / 8;
+    const long long total = static_cast<long long>(M) * vecs;
+    const __half half_ = __float2half_rn(0.5f);
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const long long m = i / vecs;
+        const int v = static_cast<int>(i - m * vecs);
+        Vec8h a = ld8(y + m * ldy + v * 8);
+        const Vec8h b = ld8(q + m * ldq + v * 8);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const __half qc = __hmax(b.v[j], half_);
+            const __half r = f2h(__fdiv_rn(1.0f, h2f(qc)));
+            a.v[j] = hmul(a.v[j], r);
+        }
+        st8(y + m * ldy + v * 8, a);
+    }
+}
+
+// ------------------------------------------------------------------------------ quantisation
+
+template <int MODE>
+__global__ void quantize_phase_kernel(int phase, const __half* __restrict__ y, int ldy,
+                                      const __half* __restrict__ scales, int lds,
+                                      const __half* __restrict__ means, int ldm,
+                                      const __half* __restrict__ q_dec, int ldd, __half thr,
+                                      __half* __restrict__ y_q, int ldq, __half* __restrict__ y_hat,
+                                      int ldh, int H, int W, int C)
+{
+    const int vecs = C / 8;
+    const int quarter_vecs = vecs / 4;
+    const long long total = static_cast<long long>(H) * W * vecs;
+    const __half qmin = __float2half_rn(-128.f), qmax = __float2half_rn(127.f);
+    const __half half_ = __float2half_rn(0.5f);
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const long long m = i / vecs;
+        const int v = static_cast<int>(i - m * vecs);
+        const int h = static_cast<int>(m / W);
+        const int w = static_cast<int>(m - static_cast<long long>(h) * W);
+        const bool on = ((h & 1) * 2 + (w & 1)) == mask_position(phase, v / quarter_vecs);
+        const Vec8h yy = ld8(y + m * ldy + v * 8);
+        const Vec8h ss = ld8(scales + m * lds + v * 8);
+        const Vec8h mm = ld8(means + m * ldm + v * 8);
+        Vec8h oq, oh, pq, ph, qd;
+        if (MODE >= 1) {
+            pq = ld8(y_q + m * ldq + v * 8);
+            ph = ld8(y_hat + m * ldh + v * 8);
+        }
+        if (MODE == 2) {
+            qd = ld8(q_dec + m * ldd + v * 8);
+        }
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const __half s_hat = on ? ss.v[j] : hzero();
+            const __half m_hat = on ? mm.v[j] : hzero();
+            __half res = hsub(yy.v[j], m_hat);
+            res = on ? res : hzero();
+            __half q = f2h(roundf(h2f(res)));
+            q = __hgt(s_hat, thr) ? q : hzero();
+            q = __hmax(__hmin(q, qmax), qmin);
+            __half yh = hadd(q, m_hat);
+            if (MODE == 0) {
+                oq.v[j] = q;
+                oh.v[j] = yh;
+            } else {
+                oq.v[j] = hadd(pq.v[j], q);
+                yh = hadd(yh, ph.v[j]);
+                if (MODE == 2) {
+                    yh = hmul(yh, __hmax(qd.v[j], half_));
+                }
+                oh.v[j] = yh;
+            }
+        }
+        st8(y_q + m * ldq + v * 8, oq);
+        st8(y_hat + m * ldh + v * 8, oh);
+    }
+}
+
+template <int MODE>
+__global__ void restore_phase_kernel(int phase, const __half* __restrict__ y_q, int ldq,
+                                     const __half* __restrict__ means, int ldm,
+                                     const __half* __restrict__ q_dec, int ldd,
+                                     __half* __restrict__ y_hat, int ldh, int H, int W, int C)
+{
+    const int vecs = C / 8;
+    const int quarter_vecs = vecs / 4;
+    const long long total = static_cast<long long>(H) * W * vecs;
+    const __half half_ = __float2half_rn(0.5f);
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const long long m = i / vecs;
+        const int v = static_cast<int>(i - m * vecs);
+        const int h = static_cast<int>(m / W);
+        const int w = static_cast<int>(m - static_cast<long long>(h) * W);
+        const bool on = ((h & 1) * 2 + (w & 1)) == mask_position(phase, v / quarter_vecs);
+        const Vec8h qq = ld8(y_q + m * ldq + v * 8);
+        const Vec8h mm = ld8(means + m * ldm + v * 8);
+        Vec8h prev, qd, o;
+        if (MODE >= 1) {
+            prev = ld8(y_hat + m * ldh + v * 8);
+        }
+        if (MODE == 2) {
+            qd = ld8(q_dec + m * ldd + v * 8);
+        }
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            __half t = hadd(qq.v[j], mm.v[j]);
+            t = on ? t : hzero();
+            if (MODE >= 1) {
+                t = hadd(t, prev.v[j]);
+            }
+            if (MODE == 2) {
+                t = hmul(t, __hmax(qd.v[j], half_));
+            }
+            o.v[j] = t;
+        }
+        st8(y_hat + m * ldh + v * 8, o);
+    }
+}
+
+template <bool ENC>
+__global__ void build_index_kernel(const __half* __restrict__ y_q, int ldq,
+                                   const __half* __restrict__ scales, int lds, __half thr,
+                                   const uint8_t* __restrict__ lut, int M, int C,
+                                   int16_t* __restrict__ sym, uint8_t* __restrict__ idx_out,
+                                   uint8_t* __restrict__ cond)
+{
+    const int vecs = C / 8;
+    const long long total = static_cast<long long>(M) * vecs;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const long long m = i / vecs;
+        const int v = static_cast<int>(i - m * vecs);
+        const Vec8h ss = ld8(scales + m * lds + v * 8);
+        const long long n = m * C + v * 8;
+        uint8_t cnd[8];
+        uint8_t ix[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            ix[j] = __ldg(lut + __half_as_ushort(ss.v[j]));
+            cnd[j] = __hgt(ss.v[j], thr) ? 1 : 0;
+        }
+        *reinterpret_cast<uint2*>(cond + n) =
+            make_uint2(cnd[0] | (cnd[1] << 8) | (cnd[2] << 16) | (cnd[3] << 24),
+                       cnd[4] | (cnd[5] << 8) | (cnd[6] << 16) | (cnd[7] << 24));
+        if (ENC) {
+            const Vec8h qq = ld8(y_q + m * ldq + v * 8);
+            int16_t o[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int qv = __half2int_rd(qq.v[j]);
+                o[j] = static_cast<int16_t>(qv * 256 + ix[j]);
+            }
+            *reinterpret_cast<uint4*>(sym + n) = *reinterpret_cast<uint4*>(o);
+        } else {
+            *reinterpret_cast<uint2*>(idx_out + n) =
+                make_uint2(ix[0] | (ix[1] << 8) | (ix[2] << 16) | (ix[3] << 24),
+                           ix[4] | (ix[5] << 8) | (ix[6] << 16) | (ix[7] << 24));
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------ compaction
+
+constexpr int kCompactThreads = 1024;
+constexpr int kCompactPer = 8;
+constexpr int kCompactBlock = kCompactThreads * kCompactPer;
+
+__device__ __forceinline__ int load_cond8(const uint8_t* cond, int base, int n, uint8_t (&c)[8])
+{
+    int cnt = 0;
+    if (base + 8 <= n) {
+        const uint2 u = *reinterpret_cast<const uint2*>(cond + base);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            c[j] = (u.x >> (8 * j)) & 0xff;
+            c[4 + j] = (u.y >> (8 * j)) & 0xff;
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            c[j] = (base + j < n) ? cond[base + j] : 0;
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        cnt += c[j] != 0;
+    }
+    return cnt;
+}
+
+// Exclusive scan of one int per thread over a 1024-thread block; returns the block total.
+__device__ __forceinline__ int block_exclusive_scan(int x, int* warp_sums, int& excl)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int incl = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) {
+            incl += t;
+        }
+    }
+    if (lane == 31) {
+        warp_sums[warp] = incl;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        int ws = warp_sums[lane];
+        int wi = ws;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) {
+                wi += t;
+            }
+        }
+        warp_sums[lane] = wi - ws;  // exclusive per warp
+        if (lane == 31) {
+            warp_sums[32] = wi;
+        }
+    }
+    __syncthreads();
+    excl = warp_sums[warp] + incl - x;
+    return warp_sums[32];
+}
+
+__global__ void __launch_bounds__(kCompactThreads) compact_count_kernel(const uint8_t* __restrict__ cond,
+                                                                        int n, int* __restrict__ counts)
+{
+    __shared__ int ws[33];
+    uint8_t c[8];
+    const int base = blockIdx.x * kCompactBlock + threadIdx.x * kCompactPer;
+    const int cnt = load_cond8(cond, base, n, c);
+    int excl;
+    const int tot = block_exclusive_scan(cnt, ws, excl);
+    if (threadIdx.x == 0) {
+        counts[blockIdx.x] = tot;
+    }
+}
+
+// Sum of counts[0, b) by one warp; the caller's warp 0 broadcasts it through shared memory.
+__device__ __forceinline__ int prefix_of_blocks(const int* counts, int b)
+{
+    int s = 0;
+    for (int i = threadIdx.x & 31; i < b; i += 32) {
+        s += counts[i];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        s += __shfl_xor_sync(0xffffffffu, s, o);
+    }
+    return s;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kCompactThreads)
+    compact_scatter_kernel(const T* __restrict__ src, const uint8_t* __restrict__ cond, int n,
+                           const int* __restrict__ counts, T* __restrict__ dst,
+                           int* __restrict__ total)
+{
+    __shared__ int ws[33];
+    __shared__ int block_off;
+    if (threadIdx.x < 32) {
+        const int s = prefix_of_blocks(counts, blockIdx.x);
+        if (threadIdx.x == 0) {
+            block_off = s;
+            if (blockIdx.x == gridDim.x - 1) {
+                *total = s + counts[blockIdx.x];
+            }
+        }
+    }
+    uint8_t c[8];
+    const int base = blockIdx.x * kCompactBlock + threadIdx.x * kCompactPer;
+    const int cnt = load_cond8(cond, base, n, c);
+    int excl;
+    block_exclusive_scan(cnt, ws, excl);  // contains __syncthreads, publishes block_off
+    int pos = block_off + excl;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        if (c[j]) {
+            dst[pos++] = src[base + j];
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kCompactThreads)
+    recover_kernel(const int8_t* __restrict__ dec, const uint8_t* __restrict__ cond,
+                   const int* __restrict__ counts, int n, __half* __restrict__ out)
+{
+    __shared__ int ws[33];
+    __shared__ int block_off;
+    if (threadIdx.x < 32) {
+        const int s = prefix_of_blocks(counts, blockIdx.x);
+        if (threadIdx.x == 0) {
+            block_off = s;
+        }
+    }
+    uint8_t c[8];
+    const int base = blockIdx.x * kCompactBlock + threadIdx.x * kCompactPer;
+    const int cnt = load_cond8(cond, base, n, c);
+    int excl;
+    block_exclusive_scan(cnt, ws, excl);
+    int pos = block_off + excl;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        if (base + j < n) {
+            out[base + j] = c[j] ? f2h(static_cast<float>(dec[pos++])) : hzero();
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------ depthwise
+
+__global__ void dwconv3x3_kernel(const __half* __restrict__ x, int H, int W, int C, int ldx,
+                                 const float* __restrict__ wt, __half* __restrict__ out, int ldo)
+{
+    const int vecs = C / 8;
+    const long long total = static_cast<long long>(H) * W * vecs;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const long long pix = i / vecs;
+        const int v = static_cast<int>(i - pix * vecs);
+        const int h = static_cast<int>(pix / W);
+        const int w = static_cast<int>(pix - static_cast<long long>(h) * W);
+        float acc[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            acc[j] = 0.f;
+        }
+#pragma unroll
+        for (int ky = 0; ky < 3; ++ky) {
+            const int hh = h + ky - 1;
+            if (hh < 0 || hh >= H) {
+                continue;
+            }
+#pragma unroll
+            for (int kx = 0; kx < 3; ++kx) {
+                const int ww = w + kx - 1;
+                if (ww < 0 || ww >= W) {
+                    continue;
+                }
+                const Vec8h a = ld8(x + (static_cast<long long>(hh) * W + ww) * ldx + v * 8);
+                const float4* wp = reinterpret_cast<const float4*>(wt + (ky * 3 + kx) * C + v * 8);
+                const float4 w0 = __ldg(wp), w1 = __ldg(wp + 1);
+                acc[0] = fmaf(h2f(a.v[0]), w0.x, acc[0]);
+                acc[1] = fmaf(h2f(a.v[1]), w0.y, acc[1]);
+                acc[2] = fmaf(h2f(a.v[2]), w0.z, acc[2]);
+                acc[3] = fmaf(h2f(a.v[3]), w0.w, acc[3]);
+                acc[4] = fmaf(h2f(a.v[4]), w1.x, acc[4]);
+                acc[5] = fmaf(h2f(a.v[5]), w1.y, acc[5]);
+                acc[6] = fmaf(h2f(a.v[6]), w1.z, acc[6]);
+                acc[7] = fmaf(h2f(a.v[7]), w1.w, acc[7]);
+            }
+        }
+        Vec8h o;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            o.v[j] = f2h(acc[j]);
+        }
+        st8(out + pix * ldo + v * 8, o);
+    }
+}
+
+inline bool al16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
+}  // namespace
+
+cudaError_t launch_pad_unshuffle8(const __half* x, int H, int W, int C, int ldx, int pad_b,
+                                  int pad_r, __half* out, int ldo, cudaStream_t s)
+{
+    if (H <= 0 || W <= 0 || (H + pad_b) % 8 || (W + pad_r) % 8 || pad_b < 0 || pad_r < 0 ||
+        ldo % 8 || !al16(out)) {
+        return cudaErrorInvalidValue;
+    }
+    const int H8 = (H + pad_b) / 8, W8 = (W + pad_r) / 8;
+    pad_unshuffle8_kernel<<<grid_for(static_cast<long long>(H8) * W8 * C * 8), kThreads, 0, s>>>(
+        x, H, W, C, ldx, H8, W8, out, ldo);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_shuffle8_clamp(const __half* in, int H8, int W8, int C, int ldi, __half* out,
+                                  cudaStream_t s)
+{
+    if (H8 <= 0 || W8 <= 0 || C <= 0) {
+        return cudaErrorInvalidValue;
+    }
+    shuffle8_clamp_kernel<<<grid_for(64LL * H8 * W8), kThreads, 0, s>>>(in, H8, W8, C, ldi, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_space_to_depth2(const __half* x, int H, int W, int C, int ldx, __half* out,
+                                   cudaStream_t s)
+{
+    if (H % 2 || W % 2 || C % 8 || ldx % 8 || !al16(x) || !al16(out)) {
+        return cudaErrorInvalidValue;
+    }
+    space_to_depth2_kernel<<<grid_for(static_cast<long long>(H / 2) * (W / 2) * C / 2), kThreads, 0,
+                             s>>>(x, H, W, C, ldx, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_im2col3x3s2(const __half* x, int H, int W, int C, int ldx, __half* out,
+                               cudaStream_t s)
+{
+    if (H % 2 || W % 2 || C % 8 || ldx % 8 || !al16(x) || !al16(out)) {
+        return cudaErrorInvalidValue;
+    }
+    im2col3x3s2_kernel<<<grid_for(static_cast<long long>(H / 2) * (W / 2) * 9 * (C / 8)),
+                         kThreads, 0, s>>>(x, H, W, C, ldx, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_replicate_pad(const __half* x, int H, int W, int C, int ldx, int pad_b,
+                                 int pad_r, __half* out, cudaStream_t s)
+{
+    if (C % 8 || ldx % 8 || pad_b < 0 || pad_r < 0 || !al16(x) || !al16(out)) {
+        return cudaErrorInvalidValue;
+    }
+    const int Hp = H + pad_b, Wp = W + pad_r;
+    replicate_pad_kernel<<<grid_for(static_cast<long long>(Hp) * Wp * (C / 8)), kThreads, 0, s>>>(
+        x, H, W, C, ldx, Hp, Wp, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_crop(const __half* x, int Wx, int ldx, int H, int W, int C, __half* out,
+                        int ldo, cudaStream_t s)
+{
+    if (C % 8 || ldx % 8 || ldo % 8 || W > Wx || !al16(x) || !al16(out)) {
+        return cudaErrorInvalidValue;
+    }
+    crop_kernel<<<grid_for(static_cast<long long>(H) * W * (C / 8)), kThreads, 0, s>>>(
+        x, Wx, ldx, H, W, C, out, ldo);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_round_z(const __half* z, int n, __half* z_hat, int8_t* z_i8, cudaStream_t s)
+{
+    if (n <= 0) {
+        return cudaErrorInvalidValue;
+    }
+    round_z_kernel<<<grid_for(n), kThreads, 0, s>>>(z, n, z_hat, z_i8);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_int8_to_half(const int8_t* x, int n, __half* out, cudaStream_t s)
+{
+    if (n <= 0) {
+        return cudaErrorInvalidValue;
+    }
+    int8_to_half_kernel<<<grid_for(n), kThreads, 0, s>>>(x, n, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mul_channel(const __half* x, int M, int C, int ldx, const __half* q,
+                               __half* out, int ldo, cudaStream_t s)
+{
+    if (C % 8 || ldx % 8 || ldo % 8 || !al16(x) || !al16(q) || !al16(out)) {
+        return cudaErrorInvalidValue;
+    }
+    mul_channel_kernel<<<grid_for(static_cast<long long>(M) * (C / 8)), kThreads, 0, s>>>(
+        x, M, C, ldx, q, out, ldo);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_div_clamp(__half* y, int M, int C, int ldy, const __half* q, int ldq,
+                             cudaStream_t s)
+{
+    if (C % 8 || ldy % 8 || ldq % 8 || !al16(y) || !al16(q)) {
+        return cudaErrorInvalidValue;
+    }
+    div_clamp_kernel<<<grid_for(static_cast<long long>(M) * (C / 8)), kThreads, 0, s>>>(y, M, C,
+                                                                                          ldy, q, ldq);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_quantize_phase(int phase, int mode, const __half* y, int ldy,
+                                  const __half* scales, int lds, const __half* means, int ldm,
+                                  const __half* q_dec, int ldd, __half thr, __half* y_q,
+                                  int ldq, __half* y_hat, int ldh, int H, int W, int C,
+                                  cudaStream_t s)
+{
+    if (phase < 0 || phase > 3 || C % 32 || (mode == 2 && q_dec == nullptr) || mode < 0 ||
+        mode > 2) {
+        return cudaErrorInvalidValue;
+    }
+    const int g = grid_for(static_cast<long long>(H) * W * (C / 8));
+    if (mode == 0) {
+        quantize_phase_kernel<0><<<g, kThreads, 0, s>>>(phase, y, ldy, scales, lds, means, ldm,
+                                                        q_dec, ldd, thr, y_q, ldq, y_hat, ldh, H,
+                                                        W, C);
+    } else if (mode == 1) {
+        quantize_phase_kernel<1><<<g, kThreads, 0, s>>>(phase, y, ldy, scales, lds, means, ldm,
+                                                        q_dec, ldd, thr, y_q, ldq, y_hat, ldh, H,
+                                                        W, C);
+    } else {
+        quantize_phase_kernel<2><<<g, kThreads, 0, s>>>(phase, y, ldy, scales, lds, means, ldm,
+                                                        q_dec, ldd, thr, y_q, ldq, y_hat, ldh, H,
+                                                        W, C);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_restore_phase(int phase, int mode, const __half* y_q, int ldq,
+                                 const __half* means, int ldm, const __half* q_dec, int ldd,
+                                 __half* y_hat, int ldh, int H, int W, int C, cudaStream_t s)
+{
+    if (phase < 0 || phase > 3 || C % 32 || (mode == 2 && q_dec == nullptr) || mode < 0 ||
+        mode > 2) {
+        return cudaErrorInvalidValue;
+    }
+    const int g = grid_for(static_cast<long long>(H) * W * (C / 8));
+    if (mode == 0) {
+        restore_phase_kernel<0><<<g, kThreads, 0, s>>>(phase, y_q, ldq, means, ldm, q_dec, ldd,
+                                                       y_hat, ldh, H, W, C);
+    } else if (mode == 1) {
+        restore_phase_kernel<1><<<g, kThreads, 0, s>>>(phase, y_q, ldq, means, ldm, q_dec, ldd,
+                                                       y_hat, ldh, H, W, C);
+    } else {
+        restore_phase_kernel<2><<<g, kThreads, 0, s>>>(phase, y_q, ldq, means, ldm, q_dec, ldd,
+                                                       y_hat, ldh, H, W, C);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_build_index_enc(const __half* y_q, int ldq, const __half* scales, int lds,
+                                   __half thr, const uint8_t* lut, int M, int C, int16_t* sym,
+                                   uint8_t* cond, cudaStream_t s)
+{
+    if (C % 8 || !al16(sym) || (reinterpret_cast<uintptr_t>(cond) & 7)) {
+        return cudaErrorInvalidValue;
+    }
+    build_index_kernel<true><<<grid_for(static_cast<long long>(M) * (C / 8)), kThreads, 0, s>>>(
+        y_q, ldq, scales, lds, thr, lut, M, C, sym, nullptr, cond);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_build_index_dec(const __half* scales, int lds, __half thr,
+                                   const uint8_t* lut, int M, int C, uint8_t* idx, uint8_t* cond,
+                                   cudaStream_t s)
+{
+    if (C % 8 || (reinterpret_cast<uintptr_t>(idx) & 7) || (reinterpret_cast<uintptr_t>(cond) & 7)) {
+        return cudaErrorInvalidValue;
+    }
+    build_index_kernel<false><<<grid_for(static_cast<long long>(M) * (C / 8)), kThreads, 0, s>>>(
+        nullptr, 0, scales, lds, thr, lut, M, C, nullptr, idx, cond);
+    return cudaGetLastError();
+}
+
+int compact_blocks(int n) { return (n + kCompactBlock - 1) / kCompactBlock; }
+
+cudaError_t launch_compact(const void* src, int elem_bytes, const uint8_t* cond, int n,
+                           int* block_counts, void* dst, int* total, cudaStream_t s)
+{
+    if (n <= 0 || (elem_bytes != 1 && elem_bytes != 2) || (reinterpret_cast<uintptr_t>(cond) & 7)) {
+        return cudaErrorInvalidValue;
+    }
+    const int nb = compact_blocks(n);
+    compact_count_kernel<<<nb, kCompactThreads, 0, s>>>(cond, n, block_counts);
+    if (elem_bytes == 1) {
+        compact_scatter_kernel<uint8_t><<<nb, kCompactThreads, 0, s>>>(
+            static_cast<const uint8_t*>(src), cond, n, block_counts, static_cast<uint8_t*>(dst),
+            total);
+    } else {
+        compact_scatter_kernel<int16_t><<<nb, kCompactThreads, 0, s>>>(
+            static_cast<const int16_t*>(src), cond, n, block_counts, static_cast<int16_t*>(dst),
+            total);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_recover(const int8_t* dec, const uint8_t* cond, const int* block_counts, int n,
+                           __half* out, cudaStream_t s)
+{
+    if (n <= 0 || (reinterpret_cast<uintptr_t>(cond) & 7)) {
+        return cudaErrorInvalidValue;
+    }
+    recover_kernel<<<compact_blocks(n), kCompactThreads, 0, s>>>(dec, cond, block_counts, n, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_dwconv3x3(const __half* x, int H, int W, int C, int ldx, const float* w,
+                             __half* out, int ldo, cudaStream_t s)
+{
+    if (C % 8 || ldx % 8 || ldo % 8 || !al16(x) || !al16(out) || !al16(w)) {
+        return cudaErrorInvalidValue;
+    }
+    dwconv3x3_kernel<<<grid_for(static_cast<long long>(H) * W * (C / 8)), kThreads, 0, s>>>(
+        x, H, W, C, ldx, w, out, ldo);
+    return cudaGetLastError();
+}
+
+}  // namespace dcvc

@@ -1,0 +1,110 @@
+// Elementwise, layout and quantisation kernels (NHWC, FP16) and their launchers.
+//
+// Arithmetic follows the reference's FP16 kernels op for op (src/layers/extensions/inference/
+// elementwise/stream.cu, cat_and_pad.cu, shuffle.cu): every FP16 op is computed in FP32 and
+// rounded once to FP16, which is what at::Half arithmetic does, so a NumPy float16
+// restatement reproduces the outputs bit for bit.
+#pragma once
+
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace dcvc {
+
+// Four-phase checkerboard masks of the spatial prior (src/models/common_model.py:175-195,
+// dmc_hts_proxy.cpp:869-890): in phase p, channel quarter q is coded at the 2x2 position
+// (h%2)*2 + (w%2) == q ^ kMaskPerm[p].
+__host__ __device__ __forceinline__ int mask_position(int phase, int quarter)
+{
+    const int perm[4] = {0, 3, 2, 1};
+    return quarter ^ perm[phase];
+}
+
+// pad_and_unshuffle_8 (cat_and_pad.cu:7-51) / pixel_unshuffle by 8 (shuffle.cu:134-185):
+// out[h8, w8, c*64 + dy*8 + dx] = x[min(8h8+dy, H-1), min(8w8+dx, W-1), c].
+cudaError_t launch_pad_unshuffle8(const __half* x, int H, int W, int C, int ldx, int pad_b,
+                                  int pad_r, __half* out, int ldo, cudaStream_t s);
+
+// pixel_shuffle_8 with clamp to [-0.5, 0.5] (shuffle.cu:40-131):
+// out[y, x, c] = clamp(in[y/8, x/8, c*64 + (y%8)*8 + x%8]).  out is [8*H8, 8*W8, C] dense.
+cudaError_t launch_shuffle8_clamp(const __half* in, int H8, int W8, int C, int ldi, __half* out,
+                                  cudaStream_t s);
+
+// out[(h, w), (dy*2 + dx)*C + c] = x[2h+dy, 2w+dx, c]   (pixel_unshuffle(2) with the channel
+// order permuted to (dy, dx, c); the stride-2 conv weight is permuted to match).
+cudaError_t launch_space_to_depth2(const __half* x, int H, int W, int C, int ldx, __half* out,
+                                   cudaStream_t s);
+
+// out[(ho, wo), (ky*3 + kx)*C + c] = x[2ho+ky-1, 2wo+kx-1, c] (zero outside): the patches of a
+// 3x3 stride-2 pad-1 convolution (conv_bias with kernel 3, conv_kernel.h:22-89).
+cudaError_t launch_im2col3x3s2(const __half* x, int H, int W, int C, int ldx, __half* out,
+                               cudaStream_t s);
+
+// replicate_pad (cat_and_pad.cu:53-84): out [H+pb, W+pr, C] dense.
+cudaError_t launch_replicate_pad(const __half* x, int H, int W, int C, int ldx, int pad_b,
+                                 int pad_r, __half* out, cudaStream_t s);
+
+// slice (cat_and_pad.cu:86-110): out[h, w, :] = x[h, w, :] for h < H, w < W; x has width Wx.
+cudaError_t launch_crop(const __half* x, int Wx, int ldx, int H, int W, int C, __half* out,
+                        int ldo, cudaStream_t s);
+
+// round_z (stream.cu:862-894): z_hat = clamp(round(z), -64, 63) as FP16 and int8.
+cudaError_t launch_round_z(const __half* z, int n, __half* z_hat, int8_t* z_i8, cudaStream_t s);
+
+// int8_to_dtype (stream.cu:454-482).
+cudaError_t launch_int8_to_half(const int8_t* x, int n, __half* out, cudaStream_t s);
+
+// multiply_with_broadcast (stream.cu:484-546): out[m, c] = x[m, c] * q[c].
+cudaError_t launch_mul_channel(const __half* x, int M, int C, int ldx, const __half* q,
+                               __half* out, int ldo, cudaStream_t s);
+
+// divide_with_clamp_inplace (stream.cu:422-452): y <- y * rcp(max(q, 0.5)), the reciprocal
+// rounded from FP32 1/q.
+cudaError_t launch_div_clamp(__half* y, int M, int C, int ldy, const __half* q, int ldq,
+                             cudaStream_t s);
+
+// process_with_mask_no_scale[_add_inplace][_add_and_multiply_inplace] (stream.cu:548-683) for
+// mask phase `phase` on an H x W grid.  mode 0: write y_q / y_hat; 1: accumulate;
+// 2: accumulate and scale y_hat by max(q_dec, 0.5).
+cudaError_t launch_quantize_phase(int phase, int mode, const __half* y, int ldy,
+                                  const __half* scales, int lds, const __half* means, int ldm,
+                                  const __half* q_dec, int ldd, __half thr, __half* y_q,
+                                  int ldq, __half* y_hat, int ldh, int H, int W, int C,
+                                  cudaStream_t s);
+
+// restore_y[_and_add_inplace][_and_add_multiply_inplace] (stream.cu:685-760).
+cudaError_t launch_restore_phase(int phase, int mode, const __half* y_q, int ldq,
+                                 const __half* means, int ldm, const __half* q_dec, int ldd,
+                                 __half* y_hat, int ldh, int H, int W, int C, cudaStream_t s);
+
+// build_index_enc (stream.cu:126-173): sym[m*C + c] = (q << 8) + idx, cond = scale > thr, in
+// NHWC symbol order.  idx comes from the 65536-entry table `lut` indexed by the FP16 bits of the
+// scale (see scale_index_table in quant_tables.cpp).
+cudaError_t launch_build_index_enc(const __half* y_q, int ldq, const __half* scales, int lds,
+                                   __half thr, const uint8_t* lut, int M, int C, int16_t* sym,
+                                   uint8_t* cond, cudaStream_t s);
+
+// build_index_dec (stream.cu:89-124).
+cudaError_t launch_build_index_dec(const __half* scales, int lds, __half thr,
+                                   const uint8_t* lut, int M, int C, uint8_t* idx, uint8_t* cond,
+                                   cudaStream_t s);
+
+// Order-preserving compaction of `src` (elem_bytes 1 or 2) under `cond` (conditional_index_part1,
+// stream.cu:175-338).  block_counts needs compact_blocks(n) ints; *total (device) receives the
+// number of kept elements.
+int compact_blocks(int n);
+cudaError_t launch_compact(const void* src, int elem_bytes, const uint8_t* cond, int n,
+                           int* block_counts, void* dst, int* total, cudaStream_t s);
+
+// conditional_recover_with_type_conversion (stream.cu:359-420): out[i] = cond[i] ? dec[rank(i)]
+// : 0, using the block counts written by launch_compact over the same cond.
+cudaError_t launch_recover(const int8_t* dec, const uint8_t* cond, const int* block_counts, int n,
+                           __half* out, cudaStream_t s);
+
+// Depthwise 3x3, pad 1, no bias (d3x3, cutlass/d3x3_kernel.h:104-166): FP32 accumulation in the
+// order ky, kx.  w is FP32 [9][C] (tap-major).
+cudaError_t launch_dwconv3x3(const __half* x, int H, int W, int C, int ldx, const float* w,
+                             __half* out, int ldo, cudaStream_t s);
+
+}  // namespace dcvc

@@ -1,0 +1,558 @@
+#include "rans_coder.h"
+
+#include <algorithm>
+#include <cstring>
+#include <thread>
+
+namespace dcvc {
+
+namespace {
+
+constexpr int kScaleBits = 16;
+constexpr uint32_t kRansL = 1u << 23;
+constexpr int kRenormShift = 23 - kScaleBits + 8;  // 15
+constexpr uint32_t kBypassMax = 3;                 // 2-bit bypass digits
+constexpr uint32_t kBypassXMax = (1u << (kScaleBits - 2)) << kRenormShift;
+
+// Sub-stream writer: bytes are produced back to front.
+struct Writer {
+    std::vector<uint8_t> buf;
+    size_t pos = 0;
+    uint32_t x = kRansL;
+    bool overflow = false;
+
+    void init(size_t cap)
+    {
+        buf.assign(cap, 0);
+        pos = cap;
+        x = kRansL;
+        overflow = false;
+    }
+    inline void byte(uint8_t b)
+    {
+        if (pos == 0) {
+            overflow = true;
+            return;
+        }
+        buf[--pos] = b;
+    }
+    inline void put(uint32_t start, uint32_t freq)
+    {
+        const uint32_t x_max = freq << kRenormShift;
+        while (x >= x_max) {
+            byte(static_cast<uint8_t>(x));
+            x >>= 8;
+        }
+        x = ((x / freq) << kScaleBits) + (x % freq) + start;
+    }
+    inline void bits(uint32_t v)
+    {
+        while (x >= kBypassXMax) {
+            byte(static_cast<uint8_t>(x));
+            x >>= 8;
+        }
+        x = (x << 2) | v;
+    }
+    inline void symbol(int32_t s, int32_t maxv, const uint32_t* enc)
+    {
+        int32_t v = (s < 0 ? -s : s) * 2 - (s > 0);
+        if (v >= maxv) {
+            const uint32_t raw = static_cast<uint32_t>(v - maxv);
+            uint32_t bins[40];
+            int nb = 0;
+            int digits = 0;
+            while (digits < 16 && (raw >> (digits * 2)) != 0) {
+                ++digits;
+            }
+            int32_t cnt = digits;
+            while (cnt >= static_cast<int32_t>(kBypassMax)) {
+                bins[nb++] = kBypassMax;
+                cnt -= kBypassMax;
+            }
+            bins[nb++] = static_cast<uint32_t>(cnt);
+            for (int j = 0; j < digits; ++j) {
+                bins[nb++] = (raw >> (2 * j)) & kBypassMax;
+            }
+            for (int j = nb - 1; j >= 0; --j) {
+                bits(bins[j]);
+            }
+            v = maxv;
+        }
+        const uint32_t e = enc[v];
+        put(e & 0xffff, e >> 16);
+    }
+    void flush()
+    {
+        for (int k = 3; k >= 0; --k) {
+            byte(static_cast<uint8_t>(x >> (8 * k)));
+        }
+    }
+    const uint8_t* data() const { return buf.data() + pos; }
+    int size() const { return static_cast<int>(buf.size() - pos); }
+};
+
+inline void split(int n, int parts, int i, int* begin, int* end)
+{
+    const int s = n / parts;
+    *begin = s * i;
+    *end = (i < parts - 1) ? *begin + s : n;
+}
+
+int shared_tail(const uint8_t* a, int na, const uint8_t* b, int nb)
+{
+    const int lim = std::min({na, nb, 8});
+    int k = 0;
+    for (int i = 0; i < lim; ++i) {
+        if (a[na - 1 - i] != 0 || b[nb - 1 - i] != 0) {
+            break;
+        }
+        ++k;
+    }
+    if (k == 0 && a[na - 1] == b[nb - 1]) {
+        k = 1;
+    }
+    return k;
+}
+
+template <typename F>
+void run_parallel(int n, F&& f)
+{
+    if (n == 1) {
+        f(0);
+        return;
+    }
+    std::vector<std::thread> th;
+    th.reserve(n - 1);
+    for (int i = 1; i < n; ++i) {
+        th.emplace_back([&f, i] { f(i); });
+    }
+    f(0);
+    for (auto& t : th) {
+        t.join();
+    }
+}
+
+}  // namespace
+
+int ec_parallel_for(int symbol_count)
+{
+    int n = symbol_count / kMinSymbolsPerStream;
+    return std::max(1, std::min(kMaxEcParallel, n));
+}
+
+std::vector<uint32_t> pmf_to_quantized_cdf(const float* pmf, int n)
+{
+    const uint32_t prob_max = 1u << 16;
+    const int m = n + 1;
+    std::vector<uint32_t> cdf(m, 0);
+    for (int i = 0; i < n; ++i) {
+        const float prod = pmf[i] * static_cast<float>(prob_max);
+        cdf[i + 1] = static_cast<uint32_t>(static_cast<double>(prod) + 0.5);
+    }
+    int total = 0;
+    for (int i = 0; i < m; ++i) {
+        total += static_cast<int>(cdf[i]);
+    }
+    if (total <= 0) {
+        return {};
+    }
+    for (int i = 0; i < m; ++i) {
+        cdf[i] = static_cast<uint32_t>((static_cast<uint64_t>(prob_max) * cdf[i]) /
+                                       static_cast<uint32_t>(total));
+    }
+    for (int i = 1; i < m; ++i) {
+        cdf[i] += cdf[i - 1];
+    }
+    cdf[m - 1] = prob_max;
+    for (int i = 0; i < m - 1; ++i) {
+        if (cdf[i] + 1 > cdf[i + 1]) {
+            uint32_t best_freq = ~0u;
+            int best = -1;
+            for (int j = 0; j < m - 1; ++j) {
+                const uint32_t f = cdf[j + 1] - cdf[j];
+                if (f >= 2 && f < best_freq) {
+                    best_freq = f;
+                    best = j;
+                }
+            }
+            if (best < 0) {
+                return {};
+            }
+            if (best < i) {
+                for (int j = best + 1; j <= i; ++j) {
+                    cdf[j] -= 1;
+                }
+            } else {
+                for (int j = i + 1; j <= best; ++j) {
+                    cdf[j] += 1;
+                }
+            }
+        }
+    }
+    return cdf;
+}
+
+bool RansTables::set(int index, const int32_t* cdf, const int32_t* lengths, int count, int stride,
+                     std::string* err)
+{
+    if (index < 0 || index > 1 || count <= 0 || stride < 3) {
+        *err = "rANS tables: bad index, count or stride";
+        return false;
+    }
+    RansTable t;
+    t.count = count;
+    t.stride = stride;
+    t.cdf.assign(cdf, cdf + static_cast<size_t>(count) * stride);
+    t.max_value.resize(count);
+    t.enc.assign(static_cast<size_t>(count) * stride, 0);
+    for (int i = 0; i < count; ++i) {
+        const int len = lengths[i];
+        if (len < 3 || len > stride) {
+            *err = "rANS tables: cdf length out of range";
+            return false;
+        }
+        t.max_value[i] = static_cast<int8_t>(len - 2);
+        const int32_t* c = t.cdf.data() + static_cast<size_t>(i) * stride;
+        for (int j = 0; j + 1 < stride; ++j) {
+            const uint32_t start = static_cast<uint16_t>(c[j]);
+            const uint32_t freq = static_cast<uint16_t>(c[j + 1] - c[j]);
+            t.enc[static_cast<size_t>(i) * stride + j] = start | (freq << 16);
+        }
+    }
+    t_[index] = std::move(t);
+    return true;
+}
+
+void RansEncoderSession::reset(int ec_parallel)
+{
+    ecp_ = ec_parallel;
+    segs_.clear();
+}
+
+void RansEncoderSession::add_y(const int16_t* sym, int n, bool copy)
+{
+    Segment s{};
+    s.is_y = true;
+    s.n = n;
+    if (copy) {
+        s.own_y.assign(sym, sym + n);
+        s.y = s.own_y.data();
+    } else {
+        s.y = sym;
+    }
+    segs_.push_back(std::move(s));
+    if (copy) {
+        segs_.back().y = segs_.back().own_y.data();
+    }
+}
+
+void RansEncoderSession::add_z(const int8_t* sym, int n, int cdf_offset, int ch, bool copy)
+{
+    Segment s{};
+    s.is_y = false;
+    s.n = n;
+    s.cdf_offset = cdf_offset;
+    s.ch = ch;
+    if (copy) {
+        s.own_z.assign(sym, sym + n);
+    } else {
+        s.z = sym;
+    }
+    segs_.push_back(std::move(s));
+    if (copy) {
+        segs_.back().z = segs_.back().own_z.data();
+    }
+}
+
+bool RansEncoderSession::finish(const RansTables& tables, std::vector<uint8_t>* out,
+                                std::string* err)
+{
+    if (!tables.ready()) {
+        *err = "rANS encode: tables not set";
+        return false;
+    }
+    const int ecp = ecp_;
+    if (ecp < 1 || ecp > kMaxEcParallel) {
+        *err = "rANS encode: ec_parallel must be in [1, 8]";
+        return false;
+    }
+    const RansTable& ty = tables.y();
+    const RansTable& tz = tables.z();
+    size_t cap[kMaxEcParallel] = {0};
+    for (const Segment& sg : segs_) {
+        if (sg.n < 0 || (!sg.is_y && (sg.ch < 1 || sg.cdf_offset < 0 ||
+                                      (sg.n > 0 && sg.cdf_offset + sg.ch > tz.count)))) {
+            *err = "rANS encode: bad segment arguments";
+            return false;
+        }
+        for (int i = 0; i < ecp; ++i) {
+            int b, e;
+            split(sg.n, ecp, i, &b, &e);
+            cap[i] += static_cast<size_t>(e - b) * 4;
+        }
+    }
+    Writer w[kMaxEcParallel];
+    bool bad_index[kMaxEcParallel] = {false};
+    run_parallel(ecp, [&](int i) {
+        w[i].init(cap[i] + 16);
+        for (const Segment& sg : segs_) {
+            int b, e;
+            split(sg.n, ecp, i, &b, &e);
+            if (sg.is_y) {
+                for (int k = e - 1; k >= b; --k) {
+                    const int16_t c = sg.y[k];
+                    const int idx = c & 0xff;
+                    if (idx >= ty.count) {
+                        bad_index[i] = true;
+                        return;
+                    }
+                    const int32_t s = static_cast<int8_t>(c >> 8);
+                    w[i].symbol(s, ty.max_value[idx],
+                                ty.enc.data() + static_cast<size_t>(idx) * ty.stride);
+                }
+            } else {
+                for (int k = e - 1; k >= b; --k) {
+                    const int t = (k % sg.ch) + sg.cdf_offset;
+                    w[i].symbol(sg.z[k], tz.max_value[t],
+                                tz.enc.data() + static_cast<size_t>(t) * tz.stride);
+                }
+            }
+        }
+        w[i].flush();
+    });
+    for (int i = 0; i < ecp; ++i) {
+        if (bad_index[i]) {
+            *err = "rANS encode: y symbol names a CDF table out of range";
+            return false;
+        }
+        if (w[i].overflow) {
+            *err = "rANS encode: sub-stream buffer overflow";
+            return false;
+        }
+    }
+    out->clear();
+    if (ecp == 1) {
+        out->assign(w[0].data(), w[0].data() + w[0].size());
+        return true;
+    }
+    const int pairs = ecp / 2;
+    const bool tail = (ecp % 2) != 0;
+    int same[kMaxEcParallel / 2], gsz[kMaxEcParallel / 2];
+    for (int p = 0; p < pairs; ++p) {
+        const Writer& a = w[2 * p];
+        const Writer& b = w[2 * p + 1];
+        same[p] = shared_tail(a.data(), a.size(), b.data(), b.size());
+        gsz[p] = a.size() + b.size() - same[p];
+    }
+    const int noff = pairs - 1 + (tail ? 1 : 0);
+    size_t total = static_cast<size_t>(noff) * 4;
+    for (int p = 0; p < pairs; ++p) {
+        total += gsz[p];
+    }
+    if (tail) {
+        total += w[ecp - 1].size();
+    }
+    out->resize(total);
+    uint8_t* o = out->data();
+    int32_t cum = gsz[0];
+    for (int k = 0; k < noff; ++k) {
+        std::memcpy(o + 4 * k, &cum, 4);
+        if (k + 1 < pairs) {
+            cum += gsz[k + 1];
+        }
+    }
+    size_t pos = static_cast<size_t>(noff) * 4;
+    for (int p = 0; p < pairs; ++p) {
+        const Writer& a = w[2 * p];
+        const Writer& b = w[2 * p + 1];
+        std::memcpy(o + pos, a.data(), a.size());
+        const int nb = b.size() - same[p];
+        std::reverse_copy(b.data(), b.data() + nb, o + pos + a.size());
+        pos += gsz[p];
+    }
+    if (tail) {
+        std::memcpy(o + pos, w[ecp - 1].data(), w[ecp - 1].size());
+    }
+    return true;
+}
+
+namespace {
+
+inline uint8_t rd_next(const uint8_t*& p, const uint8_t* end, bool& overrun)
+{
+    if (p >= end) {
+        overrun = true;
+        return 0;
+    }
+    return *p++;
+}
+
+inline uint32_t rd_bits(uint32_t& x, const uint8_t*& p, const uint8_t* end, bool& overrun)
+{
+    const uint32_t v = x & kBypassMax;
+    x >>= 2;
+    if (x < kRansL) {
+        x = (x << 8) | rd_next(p, end, overrun);
+    }
+    return v;
+}
+
+inline int8_t rd_symbol(uint32_t& x, const uint8_t*& p, const uint8_t* end, bool& overrun,
+                        const int32_t* cdf, int32_t maxv, int last)
+{
+    const uint32_t cum = x & ((1u << kScaleBits) - 1);
+    int s = 1;
+    while (s < last && static_cast<uint32_t>(cdf[s]) <= cum) {
+        ++s;
+    }
+    --s;
+    const uint32_t start = static_cast<uint32_t>(cdf[s]);
+    const uint32_t freq = static_cast<uint32_t>(cdf[s + 1] - cdf[s]);
+    x = freq * (x >> kScaleBits) + (x & ((1u << kScaleBits) - 1)) - start;
+    while (x < kRansL && !overrun) {
+        x = (x << 8) | rd_next(p, end, overrun);
+    }
+    int32_t v = s;
+    if (v == maxv) {
+        int32_t b = static_cast<int32_t>(rd_bits(x, p, end, overrun));
+        int32_t digits = b;
+        while (b == static_cast<int32_t>(kBypassMax) && digits < 64) {
+            b = static_cast<int32_t>(rd_bits(x, p, end, overrun));
+            digits += b;
+        }
+        int32_t raw = 0;
+        for (int j = 0; j < digits; ++j) {
+            const int32_t d = static_cast<int32_t>(rd_bits(x, p, end, overrun));
+            if (j < 16) {
+                raw |= d << (2 * j);
+            }
+        }
+        v = raw + maxv;
+    }
+    return static_cast<int8_t>((v % 2 == 1) ? (v + 1) / 2 : -(v + 1) / 2);
+}
+
+}  // namespace
+
+bool RansDecoderSession::begin(const uint8_t* data, int size, int ecp, std::string* err)
+{
+    ecp_ = 0;
+    if (ecp < 1 || ecp > kMaxEcParallel || size < 0 || (size > 0 && data == nullptr)) {
+        *err = "rANS decode: bad arguments";
+        return false;
+    }
+    if (ecp == 1) {
+        parts_[0].assign(data, data + size);
+    } else {
+        const int pairs = ecp / 2;
+        const bool tail = (ecp % 2) != 0;
+        const int noff = pairs - 1 + (tail ? 1 : 0);
+        if (size < noff * 4) {
+            *err = "rANS decode: stream shorter than its header";
+            return false;
+        }
+        int32_t off[kMaxEcParallel];
+        for (int k = 0; k < noff; ++k) {
+            std::memcpy(&off[k], data + 4 * k, 4);
+        }
+        const uint8_t* pay = data + noff * 4;
+        const int pay_n = size - noff * 4;
+        int prev = 0;
+        for (int k = 0; k < noff; ++k) {
+            if (off[k] < prev || off[k] > pay_n) {
+                *err = "rANS decode: inconsistent sub-stream offsets";
+                return false;
+            }
+            prev = off[k];
+        }
+        for (int p = 0; p < pairs; ++p) {
+            const int g0 = (p == 0) ? 0 : off[p - 1];
+            const int g1 = (p < noff) ? off[p] : (tail ? off[noff - 1] : pay_n);
+            parts_[2 * p].assign(pay + g0, pay + g1);
+            parts_[2 * p + 1].assign(parts_[2 * p].rbegin(), parts_[2 * p].rend());
+        }
+        if (tail) {
+            parts_[ecp - 1].assign(pay + off[noff - 1], pay + pay_n);
+        }
+    }
+    for (int i = 0; i < ecp; ++i) {
+        Reader& r = r_[i];
+        r.p = parts_[i].data();
+        r.end = r.p + parts_[i].size();
+        r.overrun = false;
+        r.x = 0;
+        for (int k = 0; k < 4; ++k) {
+            r.x |= static_cast<uint32_t>(rd_next(r.p, r.end, r.overrun)) << (8 * k);
+        }
+    }
+    ecp_ = ecp;
+    return true;
+}
+
+bool RansDecoderSession::decode_z(const RansTables& tables, int n, int cdf_offset, int ch,
+                                  int8_t* out, std::string* err)
+{
+    const RansTable& tz = tables.z();
+    if (ecp_ == 0 || tz.count == 0 || n < 0 || ch < 1 || cdf_offset < 0 ||
+        (n > 0 && cdf_offset + ch > tz.count)) {
+        *err = "rANS decode_z: bad arguments or no stream";
+        return false;
+    }
+    run_parallel(ecp_, [&](int i) {
+        Reader& r = r_[i];
+        int b, e;
+        split(n, ecp_, i, &b, &e);
+        for (int k = b; k < e; ++k) {
+            const int t = (k % ch) + cdf_offset;
+            out[k] = rd_symbol(r.x, r.p, r.end, r.overrun,
+                               tz.cdf.data() + static_cast<size_t>(t) * tz.stride, tz.max_value[t],
+                               tz.stride - 1);
+        }
+    });
+    for (int i = 0; i < ecp_; ++i) {
+        if (r_[i].overrun) {
+            *err = "rANS decode: sub-stream ran past its bytes (truncated or corrupt stream)";
+            return false;
+        }
+    }
+    return true;
+}
+
+bool RansDecoderSession::decode_y(const RansTables& tables, const uint8_t* idx, int n,
+                                  int8_t* out, std::string* err)
+{
+    const RansTable& ty = tables.y();
+    if (ecp_ == 0 || ty.count == 0 || n < 0) {
+        *err = "rANS decode_y: bad arguments or no stream";
+        return false;
+    }
+    bool bad[kMaxEcParallel] = {false};
+    run_parallel(ecp_, [&](int i) {
+        Reader& r = r_[i];
+        int b, e;
+        split(n, ecp_, i, &b, &e);
+        for (int k = b; k < e; ++k) {
+            const int t = idx[k];
+            if (t >= ty.count) {
+                bad[i] = true;
+                return;
+            }
+            out[k] = rd_symbol(r.x, r.p, r.end, r.overrun,
+                               ty.cdf.data() + static_cast<size_t>(t) * ty.stride, ty.max_value[t],
+                               ty.stride - 1);
+        }
+    });
+    for (int i = 0; i < ecp_; ++i) {
+        if (bad[i]) {
+            *err = "rANS decode: y index names a CDF table out of range";
+            return false;
+        }
+        if (r_[i].overrun) {
+            *err = "rANS decode: sub-stream ran past its bytes (truncated or corrupt stream)";
+            return false;
+        }
+    }
+    return true;
+}
+
+}  // namespace dcvc

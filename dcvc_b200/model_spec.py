@@ -1,0 +1,157 @@
+"""Parameter layout and seeded initialisation of the DCVC-UF HT-S video model and the intra model.
+
+The module tree mirrors the reference's nn.Module structure (src/models/video_model_ht.py:26-
+351, src/layers/layers.py:92-188, src/models/image_model.py:15-140) only as far as parameter
+names, shapes, registration order and initialisation go: building it under
+torch.manual_seed(s) consumes the random stream exactly as the reference constructor does
+(default Conv2d init, then BitEstimator normals, then xavier_normal_ over modules(),
+common_model.py:49-54), so `hts_state_dict(seed)` equals the reference `DMC().state_dict()`
+for the same seed.  There is no forward here: the codec runs in libdcvc_b200.so.
+"""
+import torch
+from torch import nn
+
+# HT-S sizes (video_model_ht.py:16-23)
+FRAME_DELAY = 8
+CH_SRC_INTRA = 3 * 8 * 8
+CH_SRC = CH_SRC_INTRA * FRAME_DELAY
+CH_Y = 256
+CH_Z = 128
+CH_D = 512
+CH_M = 512
+CH_RECON = 256
+QP_NUM = 64
+
+
+class _Act(nn.Module):
+    """Parameter-free placeholder (WSiLU / WSiLUChunkAdd / PixelShuffle) keeping indices aligned."""
+
+
+class DCB(nn.Module):
+    """DepthConvBlock parameters (layers.py:128-159)."""
+
+    def __init__(self, in_ch, out_ch, dcb2=False, force_adaptor=False):
+        super().__init__()
+        self.adaptor = nn.Conv2d(in_ch, out_ch, 1) if (in_ch != out_ch or force_adaptor) else None
+        r = 2 if dcb2 else 1
+        self.dc = nn.Sequential(
+            nn.Conv2d(out_ch, out_ch // r, 1), _Act(),
+            nn.Conv2d(out_ch // r, out_ch // r, 3, padding=1, groups=out_ch // r),
+            nn.Conv2d(out_ch // r, out_ch, 1))
+        self.ffn = nn.Sequential(nn.Conv2d(out_ch, out_ch * 4 // r, 1), _Act(),
+                                 nn.Conv2d(out_ch // r, out_ch, 1))
+
+
+class Subpel(nn.Module):
+    """SubpelConv2x (layers.py:92-103)."""
+
+    def __init__(self, in_ch, out_ch, k=1, padding=0, force_bias=False):
+        super().__init__()
+        self.conv = nn.Sequential(
+            nn.Conv2d(in_ch, out_ch * 4, k, padding=padding, bias=(k > 1) or force_bias), _Act())
+
+
+class RBUp(nn.Module):
+    """ResidualBlockUpsample (layers.py:162-173)."""
+
+    def __init__(self, in_ch, out_ch, dcb2=False, force_bias=False):
+        super().__init__()
+        self.up = Subpel(in_ch, out_ch, 1, force_bias=force_bias)
+        self.conv = DCB(out_ch, out_ch, dcb2=dcb2)
+
+
+class RBDown(nn.Module):
+    """ResidualBlockWithStride2 (layers.py:176-188)."""
+
+    def __init__(self, in_ch, out_ch, dcb2=False):
+        super().__init__()
+        self.down = nn.Conv2d(in_ch * 4, out_ch, 1)
+        self.conv = DCB(out_ch, out_ch, dcb2=dcb2)
+
+
+class BitEstimator(nn.Module):
+    """entropy_models.py:103-113."""
+
+    def __init__(self, qp_num, channel):
+        super().__init__()
+        self.h = nn.Parameter(nn.init.normal_(torch.empty([qp_num, channel, 4]), 0, 0.01))
+        self.b = nn.Parameter(nn.init.normal_(torch.empty([qp_num, channel, 4]), 0, 0.01))
+        self.a = nn.Parameter(nn.init.normal_(torch.empty([qp_num, channel, 3]), 0, 0.01))
+
+
+def _seq(*mods):
+    return nn.Sequential(*mods)
+
+
+class _Wrap(nn.Module):
+    def __init__(self, **kw):
+        super().__init__()
+        for k, v in kw.items():
+            setattr(self, k, v)
+
+
+def _init_xavier(model):
+    for m in model.modules():
+        if isinstance(m, nn.Conv2d):
+            nn.init.xavier_normal_(m.weight, 1.)
+            if m.bias is not None:
+                nn.init.constant_(m.bias, 0.)
+
+
+class HTSModel(nn.Module):
+    """Parameter tree of DMC(ModelStructure.HTS) (video_model_ht.py:320-351)."""
+
+    def __init__(self):
+        super().__init__()
+        self.bit_estimator_z = BitEstimator(QP_NUM, CH_Z)
+        d = lambda i, o: DCB(i, o, dcb2=True)  # noqa: E731
+        self.feature_adaptor_i = _Wrap(conv=_seq(d(CH_SRC_INTRA, CH_M), *[d(CH_M, CH_M) for _ in range(3)]))
+        self.feature_adaptor_m = _Wrap(conv=_seq(d(CH_M + CH_D, CH_M), *[d(CH_M, CH_M) for _ in range(5)]))
+        self.feature_extractor = _Wrap(conv=_seq(d(CH_M, CH_D), *[d(CH_D, CH_D) for _ in range(4)]))
+        enc = _Wrap(conv1=_seq(d(CH_SRC + CH_D, CH_D), *[d(CH_D, CH_D) for _ in range(5)]))
+        enc.down = nn.Conv2d(CH_D, CH_Y, 3, stride=2, padding=1)
+        self.encoder = enc
+        self.hyper_encoder = _Wrap(conv=_seq(DCB(CH_Y, CH_Y), RBDown(CH_Y, CH_Y), RBDown(CH_Y, CH_Z)))
+        self.hyper_decoder = _Wrap(conv=_seq(RBUp(CH_Z, CH_Y), RBUp(CH_Y, CH_Y), DCB(CH_Y, CH_Y)))
+        self.temporal_prior_encoder = _Wrap(conv=RBDown(CH_D, CH_Y * 2))
+        pf = [DCB(CH_Y * 3, CH_Y * 3) for _ in range(3)]
+        self.y_prior_fusion = _Wrap(conv=_seq(*pf, nn.Conv2d(CH_Y * 3, CH_Y * 3, 1)))
+        self.y_spatial_prior_reduction = nn.Conv2d(CH_Y * 3, CH_Y, 1)
+        for k in (1, 2, 3):
+            setattr(self, f"y_spatial_prior_adaptor_{k}", DCB(CH_Y * 2, CH_Y * 2, force_adaptor=True))
+        sp = [DCB(CH_Y * 2, CH_Y * 2) for _ in range(3)]
+        self.y_spatial_prior = _Wrap(conv=_seq(*sp, nn.Conv2d(CH_Y * 2, CH_Y, 1)))
+        dec = _Wrap(up=Subpel(CH_Y, CH_D, 1))
+        dec.conv1 = _seq(d(CH_D * 2, CH_D), *[d(CH_D, CH_D) for _ in range(6)])
+        self.decoder = dec
+        rh = _Wrap(conv1=nn.ModuleList([_seq(DCB(CH_D, CH_D)) for _ in range(FRAME_DELAY // 2)]))
+        rh.conv2 = nn.ModuleList([
+            _seq(DCB(CH_D, CH_RECON), DCB(CH_RECON, CH_RECON), DCB(CH_RECON, CH_RECON),
+                 nn.Conv2d(CH_RECON, CH_SRC_INTRA, 1)) for _ in range(FRAME_DELAY)])
+        self.recon_head = rh
+        self.q_encoder = nn.Parameter(torch.ones((QP_NUM, CH_D)))
+        self.q_decoder = nn.Parameter(torch.ones((QP_NUM, CH_D)))
+        self.q_feature = nn.Parameter(torch.ones((QP_NUM, CH_D)))
+        _init_xavier(self)
+
+
+def hts_state_dict(seed=0, dtype=torch.float32):
+    """State dict of a random-init HT-S model, equal to the reference DMC() under
+    torch.manual_seed(seed) (fp32 CPU; cast to `dtype`)."""
+    state = torch.random.get_rng_state()
+    try:
+        torch.manual_seed(seed)
+        model = HTSModel()
+    finally:
+        torch.random.set_rng_state(state)
+    return {k: v.detach().to(dtype) for k, v in model.state_dict().items()}
+
+
+def perturbed_hts_state_dict(seed=0, dtype=torch.float32, q_jitter=0.25):
+    """Seed-`seed` weights with non-trivial per-QP quant vectors (the random init sets them to
+    ones, which hides QP dependence); used by tests that must see QP-specific behaviour."""
+    sd = hts_state_dict(seed, torch.float32)
+    g = torch.Generator().manual_seed(seed + 17)
+    for k in ("q_encoder", "q_decoder", "q_feature"):
+        sd[k] = 1.0 + q_jitter * (torch.rand(sd[k].shape, generator=g) * 2 - 1)
+    return {k: v.to(dtype) for k, v in sd.items()}

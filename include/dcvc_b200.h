@@ -76,6 +76,41 @@ int dcvc_conv1x1(int dtype, int epilogue, int M, int N, int K, const void* a, in
                  int ldr2, const void* qscale, void* out, int ldo, int sub_w, int sub_cout,
                  int block_n, void* stream);
 
+/* ------------------------------------------------------------------ rANS coder (host) */
+
+/* pmf -> 16-bit quantised CDF, writes n + 1 entries.
+ * Replaces pmf_to_quantized_cdf (src/cpp/py_rans/py_rans.h:17, py_rans.cpp:35-94). */
+int dcvc_pmf_to_quantized_cdf(const float* pmf, int n, uint32_t* cdf_out);
+
+/* ec_parallel for a symbol count: clamp(count / 32768, 1, 8)
+ * (src/layers/extensions/inference/dmc_common.cpp:31-35). */
+int dcvc_ec_parallel_for(int symbol_count);
+
+/* A coder handle owns two CDF table sets (index 0: z / bit estimator, index 1: y / Gaussian),
+ * one payload being encoded and one being decoded.  Not thread-safe; one handle per thread.
+ * Replaces RansEncoder / RansDecoder (src/cpp/py_rans/py_rans.h:21-76, bind.cpp:14-40); the
+ * bytes are identical to the reference coder's for the same symbols, tables and ec_parallel. */
+int dcvc_rans_create(void** handle);
+int dcvc_rans_destroy(void* handle);
+/* cdf: [count, stride] int32, lengths: [count] (RansEncoder::set_cdf, py_rans.cpp:262-303) */
+int dcvc_rans_set_cdf(void* handle, int index, const int32_t* cdf, const int32_t* lengths,
+                      int count, int stride);
+/* reset + set_entropy_coder_parallel (py_rans.cpp:251-260, 305-309) */
+int dcvc_rans_encode_begin(void* handle, int ec_parallel);
+/* encode_y: combined symbols (value << 8) + table index (py_rans.cpp:104-124) */
+int dcvc_rans_encode_y(void* handle, const int16_t* sym, int n);
+/* encode_z: table (i % ch) + cdf_offset (py_rans.cpp:126-146) */
+int dcvc_rans_encode_z(void* handle, const int8_t* sym, int n, int cdf_offset, int ch);
+/* flush + get_encoded_stream (py_rans.cpp:148-249); *data stays valid until the next call on
+ * the handle */
+int dcvc_rans_encode_finish(void* handle, const uint8_t** data, size_t* size);
+/* set_entropy_coder_parallel + set_stream (py_rans.cpp:412-492) */
+int dcvc_rans_decode_begin(void* handle, const uint8_t* data, size_t size, int ec_parallel);
+/* decode_z / decode_y + get_decoded_tensor_cpp (py_rans.cpp:314-366); segments are decoded in
+ * the reverse order of encoding.  DCVC_CORRUPT_STREAM if a sub-stream runs out of bytes. */
+int dcvc_rans_decode_z(void* handle, int n, int cdf_offset, int ch, int8_t* out);
+int dcvc_rans_decode_y(void* handle, const uint8_t* idx, int n, int8_t* out);
+
 #ifdef __cplusplus
 }
 #endif
