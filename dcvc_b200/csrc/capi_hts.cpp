@@ -1,0 +1,207 @@
+// extern "C" entry points of the HT-S codec runtime (declared in include/dcvc_b200.h).
+#include "errors.h"
+#include "hts_codec.h"
+
+#include "../../include/dcvc_b200.h"
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include <cstring>
+#include <exception>
+
+using namespace dcvc;
+
+namespace {
+
+struct HtsHandle {
+    HtsCodec codec;
+    std::vector<uint8_t> bytes;
+};
+
+int fail(int status, const std::string& msg)
+{
+    set_last_error(msg);
+    return status;
+}
+
+size_t dtype_size(int dt)
+{
+    switch (dt) {
+    case DCVC_F16:
+    case DCVC_BF16: return 2;
+    case DCVC_F32:
+    case DCVC_I32: return 4;
+    case DCVC_I64: return 8;
+    default: return 0;
+    }
+}
+
+bool to_float(int dt, const void* src, size_t n, std::vector<float>* out)
+{
+    out->resize(n);
+    float* o = out->data();
+    switch (dt) {
+    case DCVC_F16: {
+        const __half* s = static_cast<const __half*>(src);
+        for (size_t i = 0; i < n; ++i) o[i] = __half2float(s[i]);
+        return true;
+    }
+    case DCVC_BF16: {
+        const __nv_bfloat16* s = static_cast<const __nv_bfloat16*>(src);
+        for (size_t i = 0; i < n; ++i) o[i] = __bfloat162float(s[i]);
+        return true;
+    }
+    case DCVC_F32: std::memcpy(o, src, n * 4); return true;
+    case DCVC_I32: {
+        const int32_t* s = static_cast<const int32_t*>(src);
+        for (size_t i = 0; i < n; ++i) o[i] = static_cast<float>(s[i]);
+        return true;
+    }
+    case DCVC_I64: {
+        const int64_t* s = static_cast<const int64_t*>(src);
+        for (size_t i = 0; i < n; ++i) o[i] = static_cast<float>(s[i]);
+        return true;
+    }
+    default: return false;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int dcvc_hts_create(void** handle)
+{
+    if (handle == nullptr) {
+        return fail(kInvalidArgument, "dcvc_hts_create: null output");
+    }
+    if (device_error_word() == nullptr) {
+        return fail(kCudaError, "dcvc_hts_create: no usable CUDA device");
+    }
+    try {
+        *handle = new HtsHandle();
+    } catch (const std::exception& e) {
+        return fail(kOutOfMemory, std::string("dcvc_hts_create: ") + e.what());
+    }
+    return kOk;
+}
+
+int dcvc_hts_destroy(void* handle)
+{
+    delete static_cast<HtsHandle*>(handle);
+    return kOk;
+}
+
+int dcvc_hts_set_param(void* handle, int n, const char* const* names, const void* const* data,
+                       const int64_t* shapes, const int* ndims, const int* dtypes,
+                       const int* on_device, float skip_threshold)
+{
+    if (handle == nullptr || n <= 0 || names == nullptr || data == nullptr || shapes == nullptr ||
+        ndims == nullptr || dtypes == nullptr || on_device == nullptr) {
+        return fail(kInvalidArgument, "dcvc_hts_set_param: null argument");
+    }
+    StateDict sd;
+    std::vector<uint8_t> host;
+    try {
+        for (int i = 0; i < n; ++i) {
+            if (names[i] == nullptr || ndims[i] < 0 || ndims[i] > 4 || dtype_size(dtypes[i]) == 0) {
+                return fail(kInvalidArgument, "dcvc_hts_set_param: bad entry " + std::to_string(i));
+            }
+            HostTensor t;
+            size_t numel = 1;
+            for (int d = 0; d < ndims[i]; ++d) {
+                t.shape.push_back(shapes[4 * i + d]);
+                numel *= static_cast<size_t>(shapes[4 * i + d]);
+            }
+            const size_t bytes = numel * dtype_size(dtypes[i]);
+            const void* src = data[i];
+            if (on_device[i] && numel > 0) {
+                host.resize(bytes);
+                cudaError_t e = cudaMemcpy(host.data(), data[i], bytes, cudaMemcpyDeviceToHost);
+                if (e != cudaSuccess) {
+                    return cuda_status(e, "dcvc_hts_set_param: reading a device tensor");
+                }
+                src = host.data();
+            }
+            if (numel > 0 && src == nullptr) {
+                return fail(kInvalidArgument, std::string("dcvc_hts_set_param: null data for ") + names[i]);
+            }
+            to_float(dtypes[i], src, numel, &t.data);
+            sd[names[i]] = std::move(t);
+        }
+    } catch (const std::exception& e) {
+        return fail(kOutOfMemory, std::string("dcvc_hts_set_param: ") + e.what());
+    }
+    return static_cast<HtsHandle*>(handle)->codec.set_param(sd, skip_threshold);
+}
+
+int dcvc_hts_add_ref_feature(void* handle, const void* frame, int height, int width,
+                             int apply_adaptor, void* stream)
+{
+    if (handle == nullptr) {
+        return fail(kInvalidArgument, "dcvc_hts_add_ref_feature: null handle");
+    }
+    return static_cast<HtsHandle*>(handle)->codec.add_ref_feature(
+        static_cast<const __half*>(frame), height, width, apply_adaptor != 0,
+        static_cast<cudaStream_t>(stream));
+}
+
+int dcvc_hts_compress(void* handle, const void* x, int height, int width, int qp, int reset,
+                      int pad_b, int pad_r, void* stream, const uint8_t** bytes, size_t* nbytes,
+                      int* ec_parallel)
+{
+    if (handle == nullptr || bytes == nullptr || nbytes == nullptr || ec_parallel == nullptr) {
+        return fail(kInvalidArgument, "dcvc_hts_compress: null argument");
+    }
+    HtsHandle* h = static_cast<HtsHandle*>(handle);
+    int st = h->codec.compress(static_cast<const __half*>(x), height, width, qp, reset != 0, pad_b,
+                               pad_r, static_cast<cudaStream_t>(stream), &h->bytes, ec_parallel);
+    if (st != kOk) {
+        return st;
+    }
+    *bytes = h->bytes.data();
+    *nbytes = h->bytes.size();
+    return kOk;
+}
+
+int dcvc_hts_decompress(void* handle, const uint8_t* bytes, size_t nbytes, int qp, int height,
+                        int width, int ec_parallel, int reset, void* stream, void** frames)
+{
+    if (handle == nullptr || frames == nullptr) {
+        return fail(kInvalidArgument, "dcvc_hts_decompress: null argument");
+    }
+    const __half* f[HtsCodec::kFrames] = {nullptr};
+    int st = static_cast<HtsHandle*>(handle)->codec.decompress(
+        bytes, nbytes, qp, height, width, ec_parallel, reset != 0, static_cast<cudaStream_t>(stream), f);
+    if (st == kOk) {
+        for (int i = 0; i < HtsCodec::kFrames; ++i) {
+            frames[i] = const_cast<__half*>(f[i]);
+        }
+    }
+    return st;
+}
+
+int dcvc_hts_buffer(void* handle, const char* name, const void** ptr, int* rows, int* cols,
+                    int* ld)
+{
+    if (handle == nullptr || name == nullptr || ptr == nullptr || rows == nullptr ||
+        cols == nullptr || ld == nullptr) {
+        return fail(kInvalidArgument, "dcvc_hts_buffer: null argument");
+    }
+    return static_cast<HtsHandle*>(handle)->codec.buffer(name, ptr, rows, cols, ld);
+}
+
+int dcvc_hts_stats(void* handle, int* symbols, int* kernels, size_t* device_bytes)
+{
+    if (handle == nullptr) {
+        return fail(kInvalidArgument, "dcvc_hts_stats: null handle");
+    }
+    const HtsCodec& c = static_cast<HtsHandle*>(handle)->codec;
+    if (symbols) *symbols = c.last_symbol_count();
+    if (kernels) *kernels = c.last_kernel_count();
+    if (device_bytes) *device_bytes = c.device_bytes();
+    return kOk;
+}
+
+}  // extern "C"

@@ -109,6 +109,33 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const void* tmap, uint64_
         : "memory");
 }
 
+// 2D tiled store from shared memory (bulk-group completion), no multicast.
+__device__ __forceinline__ void tma_store_2d(const void* tmap, const void* src, int c0, int c1)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%2, %3}], [%1];" ::"l"(
+            reinterpret_cast<uint64_t>(tmap)),
+        "r"(smem_u32(src)), "r"(c0), "r"(c1)
+        : "memory");
+}
+
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+
+// Waits until the shared-memory sources of all committed bulk stores have been read.
+__device__ __forceinline__ void bulk_wait_read0()
+{
+    asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+
+// Waits until all committed bulk stores have completed.
+__device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
+// Orders this thread's generic-proxy shared-memory writes before later async-proxy (TMA) reads.
+__device__ __forceinline__ void fence_proxy_async_smem()
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
 // ---------------------------------------------------------------- tcgen05
 
 __device__ __forceinline__ void tmem_alloc(uint32_t* dst_smem, uint32_t ncols)
@@ -210,10 +237,20 @@ DCVC_HOST_DEVICE uint32_t make_idesc_f16(int m, int n, int ab_format)
 
 // ---------------------------------------------------------------- math
 
-// WSiLU(x) = x * sigmoid(4x), as in the reference's layers (src/layers/layers.py:106-111).
+__device__ __forceinline__ float tanh_approx(float x)
+{
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// WSiLU(x) = x * sigmoid(4x) (src/layers/layers.py:106-111), evaluated through the identity
+// sigmoid(4x) = (1 + tanh(2x)) / 2 with the hardware tanh approximation (relative error about
+// 2^-11, the FP16 rounding step of the stored result).
 __device__ __forceinline__ float wsilu(float x)
 {
-    return x / (1.0f + __expf(-4.0f * x));
+    const float h = 0.5f * x;
+    return fmaf(h, tanh_approx(2.0f * x), h);
 }
 
 }  // namespace dcvc

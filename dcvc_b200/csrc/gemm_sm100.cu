@@ -2,6 +2,7 @@
 #include "gemm_sm100.cuh"
 #include "host_util.h"
 
+#include <cstring>
 #include <mutex>
 
 namespace dcvc {
@@ -10,9 +11,11 @@ namespace {
 
 constexpr int kBM = 128;
 constexpr int kBK = 64;  // one 128-byte swizzle atom of 16-bit elements
-constexpr int kThreads = 192;
+constexpr int kEpiWarps = 8;
+constexpr int kThreads = 64 + 32 * kEpiWarps;  // producer warp, MMA warp, epilogue warps
 // ~1 s at 2 GHz; a correct kernel never waits this long.
 constexpr long long kWaitLimit = 2000000000LL;
+constexpr int kSmemLimit = 232448;  // 227 KB per block on sm_100
 
 template <typename T>
 struct Pack2;
@@ -45,34 +48,69 @@ struct Pack2<__nv_bfloat16> {
     static constexpr int kFormat = 1;
 };
 
-template <int BN>
-struct GemmSmem {
-    static constexpr int kStages = BN >= 256 ? 4 : (BN >= 128 ? 6 : 8);
+__host__ __device__ constexpr bool epi_has_res(int e) { return e == kEpiBiasRes || e == kEpiBiasResQ || e == kEpiBiasRes2; }
+__host__ __device__ constexpr bool epi_has_q(int e) { return e == kEpiBiasResQ || e == kEpiBiasQ; }
+
+// Output columns of one epilogue store box (32 rows high).  Each epilogue warp owns 32 rows (its
+// TMEM lane quadrant) and half of the BN accumulator columns.
+__host__ __device__ constexpr int out_box_cols(int bn, int epi) { return epi == kEpiQuad ? bn / 8 : (bn / 2 < 64 ? bn / 2 : 64); }
+
+template <int BN, int EPI>
+struct GemmCfg {
+    static constexpr int kHalf = BN / 2;                        // accumulator columns per warp
+    static constexpr int kOutW = out_box_cols(BN, EPI);         // output columns per store box
+    static constexpr int kAccPerBox = EPI == kEpiQuad ? 4 * kOutW : kOutW;
+    static constexpr int kBoxes = kHalf / kAccPerBox;
+    static constexpr int kBoxBytes = kOutW * 32 * 2;            // 4 KB (64 cols) or 2 KB (32 cols)
+    static constexpr int kRowBytes = kOutW * 2;                 // 128 (SW128) or 64 (SW64)
+    static constexpr int kResBufs = EPI == kEpiBiasRes2 ? 2 : (epi_has_res(EPI) ? 1 : 0);
+    static constexpr int kWarpStage = 4096 * (1 + kResBufs);    // out + residual staging per warp
+    static constexpr int kEpiBytes = kEpiWarps * kWarpStage;
     static constexpr int kABytes = kBM * kBK * 2;
     static constexpr int kBBytes = BN * kBK * 2;
     static constexpr int kStageBytes = kABytes + kBBytes;
-    static constexpr int kBarOffset = kStages * kStageBytes;
-    // full[S], empty[S], tfull[2], tempty[2], drain, tmem slot, abort flag
-    static constexpr int kBytes = kBarOffset + (2 * kStages + 5) * 8 + 16 + 1024;
+    static constexpr int kBarBytes = 512;
+    static constexpr int kStagesFit = (kSmemLimit - 1024 - kEpiBytes - kBarBytes) / kStageBytes;
+    static constexpr int kStages = kStagesFit > 8 ? 8 : kStagesFit;
+    static constexpr int kEpiOffset = kStages * kStageBytes;
+    static constexpr int kBarOffset = kEpiOffset + kEpiBytes;
+    static constexpr int kBytes = kBarOffset + kBarBytes + 1024;
     static constexpr int kTmemCols = 2 * BN;
+    static_assert(kStages >= 2, "shared memory too small for two pipeline stages");
+    static_assert(kBytes <= kSmemLimit, "shared memory budget exceeded");
+    static_assert(EPI == kEpiSubpel || kBoxes * kAccPerBox == kHalf, "box tiling");
 };
+
+// Byte offset of the 16-byte chunk j of row r inside a swizzled staging box (the layout TMA
+// uses for SWIZZLE_128B with 128-byte rows and SWIZZLE_64B with 64-byte rows).
+template <int ROWB>
+__device__ __forceinline__ int stage_off(int r, int j)
+{
+    if constexpr (ROWB == 128) {
+        return r * 128 + ((j ^ (r & 7)) << 4);
+    } else {
+        return r * 64 + ((j ^ ((r >> 1) & 3)) << 4);
+    }
+}
 
 template <typename T, int BN, int EPI>
 __global__ void __launch_bounds__(kThreads, 1)
-    gemm_sm100_kernel(const __grid_constant__ CUtensorMap tmA,
-                      const __grid_constant__ CUtensorMap tmB, const GemmParams p)
+    gemm_sm100_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                      const __grid_constant__ CUtensorMap tmO, const __grid_constant__ CUtensorMap tmR,
+                      const __grid_constant__ CUtensorMap tmR2, const GemmParams p)
 {
-    using S = GemmSmem<BN>;
-    constexpr int kStages = S::kStages;
+    using C = GemmCfg<BN, EPI>;
+    constexpr int kStages = C::kStages;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem =
         reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    uint64_t* full = reinterpret_cast<uint64_t*>(smem + S::kBarOffset);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + C::kBarOffset);
     uint64_t* empty = full + kStages;
     uint64_t* tfull = empty + kStages;
     uint64_t* tempty = tfull + 2;
     uint64_t* drain = tempty + 2;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+    uint64_t* resbar = drain + 1;  // [kEpiWarps]
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(resbar + kEpiWarps);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5;
@@ -89,9 +127,12 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(&tfull[b], 1);
-            mbar_init(&tempty[b], 4);
+            mbar_init(&tempty[b], kEpiWarps);
         }
         mbar_init(drain, 1);
+        for (int w = 0; w < kEpiWarps; ++w) {
+            mbar_init(&resbar[w], 1);
+        }
         *abort_flag = 0;
         fence_mbar_init();
     }
@@ -100,7 +141,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         tma_prefetch_desc(&tmB);
     }
     if (warp == 1) {
-        tmem_alloc(tmem_slot, S::kTmemCols);
+        tmem_alloc(tmem_slot, C::kTmemCols);
         tmem_relinquish();
     }
     tc_fence_before();
@@ -123,10 +164,10 @@ __global__ void __launch_bounds__(kThreads, 1)
                         report_error(p.err, kErrGemmProducerTimeout);
                         break;
                     }
-                    mbar_arrive_expect_tx(&full[stage], S::kStageBytes);
-                    uint8_t* sa = smem + stage * S::kStageBytes;
+                    mbar_arrive_expect_tx(&full[stage], C::kStageBytes);
+                    uint8_t* sa = smem + stage * C::kStageBytes;
                     tma_load_2d(sa, &tmA, &full[stage], kb * kBK, m0);
-                    tma_load_2d(sa + S::kABytes, &tmB, &full[stage], kb * kBK, n0);
+                    tma_load_2d(sa + C::kABytes, &tmB, &full[stage], kb * kBK, n0);
                     ++issued;
                     if (++stage == kStages) {
                         stage = 0;
@@ -170,9 +211,9 @@ __global__ void __launch_bounds__(kThreads, 1)
                         break;
                     }
                     tc_fence_after();
-                    const uint8_t* sa = smem + stage * S::kStageBytes;
+                    const uint8_t* sa = smem + stage * C::kStageBytes;
                     const uint64_t adesc = make_sw128_kmajor_desc(smem_u32(sa));
-                    const uint64_t bdesc = make_sw128_kmajor_desc(smem_u32(sa + S::kABytes));
+                    const uint64_t bdesc = make_sw128_kmajor_desc(smem_u32(sa + C::kABytes));
 #pragma unroll
                     for (int k = 0; k < kBK / 16; ++k) {
                         // +32 bytes per K=16 step inside the swizzle atom (descriptor units of 16 B)
@@ -201,146 +242,201 @@ __global__ void __launch_bounds__(kThreads, 1)
             }
         }
     } else {
-        // ------------------------------------------------------------ epilogue warps (2..5)
-        const int quad = warp & 3;  // TMEM lane quadrant this warp may access
-        const int row = quad * 32 + lane;
+        // ------------------------------------------------------------ epilogue warps (2..9)
+        using P = Pack2<T>;
+        const int ew = warp - 2;                  // epilogue warp index 0..7
+        const int quad = warp & 3;                // TMEM lane quadrant this warp may access
+        const int half = ew >> 2;                 // which half of the BN columns
+        uint8_t* out_buf = smem + C::kEpiOffset + ew * C::kWarpStage;
+        uint8_t* res_buf = out_buf + 4096;
+        uint8_t* res2_buf = out_buf + 8192;
+        uint64_t* rbar = &resbar[ew];
+        uint32_t res_phase = 0;
         int acc = 0;
         uint32_t acc_phase = 0;
-        using P = Pack2<T>;
+        if (EPI != kEpiSubpel && lane == 0) {
+            tma_prefetch_desc(&tmO);
+        }
         for (int tile = blockIdx.x; tile < num_tiles && !*abort_flag; tile += gridDim.x) {
             const int m0 = (tile % num_m) * kBM;
             const int n0 = (tile / num_m) * BN;
+            const int row0 = m0 + quad * 32;        // first row owned by this warp
+            const bool rows_live = row0 < p.M;
+            const int nacc0 = n0 + half * C::kHalf;  // first accumulator column of this warp
+            if constexpr (epi_has_res(EPI)) {
+                if (rows_live && lane == 0) {
+                    mbar_arrive_expect_tx(rbar, C::kBoxBytes * C::kResBufs);
+                    tma_load_2d(res_buf, &tmR, rbar, nacc0, row0);
+                    if constexpr (EPI == kEpiBiasRes2) {
+                        tma_load_2d(res2_buf, &tmR2, rbar, nacc0, row0);
+                    }
+                }
+            }
             if (!mbar_wait_bounded(&tfull[acc], acc_phase, kWaitLimit)) {
                 *abort_flag = 1;
                 report_error(p.err, kErrGemmEpilogueTimeout);
                 break;
             }
             tc_fence_after();
-            const int m = m0 + row;
-            const bool live = m < p.M;
+            const uint32_t tbase = tmem_base + (static_cast<uint32_t>(quad * 32) << 16) + acc * BN +
+                                   half * C::kHalf;
+            if constexpr (EPI == kEpiSubpel) {
+                // direct stores: the shuffled rows of one box are not contiguous in memory
+                const int m = row0 + lane;
+                const bool live = m < p.M;
 #pragma unroll 1
-            for (int c = 0; c < BN / 32; ++c) {
-                uint32_t r[32];
-                tmem_ld_32x32b_x32(
-                    tmem_base + (static_cast<uint32_t>(quad * 32) << 16) + acc * BN + c * 32, r);
-                tc_wait_ld();
-                const int nc = n0 + c * 32;
-                float v[32];
-#pragma unroll
-                for (int j = 0; j < 32; ++j) {
-                    v[j] = __uint_as_float(r[j]);
-                }
-                if constexpr (EPI != kEpiSubpel) {
-                    const float4* b4 = reinterpret_cast<const float4*>(p.bias + nc);
-#pragma unroll
-                    for (int j = 0; j < 8; ++j) {
-                        const float4 b = __ldg(b4 + j);
-                        v[4 * j + 0] += b.x;
-                        v[4 * j + 1] += b.y;
-                        v[4 * j + 2] += b.z;
-                        v[4 * j + 3] += b.w;
-                    }
-                }
-                if constexpr (EPI == kEpiQuad) {
-                    uint32_t o[4];
-#pragma unroll
-                    for (int i = 0; i < 4; ++i) {
-                        float s0 = wsilu(v[8 * i + 0]) + wsilu(v[8 * i + 1]) + wsilu(v[8 * i + 2]) +
-                                   wsilu(v[8 * i + 3]);
-                        float s1 = wsilu(v[8 * i + 4]) + wsilu(v[8 * i + 5]) + wsilu(v[8 * i + 6]) +
-                                   wsilu(v[8 * i + 7]);
-                        o[i] = P::pack(s0, s1);
-                    }
+                for (int c = 0; c < C::kHalf / 32; ++c) {
+                    uint32_t r[32];
+                    tmem_ld_32x32b_x32(tbase + c * 32, r);
+                    tc_wait_ld();
                     if (live) {
-                        T* dst = reinterpret_cast<T*>(p.out) + static_cast<size_t>(m) * p.ldo + nc / 4;
-                        *reinterpret_cast<uint4*>(dst) = make_uint4(o[0], o[1], o[2], o[3]);
-                    }
-                    continue;
-                }
-                if constexpr (EPI == kEpiBiasWsilu) {
-#pragma unroll
-                    for (int j = 0; j < 32; ++j) {
-                        v[j] = wsilu(v[j]);
-                    }
-                }
-                if constexpr (EPI == kEpiBiasRes || EPI == kEpiBiasResQ || EPI == kEpiBiasRes2) {
-                    if (live) {
-                        const uint4* rs = reinterpret_cast<const uint4*>(
-                            reinterpret_cast<const T*>(p.res) + static_cast<size_t>(m) * p.ldr + nc);
-#pragma unroll
-                        for (int j = 0; j < 4; ++j) {
-                            const uint4 u = rs[j];
-                            const float2 a = P::unpack(u.x), b = P::unpack(u.y),
-                                         cc = P::unpack(u.z), d = P::unpack(u.w);
-                            v[8 * j + 0] += a.x;
-                            v[8 * j + 1] += a.y;
-                            v[8 * j + 2] += b.x;
-                            v[8 * j + 3] += b.y;
-                            v[8 * j + 4] += cc.x;
-                            v[8 * j + 5] += cc.y;
-                            v[8 * j + 6] += d.x;
-                            v[8 * j + 7] += d.y;
-                        }
-                    }
-                }
-                if constexpr (EPI == kEpiBiasRes2) {
-                    if (live) {
-                        const uint4* rs = reinterpret_cast<const uint4*>(
-                            reinterpret_cast<const T*>(p.res2) + static_cast<size_t>(m) * p.ldr2 + nc);
-#pragma unroll
-                        for (int j = 0; j < 4; ++j) {
-                            const uint4 u = rs[j];
-                            const float2 a = P::unpack(u.x), b = P::unpack(u.y),
-                                         cc = P::unpack(u.z), d = P::unpack(u.w);
-                            v[8 * j + 0] += a.x;
-                            v[8 * j + 1] += a.y;
-                            v[8 * j + 2] += b.x;
-                            v[8 * j + 3] += b.y;
-                            v[8 * j + 4] += cc.x;
-                            v[8 * j + 5] += cc.y;
-                            v[8 * j + 6] += d.x;
-                            v[8 * j + 7] += d.y;
-                        }
-                    }
-                }
-                if constexpr (EPI == kEpiBiasResQ || EPI == kEpiBiasQ) {
-                    const uint4* qs =
-                        reinterpret_cast<const uint4*>(reinterpret_cast<const T*>(p.qscale) + nc);
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        const uint4 u = __ldg(qs + j);
-                        const float2 a = P::unpack(u.x), b = P::unpack(u.y), cc = P::unpack(u.z),
-                                     d = P::unpack(u.w);
-                        v[8 * j + 0] *= a.x;
-                        v[8 * j + 1] *= a.y;
-                        v[8 * j + 2] *= b.x;
-                        v[8 * j + 3] *= b.y;
-                        v[8 * j + 4] *= cc.x;
-                        v[8 * j + 5] *= cc.y;
-                        v[8 * j + 6] *= d.x;
-                        v[8 * j + 7] *= d.y;
-                    }
-                }
-                if (live) {
-                    T* dst;
-                    if constexpr (EPI == kEpiSubpel) {
+                        const int nc = nacc0 + c * 32;
                         const int sub = nc / p.sub_cout;  // dy * 2 + dx
                         const int ch = nc - sub * p.sub_cout;
                         const int h = m / p.sub_w;
                         const int w = m - h * p.sub_w;
                         const size_t orow = static_cast<size_t>(2 * h + (sub >> 1)) * (2 * p.sub_w) +
                                             (2 * w + (sub & 1));
-                        dst = reinterpret_cast<T*>(p.out) + orow * p.ldo + ch;
-                    } else {
-                        dst = reinterpret_cast<T*>(p.out) + static_cast<size_t>(m) * p.ldo + nc;
-                    }
-                    uint4* d4 = reinterpret_cast<uint4*>(dst);
+                        uint4* d4 = reinterpret_cast<uint4*>(reinterpret_cast<T*>(p.out) + orow * p.ldo + ch);
 #pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        d4[j] = make_uint4(P::pack(v[8 * j + 0], v[8 * j + 1]),
+                        for (int j = 0; j < 4; ++j) {
+                            d4[j] = make_uint4(
+                                P::pack(__uint_as_float(r[8 * j + 0]), __uint_as_float(r[8 * j + 1])),
+                                P::pack(__uint_as_float(r[8 * j + 2]), __uint_as_float(r[8 * j + 3])),
+                                P::pack(__uint_as_float(r[8 * j + 4]), __uint_as_float(r[8 * j + 5])),
+                                P::pack(__uint_as_float(r[8 * j + 6]), __uint_as_float(r[8 * j + 7])));
+                        }
+                    }
+                }
+            } else {
+#pragma unroll 1
+                for (int b = 0; b < C::kBoxes; ++b) {
+                    const int ncol = nacc0 + b * C::kAccPerBox;  // first accumulator column of box
+                    if constexpr (epi_has_res(EPI)) {
+                        if (rows_live && !mbar_wait_bounded(rbar, res_phase, kWaitLimit)) {
+                            *abort_flag = 1;
+                            report_error(p.err, kErrGemmEpilogueTimeout);
+                        }
+                        res_phase ^= rows_live ? 1u : 0u;
+                    }
+                    // the previous box's store must have read the staging buffer
+                    if (lane == 0) {
+                        bulk_wait_read0();
+                    }
+                    __syncwarp();
+#pragma unroll 1
+                    for (int c = 0; c < C::kAccPerBox / 32; ++c) {
+                        uint32_t r[32];
+                        tmem_ld_32x32b_x32(tbase + b * C::kAccPerBox + c * 32, r);
+                        tc_wait_ld();
+                        const int nc = ncol + c * 32;
+                        float v[32];
+                        const float4* b4 = reinterpret_cast<const float4*>(p.bias + nc);
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) {
+                            const float4 bb = __ldg(b4 + j);
+                            v[4 * j + 0] = __uint_as_float(r[4 * j + 0]) + bb.x;
+                            v[4 * j + 1] = __uint_as_float(r[4 * j + 1]) + bb.y;
+                            v[4 * j + 2] = __uint_as_float(r[4 * j + 2]) + bb.z;
+                            v[4 * j + 3] = __uint_as_float(r[4 * j + 3]) + bb.w;
+                        }
+                        if constexpr (EPI == kEpiQuad) {
+                            uint32_t o[4];
+#pragma unroll
+                            for (int i = 0; i < 4; ++i) {
+                                const float s0 = wsilu(v[8 * i + 0]) + wsilu(v[8 * i + 1]) +
+                                                 wsilu(v[8 * i + 2]) + wsilu(v[8 * i + 3]);
+                                const float s1 = wsilu(v[8 * i + 4]) + wsilu(v[8 * i + 5]) +
+                                                 wsilu(v[8 * i + 6]) + wsilu(v[8 * i + 7]);
+                                o[i] = P::pack(s0, s1);
+                            }
+                            *reinterpret_cast<uint4*>(out_buf + stage_off<C::kRowBytes>(lane, c)) =
+                                make_uint4(o[0], o[1], o[2], o[3]);
+                            continue;
+                        }
+                        if constexpr (EPI == kEpiBiasWsilu) {
+#pragma unroll
+                            for (int j = 0; j < 32; ++j) {
+                                v[j] = wsilu(v[j]);
+                            }
+                        }
+                        if constexpr (epi_has_res(EPI)) {
+#pragma unroll
+                            for (int j = 0; j < 4; ++j) {
+                                const uint4 u = *reinterpret_cast<const uint4*>(
+                                    res_buf + stage_off<C::kRowBytes>(lane, c * 4 + j));
+                                const float2 a = P::unpack(u.x), bq = P::unpack(u.y),
+                                             cc = P::unpack(u.z), d = P::unpack(u.w);
+                                v[8 * j + 0] += a.x;
+                                v[8 * j + 1] += a.y;
+                                v[8 * j + 2] += bq.x;
+                                v[8 * j + 3] += bq.y;
+                                v[8 * j + 4] += cc.x;
+                                v[8 * j + 5] += cc.y;
+                                v[8 * j + 6] += d.x;
+                                v[8 * j + 7] += d.y;
+                            }
+                        }
+                        if constexpr (EPI == kEpiBiasRes2) {
+#pragma unroll
+                            for (int j = 0; j < 4; ++j) {
+                                const uint4 u = *reinterpret_cast<const uint4*>(
+                                    res2_buf + stage_off<C::kRowBytes>(lane, c * 4 + j));
+                                const float2 a = P::unpack(u.x), bq = P::unpack(u.y),
+                                             cc = P::unpack(u.z), d = P::unpack(u.w);
+                                v[8 * j + 0] += a.x;
+                                v[8 * j + 1] += a.y;
+                                v[8 * j + 2] += bq.x;
+                                v[8 * j + 3] += bq.y;
+                                v[8 * j + 4] += cc.x;
+                                v[8 * j + 5] += cc.y;
+                                v[8 * j + 6] += d.x;
+                                v[8 * j + 7] += d.y;
+                            }
+                        }
+                        if constexpr (epi_has_q(EPI)) {
+                            const uint4* qs =
+                                reinterpret_cast<const uint4*>(reinterpret_cast<const T*>(p.qscale) + nc);
+#pragma unroll
+                            for (int j = 0; j < 4; ++j) {
+                                const uint4 u = __ldg(qs + j);
+                                const float2 a = P::unpack(u.x), bq = P::unpack(u.y),
+                                             cc = P::unpack(u.z), d = P::unpack(u.w);
+                                v[8 * j + 0] *= a.x;
+                                v[8 * j + 1] *= a.y;
+                                v[8 * j + 2] *= bq.x;
+                                v[8 * j + 3] *= bq.y;
+                                v[8 * j + 4] *= cc.x;
+                                v[8 * j + 5] *= cc.y;
+                                v[8 * j + 6] *= d.x;
+                                v[8 * j + 7] *= d.y;
+                            }
+                        }
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) {
+                            *reinterpret_cast<uint4*>(out_buf + stage_off<C::kRowBytes>(lane, c * 4 + j)) =
+                                make_uint4(P::pack(v[8 * j + 0], v[8 * j + 1]),
                                            P::pack(v[8 * j + 2], v[8 * j + 3]),
                                            P::pack(v[8 * j + 4], v[8 * j + 5]),
                                            P::pack(v[8 * j + 6], v[8 * j + 7]));
+                        }
+                    }
+                    fence_proxy_async_smem();
+                    __syncwarp();
+                    if (lane == 0 && rows_live) {
+                        const int ocol = EPI == kEpiQuad ? ncol / 4 : ncol;
+                        tma_store_2d(&tmO, out_buf, ocol, row0);
+                        bulk_commit();
+                    }
+                    if constexpr (epi_has_res(EPI)) {
+                        // every lane has read this box's residual: fetch the next one
+                        if (b + 1 < C::kBoxes && rows_live && lane == 0) {
+                            mbar_arrive_expect_tx(rbar, C::kBoxBytes * C::kResBufs);
+                            tma_load_2d(res_buf, &tmR, rbar, ncol + C::kAccPerBox, row0);
+                            if constexpr (EPI == kEpiBiasRes2) {
+                                tma_load_2d(res2_buf, &tmR2, rbar, ncol + C::kAccPerBox, row0);
+                            }
+                        }
                     }
                 }
             }
@@ -354,49 +450,59 @@ __global__ void __launch_bounds__(kThreads, 1)
                 acc_phase ^= 1;
             }
         }
+        if (EPI != kEpiSubpel && lane == 0) {
+            bulk_wait0();
+        }
+        __syncwarp();
     }
 
     tc_fence_before();
     __syncthreads();
     if (warp == 1) {
         tc_fence_after();
-        tmem_dealloc(tmem_base, S::kTmemCols);
+        tmem_dealloc(tmem_base, C::kTmemCols);
     }
 }
 
+struct Maps {
+    CUtensorMap a, b, o, r, r2;
+};
+
 template <typename T, int BN, int EPI>
-cudaError_t launch_one(const CUtensorMap& ta, const CUtensorMap& tb, const GemmParams& p,
-                       cudaStream_t stream)
+cudaError_t launch_one(const Maps& m, const GemmParams& p, cudaStream_t stream)
 {
-    using S = GemmSmem<BN>;
+    using C = GemmCfg<BN, EPI>;
     auto kernel = gemm_sm100_kernel<T, BN, EPI>;
     static std::once_flag once;
     static cudaError_t attr_err = cudaSuccess;
     std::call_once(once, [&] {
-        attr_err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, S::kBytes);
+        attr_err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, C::kBytes);
     });
     if (attr_err != cudaSuccess) {
         return attr_err;
     }
     const int num_tiles = ((p.M + kBM - 1) / kBM) * (p.N / BN);
     const int grid = num_tiles < num_sms() ? num_tiles : num_sms();
-    kernel<<<grid, kThreads, S::kBytes, stream>>>(ta, tb, p);
+    kernel<<<grid, kThreads, C::kBytes, stream>>>(m.a, m.b, m.o, m.r, m.r2, p);
     return cudaGetLastError();
 }
 
 template <typename T, int BN>
-cudaError_t dispatch_epi(int epi, const CUtensorMap& ta, const CUtensorMap& tb,
-                         const GemmParams& p, cudaStream_t s)
+cudaError_t dispatch_epi(int epi, const Maps& m, const GemmParams& p, cudaStream_t s)
 {
     switch (epi) {
-    case kEpiBias: return launch_one<T, BN, kEpiBias>(ta, tb, p, s);
-    case kEpiBiasWsilu: return launch_one<T, BN, kEpiBiasWsilu>(ta, tb, p, s);
-    case kEpiBiasRes: return launch_one<T, BN, kEpiBiasRes>(ta, tb, p, s);
-    case kEpiBiasResQ: return launch_one<T, BN, kEpiBiasResQ>(ta, tb, p, s);
-    case kEpiBiasRes2: return launch_one<T, BN, kEpiBiasRes2>(ta, tb, p, s);
-    case kEpiQuad: return launch_one<T, BN, kEpiQuad>(ta, tb, p, s);
-    case kEpiSubpel: return launch_one<T, BN, kEpiSubpel>(ta, tb, p, s);
-    case kEpiBiasQ: return launch_one<T, BN, kEpiBiasQ>(ta, tb, p, s);
+    case kEpiBias: return launch_one<T, BN, kEpiBias>(m, p, s);
+    case kEpiBiasWsilu: return launch_one<T, BN, kEpiBiasWsilu>(m, p, s);
+    case kEpiBiasRes: return launch_one<T, BN, kEpiBiasRes>(m, p, s);
+    case kEpiBiasResQ: return launch_one<T, BN, kEpiBiasResQ>(m, p, s);
+    case kEpiBiasRes2: return launch_one<T, BN, kEpiBiasRes2>(m, p, s);
+    case kEpiQuad:
+        if constexpr (BN == 256) {
+            return launch_one<T, BN, kEpiQuad>(m, p, s);
+        }
+        return cudaErrorInvalidValue;
+    case kEpiSubpel: return launch_one<T, BN, kEpiSubpel>(m, p, s);
+    case kEpiBiasQ: return launch_one<T, BN, kEpiBiasQ>(m, p, s);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -405,6 +511,9 @@ cudaError_t dispatch_epi(int epi, const CUtensorMap& ta, const CUtensorMap& tb,
 
 int gemm_pick_bn(int N, int epi, int sub_cout)
 {
+    if (epi == kEpiQuad) {
+        return N % 256 == 0 ? 256 : 0;  // the quad epilogue sums groups of 4 over BN/2 columns
+    }
     int lim = (epi == kEpiSubpel) ? sub_cout : N;
     if (N % 256 == 0 && lim % 256 == 0) {
         return 256;
@@ -447,7 +556,7 @@ cudaError_t gemm_sm100(int dtype, const void* A, int lda, const void* W, const G
     if ((epi == kEpiBiasResQ || epi == kEpiBiasQ) && p.qscale == nullptr) {
         return cudaErrorInvalidValue;
     }
-    if (epi == kEpiQuad && (p.N % 4 != 0)) {
+    if (epi == kEpiQuad && (bn != 256 || p.N % 256 != 0)) {
         return cudaErrorInvalidValue;
     }
     if (epi == kEpiSubpel && (p.sub_w <= 0 || p.sub_cout % bn != 0 || p.N != 4 * p.sub_cout ||
@@ -456,22 +565,40 @@ cudaError_t gemm_sm100(int dtype, const void* A, int lda, const void* W, const G
     }
     const CUtensorMapDataType dt =
         dtype == 0 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
-    CUtensorMap ta, tb;
-    if (!make_tmap_2d(&ta, dt, A, p.K, p.M, static_cast<uint64_t>(lda) * 2, kBK, kBM) ||
-        !make_tmap_2d(&tb, dt, W, p.K, p.N, static_cast<uint64_t>(p.K) * 2, kBK, bn)) {
+    Maps m;
+    std::memset(&m, 0, sizeof(m));
+    if (!make_tmap_2d(&m.a, dt, A, p.K, p.M, static_cast<uint64_t>(lda) * 2, kBK, kBM, 128) ||
+        !make_tmap_2d(&m.b, dt, W, p.K, p.N, static_cast<uint64_t>(p.K) * 2, kBK, bn, 128)) {
         return cudaErrorInvalidValue;
+    }
+    if (epi != kEpiSubpel) {
+        const int ow = out_box_cols(bn, epi);
+        const int sw = ow * 2;  // staging row bytes = swizzle span
+        const int nout = epi == kEpiQuad ? p.N / 4 : p.N;
+        if (!make_tmap_2d(&m.o, dt, p.out, nout, p.M, static_cast<uint64_t>(p.ldo) * 2, ow, 32, sw)) {
+            return cudaErrorInvalidValue;
+        }
+        if (epi == kEpiBiasRes || epi == kEpiBiasResQ || epi == kEpiBiasRes2) {
+            if (!make_tmap_2d(&m.r, dt, p.res, p.N, p.M, static_cast<uint64_t>(p.ldr) * 2, ow, 32, sw)) {
+                return cudaErrorInvalidValue;
+            }
+        }
+        if (epi == kEpiBiasRes2 &&
+            !make_tmap_2d(&m.r2, dt, p.res2, p.N, p.M, static_cast<uint64_t>(p.ldr2) * 2, ow, 32, sw)) {
+            return cudaErrorInvalidValue;
+        }
     }
     if (dtype == 0) {
         switch (bn) {
-        case 256: return dispatch_epi<__half, 256>(epi, ta, tb, p, stream);
-        case 128: return dispatch_epi<__half, 128>(epi, ta, tb, p, stream);
-        case 64: return dispatch_epi<__half, 64>(epi, ta, tb, p, stream);
+        case 256: return dispatch_epi<__half, 256>(epi, m, p, stream);
+        case 128: return dispatch_epi<__half, 128>(epi, m, p, stream);
+        case 64: return dispatch_epi<__half, 64>(epi, m, p, stream);
         }
     } else {
         switch (bn) {
-        case 256: return dispatch_epi<__nv_bfloat16, 256>(epi, ta, tb, p, stream);
-        case 128: return dispatch_epi<__nv_bfloat16, 128>(epi, ta, tb, p, stream);
-        case 64: return dispatch_epi<__nv_bfloat16, 64>(epi, ta, tb, p, stream);
+        case 256: return dispatch_epi<__nv_bfloat16, 256>(epi, m, p, stream);
+        case 128: return dispatch_epi<__nv_bfloat16, 128>(epi, m, p, stream);
+        case 64: return dispatch_epi<__nv_bfloat16, 64>(epi, m, p, stream);
         }
     }
     return cudaErrorInvalidValue;

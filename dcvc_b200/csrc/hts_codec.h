@@ -1,0 +1,164 @@
+// DCVC-UF HT-S chunk codec runtime: the B200 counterpart of DMCHTSProxy
+// (src/layers/extensions/inference/dmc_hts_proxy.{h,cpp}).
+#pragma once
+
+#include "net.h"
+#include "rans_coder.h"
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+namespace dcvc {
+
+class HtsCodec {
+public:
+    static constexpr int kFrames = 8;       // g_frame_delay (video_model_ht.py:16)
+    static constexpr int kChSrcIntra = 192; // 3 * 8 * 8
+    static constexpr int kChSrc = 1536;
+    static constexpr int kChY = 256, kChZ = 128, kChD = 512, kChM = 512, kChRecon = 256;
+    static constexpr int kQpNum = 64;
+
+    HtsCodec();
+    ~HtsCodec();
+
+    // set_param (dmc_hts_proxy.cpp:712-762): weights + CDF tables + skip threshold.
+    int set_param(const StateDict& sd, float skip_threshold);
+    // add_ref_feature_from_frame (dmc_hts_proxy.cpp:492-502): frame is [Hp, Wp, 3] FP16 on the
+    // device, Hp and Wp multiples of 16.
+    int add_ref_feature(const __half* frame, int Hp, int Wp, bool apply_adaptor, cudaStream_t s);
+    // compress (dmc_hts_proxy.cpp:504-585): x is [H, W, 24] FP16 (8 frames x YUV, channels last)
+    // with H + pad_b and W + pad_r equal to the resolution of the last add_ref_feature.
+    int compress(const __half* x, int H, int W, int qp, bool reset, int pad_b, int pad_r,
+                 cudaStream_t s, std::vector<uint8_t>* bytes, int* ec_parallel);
+    // decompress (dmc_hts_proxy.cpp:587-710): returns 8 device frames [Hp, Wp, 3] FP16 owned by
+    // the codec and overwritten by the next call.
+    int decompress(const uint8_t* bytes, size_t n, int qp, int height, int width, int ecp,
+                   bool reset, cudaStream_t s, const __half** frames);
+
+    // Read-only view of an internal buffer for inspection and tests: "y_hat", "y_q", "memory",
+    // "ctx", "feature_p", "common", "feature_i".  rows x cols FP16 with pitch ld.
+    int buffer(const std::string& name, const void** ptr, int* rows, int* cols, int* ld) const;
+
+    // Statistics of the last call, for reporting.
+    int last_symbol_count() const { return last_count_; }
+    size_t device_bytes() const { return weights_.bytes() + acts_.bytes(); }
+    // Number of kernels the last compress/decompress enqueued (graph nodes included).
+    int last_kernel_count() const { return last_kernels_; }
+
+private:
+    struct Graph {
+        cudaGraphExec_t exec = nullptr;
+    };
+    enum Phase {
+        kEncAnalysis = 0,    // enc_0 (dmc_hts_proxy.cpp:516-559)
+        kEncUpdate = 1,      // enc_1 (2 variants: reset)
+        kDecTemporal = 3,    // dec_0 (2 variants: memory has value)
+        kDecHyper = 5,       // dec_1
+        kDecContext = 6,     // dec_2
+        kDecSynthesis = 7,   // dec_3
+        kPhaseSlots = 8,
+    };
+
+    int allocate(int Hp, int Wp);
+    void clear_graphs();
+    int run_phase(int slot, cudaStream_t s);
+    int record_phase(int slot, Launch& L);
+    int count_kernels(cudaGraphExec_t) const;
+    int sync_into_main(cudaStream_t caller);
+    int check_device_error(const char* where);
+
+    // phase bodies (enqueue onto L.s)
+    void enc_analysis(Launch& L);
+    void enc_update(Launch& L, bool reset);
+    void dec_temporal(Launch& L, bool memory_has_value);
+    void dec_hyper(Launch& L);
+    void dec_context(Launch& L);
+    void dec_synthesis(Launch& L);
+    // shared pieces
+    void feature_adaptor_m(Launch& L);
+    void feature_adaptor_i(Launch& L, const __half* feature_i);
+    void feature_extractor(Launch& L);
+    void temporal_prior(Launch& L);
+    void hyper_decoder(Launch& L);
+    void prior_fusion(Launch& L);
+    void spatial_prior(Launch& L, int k);
+    void decoder(Launch& L);
+    void recon_head(Launch& L, bool all_frames);
+    void set_qp(int qp, cudaStream_t s);
+
+    // ---------------------------------------------------------------- parameters
+    DeviceArena weights_;
+    bool ready_ = false;
+    float skip_threshold_ = 0.f;
+    __half skip_thr_half_;
+    const __half* q_enc_tab_ = nullptr;   // [64][512]
+    const __half* q_dec_tab_ = nullptr;
+    const __half* q_feat_tab_ = nullptr;
+    uint8_t* scale_lut_ = nullptr;         // [65536]
+    Dcb encoder_[6];
+    Lin enc_down_;
+    Dcb hyper_enc0_;
+    DownBlock hyper_enc1_, hyper_enc2_;
+    UpBlock hyper_dec0_, hyper_dec1_;
+    Dcb hyper_dec2_;
+    DownBlock temporal_;
+    Dcb prior_fusion_[3];
+    Lin prior_fusion_out_;
+    Lin reduction_;
+    Dcb sp_adaptor_[3];
+    Dcb spatial_prior_[3];
+    Lin spatial_prior_out_;
+    UpBlock dec_up_;   // only .up is used (decoder.up), the DCB chain is decoder_[]
+    Lin dec_up_lin_;
+    Dcb decoder_[7];
+    Dcb fa_i_[4];
+    Dcb fa_m_[6];
+    Dcb fe_[5];
+    Dcb rh_common_[4];
+    Dcb rh_frame_[8][3];
+    Lin rh_head_[8];
+    RansTables tables_;
+
+    // ---------------------------------------------------------------- resolution state
+    DeviceArena acts_;
+    int Hp_ = 0, Wp_ = 0, H8_ = 0, W8_ = 0, H16_ = 0, W16_ = 0, H16p_ = 0, W16p_ = 0;
+    int M8_ = 0, M16_ = 0, M16p_ = 0, M32_ = 0, M64_ = 0;
+    int y_num_ = 0, z_num_ = 0;
+    __half *cat_enc_ = nullptr, *cat_fam_ = nullptr, *feature_i_ = nullptr, *temporal_in_ = nullptr;
+    __half *y_ = nullptr, *y_pad_ = nullptr, *cat_pf_ = nullptr, *hyper_pad_ = nullptr;
+    __half *common_ = nullptr, *cat_spa_ = nullptr, *means_ = nullptr, *y_q_ = nullptr;
+    __half *z_ = nullptr, *z_hat_ = nullptr, *col_ = nullptr, *s2d_ = nullptr;
+    __half *lvl8_a_ = nullptr, *lvl8_b_ = nullptr, *lvl16_a_ = nullptr, *lvl32_a_ = nullptr;
+    __half *lvl64_a_ = nullptr, *head_ = nullptr;
+    __half *q_enc_ = nullptr, *q_dec_ = nullptr, *q_feat_ = nullptr;  // active QP rows
+    __half* x_hat_[kFrames] = {nullptr};
+    int8_t* z_i8_ = nullptr;
+    int16_t *sym_ = nullptr, *sym_c_ = nullptr;
+    uint8_t *idx_ = nullptr, *idx_c_ = nullptr, *cond_ = nullptr;
+    int8_t* y_dec_ = nullptr;
+    int* block_counts_ = nullptr;
+    int* count_dev_ = nullptr;
+    Scratch scratch_;
+    // pinned host staging
+    int* count_host_ = nullptr;
+    int16_t* sym_host_ = nullptr;
+    uint8_t* idx_host_ = nullptr;
+    int8_t* ydec_host_ = nullptr;
+    int8_t* z_host_ = nullptr;
+    bool memory_has_value_ = false;
+
+    Graph graphs_[kPhaseSlots];
+    bool ran_eager_[kPhaseSlots] = {false};
+    int phase_kernels_[kPhaseSlots] = {0};
+    cudaStream_t main_ = nullptr;   // compute stream (graphs run here)
+    cudaStream_t copy_ = nullptr;   // D2H/H2D of symbols overlapping compute
+    cudaEvent_t ev_in_ = nullptr, ev_phase_ = nullptr, ev_copy_ = nullptr, ev_out_ = nullptr;
+    int* err_word_ = nullptr;
+    int last_count_ = 0;
+    int last_kernels_ = 0;
+    int dev_ = 0;
+};
+
+}  // namespace dcvc

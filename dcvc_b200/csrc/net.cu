@@ -1,0 +1,303 @@
+#include "net.h"
+
+#include "elementwise.cuh"
+#include "gemm_sm100.cuh"
+
+namespace dcvc {
+
+cudaError_t gemm_sm100(int dtype, const void* A, int lda, const void* W, const GemmParams& p,
+                       int epi, int bn, cudaStream_t stream);
+
+// ------------------------------------------------------------------------------ arena
+
+void* DeviceArena::alloc(size_t bytes)
+{
+    void* p = nullptr;
+    const size_t b = (bytes + 255) & ~size_t(255);
+    if (cudaMalloc(&p, b == 0 ? 256 : b) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    blocks_.push_back(p);
+    bytes_ += b;
+    return p;
+}
+
+void DeviceArena::clear()
+{
+    for (void* p : blocks_) {
+        cudaFree(p);
+    }
+    blocks_.clear();
+    bytes_ = 0;
+}
+
+// ------------------------------------------------------------------------------ parameters
+
+const HostTensor* ParamBuilder::get(const std::string& name, size_t ndim_min)
+{
+    auto it = sd_.find(name);
+    if (it == sd_.end()) {
+        fail("missing state-dict entry '" + name + "'");
+        return nullptr;
+    }
+    if (it->second.shape.size() < ndim_min) {
+        fail("state-dict entry '" + name + "' has too few dimensions");
+        return nullptr;
+    }
+    return &it->second;
+}
+
+const __half* ParamBuilder::upload_half(const std::vector<float>& v)
+{
+    std::vector<__half> h(v.size());
+    for (size_t i = 0; i < v.size(); ++i) {
+        h[i] = __float2half_rn(v[i]);
+    }
+    __half* d = arena_.alloc_n<__half>(v.size());
+    if (d == nullptr || cudaMemcpy(d, h.data(), h.size() * 2, cudaMemcpyHostToDevice) != cudaSuccess) {
+        fail("device allocation/copy of parameters failed");
+        return nullptr;
+    }
+    return d;
+}
+
+const float* ParamBuilder::upload_float(const std::vector<float>& v)
+{
+    float* d = arena_.alloc_n<float>(v.size());
+    if (d == nullptr || cudaMemcpy(d, v.data(), v.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
+        fail("device allocation/copy of parameters failed");
+        return nullptr;
+    }
+    return d;
+}
+
+const __half* ParamBuilder::half_rows(const std::string& name, int* rows, int* cols)
+{
+    const HostTensor* t = get(name, 2);
+    if (t == nullptr) {
+        return nullptr;
+    }
+    *rows = static_cast<int>(t->shape[0]);
+    *cols = static_cast<int>(t->numel() / t->shape[0]);
+    return upload_half(t->data);
+}
+
+Lin ParamBuilder::lin(const std::string& prefix, bool bias)
+{
+    Lin l;
+    const HostTensor* w = get(prefix + "weight", 2);
+    if (w == nullptr) {
+        return l;
+    }
+    l.cout = static_cast<int>(w->shape[0]);
+    l.cin = static_cast<int>(w->numel() / w->shape[0]);
+    if (w->numel() != static_cast<int64_t>(l.cout) * l.cin ||
+        (w->shape.size() == 4 && (w->shape[2] != 1 || w->shape[3] != 1))) {
+        fail("'" + prefix + "weight' is not a 1x1 convolution");
+        return l;
+    }
+    l.w = upload_half(w->data);
+    if (bias) {
+        const HostTensor* b = get(prefix + "bias");
+        if (b != nullptr) {
+            l.b = upload_float(b->data);
+        }
+    }
+    return l;
+}
+
+Dcb ParamBuilder::dcb(const std::string& p)
+{
+    Dcb d;
+    if (has(p + "adaptor.weight")) {
+        d.adaptor = true;
+        d.ad = lin(p + "adaptor.");
+    }
+    d.dc1 = lin(p + "dc.0.");
+    const HostTensor* dw = get(p + "dc.2.weight", 4);
+    const HostTensor* dwb = get(p + "dc.2.bias");
+    const HostTensor* w3 = get(p + "dc.3.weight", 2);
+    const HostTensor* b3 = get(p + "dc.3.bias");
+    if (dw == nullptr || dwb == nullptr || w3 == nullptr || b3 == nullptr) {
+        return d;
+    }
+    d.cdc = static_cast<int>(dw->shape[0]);
+    d.C = static_cast<int>(w3->shape[0]);
+    if (dw->shape[1] != 1 || dw->shape[2] != 3 || dw->shape[3] != 3) {
+        fail("'" + p + "dc.2.weight' is not a depthwise 3x3");
+        return d;
+    }
+    // depthwise weight [c, 1, 3, 3] -> tap-major [9][c]
+    std::vector<float> dwt(9 * static_cast<size_t>(d.cdc));
+    for (int c = 0; c < d.cdc; ++c) {
+        for (int k = 0; k < 9; ++k) {
+            dwt[static_cast<size_t>(k) * d.cdc + c] = dw->data[static_cast<size_t>(c) * 9 + k];
+        }
+    }
+    d.dw = upload_float(dwt);
+    // dc.3 bias with the depthwise bias folded in: b3 + W3 . b2 (layers_proxy.cpp:175-178)
+    std::vector<float> fb(d.C);
+    for (int o = 0; o < d.C; ++o) {
+        double s = b3->data[o];
+        for (int c = 0; c < d.cdc; ++c) {
+            s += static_cast<double>(w3->data[static_cast<size_t>(o) * d.cdc + c]) * dwb->data[c];
+        }
+        fb[o] = static_cast<float>(s);
+    }
+    d.dc2.cin = d.cdc;
+    d.dc2.cout = d.C;
+    d.dc2.w = upload_half(w3->data);
+    d.dc2.b = upload_float(fb);
+    d.ffn1 = lin(p + "ffn.0.");
+    d.ffn2 = lin(p + "ffn.2.");
+    d.cffn = d.ffn2.cin;
+    d.cin = d.adaptor ? d.ad.cin : d.C;
+    if (ok() && (d.dc1.cin != d.C || d.dc1.cout != d.cdc || d.ffn1.cout != 4 * d.cffn ||
+                 d.ffn1.cin != d.C || d.ffn2.cout != d.C || (d.adaptor && d.ad.cout != d.C))) {
+        fail("inconsistent DepthConvBlock shapes under '" + p + "'");
+    }
+    return d;
+}
+
+DownBlock ParamBuilder::down(const std::string& p)
+{
+    DownBlock b;
+    const HostTensor* w = get(p + "down.weight", 2);
+    const HostTensor* bias = get(p + "down.bias");
+    if (w == nullptr || bias == nullptr) {
+        return b;
+    }
+    const int cout = static_cast<int>(w->shape[0]);
+    const int k4 = static_cast<int>(w->numel() / cout);
+    const int cin = k4 / 4;
+    // K index c*4 + dy*2 + dx (pixel_unshuffle order) -> (dy*2 + dx)*cin + c
+    std::vector<float> pw(static_cast<size_t>(cout) * k4);
+    for (int o = 0; o < cout; ++o) {
+        for (int c = 0; c < cin; ++c) {
+            for (int s = 0; s < 4; ++s) {
+                pw[static_cast<size_t>(o) * k4 + s * cin + c] =
+                    w->data[static_cast<size_t>(o) * k4 + c * 4 + s];
+            }
+        }
+    }
+    b.down.cin = k4;
+    b.down.cout = cout;
+    b.down.w = upload_half(pw);
+    b.down.b = upload_float(bias->data);
+    b.dcb = dcb(p + "conv.");
+    return b;
+}
+
+UpBlock ParamBuilder::up(const std::string& p)
+{
+    UpBlock b;
+    b.up = subpel(p + "up.");
+    b.dcb = dcb(p + "conv.");
+    return b;
+}
+
+Lin ParamBuilder::subpel(const std::string& p)
+{
+    Lin b;
+    if (has(p + "conv.0.bias")) {
+        fail("'" + p + "conv.0' has a bias: only the bias-free sub-pixel up-sampling is supported");
+        return b;
+    }
+    const HostTensor* w = get(p + "conv.0.weight", 2);
+    if (w == nullptr) {
+        return b;
+    }
+    const int n4 = static_cast<int>(w->shape[0]);
+    const int cin = static_cast<int>(w->numel() / n4);
+    const int cout = n4 / 4;
+    // row c*4 + dy*2 + dx (pixel_shuffle order) -> (dy*2 + dx)*cout + c
+    std::vector<float> pw(static_cast<size_t>(n4) * cin);
+    for (int c = 0; c < cout; ++c) {
+        for (int s = 0; s < 4; ++s) {
+            std::copy(w->data.begin() + static_cast<size_t>(c * 4 + s) * cin,
+                      w->data.begin() + static_cast<size_t>(c * 4 + s + 1) * cin,
+                      pw.begin() + static_cast<size_t>(s * cout + c) * cin);
+        }
+    }
+    b.cin = cin;
+    b.cout = n4;
+    b.w = upload_half(pw);
+    return b;
+}
+
+Lin ParamBuilder::conv3x3s2(const std::string& p)
+{
+    Lin l;
+    const HostTensor* w = get(p + "weight", 4);
+    const HostTensor* b = get(p + "bias");
+    if (w == nullptr || b == nullptr) {
+        return l;
+    }
+    const int cout = static_cast<int>(w->shape[0]);
+    const int cin = static_cast<int>(w->shape[1]);
+    if (w->shape[2] != 3 || w->shape[3] != 3) {
+        fail("'" + p + "weight' is not 3x3");
+        return l;
+    }
+    // [o][c][ky][kx] -> [o][(ky*3 + kx)*cin + c]
+    std::vector<float> pw(static_cast<size_t>(cout) * 9 * cin);
+    for (int o = 0; o < cout; ++o) {
+        for (int c = 0; c < cin; ++c) {
+            for (int k = 0; k < 9; ++k) {
+                pw[(static_cast<size_t>(o) * 9 + k) * cin + c] =
+                    w->data[(static_cast<size_t>(o) * cin + c) * 9 + k];
+            }
+        }
+    }
+    l.cin = 9 * cin;
+    l.cout = cout;
+    l.w = upload_half(pw);
+    l.b = upload_float(b->data);
+    return l;
+}
+
+// ------------------------------------------------------------------------------ execution
+
+void gemm(Launch& L, const Lin& lin, int epi, const __half* x, int ldx, int M, __half* out,
+          int ldo, const __half* res, int ldr, const __half* q, int sub_w)
+{
+    GemmParams p{};
+    p.M = M;
+    p.N = lin.cout;
+    p.K = lin.cin;
+    p.bias = lin.b;
+    p.res = res;
+    p.ldr = ldr;
+    p.qscale = q;
+    p.out = out;
+    p.ldo = ldo;
+    p.sub_w = sub_w;
+    p.sub_cout = epi == kEpiSubpel ? lin.cout / 4 : 0;
+    p.err = L.err_word;
+    L.note(gemm_sm100(0, x, ldx, lin.w, p, epi, 0, L.s));
+}
+
+void run_dcb(Launch& L, const Dcb& d, const __half* x, int ldx, int H, int W, __half* out, int ldo,
+             Scratch& s, const __half* q)
+{
+    const int M = H * W;
+    const __half* xin = x;
+    int ldin = ldx;
+    if (d.adaptor) {
+        gemm(L, d.ad, kEpiBias, x, ldx, M, s.t0, d.C);
+        xin = s.t0;
+        ldin = d.C;
+    }
+    gemm(L, d.dc1, kEpiBiasWsilu, xin, ldin, M, s.t1, d.cdc);
+    L.note(launch_dwconv3x3(s.t1, H, W, d.cdc, d.cdc, d.dw, s.t2, d.cdc, L.s));
+    gemm(L, d.dc2, kEpiBiasRes, s.t2, d.cdc, M, s.t3, d.C, xin, ldin);
+    gemm(L, d.ffn1, kEpiQuad, s.t3, d.C, M, s.t4, d.cffn);
+    if (q != nullptr) {
+        gemm(L, d.ffn2, kEpiBiasResQ, s.t4, d.cffn, M, out, ldo, s.t3, d.C, q);
+    } else {
+        gemm(L, d.ffn2, kEpiBiasRes, s.t4, d.cffn, M, out, ldo, s.t3, d.C);
+    }
+}
+
+}  // namespace dcvc

@@ -1,0 +1,141 @@
+// Network building blocks of the codec runtime: parameter containers, weight preparation from a
+// state dict, and launch sequences for the reference's layer proxies
+// (src/layers/extensions/inference/layers_proxy.cpp).
+#pragma once
+
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <map>
+#include <string>
+#include <vector>
+
+namespace dcvc {
+
+// Owns device allocations; released together.
+class DeviceArena {
+public:
+    DeviceArena() = default;
+    DeviceArena(const DeviceArena&) = delete;
+    DeviceArena& operator=(const DeviceArena&) = delete;
+    ~DeviceArena() { clear(); }
+    void* alloc(size_t bytes);  // nullptr on failure
+    template <typename T>
+    T* alloc_n(size_t n)
+    {
+        return static_cast<T*>(alloc(n * sizeof(T)));
+    }
+    void clear();
+    size_t bytes() const { return bytes_; }
+
+private:
+    std::vector<void*> blocks_;
+    size_t bytes_ = 0;
+};
+
+// Host copy of one state-dict entry, converted to float.
+struct HostTensor {
+    std::vector<int64_t> shape;
+    std::vector<float> data;
+    int64_t numel() const
+    {
+        int64_t n = 1;
+        for (auto s : shape) n *= s;
+        return n;
+    }
+};
+using StateDict = std::map<std::string, HostTensor>;
+
+// 1x1 convolution: w [cout, cin] (FP16, K-major), b [cout] (FP32, may be null).
+struct Lin {
+    const __half* w = nullptr;
+    const float* b = nullptr;
+    int cin = 0, cout = 0;
+};
+
+// DepthConvBlock (layers.py:128-159; layers_proxy.cpp:71-206).
+struct Dcb {
+    bool adaptor = false;
+    Lin ad;
+    Lin dc1;
+    const float* dw = nullptr;  // [9][cdc] FP32
+    Lin dc2;                    // bias with the depthwise bias folded in
+    Lin ffn1;                   // [4*cffn, C], rows 4c+k as in the reference
+    Lin ffn2;
+    int C = 0, cdc = 0, cffn = 0, cin = 0;
+};
+
+// ResidualBlockWithStride2: pixel_unshuffle(2) + 1x1 (K permuted to (dy, dx, c)) + DCB.
+struct DownBlock {
+    Lin down;
+    Dcb dcb;
+};
+
+// ResidualBlockUpsample without bias: 1x1 with rows permuted to (dy, dx, c) + shuffle store + DCB.
+struct UpBlock {
+    Lin up;
+    Dcb dcb;
+};
+
+// Builds device parameters from a state dict.  Errors are reported through `ok`/`err`.
+class ParamBuilder {
+public:
+    ParamBuilder(const StateDict& sd, DeviceArena& arena) : sd_(sd), arena_(arena) {}
+    bool has(const std::string& name) const { return sd_.count(name) != 0; }
+    Lin lin(const std::string& prefix, bool bias = true);
+    Dcb dcb(const std::string& prefix);
+    DownBlock down(const std::string& prefix);
+    UpBlock up(const std::string& prefix);
+    Lin subpel(const std::string& prefix);  // prefix + "conv.0.weight", rows permuted
+    Lin conv3x3s2(const std::string& prefix);  // weight K permuted to (ky, kx, c)
+    const __half* half_rows(const std::string& name, int* rows, int* cols);
+    bool ok() const { return err_.empty(); }
+    const std::string& error() const { return err_; }
+
+private:
+    const HostTensor* get(const std::string& name, size_t ndim_min = 1);
+    const __half* upload_half(const std::vector<float>& v);
+    const float* upload_float(const std::vector<float>& v);
+    void fail(const std::string& m)
+    {
+        if (err_.empty()) err_ = m;
+    }
+
+    const StateDict& sd_;
+    DeviceArena& arena_;
+    std::string err_;
+};
+
+// Per-level scratch for DCB execution.
+struct Scratch {
+    __half* t0 = nullptr;  // adaptor output
+    __half* t1 = nullptr;  // dc.0 output
+    __half* t2 = nullptr;  // depthwise output
+    __half* t3 = nullptr;  // dc output (+ residual)
+    __half* t4 = nullptr;  // ffn chunk-add output
+};
+
+struct Launch {
+    cudaStream_t s;
+    int* err_word;
+    cudaError_t first = cudaSuccess;
+    int kernels = 0;  // kernels enqueued through this context
+    void note(cudaError_t e, int n = 1)
+    {
+        kernels += n;
+        if (first == cudaSuccess && e != cudaSuccess) first = e;
+    }
+};
+
+// out[M, cout] (pitch ldo) = epilogue(x[M, cin] (pitch ldx) . lin)
+void gemm(Launch& L, const Lin& lin, int epi, const __half* x, int ldx, int M, __half* out,
+          int ldo, const __half* res = nullptr, int ldr = 0, const __half* q = nullptr,
+          int sub_w = 0);
+
+// DepthConvBlockProxy::forward.  `out` may alias `x` when the block has no adaptor input wider
+// than its output (the last GEMM reads only its own scratch and residual).
+void run_dcb(Launch& L, const Dcb& d, const __half* x, int ldx, int H, int W, __half* out, int ldo,
+             Scratch& s, const __half* q = nullptr);
+
+}  // namespace dcvc

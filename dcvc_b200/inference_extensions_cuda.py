@@ -1,0 +1,190 @@
+"""Drop-in for the reference's `inference_extensions_cuda` module (src/layers/extensions/
+inference/bind.cpp:11-39): the same proxy classes, methods, argument meaning and return values,
+backed by the sm_100a runtime in libdcvc_b200.so.
+
+DMCHTSProxy is implemented.  DMCIProxy, DMCHTLProxy and DMCLDProxy raise NotImplementedError on
+construction (the models then report that the CUDA implementation is unavailable, as the
+reference does when its extension is missing, video_model_ht.py:428-432).
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _native as N
+
+_lib = N.lib
+_vp = ctypes.c_void_p
+
+
+def _proto(name, argtypes):
+    f = getattr(_lib, name)
+    f.restype = ctypes.c_int
+    f.argtypes = argtypes
+    return f
+
+
+_proto("dcvc_hts_create", [ctypes.POINTER(_vp)])
+_proto("dcvc_hts_destroy", [_vp])
+_proto("dcvc_hts_set_param", [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_char_p),
+                              ctypes.POINTER(_vp), ctypes.POINTER(ctypes.c_int64),
+                              ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                              ctypes.POINTER(ctypes.c_int), ctypes.c_float])
+_proto("dcvc_hts_add_ref_feature", [_vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp])
+_proto("dcvc_hts_compress", [_vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                             ctypes.c_int, ctypes.c_int, _vp, ctypes.POINTER(_vp),
+                             ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_int)])
+_proto("dcvc_hts_decompress", [_vp, _vp, ctypes.c_size_t, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                               ctypes.c_int, ctypes.c_int, _vp, ctypes.POINTER(_vp)])
+_proto("dcvc_hts_buffer", [_vp, ctypes.c_char_p, ctypes.POINTER(_vp), ctypes.POINTER(ctypes.c_int),
+                           ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)])
+_proto("dcvc_hts_stats", [_vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                          ctypes.POINTER(ctypes.c_size_t)])
+
+_DTYPES = {torch.float16: 0, torch.bfloat16: 1, torch.float32: 2, torch.int32: 3, torch.int64: 4}
+FRAMES = 8
+
+
+class _DeviceView:
+    """__cuda_array_interface__ over memory owned by the native runtime (no copy)."""
+
+    def __init__(self, ptr, shape, typestr="<f2"):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr,
+                                         "data": (int(ptr), False), "version": 3, "strides": None}
+
+
+def _stream():
+    return _vp(torch.cuda.current_stream().cuda_stream)
+
+
+def _channels_last_data(t, name):
+    if not t.is_cuda or t.dtype != torch.float16 or t.dim() != 4 or t.shape[0] != 1:
+        raise ValueError(f"{name} must be a [1, C, H, W] float16 CUDA tensor")
+    if not t.is_contiguous(memory_format=torch.channels_last):
+        t = t.contiguous(memory_format=torch.channels_last)
+    return t
+
+
+class DMCHTSProxy:
+    """Chunk codec of the HT-S video model (dmc_hts_proxy.h:215-355).  One instance per stream;
+    not re-entrant."""
+
+    def __init__(self):
+        h = _vp()
+        N.check(_lib.dcvc_hts_create(ctypes.byref(h)), "DMCHTSProxy()")
+        self._h = h
+        self._frames = None
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            _lib.dcvc_hts_destroy(h)
+            self._h = None
+
+    def set_param(self, state_dict, skip_threshold):
+        """state_dict: the model state dict with the four CDF entries added
+        (common_model.py:64-70); tensors may be on any device, in f16/bf16/f32/int."""
+        keep = []
+        names, ptrs, shapes, ndims, dtypes, on_dev = [], [], [], [], [], []
+        for k, v in state_dict.items():
+            if not isinstance(v, torch.Tensor):
+                v = torch.as_tensor(np.asarray(v))
+            if v.dtype not in _DTYPES:
+                v = v.float()
+            v = v.contiguous()
+            keep.append(v)
+            names.append(k.encode())
+            ptrs.append(v.data_ptr())
+            shp = list(v.shape)[:4] + [0] * (4 - min(4, v.dim()))
+            if v.dim() > 4:
+                raise ValueError(f"state-dict entry {k} has more than 4 dimensions")
+            shapes.extend(shp)
+            ndims.append(v.dim())
+            dtypes.append(_DTYPES[v.dtype])
+            on_dev.append(1 if v.is_cuda else 0)
+        n = len(names)
+        if any(v.is_cuda for v in keep):
+            torch.cuda.current_stream().synchronize()
+        N.check(_lib.dcvc_hts_set_param(
+            self._h, n, (ctypes.c_char_p * n)(*names), (_vp * n)(*ptrs),
+            (ctypes.c_int64 * (4 * n))(*shapes), (ctypes.c_int * n)(*ndims),
+            (ctypes.c_int * n)(*dtypes), (ctypes.c_int * n)(*on_dev), float(skip_threshold)),
+            "set_param")
+
+    def add_ref_feature_from_frame(self, frame, apply_adaptor=True):
+        frame = _channels_last_data(frame, "frame")
+        if frame.shape[1] != 3:
+            raise ValueError("frame must have 3 channels")
+        N.check(_lib.dcvc_hts_add_ref_feature(self._h, frame.data_ptr(), frame.shape[2],
+                                              frame.shape[3], 1 if apply_adaptor else 0,
+                                              _stream()), "add_ref_feature_from_frame")
+
+    def compress(self, x, qp, reset_feature_memory, padding_b, padding_r):
+        """x: [1, 24, H, W] float16 CUDA (8 frames).  Returns (uint8 array, ec_parallel)."""
+        x = _channels_last_data(x, "x")
+        data = _vp()
+        size = ctypes.c_size_t()
+        ecp = ctypes.c_int()
+        N.check(_lib.dcvc_hts_compress(self._h, x.data_ptr(), x.shape[2], x.shape[3], int(qp),
+                                       1 if reset_feature_memory else 0, int(padding_b),
+                                       int(padding_r), _stream(), ctypes.byref(data),
+                                       ctypes.byref(size), ctypes.byref(ecp)), "compress")
+        if size.value == 0:
+            return np.zeros(0, dtype=np.uint8), ecp.value
+        buf = np.ctypeslib.as_array(ctypes.cast(data, ctypes.POINTER(ctypes.c_uint8)),
+                                    shape=(size.value,)).copy()
+        return buf, ecp.value
+
+    def decompress(self, bit_stream, qp, height, width, entropy_coder_parallel,
+                   reset_feature_memory):
+        """Returns 8 [1, 3, Hp, Wp] float16 CUDA tensors (channels last) that alias the proxy's
+        buffers and are overwritten by the next call (dmc_hts_proxy.h:347)."""
+        bs = np.ascontiguousarray(np.asarray(bit_stream, dtype=np.uint8).reshape(-1))
+        frames = (_vp * FRAMES)()
+        N.check(_lib.dcvc_hts_decompress(self._h, bs.ctypes.data, bs.size, int(qp), int(height),
+                                         int(width), int(entropy_coder_parallel),
+                                         1 if reset_feature_memory else 0, _stream(), frames),
+                "decompress")
+        hp = (int(height) + 15) // 16 * 16
+        wp = (int(width) + 15) // 16 * 16
+        out = []
+        for i in range(FRAMES):
+            t = torch.as_tensor(_DeviceView(frames[i], (1, hp, wp, 3)), device="cuda")
+            out.append(t.permute(0, 3, 1, 2))
+        return out
+
+    def buffer(self, name):
+        """Copy of an internal per-stream buffer as a [rows, cols] float16 tensor (see
+        dcvc_hts_buffer)."""
+        ptr, r, c, ld = _vp(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        N.check(_lib.dcvc_hts_buffer(self._h, name.encode(), ctypes.byref(ptr), ctypes.byref(r),
+                                     ctypes.byref(c), ctypes.byref(ld)), "buffer")
+        full = torch.as_tensor(_DeviceView(ptr.value, (r.value, ld.value)), device="cuda")
+        torch.cuda.synchronize()
+        return full[:, : c.value].clone()
+
+    def stats(self):
+        """(symbols coded by the last call, kernels it enqueued, device bytes held)."""
+        s, k, b = ctypes.c_int(), ctypes.c_int(), ctypes.c_size_t()
+        N.check(_lib.dcvc_hts_stats(self._h, ctypes.byref(s), ctypes.byref(k), ctypes.byref(b)),
+                "stats")
+        return s.value, k.value, b.value
+
+
+class _Unavailable:
+    _what = "this proxy"
+
+    def __init__(self, *a, **k):
+        raise NotImplementedError(f"{self._what} is not implemented by dcvc_b200 yet")
+
+
+class DMCIProxy(_Unavailable):
+    _what = "DMCIProxy (intra model)"
+
+
+class DMCHTLProxy(_Unavailable):
+    _what = "DMCHTLProxy (HT-L model)"
+
+
+class DMCLDProxy(_Unavailable):
+    _what = "DMCLDProxy (LD model)"

@@ -37,6 +37,9 @@ extern "C" {
 /* element types */
 #define DCVC_F16 0
 #define DCVC_BF16 1
+#define DCVC_F32 2
+#define DCVC_I32 3
+#define DCVC_I64 4
 
 /* 1x1-conv GEMM epilogues (dcvc_conv1x1) */
 #define DCVC_EPI_BIAS 0        /* conv1x1_bias                       */
@@ -110,6 +113,47 @@ int dcvc_rans_decode_begin(void* handle, const uint8_t* data, size_t size, int e
  * the reverse order of encoding.  DCVC_CORRUPT_STREAM if a sub-stream runs out of bytes. */
 int dcvc_rans_decode_z(void* handle, int n, int cdf_offset, int ch, int8_t* out);
 int dcvc_rans_decode_y(void* handle, const uint8_t* idx, int n, int8_t* out);
+
+/* ------------------------------------------------------------------ HT-S chunk codec */
+
+/* One handle = one video stream (its temporal context lives on the device inside the handle),
+ * the counterpart of DMCHTSProxy (src/layers/extensions/inference/dmc_hts_proxy.h:215-355,
+ * bind.cpp:26-31).  A handle is not re-entrant: one call at a time.  Work is ordered after the
+ * work already queued on `stream` and the caller's stream waits for the call's GPU work. */
+int dcvc_hts_create(void** handle);
+int dcvc_hts_destroy(void* handle);
+/* set_param(state_dict, skip_threshold) (dmc_hts_proxy.cpp:712-762): n named tensors of the
+ * DMC state dict plus gaussian_encoder.{quantized_cdf,cdf_length} and
+ * bit_estimator_z.{quantized_cdf,cdf_length}.  shapes: n x 4 int64 (first ndims[i] used);
+ * dtypes: DCVC_F16/BF16/F32/I32/I64; on_device[i] != 0 if data[i] is device memory. */
+int dcvc_hts_set_param(void* handle, int n, const char* const* names, const void* const* data,
+                       const int64_t* shapes, const int* ndims, const int* dtypes,
+                       const int* on_device, float skip_threshold);
+/* add_ref_feature_from_frame (dmc_hts_proxy.cpp:492-502): frame = [height, width, 3] FP16
+ * (a [1, 3, H, W] channels-last tensor), height and width multiples of 16.  Sizes the
+ * per-resolution buffers. */
+int dcvc_hts_add_ref_feature(void* handle, const void* frame, int height, int width,
+                             int apply_adaptor, void* stream);
+/* compress (dmc_hts_proxy.cpp:504-585): x = [height, width, 24] FP16 (8 frames, channels
+ * last); height + pad_b, width + pad_r must equal the reference frame size.  On success *bytes
+ * (valid until the next call on the handle) holds the MLCodec rANS payload and *ec_parallel
+ * its sub-stream count. */
+int dcvc_hts_compress(void* handle, const void* x, int height, int width, int qp, int reset,
+                      int pad_b, int pad_r, void* stream, const uint8_t** bytes, size_t* nbytes,
+                      int* ec_parallel);
+/* decompress (dmc_hts_proxy.cpp:587-710): height/width are the picture size of the stream.
+ * frames receives 8 device pointers to [Hp, Wp, 3] FP16 reconstructions in [-0.5, 0.5], owned
+ * by the handle and overwritten by the next call.  DCVC_CORRUPT_STREAM for a payload that does
+ * not decode. */
+int dcvc_hts_decompress(void* handle, const uint8_t* bytes, size_t nbytes, int qp, int height,
+                        int width, int ec_parallel, int reset, void* stream, void** frames);
+/* Read-only view of a per-stream device buffer (FP16 rows x cols, pitch ld): "y_hat", "y_q",
+ * "memory", "ctx", "feature_p", "common", "feature_i".  For inspection and tests; no
+ * counterpart in the reference. */
+int dcvc_hts_buffer(void* handle, const char* name, const void** ptr, int* rows, int* cols,
+                    int* ld);
+/* symbols coded by the last call, kernels it enqueued, device bytes held by the handle */
+int dcvc_hts_stats(void* handle, int* symbols, int* kernels, size_t* device_bytes);
 
 #ifdef __cplusplus
 }

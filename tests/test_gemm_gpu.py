@@ -51,10 +51,16 @@ CASES = [
     ("EPI_BIAS_RES_Q", 3000, 512, 256, torch.float16, 0),
     ("EPI_BIAS_RES2", 3000, 256, 256, torch.float16, 0),
     ("EPI_QUAD", 32640, 1024, 512, torch.float16, 0),
-    ("EPI_QUAD", 2040, 1024, 256, torch.float16, 128),
+    ("EPI_QUAD", 2040, 1024, 256, torch.float16, 0),
+    ("EPI_QUAD", 8160, 3072, 768, torch.float16, 0),
+    ("EPI_BIAS_RES", 700, 192, 256, torch.float16, 64),
+    ("EPI_BIAS_WSILU", 1300, 256, 128, torch.float16, 64),
+    ("EPI_BIAS_RES_Q", 2000, 256, 512, torch.float16, 128),
+    ("EPI_BIAS_RES2", 2100, 512, 512, torch.float16, 256),
     ("EPI_BIAS_Q", 1500, 512, 512, torch.float16, 0),
     ("EPI_BIAS", 5000, 512, 512, torch.bfloat16, 0),
     ("EPI_QUAD", 5000, 1024, 512, torch.bfloat16, 0),
+    ("EPI_BIAS_RES", 5000, 512, 256, torch.bfloat16, 0),
 ]
 
 
