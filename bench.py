@@ -1,0 +1,378 @@
+#!/usr/bin/env python
+"""Benchmark of the DCVC-UF HT-S chunk encode+decode hot path on B200.
+
+Workload (one step = one request): one 8-frame 1920x1080 YUV420 chunk (padded to 1920x1088)
+compressed by one proxy and decompressed by a second one, QP cycling 0, 21, 42, 63, FP16
+activations/weights with FP32 accumulation, synthetic content (dcvc_b200.synthetic), random-init
+weights of the HT-S architecture from seed 0 (see `weights` in the JSON config).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl dcvc_b200|reference]
+
+Under torchrun every rank runs its own stream pair on its own GPU (weak scaling, no data-path
+collective); the timed region is bracketed by a barrier + device synchronisation and the time is
+the maximum over ranks.  `--impl reference` times the reference's CPU path instead (the network
+restated on PyTorch CPU in FP32 plus the reference's own rANS coder compiled from its sources) on
+the host cores, rank 0 only.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+import torch
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "1080p YUV420 enc+dec frames/s, batched BF16/FP8 vs plain; p50/p99 chunk latency"
+UNIT = "frames/s"
+QPS = (0, 21, 42, 63)
+FRAMES = 8
+SKIP_THRES = 0.15
+WEIGHTS = ("seed-0 random init of the HT-S architecture (equal to the reference DMC() under "
+           "torch.manual_seed(0)), residual-branch output convs scaled x0.1 so activations stay "
+           "finite in FP16 (the plain init grows ~1e14x per chunk, in FP64 too)")
+PUBLISHED = {"enc_fps_b200": 1415.1, "dec_fps_b200": 945.8, "combined_fps_derived": 567.0}
+QUAD_SHAPE = (32640, 1024, 512)  # ffn.0 of a 512-channel dcb2 DepthConvBlock at 1080p
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=4)
+    ap.add_argument("--impl", default="dcvc_b200", choices=["dcvc_b200", "reference"])
+    ap.add_argument("--height", type=int, default=1080)
+    ap.add_argument("--width", type=int, default=1920)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload_config(H, W, n):
+    return {
+        "workload": f"DCVC-UF HT-S {W}x{H} YUV420 8-frame chunk encode+decode, QPs 0/21/42/63 "
+                    "one request at a time (plain FP16 form)",
+        "model": "DCVC-UF HT-S (DMC, ModelStructure.HTS)",
+        "resolution": f"{W}x{H}",
+        "chunk_frames": FRAMES,
+        "qps": list(QPS),
+        "skip_threshold": SKIP_THRES,
+        "weights": WEIGHTS,
+        "l2": "no flush: every step's working set (weights 162 MB + activations > 1 GB) exceeds the 126 MB L2",
+        "global_batch": n,
+        "parallelism": f"{n} independent stream(s), one per GPU",
+    }
+
+
+# ----------------------------------------------------------------------------- helpers
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        uuid = None
+        try:
+            uuid = "GPU-" + str(torch.cuda.get_device_properties(device_index).uuid)
+        except Exception:
+            pass
+        cmd = ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits", "-lms", "200"]
+        if uuid:
+            cmd += ["-i", uuid]
+        try:
+            self.p = subprocess.Popen(cmd, stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        os.unlink(self.f.name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        loaded = [s for s in sm if s > 0.5 * max(sm)] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": max(smax),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return d["hbm_gbs"], d["bf16_tflops"], "measured"
+    except Exception:
+        return 6650.0, 1590.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per launch of the quad GEMM from the committed ncu summary, or None."""
+    path = os.path.join(ROOT, "profiles", "gemm_quad_1080p.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return int(line.split(":")[1].strip())
+    except OSError:
+        pass
+    return None
+
+
+def roofline_quad(stream):
+    """Times the dominant kernel (the quad GEMM of the 512-channel blocks at 1080p) on its
+    launching stream with CUDA events and relates it to the measured tensor peak."""
+    from dcvc_b200 import _native as N, ops
+    M, Nn, K = QUAD_SHAPE
+    g = torch.Generator(device="cuda").manual_seed(7)
+    a = torch.randn(M, K, device="cuda", generator=g).half()
+    w = (torch.randn(Nn, K, device="cuda", generator=g) / K ** 0.5).half()
+    b = torch.zeros(Nn, device="cuda")
+    out = torch.empty(M, Nn // 4, device="cuda", dtype=torch.float16)
+    with torch.cuda.stream(stream):
+        for _ in range(5):
+            ops.conv1x1(a, w, b, N.EPI_QUAD, out=out)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = 50
+        e0.record(stream)
+        for _ in range(reps):
+            ops.conv1x1(a, w, b, N.EPI_QUAD, out=out)
+        e1.record(stream)
+    e1.synchronize()
+    sec = e0.elapsed_time(e1) / 1e3 / reps
+    flops = 2.0 * M * Nn * K
+    _, peak_tf, kind = measured_peaks()
+    achieved = flops / sec / 1e12
+    return {"kernel": "gemm_sm100_kernel<half, 256, quad> (ffn.0 + WSiLU chunk-add, M=32640 N=1024 K=512)",
+            "bound": "tensor", "achieved": round(achieved, 1), "peak": peak_tf, "unit": "TFLOP/s",
+            "frac": round(achieved / peak_tf, 3), "peak_kind": f"{kind} bf16 burst",
+            "us_per_launch": round(sec * 1e6, 2), "flops_per_launch": flops,
+            "traffic": profiled_traffic()}
+
+
+def cpu_baseline(H, W, strip_rows=272, chunks=2):
+    """The reference's CPU path (network on PyTorch CPU FP32 + the reference's own rANS coder)
+    on the host cores, on a bounded sample: `chunks` chunks of a W x strip_rows strip of the
+    same content, scaled to 1080p frames/s by pixel count."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import hts_oracle
+    from dcvc_b200 import synthetic
+    from dcvc_b200.entropy_tables import add_cdf_to_state_dict
+    from dcvc_b200.model_spec import calibrated_hts_state_dict
+    kind = "port"
+    try:
+        hts_oracle.use_reference_coder(True)
+        coder = "reference rANS (compiled from the reference sources)"
+    except Exception:
+        coder = "rANS C restatement"
+    cores = os.cpu_count() or 1
+    torch.set_num_threads(cores)
+    sd = add_cdf_to_state_dict(calibrated_hts_state_dict(0))
+    sd = {k: (v.half() if v.is_floating_point() else v) for k, v in sd.items()}
+    hs = strip_rows
+    enc = hts_oracle.HtsOracle(sd, SKIP_THRES, torch.float32)
+    dec = hts_oracle.HtsOracle(sd, SKIP_THRES, torch.float32)
+    ref = synthetic.padded_reference_frame(synthetic.video_chunk_yuv420(2, hs, W, 1, 0)[0], device="cpu")
+    enc.add_ref_feature_from_frame(ref, True)
+    dec.add_ref_feature_from_frame(ref, False)
+    pr, pb = synthetic.padding_for(hs, W)
+    xs = [synthetic.to_model_input(synthetic.video_chunk_yuv420(2, hs, W, 8, 8 * k), device="cpu")
+          for k in range(chunks)]
+    t0 = time.perf_counter()
+    for k in range(chunks):
+        qp = QPS[k % len(QPS)]
+        r = enc.compress(xs[k], qp, False, pb, pr)
+        dec.decompress(r["bit_stream"], qp, hs, W, r["ec_parallel"], False)
+    sec = time.perf_counter() - t0
+    fps_strip = FRAMES * chunks / sec
+    fps_1080 = fps_strip * (hs * W) / (H * W)
+    return {"value": round(fps_1080, 4), "unit": UNIT, "cores": cores, "kind": kind,
+            "sample": f"{chunks} chunk(s) enc+dec of a {W}x{hs} strip (FP32 PyTorch CPU network + "
+                      f"{coder}), scaled to {W}x{H} by pixel count; {sec:.1f} s"}
+
+
+# ----------------------------------------------------------------------------- arms
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return  # rank 0 alone times the CPU path
+    H, W = args.height, args.width
+    per_step = []
+    base = None
+    for i in range(args.warmup + args.steps):
+        r = cpu_baseline(H, W, strip_rows=144, chunks=1)
+        if i >= args.warmup:
+            per_step.append(r["value"])
+        base = r
+    value = statistics.median(per_step)
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(FRAMES / value * 1e3, 1), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": workload_config(H, W, args.gpus),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": base["cores"], "kind": base["kind"],
+                         "sample": "per step: " + base["sample"]},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def run_gpu(args):
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    from dcvc_b200 import synthetic
+    from dcvc_b200.entropy_tables import add_cdf_to_state_dict
+    from dcvc_b200.inference_extensions_cuda import DMCHTSProxy
+    from dcvc_b200.model_spec import calibrated_hts_state_dict
+
+    H, W = args.height, args.width
+    sd = add_cdf_to_state_dict(calibrated_hts_state_dict(0))
+    sd = {k: (v.half().cuda() if v.is_floating_point() else v) for k, v in sd.items()}
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    enc, dec = DMCHTSProxy(), DMCHTSProxy()
+    enc.set_param(sd, SKIP_THRES)
+    dec.set_param(sd, SKIP_THRES)
+    del sd
+    # stream content differs per rank
+    seed = 2 + rank
+    ref = synthetic.padded_reference_frame(synthetic.video_chunk_yuv420(seed, H, W, 1, 0)[0])
+    enc.add_ref_feature_from_frame(ref, True)
+    dec.add_ref_feature_from_frame(ref, False)
+    pr, pb = synthetic.padding_for(H, W)
+    host_chunks = [synthetic.video_chunk_yuv420(seed, H, W, FRAMES, FRAMES * k) for k in range(2)]
+    xs = [synthetic.to_model_input(c) for c in host_chunks]
+
+    def step(i, x):
+        qp = QPS[i % len(QPS)]
+        bits, ecp = enc.compress(x, qp, False, pb, pr)
+        return dec.decompress(bits, qp, H, W, ecp, False), bits.size
+
+    for i in range(args.warmup):
+        step(i, xs[i % 2])
+    torch.cuda.synchronize()
+
+    # ---------------- timed region: inputs resident in HBM
+    kernels_per_step = enc.stats()[1] + dec.stats()[1]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    marks = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    marks[0].record(stream)
+    nbytes = []
+    for i in range(args.steps):
+        _, nb = step(args.warmup + i, xs[i % 2])
+        nbytes.append(nb)
+        marks[i + 1].record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    if world > 1:
+        dist.barrier()
+    ms = marks[0].elapsed_time(marks[-1])
+    lat = [marks[i].elapsed_time(marks[i + 1]) for i in range(args.steps)]
+    t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = FRAMES * args.steps * world / (ms_max / 1e3)
+
+    # ---------------- end to end through the proxy API from pinned host memory
+    x_host = [x.cpu().pin_memory() for x in xs]
+    x_dev = torch.empty_like(xs[0])
+    hp, wp = (H + 15) // 16 * 16, (W + 15) // 16 * 16
+    out_host = torch.empty((FRAMES, 3, hp, wp), dtype=torch.float16).pin_memory()
+    h2d = x_host[0].numel() * 2
+    d2h = out_host.numel() * 2
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(args.steps):
+        x_dev.copy_(x_host[i % 2], non_blocking=True)
+        frames, _ = step(args.warmup + i, x_dev)
+        for f in range(FRAMES):
+            out_host[f].copy_(frames[f][0], non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t2 = torch.tensor([e0.elapsed_time(e1)], device="cuda", dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t2, op=dist.ReduceOp.MAX)
+    e2e = FRAMES * args.steps * world / (float(t2.item()) / 1e3)
+
+    roof = roofline_quad(stream)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(H, W)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    lat_sorted = sorted(lat)
+    out = {
+        "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f16",
+        "data": "synthetic", "config": workload_config(H, W, world),
+        "latency_ms": {"p50": round(float(np.percentile(lat_sorted, 50)), 3),
+                       "p99": round(float(np.percentile(lat_sorted, 99)), 3)},
+        "bytes_per_chunk": {"mean": int(np.mean(nbytes)), "min": int(min(nbytes)), "max": int(max(nbytes))},
+        "reference_published": PUBLISHED,
+        "e2e": {"value": round(e2e, 2), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": kernels_per_step * args.steps,
+        "roofline": roof,
+        "clocks": clk,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -60,6 +60,9 @@ _proto("dcvc_conv1x1", c_int,
         c_vp, c_vp, c_int, c_int, c_int, c_int, c_vp])
 
 
+_proto("dcvc_dwconv3x3", c_int, [c_vp, c_int, c_int, c_int, c_int, c_vp, c_vp, c_int, c_vp])
+
+
 def device_error(clear=True):
     code = c_int(0)
     check(lib.dcvc_device_error(ctypes.byref(code), 1 if clear else 0), "dcvc_device_error")

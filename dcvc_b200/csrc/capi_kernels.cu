@@ -1,6 +1,8 @@
 // extern "C" kernel-level entry points (declared in include/dcvc_b200.h).
 #include "errors.h"
+#include "elementwise.cuh"
 #include "gemm_sm100.cuh"
+#include "quant_tables.h"
 
 #include "../../include/dcvc_b200.h"
 
@@ -35,6 +37,16 @@ int dcvc_device_error(int* code, int clear)
     return st;
 }
 
+int dcvc_scale_index_table(uint8_t* lut)
+{
+    if (lut == nullptr) {
+        set_last_error("dcvc_scale_index_table: null output");
+        return kInvalidArgument;
+    }
+    scale_index_table(lut);
+    return kOk;
+}
+
 int dcvc_conv1x1(int dtype, int epilogue, int M, int N, int K, const void* a, int lda,
                  const void* w, const float* bias, const void* res, int ldr, const void* res2,
                  int ldr2, const void* qscale, void* out, int ldo, int sub_w, int sub_cout,
@@ -66,6 +78,22 @@ int dcvc_conv1x1(int dtype, int epilogue, int M, int N, int K, const void* a, in
         return kInvalidArgument;
     }
     return cuda_status(e, "dcvc_conv1x1");
+}
+
+int dcvc_dwconv3x3(const void* x, int H, int W, int C, int ldx, const float* w, void* out, int ldo,
+                   void* stream)
+{
+    if (x == nullptr || w == nullptr || out == nullptr || H <= 0 || W <= 0) {
+        set_last_error("dcvc_dwconv3x3: bad arguments");
+        return kInvalidArgument;
+    }
+    cudaError_t e = launch_dwconv3x3(static_cast<const __half*>(x), H, W, C, ldx, w,
+                                     static_cast<__half*>(out), ldo, static_cast<cudaStream_t>(stream));
+    if (e == cudaErrorInvalidValue) {
+        set_last_error("dcvc_dwconv3x3: C, pitches and pointers must be multiples of 8 elements / 16 bytes");
+        return kInvalidArgument;
+    }
+    return cuda_status(e, "dcvc_dwconv3x3");
 }
 
 }  // extern "C"

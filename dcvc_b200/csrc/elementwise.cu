@@ -521,17 +521,71 @@ __global__ void __launch_bounds__(kCompactThreads)
 
 // ------------------------------------------------------------------------------ depthwise
 
-__global__ void dwconv3x3_kernel(const __half* __restrict__ x, int H, int W, int C, int ldx,
-                                 const float* __restrict__ wt, __half* __restrict__ out, int ldo)
+// Tiled depthwise 3x3: one CTA computes a kDwTH x kDwTW pixel tile for 64 channels (8 vectors
+// of 8); the (kDwTH+2) x (kDwTW+2) halo tile is staged once in shared memory with 16-byte loads
+// (zeros outside the image) and every thread keeps the 9 taps of its channel vector in registers.
+constexpr int kDwTH = 8;
+constexpr int kDwTW = 32;
+constexpr int kDwCV = 8;  // channel vectors (of 8 halves) per CTA
+constexpr int kDwThreads = 256;
+
+__global__ void __launch_bounds__(kDwThreads) dwconv3x3_kernel(const __half* __restrict__ x, int H,
+                                                               int W, int C, int ldx,
+                                                               const float* __restrict__ wt,
+                                                               __half* __restrict__ out, int ldo)
 {
-    const int vecs = C / 8;
-    const long long total = static_cast<long long>(H) * W * vecs;
-    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
-         i += static_cast<long long>(gridDim.x) * blockDim.x) {
-        const long long pix = i / vecs;
-        const int v = static_cast<int>(i - pix * vecs);
-        const int h = static_cast<int>(pix / W);
-        const int w = static_cast<int>(pix - static_cast<long long>(h) * W);
+    __shared__ Vec8h tile[kDwTH + 2][kDwTW + 2][kDwCV];
+    const int c0 = blockIdx.x * kDwCV;  // first channel vector
+    const int h0 = blockIdx.y * kDwTH;
+    const int w0 = blockIdx.z * kDwTW;
+    const int cvecs = C / 8;
+    const int nv = min(kDwCV, cvecs - c0);
+    for (int i = threadIdx.x; i < (kDwTH + 2) * (kDwTW + 2) * kDwCV; i += kDwThreads) {
+        const int v = i % kDwCV;
+        const int pix = i / kDwCV;
+        const int tx = pix % (kDwTW + 2);
+        const int ty = pix / (kDwTW + 2);
+        const int h = h0 + ty - 1, w = w0 + tx - 1;
+        Vec8h val;
+        if (v < nv && h >= 0 && h < H && w >= 0 && w < W) {
+            val = ld8(x + (static_cast<long long>(h) * W + w) * ldx + (c0 + v) * 8);
+        } else {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                val.v[j] = hzero();
+            }
+        }
+        tile[ty][tx][v] = val;
+    }
+    const int v = threadIdx.x % kDwCV;
+    const int slot = threadIdx.x / kDwCV;  // 0..31
+    float w9[9][8];
+    if (v < nv) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            const float4* wp = reinterpret_cast<const float4*>(wt + k * C + (c0 + v) * 8);
+            const float4 a = __ldg(wp), b = __ldg(wp + 1);
+            w9[k][0] = a.x;
+            w9[k][1] = a.y;
+            w9[k][2] = a.z;
+            w9[k][3] = a.w;
+            w9[k][4] = b.x;
+            w9[k][5] = b.y;
+            w9[k][6] = b.z;
+            w9[k][7] = b.w;
+        }
+    }
+    __syncthreads();
+    if (v >= nv) {
+        return;
+    }
+#pragma unroll 1
+    for (int p = slot; p < kDwTH * kDwTW; p += kDwThreads / kDwCV) {
+        const int ty = p / kDwTW, tx = p % kDwTW;
+        const int h = h0 + ty, w = w0 + tx;
+        if (h >= H || w >= W) {
+            continue;
+        }
         float acc[8];
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
@@ -539,27 +593,13 @@ __global__ void dwconv3x3_kernel(const __half* __restrict__ x, int H, int W, int
         }
 #pragma unroll
         for (int ky = 0; ky < 3; ++ky) {
-            const int hh = h + ky - 1;
-            if (hh < 0 || hh >= H) {
-                continue;
-            }
 #pragma unroll
             for (int kx = 0; kx < 3; ++kx) {
-                const int ww = w + kx - 1;
-                if (ww < 0 || ww >= W) {
-                    continue;
+                const Vec8h a = tile[ty + ky][tx + kx][v];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    acc[j] = fmaf(h2f(a.v[j]), w9[ky * 3 + kx][j], acc[j]);
                 }
-                const Vec8h a = ld8(x + (static_cast<long long>(hh) * W + ww) * ldx + v * 8);
-                const float4* wp = reinterpret_cast<const float4*>(wt + (ky * 3 + kx) * C + v * 8);
-                const float4 w0 = __ldg(wp), w1 = __ldg(wp + 1);
-                acc[0] = fmaf(h2f(a.v[0]), w0.x, acc[0]);
-                acc[1] = fmaf(h2f(a.v[1]), w0.y, acc[1]);
-                acc[2] = fmaf(h2f(a.v[2]), w0.z, acc[2]);
-                acc[3] = fmaf(h2f(a.v[3]), w0.w, acc[3]);
-                acc[4] = fmaf(h2f(a.v[4]), w1.x, acc[4]);
-                acc[5] = fmaf(h2f(a.v[5]), w1.y, acc[5]);
-                acc[6] = fmaf(h2f(a.v[6]), w1.z, acc[6]);
-                acc[7] = fmaf(h2f(a.v[7]), w1.w, acc[7]);
             }
         }
         Vec8h o;
@@ -567,7 +607,7 @@ __global__ void dwconv3x3_kernel(const __half* __restrict__ x, int H, int W, int
         for (int j = 0; j < 8; ++j) {
             o.v[j] = f2h(acc[j]);
         }
-        st8(out + pix * ldo + v * 8, o);
+        st8(out + (static_cast<long long>(h) * W + w) * ldo + (c0 + v) * 8, o);
     }
 }
 
@@ -794,8 +834,8 @@ cudaError_t launch_dwconv3x3(const __half* x, int H, int W, int C, int ldx, cons
     if (C % 8 || ldx % 8 || ldo % 8 || !al16(x) || !al16(out) || !al16(w)) {
         return cudaErrorInvalidValue;
     }
-    dwconv3x3_kernel<<<grid_for(static_cast<long long>(H) * W * (C / 8)), kThreads, 0, s>>>(
-        x, H, W, C, ldx, w, out, ldo);
+    const dim3 grid((C / 8 + kDwCV - 1) / kDwCV, (H + kDwTH - 1) / kDwTH, (W + kDwTW - 1) / kDwTW);
+    dwconv3x3_kernel<<<grid, kDwThreads, 0, s>>>(x, H, W, C, ldx, w, out, ldo);
     return cudaGetLastError();
 }
 

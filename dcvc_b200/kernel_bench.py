@@ -1,0 +1,73 @@
+"""Micro-benchmark of the codec's kernels at their 1080p shapes (CUDA events on the launching
+stream), also the small fixed case used for ncu captures.
+
+    python -m dcvc_b200.kernel_bench [--case quad|wsilu|res|bias2048|dwconv|all] [--reps N]
+
+Shapes are those of a 512-channel dcb2 DepthConvBlock at 1920x1088 (M = 136 x 240 = 32640
+pixels): dc.0 (512 -> 256, WSiLU), depthwise 3x3 on 256 channels, dc.3 (256 -> 512 + residual),
+ffn.0 (512 -> 4 x 256, WSiLU chunk-add), and the encoder's 2048 -> 512 adaptor.
+"""
+import argparse
+import json
+
+import torch
+
+from . import _native as N
+from . import ops
+
+M8 = 136 * 240
+
+
+def _case(name):
+    g = torch.Generator(device="cuda").manual_seed(11)
+
+    def rnd(*s, scale=1.0):
+        return (torch.randn(*s, device="cuda", generator=g) * scale).half()
+
+    if name == "dwconv":
+        x = rnd(M8, 256)
+        w = torch.randn(9, 256, device="cuda", generator=g)
+        out = torch.empty_like(x)
+        fn = lambda: ops.dwconv3x3(x, 136, 240, w, out)  # noqa: E731
+        return fn, 0.0, 2 * x.numel() * 2 + w.numel() * 4
+    shapes = {"quad": (M8, 1024, 512, N.EPI_QUAD), "wsilu": (M8, 256, 512, N.EPI_BIAS_WSILU),
+              "res": (M8, 512, 256, N.EPI_BIAS_RES), "bias2048": (M8, 512, 2048, N.EPI_BIAS)}
+    M, Nn, K, epi = shapes[name]
+    a = rnd(M, K)
+    w = rnd(Nn, K, scale=K ** -0.5)
+    b = torch.zeros(Nn, device="cuda")
+    res = rnd(M, Nn) if epi == N.EPI_BIAS_RES else None
+    nout = Nn // 4 if epi == N.EPI_QUAD else Nn
+    out = torch.empty(M, nout, device="cuda", dtype=torch.float16)
+    fn = lambda: ops.conv1x1(a, w, b, epi, res=res, out=out)  # noqa: E731
+    byts = (M * K + Nn * K + M * nout + (M * Nn if res is not None else 0)) * 2
+    return fn, 2.0 * M * Nn * K, byts
+
+
+def run(name, reps=20, warmup=5):
+    fn, flops, byts = _case(name)
+    for _ in range(warmup):
+        fn()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(reps):
+        fn()
+    e.record()
+    e.synchronize()
+    sec = s.elapsed_time(e) / 1e3 / reps
+    return {"case": name, "us": round(sec * 1e6, 2), "tflops": round(flops / sec / 1e12, 1),
+            "gbs": round(byts / sec / 1e9, 1)}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--case", default="all")
+    ap.add_argument("--reps", type=int, default=20)
+    args = ap.parse_args()
+    cases = ["quad", "wsilu", "res", "bias2048", "dwconv"] if args.case == "all" else [args.case]
+    for c in cases:
+        print(json.dumps(run(c, args.reps)), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -147,10 +147,32 @@ def hts_state_dict(seed=0, dtype=torch.float32):
     return {k: v.detach().to(dtype) for k, v in model.state_dict().items()}
 
 
-def perturbed_hts_state_dict(seed=0, dtype=torch.float32, q_jitter=0.25):
-    """Seed-`seed` weights with non-trivial per-QP quant vectors (the random init sets them to
-    ones, which hides QP dependence); used by tests that must see QP-specific behaviour."""
+# Residual-branch scale of the calibrated variant (see calibrated_hts_state_dict).
+CALIBRATION_ALPHA = 0.1
+
+
+def calibrated_hts_state_dict(seed=0, dtype=torch.float32, alpha=CALIBRATION_ALPHA):
+    """The seed-`seed` random-init weights with the output convolution of every residual branch
+    (dc.3 and ffn.2 of each DepthConvBlock) scaled by `alpha`.
+
+    The plain random init is numerically unstable: every DepthConvBlock adds its branch to its
+    input at full gain, so activations grow by orders of magnitude per block and the temporal
+    memory by about 1e14 per chunk (in FP64 as well), and any FP16 implementation overflows in
+    the first chunk.  With alpha = 0.1 activations stay O(1) across chunks and 10-20 % of the y
+    latents are coded, a realistic entropy-coding load.  Architecture, shapes and FLOPs are
+    unchanged."""
     sd = hts_state_dict(seed, torch.float32)
+    for k in list(sd):
+        if k.endswith(("dc.3.weight", "ffn.2.weight")):
+            sd[k] = sd[k] * alpha
+    return {k: v.to(dtype) for k, v in sd.items()}
+
+
+def perturbed_hts_state_dict(seed=0, dtype=torch.float32, q_jitter=0.25, calibrated=True):
+    """Seed-`seed` weights (calibrated by default) with non-trivial per-QP quant vectors (the
+    random init sets them to ones, which hides QP dependence); used by tests that must see
+    QP-specific behaviour."""
+    sd = calibrated_hts_state_dict(seed) if calibrated else hts_state_dict(seed, torch.float32)
     g = torch.Generator().manual_seed(seed + 17)
     for k in ("q_encoder", "q_decoder", "q_feature"):
         sd[k] = 1.0 + q_jitter * (torch.rand(sd[k].shape, generator=g) * 2 - 1)

@@ -42,3 +42,180 @@ def conv1x1(a, w, bias=None, epilogue=N.EPI_BIAS, res=None, res2=None, qscale=No
         _ptr(res2), res2.stride(0) if res2 is not None else 0, _ptr(qscale),
         out.data_ptr(), out.stride(0), sub_w, sub_cout, block_n, _stream()), "dcvc_conv1x1")
     return out
+
+
+def dwconv3x3(x, H, W, w, out=None):
+    """Depthwise 3x3 (pad 1, no bias) over an [H*W, C] NHWC tensor; w is fp32 [9, C]."""
+    C = x.shape[1]
+    if out is None:
+        out = torch.empty_like(x)
+    N.check(N.lib.dcvc_dwconv3x3(x.data_ptr(), H, W, C, x.stride(0), w.data_ptr(), out.data_ptr(),
+                                 out.stride(0), _stream()), "dcvc_dwconv3x3")
+    return out
+
+
+# ----------------------------------------------------------------------------- elementwise
+
+def _sig(name, args):
+    f = getattr(N.lib, name)
+    f.restype = ctypes.c_int
+    f.argtypes = args
+    return f
+
+
+import ctypes  # noqa: E402
+
+_i, _v, _f = ctypes.c_int, ctypes.c_void_p, ctypes.c_float
+_sig("dcvc_pad_unshuffle8", [_v, _i, _i, _i, _i, _i, _i, _v, _i, _v])
+_sig("dcvc_shuffle8_clamp", [_v, _i, _i, _i, _i, _v, _v])
+_sig("dcvc_space_to_depth2", [_v, _i, _i, _i, _i, _v, _v])
+_sig("dcvc_im2col3x3s2", [_v, _i, _i, _i, _i, _v, _v])
+_sig("dcvc_replicate_pad", [_v, _i, _i, _i, _i, _i, _i, _v, _v])
+_sig("dcvc_crop", [_v, _i, _i, _i, _i, _i, _v, _i, _v])
+_sig("dcvc_round_z", [_v, _i, _v, _v, _v])
+_sig("dcvc_int8_to_half", [_v, _i, _v, _v])
+_sig("dcvc_mul_channel", [_v, _i, _i, _i, _v, _v, _i, _v])
+_sig("dcvc_div_clamp", [_v, _i, _i, _i, _v, _i, _v])
+_sig("dcvc_quantize_phase", [_i, _i, _v, _i, _v, _i, _v, _i, _v, _i, _f, _v, _i, _v, _i, _i, _i, _i, _v])
+_sig("dcvc_restore_phase", [_i, _i, _v, _i, _v, _i, _v, _i, _v, _i, _i, _i, _i, _v])
+_sig("dcvc_build_index", [_i, _v, _i, _v, _i, _f, _v, _i, _i, _v, _v, _v, _v])
+_sig("dcvc_compact_blocks", [_i])
+_sig("dcvc_compact", [_v, _i, _v, _i, _v, _v, _v, _v])
+_sig("dcvc_recover", [_v, _v, _v, _i, _v, _v])
+_sig("dcvc_scale_index_table", [_v])
+
+
+def pad_unshuffle8(x, pad_b, pad_r, out=None):
+    """x: [H, W, C] fp16 (dense) -> [(H+pad_b)/8 * (W+pad_r)/8, 64 C]."""
+    H, W, C = x.shape
+    if out is None:
+        out = torch.empty(((H + pad_b) // 8) * ((W + pad_r) // 8), 64 * C, dtype=x.dtype, device=x.device)
+    N.check(N.lib.dcvc_pad_unshuffle8(x.data_ptr(), H, W, C, C, pad_b, pad_r, out.data_ptr(),
+                                      out.stride(0), _stream()), "pad_unshuffle8")
+    return out
+
+
+def shuffle8_clamp(x, H8, W8):
+    """x: [H8*W8, 64 C] -> [8 H8, 8 W8, C]."""
+    C = x.shape[1] // 64
+    out = torch.empty(8 * H8, 8 * W8, C, dtype=x.dtype, device=x.device)
+    N.check(N.lib.dcvc_shuffle8_clamp(x.data_ptr(), H8, W8, C, x.stride(0), out.data_ptr(),
+                                      _stream()), "shuffle8_clamp")
+    return out
+
+
+def space_to_depth2(x, H, W):
+    C = x.shape[1]
+    out = torch.empty((H // 2) * (W // 2), 4 * C, dtype=x.dtype, device=x.device)
+    N.check(N.lib.dcvc_space_to_depth2(x.data_ptr(), H, W, C, x.stride(0), out.data_ptr(), _stream()),
+            "space_to_depth2")
+    return out
+
+
+def im2col3x3s2(x, H, W):
+    C = x.shape[1]
+    out = torch.empty((H // 2) * (W // 2), 9 * C, dtype=x.dtype, device=x.device)
+    N.check(N.lib.dcvc_im2col3x3s2(x.data_ptr(), H, W, C, x.stride(0), out.data_ptr(), _stream()),
+            "im2col3x3s2")
+    return out
+
+
+def replicate_pad(x, H, W, pad_b, pad_r):
+    C = x.shape[1]
+    out = torch.empty((H + pad_b) * (W + pad_r), C, dtype=x.dtype, device=x.device)
+    N.check(N.lib.dcvc_replicate_pad(x.data_ptr(), H, W, C, x.stride(0), pad_b, pad_r,
+                                     out.data_ptr(), _stream()), "replicate_pad")
+    return out
+
+
+def crop(x, Wx, H, W):
+    C = x.shape[1]
+    out = torch.empty(H * W, C, dtype=x.dtype, device=x.device)
+    N.check(N.lib.dcvc_crop(x.data_ptr(), Wx, x.stride(0), H, W, C, out.data_ptr(), out.stride(0),
+                            _stream()), "crop")
+    return out
+
+
+def round_z(z):
+    z_hat = torch.empty_like(z)
+    z_i8 = torch.empty(z.shape, dtype=torch.int8, device=z.device)
+    N.check(N.lib.dcvc_round_z(z.data_ptr(), z.numel(), z_hat.data_ptr(), z_i8.data_ptr(), _stream()),
+            "round_z")
+    return z_hat, z_i8
+
+
+def int8_to_half(x):
+    out = torch.empty(x.shape, dtype=torch.float16, device=x.device)
+    N.check(N.lib.dcvc_int8_to_half(x.data_ptr(), x.numel(), out.data_ptr(), _stream()), "int8_to_half")
+    return out
+
+
+def mul_channel(x, q):
+    M, C = x.shape
+    out = torch.empty_like(x)
+    N.check(N.lib.dcvc_mul_channel(x.data_ptr(), M, C, x.stride(0), q.data_ptr(), out.data_ptr(),
+                                   out.stride(0), _stream()), "mul_channel")
+    return out
+
+
+def div_clamp_(y, q):
+    M, C = y.shape
+    N.check(N.lib.dcvc_div_clamp(y.data_ptr(), M, C, y.stride(0), q.data_ptr(), q.stride(0), _stream()),
+            "div_clamp")
+    return y
+
+
+def quantize_phase(phase, mode, y, scales, means, q_dec, thr, y_q, y_hat, H, W):
+    C = y.shape[1]
+    N.check(N.lib.dcvc_quantize_phase(
+        phase, mode, y.data_ptr(), y.stride(0), scales.data_ptr(), scales.stride(0), means.data_ptr(),
+        means.stride(0), _ptr(q_dec), q_dec.stride(0) if q_dec is not None else 0, float(thr),
+        y_q.data_ptr(), y_q.stride(0), y_hat.data_ptr(), y_hat.stride(0), H, W, C, _stream()),
+        "quantize_phase")
+
+
+def restore_phase(phase, mode, y_q, means, q_dec, y_hat, H, W):
+    C = y_q.shape[1]
+    N.check(N.lib.dcvc_restore_phase(
+        phase, mode, y_q.data_ptr(), y_q.stride(0), means.data_ptr(), means.stride(0), _ptr(q_dec),
+        q_dec.stride(0) if q_dec is not None else 0, y_hat.data_ptr(), y_hat.stride(0), H, W, C,
+        _stream()), "restore_phase")
+
+
+def scale_index_table(device="cuda"):
+    lut = torch.empty(65536, dtype=torch.uint8)
+    N.check(N.lib.dcvc_scale_index_table(lut.data_ptr()), "scale_index_table")
+    return lut.to(device)
+
+
+def build_index(encode, y_q, scales, thr, lut):
+    M, C = scales.shape
+    n = M * C
+    sym = torch.empty(n, dtype=torch.int16, device=scales.device) if encode else None
+    idx = None if encode else torch.empty(n, dtype=torch.uint8, device=scales.device)
+    cond = torch.empty(n, dtype=torch.uint8, device=scales.device)
+    N.check(N.lib.dcvc_build_index(
+        1 if encode else 0, _ptr(y_q), y_q.stride(0) if y_q is not None else 0, scales.data_ptr(),
+        scales.stride(0), float(thr), lut.data_ptr(), M, C, _ptr(sym), _ptr(idx), cond.data_ptr(),
+        _stream()), "build_index")
+    return (sym if encode else idx), cond
+
+
+def compact(src, cond):
+    n = src.numel()
+    nb = N.lib.dcvc_compact_blocks(n)
+    counts = torch.empty(nb, dtype=torch.int32, device=src.device)
+    dst = torch.empty_like(src)
+    total = torch.empty(1, dtype=torch.int32, device=src.device)
+    N.check(N.lib.dcvc_compact(src.data_ptr(), src.element_size(), cond.data_ptr(), n,
+                               counts.data_ptr(), dst.data_ptr(), total.data_ptr(), _stream()),
+            "compact")
+    return dst, total, counts
+
+
+def recover(dec, cond, counts):
+    n = cond.numel()
+    out = torch.empty(n, dtype=torch.float16, device=cond.device)
+    N.check(N.lib.dcvc_recover(dec.data_ptr(), cond.data_ptr(), counts.data_ptr(), n, out.data_ptr(),
+                               _stream()), "recover")
+    return out

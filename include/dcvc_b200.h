@@ -79,6 +79,69 @@ int dcvc_conv1x1(int dtype, int epilogue, int M, int N, int K, const void* a, in
                  int ldr2, const void* qscale, void* out, int ldo, int sub_w, int sub_cout,
                  int block_n, void* stream);
 
+/* Depthwise 3x3, pad 1, no bias, FP32 accumulation: x, out [H*W, C] FP16 (pitches ldx, ldo),
+ * w FP32 [9][C] tap-major.  Replaces d3x3 (src/layers/extensions/inference/cutlass/
+ * d3x3_kernel.h:104-166, d3x3.cu). */
+int dcvc_dwconv3x3(const void* x, int H, int W, int C, int ldx, const float* w, void* out, int ldo,
+                   void* stream);
+
+/* Layout kernels (FP16, NHWC rows with pitches in elements). */
+/* pad_and_unshuffle_8 / pixel_unshuffle(8) (elementwise/cat_and_pad.cu:7-51, shuffle.cu:134-185):
+ * out[h8, w8, c*64 + dy*8 + dx] = x[min(8 h8 + dy, H-1), min(8 w8 + dx, W-1), c]. */
+int dcvc_pad_unshuffle8(const void* x, int H, int W, int C, int ldx, int pad_b, int pad_r,
+                        void* out, int ldo, void* stream);
+/* pixel_shuffle_8 with clamp to [-0.5, 0.5] (shuffle.cu:40-131); out [8 H8, 8 W8, C] dense. */
+int dcvc_shuffle8_clamp(const void* in, int H8, int W8, int C, int ldi, void* out, void* stream);
+/* pixel_unshuffle(2) with channels in (dy, dx, c) order, the A operand of the stride-2 1x1
+ * conv of ResidualBlockWithStride2 (layers_proxy.cpp:234-267). */
+int dcvc_space_to_depth2(const void* x, int H, int W, int C, int ldx, void* out, void* stream);
+/* 3x3 stride-2 pad-1 patches in (ky, kx, c) order, the A operand of conv_bias with kernel 3
+ * (cutlass/conv_kernel.h:22-89). */
+int dcvc_im2col3x3s2(const void* x, int H, int W, int C, int ldx, void* out, void* stream);
+/* replicate_pad / slice (cat_and_pad.cu:53-110). */
+int dcvc_replicate_pad(const void* x, int H, int W, int C, int ldx, int pad_b, int pad_r, void* out,
+                       void* stream);
+int dcvc_crop(const void* x, int Wx, int ldx, int H, int W, int C, void* out, int ldo, void* stream);
+
+/* Latent kernels (elementwise/stream.cu). */
+/* round_z :862-894: z_hat = clamp(round(z), -64, 63) as FP16 and int8. */
+int dcvc_round_z(const void* z, int n, void* z_hat, int8_t* z_i8, void* stream);
+/* int8_to_dtype :454-482. */
+int dcvc_int8_to_half(const int8_t* x, int n, void* out, void* stream);
+/* multiply_with_broadcast :484-546: out[m, c] = x[m, c] * q[c]. */
+int dcvc_mul_channel(const void* x, int M, int C, int ldx, const void* q, void* out, int ldo,
+                     void* stream);
+/* divide_with_clamp_inplace :422-452: y *= rcp(max(q, 0.5)). */
+int dcvc_div_clamp(void* y, int M, int C, int ldy, const void* q, int ldq, void* stream);
+/* process_with_mask_no_scale[_add_inplace][_add_and_multiply_inplace] :548-683 for checkerboard
+ * phase 0..3; mode 0 writes, 1 accumulates, 2 accumulates and scales y_hat by max(q_dec, 0.5). */
+int dcvc_quantize_phase(int phase, int mode, const void* y, int ldy, const void* scales, int lds,
+                        const void* means, int ldm, const void* q_dec, int ldd, float thr, void* y_q,
+                        int ldq, void* y_hat, int ldh, int H, int W, int C, void* stream);
+/* restore_y[_and_add_inplace][_and_add_multiply_inplace] :685-760. */
+int dcvc_restore_phase(int phase, int mode, const void* y_q, int ldq, const void* means, int ldm,
+                       const void* q_dec, int ldd, void* y_hat, int ldh, int H, int W, int C,
+                       void* stream);
+/* build_index_enc / build_index_dec :89-173 (encode != 0: sym = (q << 8) + idx, else idx), with
+ * cond = scale > thr, NHWC symbol order; lut from dcvc_scale_index_table on the device. */
+int dcvc_build_index(int encode, const void* y_q, int ldq, const void* scales, int lds, float thr,
+                     const uint8_t* lut, int M, int C, int16_t* sym, uint8_t* idx, uint8_t* cond,
+                     void* stream);
+/* conditional_index_part1 :175-338: order-preserving compaction of src (1- or 2-byte
+ * elements) under cond; block_counts needs dcvc_compact_blocks(n) ints; *total (device) gets
+ * the kept count. */
+int dcvc_compact_blocks(int n);
+int dcvc_compact(const void* src, int elem_bytes, const uint8_t* cond, int n, int* block_counts,
+                 void* dst, int* total, void* stream);
+/* conditional_recover_with_type_conversion :359-420, with the block counts of dcvc_compact. */
+int dcvc_recover(const int8_t* dec, const uint8_t* cond, const int* block_counts, int n, void* out,
+                 void* stream);
+
+/* The 65536-entry table mapping the FP16 bits of a Gaussian scale to its CDF table index, as
+ * scale_to_index evaluates it in FP16 (src/layers/extensions/inference/elementwise/
+ * stream.cu:77-87 with the constants of def_const.h:6-12); used by the index kernels. */
+int dcvc_scale_index_table(uint8_t* lut);
+
 /* ------------------------------------------------------------------ rANS coder (host) */
 
 /* pmf -> 16-bit quantised CDF, writes n + 1 entries.

@@ -1,0 +1,421 @@
+"""ORACLE (test infrastructure only; never imported by the product).
+
+CPU restatement of the reference's DCVC-UF HT-S chunk codec as its CUDA proxy runs it
+(src/layers/extensions/inference/dmc_hts_proxy.cpp:504-710), written with plain PyTorch CPU
+ops in float64 ("FP64 oracle") or float32 (the timed CPU baseline), reading the weights from
+a state dict.  Used by tests/ (PSNR / bpp / symbol agreement against the GPU path) and by
+bench.py's reference arm; the module math is pinned against the reference nn.Modules by
+tests/golden/modules_golden.npz.
+
+Layer math follows src/layers/layers.py (DepthConvBlock :128-159, ResidualBlockWithStride2
+:176-188, ResidualBlockUpsample :162-173, SubpelConv2x :92-103, WSiLU :106-111,
+WSiLUChunkAdd :114-125) and src/models/video_model_ht.py (Encoder :64-92, HyperEncoder
+:186-200, HyperDecoder :167-183, PriorFusion :203-212, SpatialPrior :278-289, Decoder
+:26-61, ReconHead :215-275, FeatureAdaptorI/M :95-147, FeatureExtractor :150-164,
+TemporalPriorEncoder :305-317).  The proxy-only steps follow the reference kernels:
+replicate padding + unshuffle (cat_and_pad.cu:7-84), round_z with clamp [-64, 63]
+(stream.cu:862-894), divide by max(q_dec, 0.5) (stream.cu:422-452), the 4-phase masked
+quantisation with skip threshold and clamp [-128, 127] (stream.cu:548-683), the NHWC symbol
+order and skip condition (stream.cu:126-173), and the clamped x8 pixel shuffle
+(shuffle.cu:40-131).
+"""
+import ctypes
+import math
+import os
+
+import numpy as np
+import torch
+import torch.nn.functional as F
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+SCALE_MIN, SCALE_MAX = 0.11, 16.0
+LOG_SCALE_MIN, LOG_SCALE_MAX, SCALE_LEVEL = -2.2073, 2.7726, 128
+MASK_PERM = (0, 3, 2, 1)
+
+
+# ----------------------------------------------------------------------------- scale index
+
+def scale_index_lut():
+    """The 65536-entry FP16-scale -> CDF-index table (restates quant_tables.cu with NumPy
+    float16 arithmetic: every op in float32, rounded to float16)."""
+    h = np.arange(65536, dtype=np.uint32).astype(np.uint16).view(np.float16)
+    f16 = np.float16
+    smin, smax = f16(0.11), f16(16.0)
+    log_min = f16(-2.2073)
+    step_recip = f16(np.float32(1.0) / np.float32((np.float32(2.7726) - np.float32(-2.2073)) /
+                                                  np.float32(127)))
+    s = h.astype(np.float32)
+    s = np.where(np.isnan(s), np.float32(smin), np.maximum(s, np.float32(smin)))
+    s = np.minimum(s, np.float32(smax))
+    t = np.log(s.astype(np.float64)).astype(np.float32).astype(np.float16)
+    u = (t.astype(np.float32) - np.float32(log_min)).astype(np.float16)
+    v = (u.astype(np.float32) * np.float32(step_recip)).astype(np.float16)
+    idx = np.clip(np.floor(v.astype(np.float32)), 0, 127)
+    return idx.astype(np.uint8)
+
+
+_LUT = None
+
+
+def scale_index(scales):
+    """CDF index of each scale: the table applied to the scale rounded to float16."""
+    global _LUT
+    if _LUT is None:
+        _LUT = scale_index_lut()
+    bits = np.asarray(scales, dtype=np.float64).astype(np.float16).view(np.uint16)
+    return _LUT[bits]
+
+
+def round_half_away(x):
+    return torch.copysign(torch.floor(torch.abs(x) + 0.5), x)
+
+
+def checker_mask(phase, C, H, W, dtype):
+    """Mask of phase `phase` (common_model.py:175-195): quarter q of the channels is coded at
+    2x2 position q ^ perm[phase]."""
+    q = torch.arange(C) // (C // 4)
+    pos = q ^ MASK_PERM[phase]
+    hh = (torch.arange(H) % 2)[:, None]
+    ww = (torch.arange(W) % 2)[None, :]
+    p = (hh * 2 + ww)[None, :, :]
+    return (p == pos[:, None, None]).to(dtype)[None]
+
+
+# ----------------------------------------------------------------------------- rANS oracle
+
+_ORACLE_LIB = None
+
+
+def _oracle_lib():
+    global _ORACLE_LIB
+    if _ORACLE_LIB is None:
+        so = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(so):
+            import subprocess
+            subprocess.run(["make", "-C", HERE, so], check=True, capture_output=True)
+        _ORACLE_LIB = ctypes.CDLL(so)
+    return _ORACLE_LIB
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+_REF_LIB = None
+USE_REFERENCE_CODER = False
+
+
+def use_reference_coder(flag=True):
+    """Route the entropy coding through the reference's own coder compiled from its sources
+    (oracle/_ref/librans_ref.so) instead of the C restatement; both emit the same bytes."""
+    global USE_REFERENCE_CODER, _REF_LIB
+    if flag and _REF_LIB is None:
+        so = os.path.join(HERE, "_ref", "librans_ref.so")
+        if not os.path.exists(so):
+            raise FileNotFoundError(so)
+        _REF_LIB = ctypes.PyDLL(so)
+    USE_REFERENCE_CODER = bool(flag)
+
+
+def rans_encode(cdf_z, len_z, cdf_y, len_y, y_sym, z_sym, z_offset, z_ch, ecp):
+    cap = (y_sym.size + z_sym.size) * 4 + 1024
+    out = np.zeros(cap, np.uint8)
+    if USE_REFERENCE_CODER:
+        n = _REF_LIB.ref_encode(_p(cdf_z), _p(len_z), cdf_z.shape[0], cdf_z.shape[1], _p(cdf_y),
+                                _p(len_y), cdf_y.shape[0], cdf_y.shape[1], _p(y_sym), y_sym.size,
+                                _p(z_sym), z_sym.size, z_offset, z_ch, ecp, _p(out), cap)
+    else:
+        n = _oracle_lib().oracle_encode(_p(cdf_z), _p(len_z), cdf_z.shape[1], _p(cdf_y), _p(len_y),
+                                        cdf_y.shape[1], _p(y_sym), y_sym.size, _p(z_sym),
+                                        z_sym.size, z_offset, z_ch, ecp, _p(out), cap)
+    if n < 0:
+        raise RuntimeError("oracle rANS encode failed")
+    return out[:n].copy()
+
+
+def rans_decode(cdf_z, len_z, cdf_y, len_y, data, y_idx, n_z, z_offset, z_ch, ecp):
+    y = np.zeros(max(1, y_idx.size), np.int8)
+    z = np.zeros(max(1, n_z), np.int8)
+    if USE_REFERENCE_CODER:
+        _REF_LIB.ref_decode(_p(cdf_z), _p(len_z), cdf_z.shape[0], cdf_z.shape[1], _p(cdf_y),
+                            _p(len_y), cdf_y.shape[0], cdf_y.shape[1], _p(data), data.size,
+                            _p(y_idx), y_idx.size, n_z, z_offset, z_ch, ecp, _p(y), _p(z))
+        return y[: y_idx.size], z[:n_z]
+    lib = _oracle_lib()
+    rc = lib.oracle_decode(_p(cdf_z), _p(len_z), cdf_z.shape[1], _p(cdf_y), _p(len_y),
+                           cdf_y.shape[1], _p(data), data.size, _p(y_idx), y_idx.size, n_z,
+                           z_offset, z_ch, ecp, _p(y), _p(z))
+    if rc != 0:
+        raise RuntimeError("oracle rANS decode failed")
+    return y[: y_idx.size], z[:n_z]
+
+
+def ec_parallel_for(n):
+    return max(1, min(8, n // 32768))
+
+
+# ----------------------------------------------------------------------------- network
+
+class HtsOracle:
+    """One stream of the HT-S codec on the CPU.  `sd`: state dict (any float dtype) plus the
+    four CDF entries; `dtype`: torch.float64 or torch.float32."""
+
+    def __init__(self, sd, skip_thres=0.15, dtype=torch.float64, threads=None):
+        if threads:
+            torch.set_num_threads(threads)
+        self.dtype = dtype
+        self.w = {k: (v.detach().to("cpu", dtype) if v.is_floating_point() else v.detach().cpu())
+                  for k, v in sd.items()}
+        # the reference compares against the threshold as FP16 in both the quantiser and the
+        # skip condition (stream.cu:548-683, 126-173)
+        self.thr = float(np.float16(skip_thres))
+        self.cdf_y = np.ascontiguousarray(sd["gaussian_encoder.quantized_cdf"].cpu().numpy(), np.int32)
+        self.len_y = np.ascontiguousarray(sd["gaussian_encoder.cdf_length"].cpu().numpy(), np.int32).reshape(-1)
+        self.cdf_z = np.ascontiguousarray(sd["bit_estimator_z.quantized_cdf"].cpu().numpy(), np.int32)
+        self.len_z = np.ascontiguousarray(sd["bit_estimator_z.cdf_length"].cpu().numpy(), np.int32).reshape(-1)
+        self.memory = None
+        self.ctx = None
+        self.feature_i = None
+        self.feature_p = None
+        self.memory_has_value = False
+
+    # ---- layers
+    def has(self, k):
+        return k in self.w
+
+    def conv(self, p, x, stride=1, padding=0, groups=1):
+        b = self.w.get(p + "bias")
+        return F.conv2d(x, self.w[p + "weight"], b, stride=stride, padding=padding, groups=groups)
+
+    @staticmethod
+    def wsilu(x):
+        return torch.sigmoid(4.0 * x) * x
+
+    def dcb(self, p, x, quant=None):
+        if self.has(p + "adaptor.weight"):
+            x = self.conv(p + "adaptor.", x)
+        c = self.w[p + "dc.2.weight"].shape[0]
+        out = self.wsilu(self.conv(p + "dc.0.", x))
+        out = self.conv(p + "dc.2.", out, padding=1, groups=c)
+        out = self.conv(p + "dc.3.", out) + x
+        t = self.wsilu(self.conv(p + "ffn.0.", out))
+        t = t[:, 0::4] + t[:, 1::4] + t[:, 2::4] + t[:, 3::4]
+        out = self.conv(p + "ffn.2.", t) + out
+        if quant is not None:
+            out = out * quant
+        return out
+
+    def seq(self, prefix, n, x, quant=None):
+        for i in range(n):
+            x = self.dcb(f"{prefix}{i}.", x, quant if i == n - 1 else None)
+        return x
+
+    def rb_down(self, p, x):
+        return self.dcb(p + "conv.", self.conv(p + "down.", F.pixel_unshuffle(x, 2)))
+
+    def subpel(self, p, x):
+        return F.pixel_shuffle(self.conv(p + "conv.0.", x), 2)
+
+    def rb_up(self, p, x):
+        return self.dcb(p + "conv.", self.subpel(p + "up.", x))
+
+    def q(self, name, qp):
+        return self.w[name][qp][None, :, None, None]
+
+    # ---- sub-networks (video_model_ht.py)
+    def encoder(self, x, ctx, q_enc):
+        f = torch.cat((F.pixel_unshuffle(x, 8), ctx), dim=1)
+        f = self.seq("encoder.conv1.", 6, f, q_enc)
+        return self.conv("encoder.down.", f, stride=2, padding=1)
+
+    def hyper_encoder(self, y):
+        z = self.dcb("hyper_encoder.conv.0.", y)
+        z = self.rb_down("hyper_encoder.conv.1.", z)
+        return self.rb_down("hyper_encoder.conv.2.", z)
+
+    def hyper_decoder(self, z_hat):
+        h = self.rb_up("hyper_decoder.conv.0.", z_hat)
+        h = self.rb_up("hyper_decoder.conv.1.", h)
+        return self.dcb("hyper_decoder.conv.2.", h)
+
+    def temporal_prior(self, memory, q_feat):
+        return self.rb_down("temporal_prior_encoder.conv.", memory * q_feat)
+
+    def prior_fusion(self, hyper, temporal):
+        x = self.seq("y_prior_fusion.conv.", 3, torch.cat((hyper, temporal), dim=1))
+        return self.conv("y_prior_fusion.conv.3.", x)
+
+    def spatial_prior(self, k, y_hat, reduced):
+        x = self.dcb(f"y_spatial_prior_adaptor_{k}.", torch.cat((y_hat, reduced), dim=1))
+        x = self.seq("y_spatial_prior.conv.", 3, x)
+        return self.conv("y_spatial_prior.conv.3.", x)
+
+    def decoder(self, y_hat, ctx, q_dec):
+        up = self.subpel("decoder.up.", y_hat)
+        return self.seq("decoder.conv1.", 7, torch.cat((up, ctx), dim=1), q_dec)
+
+    def feature_adaptor_i(self, f):
+        return self.seq("feature_adaptor_i.conv.", 4, f)
+
+    def feature_adaptor_m(self, memory, feature):
+        return self.seq("feature_adaptor_m.conv.", 6, torch.cat((memory, feature), dim=1))
+
+    def feature_extractor(self, memory):
+        return self.seq("feature_extractor.conv.", 5, memory)
+
+    def recon_head_frame(self, i, common):
+        out = self.seq(f"recon_head.conv2.{i}.", 3, common)
+        return self.conv(f"recon_head.conv2.{i}.3.", out)
+
+    def recon_head(self, feature):
+        frames = []
+        head7 = None
+        for i in range(8):
+            if i % 2 == 0:
+                common = self.dcb(f"recon_head.conv1.{i // 2}.0.", feature)
+            h = self.recon_head_frame(i, common)
+            if i == 7:
+                head7 = h
+            frames.append(torch.clamp(F.pixel_shuffle(h, 8), -0.5, 0.5))
+        return frames, head7
+
+    def recon_head_reset(self, feature):
+        common = self.dcb("recon_head.conv1.3.0.", feature)
+        return self.recon_head_frame(7, common)
+
+    # ---- entropy parameters
+    def entropy_params(self, z_hat, temporal, H16, W16):
+        hyper = self.hyper_decoder(z_hat)[:, :, :H16, :W16]
+        common = self.prior_fusion(hyper, temporal)
+        q_dec, scales, means = common.chunk(3, 1)
+        return common, torch.clamp_min(q_dec, 0.5), scales, means
+
+    # ---- public API mirroring DMCHTSProxy
+    def add_ref_feature_from_frame(self, frame, apply_adaptor=True):
+        self.feature_i = F.pixel_unshuffle(frame.to("cpu", self.dtype), 8)
+        if apply_adaptor:
+            self.memory = self.feature_adaptor_i(self.feature_i)
+            self.ctx = self.feature_extractor(self.memory)
+        self.memory_has_value = bool(apply_adaptor)
+
+    @torch.no_grad()
+    def compress(self, x, qp, reset_feature_memory, padding_b, padding_r, ec_parallel=None):
+        """Returns a dict with the payload bytes and the intermediate integer tensors."""
+        x = x.to("cpu", self.dtype)
+        x = F.pad(x, (0, padding_r, 0, padding_b), mode="replicate")
+        y = self.encoder(x, self.ctx, self.q("q_encoder", qp))
+        _, C, H16, W16 = y.shape
+        ph, pw = (-H16) % 4, (-W16) % 4
+        y_pad = F.pad(y, (0, pw, 0, ph), mode="replicate") if (ph or pw) else y
+        z = self.hyper_encoder(y_pad)
+        z_hat = torch.clamp(round_half_away(z), -64, 63)
+        temporal = self.temporal_prior(self.memory, self.q("q_feature", qp))
+        common, q_dec, scales, means = self.entropy_params(z_hat, temporal, H16, W16)
+        y = y / q_dec
+        reduced = self.conv("y_spatial_prior_reduction.", common)
+        y_q = torch.zeros_like(y)
+        y_hat = torch.zeros_like(y)
+        for k in range(4):
+            if k > 0:
+                means = self.spatial_prior(k, y_hat, reduced)
+            m = checker_mask(k, C, H16, W16, self.dtype)
+            s_hat = scales * m
+            m_hat = means * m
+            q = round_half_away((y - m_hat) * m) * (s_hat > self.thr).to(self.dtype)
+            q = torch.clamp(q, -128, 127)
+            # same association as the reference kernel: (q + mean) first, then the running sum
+            y_q = y_q + q
+            y_hat = y_hat + (q + m_hat)
+        y_hat = y_hat * q_dec
+        # symbols in NHWC order (stream.cu:126-173)
+        s_nhwc = scales[0].permute(1, 2, 0).reshape(-1).numpy()
+        q_nhwc = y_q[0].permute(1, 2, 0).reshape(-1).numpy().astype(np.int64)
+        cond = s_nhwc > self.thr
+        idx = scale_index(s_nhwc)
+        sym = ((q_nhwc << 8) + idx.astype(np.int64)).astype(np.int16)[cond]
+        z_i8 = z_hat[0].permute(1, 2, 0).reshape(-1).numpy().astype(np.int8)
+        ecp = ec_parallel or ec_parallel_for(sym.size)
+        data = rans_encode(self.cdf_z, self.len_z, self.cdf_y, self.len_y, sym, z_i8,
+                           qp * 128, 128, ecp)
+        # memory update (enc_1)
+        feature = self.decoder(y_hat, self.ctx, self.q("q_decoder", qp))
+        if reset_feature_memory:
+            self.memory = self.feature_adaptor_i(self.recon_head_reset(feature))
+        else:
+            self.memory = self.feature_adaptor_m(self.memory, feature)
+        self.ctx = self.feature_extractor(self.memory)
+        return {"bit_stream": data, "ec_parallel": ecp, "y_q": y_q, "y_hat": y_hat,
+                "z_hat": z_hat, "scales": scales, "symbols": sym, "cond": cond, "idx": idx,
+                "feature": feature}
+
+    @torch.no_grad()
+    def decompress(self, bit_stream, qp, height, width, ec_parallel, reset_feature_memory):
+        Hp, Wp = (height + 15) // 16 * 16, (width + 15) // 16 * 16
+        H16, W16 = Hp // 16, Wp // 16
+        H64, W64 = (height + 63) // 64, (width + 63) // 64
+        if self.memory_has_value:
+            self.memory = self.feature_adaptor_m(self.memory, self.feature_p)
+        else:
+            self.memory = self.feature_adaptor_i(self.feature_i)
+        temporal = self.temporal_prior(self.memory, self.q("q_feature", qp))
+        n_z = 128 * H64 * W64
+        # z first (the payload is decoded in the reverse order of encoding)
+        _, z_i8 = rans_decode(self.cdf_z, self.len_z, self.cdf_y, self.len_y, bit_stream,
+                              np.zeros(0, np.uint8), n_z, qp * 128, 128, ec_parallel)
+        z_hat = torch.from_numpy(z_i8.astype(np.float64)).to(self.dtype).reshape(H64, W64, 128)
+        z_hat = z_hat.permute(2, 0, 1)[None]
+        common, q_dec, scales, means = self.entropy_params(z_hat, temporal, H16, W16)
+        s_nhwc = scales[0].permute(1, 2, 0).reshape(-1).numpy()
+        cond = s_nhwc > self.thr
+        idx = scale_index(s_nhwc)[cond]
+        y_dec, _ = rans_decode_y(self, bit_stream, idx, n_z, qp, ec_parallel)
+        full = np.zeros(s_nhwc.size, np.float64)
+        full[cond] = y_dec
+        C = scales.shape[1]
+        y_q = torch.from_numpy(full).to(self.dtype).reshape(H16, W16, C).permute(2, 0, 1)[None]
+        self.ctx = self.feature_extractor(self.memory)
+        reduced = self.conv("y_spatial_prior_reduction.", common)
+        y_hat = torch.zeros_like(y_q)
+        for k in range(4):
+            if k > 0:
+                means = self.spatial_prior(k, y_hat, reduced)
+            m = checker_mask(k, C, H16, W16, self.dtype)
+            y_hat = y_hat + (y_q + means) * m
+        y_hat = y_hat * q_dec
+        feature = self.decoder(y_hat, self.ctx, self.q("q_decoder", qp))
+        frames, head7 = self.recon_head(feature)
+        self.feature_p = feature
+        self.feature_i = head7
+        self.memory_has_value = not reset_feature_memory
+        return {"x_hat": frames, "y_q": y_q, "y_hat": y_hat, "z_hat": z_hat, "scales": scales}
+
+
+def rans_decode_y(oracle, data, y_idx, n_z, qp, ecp):
+    """Decodes z then y from one payload (z is discarded here)."""
+    y, z = rans_decode(oracle.cdf_z, oracle.len_z, oracle.cdf_y, oracle.len_y, data,
+                       np.ascontiguousarray(y_idx, np.uint8), n_z, qp * 128, 128, ecp)
+    return y, z
+
+
+# ----------------------------------------------------------------------------- metrics
+
+def psnr_yuv420(x_hat, y, u, v):
+    """PSNR of one model-domain frame [1, 3, H, W] against uint8 4:2:0 planes as the reference
+    harness computes it (test_video.py:32-66, metrics.py:10-24): x_hat + 0.5, chroma average-
+    pooled 2x2, x255 and clamped; returns (weighted, y, u, v) with weights (6, 1, 1) / 8."""
+    x = x_hat.double().cpu() + 0.5
+    H, W = y.shape
+    x = x[:, :, :H, :W]
+    yr = torch.clamp(x[:, :1] * 255, 0, 255)[0, 0].numpy()
+    uv = F.avg_pool2d(x[:, 1:], kernel_size=2, stride=2)
+    uv = torch.clamp(uv * 255, 0, 255)[0].numpy()
+
+    def p(a, b):
+        mse = np.mean((a.astype(np.float64) - b.astype(np.float64)) ** 2)
+        if mse <= 1e-10:
+            return 999.9
+        return min(10 * math.log10(255.0 * 255.0 / mse), 99.9)
+
+    py, pu, pv = p(y, yr), p(u, uv[0]), p(v, uv[1])
+    return (6 * py + pu + pv) / 8, py, pu, pv

@@ -11,14 +11,15 @@ SKIP_THRES = 0.15
 
 
 @functools.lru_cache(maxsize=4)
-def state_dict(seed=0, perturbed=True):
-    """fp16 CUDA state dict with CDF tables (built from the fp32 parameters first, as the
-    reference harness runs update() before .half())."""
+def state_dict(seed=0, perturbed=True, device="cuda"):
+    """fp16 state dict with CDF tables (built from the fp32 parameters first, as the reference
+    harness runs update() before .half()).  perturbed=True: the calibrated seed-0 weights with
+    per-QP quant vectors (numerically stable); False: the exact random init."""
     sd = perturbed_hts_state_dict(seed) if perturbed else hts_state_dict(seed)
     sd = add_cdf_to_state_dict(sd)
     out = {}
     for k, v in sd.items():
-        out[k] = v.half().cuda() if v.is_floating_point() else v
+        out[k] = v.half().to(device) if v.is_floating_point() else v
     return out
 
 

@@ -1,0 +1,162 @@
+"""Elementwise, layout, quantisation and compaction kernels through the C ABI against the NumPy
+FP16 oracle (oracle/elementwise_oracle.py): bit-exact.  Depthwise 3x3 against PyTorch FP32."""
+import os
+import sys
+
+import numpy as np
+import pytest
+import torch
+
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(__file__)), "oracle"))
+import elementwise_oracle as O  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+def _rng(seed):
+    return np.random.default_rng(seed)
+
+
+def _f16(a):
+    return np.asarray(a, dtype=np.float32).astype(np.float16)
+
+
+def _dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def _same(gpu, ref):
+    """Bitwise equality; on a mismatch, reports the first differing elements."""
+    g = gpu.cpu().numpy()
+    ref = np.asarray(ref)
+    assert g.shape == ref.shape, (g.shape, ref.shape)
+    if g.dtype == np.float16:
+        a, b = g.view(np.uint16), ref.astype(np.float16).view(np.uint16)
+    else:
+        a, b = g, ref
+    bad = np.flatnonzero(a.reshape(-1) != b.reshape(-1))
+    if bad.size:
+        i = bad[:5]
+        raise AssertionError(f"{bad.size} mismatches, first at {i.tolist()}: gpu "
+                             f"{g.reshape(-1)[i].tolist()} oracle {ref.reshape(-1)[i].tolist()}")
+    return True
+
+
+def _edge_values(rng, n, scale=4.0):
+    v = rng.standard_normal(n) * scale
+    k = n // 8
+    v[:k] = np.round(v[:k] * 2) / 2           # exact halves: rounding ties
+    v[k:2 * k] = rng.integers(-300, 300, k)   # integers, some beyond the int8 range
+    return _f16(v)
+
+
+def test_layout_kernels():
+    from dcvc_b200 import ops
+    rng = _rng(1)
+    x = _f16(rng.standard_normal((100, 120, 24)))
+    assert _same(ops.pad_unshuffle8(_dev(x), 4, 8), O.pad_unshuffle8(x, 4, 8))
+    y = _f16(rng.standard_normal((13 * 15, 192)) * 0.7)
+    y[0, :5] = np.nan
+    assert _same(ops.shuffle8_clamp(_dev(y), 13, 15), O.shuffle8_clamp(y, 13, 15))
+    z = _f16(rng.standard_normal((34 * 60, 256)))
+    assert _same(ops.space_to_depth2(_dev(z), 34, 60), O.space_to_depth2(z, 34, 60))
+    assert _same(ops.im2col3x3s2(_dev(z), 34, 60), O.im2col3x3s2(z, 34, 60))
+    w = _f16(rng.standard_normal((45 * 30, 256)))
+    assert _same(ops.replicate_pad(_dev(w), 45, 30, 3, 2), O.replicate_pad(w, 45, 30, 3, 2))
+    p = O.replicate_pad(w, 45, 30, 3, 2)
+    assert _same(ops.crop(_dev(p), 32, 45, 30), w)
+
+
+def test_latent_kernels():
+    from dcvc_b200 import ops
+    rng = _rng(2)
+    z = _edge_values(rng, 17 * 30 * 128, 20.0)
+    z[:3] = [np.nan, 63.5, -64.5]
+    zh, zi = ops.round_z(_dev(z))
+    rh, ri = O.round_z(z)
+    assert _same(zh, rh) and _same(zi, ri)
+    assert _same(ops.int8_to_half(_dev(ri)), ri.astype(np.float16))
+    x = _f16(rng.standard_normal((2040, 512)))
+    q = _f16(rng.uniform(0.2, 3.0, 512))
+    assert _same(ops.mul_channel(_dev(x), _dev(q)), O.mul_channel(x, q))
+    y = _f16(rng.standard_normal((2040, 256)) * 3)
+    qd = _f16(rng.uniform(-1.0, 4.0, (2040, 768)))[:, :256]
+    qd_full = _f16(rng.uniform(-1.0, 4.0, (2040, 768)))
+    yd = _dev(y)
+    ops.div_clamp_(yd, _dev(qd_full)[:, :256])
+    assert _same(yd, O.div_clamp(y, qd_full[:, :256]))
+
+
+@pytest.mark.parametrize("phase", [0, 1, 2, 3])
+def test_quantize_and_restore(phase):
+    from dcvc_b200 import ops
+    rng = _rng(10 + phase)
+    H, W, C = 14, 18, 256
+    M = H * W
+    thr = 0.15
+    y = _edge_values(rng, M * C, 3.0).reshape(M, C)
+    common = _f16(rng.standard_normal((M, 768)))
+    common[:, 256:512] = _f16(np.abs(rng.standard_normal((M, 256))) * 0.3)
+    common[0, 256:264] = [0.15, np.float16(0.15), 0.1501, 0.1499, np.nan, -1, 0, 1e4]
+    scales, means, q_dec = common[:, 256:512], common[:, 512:768], common[:, 0:256]
+    prev_q = _f16(rng.integers(-3, 4, (M, C)))
+    prev_h = _f16(rng.standard_normal((M, C)))
+    for mode in (0, 1, 2):
+        yq = _dev(prev_q)
+        yh = _dev(prev_h)
+        cd = _dev(common)
+        ops.quantize_phase(phase, mode, _dev(y), cd[:, 256:512], cd[:, 512:768],
+                           cd[:, 0:256] if mode == 2 else None, thr, yq, yh, H, W)
+        rq, rh = O.quantize_phase(phase, mode, y, scales, means, q_dec, thr, prev_q, prev_h, H, W)
+        assert _same(yq, rq) and _same(yh, rh), mode
+        out = _dev(prev_h)
+        ops.restore_phase(phase, mode, _dev(rq), cd[:, 512:768], cd[:, 0:256] if mode == 2 else None,
+                          out, H, W)
+        assert _same(out, O.restore_phase(phase, mode, rq, means, q_dec, prev_h, H, W)), mode
+
+
+def test_build_index_over_all_scales():
+    from dcvc_b200 import ops
+    lut_dev = ops.scale_index_table()
+    lut = lut_dev.cpu().numpy()
+    bits = np.arange(65536, dtype=np.uint32).astype(np.uint16)
+    scales = bits.view(np.float16).reshape(-1, 256)
+    rng = _rng(3)
+    y_q = _f16(rng.integers(-128, 128, scales.shape))
+    for enc in (True, False):
+        out, cond = ops.build_index(enc, _dev(y_q) if enc else None, _dev(scales), 0.15, lut_dev)
+        rout, rcond = O.build_index(enc, y_q, scales, 0.15, lut)
+        assert _same(out, rout) and _same(cond, rcond)
+    assert lut.max() == 127 and lut.min() == 0
+
+
+@pytest.mark.parametrize("n", [1, 7, 8, 8191, 8192, 8193, 100003, 2088960])
+def test_compaction_and_recover(n):
+    from dcvc_b200 import ops
+    rng = _rng(n)
+    density = [0.0, 0.05, 0.5, 1.0][n % 4]
+    cond = (rng.random(n) < density).astype(np.uint8)
+    sym = rng.integers(-32768, 32767, n).astype(np.int16)
+    idx = rng.integers(0, 256, n).astype(np.uint8)
+    for src in (sym, idx):
+        dst, total, counts = ops.compact(_dev(src), _dev(cond))
+        ref, k = O.compact(src, cond)
+        assert int(total.item()) == k
+        assert _same(dst[:k], ref)
+    dec = rng.integers(-128, 128, n).astype(np.int8)
+    _, total, counts = ops.compact(_dev(idx), _dev(cond))
+    assert _same(ops.recover(_dev(dec), _dev(cond), counts), O.recover(dec, cond))
+
+
+@pytest.mark.parametrize("H,W,C", [(136, 240, 256), (17, 30, 128), (45, 60, 768), (7, 9, 64)])
+def test_dwconv3x3(H, W, C):
+    from dcvc_b200 import ops
+    g = torch.Generator(device="cuda").manual_seed(H * W + C)
+    x = torch.randn(H * W, C, device="cuda", generator=g).half()
+    w = torch.randn(9, C, device="cuda", generator=g)
+    out = ops.dwconv3x3(x, H, W, w)
+    ref = torch.nn.functional.conv2d(
+        x.float().view(1, H, W, C).permute(0, 3, 1, 2), w.t().reshape(C, 1, 3, 3), padding=1,
+        groups=C).permute(0, 2, 3, 1).reshape(H * W, C)
+    err = (out.float() - ref).abs()
+    assert bool((err <= 1e-2 + 1e-2 * ref.abs()).all()), float(err.max())
