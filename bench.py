@@ -71,6 +71,16 @@ def workload_config(H, W, n):
 
 # ----------------------------------------------------------------------------- helpers
 
+def max_over_ranks(value, device):
+    """Maximum of a float over all ranks of the default process group (or the value itself
+    without one); gloo (CPU tensor) or NCCL (device tensor)."""
+    import torch.distributed as dist
+    t = torch.tensor([float(value)], device=device, dtype=torch.float64)
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 class ClockSampler:
     """nvidia-smi clock/throttle sampling during the timed region."""
 
@@ -306,10 +316,7 @@ def run_gpu(args):
         dist.barrier()
     ms = marks[0].elapsed_time(marks[-1])
     lat = [marks[i].elapsed_time(marks[i + 1]) for i in range(args.steps)]
-    t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max = max_over_ranks(ms, "cuda")
     value = FRAMES * args.steps * world / (ms_max / 1e3)
 
     # ---------------- end to end through the proxy API from pinned host memory
@@ -331,10 +338,7 @@ def run_gpu(args):
             out_host[f].copy_(frames[f][0], non_blocking=True)
     e1.record(stream)
     torch.cuda.synchronize()
-    t2 = torch.tensor([e0.elapsed_time(e1)], device="cuda", dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(t2, op=dist.ReduceOp.MAX)
-    e2e = FRAMES * args.steps * world / (float(t2.item()) / 1e3)
+    e2e = FRAMES * args.steps * world / (max_over_ranks(e0.elapsed_time(e1), "cuda") / 1e3)
 
     roof = roofline_quad(stream)
     cpu = None
