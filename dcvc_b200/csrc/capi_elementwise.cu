@@ -122,6 +122,19 @@ int dcvc_compact(const void* src, int elem_bytes, const uint8_t* cond, int n, in
                 "dcvc_compact");
 }
 
+int dcvc_compact_noalloc(const void* src, int elem_bytes, const uint8_t* cond, int n, void* dst,
+                         int* total, void* stream)
+{
+    if (n > compact_noalloc_max_elements()) {
+        set_last_error("dcvc_compact_noalloc: n = " + std::to_string(n) + " exceeds the maximum of " +
+                       std::to_string(compact_noalloc_max_elements()) +
+                       " elements of the built-in scratch; use dcvc_compact with a caller buffer");
+        return kInvalidArgument;
+    }
+    return wrap(launch_compact_noalloc(src, elem_bytes, cond, n, dst, total, S(stream)),
+                "dcvc_compact_noalloc");
+}
+
 int dcvc_recover(const int8_t* dec, const uint8_t* cond, const int* block_counts, int n, void* out,
                  void* stream)
 {

@@ -1,6 +1,8 @@
 #include "elementwise.cuh"
 #include "host_util.h"
 
+#include <mutex>
+
 namespace dcvc {
 
 namespace {
@@ -836,6 +838,73 @@ cudaError_t launch_dwconv3x3(const __half* x, int H, int W, int C, int ldx, cons
     }
     const dim3 grid((C / 8 + kDwCV - 1) / kDwCV, (H + kDwTH - 1) / kDwTH, (W + kDwTW - 1) / kDwTW);
     dwconv3x3_kernel<<<grid, kDwThreads, 0, s>>>(x, H, W, C, ldx, w, out, ldo);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------ no-alloc compaction
+//
+// Allocation-free variant of launch_compact for callers that cannot allocate device memory.  The
+// per-block counts live in this file-scope device array instead of a caller buffer: 16 KB, enough
+// for kCompactNoAllocMaxBlocks blocks of 8192 elements (n <= 33,554,432).  Every GPU that loads the
+// library holds the array until the process exits.  All calls share it and it keeps the last
+// call's contents; each call's count kernel writes every entry its scatter kernel reads, so
+// nothing needs clearing, but two calls whose kernels overlap on the GPU (different streams, no
+// ordering) race on it.
+
+constexpr int kCompactNoAllocMaxBlocks = 4096;
+static __device__ __align__(256) int g_compact_block_counts[kCompactNoAllocMaxBlocks];
+
+int compact_noalloc_max_elements() { return kCompactNoAllocMaxBlocks * kCompactBlock; }
+
+// The host cannot use g_compact_block_counts as a device address: its device address is looked
+// up once per device (with that device current) and cached.  The lookup happens on the first call
+// on each device, so that first call must not be made while a stream is being captured.
+static int* compact_noalloc_scratch(cudaError_t* err)
+{
+    static std::mutex mu;
+    static int* addr[64] = {nullptr};
+    int dev = 0;
+    *err = cudaGetDevice(&dev);
+    if (*err != cudaSuccess) {
+        return nullptr;
+    }
+    if (dev < 0 || dev >= 64) {
+        *err = cudaErrorInvalidDevice;
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lk(mu);
+    if (addr[dev] == nullptr) {
+        void* p = nullptr;
+        *err = cudaGetSymbolAddress(&p, g_compact_block_counts);
+        if (*err != cudaSuccess) {
+            return nullptr;
+        }
+        addr[dev] = static_cast<int*>(p);
+    }
+    return addr[dev];
+}
+
+cudaError_t launch_compact_noalloc(const void* src, int elem_bytes, const uint8_t* cond, int n,
+                                   void* dst, int* total, cudaStream_t s)
+{
+    if (n <= 0 || n > compact_noalloc_max_elements() || (elem_bytes != 1 && elem_bytes != 2) ||
+        (reinterpret_cast<uintptr_t>(cond) & 7)) {
+        return cudaErrorInvalidValue;
+    }
+    cudaError_t err = cudaSuccess;
+    int* counts = compact_noalloc_scratch(&err);
+    if (counts == nullptr) {
+        return err;
+    }
+    const int nb = compact_blocks(n);
+    compact_count_kernel<<<nb, kCompactThreads, 0, s>>>(cond, n, counts);
+    if (elem_bytes == 1) {
+        compact_scatter_kernel<uint8_t><<<nb, kCompactThreads, 0, s>>>(
+            static_cast<const uint8_t*>(src), cond, n, counts, static_cast<uint8_t*>(dst), total);
+    } else {
+        compact_scatter_kernel<int16_t><<<nb, kCompactThreads, 0, s>>>(
+            static_cast<const int16_t*>(src), cond, n, counts, static_cast<int16_t*>(dst), total);
+    }
     return cudaGetLastError();
 }
 

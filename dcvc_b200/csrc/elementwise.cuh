@@ -97,6 +97,12 @@ int compact_blocks(int n);
 cudaError_t launch_compact(const void* src, int elem_bytes, const uint8_t* cond, int n,
                            int* block_counts, void* dst, int* total, cudaStream_t s);
 
+// Allocation-free variant of launch_compact: the block counts live in a file-scope device array
+// (n <= compact_noalloc_max_elements()); see elementwise.cu for the sharing rules.
+int compact_noalloc_max_elements();
+cudaError_t launch_compact_noalloc(const void* src, int elem_bytes, const uint8_t* cond, int n,
+                                   void* dst, int* total, cudaStream_t s);
+
 // conditional_recover_with_type_conversion (stream.cu:359-420): out[i] = cond[i] ? dec[rank(i)]
 // : 0, using the block counts written by launch_compact over the same cond.
 cudaError_t launch_recover(const int8_t* dec, const uint8_t* cond, const int* block_counts, int n,

@@ -133,6 +133,16 @@ int dcvc_build_index(int encode, const void* y_q, int ldq, const void* scales, i
 int dcvc_compact_blocks(int n);
 int dcvc_compact(const void* src, int elem_bytes, const uint8_t* cond, int n, int* block_counts,
                  void* dst, int* total, void* stream);
+/* Allocation-free dcvc_compact, for callers that cannot allocate device memory (a caller whose
+ * device memory is pre-partitioned by its own allocator, or that cannot take cudaMalloc's implicit
+ * synchronisation on its path): same inputs and outputs, no block_counts argument.  No counterpart
+ * in the reference.  The block counts live in a 16 KB array inside the library (every GPU that
+ * loads the library holds it until exit), so n <= 33,554,432 (4096 blocks of 8192); larger n is
+ * rejected with DCVC_INVALID_ARGUMENT.  The first call on a device looks up the array's device
+ * address and must not be made during stream capture.  All calls share the array: calls whose
+ * kernels may overlap on the GPU race and must be ordered by the caller.  Allocates nothing. */
+int dcvc_compact_noalloc(const void* src, int elem_bytes, const uint8_t* cond, int n, void* dst,
+                         int* total, void* stream);
 /* conditional_recover_with_type_conversion :359-420, with the block counts of dcvc_compact. */
 int dcvc_recover(const int8_t* dec, const uint8_t* cond, const int* block_counts, int n, void* out,
                  void* stream);
