@@ -30,6 +30,20 @@ __device__ __forceinline__ void report_error(int* flag, int code)
     }
 }
 
+// ---------------------------------------------------------------- programmatic dependent launch
+//
+// Kernels are launched with programmatic stream serialisation: a kernel may start while its
+// predecessor in the stream drains.  Each kernel signals early that its dependents may launch and
+// waits for the full completion (and memory flush) of its predecessor before touching any data
+// the predecessor produces.
+
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+__device__ __forceinline__ void griddep_launch_dependents()
+{
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // ---------------------------------------------------------------- shared-memory helpers
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p)

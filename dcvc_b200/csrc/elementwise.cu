@@ -1,4 +1,5 @@
 #include "elementwise.cuh"
+#include "common.cuh"
 #include "host_util.h"
 
 #include <mutex>
@@ -39,6 +40,8 @@ __device__ __forceinline__ void st8(__half* p, const Vec8h& v) { *reinterpret_ca
 __global__ void pad_unshuffle8_kernel(const __half* __restrict__ x, int H, int W, int C, int ldx,
                                       int H8, int W8, __half* __restrict__ out, int ldo)
 {
+    griddep_launch_dependents();
+    griddep_wait();
     // one thread = 8 output channels c*64 + dy*8 + [0, 8) of one output pixel
     const long long vec_per_pix = static_cast<long long>(C) * 8;
     const long long total = static_cast<long long>(H8) * W8 * vec_per_pix;
@@ -64,6 +67,8 @@ __global__ void pad_unshuffle8_kernel(const __half* __restrict__ x, int H, int W
 __global__ void shuffle8_clamp_kernel(const __half* __restrict__ in, int H8, int W8, int C, int ldi,
                                       __half* __restrict__ out)
 {
+    griddep_launch_dependents();
+    griddep_wait();
     const int Wp = W8 * 8;
     const long long total = static_cast<long long>(H8) * 8 * Wp;
     const __half lo = __float2half_rn(-0.5f);
@@ -86,6 +91,8 @@ __global__ void shuffle8_clamp_kernel(const __half* __restrict__ in, int H8, int
 __global__ void space_to_depth2_kernel(const __half* __restrict__ x, int H, int W, int C, int ldx,
                                        __half* __restrict__ out)
 {
+    griddep_launch_dependents();
+    griddep_wait();
     const int Ho = H / 2, Wo = W / 2;
     const int vecs = C / 8;
     const long long total = static_cast<long long>(Ho) * Wo * 4 * vecs;
@@ -107,6 +114,8 @@ __global__ void space_to_depth2_kernel(const __half* __restrict__ x, int H, int 
 __global__ void im2col3x3s2_kernel(const __half* __restrict__ x, int H, int W, int C, int ldx,
                                    __half* __restrict__ out)
 {
+    griddep_launch_dependents();
+    griddep_wait();
     const int Ho = H / 2, Wo = W / 2;
     const int vecs = C / 8;
     const long long total = static_cast<long long>(Ho) * Wo * 9 * vecs;
@@ -136,6 +145,8 @@ __global__ void im2col3x3s2_kernel(const __half* __restrict__ x, int H, int W, i
 __global__ void replicate_pad_kernel(const __half* __restrict__ x, int H, int W, int C, int ldx,
                                      int Hp, int Wp, __half* __restrict__ out)
 {
+    griddep_launch_dependents();
+    griddep_wait();
     const int vecs = C / 8;
     const long long total = static_cast<long long>(Hp) * Wp * vecs;
     for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
@@ -152,6 +163,8 @@ __global__ void replicate_pad_kernel(const __half* __restrict__ x, int H, int W,
 __global__ void crop_kernel(const __half* __restrict__ x, int Wx, int ldx, int H, int W, int C,
                             __half* __restrict__ out, int ldo)
 {
+    griddep_launch_dependents();
+    griddep_wait();
     const int vecs = C / 8;
     const long long total = static_cast<long long>(H) * W * vecs;
     for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
@@ -169,6 +182,8 @@ __global__ void crop_kernel(const __half* __restrict__ x, int Wx, int ldx, int H
 __global__ void round_z_kernel(const __half* __restrict__ z, int n, __half* __restrict__ z_hat,
                                int8_t* __restrict__ z_i8)
 {
+    griddep_launch_dependents();
+    griddep_wait();
     const __half lo = __float2half_rn(-64.f), hi = __float2half_rn(63.f);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         __half v = f2h(roundf(h2f(z[i])));
@@ -181,6 +196,8 @@ __global__ void round_z_kernel(const __half* __restrict__ z, int n, __half* __re
 
 __global__ void int8_to_half_kernel(const int8_t* __restrict__ x, int n, __half* __restrict__ out)
 {
+    griddep_launch_dependents();
+    griddep_wait();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         out[i] = f2h(static_cast<float>(x[i]));
     }
@@ -189,6 +206,8 @@ __global__ void int8_to_half_kernel(const int8_t* __restrict__ x, int n, __half*
 __global__ void mul_channel_kernel(const __half* __restrict__ x, int M, int C, int ldx,
                                    const __half* __restrict__ q, __half* __restrict__ out, int ldo)
 {
+    griddep_launch_dependents();
+    griddep_wait();
     const int vecs = C / 8;
     const long long total = static_cast<long long>(M) * vecs;
     for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
@@ -208,6 +227,8 @@ __global__ void mul_channel_kernel(const __half* __restrict__ x, int M, int C, i
 __global__ void div_clamp_kernel(__half* __restrict__ y, int M, int C, int ldy,
                                  const __half* __restrict__ q, int ldq)
 {
+    griddep_launch_dependents();
+    griddep_wait();
     const int vecs = C / 8;
     const long long total = static_cast<long long>(M) * vecs;
     const __half half_ = __float2half_rn(0.5f);
@@ -237,6 +258,8 @@ __global__ void quantize_phase_kernel(int phase, const __half* __restrict__ y, i
                                       __half* __restrict__ y_q, int ldq, __half* __restrict__ y_hat,
                                       int ldh, int H, int W, int C)
 {
+    griddep_launch_dependents();
+    griddep_wait();
     const int vecs = C / 8;
     const int quarter_vecs = vecs / 4;
     const long long total = static_cast<long long>(H) * W * vecs;
@@ -293,6 +316,8 @@ __global__ void restore_phase_kernel(int phase, const __half* __restrict__ y_q, 
                                      const __half* __restrict__ q_dec, int ldd,
                                      __half* __restrict__ y_hat, int ldh, int H, int W, int C)
 {
+    griddep_launch_dependents();
+    griddep_wait();
     const int vecs = C / 8;
     const int quarter_vecs = vecs / 4;
     const long long total = static_cast<long long>(H) * W * vecs;
@@ -336,6 +361,8 @@ __global__ void build_index_kernel(const __half* __restrict__ y_q, int ldq,
                                    int16_t* __restrict__ sym, uint8_t* __restrict__ idx_out,
                                    uint8_t* __restrict__ cond)
 {
+    griddep_launch_dependents();
+    griddep_wait();
     const int vecs = C / 8;
     const long long total = static_cast<long long>(M) * vecs;
     for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
@@ -439,6 +466,8 @@ __device__ __forceinline__ int block_exclusive_scan(int x, int* warp_sums, int& 
 __global__ void __launch_bounds__(kCompactThreads) compact_count_kernel(const uint8_t* __restrict__ cond,
                                                                         int n, int* __restrict__ counts)
 {
+    griddep_launch_dependents();
+    griddep_wait();
     __shared__ int ws[33];
     uint8_t c[8];
     const int base = blockIdx.x * kCompactBlock + threadIdx.x * kCompactPer;
@@ -470,6 +499,8 @@ __global__ void __launch_bounds__(kCompactThreads)
                            const int* __restrict__ counts, T* __restrict__ dst,
                            int* __restrict__ total)
 {
+    griddep_launch_dependents();
+    griddep_wait();
     __shared__ int ws[33];
     __shared__ int block_off;
     if (threadIdx.x < 32) {
@@ -499,6 +530,8 @@ __global__ void __launch_bounds__(kCompactThreads)
     recover_kernel(const int8_t* __restrict__ dec, const uint8_t* __restrict__ cond,
                    const int* __restrict__ counts, int n, __half* __restrict__ out)
 {
+    griddep_launch_dependents();
+    griddep_wait();
     __shared__ int ws[33];
     __shared__ int block_off;
     if (threadIdx.x < 32) {
@@ -536,6 +569,8 @@ __global__ void __launch_bounds__(kDwThreads) dwconv3x3_kernel(const __half* __r
                                                                const float* __restrict__ wt,
                                                                __half* __restrict__ out, int ldo)
 {
+    griddep_launch_dependents();
+    griddep_wait();
     __shared__ Vec8h tile[kDwTH + 2][kDwTW + 2][kDwCV];
     const int c0 = blockIdx.x * kDwCV;  // first channel vector
     const int h0 = blockIdx.y * kDwTH;
@@ -625,7 +660,7 @@ cudaError_t launch_pad_unshuffle8(const __half* x, int H, int W, int C, int ldx,
         return cudaErrorInvalidValue;
     }
     const int H8 = (H + pad_b) / 8, W8 = (W + pad_r) / 8;
-    pad_unshuffle8_kernel<<<grid_for(static_cast<long long>(H8) * W8 * C * 8), kThreads, 0, s>>>(
+    launch_pdl(pad_unshuffle8_kernel, dim3(grid_for(static_cast<long long>(H8) * W8 * C * 8)), dim3(kThreads), 0, s, 
         x, H, W, C, ldx, H8, W8, out, ldo);
     return cudaGetLastError();
 }
@@ -636,7 +671,7 @@ cudaError_t launch_shuffle8_clamp(const __half* in, int H8, int W8, int C, int l
     if (H8 <= 0 || W8 <= 0 || C <= 0) {
         return cudaErrorInvalidValue;
     }
-    shuffle8_clamp_kernel<<<grid_for(64LL * H8 * W8), kThreads, 0, s>>>(in, H8, W8, C, ldi, out);
+    launch_pdl(shuffle8_clamp_kernel, dim3(grid_for(64LL * H8 * W8)), dim3(kThreads), 0, s, in, H8, W8, C, ldi, out);
     return cudaGetLastError();
 }
 
@@ -646,8 +681,7 @@ cudaError_t launch_space_to_depth2(const __half* x, int H, int W, int C, int ldx
     if (H % 2 || W % 2 || C % 8 || ldx % 8 || !al16(x) || !al16(out)) {
         return cudaErrorInvalidValue;
     }
-    space_to_depth2_kernel<<<grid_for(static_cast<long long>(H / 2) * (W / 2) * C / 2), kThreads, 0,
-                             s>>>(x, H, W, C, ldx, out);
+    launch_pdl(space_to_depth2_kernel, dim3(grid_for(static_cast<long long>(H / 2) * (W / 2) * C / 2)), dim3(kThreads), 0, s, x, H, W, C, ldx, out);
     return cudaGetLastError();
 }
 
@@ -657,8 +691,7 @@ cudaError_t launch_im2col3x3s2(const __half* x, int H, int W, int C, int ldx, __
     if (H % 2 || W % 2 || C % 8 || ldx % 8 || !al16(x) || !al16(out)) {
         return cudaErrorInvalidValue;
     }
-    im2col3x3s2_kernel<<<grid_for(static_cast<long long>(H / 2) * (W / 2) * 9 * (C / 8)),
-                         kThreads, 0, s>>>(x, H, W, C, ldx, out);
+    launch_pdl(im2col3x3s2_kernel, dim3(grid_for(static_cast<long long>(H / 2) * (W / 2) * 9 * (C / 8))), dim3(kThreads), 0, s, x, H, W, C, ldx, out);
     return cudaGetLastError();
 }
 
@@ -669,7 +702,7 @@ cudaError_t launch_replicate_pad(const __half* x, int H, int W, int C, int ldx, 
         return cudaErrorInvalidValue;
     }
     const int Hp = H + pad_b, Wp = W + pad_r;
-    replicate_pad_kernel<<<grid_for(static_cast<long long>(Hp) * Wp * (C / 8)), kThreads, 0, s>>>(
+    launch_pdl(replicate_pad_kernel, dim3(grid_for(static_cast<long long>(Hp) * Wp * (C / 8))), dim3(kThreads), 0, s, 
         x, H, W, C, ldx, Hp, Wp, out);
     return cudaGetLastError();
 }
@@ -680,7 +713,7 @@ cudaError_t launch_crop(const __half* x, int Wx, int ldx, int H, int W, int C, _
     if (C % 8 || ldx % 8 || ldo % 8 || W > Wx || !al16(x) || !al16(out)) {
         return cudaErrorInvalidValue;
     }
-    crop_kernel<<<grid_for(static_cast<long long>(H) * W * (C / 8)), kThreads, 0, s>>>(
+    launch_pdl(crop_kernel, dim3(grid_for(static_cast<long long>(H) * W * (C / 8))), dim3(kThreads), 0, s, 
         x, Wx, ldx, H, W, C, out, ldo);
     return cudaGetLastError();
 }
@@ -690,7 +723,7 @@ cudaError_t launch_round_z(const __half* z, int n, __half* z_hat, int8_t* z_i8, 
     if (n <= 0) {
         return cudaErrorInvalidValue;
     }
-    round_z_kernel<<<grid_for(n), kThreads, 0, s>>>(z, n, z_hat, z_i8);
+    launch_pdl(round_z_kernel, dim3(grid_for(n)), dim3(kThreads), 0, s, z, n, z_hat, z_i8);
     return cudaGetLastError();
 }
 
@@ -699,7 +732,7 @@ cudaError_t launch_int8_to_half(const int8_t* x, int n, __half* out, cudaStream_
     if (n <= 0) {
         return cudaErrorInvalidValue;
     }
-    int8_to_half_kernel<<<grid_for(n), kThreads, 0, s>>>(x, n, out);
+    launch_pdl(int8_to_half_kernel, dim3(grid_for(n)), dim3(kThreads), 0, s, x, n, out);
     return cudaGetLastError();
 }
 
@@ -709,7 +742,7 @@ cudaError_t launch_mul_channel(const __half* x, int M, int C, int ldx, const __h
     if (C % 8 || ldx % 8 || ldo % 8 || !al16(x) || !al16(q) || !al16(out)) {
         return cudaErrorInvalidValue;
     }
-    mul_channel_kernel<<<grid_for(static_cast<long long>(M) * (C / 8)), kThreads, 0, s>>>(
+    launch_pdl(mul_channel_kernel, dim3(grid_for(static_cast<long long>(M) * (C / 8))), dim3(kThreads), 0, s, 
         x, M, C, ldx, q, out, ldo);
     return cudaGetLastError();
 }
@@ -720,7 +753,7 @@ cudaError_t launch_div_clamp(__half* y, int M, int C, int ldy, const __half* q, 
     if (C % 8 || ldy % 8 || ldq % 8 || !al16(y) || !al16(q)) {
         return cudaErrorInvalidValue;
     }
-    div_clamp_kernel<<<grid_for(static_cast<long long>(M) * (C / 8)), kThreads, 0, s>>>(y, M, C,
+    launch_pdl(div_clamp_kernel, dim3(grid_for(static_cast<long long>(M) * (C / 8))), dim3(kThreads), 0, s, y, M, C,
                                                                                           ldy, q, ldq);
     return cudaGetLastError();
 }
@@ -737,15 +770,15 @@ cudaError_t launch_quantize_phase(int phase, int mode, const __half* y, int ldy,
     }
     const int g = grid_for(static_cast<long long>(H) * W * (C / 8));
     if (mode == 0) {
-        quantize_phase_kernel<0><<<g, kThreads, 0, s>>>(phase, y, ldy, scales, lds, means, ldm,
+        launch_pdl(quantize_phase_kernel<0>, dim3(g), dim3(kThreads), 0, s, phase, y, ldy, scales, lds, means, ldm,
                                                         q_dec, ldd, thr, y_q, ldq, y_hat, ldh, H,
                                                         W, C);
     } else if (mode == 1) {
-        quantize_phase_kernel<1><<<g, kThreads, 0, s>>>(phase, y, ldy, scales, lds, means, ldm,
+        launch_pdl(quantize_phase_kernel<1>, dim3(g), dim3(kThreads), 0, s, phase, y, ldy, scales, lds, means, ldm,
                                                         q_dec, ldd, thr, y_q, ldq, y_hat, ldh, H,
                                                         W, C);
     } else {
-        quantize_phase_kernel<2><<<g, kThreads, 0, s>>>(phase, y, ldy, scales, lds, means, ldm,
+        launch_pdl(quantize_phase_kernel<2>, dim3(g), dim3(kThreads), 0, s, phase, y, ldy, scales, lds, means, ldm,
                                                         q_dec, ldd, thr, y_q, ldq, y_hat, ldh, H,
                                                         W, C);
     }
@@ -762,13 +795,13 @@ cudaError_t launch_restore_phase(int phase, int mode, const __half* y_q, int ldq
     }
     const int g = grid_for(static_cast<long long>(H) * W * (C / 8));
     if (mode == 0) {
-        restore_phase_kernel<0><<<g, kThreads, 0, s>>>(phase, y_q, ldq, means, ldm, q_dec, ldd,
+        launch_pdl(restore_phase_kernel<0>, dim3(g), dim3(kThreads), 0, s, phase, y_q, ldq, means, ldm, q_dec, ldd,
                                                        y_hat, ldh, H, W, C);
     } else if (mode == 1) {
-        restore_phase_kernel<1><<<g, kThreads, 0, s>>>(phase, y_q, ldq, means, ldm, q_dec, ldd,
+        launch_pdl(restore_phase_kernel<1>, dim3(g), dim3(kThreads), 0, s, phase, y_q, ldq, means, ldm, q_dec, ldd,
                                                        y_hat, ldh, H, W, C);
     } else {
-        restore_phase_kernel<2><<<g, kThreads, 0, s>>>(phase, y_q, ldq, means, ldm, q_dec, ldd,
+        launch_pdl(restore_phase_kernel<2>, dim3(g), dim3(kThreads), 0, s, phase, y_q, ldq, means, ldm, q_dec, ldd,
                                                        y_hat, ldh, H, W, C);
     }
     return cudaGetLastError();
@@ -781,7 +814,7 @@ cudaError_t launch_build_index_enc(const __half* y_q, int ldq, const __half* sca
     if (C % 8 || !al16(sym) || (reinterpret_cast<uintptr_t>(cond) & 7)) {
         return cudaErrorInvalidValue;
     }
-    build_index_kernel<true><<<grid_for(static_cast<long long>(M) * (C / 8)), kThreads, 0, s>>>(
+    launch_pdl(build_index_kernel<true>, dim3(grid_for(static_cast<long long>(M) * (C / 8))), dim3(kThreads), 0, s, 
         y_q, ldq, scales, lds, thr, lut, M, C, sym, nullptr, cond);
     return cudaGetLastError();
 }
@@ -793,7 +826,7 @@ cudaError_t launch_build_index_dec(const __half* scales, int lds, __half thr,
     if (C % 8 || (reinterpret_cast<uintptr_t>(idx) & 7) || (reinterpret_cast<uintptr_t>(cond) & 7)) {
         return cudaErrorInvalidValue;
     }
-    build_index_kernel<false><<<grid_for(static_cast<long long>(M) * (C / 8)), kThreads, 0, s>>>(
+    launch_pdl(build_index_kernel<false>, dim3(grid_for(static_cast<long long>(M) * (C / 8))), dim3(kThreads), 0, s, 
         nullptr, 0, scales, lds, thr, lut, M, C, nullptr, idx, cond);
     return cudaGetLastError();
 }
@@ -807,13 +840,13 @@ cudaError_t launch_compact(const void* src, int elem_bytes, const uint8_t* cond,
         return cudaErrorInvalidValue;
     }
     const int nb = compact_blocks(n);
-    compact_count_kernel<<<nb, kCompactThreads, 0, s>>>(cond, n, block_counts);
+    launch_pdl(compact_count_kernel, dim3(nb), dim3(kCompactThreads), 0, s, cond, n, block_counts);
     if (elem_bytes == 1) {
-        compact_scatter_kernel<uint8_t><<<nb, kCompactThreads, 0, s>>>(
+        launch_pdl(compact_scatter_kernel<uint8_t>, dim3(nb), dim3(kCompactThreads), 0, s, 
             static_cast<const uint8_t*>(src), cond, n, block_counts, static_cast<uint8_t*>(dst),
             total);
     } else {
-        compact_scatter_kernel<int16_t><<<nb, kCompactThreads, 0, s>>>(
+        launch_pdl(compact_scatter_kernel<int16_t>, dim3(nb), dim3(kCompactThreads), 0, s, 
             static_cast<const int16_t*>(src), cond, n, block_counts, static_cast<int16_t*>(dst),
             total);
     }
@@ -826,7 +859,7 @@ cudaError_t launch_recover(const int8_t* dec, const uint8_t* cond, const int* bl
     if (n <= 0 || (reinterpret_cast<uintptr_t>(cond) & 7)) {
         return cudaErrorInvalidValue;
     }
-    recover_kernel<<<compact_blocks(n), kCompactThreads, 0, s>>>(dec, cond, block_counts, n, out);
+    launch_pdl(recover_kernel, dim3(compact_blocks(n)), dim3(kCompactThreads), 0, s, dec, cond, block_counts, n, out);
     return cudaGetLastError();
 }
 
@@ -837,7 +870,7 @@ cudaError_t launch_dwconv3x3(const __half* x, int H, int W, int C, int ldx, cons
         return cudaErrorInvalidValue;
     }
     const dim3 grid((C / 8 + kDwCV - 1) / kDwCV, (H + kDwTH - 1) / kDwTH, (W + kDwTW - 1) / kDwTW);
-    dwconv3x3_kernel<<<grid, kDwThreads, 0, s>>>(x, H, W, C, ldx, w, out, ldo);
+    launch_pdl(dwconv3x3_kernel, dim3(grid), dim3(kDwThreads), 0, s, x, H, W, C, ldx, w, out, ldo);
     return cudaGetLastError();
 }
 

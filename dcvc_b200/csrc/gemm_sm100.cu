@@ -148,6 +148,9 @@ __global__ void __launch_bounds__(kThreads, 1)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem_base = *tmem_slot;
+    // setup above overlaps the predecessor's tail; its outputs are read only after this
+    griddep_launch_dependents();
+    griddep_wait();
 
     if (warp == 0) {
         // ------------------------------------------------------------ TMA producer
@@ -483,8 +486,7 @@ cudaError_t launch_one(const Maps& m, const GemmParams& p, cudaStream_t stream)
     }
     const int num_tiles = ((p.M + kBM - 1) / kBM) * (p.N / BN);
     const int grid = num_tiles < num_sms() ? num_tiles : num_sms();
-    kernel<<<grid, kThreads, C::kBytes, stream>>>(m.a, m.b, m.o, m.r, m.r2, p);
-    return cudaGetLastError();
+    return launch_pdl(kernel, dim3(grid), dim3(kThreads), C::kBytes, stream, m.a, m.b, m.o, m.r, m.r2, p);
 }
 
 template <typename T, int BN>

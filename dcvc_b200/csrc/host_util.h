@@ -19,4 +19,22 @@ bool make_tmap_2d(CUtensorMap* map, CUtensorMapDataType dtype, const void* base,
                   uint64_t outer, uint64_t row_bytes, uint32_t box_inner, uint32_t box_outer,
                   int swizzle_bytes = 128);
 
+// Launches `kernel` with programmatic stream serialisation (see griddep_wait in common.cuh).
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                       cudaStream_t stream, Args&&... args)
+{
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 }  // namespace dcvc
