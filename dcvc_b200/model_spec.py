@@ -21,6 +21,8 @@ CH_D = 512
 CH_M = 512
 CH_RECON = 256
 QP_NUM = 64
+# intra model sizes (image_model.py:11-14)
+CH_ENC_DEC_INTRA = 384
 
 
 class _Act(nn.Module):
@@ -135,16 +137,56 @@ class HTSModel(nn.Module):
         _init_xavier(self)
 
 
-def hts_state_dict(seed=0, dtype=torch.float32):
-    """State dict of a random-init HT-S model, equal to the reference DMC() under
-    torch.manual_seed(seed) (fp32 CPU; cast to `dtype`)."""
+class DMCIModel(nn.Module):
+    """Parameter tree of DMCI, the intra model (image_model.py:15-140).  Its resampling blocks
+    keep the reference's default shortcut (layers.py:162-188), which has no parameters."""
+
+    def __init__(self):
+        super().__init__()
+        self.bit_estimator_z = BitEstimator(QP_NUM, CH_Z)
+        c = CH_ENC_DEC_INTRA
+        enc = _Wrap(enc_1=DCB(CH_SRC_INTRA, c))
+        enc.enc_2 = _seq(*[DCB(c, c) for _ in range(6)], nn.Conv2d(c, CH_Y, 3, stride=2, padding=1))
+        self.enc = enc
+        self.hyper_enc = _Wrap(conv=_seq(DCB(CH_Y, CH_Z), RBDown(CH_Z, CH_Z), RBDown(CH_Z, CH_Z)))
+        self.hyper_dec = _Wrap(conv=_seq(RBUp(CH_Z, CH_Z), RBUp(CH_Z, CH_Z), DCB(CH_Z, CH_Y)))
+        self.y_prior_fusion = _Wrap(conv=_seq(DCB(CH_Y, CH_Y * 2), DCB(CH_Y * 2, CH_Y * 2),
+                                              DCB(CH_Y * 2, CH_Y * 2), nn.Conv2d(CH_Y * 2, CH_Y * 2, 1)))
+        self.y_spatial_prior_reduction = nn.Conv2d(CH_Y * 2, CH_Y, 1)
+        for k in (1, 2, 3):
+            setattr(self, f"y_spatial_prior_adaptor_{k}", DCB(CH_Y * 2, CH_Y * 2, force_adaptor=True))
+        sp = [DCB(CH_Y * 2, CH_Y * 2) for _ in range(3)]
+        self.y_spatial_prior = _Wrap(conv=_seq(*sp, nn.Conv2d(CH_Y * 2, CH_Y * 2, 1)))
+        dec = _Wrap(dec_1=_seq(RBUp(CH_Y, c), *[DCB(c, c) for _ in range(12)]))
+        dec.dec_2 = DCB(c, CH_SRC_INTRA)
+        self.dec = dec
+        self.q_scale_enc = nn.Parameter(torch.ones((QP_NUM, c)))
+        self.q_scale_dec = nn.Parameter(torch.ones((QP_NUM, c)))
+        self.q_scale_y_enc = nn.Parameter(torch.ones((QP_NUM, CH_Y)))
+        self.q_scale_y_dec = nn.Parameter(torch.ones((QP_NUM, CH_Y)))
+        _init_xavier(self)
+
+
+def _seeded(cls, seed, dtype):
     state = torch.random.get_rng_state()
     try:
         torch.manual_seed(seed)
-        model = HTSModel()
+        model = cls()
     finally:
         torch.random.set_rng_state(state)
     return {k: v.detach().to(dtype) for k, v in model.state_dict().items()}
+
+
+def dmci_state_dict(seed=0, dtype=torch.float32):
+    """State dict of a random-init intra model, equal to the reference DMCI() under
+    torch.manual_seed(seed) (fp32 CPU; cast to `dtype`)."""
+    return _seeded(DMCIModel, seed, dtype)
+
+
+def hts_state_dict(seed=0, dtype=torch.float32):
+    """State dict of a random-init HT-S model, equal to the reference DMC() under
+    torch.manual_seed(seed) (fp32 CPU; cast to `dtype`)."""
+    return _seeded(HTSModel, seed, dtype)
 
 
 # Residual-branch scale of the calibrated variant (see calibrated_hts_state_dict).
@@ -165,6 +207,25 @@ def calibrated_hts_state_dict(seed=0, dtype=torch.float32, alpha=CALIBRATION_ALP
     for k in list(sd):
         if k.endswith(("dc.3.weight", "ffn.2.weight")):
             sd[k] = sd[k] * alpha
+    return {k: v.to(dtype) for k, v in sd.items()}
+
+
+def calibrated_dmci_state_dict(seed=0, dtype=torch.float32, alpha=CALIBRATION_ALPHA):
+    """The seed-`seed` intra weights with the residual-branch output convolutions scaled by
+    `alpha`, for the reason given in calibrated_hts_state_dict."""
+    sd = dmci_state_dict(seed, torch.float32)
+    for k in list(sd):
+        if k.endswith(("dc.3.weight", "ffn.2.weight")):
+            sd[k] = sd[k] * alpha
+    return {k: v.to(dtype) for k, v in sd.items()}
+
+
+def perturbed_dmci_state_dict(seed=0, dtype=torch.float32, q_jitter=0.25, calibrated=True):
+    """Seed-`seed` intra weights with non-trivial per-QP quant vectors."""
+    sd = calibrated_dmci_state_dict(seed) if calibrated else dmci_state_dict(seed, torch.float32)
+    g = torch.Generator().manual_seed(seed + 19)
+    for k in ("q_scale_enc", "q_scale_dec", "q_scale_y_enc", "q_scale_y_dec"):
+        sd[k] = 1.0 + q_jitter * (torch.rand(sd[k].shape, generator=g) * 2 - 1)
     return {k: v.to(dtype) for k, v in sd.items()}
 
 

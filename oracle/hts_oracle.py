@@ -7,7 +7,7 @@ a state dict.  Used by tests/ (PSNR / bpp / symbol agreement against the GPU pat
 bench.py's reference arm; the module math is pinned against the reference nn.Modules by
 tests/golden/modules_golden.npz.
 
-Layer math follows src/layers/layers.py (DepthConvBlock :128-159, ResidualBlockWithStride2
+Layer math follows src/layers/layers.py (DepthConvBlock :128-159 with its shortcut :155-158, ResidualBlockWithStride2
 :176-188, ResidualBlockUpsample :162-173, SubpelConv2x :92-103, WSiLU :106-111,
 WSiLUChunkAdd :114-125) and src/models/video_model_ht.py (Encoder :64-92, HyperEncoder
 :186-200, HyperDecoder :167-183, PriorFusion :203-212, SpatialPrior :278-289, Decoder
@@ -91,7 +91,8 @@ def _oracle_lib():
     global _ORACLE_LIB
     if _ORACLE_LIB is None:
         so = os.path.join(HERE, "liboracle.so")
-        if not os.path.exists(so):
+        src = os.path.join(HERE, "rans_oracle.c")
+        if not os.path.exists(so) or os.path.getmtime(so) < os.path.getmtime(src):
             import subprocess
             subprocess.run(["make", "-C", HERE, so], check=True, capture_output=True)
         _ORACLE_LIB = ctypes.CDLL(so)
@@ -151,6 +152,87 @@ def rans_decode(cdf_z, len_z, cdf_y, len_y, data, y_idx, n_z, z_offset, z_ch, ec
     return y[: y_idx.size], z[:n_z]
 
 
+def rans_encode_segments(cdf_z, len_z, cdf_y, len_y, y_segments, z_sym, z_offset, z_ch, ecp):
+    """Several y segments (one encode_y call each, in coding order) then z."""
+    counts = np.array([s.size for s in y_segments], np.int32)
+    y_all = (np.ascontiguousarray(np.concatenate(y_segments), np.int16) if len(y_segments)
+             else np.zeros(0, np.int16))
+    cap = (y_all.size + z_sym.size) * 4 + 1024 + 64 * len(y_segments)
+    out = np.zeros(cap, np.uint8)
+    if USE_REFERENCE_CODER:
+        n = _REF_LIB.ref_encode_segments(
+            _p(cdf_z), _p(len_z), cdf_z.shape[0], cdf_z.shape[1], _p(cdf_y), _p(len_y),
+            cdf_y.shape[0], cdf_y.shape[1], _p(y_all), _p(counts), counts.size, _p(z_sym),
+            z_sym.size, z_offset, z_ch, ecp, _p(out), cap)
+    else:
+        n = _oracle_lib().oracle_encode_segments(
+            _p(cdf_z), _p(len_z), cdf_z.shape[1], _p(cdf_y), _p(len_y), cdf_y.shape[1],
+            _p(y_all), _p(counts), counts.size, _p(z_sym), z_sym.size, z_offset, z_ch, ecp,
+            _p(out), cap)
+    if n < 0:
+        raise RuntimeError("oracle rANS encode failed")
+    return out[:n].copy()
+
+
+class RansSegmentDecoder:
+    """Incremental decoding of one payload: z first, then y segments in the reverse order of
+    encoding (the reference decoder's call sequence, one decode_y per segment)."""
+
+    def __init__(self, cdf_z, len_z, cdf_y, len_y, data, ecp):
+        self.t = (cdf_z, len_z, cdf_y, len_y)
+        self.data = np.ascontiguousarray(data, np.uint8)
+        self.ref = USE_REFERENCE_CODER
+        if self.ref:
+            lib = _REF_LIB
+            lib.ref_dec_open.restype = ctypes.c_void_p
+            self.h = lib.ref_dec_open(_p(cdf_z), _p(len_z), cdf_z.shape[0], cdf_z.shape[1],
+                                      _p(cdf_y), _p(len_y), cdf_y.shape[0], cdf_y.shape[1],
+                                      _p(self.data), self.data.size, ecp)
+        else:
+            lib = _oracle_lib()
+            lib.oracle_dec_open.restype = ctypes.c_void_p
+            self.h = lib.oracle_dec_open(_p(self.data), self.data.size, ecp)
+        if not self.h:
+            raise RuntimeError("oracle rANS decoder: malformed container")
+        self.h = ctypes.c_void_p(self.h)
+
+    def decode_z(self, n_z, z_offset, z_ch):
+        cdf_z, len_z, _, _ = self.t
+        z = np.zeros(max(1, n_z), np.int8)
+        if self.ref:
+            rc = _REF_LIB.ref_dec_z(self.h, n_z, z_offset, z_ch, _p(z))
+        else:
+            rc = _oracle_lib().oracle_dec_z(self.h, _p(cdf_z), _p(len_z), cdf_z.shape[1], n_z,
+                                            z_offset, z_ch, _p(z))
+        if rc != 0:
+            raise RuntimeError("oracle rANS decode failed")
+        return z[:n_z]
+
+    def decode_y(self, idx):
+        _, _, cdf_y, len_y = self.t
+        idx = np.ascontiguousarray(idx, np.uint8)
+        y = np.zeros(max(1, idx.size), np.int8)
+        if self.ref:
+            rc = _REF_LIB.ref_dec_y(self.h, _p(idx), idx.size, _p(y))
+        else:
+            rc = _oracle_lib().oracle_dec_y(self.h, _p(cdf_y), _p(len_y), cdf_y.shape[1], _p(idx),
+                                            idx.size, _p(y))
+        if rc != 0:
+            raise RuntimeError("oracle rANS decode failed")
+        return y[: idx.size]
+
+    def close(self):
+        if self.h:
+            if self.ref:
+                _REF_LIB.ref_dec_close(self.h)
+            else:
+                _oracle_lib().oracle_dec_close(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
 def ec_parallel_for(n):
     return max(1, min(8, n // 32768))
 
@@ -192,7 +274,7 @@ class HtsOracle:
     def wsilu(x):
         return torch.sigmoid(4.0 * x) * x
 
-    def dcb(self, p, x, quant=None):
+    def dcb(self, p, x, quant=None, shortcut=False):
         if self.has(p + "adaptor.weight"):
             x = self.conv(p + "adaptor.", x)
         c = self.w[p + "dc.2.weight"].shape[0]
@@ -202,6 +284,8 @@ class HtsOracle:
         t = self.wsilu(self.conv(p + "ffn.0.", out))
         t = t[:, 0::4] + t[:, 1::4] + t[:, 2::4] + t[:, 3::4]
         out = self.conv(p + "ffn.2.", t) + out
+        if shortcut:
+            out = out + x
         if quant is not None:
             out = out * quant
         return out
@@ -211,14 +295,15 @@ class HtsOracle:
             x = self.dcb(f"{prefix}{i}.", x, quant if i == n - 1 else None)
         return x
 
-    def rb_down(self, p, x):
-        return self.dcb(p + "conv.", self.conv(p + "down.", F.pixel_unshuffle(x, 2)))
+    def rb_down(self, p, x, shortcut=False):
+        return self.dcb(p + "conv.", self.conv(p + "down.", F.pixel_unshuffle(x, 2)),
+                        shortcut=shortcut)
 
     def subpel(self, p, x):
         return F.pixel_shuffle(self.conv(p + "conv.0.", x), 2)
 
-    def rb_up(self, p, x):
-        return self.dcb(p + "conv.", self.subpel(p + "up.", x))
+    def rb_up(self, p, x, shortcut=False):
+        return self.dcb(p + "conv.", self.subpel(p + "up.", x), shortcut=shortcut)
 
     def q(self, name, qp):
         return self.w[name][qp][None, :, None, None]

@@ -206,15 +206,6 @@ static int8_t dec_symbol(dec_t* d, const int32_t* cdf, int32_t maxv)
 
 /* ---------------------------------------------------------------- container */
 
-typedef struct {
-    const int32_t* cdf_z;
-    const int32_t* len_z;
-    int z_stride;
-    const int32_t* cdf_y;
-    const int32_t* len_y;
-    int y_stride;
-} tables_t;
-
 static int common_tail_bytes(const uint8_t* a, int na, const uint8_t* b, int nb)
 {
     int lim = na < nb ? na : nb;
@@ -228,33 +219,45 @@ static int common_tail_bytes(const uint8_t* a, int na, const uint8_t* b, int nb)
     return k;
 }
 
-/* Encodes the y then z symbols into `ecp` sub-streams and merges them.  Returns the number of
- * bytes written, -1 on a capacity problem, -2 on bad arguments. */
-int oracle_encode(const int32_t* cdf_z, const int32_t* len_z, int z_stride, const int32_t* cdf_y,
-                  const int32_t* len_y, int y_stride, const int16_t* y_sym, int n_y,
-                  const int8_t* z_sym, int n_z, int z_cdf_offset, int z_ch, int ecp, uint8_t* out,
-                  int out_cap)
+/* Encodes `n_seg` y segments (concatenated in y_sym, lengths y_counts, in coding order) then the
+ * z symbols into `ecp` sub-streams and merges them.  Every segment is split evenly over the
+ * sub-streams and each sub-stream codes its slices back to front, segment after segment (one
+ * encode_y call per segment, py_rans.cpp:104-135).  Returns the number of bytes written, -1 on
+ * a capacity problem, -2 on bad arguments. */
+int oracle_encode_segments(const int32_t* cdf_z, const int32_t* len_z, int z_stride,
+                           const int32_t* cdf_y, const int32_t* len_y, int y_stride,
+                           const int16_t* y_sym, const int* y_counts, int n_seg,
+                           const int8_t* z_sym, int n_z, int z_cdf_offset, int z_ch, int ecp,
+                           uint8_t* out, int out_cap)
 {
-    if (ecp < 1 || ecp > 8 || z_ch < 1) return -2;
+    if (ecp < 1 || ecp > 8 || z_ch < 1 || n_seg < 0) return -2;
+    int n_y = 0;
+    for (int g = 0; g < n_seg; g++) {
+        if (y_counts[g] < 0) return -2;
+        n_y += y_counts[g];
+    }
     enc_t e[8];
     int rc = 0;
     for (int i = 0; i < ecp; i++) {
-        int ny_i = (i < ecp - 1) ? n_y / ecp : n_y - (n_y / ecp) * (ecp - 1);
-        int nz_i = (i < ecp - 1) ? n_z / ecp : n_z - (n_z / ecp) * (ecp - 1);
-        e[i].cap = (ny_i + nz_i) * 4 + 4;
+        e[i].cap = (n_y / ecp + 8 * n_seg + n_z / ecp + 8) * 4 + 4;
         e[i].buf = (uint8_t*)malloc((size_t)e[i].cap + 1);
         e[i].pos = e[i].cap;
         e[i].x = RANS_L;
     }
     for (int i = 0; i < ecp && rc == 0; i++) {
-        int sy = n_y / ecp;
-        int y0 = sy * i;
-        int y1 = (i < ecp - 1) ? y0 + sy : n_y;
-        for (int k = y1 - 1; k >= y0 && rc == 0; k--) {
-            int16_t c = y_sym[k];
-            int idx = c & 0xff;
-            int32_t s = (int8_t)(c >> 8);
-            rc = enc_symbol(&e[i], s, cdf_y + (size_t)idx * y_stride, len_y[idx] - 2);
+        const int16_t* seg = y_sym;
+        for (int g = 0; g < n_seg && rc == 0; g++) {
+            int ng = y_counts[g];
+            int sy = ng / ecp;
+            int y0 = sy * i;
+            int y1 = (i < ecp - 1) ? y0 + sy : ng;
+            for (int k = y1 - 1; k >= y0 && rc == 0; k--) {
+                int16_t c = seg[k];
+                int idx = c & 0xff;
+                int32_t s = (int8_t)(c >> 8);
+                rc = enc_symbol(&e[i], s, cdf_y + (size_t)idx * y_stride, len_y[idx] - 2);
+            }
+            seg += ng;
         }
         int sz = n_z / ecp;
         int z0 = sz * i;
@@ -316,27 +319,53 @@ int oracle_encode(const int32_t* cdf_z, const int32_t* len_z, int z_stride, cons
     return total;
 }
 
-/* Decodes z then y from a container made by oracle_encode.  Returns 0, -2 on bad arguments,
- * -3 if a sub-stream ran past its bytes. */
-int oracle_decode(const int32_t* cdf_z, const int32_t* len_z, int z_stride, const int32_t* cdf_y,
-                  const int32_t* len_y, int y_stride, const uint8_t* stream, int size,
-                  const uint8_t* y_idx, int n_y, int n_z, int z_cdf_offset, int z_ch, int ecp,
-                  int8_t* y_out, int8_t* z_out)
+/* One y segment then z (the video model's payload). */
+int oracle_encode(const int32_t* cdf_z, const int32_t* len_z, int z_stride, const int32_t* cdf_y,
+                  const int32_t* len_y, int y_stride, const int16_t* y_sym, int n_y,
+                  const int8_t* z_sym, int n_z, int z_cdf_offset, int z_ch, int ecp, uint8_t* out,
+                  int out_cap)
 {
-    if (ecp < 1 || ecp > 8 || z_ch < 1) return -2;
+    return oracle_encode_segments(cdf_z, len_z, z_stride, cdf_y, len_y, y_stride, y_sym, &n_y, 1,
+                                  z_sym, n_z, z_cdf_offset, z_ch, ecp, out, out_cap);
+}
+
+/* Incremental decoder over one container: split once (py_rans.cpp:412-492), then segments are
+ * decoded in the reverse order of encoding, each split evenly over the sub-streams. */
+typedef struct {
+    int ecp;
     uint8_t* part[8];
     int psz[8];
-    memset(part, 0, sizeof(part));
+    dec_t d[8];
+} odec_t;
+
+void oracle_dec_close(void* h)
+{
+    odec_t* o = (odec_t*)h;
+    if (o == NULL) return;
+    for (int i = 0; i < 8; i++) free(o->part[i]);
+    free(o);
+}
+
+/* NULL on a malformed container or bad arguments. */
+void* oracle_dec_open(const uint8_t* stream, int size, int ecp)
+{
+    if (ecp < 1 || ecp > 8 || size < 0) return NULL;
+    odec_t* o = (odec_t*)calloc(1, sizeof(odec_t));
+    if (o == NULL) return NULL;
+    o->ecp = ecp;
     if (ecp == 1) {
-        part[0] = (uint8_t*)malloc((size_t)size + 1);
-        memcpy(part[0], stream, (size_t)size);
-        psz[0] = size;
+        o->part[0] = (uint8_t*)malloc((size_t)size + 1);
+        memcpy(o->part[0], stream, (size_t)size);
+        o->psz[0] = size;
     } else {
         int pairs = ecp / 2;
         int tail = ecp % 2;
         int noff = pairs - 1 + tail;
         int off[4];
-        if (size < noff * 4) return -2;
+        if (size < noff * 4) {
+            oracle_dec_close(o);
+            return NULL;
+        }
         for (int k = 0; k < noff; k++) memcpy(&off[k], stream + 4 * k, 4);
         const uint8_t* pay = stream + noff * 4;
         int pay_n = size - noff * 4;
@@ -347,48 +376,81 @@ int oracle_decode(const int32_t* cdf_z, const int32_t* len_z, int z_stride, cons
             else g1 = tail ? off[noff - 1] : pay_n;
             if (noff == 0) g1 = pay_n;
             if (g0 < 0 || g1 > pay_n || g1 < g0) {
-                for (int i = 0; i < ecp; i++) free(part[i]);
-                return -2;
+                oracle_dec_close(o);
+                return NULL;
             }
             int gs = g1 - g0;
-            part[2 * p] = (uint8_t*)malloc((size_t)gs + 1);
-            part[2 * p + 1] = (uint8_t*)malloc((size_t)gs + 1);
-            memcpy(part[2 * p], pay + g0, (size_t)gs);
-            for (int j = 0; j < gs; j++) part[2 * p + 1][j] = pay[g1 - 1 - j];
-            psz[2 * p] = psz[2 * p + 1] = gs;
+            o->part[2 * p] = (uint8_t*)malloc((size_t)gs + 1);
+            o->part[2 * p + 1] = (uint8_t*)malloc((size_t)gs + 1);
+            memcpy(o->part[2 * p], pay + g0, (size_t)gs);
+            for (int j = 0; j < gs; j++) o->part[2 * p + 1][j] = pay[g1 - 1 - j];
+            o->psz[2 * p] = o->psz[2 * p + 1] = gs;
         }
         if (tail) {
             int t0 = off[noff - 1];
             int ts = pay_n - t0;
             if (t0 < 0 || ts < 0) {
-                for (int i = 0; i < ecp; i++) free(part[i]);
-                return -2;
+                oracle_dec_close(o);
+                return NULL;
             }
-            part[ecp - 1] = (uint8_t*)malloc((size_t)ts + 1);
-            memcpy(part[ecp - 1], pay + t0, (size_t)ts);
-            psz[ecp - 1] = ts;
+            o->part[ecp - 1] = (uint8_t*)malloc((size_t)ts + 1);
+            memcpy(o->part[ecp - 1], pay + t0, (size_t)ts);
+            o->psz[ecp - 1] = ts;
         }
     }
+    for (int i = 0; i < ecp; i++) dec_init(&o->d[i], o->part[i], o->psz[i]);
+    return o;
+}
+
+/* 0, or -3 if a sub-stream ran past its bytes. */
+int oracle_dec_z(void* h, const int32_t* cdf_z, const int32_t* len_z, int z_stride, int n_z,
+                 int z_cdf_offset, int z_ch, int8_t* z_out)
+{
+    odec_t* o = (odec_t*)h;
     int rc = 0;
-    for (int i = 0; i < ecp; i++) {
-        dec_t d;
-        dec_init(&d, part[i], psz[i]);
-        int sz = n_z / ecp;
+    for (int i = 0; i < o->ecp; i++) {
+        int sz = n_z / o->ecp;
         int z0 = sz * i;
-        int z1 = (i < ecp - 1) ? z0 + sz : n_z;
+        int z1 = (i < o->ecp - 1) ? z0 + sz : n_z;
         for (int k = z0; k < z1; k++) {
             int t = (k % z_ch) + z_cdf_offset;
-            z_out[k] = dec_symbol(&d, cdf_z + (size_t)t * z_stride, len_z[t] - 2);
+            z_out[k] = dec_symbol(&o->d[i], cdf_z + (size_t)t * z_stride, len_z[t] - 2);
         }
-        int sy = n_y / ecp;
+        if (o->d[i].overrun) rc = -3;
+    }
+    return rc;
+}
+
+int oracle_dec_y(void* h, const int32_t* cdf_y, const int32_t* len_y, int y_stride,
+                 const uint8_t* y_idx, int n_y, int8_t* y_out)
+{
+    odec_t* o = (odec_t*)h;
+    int rc = 0;
+    for (int i = 0; i < o->ecp; i++) {
+        int sy = n_y / o->ecp;
         int y0 = sy * i;
-        int y1 = (i < ecp - 1) ? y0 + sy : n_y;
+        int y1 = (i < o->ecp - 1) ? y0 + sy : n_y;
         for (int k = y0; k < y1; k++) {
             int idx = y_idx[k];
-            y_out[k] = dec_symbol(&d, cdf_y + (size_t)idx * y_stride, len_y[idx] - 2);
+            y_out[k] = dec_symbol(&o->d[i], cdf_y + (size_t)idx * y_stride, len_y[idx] - 2);
         }
-        if (d.overrun) rc = -3;
+        if (o->d[i].overrun) rc = -3;
     }
-    for (int i = 0; i < ecp; i++) free(part[i]);
     return rc;
+}
+
+/* Decodes z then y from a container made by oracle_encode.  Returns 0, -2 on bad arguments,
+ * -3 if a sub-stream ran past its bytes. */
+int oracle_decode(const int32_t* cdf_z, const int32_t* len_z, int z_stride, const int32_t* cdf_y,
+                  const int32_t* len_y, int y_stride, const uint8_t* stream, int size,
+                  const uint8_t* y_idx, int n_y, int n_z, int z_cdf_offset, int z_ch, int ecp,
+                  int8_t* y_out, int8_t* z_out)
+{
+    if (z_ch < 1) return -2;
+    void* h = oracle_dec_open(stream, size, ecp);
+    if (h == NULL) return -2;
+    int rc = oracle_dec_z(h, cdf_z, len_z, z_stride, n_z, z_cdf_offset, z_ch, z_out);
+    int rc2 = oracle_dec_y(h, cdf_y, len_y, y_stride, y_idx, n_y, y_out);
+    oracle_dec_close(h);
+    return rc != 0 ? rc : rc2;
 }

@@ -10,6 +10,9 @@
 //           (src/layers/extensions/inference/dmc_hts_proxy.cpp:778-793)
 //   decode: set_entropy_coder_parallel, set_stream, decode_z, get_decoded_tensor_cpp,
 //           decode_y, get_decoded_tensor_cpp (dmc_hts_proxy.cpp:794-823)
+// and the intra worker: encode_y once per mask step (steps 3, 2, 1, 0), then encode_z
+// (dmci_proxy.cpp:818-846); decode_z, then one decode_y per step in step order
+// (dmci_proxy.cpp:846-870).
 #include "py_rans.h"
 
 #include <cstring>
@@ -84,5 +87,67 @@ int ref_decode(const int32_t* cdf_z, const int32_t* len_z, int n_z_cdf, int z_st
     std::memcpy(y_out, y->data(), n_y);
     return 0;
 }
+
+// Several y segments (lengths y_counts, concatenated in y_sym in coding order), then z.
+int ref_encode_segments(const int32_t* cdf_z, const int32_t* len_z, int n_z_cdf, int z_stride,
+                        const int32_t* cdf_y, const int32_t* len_y, int n_y_cdf, int y_stride,
+                        const int16_t* y_sym, const int* y_counts, int n_seg, const int8_t* z_sym,
+                        int n_z, int z_cdf_offset, int z_ch, int ec_parallel, uint8_t* out,
+                        int out_cap)
+{
+    RansEncoder enc;
+    enc.set_cdf(to_vec(cdf_z, n_z_cdf * z_stride), to_vec(len_z, n_z_cdf), 0);
+    enc.set_cdf(to_vec(cdf_y, n_y_cdf * y_stride), to_vec(len_y, n_y_cdf), 1);
+    enc.reset();
+    enc.set_entropy_coder_parallel(ec_parallel);
+    for (int g = 0; g < n_seg; ++g) {
+        enc.encode_y(to_vec(y_sym, y_counts[g]), y_counts[g]);
+        y_sym += y_counts[g];
+    }
+    enc.encode_z(to_vec(z_sym, n_z), z_cdf_offset, z_ch);
+    enc.flush();
+    py::array_t<uint8_t> s = enc.get_encoded_stream();
+    const int n = static_cast<int>(s.size());
+    if (n > out_cap) {
+        return -1;
+    }
+    std::memcpy(out, s.data(), n);
+    return n;
+}
+
+// Incremental decoding: open, decode_z, decode_y (any number of times), close.
+void* ref_dec_open(const int32_t* cdf_z, const int32_t* len_z, int n_z_cdf, int z_stride,
+                   const int32_t* cdf_y, const int32_t* len_y, int n_y_cdf, int y_stride,
+                   const uint8_t* stream, int stream_size, int ec_parallel)
+{
+    auto* dec = new RansDecoder();
+    dec->set_cdf(to_vec(cdf_z, n_z_cdf * z_stride), to_vec(len_z, n_z_cdf), 0);
+    dec->set_cdf(to_vec(cdf_y, n_y_cdf * y_stride), to_vec(len_y, n_y_cdf), 1);
+    dec->set_entropy_coder_parallel(ec_parallel);
+    dec->set_stream(stream, stream_size);
+    return dec;
+}
+
+int ref_dec_z(void* h, int n_z, int z_cdf_offset, int z_ch, int8_t* z_out)
+{
+    auto* dec = static_cast<RansDecoder*>(h);
+    dec->decode_z(n_z, z_cdf_offset, z_ch);
+    auto z = dec->get_decoded_tensor_cpp();
+    std::memcpy(z_out, z->data(), n_z);
+    return 0;
+}
+
+int ref_dec_y(void* h, const uint8_t* y_idx, int n_y, int8_t* y_out)
+{
+    auto* dec = static_cast<RansDecoder*>(h);
+    dec->decode_y(to_vec(y_idx, n_y), n_y);
+    auto y = dec->get_decoded_tensor_cpp();
+    if (n_y > 0) {
+        std::memcpy(y_out, y->data(), n_y);
+    }
+    return 0;
+}
+
+void ref_dec_close(void* h) { delete static_cast<RansDecoder*>(h); }
 
 }  // extern "C"

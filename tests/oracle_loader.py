@@ -1,5 +1,5 @@
 """Loads the oracle (test infrastructure): oracle/liboracle.so, built from oracle/rans_oracle.c
-by oracle/Makefile (gcc).  Built on first use if missing."""
+by oracle/Makefile (gcc).  Built on first use if missing or older than its source."""
 import ctypes
 import os
 import subprocess
@@ -12,7 +12,8 @@ _lib = None
 def oracle_lib():
     global _lib
     if _lib is None:
-        if not os.path.exists(ORACLE_SO):
+        src = os.path.join(ROOT, "oracle", "rans_oracle.c")
+        if not os.path.exists(ORACLE_SO) or os.path.getmtime(ORACLE_SO) < os.path.getmtime(src):
             subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), ORACLE_SO], check=True,
                            capture_output=True)
         _lib = ctypes.CDLL(ORACLE_SO)
