@@ -1,13 +1,10 @@
 // extern "C" entry points of the HT-S codec runtime (declared in include/dcvc_b200.h).
+#include "capi_state_dict.h"
 #include "errors.h"
 #include "hts_codec.h"
 
 #include "../../include/dcvc_b200.h"
 
-#include <cuda_bf16.h>
-#include <cuda_fp16.h>
-
-#include <cstring>
 #include <exception>
 
 using namespace dcvc;
@@ -23,48 +20,6 @@ int fail(int status, const std::string& msg)
 {
     set_last_error(msg);
     return status;
-}
-
-size_t dtype_size(int dt)
-{
-    switch (dt) {
-    case DCVC_F16:
-    case DCVC_BF16: return 2;
-    case DCVC_F32:
-    case DCVC_I32: return 4;
-    case DCVC_I64: return 8;
-    default: return 0;
-    }
-}
-
-bool to_float(int dt, const void* src, size_t n, std::vector<float>* out)
-{
-    out->resize(n);
-    float* o = out->data();
-    switch (dt) {
-    case DCVC_F16: {
-        const __half* s = static_cast<const __half*>(src);
-        for (size_t i = 0; i < n; ++i) o[i] = __half2float(s[i]);
-        return true;
-    }
-    case DCVC_BF16: {
-        const __nv_bfloat16* s = static_cast<const __nv_bfloat16*>(src);
-        for (size_t i = 0; i < n; ++i) o[i] = __bfloat162float(s[i]);
-        return true;
-    }
-    case DCVC_F32: std::memcpy(o, src, n * 4); return true;
-    case DCVC_I32: {
-        const int32_t* s = static_cast<const int32_t*>(src);
-        for (size_t i = 0; i < n; ++i) o[i] = static_cast<float>(s[i]);
-        return true;
-    }
-    case DCVC_I64: {
-        const int64_t* s = static_cast<const int64_t*>(src);
-        for (size_t i = 0; i < n; ++i) o[i] = static_cast<float>(s[i]);
-        return true;
-    }
-    default: return false;
-    }
 }
 
 }  // namespace
@@ -97,41 +52,14 @@ int dcvc_hts_set_param(void* handle, int n, const char* const* names, const void
                        const int64_t* shapes, const int* ndims, const int* dtypes,
                        const int* on_device, float skip_threshold)
 {
-    if (handle == nullptr || n <= 0 || names == nullptr || data == nullptr || shapes == nullptr ||
-        ndims == nullptr || dtypes == nullptr || on_device == nullptr) {
-        return fail(kInvalidArgument, "dcvc_hts_set_param: null argument");
+    if (handle == nullptr) {
+        return fail(kInvalidArgument, "dcvc_hts_set_param: null handle");
     }
     StateDict sd;
-    std::vector<uint8_t> host;
-    try {
-        for (int i = 0; i < n; ++i) {
-            if (names[i] == nullptr || ndims[i] < 0 || ndims[i] > 4 || dtype_size(dtypes[i]) == 0) {
-                return fail(kInvalidArgument, "dcvc_hts_set_param: bad entry " + std::to_string(i));
-            }
-            HostTensor t;
-            size_t numel = 1;
-            for (int d = 0; d < ndims[i]; ++d) {
-                t.shape.push_back(shapes[4 * i + d]);
-                numel *= static_cast<size_t>(shapes[4 * i + d]);
-            }
-            const size_t bytes = numel * dtype_size(dtypes[i]);
-            const void* src = data[i];
-            if (on_device[i] && numel > 0) {
-                host.resize(bytes);
-                cudaError_t e = cudaMemcpy(host.data(), data[i], bytes, cudaMemcpyDeviceToHost);
-                if (e != cudaSuccess) {
-                    return cuda_status(e, "dcvc_hts_set_param: reading a device tensor");
-                }
-                src = host.data();
-            }
-            if (numel > 0 && src == nullptr) {
-                return fail(kInvalidArgument, std::string("dcvc_hts_set_param: null data for ") + names[i]);
-            }
-            to_float(dtypes[i], src, numel, &t.data);
-            sd[names[i]] = std::move(t);
-        }
-    } catch (const std::exception& e) {
-        return fail(kOutOfMemory, std::string("dcvc_hts_set_param: ") + e.what());
+    const int st = build_state_dict(n, names, data, shapes, ndims, dtypes, on_device, &sd,
+                                    "dcvc_hts_set_param");
+    if (st != kOk) {
+        return st;
     }
     return static_cast<HtsHandle*>(handle)->codec.set_param(sd, skip_threshold);
 }

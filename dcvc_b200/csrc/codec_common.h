@@ -1,0 +1,46 @@
+// Pieces shared by the codec runtimes (the HT-S video codec and the intra codec): per-phase CUDA
+// graphs, CDF-table loading from a state dict and the device error word check.  They play the
+// part of the reference's DMCCommon (src/layers/extensions/inference/dmc_common.cpp:10-134).
+#pragma once
+
+#include "net.h"
+#include "rans_coder.h"
+
+#include <cuda_runtime.h>
+
+#include <functional>
+#include <vector>
+
+namespace dcvc {
+
+// One CUDA graph per phase slot.  The first run of a slot is eager (it initialises every
+// kernel's attributes and validates the launches), the second is captured into a graph, later
+// runs replay it (DMCCommon::run / capture_cuda_graph, dmc_common.cpp:85-134).
+class PhaseGraphs {
+public:
+    explicit PhaseGraphs(int slots) : slots_(slots) {}
+    PhaseGraphs(const PhaseGraphs&) = delete;
+    PhaseGraphs& operator=(const PhaseGraphs&) = delete;
+    ~PhaseGraphs() { clear(); }
+    void clear();
+    // Enqueues phase `slot` on s; adds the phase's kernel count to *kernels.
+    int run(int slot, cudaStream_t s, int* err_word, const std::function<void(Launch&)>& body,
+            int* kernels);
+
+private:
+    struct Slot {
+        cudaGraphExec_t exec = nullptr;
+        bool ran_eager = false;
+        int kernels = 0;
+    };
+    std::vector<Slot> slots_;
+};
+
+// Loads "bit_estimator_z.{quantized_cdf,cdf_length}" (table set 0) and
+// "gaussian_encoder.{quantized_cdf,cdf_length}" (table set 1) and checks their counts.
+int load_cdf_tables(const StateDict& sd, RansTables* tables, int z_count, int y_count);
+
+// Reads (and clears) the device error word; kDeviceTimeout if a kernel's bounded wait gave up.
+int check_device_error_word(int* err_word, const char* where);
+
+}  // namespace dcvc

@@ -280,7 +280,7 @@ __global__ void quantize_phase_kernel(int phase, const __half* __restrict__ y, i
             pq = ld8(y_q + m * ldq + v * 8);
             ph = ld8(y_hat + m * ldh + v * 8);
         }
-        if (MODE == 2) {
+        if (MODE >= 2) {
             qd = ld8(q_dec + m * ldd + v * 8);
         }
 #pragma unroll
@@ -301,6 +301,8 @@ __global__ void quantize_phase_kernel(int phase, const __half* __restrict__ y, i
                 yh = hadd(yh, ph.v[j]);
                 if (MODE == 2) {
                     yh = hmul(yh, __hmax(qd.v[j], half_));
+                } else if (MODE == 3) {
+                    yh = hmul(yh, qd.v[j]);
                 }
                 oh.v[j] = yh;
             }
@@ -395,6 +397,120 @@ __global__ void build_index_kernel(const __half* __restrict__ y_q, int ldq,
                 make_uint2(ix[0] | (ix[1] << 8) | (ix[2] << 16) | (ix[3] << 24),
                            ix[4] | (ix[5] << 8) | (ix[6] << 16) | (ix[7] << 24));
         }
+    }
+}
+
+// The active quarter of the channels at each 2x2 position in mask phase `phase`.
+__device__ __forceinline__ int active_quarter(int phase, int h, int w)
+{
+    return ((h & 1) * 2 + (w & 1)) ^ mask_position(phase, 0);
+}
+
+// build_index_enc/dec over the active quarter of a mask phase (single_part_for_writing_4x /
+// single_part_for_reading_4x + build_index_*, stream.cu:89-173, 896-962): for every pixel m and
+// channel c of the quarter-width part (C/4 channels), scale = the masked quarters summed in FP16,
+// ((s0*m0 + s1*m1) + s2*m2) + s3*m3, and y_q = the active quarter's value (the other quarters
+// of the running y_q hold zeros at this pixel); output in NHWC order of the part (m * C/4 + c).
+template <bool ENC>
+__global__ void build_index_4x_kernel(int phase, const __half* __restrict__ y_q, int ldq,
+                                      const __half* __restrict__ scales, int lds, __half thr,
+                                      const uint8_t* __restrict__ lut, int H, int W, int C,
+                                      int16_t* __restrict__ sym, uint8_t* __restrict__ idx_out,
+                                      uint8_t* __restrict__ cond)
+{
+    griddep_launch_dependents();
+    griddep_wait();
+    const int Cq = C / 4;
+    const int vecs = Cq / 8;
+    const long long total = static_cast<long long>(H) * W * vecs;
+    const __half one = __float2half_rn(1.f);
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const long long m = i / vecs;
+        const int v = static_cast<int>(i - m * vecs);
+        const int h = static_cast<int>(m / W);
+        const int w = static_cast<int>(m - static_cast<long long>(h) * W);
+        const int qa = active_quarter(phase, h, w);
+        Vec8h ss[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            ss[q] = ld8(scales + m * lds + q * Cq + v * 8);
+        }
+        const long long n = m * Cq + v * 8;
+        uint8_t cnd[8];
+        uint8_t ix[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            __half acc = hmul(ss[0].v[j], qa == 0 ? one : hzero());
+#pragma unroll
+            for (int q = 1; q < 4; ++q) {
+                acc = hadd(acc, hmul(ss[q].v[j], qa == q ? one : hzero()));
+            }
+            ix[j] = __ldg(lut + __half_as_ushort(acc));
+            cnd[j] = __hgt(acc, thr) ? 1 : 0;
+        }
+        *reinterpret_cast<uint2*>(cond + n) =
+            make_uint2(cnd[0] | (cnd[1] << 8) | (cnd[2] << 16) | (cnd[3] << 24),
+                       cnd[4] | (cnd[5] << 8) | (cnd[6] << 16) | (cnd[7] << 24));
+        if (ENC) {
+            const Vec8h qq = ld8(y_q + m * ldq + qa * Cq + v * 8);
+            int16_t o[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int qv = __half2int_rd(qq.v[j]);
+                o[j] = static_cast<int16_t>(qv * 256 + ix[j]);
+            }
+            *reinterpret_cast<uint4*>(sym + n) = *reinterpret_cast<uint4*>(o);
+        } else {
+            *reinterpret_cast<uint2*>(idx_out + n) =
+                make_uint2(ix[0] | (ix[1] << 8) | (ix[2] << 16) | (ix[3] << 24),
+                           ix[4] | (ix[5] << 8) | (ix[6] << 16) | (ix[7] << 24));
+        }
+    }
+}
+
+// restore_y_4x[_and_add_inplace] / restore_y_4x_add_and_multiply_broadcast (stream.cu:757-860):
+// t = part[m, c % (C/4)] + means[m, c] on the phase's active quarter, 0 elsewhere;
+// MODE 0: y_hat = t; 1: y_hat = y_hat + t; 3: y_hat = (y_hat + t) * q[c].
+template <int MODE>
+__global__ void restore_4x_kernel(int phase, const __half* __restrict__ part,
+                                  const __half* __restrict__ means, int ldm,
+                                  const __half* __restrict__ q, __half* __restrict__ y_hat, int ldh,
+                                  int H, int W, int C)
+{
+    griddep_launch_dependents();
+    griddep_wait();
+    const int vecs = C / 8;
+    const int quarter_vecs = vecs / 4;
+    const long long total = static_cast<long long>(H) * W * vecs;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const long long m = i / vecs;
+        const int v = static_cast<int>(i - m * vecs);
+        const int h = static_cast<int>(m / W);
+        const int w = static_cast<int>(m - static_cast<long long>(h) * W);
+        const bool on = ((h & 1) * 2 + (w & 1)) == mask_position(phase, v / quarter_vecs);
+        const Vec8h pp = ld8(part + m * (C / 4) + (v % quarter_vecs) * 8);
+        const Vec8h mm = ld8(means + m * ldm + v * 8);
+        Vec8h prev, qd, o;
+        if (MODE >= 1) {
+            prev = ld8(y_hat + m * ldh + v * 8);
+        }
+        if (MODE == 3) {
+            qd = ld8(q + v * 8);
+        }
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            __half t = on ? hadd(pp.v[j], mm.v[j]) : hzero();
+            if (MODE >= 1) {
+                t = hadd(prev.v[j], t);
+            }
+            if (MODE == 3) {
+                t = hmul(t, qd.v[j]);
+            }
+            o.v[j] = t;
+        }
+        st8(y_hat + m * ldh + v * 8, o);
     }
 }
 
@@ -764,12 +880,15 @@ cudaError_t launch_quantize_phase(int phase, int mode, const __half* y, int ldy,
                                   int ldq, __half* y_hat, int ldh, int H, int W, int C,
                                   cudaStream_t s)
 {
-    if (phase < 0 || phase > 3 || C % 32 || (mode == 2 && q_dec == nullptr) || mode < 0 ||
-        mode > 2) {
+    if (phase < 0 || phase > 3 || C % 32 || (mode >= 2 && q_dec == nullptr) || mode < 0 ||
+        mode > 3) {
         return cudaErrorInvalidValue;
     }
     const int g = grid_for(static_cast<long long>(H) * W * (C / 8));
-    if (mode == 0) {
+    if (mode == 3) {
+        launch_pdl(quantize_phase_kernel<3>, dim3(g), dim3(kThreads), 0, s, phase, y, ldy, scales,
+                   lds, means, ldm, q_dec, ldd, thr, y_q, ldq, y_hat, ldh, H, W, C);
+    } else if (mode == 0) {
         launch_pdl(quantize_phase_kernel<0>, dim3(g), dim3(kThreads), 0, s, phase, y, ldy, scales, lds, means, ldm,
                                                         q_dec, ldd, thr, y_q, ldq, y_hat, ldh, H,
                                                         W, C);
@@ -828,6 +947,57 @@ cudaError_t launch_build_index_dec(const __half* scales, int lds, __half thr,
     }
     launch_pdl(build_index_kernel<false>, dim3(grid_for(static_cast<long long>(M) * (C / 8))), dim3(kThreads), 0, s, 
         nullptr, 0, scales, lds, thr, lut, M, C, nullptr, idx, cond);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_build_index_enc_4x(int phase, const __half* y_q, int ldq,
+                                      const __half* scales, int lds, __half thr,
+                                      const uint8_t* lut, int H, int W, int C, int16_t* sym,
+                                      uint8_t* cond, cudaStream_t s)
+{
+    if (phase < 0 || phase > 3 || C % 32 || ldq % 8 || lds % 8 || !al16(sym) ||
+        (reinterpret_cast<uintptr_t>(cond) & 7)) {
+        return cudaErrorInvalidValue;
+    }
+    launch_pdl(build_index_4x_kernel<true>, dim3(grid_for(static_cast<long long>(H) * W * (C / 32))),
+               dim3(kThreads), 0, s, phase, y_q, ldq, scales, lds, thr, lut, H, W, C, sym, nullptr,
+               cond);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_build_index_dec_4x(int phase, const __half* scales, int lds, __half thr,
+                                      const uint8_t* lut, int H, int W, int C, uint8_t* idx,
+                                      uint8_t* cond, cudaStream_t s)
+{
+    if (phase < 0 || phase > 3 || C % 32 || lds % 8 || (reinterpret_cast<uintptr_t>(idx) & 7) ||
+        (reinterpret_cast<uintptr_t>(cond) & 7)) {
+        return cudaErrorInvalidValue;
+    }
+    launch_pdl(build_index_4x_kernel<false>, dim3(grid_for(static_cast<long long>(H) * W * (C / 32))),
+               dim3(kThreads), 0, s, phase, nullptr, 0, scales, lds, thr, lut, H, W, C, nullptr,
+               idx, cond);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_restore_4x(int phase, int mode, const __half* part, const __half* means,
+                              int ldm, const __half* q, __half* y_hat, int ldh, int H, int W,
+                              int C, cudaStream_t s)
+{
+    if (phase < 0 || phase > 3 || C % 32 || ldm % 8 || ldh % 8 || !al16(part) ||
+        (mode != 0 && mode != 1 && mode != 3) || (mode == 3 && q == nullptr)) {
+        return cudaErrorInvalidValue;
+    }
+    const int g = grid_for(static_cast<long long>(H) * W * (C / 8));
+    if (mode == 0) {
+        launch_pdl(restore_4x_kernel<0>, dim3(g), dim3(kThreads), 0, s, phase, part, means, ldm, q,
+                   y_hat, ldh, H, W, C);
+    } else if (mode == 1) {
+        launch_pdl(restore_4x_kernel<1>, dim3(g), dim3(kThreads), 0, s, phase, part, means, ldm, q,
+                   y_hat, ldh, H, W, C);
+    } else {
+        launch_pdl(restore_4x_kernel<3>, dim3(g), dim3(kThreads), 0, s, phase, part, means, ldm, q,
+                   y_hat, ldh, H, W, C);
+    }
     return cudaGetLastError();
 }
 

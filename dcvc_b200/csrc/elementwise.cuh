@@ -66,7 +66,8 @@ cudaError_t launch_div_clamp(__half* y, int M, int C, int ldy, const __half* q, 
 
 // process_with_mask_no_scale[_add_inplace][_add_and_multiply_inplace] (stream.cu:548-683) for
 // mask phase `phase` on an H x W grid.  mode 0: write y_q / y_hat; 1: accumulate;
-// 2: accumulate and scale y_hat by max(q_dec, 0.5).
+// 2: accumulate and scale y_hat by max(q_dec, 0.5); 3: accumulate and scale y_hat by q_dec
+// (add_and_multiply_broadcast, stream.cu:8-37: with ldd = 0, q_dec is one row of C scales).
 cudaError_t launch_quantize_phase(int phase, int mode, const __half* y, int ldy,
                                   const __half* scales, int lds, const __half* means, int ldm,
                                   const __half* q_dec, int ldd, __half thr, __half* y_q,
@@ -89,6 +90,23 @@ cudaError_t launch_build_index_enc(const __half* y_q, int ldq, const __half* sca
 cudaError_t launch_build_index_dec(const __half* scales, int lds, __half thr,
                                    const uint8_t* lut, int M, int C, uint8_t* idx, uint8_t* cond,
                                    cudaStream_t s);
+
+// The intra model's per-step index building over the active quarter of mask phase `phase`
+// (single_part_for_writing_4x / single_part_for_reading_4x + build_index_enc/dec,
+// stream.cu:89-173, 896-962): outputs [H*W, C/4] in NHWC order of the quarter-width part.
+cudaError_t launch_build_index_enc_4x(int phase, const __half* y_q, int ldq,
+                                      const __half* scales, int lds, __half thr,
+                                      const uint8_t* lut, int H, int W, int C, int16_t* sym,
+                                      uint8_t* cond, cudaStream_t s);
+cudaError_t launch_build_index_dec_4x(int phase, const __half* scales, int lds, __half thr,
+                                      const uint8_t* lut, int H, int W, int C, uint8_t* idx,
+                                      uint8_t* cond, cudaStream_t s);
+
+// restore_y_4x* (stream.cu:757-860): part is the dense [H*W, C/4] FP16 step values; mode 0
+// writes y_hat, 1 accumulates, 3 accumulates and multiplies by the C scales q.
+cudaError_t launch_restore_4x(int phase, int mode, const __half* part, const __half* means,
+                              int ldm, const __half* q, __half* y_hat, int ldh, int H, int W,
+                              int C, cudaStream_t s);
 
 // Order-preserving compaction of `src` (elem_bytes 1 or 2) under `cond` (conditional_index_part1,
 // stream.cu:175-338).  block_counts needs compact_blocks(n) ints; *total (device) receives the

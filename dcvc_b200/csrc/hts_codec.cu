@@ -58,18 +58,7 @@ HtsCodec::~HtsCodec()
     cudaStreamDestroy(copy_);
 }
 
-void HtsCodec::clear_graphs()
-{
-    for (auto& g : graphs_) {
-        if (g.exec != nullptr) {
-            cudaGraphExecDestroy(g.exec);
-            g.exec = nullptr;
-        }
-    }
-    for (auto& r : ran_eager_) {
-        r = false;
-    }
-}
+void HtsCodec::clear_graphs() { graphs_.clear(); }
 
 int HtsCodec::set_param(const StateDict& sd, float skip_threshold)
 {
@@ -148,35 +137,7 @@ int HtsCodec::set_param(const StateDict& sd, float skip_threshold)
         return kInvalidArgument;
     }
     // CDF tables (set_param, dmc_hts_proxy.cpp:748-761)
-    auto table = [&](const char* cdf_name, const char* len_name, int index) -> bool {
-        auto a = sd.find(cdf_name), b = sd.find(len_name);
-        if (a == sd.end() || b == sd.end() || a->second.shape.size() != 2) {
-            set_last_error(std::string("set_param: missing or malformed ") + cdf_name);
-            return false;
-        }
-        const int count = static_cast<int>(a->second.shape[0]);
-        const int stride = static_cast<int>(a->second.shape[1]);
-        if (b->second.numel() != count) {
-            set_last_error(std::string("set_param: ") + len_name + " does not match its table");
-            return false;
-        }
-        std::vector<int32_t> cdf(a->second.data.size()), len(count);
-        for (size_t i = 0; i < cdf.size(); ++i) cdf[i] = static_cast<int32_t>(a->second.data[i]);
-        for (int i = 0; i < count; ++i) len[i] = static_cast<int32_t>(b->second.data[i]);
-        std::string err;
-        if (!tables_.set(index, cdf.data(), len.data(), count, stride, &err)) {
-            set_last_error("set_param: " + err);
-            return false;
-        }
-        return true;
-    };
-    if (!table("bit_estimator_z.quantized_cdf", "bit_estimator_z.cdf_length", 0) ||
-        !table("gaussian_encoder.quantized_cdf", "gaussian_encoder.cdf_length", 1)) {
-        weights_.clear();
-        return kInvalidArgument;
-    }
-    if (tables_.z().count != kQpNum * kChZ || tables_.y().count != 128) {
-        set_last_error("set_param: expected 8192 bit-estimator tables and 128 Gaussian tables");
+    if (load_cdf_tables(sd, &tables_, kQpNum * kChZ, 128) != kOk) {
         weights_.clear();
         return kInvalidArgument;
     }
@@ -534,7 +495,7 @@ void HtsCodec::dec_synthesis(Launch& L)
 
 // ------------------------------------------------------------------------------ graphs
 
-int HtsCodec::record_phase(int slot, Launch& L)
+void HtsCodec::record_phase(int slot, Launch& L)
 {
     switch (slot) {
     case kEncAnalysis: enc_analysis(L); break;
@@ -545,74 +506,14 @@ int HtsCodec::record_phase(int slot, Launch& L)
     case kDecHyper: dec_hyper(L); break;
     case kDecContext: dec_context(L); break;
     case kDecSynthesis: dec_synthesis(L); break;
-    default: return kInternal;
+    default: break;
     }
-    return kOk;
 }
 
-// The first execution of a phase runs eagerly (and initialises every kernel's attributes); the
-// second captures it into a CUDA graph; later executions replay the graph.
 int HtsCodec::run_phase(int slot, cudaStream_t s)
 {
-    Graph& g = graphs_[slot];
-    if (g.exec != nullptr) {
-        last_kernels_ += phase_kernels_[slot];
-        return cuda_status(cudaGraphLaunch(g.exec, s), "cudaGraphLaunch");
-    }
-    Launch L{s, err_word_};
-    if (!ran_eager_[slot]) {
-        const int st = record_phase(slot, L);
-        if (st != kOk) {
-            return st;
-        }
-        ran_eager_[slot] = true;
-        phase_kernels_[slot] = L.kernels;
-        last_kernels_ += L.kernels;
-        if (L.first != cudaSuccess) {
-            return cuda_status(L.first, "phase launch");
-        }
-        return kOk;
-    }
-    cudaGraph_t graph = nullptr;
-    cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
-    if (e != cudaSuccess) {
-        return cuda_status(e, "cudaStreamBeginCapture");
-    }
-    record_phase(slot, L);
-    e = cudaStreamEndCapture(s, &graph);
-    if (L.first != cudaSuccess || e != cudaSuccess) {
-        if (graph != nullptr) {
-            cudaGraphDestroy(graph);
-        }
-        cudaGetLastError();
-        return cuda_status(L.first != cudaSuccess ? L.first : e, "graph capture");
-    }
-    e = cudaGraphInstantiate(&g.exec, graph, 0);
-    cudaGraphDestroy(graph);
-    if (e != cudaSuccess) {
-        g.exec = nullptr;
-        return cuda_status(e, "cudaGraphInstantiate");
-    }
-    last_kernels_ += phase_kernels_[slot];
-    return cuda_status(cudaGraphLaunch(g.exec, s), "cudaGraphLaunch");
-}
-
-int HtsCodec::check_device_error(const char* where)
-{
-    int code = 0;
-    if (err_word_ == nullptr) {
-        return kOk;
-    }
-    if (cudaMemcpy(&code, err_word_, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) {
-        return cuda_status(cudaGetLastError(), where);
-    }
-    if (code != 0) {
-        cudaMemset(err_word_, 0, sizeof(int));
-        set_last_error(std::string(where) + ": a kernel's bounded wait gave up (device error " +
-                       std::to_string(code) + ")");
-        return kDeviceTimeout;
-    }
-    return kOk;
+    return graphs_.run(slot, s, err_word_, [&](Launch& L) { record_phase(slot, L); },
+                       &last_kernels_);
 }
 
 int HtsCodec::buffer(const std::string& name, const void** ptr, int* rows, int* cols,
@@ -715,7 +616,7 @@ int HtsCodec::compress(const __half* x, int H, int W, int qp, bool reset, int pa
     if (cudaEventSynchronize(ev_phase_) != cudaSuccess) {
         return cuda_status(cudaGetLastError(), "compress: analysis");
     }
-    st = check_device_error("compress");
+    st = check_device_error_word(err_word_, "compress");
     if (st != kOk) {
         return st;
     }
@@ -788,7 +689,7 @@ int HtsCodec::decompress(const uint8_t* bytes, size_t n, int qp, int height, int
             st = cuda_status(cudaGetLastError(), "decompress: hyper prior");
         }
     }
-    if (st == kOk) st = check_device_error("decompress");
+    if (st == kOk) st = check_device_error_word(err_word_, "decompress");
     int count = 0;
     if (st == kOk) {
         count = *count_host_;

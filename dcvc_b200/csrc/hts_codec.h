@@ -2,6 +2,7 @@
 // (src/layers/extensions/inference/dmc_hts_proxy.{h,cpp}).
 #pragma once
 
+#include "codec_common.h"
 #include "net.h"
 #include "rans_coder.h"
 
@@ -48,9 +49,6 @@ public:
     int last_kernel_count() const { return last_kernels_; }
 
 private:
-    struct Graph {
-        cudaGraphExec_t exec = nullptr;
-    };
     enum Phase {
         kEncAnalysis = 0,    // enc_0 (dmc_hts_proxy.cpp:516-559)
         kEncUpdate = 1,      // enc_1 (2 variants: reset)
@@ -64,10 +62,7 @@ private:
     int allocate(int Hp, int Wp);
     void clear_graphs();
     int run_phase(int slot, cudaStream_t s);
-    int record_phase(int slot, Launch& L);
-    int count_kernels(cudaGraphExec_t) const;
-    int sync_into_main(cudaStream_t caller);
-    int check_device_error(const char* where);
+    void record_phase(int slot, Launch& L);
 
     // phase bodies (enqueue onto L.s)
     void enc_analysis(Launch& L);
@@ -149,9 +144,7 @@ private:
     int8_t* z_host_ = nullptr;
     bool memory_has_value_ = false;
 
-    Graph graphs_[kPhaseSlots];
-    bool ran_eager_[kPhaseSlots] = {false};
-    int phase_kernels_[kPhaseSlots] = {0};
+    PhaseGraphs graphs_{kPhaseSlots};
     cudaStream_t main_ = nullptr;   // compute stream (graphs run here)
     cudaStream_t copy_ = nullptr;   // D2H/H2D of symbols overlapping compute
     cudaEvent_t ev_in_ = nullptr, ev_phase_ = nullptr, ev_copy_ = nullptr, ev_out_ = nullptr;

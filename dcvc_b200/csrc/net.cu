@@ -107,9 +107,10 @@ Lin ParamBuilder::lin(const std::string& prefix, bool bias)
     return l;
 }
 
-Dcb ParamBuilder::dcb(const std::string& p)
+Dcb ParamBuilder::dcb(const std::string& p, bool shortcut)
 {
     Dcb d;
+    d.shortcut = shortcut;
     if (has(p + "adaptor.weight")) {
         d.adaptor = true;
         d.ad = lin(p + "adaptor.");
@@ -160,7 +161,7 @@ Dcb ParamBuilder::dcb(const std::string& p)
     return d;
 }
 
-DownBlock ParamBuilder::down(const std::string& p)
+DownBlock ParamBuilder::down(const std::string& p, bool shortcut)
 {
     DownBlock b;
     const HostTensor* w = get(p + "down.weight", 2);
@@ -185,15 +186,15 @@ DownBlock ParamBuilder::down(const std::string& p)
     b.down.cout = cout;
     b.down.w = upload_half(pw);
     b.down.b = upload_float(bias->data);
-    b.dcb = dcb(p + "conv.");
+    b.dcb = dcb(p + "conv.", shortcut);
     return b;
 }
 
-UpBlock ParamBuilder::up(const std::string& p)
+UpBlock ParamBuilder::up(const std::string& p, bool shortcut)
 {
     UpBlock b;
     b.up = subpel(p + "up.");
-    b.dcb = dcb(p + "conv.");
+    b.dcb = dcb(p + "conv.", shortcut);
     return b;
 }
 
@@ -260,7 +261,8 @@ Lin ParamBuilder::conv3x3s2(const std::string& p)
 // ------------------------------------------------------------------------------ execution
 
 void gemm(Launch& L, const Lin& lin, int epi, const __half* x, int ldx, int M, __half* out,
-          int ldo, const __half* res, int ldr, const __half* q, int sub_w)
+          int ldo, const __half* res, int ldr, const __half* q, int sub_w, const __half* res2,
+          int ldr2)
 {
     GemmParams p{};
     p.M = M;
@@ -269,6 +271,8 @@ void gemm(Launch& L, const Lin& lin, int epi, const __half* x, int ldx, int M, _
     p.bias = lin.b;
     p.res = res;
     p.ldr = ldr;
+    p.res2 = res2;
+    p.ldr2 = ldr2;
     p.qscale = q;
     p.out = out;
     p.ldo = ldo;
@@ -293,6 +297,11 @@ void run_dcb(Launch& L, const Dcb& d, const __half* x, int ldx, int H, int W, __
     L.note(launch_dwconv3x3(s.t1, H, W, d.cdc, d.cdc, d.dw, s.t2, d.cdc, L.s));
     gemm(L, d.dc2, kEpiBiasRes, s.t2, d.cdc, M, s.t3, d.C, xin, ldin);
     gemm(L, d.ffn1, kEpiQuad, s.t3, d.C, M, s.t4, d.cffn);
+    if (d.shortcut) {
+        // conv1x1_bias_shortcut2 (layers_proxy.cpp:89-91): ffn + ffn input + block input
+        gemm(L, d.ffn2, kEpiBiasRes2, s.t4, d.cffn, M, out, ldo, s.t3, d.C, nullptr, 0, xin, ldin);
+        return;
+    }
     if (q != nullptr) {
         gemm(L, d.ffn2, kEpiBiasResQ, s.t4, d.cffn, M, out, ldo, s.t3, d.C, q);
     } else {

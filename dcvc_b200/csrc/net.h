@@ -64,9 +64,11 @@ struct Dcb {
     Lin ffn1;                   // [4*cffn, C], rows 4c+k as in the reference
     Lin ffn2;
     int C = 0, cdc = 0, cffn = 0, cin = 0;
+    bool shortcut = false;      // out += block input (layers.py:155-158)
 };
 
-// ResidualBlockWithStride2: pixel_unshuffle(2) + 1x1 (K permuted to (dy, dx, c)) + DCB.
+// ResidualBlockWithStride2: pixel_unshuffle(2) + 1x1 (K permuted to (dy, dx, c)) + DCB (with the
+// block shortcut when the model keeps the reference's default, layers.py:176-188).
 struct DownBlock {
     Lin down;
     Dcb dcb;
@@ -84,9 +86,9 @@ public:
     ParamBuilder(const StateDict& sd, DeviceArena& arena) : sd_(sd), arena_(arena) {}
     bool has(const std::string& name) const { return sd_.count(name) != 0; }
     Lin lin(const std::string& prefix, bool bias = true);
-    Dcb dcb(const std::string& prefix);
-    DownBlock down(const std::string& prefix);
-    UpBlock up(const std::string& prefix);
+    Dcb dcb(const std::string& prefix, bool shortcut = false);
+    DownBlock down(const std::string& prefix, bool shortcut = false);
+    UpBlock up(const std::string& prefix, bool shortcut = false);
     Lin subpel(const std::string& prefix);  // prefix + "conv.0.weight", rows permuted
     Lin conv3x3s2(const std::string& prefix);  // weight K permuted to (ky, kx, c)
     const __half* half_rows(const std::string& name, int* rows, int* cols);
@@ -131,10 +133,10 @@ struct Launch {
 // out[M, cout] (pitch ldo) = epilogue(x[M, cin] (pitch ldx) . lin)
 void gemm(Launch& L, const Lin& lin, int epi, const __half* x, int ldx, int M, __half* out,
           int ldo, const __half* res = nullptr, int ldr = 0, const __half* q = nullptr,
-          int sub_w = 0);
+          int sub_w = 0, const __half* res2 = nullptr, int ldr2 = 0);
 
-// DepthConvBlockProxy::forward.  `out` may alias `x` when the block has no adaptor input wider
-// than its output (the last GEMM reads only its own scratch and residual).
+// DepthConvBlockProxy::forward (layers_proxy.cpp:71-101).  `out` may alias `x` unless the block
+// has a shortcut (its last GEMM then reads the block input as a second residual).
 void run_dcb(Launch& L, const Dcb& d, const __half* x, int ldx, int H, int W, __half* out, int ldo,
              Scratch& s, const __half* q = nullptr);
 

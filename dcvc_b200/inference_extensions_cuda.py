@@ -2,9 +2,10 @@
 inference/bind.cpp:11-39): the same proxy classes, methods, argument meaning and return values,
 backed by the sm_100a runtime in libdcvc_b200.so.
 
-DMCHTSProxy is implemented.  DMCIProxy, DMCHTLProxy and DMCLDProxy raise NotImplementedError on
-construction (the models then report that the CUDA implementation is unavailable, as the
-reference does when its extension is missing, video_model_ht.py:428-432).
+DMCHTSProxy (the HT-S video model) and DMCIProxy (the intra model) are implemented.  DMCHTLProxy
+and DMCLDProxy raise NotImplementedError on construction (the models then report that the CUDA
+implementation is unavailable, as the reference does when its extension is missing,
+video_model_ht.py:428-432).
 """
 import ctypes
 
@@ -40,6 +41,22 @@ _proto("dcvc_hts_buffer", [_vp, ctypes.c_char_p, ctypes.POINTER(_vp), ctypes.POI
                            ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)])
 _proto("dcvc_hts_stats", [_vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                           ctypes.POINTER(ctypes.c_size_t)])
+_proto("dcvc_intra_create", [ctypes.POINTER(_vp)])
+_proto("dcvc_intra_destroy", [_vp])
+_proto("dcvc_intra_set_param", [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_char_p),
+                                ctypes.POINTER(_vp), ctypes.POINTER(ctypes.c_int64),
+                                ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                ctypes.POINTER(ctypes.c_int), ctypes.c_float])
+_proto("dcvc_intra_compress", [_vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                               ctypes.c_int, _vp, ctypes.POINTER(_vp),
+                               ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_int),
+                               ctypes.POINTER(_vp)])
+_proto("dcvc_intra_decompress", [_vp, _vp, ctypes.c_size_t, ctypes.c_int, ctypes.c_int,
+                                 ctypes.c_int, ctypes.c_int, _vp, ctypes.POINTER(_vp)])
+_proto("dcvc_intra_buffer", [_vp, ctypes.c_char_p, ctypes.POINTER(_vp), ctypes.POINTER(ctypes.c_int),
+                             ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)])
+_proto("dcvc_intra_stats", [_vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                            ctypes.POINTER(ctypes.c_size_t)])
 
 _DTYPES = {torch.float16: 0, torch.bfloat16: 1, torch.float32: 2, torch.int32: 3, torch.int64: 4}
 FRAMES = 8
@@ -65,20 +82,31 @@ def _channels_last_data(t, name):
     return t
 
 
-class DMCHTSProxy:
-    """Chunk codec of the HT-S video model (dmc_hts_proxy.h:215-355).  One instance per stream;
-    not re-entrant."""
+def _bytes_out(data, size):
+    if size.value == 0:
+        return np.zeros(0, dtype=np.uint8)
+    return np.ctypeslib.as_array(ctypes.cast(data, ctypes.POINTER(ctypes.c_uint8)),
+                                 shape=(size.value,)).copy()
+
+
+class _Proxy:
+    """Handle lifetime, set_param, buffer and stats shared by the codec proxies; `_kind` selects
+    the dcvc_<kind>_* entry points."""
+
+    _kind = ""
 
     def __init__(self):
         h = _vp()
-        N.check(_lib.dcvc_hts_create(ctypes.byref(h)), "DMCHTSProxy()")
+        N.check(self._fn("create")(ctypes.byref(h)), f"{type(self).__name__}()")
         self._h = h
-        self._frames = None
+
+    def _fn(self, name):
+        return getattr(_lib, f"dcvc_{self._kind}_{name}")
 
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:
-            _lib.dcvc_hts_destroy(h)
+            self._fn("destroy")(h)
             self._h = None
 
     def set_param(self, state_dict, skip_threshold):
@@ -105,11 +133,35 @@ class DMCHTSProxy:
         n = len(names)
         if any(v.is_cuda for v in keep):
             torch.cuda.current_stream().synchronize()
-        N.check(_lib.dcvc_hts_set_param(
+        N.check(self._fn("set_param")(
             self._h, n, (ctypes.c_char_p * n)(*names), (_vp * n)(*ptrs),
             (ctypes.c_int64 * (4 * n))(*shapes), (ctypes.c_int * n)(*ndims),
             (ctypes.c_int * n)(*dtypes), (ctypes.c_int * n)(*on_dev), float(skip_threshold)),
             "set_param")
+
+    def buffer(self, name):
+        """Copy of an internal device buffer as a [rows, cols] float16 tensor (see
+        dcvc_hts_buffer / dcvc_intra_buffer)."""
+        ptr, r, c, ld = _vp(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        N.check(self._fn("buffer")(self._h, name.encode(), ctypes.byref(ptr), ctypes.byref(r),
+                                   ctypes.byref(c), ctypes.byref(ld)), "buffer")
+        full = torch.as_tensor(_DeviceView(ptr.value, (r.value, ld.value)), device="cuda")
+        torch.cuda.synchronize()
+        return full[:, : c.value].clone()
+
+    def stats(self):
+        """(symbols coded by the last call, kernels it enqueued, device bytes held)."""
+        s, k, b = ctypes.c_int(), ctypes.c_int(), ctypes.c_size_t()
+        N.check(self._fn("stats")(self._h, ctypes.byref(s), ctypes.byref(k), ctypes.byref(b)),
+                "stats")
+        return s.value, k.value, b.value
+
+
+class DMCHTSProxy(_Proxy):
+    """Chunk codec of the HT-S video model (dmc_hts_proxy.h:215-355).  One instance per stream;
+    not re-entrant."""
+
+    _kind = "hts"
 
     def add_ref_feature_from_frame(self, frame, apply_adaptor=True):
         frame = _channels_last_data(frame, "frame")
@@ -129,11 +181,7 @@ class DMCHTSProxy:
                                        1 if reset_feature_memory else 0, int(padding_b),
                                        int(padding_r), _stream(), ctypes.byref(data),
                                        ctypes.byref(size), ctypes.byref(ecp)), "compress")
-        if size.value == 0:
-            return np.zeros(0, dtype=np.uint8), ecp.value
-        buf = np.ctypeslib.as_array(ctypes.cast(data, ctypes.POINTER(ctypes.c_uint8)),
-                                    shape=(size.value,)).copy()
-        return buf, ecp.value
+        return _bytes_out(data, size), ecp.value
 
     def decompress(self, bit_stream, qp, height, width, entropy_coder_parallel,
                    reset_feature_memory):
@@ -153,22 +201,41 @@ class DMCHTSProxy:
             out.append(t.permute(0, 3, 1, 2))
         return out
 
-    def buffer(self, name):
-        """Copy of an internal per-stream buffer as a [rows, cols] float16 tensor (see
-        dcvc_hts_buffer)."""
-        ptr, r, c, ld = _vp(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
-        N.check(_lib.dcvc_hts_buffer(self._h, name.encode(), ctypes.byref(ptr), ctypes.byref(r),
-                                     ctypes.byref(c), ctypes.byref(ld)), "buffer")
-        full = torch.as_tensor(_DeviceView(ptr.value, (r.value, ld.value)), device="cuda")
-        torch.cuda.synchronize()
-        return full[:, : c.value].clone()
 
-    def stats(self):
-        """(symbols coded by the last call, kernels it enqueued, device bytes held)."""
-        s, k, b = ctypes.c_int(), ctypes.c_int(), ctypes.c_size_t()
-        N.check(_lib.dcvc_hts_stats(self._h, ctypes.byref(s), ctypes.byref(k), ctypes.byref(b)),
-                "stats")
-        return s.value, k.value, b.value
+
+class DMCIProxy(_Proxy):
+    """Intra (DMCI) frame codec (dmci_proxy.h:132-230).  Not re-entrant."""
+
+    _kind = "intra"
+
+    def compress(self, x, qp, padding_b, padding_r):
+        """x: [1, 3, H, W] float16 CUDA.  Returns (uint8 array, x_hat, ec_parallel), x_hat a
+        [1, 3, H + padding_b, W + padding_r] float16 CUDA tensor (channels last) aliasing the
+        proxy's buffer (overwritten by the next call)."""
+        x = _channels_last_data(x, "x")
+        if x.shape[1] != 3:
+            raise ValueError("x must have 3 channels")
+        data, size, ecp, xh = _vp(), ctypes.c_size_t(), ctypes.c_int(), _vp()
+        N.check(_lib.dcvc_intra_compress(self._h, x.data_ptr(), x.shape[2], x.shape[3], int(qp),
+                                         int(padding_b), int(padding_r), _stream(),
+                                         ctypes.byref(data), ctypes.byref(size),
+                                         ctypes.byref(ecp), ctypes.byref(xh)), "compress")
+        hp, wp = x.shape[2] + int(padding_b), x.shape[3] + int(padding_r)
+        x_hat = torch.as_tensor(_DeviceView(xh.value, (1, hp, wp, 3)), device="cuda")
+        return _bytes_out(data, size), x_hat.permute(0, 3, 1, 2), ecp.value
+
+    def decompress(self, bit_stream, qp, height, width, entropy_coder_parallel):
+        """Returns the [1, 3, Hp, Wp] float16 reconstruction (Hp, Wp = height, width rounded up
+        to multiples of 16), aliasing the proxy's buffer."""
+        bs = np.ascontiguousarray(np.asarray(bit_stream, dtype=np.uint8).reshape(-1))
+        xh = _vp()
+        N.check(_lib.dcvc_intra_decompress(self._h, bs.ctypes.data, bs.size, int(qp), int(height),
+                                           int(width), int(entropy_coder_parallel), _stream(),
+                                           ctypes.byref(xh)), "decompress")
+        hp = (int(height) + 15) // 16 * 16
+        wp = (int(width) + 15) // 16 * 16
+        x_hat = torch.as_tensor(_DeviceView(xh.value, (1, hp, wp, 3)), device="cuda")
+        return x_hat.permute(0, 3, 1, 2)
 
 
 class _Unavailable:
@@ -176,10 +243,6 @@ class _Unavailable:
 
     def __init__(self, *a, **k):
         raise NotImplementedError(f"{self._what} is not implemented by dcvc_b200 yet")
-
-
-class DMCIProxy(_Unavailable):
-    _what = "DMCIProxy (intra model)"
 
 
 class DMCHTLProxy(_Unavailable):

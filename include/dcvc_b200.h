@@ -228,6 +228,38 @@ int dcvc_hts_buffer(void* handle, const char* name, const void** ptr, int* rows,
 /* symbols coded by the last call, kernels it enqueued, device bytes held by the handle */
 int dcvc_hts_stats(void* handle, int* symbols, int* kernels, size_t* device_bytes);
 
+/* ------------------------------------------------------------------ intra (DMCI) codec */
+
+/* One handle = one intra coder, the counterpart of DMCIProxy
+ * (src/layers/extensions/inference/dmci_proxy.h:132-230, bind.cpp:13-17).  Same threading and
+ * stream rules as the HT-S handle. */
+int dcvc_intra_create(void** handle);
+int dcvc_intra_destroy(void* handle);
+/* set_param(state_dict, skip_threshold) (dmci_proxy.cpp:604-646): the DMCI state dict plus the
+ * four CDF entries, passed as for dcvc_hts_set_param. */
+int dcvc_intra_set_param(void* handle, int n, const char* const* names, const void* const* data,
+                         const int64_t* shapes, const int* ndims, const int* dtypes,
+                         const int* on_device, float skip_threshold);
+/* compress(x, qp, padding_b, padding_r) (dmci_proxy.cpp:296-421): x = [height, width, 3] FP16
+ * (a [1, 3, H, W] channels-last tensor); height + pad_b and width + pad_r multiples of 16.  On
+ * success *bytes (valid until the next call on the handle) holds the rANS payload (the four
+ * checkerboard steps' y symbols in the order 3, 2, 1, 0, then z), *ec_parallel its sub-stream
+ * count and *x_hat a device pointer to the [height + pad_b, width + pad_r, 3] FP16
+ * reconstruction, owned by the handle and overwritten by the next call. */
+int dcvc_intra_compress(void* handle, const void* x, int height, int width, int qp, int pad_b,
+                        int pad_r, void* stream, const uint8_t** bytes, size_t* nbytes,
+                        int* ec_parallel, void** x_hat);
+/* decompress(bit_stream, qp, height, width, ec_parallel) (dmci_proxy.cpp:423-602): *x_hat as
+ * for compress, at the picture size rounded up to multiples of 16.  DCVC_CORRUPT_STREAM for a
+ * payload that does not decode. */
+int dcvc_intra_decompress(void* handle, const uint8_t* bytes, size_t nbytes, int qp, int height,
+                          int width, int ec_parallel, void* stream, void** x_hat);
+/* Read-only view of a device buffer: "y_hat", "y_q", "params", "z_hat".  No counterpart in the
+ * reference. */
+int dcvc_intra_buffer(void* handle, const char* name, const void** ptr, int* rows, int* cols,
+                      int* ld);
+int dcvc_intra_stats(void* handle, int* symbols, int* kernels, size_t* device_bytes);
+
 #ifdef __cplusplus
 }
 #endif
