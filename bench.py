@@ -20,7 +20,6 @@ import os
 import statistics
 import subprocess
 import sys
-import tempfile
 import time
 
 import numpy as np
@@ -50,6 +49,7 @@ def parse_args():
     ap.add_argument("--height", type=int, default=1080)
     ap.add_argument("--width", type=int, default=1920)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-intra", action="store_true", help="skip the intra-codec measurement")
     return ap.parse_args()
 
 
@@ -84,26 +84,47 @@ def max_over_ranks(value, device):
 class ClockSampler:
     """nvidia-smi clock/throttle sampling during the timed region."""
 
-    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    QUERY = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
+    # Started before the warm-up so that nvidia-smi is sampling when the timed region begins;
+    # stop() keeps the samples whose nvidia-smi timestamp (host local time) falls inside the
+    # windows passed to it.
     def __init__(self, device_index):
-        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         uuid = None
         try:
             uuid = "GPU-" + str(torch.cuda.get_device_properties(device_index).uuid)
         except Exception:
             pass
-        cmd = ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits", "-lms", "200"]
+        cmd = ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits", "-lms", "50"]
         if uuid:
             cmd += ["-i", uuid]
+        self.lines = []
         try:
-            self.p = subprocess.Popen(cmd, stdout=self.f, stderr=subprocess.DEVNULL)
+            import threading
+            self.p = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
         except Exception:
             self.p = None
 
-    def stop(self):
+    def _read(self):
+        import datetime
+        for line in self.p.stdout:
+            try:
+                ts = datetime.datetime.strptime(line.split(",")[0].strip(),
+                                                "%Y/%m/%d %H:%M:%S.%f").timestamp()
+            except ValueError:
+                continue
+            self.lines.append((ts, line))
+
+    def wait_first_sample(self, timeout=5.0):
+        t0 = time.time()
+        while self.p is not None and not self.lines and time.time() - t0 < timeout:
+            time.sleep(0.01)
+
+    def stop(self, windows=None):
         if self.p is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.p.terminate()
@@ -111,12 +132,13 @@ class ClockSampler:
             self.p.wait(timeout=5)
         except Exception:
             self.p.kill()
-        self.f.flush()
-        self.f.seek(0)
+        self.t.join(timeout=5)
         sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.f.read().splitlines():
-            parts = [x.strip() for x in line.split(",")]
+        for ts, line in self.lines:
+            if windows and not any(a <= ts <= b for a, b in windows):
+                continue
+            parts = [x.strip() for x in line.split(",")][1:]
             if len(parts) < 9:
                 continue
             try:
@@ -127,7 +149,6 @@ class ClockSampler:
             for name, val in zip(names, parts[5:9]):
                 if val.lower() == "active":
                     reasons.add(name)
-        os.unlink(self.f.name)
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
         loaded = [s for s in sm if s > 0.5 * max(sm)] or sm
@@ -228,6 +249,69 @@ def cpu_baseline(H, W, strip_rows=272, chunks=2):
                       f"{coder}), scaled to {W}x{H} by pixel count; {sec:.1f} s"}
 
 
+def split_enc_dec(enc, dec, xs, args, pb, pr, H, W, stream):
+    """Encode-only and decode-only throughput of the same chunks (separate timed loops); the
+    decoder replays the payloads recorded by the encoder, so both keep their temporal state in
+    step."""
+    n = max(4, args.steps)
+    payloads = []
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(n):
+        qp = QPS[i % len(QPS)]
+        bits, ecp = enc.compress(xs[i % 2], qp, False, pb, pr)
+        payloads.append((bits, qp, ecp))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    enc_ms = e0.elapsed_time(e1)
+    e0.record(stream)
+    for bits, qp, ecp in payloads:
+        dec.decompress(bits, qp, H, W, ecp, False)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    dec_ms = e0.elapsed_time(e1)
+    return {"enc": round(FRAMES * n / (enc_ms / 1e3), 1), "dec": round(FRAMES * n / (dec_ms / 1e3), 1),
+            "chunks": n, "note": "device-timed, inputs resident; compare reference_published"}
+
+
+def intra_bench(stream, H, W, reps=10):
+    """The intra (DMCI) codec: encode-only and decode-only frames/s at the bench resolution and
+    at 256x256 (the reference's CPU-runnable intra case), QP 32."""
+    from dcvc_b200 import synthetic
+    from dcvc_b200.entropy_tables import add_cdf_to_state_dict
+    from dcvc_b200.inference_extensions_cuda import DMCIProxy
+    from dcvc_b200.model_spec import calibrated_dmci_state_dict
+    sd = add_cdf_to_state_dict(calibrated_dmci_state_dict(0))
+    sd = {k: (v.half().cuda() if v.is_floating_point() else v) for k, v in sd.items()}
+    enc, dec = DMCIProxy(), DMCIProxy()
+    enc.set_param(sd, SKIP_THRES)
+    dec.set_param(sd, SKIP_THRES)
+    out = {}
+    for (h, w), key in (((H, W), f"{W}x{H}"), ((256, 256), "256x256")):
+        x = synthetic.to_model_input([synthetic.intra_frame_yuv420(1, h, w)])
+        pr, pb = synthetic.padding_for(h, w)
+        for i in range(3):
+            bits, _, ecp = enc.compress(x, 32, pb, pr)
+            dec.decompress(bits, 32, h, w, ecp)
+        torch.cuda.synchronize()
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        e[0].record(stream)
+        for i in range(reps):
+            bits, _, ecp = enc.compress(x, 32, pb, pr)
+        e[1].record(stream)
+        for i in range(reps):
+            dec.decompress(bits, 32, h, w, ecp)
+        e[2].record(stream)
+        torch.cuda.synchronize()
+        te, td = e[0].elapsed_time(e[1]) / reps, e[1].elapsed_time(e[2]) / reps
+        out[key] = {"enc_fps": round(1e3 / te, 1), "dec_fps": round(1e3 / td, 1),
+                    "enc_ms": round(te, 3), "dec_ms": round(td, 3), "bytes": int(bits.size)}
+    out["qp"] = 32
+    out["reference_published"] = "DCVC-UF-Intra 1080p enc/dec 81.5/95.0 frames/s on A100 (README)"
+    return out
+
+
 # ----------------------------------------------------------------------------- arms
 
 def run_reference(args):
@@ -293,6 +377,8 @@ def run_gpu(args):
         bits, ecp = enc.compress(x, qp, False, pb, pr)
         return dec.decompress(bits, qp, H, W, ecp, False), bits.size
 
+    clocks = ClockSampler(local)
+    clocks.wait_first_sample()
     for i in range(args.warmup):
         step(i, xs[i % 2])
     torch.cuda.synchronize()
@@ -302,7 +388,7 @@ def run_gpu(args):
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    clocks = ClockSampler(local)
+    windows = [[time.time(), None]]
     marks = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
     marks[0].record(stream)
     nbytes = []
@@ -311,7 +397,7 @@ def run_gpu(args):
         nbytes.append(nb)
         marks[i + 1].record(stream)
     torch.cuda.synchronize()
-    clk = clocks.stop()
+    windows[-1][1] = time.time()
     if world > 1:
         dist.barrier()
     ms = marks[0].elapsed_time(marks[-1])
@@ -330,6 +416,7 @@ def run_gpu(args):
         dist.barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    windows.append([time.time(), None])
     e0.record(stream)
     for i in range(args.steps):
         x_dev.copy_(x_host[i % 2], non_blocking=True)
@@ -338,9 +425,14 @@ def run_gpu(args):
             out_host[f].copy_(frames[f][0], non_blocking=True)
     e1.record(stream)
     torch.cuda.synchronize()
+    windows[-1][1] = time.time()
     e2e = FRAMES * args.steps * world / (max_over_ranks(e0.elapsed_time(e1), "cuda") / 1e3)
 
+    # ---------------- encode alone and decode alone (the reference publishes them separately)
+    split = split_enc_dec(enc, dec, xs, args, pb, pr, H, W, stream)
+    clk = clocks.stop(windows)
     roof = roofline_quad(stream)
+    intra = None if args.no_intra else intra_bench(stream, H, W)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(H, W)
@@ -358,7 +450,9 @@ def run_gpu(args):
         "latency_ms": {"p50": round(float(np.percentile(lat_sorted, 50)), 3),
                        "p99": round(float(np.percentile(lat_sorted, 99)), 3)},
         "bytes_per_chunk": {"mean": int(np.mean(nbytes)), "min": int(min(nbytes)), "max": int(max(nbytes))},
+        "enc_decomposed_fps": split,
         "reference_published": PUBLISHED,
+        "intra": intra,
         "e2e": {"value": round(e2e, 2), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": kernels_per_step * args.steps,
         "roofline": roof,
