@@ -50,6 +50,8 @@ def parse_args():
     ap.add_argument("--width", type=int, default=1920)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-intra", action="store_true", help="skip the intra-codec measurement")
+    ap.add_argument("--streams", type=int, default=4,
+                    help="concurrent streams of the batched form (0 skips it)")
     return ap.parse_args()
 
 
@@ -249,6 +251,87 @@ def cpu_baseline(H, W, strip_rows=272, chunks=2):
                       f"{coder}), scaled to {W}x{H} by pixel count; {sec:.1f} s"}
 
 
+def batched_streams(args, H, W, n_streams):
+    """The batched form: `n_streams` independent video streams served concurrently on one GPU,
+    each by its own host thread, CUDA stream and encoder/decoder proxy pair (the codec calls
+    release the GIL).  Kernels of different streams fill each other's launch gaps, tails and
+    CPU entropy-coding waits.  Device-timed: every stream waits on one start event and one end
+    event waits on every stream."""
+    import threading
+    from dcvc_b200 import synthetic
+    from dcvc_b200.entropy_tables import add_cdf_to_state_dict
+    from dcvc_b200.inference_extensions_cuda import DMCHTSProxy
+    from dcvc_b200.model_spec import calibrated_hts_state_dict
+    sd = add_cdf_to_state_dict(calibrated_hts_state_dict(0))
+    sd = {k: (v.half().cuda() if v.is_floating_point() else v) for k, v in sd.items()}
+    pr, pb = synthetic.padding_for(H, W)
+    dev = torch.cuda.current_device()
+    workers = []
+    for i in range(n_streams):
+        seed = 100 + i
+        enc, dec = DMCHTSProxy(), DMCHTSProxy()
+        enc.set_param(sd, SKIP_THRES)
+        dec.set_param(sd, SKIP_THRES)
+        ref = synthetic.padded_reference_frame(synthetic.video_chunk_yuv420(seed, H, W, 1, 0)[0])
+        enc.add_ref_feature_from_frame(ref, True)
+        dec.add_ref_feature_from_frame(ref, False)
+        xs = [synthetic.to_model_input(synthetic.video_chunk_yuv420(seed, H, W, FRAMES, FRAMES * k))
+              for k in range(2)]
+        workers.append({"enc": enc, "dec": dec, "xs": xs, "stream": torch.cuda.Stream(),
+                        "err": None})
+    del sd
+    start_stream = torch.cuda.Stream()
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    gate = threading.Barrier(n_streams + 1)
+
+    def run(w, first, count, timed):
+        try:
+            torch.cuda.set_device(dev)
+            with torch.cuda.stream(w["stream"]):
+                if timed:
+                    gate.wait()  # the start event has been recorded
+                    w["stream"].wait_event(start)
+                for i in range(first, first + count):
+                    qp = QPS[i % len(QPS)]
+                    bits, ecp = w["enc"].compress(w["xs"][i % 2], qp, False, pb, pr)
+                    w["dec"].decompress(bits, qp, H, W, ecp, False)
+                w["done"] = torch.cuda.Event()
+                w["done"].record(w["stream"])
+        except Exception as e:  # reported by the caller
+            w["err"] = e
+            if timed:
+                gate.abort()
+
+    def round_(first, count, timed):
+        threads = [threading.Thread(target=run, args=(w, first, count, timed)) for w in workers]
+        for t in threads:
+            t.start()
+        if timed:
+            start.record(start_stream)
+            try:
+                gate.wait()
+            except threading.BrokenBarrierError:
+                pass
+        for t in threads:
+            t.join()
+        for w in workers:
+            if w["err"] is not None:
+                raise w["err"]
+
+    round_(0, args.warmup, False)
+    torch.cuda.synchronize()
+    round_(args.warmup, args.steps, True)
+    for w in workers:
+        start_stream.wait_event(w["done"])
+    end.record(start_stream)
+    torch.cuda.synchronize()
+    ms = start.elapsed_time(end)
+    return {"streams": n_streams, "value": round(FRAMES * args.steps * n_streams / (ms / 1e3), 2),
+            "unit": UNIT, "ms": round(ms, 2), "chunks": args.steps * n_streams,
+            "note": "concurrent independent 1080p streams on one GPU (plain FP16 kernels)"}
+
+
 def split_enc_dec(enc, dec, xs, args, pb, pr, H, W, stream):
     """Encode-only and decode-only throughput of the same chunks (separate timed loops); the
     decoder replays the payloads recorded by the encoder, so both keep their temporal state in
@@ -433,6 +516,9 @@ def run_gpu(args):
     clk = clocks.stop(windows)
     roof = roofline_quad(stream)
     intra = None if args.no_intra else intra_bench(stream, H, W)
+    del enc, dec
+    torch.cuda.empty_cache()
+    batched = batched_streams(args, H, W, args.streams) if args.streams > 0 else None
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(H, W)
@@ -451,6 +537,7 @@ def run_gpu(args):
                        "p99": round(float(np.percentile(lat_sorted, 99)), 3)},
         "bytes_per_chunk": {"mean": int(np.mean(nbytes)), "min": int(min(nbytes)), "max": int(max(nbytes))},
         "enc_decomposed_fps": split,
+        "batched": batched,
         "reference_published": PUBLISHED,
         "intra": intra,
         "e2e": {"value": round(e2e, 2), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},

@@ -672,13 +672,24 @@ __global__ void __launch_bounds__(kCompactThreads)
 
 // ------------------------------------------------------------------------------ depthwise
 
-// Tiled depthwise 3x3: one CTA computes a kDwTH x kDwTW pixel tile for 64 channels (8 vectors
-// of 8); the (kDwTH+2) x (kDwTW+2) halo tile is staged once in shared memory with 16-byte loads
-// (zeros outside the image) and every thread keeps the 9 taps of its channel vector in registers.
+// Tiled depthwise 3x3: one CTA computes a kDwTH x kDwTW pixel tile for 64 channels.  The
+// (kDwTH+2) x (kDwTW+2) halo tile is staged in shared memory by 16-byte asynchronous copies
+// (cp.async, zero-filled outside the image), so all of a thread's loads are in flight at once.
+// Each thread then owns one channel pair of one tile row and slides a 3x3 window of FP32 values
+// along the row: three 4-byte shared loads per output pair instead of nine 16-byte ones.
 constexpr int kDwTH = 8;
 constexpr int kDwTW = 32;
-constexpr int kDwCV = 8;  // channel vectors (of 8 halves) per CTA
-constexpr int kDwThreads = 256;
+constexpr int kDwCV = 8;  // channel vectors (of 8 halves) per CTA = 64 channels
+constexpr int kDwThreads = 256;  // 32 channel pairs x kDwTH rows
+static_assert(kDwThreads == 32 * kDwTH, "one warp per tile row");
+
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src, int src_bytes)
+{
+    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(smem_dst));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(gmem_src),
+                 "r"(src_bytes)
+                 : "memory");
+}
 
 __global__ void __launch_bounds__(kDwThreads) dwconv3x3_kernel(const __half* __restrict__ x, int H,
                                                                int W, int C, int ldx,
@@ -693,74 +704,73 @@ __global__ void __launch_bounds__(kDwThreads) dwconv3x3_kernel(const __half* __r
     const int w0 = blockIdx.z * kDwTW;
     const int cvecs = C / 8;
     const int nv = min(kDwCV, cvecs - c0);
-    for (int i = threadIdx.x; i < (kDwTH + 2) * (kDwTW + 2) * kDwCV; i += kDwThreads) {
+    constexpr int kLoads = (kDwTH + 2) * (kDwTW + 2) * kDwCV;
+#pragma unroll 4
+    for (int i = threadIdx.x; i < kLoads; i += kDwThreads) {
         const int v = i % kDwCV;
         const int pix = i / kDwCV;
         const int tx = pix % (kDwTW + 2);
         const int ty = pix / (kDwTW + 2);
         const int h = h0 + ty - 1, w = w0 + tx - 1;
-        Vec8h val;
-        if (v < nv && h >= 0 && h < H && w >= 0 && w < W) {
-            val = ld8(x + (static_cast<long long>(h) * W + w) * ldx + (c0 + v) * 8);
-        } else {
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                val.v[j] = hzero();
-            }
-        }
-        tile[ty][tx][v] = val;
+        const bool in = v < nv && h >= 0 && h < H && w >= 0 && w < W;
+        // out-of-image elements read 0 bytes from a valid address and are zero-filled
+        const __half* src = in ? x + (static_cast<long long>(h) * W + w) * ldx + (c0 + v) * 8 : x;
+        cp_async16(&tile[ty][tx][v], src, in ? 16 : 0);
     }
-    const int v = threadIdx.x % kDwCV;
-    const int slot = threadIdx.x / kDwCV;  // 0..31
-    float w9[9][8];
-    if (v < nv) {
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    const int cp = threadIdx.x & 31;  // channel pair within the CTA's 64 channels
+    const int ty = threadIdx.x >> 5;  // tile row
+    const int ch = c0 * 8 + 2 * cp;   // first of the pair's two channels
+    const bool live = 2 * cp < nv * 8;
+    float wa[9], wb[9];
+    if (live) {
 #pragma unroll
         for (int k = 0; k < 9; ++k) {
-            const float4* wp = reinterpret_cast<const float4*>(wt + k * C + (c0 + v) * 8);
-            const float4 a = __ldg(wp), b = __ldg(wp + 1);
-            w9[k][0] = a.x;
-            w9[k][1] = a.y;
-            w9[k][2] = a.z;
-            w9[k][3] = a.w;
-            w9[k][4] = b.x;
-            w9[k][5] = b.y;
-            w9[k][6] = b.z;
-            w9[k][7] = b.w;
+            const float2 t = __ldg(reinterpret_cast<const float2*>(wt + k * C + ch));
+            wa[k] = t.x;
+            wb[k] = t.y;
         }
     }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
     __syncthreads();
-    if (v >= nv) {
+    const int h = h0 + ty;
+    if (!live || h >= H) {
         return;
     }
-#pragma unroll 1
-    for (int p = slot; p < kDwTH * kDwTW; p += kDwThreads / kDwCV) {
-        const int ty = p / kDwTW, tx = p % kDwTW;
-        const int h = h0 + ty, w = w0 + tx;
-        if (h >= H || w >= W) {
-            continue;
-        }
-        float acc[8];
+    const __half2* t2 = reinterpret_cast<const __half2*>(&tile[0][0][0]);
+    auto at = [&](int r, int c) { return __half22float2(t2[(r * (kDwTW + 2) + c) * (4 * kDwCV) + cp]); };
+    float2 win[3][3];  // [ky][kx] window of the current output pixel
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            acc[j] = 0.f;
+    for (int r = 0; r < 3; ++r) {
+        win[r][0] = at(ty + r, 0);
+        win[r][1] = at(ty + r, 1);
+    }
+    __half* orow = out + static_cast<long long>(h) * W * ldo + ch;
+#pragma unroll
+    for (int tx = 0; tx < kDwTW; ++tx) {
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+            win[r][2] = at(ty + r, tx + 2);
         }
+        // FP32 accumulation in the order ky, kx (d3x3_kernel.h:104-166)
+        float a0 = 0.f, a1 = 0.f;
 #pragma unroll
         for (int ky = 0; ky < 3; ++ky) {
 #pragma unroll
             for (int kx = 0; kx < 3; ++kx) {
-                const Vec8h a = tile[ty + ky][tx + kx][v];
-#pragma unroll
-                for (int j = 0; j < 8; ++j) {
-                    acc[j] = fmaf(h2f(a.v[j]), w9[ky * 3 + kx][j], acc[j]);
-                }
+                a0 = fmaf(win[ky][kx].x, wa[ky * 3 + kx], a0);
+                a1 = fmaf(win[ky][kx].y, wb[ky * 3 + kx], a1);
             }
         }
-        Vec8h o;
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            o.v[j] = f2h(acc[j]);
+        const int w = w0 + tx;
+        if (w < W) {
+            *reinterpret_cast<__half2*>(orow + static_cast<long long>(w) * ldo) = __floats2half2_rn(a0, a1);
         }
-        st8(out + (static_cast<long long>(h) * W + w) * ldo + (c0 + v) * 8, o);
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+            win[r][0] = win[r][1];
+            win[r][1] = win[r][2];
+        }
     }
 }
 

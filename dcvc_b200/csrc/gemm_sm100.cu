@@ -11,8 +11,7 @@ namespace {
 
 constexpr int kBM = 128;
 constexpr int kBK = 64;  // one 128-byte swizzle atom of 16-bit elements
-constexpr int kEpiWarps = 8;
-constexpr int kThreads = 64 + 32 * kEpiWarps;  // producer warp, MMA warp, epilogue warps
+constexpr int kMaxEpiWarps = 16;
 // ~1 s at 2 GHz; a correct kernel never waits this long.
 constexpr long long kWaitLimit = 2000000000LL;
 constexpr int kSmemLimit = 232448;  // 227 KB per block on sm_100
@@ -51,20 +50,38 @@ struct Pack2<__nv_bfloat16> {
 __host__ __device__ constexpr bool epi_has_res(int e) { return e == kEpiBiasRes || e == kEpiBiasResQ || e == kEpiBiasRes2; }
 __host__ __device__ constexpr bool epi_has_q(int e) { return e == kEpiBiasResQ || e == kEpiBiasQ; }
 
-// Output columns of one epilogue store box (32 rows high).  Each epilogue warp owns 32 rows (its
-// TMEM lane quadrant) and half of the BN accumulator columns.
-__host__ __device__ constexpr int out_box_cols(int bn, int epi) { return epi == kEpiQuad ? bn / 8 : (bn / 2 < 64 ? bn / 2 : 64); }
+// Epilogue warps: 16 (four per TMEM lane quadrant, each owning a quarter of the BN accumulator
+// columns) for the residual epilogues with BN >= 128, whose per-tile epilogue (residual load,
+// add, store) is longer than the tile's main loop (K = 256); 8 (two per quadrant, half the
+// columns each) otherwise, which leaves shared memory for a deeper operand pipeline.
+__host__ __device__ constexpr int epi_warps(int bn, int epi)
+{
+    return (epi_has_res(epi) && bn >= 128) ? 16 : 8;
+}
+// Accumulator columns per epilogue warp, and output columns of one store box (32 rows high).
+__host__ __device__ constexpr int epi_cols(int bn, int epi) { return bn / (epi_warps(bn, epi) / 4); }
+__host__ __device__ constexpr int out_box_cols(int bn, int epi)
+{
+    return epi == kEpiQuad ? epi_cols(bn, epi) / 4 : (epi_cols(bn, epi) < 64 ? epi_cols(bn, epi) : 64);
+}
 
 template <int BN, int EPI>
 struct GemmCfg {
-    static constexpr int kHalf = BN / 2;                        // accumulator columns per warp
+    static constexpr int kEpiWarps = epi_warps(BN, EPI);
+    static constexpr int kThreads = 64 + 32 * kEpiWarps;  // producer warp, MMA warp, epilogue warps
+    static constexpr int kCols = epi_cols(BN, EPI);             // accumulator columns per warp
     static constexpr int kOutW = out_box_cols(BN, EPI);         // output columns per store box
     static constexpr int kAccPerBox = EPI == kEpiQuad ? 4 * kOutW : kOutW;
-    static constexpr int kBoxes = kHalf / kAccPerBox;
+    static constexpr int kBoxes = kCols / kAccPerBox;
     static constexpr int kBoxBytes = kOutW * 32 * 2;            // 4 KB (64 cols) or 2 KB (32 cols)
     static constexpr int kRowBytes = kOutW * 2;                 // 128 (SW128) or 64 (SW64)
     static constexpr int kResBufs = EPI == kEpiBiasRes2 ? 2 : (epi_has_res(EPI) ? 1 : 0);
-    static constexpr int kWarpStage = 4096 * (1 + kResBufs);    // out + residual staging per warp
+    // Residual boxes in flight per warp: a ring of kResSlots box slots filled in (tile, box)
+    // order, so a tile's residual streams in while its accumulator is still being computed.  The
+    // result is written over the residual in its slot and stored from there; epilogues without a
+    // residual stage their output in one buffer of their own.
+    static constexpr int kResSlots = kResBufs == 1 ? (kBoxes < 2 ? kBoxes : 2) : (kResBufs == 2 ? 1 : 0);
+    static constexpr int kWarpStage = 4096 * (kResBufs == 0 ? 1 : kResBufs * kResSlots);
     static constexpr int kEpiBytes = kEpiWarps * kWarpStage;
     static constexpr int kABytes = kBM * kBK * 2;
     static constexpr int kBBytes = BN * kBK * 2;
@@ -78,7 +95,10 @@ struct GemmCfg {
     static constexpr int kTmemCols = 2 * BN;
     static_assert(kStages >= 2, "shared memory too small for two pipeline stages");
     static_assert(kBytes <= kSmemLimit, "shared memory budget exceeded");
-    static_assert(EPI == kEpiSubpel || kBoxes * kAccPerBox == kHalf, "box tiling");
+    static_assert(EPI == kEpiSubpel || kBoxes * kAccPerBox == kCols, "box tiling");
+    static_assert(EPI == kEpiSubpel || kOutW * 2 == 128 || kOutW * 2 == 64, "staging row width");
+    static_assert(kEpiWarps <= kMaxEpiWarps, "epilogue warps");
+    static_assert(kResSlots <= 2, "residual ring");
 };
 
 // Byte offset of the 16-byte chunk j of row r inside a swizzled staging box (the layout TMA
@@ -94,7 +114,7 @@ __device__ __forceinline__ int stage_off(int r, int j)
 }
 
 template <typename T, int BN, int EPI>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(GemmCfg<BN, EPI>::kThreads, 1)
     gemm_sm100_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                       const __grid_constant__ CUtensorMap tmO, const __grid_constant__ CUtensorMap tmR,
                       const __grid_constant__ CUtensorMap tmR2, const GemmParams p)
@@ -109,8 +129,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     uint64_t* tfull = empty + kStages;
     uint64_t* tempty = tfull + 2;
     uint64_t* drain = tempty + 2;
-    uint64_t* resbar = drain + 1;  // [kEpiWarps]
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(resbar + kEpiWarps);
+    uint64_t* resbar = drain + 1;  // [kEpiWarps][2]: one barrier per residual ring slot
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(resbar + 2 * C::kEpiWarps);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5;
@@ -127,10 +147,10 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(&tfull[b], 1);
-            mbar_init(&tempty[b], kEpiWarps);
+            mbar_init(&tempty[b], C::kEpiWarps);
         }
         mbar_init(drain, 1);
-        for (int w = 0; w < kEpiWarps; ++w) {
+        for (int w = 0; w < 2 * C::kEpiWarps; ++w) {
             mbar_init(&resbar[w], 1);
         }
         *abort_flag = 0;
@@ -245,36 +265,55 @@ __global__ void __launch_bounds__(kThreads, 1)
             }
         }
     } else {
-        // ------------------------------------------------------------ epilogue warps (2..9)
+        // ------------------------------------------------------------ epilogue warps
         using P = Pack2<T>;
-        const int ew = warp - 2;                  // epilogue warp index 0..7
+        const int ew = warp - 2;                  // epilogue warp index
         const int quad = warp & 3;                // TMEM lane quadrant this warp may access
-        const int half = ew >> 2;                 // which half of the BN columns
-        uint8_t* out_buf = smem + C::kEpiOffset + ew * C::kWarpStage;
-        uint8_t* res_buf = out_buf + 4096;
-        uint8_t* res2_buf = out_buf + 8192;
-        uint64_t* rbar = &resbar[ew];
-        uint32_t res_phase = 0;
+        const int half = ew >> 2;                 // which column part of the BN columns
+        uint8_t* wbuf = smem + C::kEpiOffset + ew * C::kWarpStage;
+        // residual ring slot s: res at wbuf + 4096 * s * kResBufs, res2 right after it
+        auto res_slot = [&](int s) { return wbuf + 4096 * s * C::kResBufs; };
+        uint64_t* rbar = &resbar[2 * ew];
+        uint32_t res_phase = 0;    // phase bit per ring slot
+        uint32_t res_pending = 0;  // ring slots with a load in flight
         int acc = 0;
         uint32_t acc_phase = 0;
         if (EPI != kEpiSubpel && lane == 0) {
             tma_prefetch_desc(&tmO);
         }
-        for (int tile = blockIdx.x; tile < num_tiles && !*abort_flag; tile += gridDim.x) {
+        // Issues the residual load of box `b` of this CTA's `k`-th tile into ring slot `s`
+        // (lane 0; nothing for tiles past the end or rows past M).
+        auto issue_res = [&](int k, int b, int s) {
+            const int t = blockIdx.x + k * gridDim.x;
+            if (t >= num_tiles) {
+                return;
+            }
+            const int r0 = (t % num_m) * kBM + quad * 32;
+            if (r0 >= p.M) {
+                return;
+            }
+            const int col = (t / num_m) * BN + half * C::kCols + b * C::kAccPerBox;
+            mbar_arrive_expect_tx(&rbar[s], C::kBoxBytes * C::kResBufs);
+            tma_load_2d(res_slot(s), &tmR, &rbar[s], col, r0);
+            if constexpr (EPI == kEpiBiasRes2) {
+                tma_load_2d(res_slot(s) + 4096, &tmR2, &rbar[s], col, r0);
+            }
+            res_pending |= 1u << s;
+        };
+        if constexpr (epi_has_res(EPI)) {
+            if (lane == 0) {
+                for (int i = 0; i < C::kResSlots; ++i) {
+                    issue_res(i / C::kBoxes, i % C::kBoxes, i);
+                }
+            }
+        }
+        int item = 0;  // (tile, box) sequence number of this warp
+        for (int tile = blockIdx.x, k = 0; tile < num_tiles && !*abort_flag; tile += gridDim.x, ++k) {
             const int m0 = (tile % num_m) * kBM;
             const int n0 = (tile / num_m) * BN;
             const int row0 = m0 + quad * 32;        // first row owned by this warp
             const bool rows_live = row0 < p.M;
-            const int nacc0 = n0 + half * C::kHalf;  // first accumulator column of this warp
-            if constexpr (epi_has_res(EPI)) {
-                if (rows_live && lane == 0) {
-                    mbar_arrive_expect_tx(rbar, C::kBoxBytes * C::kResBufs);
-                    tma_load_2d(res_buf, &tmR, rbar, nacc0, row0);
-                    if constexpr (EPI == kEpiBiasRes2) {
-                        tma_load_2d(res2_buf, &tmR2, rbar, nacc0, row0);
-                    }
-                }
-            }
+            const int nacc0 = n0 + half * C::kCols;  // first accumulator column of this warp
             if (!mbar_wait_bounded(&tfull[acc], acc_phase, kWaitLimit)) {
                 *abort_flag = 1;
                 report_error(p.err, kErrGemmEpilogueTimeout);
@@ -282,13 +321,13 @@ __global__ void __launch_bounds__(kThreads, 1)
             }
             tc_fence_after();
             const uint32_t tbase = tmem_base + (static_cast<uint32_t>(quad * 32) << 16) + acc * BN +
-                                   half * C::kHalf;
+                                   half * C::kCols;
             if constexpr (EPI == kEpiSubpel) {
                 // direct stores: the shuffled rows of one box are not contiguous in memory
                 const int m = row0 + lane;
                 const bool live = m < p.M;
 #pragma unroll 1
-                for (int c = 0; c < C::kHalf / 32; ++c) {
+                for (int c = 0; c < C::kCols / 32; ++c) {
                     uint32_t r[32];
                     tmem_ld_32x32b_x32(tbase + c * 32, r);
                     tc_wait_ld();
@@ -313,17 +352,28 @@ __global__ void __launch_bounds__(kThreads, 1)
                 }
             } else {
 #pragma unroll 1
-                for (int b = 0; b < C::kBoxes; ++b) {
+                for (int b = 0; b < C::kBoxes; ++b, ++item) {
                     const int ncol = nacc0 + b * C::kAccPerBox;  // first accumulator column of box
+                    const int slot = C::kResSlots > 1 ? item % C::kResSlots : 0;
+                    const uint8_t* res_buf = res_slot(slot);
+                    const uint8_t* res2_buf = res_buf + 4096;
+                    // the result replaces the residual in its slot; without a residual the
+                    // warp's own buffer stages it
+                    uint8_t* out_buf = epi_has_res(EPI) ? res_slot(slot) : wbuf;
                     if constexpr (epi_has_res(EPI)) {
-                        if (rows_live && !mbar_wait_bounded(rbar, res_phase, kWaitLimit)) {
-                            *abort_flag = 1;
-                            report_error(p.err, kErrGemmEpilogueTimeout);
+                        if (rows_live) {
+                            if (!mbar_wait_bounded(&rbar[slot], (res_phase >> slot) & 1u, kWaitLimit)) {
+                                *abort_flag = 1;
+                                report_error(p.err, kErrGemmEpilogueTimeout);
+                            } else {
+                                res_pending &= ~(1u << slot);
+                            }
+                            res_phase ^= 1u << slot;
                         }
-                        res_phase ^= rows_live ? 1u : 0u;
                     }
-                    // the previous box's store must have read the staging buffer
-                    if (lane == 0) {
+                    // the previous box's store must have read the staging buffer (a residual slot
+                    // was already waited for before its refill)
+                    if (!epi_has_res(EPI) && lane == 0) {
                         bulk_wait_read0();
                     }
                     __syncwarp();
@@ -432,13 +482,12 @@ __global__ void __launch_bounds__(kThreads, 1)
                         bulk_commit();
                     }
                     if constexpr (epi_has_res(EPI)) {
-                        // every lane has read this box's residual: fetch the next one
-                        if (b + 1 < C::kBoxes && rows_live && lane == 0) {
-                            mbar_arrive_expect_tx(rbar, C::kBoxBytes * C::kResBufs);
-                            tma_load_2d(res_buf, &tmR, rbar, ncol + C::kAccPerBox, row0);
-                            if constexpr (EPI == kEpiBiasRes2) {
-                                tma_load_2d(res2_buf, &tmR2, rbar, ncol + C::kAccPerBox, row0);
-                            }
+                        // every lane has read this box's residual: refill the slot with the box
+                        // kResSlots items ahead (possibly in this CTA's next tile)
+                        if (lane == 0 && !*abort_flag) {
+                            bulk_wait_read0();  // the store has read the slot
+                            const int nxt = item + C::kResSlots;
+                            issue_res(nxt / C::kBoxes, nxt % C::kBoxes, slot);
                         }
                     }
                 }
@@ -453,8 +502,20 @@ __global__ void __launch_bounds__(kThreads, 1)
                 acc_phase ^= 1;
             }
         }
+        if constexpr (epi_has_res(EPI)) {
+            // after an abort, let this warp's residual loads land before the CTA winds down
+            if (lane == 0) {
+                for (int s = 0; s < C::kResSlots; ++s) {
+                    if (res_pending & (1u << s)) {
+                        mbar_wait_bounded(&rbar[s], (res_phase >> s) & 1u, kWaitLimit / 16);
+                    }
+                }
+            }
+        }
+        // the staging buffers must have been read before the CTA's shared memory is released;
+        // the global writes themselves complete with the grid
         if (EPI != kEpiSubpel && lane == 0) {
-            bulk_wait0();
+            bulk_wait_read0();
         }
         __syncwarp();
     }
@@ -486,7 +547,7 @@ cudaError_t launch_one(const Maps& m, const GemmParams& p, cudaStream_t stream)
     }
     const int num_tiles = ((p.M + kBM - 1) / kBM) * (p.N / BN);
     const int grid = num_tiles < num_sms() ? num_tiles : num_sms();
-    return launch_pdl(kernel, dim3(grid), dim3(kThreads), C::kBytes, stream, m.a, m.b, m.o, m.r, m.r2, p);
+    return launch_pdl(kernel, dim3(grid), dim3(C::kThreads), C::kBytes, stream, m.a, m.b, m.o, m.r, m.r2, p);
 }
 
 template <typename T, int BN>

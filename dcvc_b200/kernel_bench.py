@@ -2,6 +2,11 @@
 stream), also the small fixed case used for ncu captures.
 
     python -m dcvc_b200.kernel_bench [--case quad|wsilu|res|bias2048|dwconv|all] [--reps N]
+                                     [--sets S] [--bn 0|64|128|256]
+
+Consecutive launches cycle through S independent operand sets (default: enough sets for 300 MB),
+so the timed launches read their inputs from HBM rather than from the 126 MB L2, as they do
+inside a chunk.
 
 Shapes are those of a 512-channel dcb2 DepthConvBlock at 1920x1088 (M = 136 x 240 = 32640
 pixels): dc.0 (512 -> 256, WSiLU), depthwise 3x3 on 256 channels, dc.3 (256 -> 512 + residual),
@@ -18,9 +23,7 @@ from . import ops
 M8 = 136 * 240
 
 
-def _case(name):
-    g = torch.Generator(device="cuda").manual_seed(11)
-
+def _case(name, g, bn=0):
     def rnd(*s, scale=1.0):
         return (torch.randn(*s, device="cuda", generator=g) * scale).half()
 
@@ -31,7 +34,9 @@ def _case(name):
         fn = lambda: ops.dwconv3x3(x, 136, 240, w, out)  # noqa: E731
         return fn, 0.0, 2 * x.numel() * 2 + w.numel() * 4
     shapes = {"quad": (M8, 1024, 512, N.EPI_QUAD), "wsilu": (M8, 256, 512, N.EPI_BIAS_WSILU),
-              "res": (M8, 512, 256, N.EPI_BIAS_RES), "bias2048": (M8, 512, 2048, N.EPI_BIAS)}
+              "res": (M8, 512, 256, N.EPI_BIAS_RES), "bias2048": (M8, 512, 2048, N.EPI_BIAS),
+              # launch and ramp cost: one tile, and the residual GEMM at a quarter of the pixels
+              "tiny": (128, 256, 64, N.EPI_BIAS), "res_quarter": (M8 // 4, 512, 256, N.EPI_BIAS_RES)}
     M, Nn, K, epi = shapes[name]
     a = rnd(M, K)
     w = rnd(Nn, K, scale=K ** -0.5)
@@ -39,23 +44,39 @@ def _case(name):
     res = rnd(M, Nn) if epi == N.EPI_BIAS_RES else None
     nout = Nn // 4 if epi == N.EPI_QUAD else Nn
     out = torch.empty(M, nout, device="cuda", dtype=torch.float16)
-    fn = lambda: ops.conv1x1(a, w, b, epi, res=res, out=out)  # noqa: E731
+    fn = lambda: ops.conv1x1(a, w, b, epi, res=res, out=out, block_n=bn)  # noqa: E731
     byts = (M * K + Nn * K + M * nout + (M * Nn if res is not None else 0)) * 2
     return fn, 2.0 * M * Nn * K, byts
 
 
-def run(name, reps=20, warmup=5):
-    fn, flops, byts = _case(name)
-    for _ in range(warmup):
-        fn()
-    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    s.record()
-    for _ in range(reps):
-        fn()
-    e.record()
+def run(name, reps=20, warmup=5, sets=0, bn=0):
+    """Device time per launch: `reps` launches cycling through the operand sets are captured in
+    one CUDA graph (no host launch cost between them, as inside the codec's phase graphs), the
+    graph is replayed once to warm up and timed on the next replay."""
+    g = torch.Generator(device="cuda").manual_seed(11)
+    made = [_case(name, g, bn)]
+    if sets <= 0:
+        sets = -(-300_000_000 // made[0][2])
+    made += [_case(name, g, bn) for _ in range(sets - 1)]
+    fns = [m[0] for m in made]
+    flops, byts = made[0][1], made[0][2]
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        for i in range(warmup):
+            fns[i % len(fns)]()
+        stream.synchronize()
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=stream):
+            for i in range(reps):
+                fns[i % len(fns)]()
+        graph.replay()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        graph.replay()
+        e.record(stream)
     e.synchronize()
     sec = s.elapsed_time(e) / 1e3 / reps
-    return {"case": name, "us": round(sec * 1e6, 2), "tflops": round(flops / sec / 1e12, 1),
+    return {"case": name, "bn": bn, "us": round(sec * 1e6, 2), "tflops": round(flops / sec / 1e12, 1),
             "gbs": round(byts / sec / 1e9, 1)}
 
 
@@ -63,10 +84,12 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--case", default="all")
     ap.add_argument("--reps", type=int, default=20)
+    ap.add_argument("--sets", type=int, default=0)
+    ap.add_argument("--bn", type=int, default=0, help="GEMM N tile (0 = the library's choice)")
     args = ap.parse_args()
     cases = ["quad", "wsilu", "res", "bias2048", "dwconv"] if args.case == "all" else [args.case]
     for c in cases:
-        print(json.dumps(run(c, args.reps)), flush=True)
+        print(json.dumps(run(c, args.reps, sets=args.sets, bn=args.bn)), flush=True)
 
 
 if __name__ == "__main__":
