@@ -23,6 +23,8 @@ CH_RECON = 256
 QP_NUM = 64
 # intra model sizes (image_model.py:11-14)
 CH_ENC_DEC_INTRA = 384
+# Residual-branch scale of the calibrated variants (see calibrated_hts_state_dict).
+CALIBRATION_ALPHA = 0.1
 
 
 class _Act(nn.Module):
@@ -137,6 +139,68 @@ class HTSModel(nn.Module):
         _init_xavier(self)
 
 
+class HTLModel(nn.Module):
+    """Parameter tree of DMC(ModelStructure.HTL) (video_model_ht.py:24-351 with is_hts False):
+    plain (not dcb2) DepthConvBlocks, a 3x3 sub-pixel decoder up-sampling with bias, biased
+    hyper-decoder up-sampling, and resampling blocks with the default shortcut."""
+
+    def __init__(self):
+        super().__init__()
+        self.bit_estimator_z = BitEstimator(QP_NUM, CH_Z)
+        self.feature_adaptor_i = _Wrap(conv=_seq(DCB(CH_SRC_INTRA, CH_M), DCB(CH_M, CH_M), DCB(CH_M, CH_M)))
+        self.feature_adaptor_m = _Wrap(conv=_seq(DCB(CH_M + CH_D, CH_M), *[DCB(CH_M, CH_M) for _ in range(9)]))
+        self.feature_extractor = _Wrap(conv=_seq(DCB(CH_M, CH_D), DCB(CH_D, CH_D)))
+        enc = _Wrap(conv1=_seq(DCB(CH_SRC + CH_D, CH_D), *[DCB(CH_D, CH_D) for _ in range(6)]))
+        enc.down = nn.Conv2d(CH_D, CH_Y, 3, stride=2, padding=1)
+        self.encoder = enc
+        self.hyper_encoder = _Wrap(conv=_seq(DCB(CH_Y, CH_Y), RBDown(CH_Y, CH_Y), RBDown(CH_Y, CH_Z)))
+        self.hyper_decoder = _Wrap(conv=_seq(RBUp(CH_Z, CH_Y, force_bias=True),
+                                             RBUp(CH_Y, CH_Y, force_bias=True), DCB(CH_Y, CH_Y)))
+        self.temporal_prior_encoder = _Wrap(conv=RBDown(CH_D, CH_Y * 2))
+        pf = [DCB(CH_Y * 3, CH_Y * 3) for _ in range(3)]
+        self.y_prior_fusion = _Wrap(conv=_seq(*pf, nn.Conv2d(CH_Y * 3, CH_Y * 3, 1)))
+        self.y_spatial_prior_reduction = nn.Conv2d(CH_Y * 3, CH_Y, 1)
+        for k in (1, 2, 3):
+            setattr(self, f"y_spatial_prior_adaptor_{k}", DCB(CH_Y * 2, CH_Y * 2, force_adaptor=True))
+        sp = [DCB(CH_Y * 2, CH_Y * 2) for _ in range(3)]
+        self.y_spatial_prior = _Wrap(conv=_seq(*sp, nn.Conv2d(CH_Y * 2, CH_Y * 2, 1)))
+        dec = _Wrap(up=Subpel(CH_Y, CH_D, 3, padding=1, force_bias=True))
+        dec.conv1 = _seq(DCB(CH_D * 2, CH_D), *[DCB(CH_D, CH_D) for _ in range(10)])
+        self.decoder = dec
+        self.recon_head = _Wrap(conv=nn.ModuleList([
+            _seq(DCB(CH_D, CH_RECON), *[DCB(CH_RECON, CH_RECON) for _ in range(4)],
+                 nn.Conv2d(CH_RECON, CH_SRC_INTRA, 1)) for _ in range(FRAME_DELAY)]))
+        self.q_encoder = nn.Parameter(torch.ones((QP_NUM, CH_D)))
+        self.q_decoder = nn.Parameter(torch.ones((QP_NUM, CH_D)))
+        self.q_feature = nn.Parameter(torch.ones((QP_NUM, CH_D)))
+        _init_xavier(self)
+
+
+def htl_state_dict(seed=0, dtype=torch.float32):
+    """State dict of a random-init HT-L model, equal to the reference DMC(ModelStructure.HTL)
+    under torch.manual_seed(seed) (fp32 CPU; cast to `dtype`)."""
+    return _seeded(HTLModel, seed, dtype)
+
+
+def calibrated_htl_state_dict(seed=0, dtype=torch.float32, alpha=CALIBRATION_ALPHA):
+    """The seed-`seed` HT-L weights with the residual-branch output convolutions scaled by
+    `alpha` (see calibrated_hts_state_dict)."""
+    sd = htl_state_dict(seed, torch.float32)
+    for k in list(sd):
+        if k.endswith(("dc.3.weight", "ffn.2.weight")):
+            sd[k] = sd[k] * alpha
+    return {k: v.to(dtype) for k, v in sd.items()}
+
+
+def perturbed_htl_state_dict(seed=0, dtype=torch.float32, q_jitter=0.25, calibrated=True):
+    """Seed-`seed` HT-L weights with non-trivial per-QP quant vectors."""
+    sd = calibrated_htl_state_dict(seed) if calibrated else htl_state_dict(seed, torch.float32)
+    g = torch.Generator().manual_seed(seed + 23)
+    for k in ("q_encoder", "q_decoder", "q_feature"):
+        sd[k] = 1.0 + q_jitter * (torch.rand(sd[k].shape, generator=g) * 2 - 1)
+    return {k: v.to(dtype) for k, v in sd.items()}
+
+
 class DMCIModel(nn.Module):
     """Parameter tree of DMCI, the intra model (image_model.py:15-140).  Its resampling blocks
     keep the reference's default shortcut (layers.py:162-188), which has no parameters."""
@@ -188,9 +252,6 @@ def hts_state_dict(seed=0, dtype=torch.float32):
     torch.manual_seed(seed) (fp32 CPU; cast to `dtype`)."""
     return _seeded(HTSModel, seed, dtype)
 
-
-# Residual-branch scale of the calibrated variant (see calibrated_hts_state_dict).
-CALIBRATION_ALPHA = 0.1
 
 
 def calibrated_hts_state_dict(seed=0, dtype=torch.float32, alpha=CALIBRATION_ALPHA):
