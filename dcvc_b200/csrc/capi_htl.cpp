@@ -1,0 +1,135 @@
+// extern "C" entry points of the HT-L codec runtime (declared in include/dcvc_b200.h).
+#include "capi_state_dict.h"
+#include "errors.h"
+#include "htl_codec.h"
+
+#include "../../include/dcvc_b200.h"
+
+#include <exception>
+
+using namespace dcvc;
+
+namespace {
+
+struct HtlHandle {
+    HtlCodec codec;
+    std::vector<uint8_t> bytes;
+};
+
+int fail(int status, const std::string& msg)
+{
+    set_last_error(msg);
+    return status;
+}
+
+}  // namespace
+
+extern "C" {
+
+int dcvc_htl_create(void** handle)
+{
+    if (handle == nullptr) {
+        return fail(kInvalidArgument, "dcvc_htl_create: null output");
+    }
+    if (device_error_word() == nullptr) {
+        return fail(kCudaError, "dcvc_htl_create: no usable CUDA device");
+    }
+    try {
+        *handle = new HtlHandle();
+    } catch (const std::exception& e) {
+        return fail(kOutOfMemory, std::string("dcvc_htl_create: ") + e.what());
+    }
+    return kOk;
+}
+
+int dcvc_htl_destroy(void* handle)
+{
+    delete static_cast<HtlHandle*>(handle);
+    return kOk;
+}
+
+int dcvc_htl_set_param(void* handle, int n, const char* const* names, const void* const* data,
+                       const int64_t* shapes, const int* ndims, const int* dtypes,
+                       const int* on_device, float skip_threshold)
+{
+    if (handle == nullptr) {
+        return fail(kInvalidArgument, "dcvc_htl_set_param: null handle");
+    }
+    StateDict sd;
+    const int st = build_state_dict(n, names, data, shapes, ndims, dtypes, on_device, &sd,
+                                    "dcvc_htl_set_param");
+    if (st != kOk) {
+        return st;
+    }
+    return static_cast<HtlHandle*>(handle)->codec.set_param(sd, skip_threshold);
+}
+
+int dcvc_htl_add_ref_feature(void* handle, const void* frame, int height, int width,
+                             int apply_adaptor, void* stream)
+{
+    if (handle == nullptr) {
+        return fail(kInvalidArgument, "dcvc_htl_add_ref_feature: null handle");
+    }
+    return static_cast<HtlHandle*>(handle)->codec.add_ref_feature(
+        static_cast<const __half*>(frame), height, width, apply_adaptor != 0,
+        static_cast<cudaStream_t>(stream));
+}
+
+int dcvc_htl_compress(void* handle, const void* x, int height, int width, int qp, int reset,
+                      int pad_b, int pad_r, void* stream, const uint8_t** bytes, size_t* nbytes,
+                      int* ec_parallel)
+{
+    if (handle == nullptr || bytes == nullptr || nbytes == nullptr || ec_parallel == nullptr) {
+        return fail(kInvalidArgument, "dcvc_htl_compress: null argument");
+    }
+    HtlHandle* h = static_cast<HtlHandle*>(handle);
+    int st = h->codec.compress(static_cast<const __half*>(x), height, width, qp, reset != 0, pad_b,
+                               pad_r, static_cast<cudaStream_t>(stream), &h->bytes, ec_parallel);
+    if (st != kOk) {
+        return st;
+    }
+    *bytes = h->bytes.data();
+    *nbytes = h->bytes.size();
+    return kOk;
+}
+
+int dcvc_htl_decompress(void* handle, const uint8_t* bytes, size_t nbytes, int qp, int height,
+                        int width, int ec_parallel, int reset, void* stream, void** frames)
+{
+    if (handle == nullptr || frames == nullptr) {
+        return fail(kInvalidArgument, "dcvc_htl_decompress: null argument");
+    }
+    const __half* f[HtlCodec::kFrames] = {nullptr};
+    int st = static_cast<HtlHandle*>(handle)->codec.decompress(
+        bytes, nbytes, qp, height, width, ec_parallel, reset != 0, static_cast<cudaStream_t>(stream), f);
+    if (st == kOk) {
+        for (int i = 0; i < HtlCodec::kFrames; ++i) {
+            frames[i] = const_cast<__half*>(f[i]);
+        }
+    }
+    return st;
+}
+
+int dcvc_htl_buffer(void* handle, const char* name, const void** ptr, int* rows, int* cols,
+                    int* ld)
+{
+    if (handle == nullptr || name == nullptr || ptr == nullptr || rows == nullptr ||
+        cols == nullptr || ld == nullptr) {
+        return fail(kInvalidArgument, "dcvc_htl_buffer: null argument");
+    }
+    return static_cast<HtlHandle*>(handle)->codec.buffer(name, ptr, rows, cols, ld);
+}
+
+int dcvc_htl_stats(void* handle, int* symbols, int* kernels, size_t* device_bytes)
+{
+    if (handle == nullptr) {
+        return fail(kInvalidArgument, "dcvc_htl_stats: null handle");
+    }
+    const HtlCodec& c = static_cast<HtlHandle*>(handle)->codec;
+    if (symbols) *symbols = c.last_symbol_count();
+    if (kernels) *kernels = c.last_kernel_count();
+    if (device_bytes) *device_bytes = c.device_bytes();
+    return kOk;
+}
+
+}  // extern "C"

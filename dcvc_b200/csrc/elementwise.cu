@@ -111,12 +111,13 @@ __global__ void space_to_depth2_kernel(const __half* __restrict__ x, int H, int 
     }
 }
 
-__global__ void im2col3x3s2_kernel(const __half* __restrict__ x, int H, int W, int C, int ldx,
-                                   __half* __restrict__ out)
+template <int S>
+__global__ void im2col3x3_kernel(const __half* __restrict__ x, int H, int W, int C, int ldx,
+                                 __half* __restrict__ out)
 {
     griddep_launch_dependents();
     griddep_wait();
-    const int Ho = H / 2, Wo = W / 2;
+    const int Ho = H / S, Wo = W / S;
     const int vecs = C / 8;
     const long long total = static_cast<long long>(Ho) * Wo * 9 * vecs;
     for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
@@ -127,8 +128,8 @@ __global__ void im2col3x3s2_kernel(const __half* __restrict__ x, int H, int W, i
         const int v = r - tap * vecs;
         const int ho = static_cast<int>(pix / Wo);
         const int wo = static_cast<int>(pix - static_cast<long long>(ho) * Wo);
-        const int h = 2 * ho + tap / 3 - 1;
-        const int w = 2 * wo + tap % 3 - 1;
+        const int h = S * ho + tap / 3 - 1;
+        const int w = S * wo + tap % 3 - 1;
         Vec8h o;
         if (h >= 0 && h < H && w >= 0 && w < W) {
             o = ld8(x + (static_cast<long long>(h) * W + w) * ldx + v * 8);
@@ -469,14 +470,15 @@ __global__ void build_index_4x_kernel(int phase, const __half* __restrict__ y_q,
     }
 }
 
-// restore_y_4x[_and_add_inplace] / restore_y_4x_add_and_multiply_broadcast (stream.cu:757-860):
-// t = part[m, c % (C/4)] + means[m, c] on the phase's active quarter, 0 elsewhere;
-// MODE 0: y_hat = t; 1: y_hat = y_hat + t; 3: y_hat = (y_hat + t) * q[c].
+// restore_y_4x[_and_add_inplace] / restore_y_4x_add_and_multiply_broadcast (stream.cu:757-860)
+// and add_and_multiply_with_clamp_min_inplace (stream.cu:40-76): t = part[m, c % (C/4)] + means[m, c] on
+// the phase's active quarter, 0 elsewhere; MODE 0: y_hat = t; 1: y_hat = y_hat + t;
+// 2: y_hat = (y_hat + t) * max(q[m, c], 0.5); 3: y_hat = (y_hat + t) * q[m, c] (ldq = 0: one row).
 template <int MODE>
 __global__ void restore_4x_kernel(int phase, const __half* __restrict__ part,
                                   const __half* __restrict__ means, int ldm,
-                                  const __half* __restrict__ q, __half* __restrict__ y_hat, int ldh,
-                                  int H, int W, int C)
+                                  const __half* __restrict__ q, int ldq, __half* __restrict__ y_hat,
+                                  int ldh, int H, int W, int C)
 {
     griddep_launch_dependents();
     griddep_wait();
@@ -496,16 +498,19 @@ __global__ void restore_4x_kernel(int phase, const __half* __restrict__ part,
         if (MODE >= 1) {
             prev = ld8(y_hat + m * ldh + v * 8);
         }
-        if (MODE == 3) {
-            qd = ld8(q + v * 8);
+        if (MODE >= 2) {
+            qd = ld8(q + m * ldq + v * 8);
         }
+        const __half half_ = __float2half_rn(0.5f);
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
             __half t = on ? hadd(pp.v[j], mm.v[j]) : hzero();
             if (MODE >= 1) {
                 t = hadd(prev.v[j], t);
             }
-            if (MODE == 3) {
+            if (MODE == 2) {
+                t = hmul(t, __hmax(qd.v[j], half_));
+            } else if (MODE == 3) {
                 t = hmul(t, qd.v[j]);
             }
             o.v[j] = t;
@@ -817,7 +822,18 @@ cudaError_t launch_im2col3x3s2(const __half* x, int H, int W, int C, int ldx, __
     if (H % 2 || W % 2 || C % 8 || ldx % 8 || !al16(x) || !al16(out)) {
         return cudaErrorInvalidValue;
     }
-    launch_pdl(im2col3x3s2_kernel, dim3(grid_for(static_cast<long long>(H / 2) * (W / 2) * 9 * (C / 8))), dim3(kThreads), 0, s, x, H, W, C, ldx, out);
+    launch_pdl(im2col3x3_kernel<2>, dim3(grid_for(static_cast<long long>(H / 2) * (W / 2) * 9 * (C / 8))), dim3(kThreads), 0, s, x, H, W, C, ldx, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_im2col3x3s1(const __half* x, int H, int W, int C, int ldx, __half* out,
+                               cudaStream_t s)
+{
+    if (H <= 0 || W <= 0 || C % 8 || ldx % 8 || !al16(x) || !al16(out)) {
+        return cudaErrorInvalidValue;
+    }
+    launch_pdl(im2col3x3_kernel<1>, dim3(grid_for(static_cast<long long>(H) * W * 9 * (C / 8))),
+               dim3(kThreads), 0, s, x, H, W, C, ldx, out);
     return cudaGetLastError();
 }
 
@@ -990,23 +1006,26 @@ cudaError_t launch_build_index_dec_4x(int phase, const __half* scales, int lds, 
 }
 
 cudaError_t launch_restore_4x(int phase, int mode, const __half* part, const __half* means,
-                              int ldm, const __half* q, __half* y_hat, int ldh, int H, int W,
-                              int C, cudaStream_t s)
+                              int ldm, const __half* q, int ldq, __half* y_hat, int ldh, int H,
+                              int W, int C, cudaStream_t s)
 {
-    if (phase < 0 || phase > 3 || C % 32 || ldm % 8 || ldh % 8 || !al16(part) ||
-        (mode != 0 && mode != 1 && mode != 3) || (mode == 3 && q == nullptr)) {
+    if (phase < 0 || phase > 3 || C % 32 || ldm % 8 || ldh % 8 || ldq % 8 || !al16(part) ||
+        mode < 0 || mode > 3 || (mode >= 2 && q == nullptr)) {
         return cudaErrorInvalidValue;
     }
     const int g = grid_for(static_cast<long long>(H) * W * (C / 8));
     if (mode == 0) {
         launch_pdl(restore_4x_kernel<0>, dim3(g), dim3(kThreads), 0, s, phase, part, means, ldm, q,
-                   y_hat, ldh, H, W, C);
+                   ldq, y_hat, ldh, H, W, C);
     } else if (mode == 1) {
         launch_pdl(restore_4x_kernel<1>, dim3(g), dim3(kThreads), 0, s, phase, part, means, ldm, q,
-                   y_hat, ldh, H, W, C);
+                   ldq, y_hat, ldh, H, W, C);
+    } else if (mode == 2) {
+        launch_pdl(restore_4x_kernel<2>, dim3(g), dim3(kThreads), 0, s, phase, part, means, ldm, q,
+                   ldq, y_hat, ldh, H, W, C);
     } else {
         launch_pdl(restore_4x_kernel<3>, dim3(g), dim3(kThreads), 0, s, phase, part, means, ldm, q,
-                   y_hat, ldh, H, W, C);
+                   ldq, y_hat, ldh, H, W, C);
     }
     return cudaGetLastError();
 }

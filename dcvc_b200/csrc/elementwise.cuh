@@ -41,6 +41,11 @@ cudaError_t launch_space_to_depth2(const __half* x, int H, int W, int C, int ldx
 cudaError_t launch_im2col3x3s2(const __half* x, int H, int W, int C, int ldx, __half* out,
                                cudaStream_t s);
 
+// out[(h, w), (ky*3 + kx)*C + c] = x[h+ky-1, w+kx-1, c] (zero outside): the patches of a 3x3
+// stride-1 pad-1 convolution (conv2d of the biased sub-pixel up-sampling, layers_proxy.cpp:269-276).
+cudaError_t launch_im2col3x3s1(const __half* x, int H, int W, int C, int ldx, __half* out,
+                               cudaStream_t s);
+
 // replicate_pad (cat_and_pad.cu:53-84): out [H+pb, W+pr, C] dense.
 cudaError_t launch_replicate_pad(const __half* x, int H, int W, int C, int ldx, int pad_b,
                                  int pad_r, __half* out, cudaStream_t s);
@@ -103,10 +108,11 @@ cudaError_t launch_build_index_dec_4x(int phase, const __half* scales, int lds, 
                                       uint8_t* cond, cudaStream_t s);
 
 // restore_y_4x* (stream.cu:757-860): part is the dense [H*W, C/4] FP16 step values; mode 0
-// writes y_hat, 1 accumulates, 3 accumulates and multiplies by the C scales q.
+// writes y_hat, 1 accumulates, 2 accumulates and multiplies by max(q, 0.5), 3 accumulates and
+// multiplies by q; q is [H*W, C] with pitch ldq (0: one row of C scales for every pixel).
 cudaError_t launch_restore_4x(int phase, int mode, const __half* part, const __half* means,
-                              int ldm, const __half* q, __half* y_hat, int ldh, int H, int W,
-                              int C, cudaStream_t s);
+                              int ldm, const __half* q, int ldq, __half* y_hat, int ldh, int H,
+                              int W, int C, cudaStream_t s);
 
 // Order-preserving compaction of `src` (elem_bytes 1 or 2) under `cond` (conditional_index_part1,
 // stream.cu:175-338).  block_counts needs compact_blocks(n) ints; *total (device) receives the

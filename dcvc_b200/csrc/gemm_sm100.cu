@@ -340,13 +340,28 @@ __global__ void __launch_bounds__(GemmCfg<BN, EPI>::kThreads, 1)
                         const size_t orow = static_cast<size_t>(2 * h + (sub >> 1)) * (2 * p.sub_w) +
                                             (2 * w + (sub & 1));
                         uint4* d4 = reinterpret_cast<uint4*>(reinterpret_cast<T*>(p.out) + orow * p.ldo + ch);
+                        float v[32];
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) {
+                            v[j] = __uint_as_float(r[j]);
+                        }
+                        if (p.bias != nullptr) {  // the biased form (SubpelConv2x with a bias)
+                            const float4* b4 = reinterpret_cast<const float4*>(p.bias + nc);
+#pragma unroll
+                            for (int j = 0; j < 8; ++j) {
+                                const float4 bb = __ldg(b4 + j);
+                                v[4 * j + 0] += bb.x;
+                                v[4 * j + 1] += bb.y;
+                                v[4 * j + 2] += bb.z;
+                                v[4 * j + 3] += bb.w;
+                            }
+                        }
 #pragma unroll
                         for (int j = 0; j < 4; ++j) {
-                            d4[j] = make_uint4(
-                                P::pack(__uint_as_float(r[8 * j + 0]), __uint_as_float(r[8 * j + 1])),
-                                P::pack(__uint_as_float(r[8 * j + 2]), __uint_as_float(r[8 * j + 3])),
-                                P::pack(__uint_as_float(r[8 * j + 4]), __uint_as_float(r[8 * j + 5])),
-                                P::pack(__uint_as_float(r[8 * j + 6]), __uint_as_float(r[8 * j + 7])));
+                            d4[j] = make_uint4(P::pack(v[8 * j + 0], v[8 * j + 1]),
+                                               P::pack(v[8 * j + 2], v[8 * j + 3]),
+                                               P::pack(v[8 * j + 4], v[8 * j + 5]),
+                                               P::pack(v[8 * j + 6], v[8 * j + 7]));
                         }
                     }
                 }

@@ -384,8 +384,8 @@ void IntraCodec::dec_step(Launch& L, int k)
     const int C2 = 2 * kChY;
     const __half* means_prev = (k == 1 ? params_ : sp_out_) + kChY;
     L.note(launch_recover(y_dec_, cond_, block_counts_, part_num_, part_, L.s));
-    L.note(launch_restore_4x(k - 1, k == 1 ? 0 : 1, part_, means_prev, C2, nullptr, cat_sp_, C2,
-                             H16_, W16_, kChY, L.s));
+    L.note(launch_restore_4x(k - 1, k == 1 ? 0 : 1, part_, means_prev, C2, nullptr, 0, cat_sp_,
+                             C2, H16_, W16_, kChY, L.s));
     spatial_prior(L, k);
     L.note(launch_build_index_dec_4x(k, sp_out_, C2, skip_thr_half_, scale_lut_, H16_, W16_, kChY,
                                      idx_, cond_, L.s));
@@ -397,8 +397,8 @@ void IntraCodec::dec_final(Launch& L)
 {
     const int C2 = 2 * kChY;
     L.note(launch_recover(y_dec_, cond_, block_counts_, part_num_, part_, L.s));
-    L.note(launch_restore_4x(kSteps - 1, 3, part_, sp_out_ + kChY, C2, q_y_dec_, cat_sp_, C2, H16_,
-                             W16_, kChY, L.s));
+    L.note(launch_restore_4x(kSteps - 1, 3, part_, sp_out_ + kChY, C2, q_y_dec_, 0, cat_sp_, C2,
+                             H16_, W16_, kChY, L.s));
     decoder(L);
 }
 

@@ -201,29 +201,54 @@ UpBlock ParamBuilder::up(const std::string& p, bool shortcut)
 Lin ParamBuilder::subpel(const std::string& p)
 {
     Lin b;
-    if (has(p + "conv.0.bias")) {
-        fail("'" + p + "conv.0' has a bias: only the bias-free sub-pixel up-sampling is supported");
-        return b;
-    }
     const HostTensor* w = get(p + "conv.0.weight", 2);
     if (w == nullptr) {
         return b;
     }
     const int n4 = static_cast<int>(w->shape[0]);
-    const int cin = static_cast<int>(w->numel() / n4);
+    const int kin = static_cast<int>(w->numel() / n4);  // cin (1x1) or 9 * cin (3x3)
     const int cout = n4 / 4;
-    // row c*4 + dy*2 + dx (pixel_shuffle order) -> (dy*2 + dx)*cout + c
-    std::vector<float> pw(static_cast<size_t>(n4) * cin);
+    const bool k3 = w->shape.size() == 4 && w->shape[2] == 3 && w->shape[3] == 3;
+    if (w->shape.size() == 4 && !k3 && (w->shape[2] != 1 || w->shape[3] != 1)) {
+        fail("'" + p + "conv.0.weight' is neither 1x1 nor 3x3");
+        return b;
+    }
+    const int cin = k3 ? kin / 9 : kin;
+    // row c*4 + dy*2 + dx (pixel_shuffle order) -> (dy*2 + dx)*cout + c; a 3x3 kernel's K axis
+    // [c][ky][kx] -> (ky*3 + kx)*cin + c to match the stride-1 patches
+    std::vector<float> pw(static_cast<size_t>(n4) * kin);
     for (int c = 0; c < cout; ++c) {
-        for (int s = 0; s < 4; ++s) {
-            std::copy(w->data.begin() + static_cast<size_t>(c * 4 + s) * cin,
-                      w->data.begin() + static_cast<size_t>(c * 4 + s + 1) * cin,
-                      pw.begin() + static_cast<size_t>(s * cout + c) * cin);
+        for (int s4 = 0; s4 < 4; ++s4) {
+            const float* src = w->data.data() + static_cast<size_t>(c * 4 + s4) * kin;
+            float* dst = pw.data() + static_cast<size_t>(s4 * cout + c) * kin;
+            if (!k3) {
+                std::copy(src, src + kin, dst);
+            } else {
+                for (int ci = 0; ci < cin; ++ci) {
+                    for (int t = 0; t < 9; ++t) {
+                        dst[t * cin + ci] = src[ci * 9 + t];
+                    }
+                }
+            }
         }
     }
-    b.cin = cin;
+    b.cin = kin;
     b.cout = n4;
     b.w = upload_half(pw);
+    if (has(p + "conv.0.bias")) {
+        const HostTensor* bias = get(p + "conv.0.bias");
+        if (bias == nullptr || bias->numel() != n4) {
+            fail("'" + p + "conv.0.bias' does not match its weight");
+            return b;
+        }
+        std::vector<float> pb(n4);
+        for (int c = 0; c < cout; ++c) {
+            for (int s4 = 0; s4 < 4; ++s4) {
+                pb[s4 * cout + c] = bias->data[c * 4 + s4];
+            }
+        }
+        b.b = upload_float(pb);
+    }
     return b;
 }
 

@@ -74,7 +74,8 @@ struct DownBlock {
     Dcb dcb;
 };
 
-// ResidualBlockUpsample without bias: 1x1 with rows permuted to (dy, dx, c) + shuffle store + DCB.
+// ResidualBlockUpsample: 1x1 (optionally biased) with rows permuted to (dy, dx, c) + shuffle
+// store + DCB.
 struct UpBlock {
     Lin up;
     Dcb dcb;
@@ -89,7 +90,9 @@ public:
     Dcb dcb(const std::string& prefix, bool shortcut = false);
     DownBlock down(const std::string& prefix, bool shortcut = false);
     UpBlock up(const std::string& prefix, bool shortcut = false);
-    Lin subpel(const std::string& prefix);  // prefix + "conv.0.weight", rows permuted
+    // SubpelConv2x (layers.py:92-103): prefix + "conv.0.{weight,bias}", 1x1 or 3x3 (K in
+    // (ky, kx, c) order), rows and bias permuted to (dy, dx, c)
+    Lin subpel(const std::string& prefix);
     Lin conv3x3s2(const std::string& prefix);  // weight K permuted to (ky, kx, c)
     const __half* half_rows(const std::string& name, int* rows, int* cols);
     bool ok() const { return err_.empty(); }

@@ -2,9 +2,9 @@
 inference/bind.cpp:11-39): the same proxy classes, methods, argument meaning and return values,
 backed by the sm_100a runtime in libdcvc_b200.so.
 
-DMCHTSProxy (the HT-S video model) and DMCIProxy (the intra model) are implemented.  DMCHTLProxy
-and DMCLDProxy raise NotImplementedError on construction (the models then report that the CUDA
-implementation is unavailable, as the reference does when its extension is missing,
+DMCHTSProxy and DMCHTLProxy (the HT-S and HT-L video models) and DMCIProxy (the intra model) are
+implemented.  DMCLDProxy raises NotImplementedError on construction (the model then reports that
+the CUDA implementation is unavailable, as the reference does when its extension is missing,
 video_model_ht.py:428-432).
 """
 import ctypes
@@ -25,22 +25,24 @@ def _proto(name, argtypes):
     return f
 
 
-_proto("dcvc_hts_create", [ctypes.POINTER(_vp)])
-_proto("dcvc_hts_destroy", [_vp])
-_proto("dcvc_hts_set_param", [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_char_p),
-                              ctypes.POINTER(_vp), ctypes.POINTER(ctypes.c_int64),
-                              ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
-                              ctypes.POINTER(ctypes.c_int), ctypes.c_float])
-_proto("dcvc_hts_add_ref_feature", [_vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp])
-_proto("dcvc_hts_compress", [_vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
-                             ctypes.c_int, ctypes.c_int, _vp, ctypes.POINTER(_vp),
-                             ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_int)])
-_proto("dcvc_hts_decompress", [_vp, _vp, ctypes.c_size_t, ctypes.c_int, ctypes.c_int, ctypes.c_int,
-                               ctypes.c_int, ctypes.c_int, _vp, ctypes.POINTER(_vp)])
-_proto("dcvc_hts_buffer", [_vp, ctypes.c_char_p, ctypes.POINTER(_vp), ctypes.POINTER(ctypes.c_int),
-                           ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)])
-_proto("dcvc_hts_stats", [_vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
-                          ctypes.POINTER(ctypes.c_size_t)])
+for _k in ("hts", "htl"):
+    _proto(f"dcvc_{_k}_create", [ctypes.POINTER(_vp)])
+    _proto(f"dcvc_{_k}_destroy", [_vp])
+    _proto(f"dcvc_{_k}_set_param", [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_char_p),
+                                     ctypes.POINTER(_vp), ctypes.POINTER(ctypes.c_int64),
+                                     ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                     ctypes.POINTER(ctypes.c_int), ctypes.c_float])
+    _proto(f"dcvc_{_k}_add_ref_feature", [_vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp])
+    _proto(f"dcvc_{_k}_compress", [_vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                    ctypes.c_int, ctypes.c_int, _vp, ctypes.POINTER(_vp),
+                                    ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_int)])
+    _proto(f"dcvc_{_k}_decompress", [_vp, _vp, ctypes.c_size_t, ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp,
+                                      ctypes.POINTER(_vp)])
+    _proto(f"dcvc_{_k}_buffer", [_vp, ctypes.c_char_p, ctypes.POINTER(_vp), ctypes.POINTER(ctypes.c_int),
+                                  ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)])
+    _proto(f"dcvc_{_k}_stats", [_vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                 ctypes.POINTER(ctypes.c_size_t)])
 _proto("dcvc_intra_create", [ctypes.POINTER(_vp)])
 _proto("dcvc_intra_destroy", [_vp])
 _proto("dcvc_intra_set_param", [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_char_p),
@@ -167,9 +169,9 @@ class DMCHTSProxy(_Proxy):
         frame = _channels_last_data(frame, "frame")
         if frame.shape[1] != 3:
             raise ValueError("frame must have 3 channels")
-        N.check(_lib.dcvc_hts_add_ref_feature(self._h, frame.data_ptr(), frame.shape[2],
-                                              frame.shape[3], 1 if apply_adaptor else 0,
-                                              _stream()), "add_ref_feature_from_frame")
+        N.check(self._fn("add_ref_feature")(self._h, frame.data_ptr(), frame.shape[2],
+                                            frame.shape[3], 1 if apply_adaptor else 0,
+                                            _stream()), "add_ref_feature_from_frame")
 
     def compress(self, x, qp, reset_feature_memory, padding_b, padding_r):
         """x: [1, 24, H, W] float16 CUDA (8 frames).  Returns (uint8 array, ec_parallel)."""
@@ -177,10 +179,10 @@ class DMCHTSProxy(_Proxy):
         data = _vp()
         size = ctypes.c_size_t()
         ecp = ctypes.c_int()
-        N.check(_lib.dcvc_hts_compress(self._h, x.data_ptr(), x.shape[2], x.shape[3], int(qp),
-                                       1 if reset_feature_memory else 0, int(padding_b),
-                                       int(padding_r), _stream(), ctypes.byref(data),
-                                       ctypes.byref(size), ctypes.byref(ecp)), "compress")
+        N.check(self._fn("compress")(self._h, x.data_ptr(), x.shape[2], x.shape[3], int(qp),
+                                     1 if reset_feature_memory else 0, int(padding_b),
+                                     int(padding_r), _stream(), ctypes.byref(data),
+                                     ctypes.byref(size), ctypes.byref(ecp)), "compress")
         return _bytes_out(data, size), ecp.value
 
     def decompress(self, bit_stream, qp, height, width, entropy_coder_parallel,
@@ -189,9 +191,9 @@ class DMCHTSProxy(_Proxy):
         buffers and are overwritten by the next call (dmc_hts_proxy.h:347)."""
         bs = np.ascontiguousarray(np.asarray(bit_stream, dtype=np.uint8).reshape(-1))
         frames = (_vp * FRAMES)()
-        N.check(_lib.dcvc_hts_decompress(self._h, bs.ctypes.data, bs.size, int(qp), int(height),
-                                         int(width), int(entropy_coder_parallel),
-                                         1 if reset_feature_memory else 0, _stream(), frames),
+        N.check(self._fn("decompress")(self._h, bs.ctypes.data, bs.size, int(qp), int(height),
+                                       int(width), int(entropy_coder_parallel),
+                                       1 if reset_feature_memory else 0, _stream(), frames),
                 "decompress")
         hp = (int(height) + 15) // 16 * 16
         wp = (int(width) + 15) // 16 * 16
@@ -201,6 +203,13 @@ class DMCHTSProxy(_Proxy):
             out.append(t.permute(0, 3, 1, 2))
         return out
 
+
+
+class DMCHTLProxy(DMCHTSProxy):
+    """Chunk codec of the HT-L video model (dmc_htl_proxy.h): the DMCHTSProxy interface, with
+    4-step entropy coding inside (bind.cpp:19-24)."""
+
+    _kind = "htl"
 
 
 class DMCIProxy(_Proxy):
@@ -243,10 +252,6 @@ class _Unavailable:
 
     def __init__(self, *a, **k):
         raise NotImplementedError(f"{self._what} is not implemented by dcvc_b200 yet")
-
-
-class DMCHTLProxy(_Unavailable):
-    _what = "DMCHTLProxy (HT-L model)"
 
 
 class DMCLDProxy(_Unavailable):

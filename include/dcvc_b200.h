@@ -228,6 +228,31 @@ int dcvc_hts_buffer(void* handle, const char* name, const void** ptr, int* rows,
 /* symbols coded by the last call, kernels it enqueued, device bytes held by the handle */
 int dcvc_hts_stats(void* handle, int* symbols, int* kernels, size_t* device_bytes);
 
+/* ------------------------------------------------------------------ HT-L chunk codec */
+
+/* The counterpart of DMCHTLProxy (src/layers/extensions/inference/dmc_htl_proxy.h, bind.cpp:
+ * 19-24), with the same arguments, ownership and stream rules as the dcvc_hts_* functions:
+ * set_param (dmc_htl_proxy.cpp:917-967), add_ref_feature_from_frame (:583-593), compress
+ * (:595-716; the payload holds the four checkerboard steps' y symbols in the order 3, 2, 1, 0,
+ * then z), decompress (:718-915). */
+int dcvc_htl_create(void** handle);
+int dcvc_htl_destroy(void* handle);
+int dcvc_htl_set_param(void* handle, int n, const char* const* names, const void* const* data,
+                       const int64_t* shapes, const int* ndims, const int* dtypes,
+                       const int* on_device, float skip_threshold);
+int dcvc_htl_add_ref_feature(void* handle, const void* frame, int height, int width,
+                             int apply_adaptor, void* stream);
+int dcvc_htl_compress(void* handle, const void* x, int height, int width, int qp, int reset,
+                      int pad_b, int pad_r, void* stream, const uint8_t** bytes, size_t* nbytes,
+                      int* ec_parallel);
+int dcvc_htl_decompress(void* handle, const uint8_t* bytes, size_t nbytes, int qp, int height,
+                        int width, int ec_parallel, int reset, void* stream, void** frames);
+/* Read-only view of a per-stream device buffer, as dcvc_hts_buffer; no counterpart in the
+ * reference. */
+int dcvc_htl_buffer(void* handle, const char* name, const void** ptr, int* rows, int* cols,
+                    int* ld);
+int dcvc_htl_stats(void* handle, int* symbols, int* kernels, size_t* device_bytes);
+
 /* ------------------------------------------------------------------ intra (DMCI) codec */
 
 /* One handle = one intra coder, the counterpart of DMCIProxy

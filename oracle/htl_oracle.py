@@ -140,7 +140,9 @@ class HtlOracle(HtsOracle):
         Hp, Wp = (height + 15) // 16 * 16, (width + 15) // 16 * 16
         H16, W16 = Hp // 16, Wp // 16
         H64, W64 = (height + 63) // 64, (width + 63) // 64
-        if self.memory_has_value:
+        if getattr(self, "_memory_ready", False):
+            self._memory_ready = False
+        elif self.memory_has_value:
             self.memory = self.feature_adaptor_m(self.memory, self.feature_p)
         else:
             self.memory = self.feature_adaptor_i(self.feature_i)

@@ -377,6 +377,13 @@ class HtsOracle:
         return common, torch.clamp_min(q_dec, 0.5), scales, means
 
     # ---- public API mirroring DMCHTSProxy
+    def set_temporal_state(self, memory):
+        """Tests: the temporal memory the next chunk is coded with (already updated, e.g. read
+        from the GPU codec), the same on an encoder and on a decoder instance."""
+        self.memory = memory.to(self.dtype)
+        self.ctx = self.feature_extractor(self.memory)
+        self._memory_ready = True
+
     def add_ref_feature_from_frame(self, frame, apply_adaptor=True):
         self.feature_i = F.pixel_unshuffle(frame.to("cpu", self.dtype), 8)
         if apply_adaptor:
@@ -439,7 +446,9 @@ class HtsOracle:
         Hp, Wp = (height + 15) // 16 * 16, (width + 15) // 16 * 16
         H16, W16 = Hp // 16, Wp // 16
         H64, W64 = (height + 63) // 64, (width + 63) // 64
-        if self.memory_has_value:
+        if getattr(self, "_memory_ready", False):
+            self._memory_ready = False
+        elif self.memory_has_value:
             self.memory = self.feature_adaptor_m(self.memory, self.feature_p)
         else:
             self.memory = self.feature_adaptor_i(self.feature_i)
