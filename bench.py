@@ -50,6 +50,7 @@ def parse_args():
     ap.add_argument("--width", type=int, default=1920)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-intra", action="store_true", help="skip the intra-codec measurement")
+    ap.add_argument("--no-htl", action="store_true", help="skip the HT-L measurement")
     ap.add_argument("--streams", type=int, default=4,
                     help="concurrent streams of the batched form (0 skips it)")
     return ap.parse_args()
@@ -358,6 +359,49 @@ def split_enc_dec(enc, dec, xs, args, pb, pr, H, W, stream):
             "chunks": n, "note": "device-timed, inputs resident; compare reference_published"}
 
 
+def htl_bench(stream, H, W, chunks=8, warmup=3):
+    """The HT-L model (DMCHTLProxy): encode-only and decode-only frames/s of 1080p chunks, QPs
+    cycling as in the main workload; the reference publishes these for B200."""
+    from dcvc_b200 import synthetic
+    from dcvc_b200.entropy_tables import add_cdf_to_state_dict
+    from dcvc_b200.inference_extensions_cuda import DMCHTLProxy
+    from dcvc_b200.model_spec import calibrated_htl_state_dict
+    sd = add_cdf_to_state_dict(calibrated_htl_state_dict(0))
+    sd = {k: (v.half().cuda() if v.is_floating_point() else v) for k, v in sd.items()}
+    enc, dec = DMCHTLProxy(), DMCHTLProxy()
+    enc.set_param(sd, SKIP_THRES)
+    dec.set_param(sd, SKIP_THRES)
+    del sd
+    ref = synthetic.padded_reference_frame(synthetic.video_chunk_yuv420(2, H, W, 1, 0)[0])
+    enc.add_ref_feature_from_frame(ref, True)
+    dec.add_ref_feature_from_frame(ref, False)
+    pr, pb = synthetic.padding_for(H, W)
+    xs = [synthetic.to_model_input(synthetic.video_chunk_yuv420(2, H, W, FRAMES, FRAMES * k))
+          for k in range(2)]
+    for i in range(warmup):
+        qp = QPS[i % len(QPS)]
+        bits, ecp = enc.compress(xs[i % 2], qp, False, pb, pr)
+        dec.decompress(bits, qp, H, W, ecp, False)
+    torch.cuda.synchronize()
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    payloads = []
+    e[0].record(stream)
+    for i in range(chunks):
+        qp = QPS[i % len(QPS)]
+        bits, ecp = enc.compress(xs[i % 2], qp, False, pb, pr)
+        payloads.append((bits, qp, ecp))
+    e[1].record(stream)
+    for bits, qp, ecp in payloads:
+        dec.decompress(bits, qp, H, W, ecp, False)
+    e[2].record(stream)
+    torch.cuda.synchronize()
+    te, td = e[0].elapsed_time(e[1]) / chunks, e[1].elapsed_time(e[2]) / chunks
+    return {"enc_fps": round(FRAMES * 1e3 / te, 1), "dec_fps": round(FRAMES * 1e3 / td, 1),
+            "enc_ms_per_chunk": round(te, 3), "dec_ms_per_chunk": round(td, 3),
+            "bytes_per_chunk": int(np.mean([p[0].size for p in payloads])), "chunks": chunks,
+            "reference_published": {"enc_fps_b200": 811.7, "dec_fps_b200": 551.6}}
+
+
 def intra_bench(stream, H, W, reps=10):
     """The intra (DMCI) codec: encode-only and decode-only frames/s at the bench resolution and
     at 256x256 (the reference's CPU-runnable intra case), QP 32."""
@@ -516,6 +560,7 @@ def run_gpu(args):
     clk = clocks.stop(windows)
     roof = roofline_quad(stream)
     intra = None if args.no_intra else intra_bench(stream, H, W)
+    htl = None if args.no_htl else htl_bench(stream, H, W)
     del enc, dec
     torch.cuda.empty_cache()
     batched = batched_streams(args, H, W, args.streams) if args.streams > 0 else None
@@ -540,6 +585,7 @@ def run_gpu(args):
         "batched": batched,
         "reference_published": PUBLISHED,
         "intra": intra,
+        "htl": htl,
         "e2e": {"value": round(e2e, 2), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": kernels_per_step * args.steps,
         "roofline": roof,
