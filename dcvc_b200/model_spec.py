@@ -201,6 +201,70 @@ def perturbed_htl_state_dict(seed=0, dtype=torch.float32, q_jitter=0.25, calibra
     return {k: v.to(dtype) for k, v in sd.items()}
 
 
+# LD model sizes (video_model_ld.py:11-16)
+LD_CH_Y, LD_CH_Z, LD_CH_D, LD_CH_M = 128, 128, 256, 256
+
+
+class LDModel(nn.Module):
+    """Parameter tree of the low-delay model DMC (video_model_ld.py:18-213): one frame per call,
+    dcb2 DepthConvBlocks, resampling blocks without shortcut, a means-only spatial prior."""
+
+    def __init__(self):
+        super().__init__()
+        y, z, dd, m = LD_CH_Y, LD_CH_Z, LD_CH_D, LD_CH_M
+        d = lambda i, o: DCB(i, o, dcb2=True)  # noqa: E731
+        self.bit_estimator_z = BitEstimator(QP_NUM, z)
+        self.feature_adaptor_i = _Wrap(conv=_seq(d(CH_SRC_INTRA, m), d(m, m), d(m, m), d(m, m)))
+        self.feature_adaptor_m = _Wrap(conv=_seq(d(m + dd, m), d(m, m), d(m, m), d(m, m)))
+        self.feature_extractor = _Wrap(conv=_seq(*[d(m, m) for _ in range(5)]))
+        enc = _Wrap(conv1=_seq(d(CH_SRC_INTRA + m, dd), d(dd, dd)))
+        enc.conv2 = d(dd, dd)
+        enc.down = nn.Conv2d(dd, y, 3, stride=2, padding=1)
+        self.encoder = enc
+        self.hyper_encoder = _Wrap(conv=_seq(d(y, z), RBDown(z, z, dcb2=True), RBDown(z, z, dcb2=True)))
+        self.hyper_decoder = _Wrap(conv=_seq(RBUp(z, z, dcb2=True), RBUp(z, z, dcb2=True), d(z, y)))
+        self.temporal_prior_encoder = _Wrap(conv=RBDown(m, y * 2, dcb2=True))
+        self.y_prior_fusion = _Wrap(conv=_seq(d(y * 3, y * 3), d(y * 3, y * 3), d(y * 3, y * 3),
+                                              nn.Conv2d(y * 3, y * 3, 1)))
+        self.y_spatial_prior = _Wrap(conv=_seq(d(y * 4, y * 2), d(y * 2, y * 2), nn.Conv2d(y * 2, y, 1)))
+        dec = _Wrap(up=Subpel(y, dd, 1))
+        dec.conv1 = _seq(d(dd + m, dd), d(dd, dd), d(dd, dd))
+        dec.conv2 = nn.Conv2d(dd, dd, 1)
+        self.decoder = dec
+        rh = _Wrap(conv=_seq(d(dd, dd), d(dd, dd), d(dd, dd)))
+        rh.head = nn.Conv2d(dd, CH_SRC_INTRA, 1)
+        self.recon_head = rh
+        self.q_encoder = nn.Parameter(torch.ones((QP_NUM, dd)))
+        self.q_decoder = nn.Parameter(torch.ones((QP_NUM, dd)))
+        self.q_feature = nn.Parameter(torch.ones((QP_NUM, y * 2)))
+        _init_xavier(self)
+
+
+def ld_state_dict(seed=0, dtype=torch.float32):
+    """State dict of a random-init LD model, equal to the reference video_model_ld.DMC() under
+    torch.manual_seed(seed) (fp32 CPU; cast to `dtype`)."""
+    return _seeded(LDModel, seed, dtype)
+
+
+def calibrated_ld_state_dict(seed=0, dtype=torch.float32, alpha=CALIBRATION_ALPHA):
+    """The seed-`seed` LD weights with the residual-branch output convolutions scaled by
+    `alpha` (see calibrated_hts_state_dict)."""
+    sd = ld_state_dict(seed, torch.float32)
+    for k in list(sd):
+        if k.endswith(("dc.3.weight", "ffn.2.weight")):
+            sd[k] = sd[k] * alpha
+    return {k: v.to(dtype) for k, v in sd.items()}
+
+
+def perturbed_ld_state_dict(seed=0, dtype=torch.float32, q_jitter=0.25, calibrated=True):
+    """Seed-`seed` LD weights with non-trivial per-QP quant vectors."""
+    sd = calibrated_ld_state_dict(seed) if calibrated else ld_state_dict(seed, torch.float32)
+    g = torch.Generator().manual_seed(seed + 29)
+    for k in ("q_encoder", "q_decoder", "q_feature"):
+        sd[k] = 1.0 + q_jitter * (torch.rand(sd[k].shape, generator=g) * 2 - 1)
+    return {k: v.to(dtype) for k, v in sd.items()}
+
+
 class DMCIModel(nn.Module):
     """Parameter tree of DMCI, the intra model (image_model.py:15-140).  Its resampling blocks
     keep the reference's default shortcut (layers.py:162-188), which has no parameters."""

@@ -1,0 +1,83 @@
+"""Generates the LD-model golden fixtures under tests/golden/ from the reference itself.
+
+Run here, where the reference sources exist (default /root/reference):
+
+    python tests/golden/make_ld_golden.py [--ref /root/reference]
+
+Outputs (small, committed):
+  weights_ld_seed0.json   fingerprints of the reference video_model_ld.DMC() state dict for
+                          torch.manual_seed(0)
+  ld_modules_golden.npz   reference LD sub-network outputs for seeded inputs (float64)
+"""
+import argparse
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+# 64 x 128 frames: H8 x W8 = 8 x 16, y level 4 x 8, z level 1 x 2
+H, W = 64, 128
+
+
+def ld_module_inputs():
+    import torch
+    g = torch.Generator().manual_seed(2027)
+    r = lambda *s: torch.rand(*s, generator=g, dtype=torch.float64)  # noqa: E731
+    h8, w8 = H // 8, W // 8
+    return {
+        "x": r(1, 3, H, W) - 0.5,
+        "ctx": r(1, 256, h8, w8) * 2 - 1,
+        "memory": r(1, 256, h8, w8) * 2 - 1,
+        "feature": r(1, 256, h8, w8) * 2 - 1,
+        "feature_i": r(1, 192, h8, w8) - 0.5,
+        "q_enc": r(1, 256, 1, 1) + 0.5,
+        "q_dec": r(1, 256, 1, 1) + 0.5,
+        "q_feat": r(1, 256, 1, 1) + 0.5,
+        "z_hat": torch.round((r(1, 128, h8 // 8, w8 // 8) - 0.5) * 8),
+        "y_hat": (r(1, 128, h8 // 2, w8 // 2) - 0.5) * 4,
+        "params": r(1, 384, h8 // 2, w8 // 2) * 2 - 1,
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default="/root/reference")
+    args = ap.parse_args()
+    sys.path.insert(0, args.ref)
+    import torch
+    from src.models.video_model_ld import DMC
+    from make_golden import fingerprint
+
+    torch.manual_seed(0)
+    model = DMC()
+    sd = {k: v.clone() for k, v in model.state_dict().items()}
+    with open(os.path.join(HERE, "weights_ld_seed0.json"), "w") as f:
+        json.dump(fingerprint(sd), f)
+    m = model.double().eval()
+    inp = ld_module_inputs()
+    out = {}
+    with torch.no_grad():
+        out["encoder"] = m.encoder(inp["x"], inp["ctx"], inp["q_enc"])
+        out["hyper_encoder"] = m.hyper_encoder(out["encoder"])
+        out["hyper_decoder"] = m.hyper_decoder(inp["z_hat"])
+        out["temporal_prior_encoder"] = m.temporal_prior_encoder(inp["memory"])
+        out["prior_fusion"] = m.y_prior_fusion(out["hyper_decoder"], out["temporal_prior_encoder"],
+                                               inp["q_feat"])
+        out["spatial_prior"] = m.y_spatial_prior(inp["y_hat"], inp["params"])
+        out["decoder"] = m.decoder(inp["y_hat"], inp["ctx"], inp["q_dec"])
+        out["recon"] = m.recon_head(inp["feature"])
+        out["recon_reset"] = m.recon_head(inp["feature"], for_reset=True)
+        out["feature_adaptor_i"] = m.feature_adaptor_i(inp["feature_i"])
+        out["feature_adaptor_m"] = m.feature_adaptor_m(inp["memory"], inp["feature"])
+        out["feature_extractor"] = m.feature_extractor(inp["memory"])
+    np.savez_compressed(os.path.join(HERE, "ld_modules_golden.npz"),
+                        **{k: v.float().numpy() for k, v in out.items()})
+    print("LD golden fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    sys.path.insert(0, HERE)
+    main()
