@@ -251,8 +251,20 @@ __global__ void div_clamp_kernel(__half* __restrict__ y, int M, int C, int ldy,
 
 // ------------------------------------------------------------------------------ quantisation
 
+// Whether channel vector v (of `vecs`) at (h, w) is coded in mask phase `phase`: the 4-phase masks
+// (get_mask_4x, common_model.py:175-195) or, with groups == 2, the 2-phase checkerboard
+// (get_mask_2x, common_model.py:157-172: channel half g at the positions with h + w + g + phase
+// even).
+__device__ __forceinline__ bool mask_on(int groups, int phase, int h, int w, int v, int vecs)
+{
+    if (groups == 2) {
+        return ((h + w + v / (vecs / 2) + phase) & 1) == 0;
+    }
+    return ((h & 1) * 2 + (w & 1)) == mask_position(phase, v / (vecs / 4));
+}
+
 template <int MODE>
-__global__ void quantize_phase_kernel(int phase, const __half* __restrict__ y, int ldy,
+__global__ void quantize_phase_kernel(int groups, int phase, const __half* __restrict__ y, int ldy,
                                       const __half* __restrict__ scales, int lds,
                                       const __half* __restrict__ means, int ldm,
                                       const __half* __restrict__ q_dec, int ldd, __half thr,
@@ -262,7 +274,6 @@ __global__ void quantize_phase_kernel(int phase, const __half* __restrict__ y, i
     griddep_launch_dependents();
     griddep_wait();
     const int vecs = C / 8;
-    const int quarter_vecs = vecs / 4;
     const long long total = static_cast<long long>(H) * W * vecs;
     const __half qmin = __float2half_rn(-128.f), qmax = __float2half_rn(127.f);
     const __half half_ = __float2half_rn(0.5f);
@@ -272,7 +283,7 @@ __global__ void quantize_phase_kernel(int phase, const __half* __restrict__ y, i
         const int v = static_cast<int>(i - m * vecs);
         const int h = static_cast<int>(m / W);
         const int w = static_cast<int>(m - static_cast<long long>(h) * W);
-        const bool on = ((h & 1) * 2 + (w & 1)) == mask_position(phase, v / quarter_vecs);
+        const bool on = mask_on(groups, phase, h, w, v, vecs);
         const Vec8h yy = ld8(y + m * ldy + v * 8);
         const Vec8h ss = ld8(scales + m * lds + v * 8);
         const Vec8h mm = ld8(means + m * ldm + v * 8);
@@ -314,7 +325,7 @@ __global__ void quantize_phase_kernel(int phase, const __half* __restrict__ y, i
 }
 
 template <int MODE>
-__global__ void restore_phase_kernel(int phase, const __half* __restrict__ y_q, int ldq,
+__global__ void restore_phase_kernel(int groups, int phase, const __half* __restrict__ y_q, int ldq,
                                      const __half* __restrict__ means, int ldm,
                                      const __half* __restrict__ q_dec, int ldd,
                                      __half* __restrict__ y_hat, int ldh, int H, int W, int C)
@@ -322,7 +333,6 @@ __global__ void restore_phase_kernel(int phase, const __half* __restrict__ y_q, 
     griddep_launch_dependents();
     griddep_wait();
     const int vecs = C / 8;
-    const int quarter_vecs = vecs / 4;
     const long long total = static_cast<long long>(H) * W * vecs;
     const __half half_ = __float2half_rn(0.5f);
     for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
@@ -331,7 +341,7 @@ __global__ void restore_phase_kernel(int phase, const __half* __restrict__ y_q, 
         const int v = static_cast<int>(i - m * vecs);
         const int h = static_cast<int>(m / W);
         const int w = static_cast<int>(m - static_cast<long long>(h) * W);
-        const bool on = ((h & 1) * 2 + (w & 1)) == mask_position(phase, v / quarter_vecs);
+        const bool on = mask_on(groups, phase, h, w, v, vecs);
         const Vec8h qq = ld8(y_q + m * ldq + v * 8);
         const Vec8h mm = ld8(means + m * ldm + v * 8);
         Vec8h prev, qd, o;
@@ -904,26 +914,26 @@ cudaError_t launch_quantize_phase(int phase, int mode, const __half* y, int ldy,
                                   const __half* scales, int lds, const __half* means, int ldm,
                                   const __half* q_dec, int ldd, __half thr, __half* y_q,
                                   int ldq, __half* y_hat, int ldh, int H, int W, int C,
-                                  cudaStream_t s)
+                                  cudaStream_t s, int groups)
 {
-    if (phase < 0 || phase > 3 || C % 32 || (mode >= 2 && q_dec == nullptr) || mode < 0 ||
+    if ((groups != 2 && groups != 4) || phase < 0 || phase >= groups || C % (8 * groups) || (mode >= 2 && q_dec == nullptr) || mode < 0 ||
         mode > 3) {
         return cudaErrorInvalidValue;
     }
     const int g = grid_for(static_cast<long long>(H) * W * (C / 8));
     if (mode == 3) {
-        launch_pdl(quantize_phase_kernel<3>, dim3(g), dim3(kThreads), 0, s, phase, y, ldy, scales,
+        launch_pdl(quantize_phase_kernel<3>, dim3(g), dim3(kThreads), 0, s, groups, phase, y, ldy, scales,
                    lds, means, ldm, q_dec, ldd, thr, y_q, ldq, y_hat, ldh, H, W, C);
     } else if (mode == 0) {
-        launch_pdl(quantize_phase_kernel<0>, dim3(g), dim3(kThreads), 0, s, phase, y, ldy, scales, lds, means, ldm,
+        launch_pdl(quantize_phase_kernel<0>, dim3(g), dim3(kThreads), 0, s, groups, phase, y, ldy, scales, lds, means, ldm,
                                                         q_dec, ldd, thr, y_q, ldq, y_hat, ldh, H,
                                                         W, C);
     } else if (mode == 1) {
-        launch_pdl(quantize_phase_kernel<1>, dim3(g), dim3(kThreads), 0, s, phase, y, ldy, scales, lds, means, ldm,
+        launch_pdl(quantize_phase_kernel<1>, dim3(g), dim3(kThreads), 0, s, groups, phase, y, ldy, scales, lds, means, ldm,
                                                         q_dec, ldd, thr, y_q, ldq, y_hat, ldh, H,
                                                         W, C);
     } else {
-        launch_pdl(quantize_phase_kernel<2>, dim3(g), dim3(kThreads), 0, s, phase, y, ldy, scales, lds, means, ldm,
+        launch_pdl(quantize_phase_kernel<2>, dim3(g), dim3(kThreads), 0, s, groups, phase, y, ldy, scales, lds, means, ldm,
                                                         q_dec, ldd, thr, y_q, ldq, y_hat, ldh, H,
                                                         W, C);
     }
@@ -932,21 +942,22 @@ cudaError_t launch_quantize_phase(int phase, int mode, const __half* y, int ldy,
 
 cudaError_t launch_restore_phase(int phase, int mode, const __half* y_q, int ldq,
                                  const __half* means, int ldm, const __half* q_dec, int ldd,
-                                 __half* y_hat, int ldh, int H, int W, int C, cudaStream_t s)
+                                 __half* y_hat, int ldh, int H, int W, int C, cudaStream_t s,
+                                 int groups)
 {
-    if (phase < 0 || phase > 3 || C % 32 || (mode == 2 && q_dec == nullptr) || mode < 0 ||
+    if ((groups != 2 && groups != 4) || phase < 0 || phase >= groups || C % (8 * groups) || (mode == 2 && q_dec == nullptr) || mode < 0 ||
         mode > 2) {
         return cudaErrorInvalidValue;
     }
     const int g = grid_for(static_cast<long long>(H) * W * (C / 8));
     if (mode == 0) {
-        launch_pdl(restore_phase_kernel<0>, dim3(g), dim3(kThreads), 0, s, phase, y_q, ldq, means, ldm, q_dec, ldd,
+        launch_pdl(restore_phase_kernel<0>, dim3(g), dim3(kThreads), 0, s, groups, phase, y_q, ldq, means, ldm, q_dec, ldd,
                                                        y_hat, ldh, H, W, C);
     } else if (mode == 1) {
-        launch_pdl(restore_phase_kernel<1>, dim3(g), dim3(kThreads), 0, s, phase, y_q, ldq, means, ldm, q_dec, ldd,
+        launch_pdl(restore_phase_kernel<1>, dim3(g), dim3(kThreads), 0, s, groups, phase, y_q, ldq, means, ldm, q_dec, ldd,
                                                        y_hat, ldh, H, W, C);
     } else {
-        launch_pdl(restore_phase_kernel<2>, dim3(g), dim3(kThreads), 0, s, phase, y_q, ldq, means, ldm, q_dec, ldd,
+        launch_pdl(restore_phase_kernel<2>, dim3(g), dim3(kThreads), 0, s, groups, phase, y_q, ldq, means, ldm, q_dec, ldd,
                                                        y_hat, ldh, H, W, C);
     }
     return cudaGetLastError();

@@ -73,16 +73,19 @@ cudaError_t launch_div_clamp(__half* y, int M, int C, int ldy, const __half* q, 
 // mask phase `phase` on an H x W grid.  mode 0: write y_q / y_hat; 1: accumulate;
 // 2: accumulate and scale y_hat by max(q_dec, 0.5); 3: accumulate and scale y_hat by q_dec
 // (add_and_multiply_broadcast, stream.cu:8-37: with ldd = 0, q_dec is one row of C scales).
+// groups = 4: the 4-phase masks; groups = 2: the 2-phase checkerboard of the LD model
+// (phase p codes channel half g where h + w + g + p is even).
 cudaError_t launch_quantize_phase(int phase, int mode, const __half* y, int ldy,
                                   const __half* scales, int lds, const __half* means, int ldm,
                                   const __half* q_dec, int ldd, __half thr, __half* y_q,
                                   int ldq, __half* y_hat, int ldh, int H, int W, int C,
-                                  cudaStream_t s);
+                                  cudaStream_t s, int groups = 4);
 
 // restore_y[_and_add_inplace][_and_add_multiply_inplace] (stream.cu:685-760).
 cudaError_t launch_restore_phase(int phase, int mode, const __half* y_q, int ldq,
                                  const __half* means, int ldm, const __half* q_dec, int ldd,
-                                 __half* y_hat, int ldh, int H, int W, int C, cudaStream_t s);
+                                 __half* y_hat, int ldh, int H, int W, int C, cudaStream_t s,
+                                 int groups = 4);
 
 // build_index_enc (stream.cu:126-173): sym[m*C + c] = (q << 8) + idx, cond = scale > thr, in
 // NHWC symbol order.  idx comes from the 65536-entry table `lut` indexed by the FP16 bits of the

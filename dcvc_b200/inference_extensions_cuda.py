@@ -2,10 +2,8 @@
 inference/bind.cpp:11-39): the same proxy classes, methods, argument meaning and return values,
 backed by the sm_100a runtime in libdcvc_b200.so.
 
-DMCHTSProxy and DMCHTLProxy (the HT-S and HT-L video models) and DMCIProxy (the intra model) are
-implemented.  DMCLDProxy raises NotImplementedError on construction (the model then reports that
-the CUDA implementation is unavailable, as the reference does when its extension is missing,
-video_model_ht.py:428-432).
+DMCHTSProxy and DMCHTLProxy (the HT-S and HT-L chunk codecs), DMCLDProxy (the low-delay frame
+codec) and DMCIProxy (the intra model) are all implemented.
 """
 import ctypes
 
@@ -25,7 +23,7 @@ def _proto(name, argtypes):
     return f
 
 
-for _k in ("hts", "htl"):
+for _k in ("hts", "htl", "ld"):
     _proto(f"dcvc_{_k}_create", [ctypes.POINTER(_vp)])
     _proto(f"dcvc_{_k}_destroy", [_vp])
     _proto(f"dcvc_{_k}_set_param", [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_char_p),
@@ -247,12 +245,29 @@ class DMCIProxy(_Proxy):
         return x_hat.permute(0, 3, 1, 2)
 
 
-class _Unavailable:
-    _what = "this proxy"
+class DMCLDProxy(DMCHTSProxy):
+    """Low-delay frame codec (dmc_ld_proxy.h, bind.cpp:33-38): the DMCHTSProxy interface on one
+    frame per call.  Not re-entrant."""
 
-    def __init__(self, *a, **k):
-        raise NotImplementedError(f"{self._what} is not implemented by dcvc_b200 yet")
+    _kind = "ld"
 
+    def compress(self, x, qp, reset_feature_memory, padding_b, padding_r):
+        """x: [1, 3, H, W] float16 CUDA.  Returns (uint8 array, ec_parallel)."""
+        if x.dim() != 4 or x.shape[1] != 3:
+            raise ValueError("x must be a [1, 3, H, W] tensor")
+        return super().compress(x, qp, reset_feature_memory, padding_b, padding_r)
 
-class DMCLDProxy(_Unavailable):
-    _what = "DMCLDProxy (LD model)"
+    def decompress(self, bit_stream, qp, height, width, entropy_coder_parallel,
+                   reset_feature_memory):
+        """Returns the [1, 3, Hp, Wp] float16 reconstruction (channels last), aliasing the
+        proxy's buffer (overwritten by the next call)."""
+        bs = np.ascontiguousarray(np.asarray(bit_stream, dtype=np.uint8).reshape(-1))
+        xh = _vp()
+        N.check(self._fn("decompress")(self._h, bs.ctypes.data, bs.size, int(qp), int(height),
+                                       int(width), int(entropy_coder_parallel),
+                                       1 if reset_feature_memory else 0, _stream(), ctypes.byref(xh)),
+                "decompress")
+        hp = (int(height) + 15) // 16 * 16
+        wp = (int(width) + 15) // 16 * 16
+        x_hat = torch.as_tensor(_DeviceView(xh.value, (1, hp, wp, 3)), device="cuda")
+        return x_hat.permute(0, 3, 1, 2)

@@ -253,6 +253,32 @@ int dcvc_htl_buffer(void* handle, const char* name, const void** ptr, int* rows,
                     int* ld);
 int dcvc_htl_stats(void* handle, int* symbols, int* kernels, size_t* device_bytes);
 
+/* ------------------------------------------------------------------ low-delay (LD) codec */
+
+/* The counterpart of DMCLDProxy (src/layers/extensions/inference/dmc_ld_proxy.h, bind.cpp:
+ * 33-38), one frame per call, with the same arguments, ownership and stream rules as the
+ * dcvc_hts_* functions: set_param (dmc_ld_proxy.cpp:595-637), add_ref_feature_from_frame
+ * (:407-418), compress (:420-485; x = [height, width, 3] FP16, the payload holds the y symbols of
+ * both checkerboard phases as one segment, then z), decompress (:487-593; *frame receives one
+ * device frame [Hp, Wp, 3] FP16 owned by the handle, valid until the next call on it). */
+int dcvc_ld_create(void** handle);
+int dcvc_ld_destroy(void* handle);
+int dcvc_ld_set_param(void* handle, int n, const char* const* names, const void* const* data,
+                      const int64_t* shapes, const int* ndims, const int* dtypes,
+                      const int* on_device, float skip_threshold);
+int dcvc_ld_add_ref_feature(void* handle, const void* frame, int height, int width,
+                            int apply_adaptor, void* stream);
+int dcvc_ld_compress(void* handle, const void* x, int height, int width, int qp, int reset,
+                     int pad_b, int pad_r, void* stream, const uint8_t** bytes, size_t* nbytes,
+                     int* ec_parallel);
+int dcvc_ld_decompress(void* handle, const uint8_t* bytes, size_t nbytes, int qp, int height,
+                       int width, int ec_parallel, int reset, void* stream, void** frame);
+/* Read-only view of a per-stream device buffer, as dcvc_hts_buffer ("temporal" adds the
+ * temporal-prior parameters); no counterpart in the reference. */
+int dcvc_ld_buffer(void* handle, const char* name, const void** ptr, int* rows, int* cols,
+                   int* ld);
+int dcvc_ld_stats(void* handle, int* symbols, int* kernels, size_t* device_bytes);
+
 /* ------------------------------------------------------------------ intra (DMCI) codec */
 
 /* One handle = one intra coder, the counterpart of DMCIProxy
