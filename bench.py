@@ -51,6 +51,7 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-intra", action="store_true", help="skip the intra-codec measurement")
     ap.add_argument("--no-htl", action="store_true", help="skip the HT-L measurement")
+    ap.add_argument("--no-ld", action="store_true", help="skip the low-delay (LD) measurement")
     ap.add_argument("--streams", type=int, default=4,
                     help="concurrent streams of the batched form (0 skips it)")
     return ap.parse_args()
@@ -402,6 +403,49 @@ def htl_bench(stream, H, W, chunks=8, warmup=3):
             "reference_published": {"enc_fps_b200": 811.7, "dec_fps_b200": 551.6}}
 
 
+def ld_bench(stream, H, W, frames=32, warmup=4):
+    """The low-delay model (DMCLDProxy): encode-only and decode-only frames/s at 1080p, one frame
+    per call, QPs cycling as in the main workload; the reference publishes these for B200."""
+    from dcvc_b200 import synthetic
+    from dcvc_b200.entropy_tables import add_cdf_to_state_dict
+    from dcvc_b200.inference_extensions_cuda import DMCLDProxy
+    from dcvc_b200.model_spec import calibrated_ld_state_dict
+    sd = add_cdf_to_state_dict(calibrated_ld_state_dict(0))
+    sd = {k: (v.half().cuda() if v.is_floating_point() else v) for k, v in sd.items()}
+    enc, dec = DMCLDProxy(), DMCLDProxy()
+    enc.set_param(sd, SKIP_THRES)
+    dec.set_param(sd, SKIP_THRES)
+    del sd
+    yuv = synthetic.video_chunk_yuv420(2, H, W, FRAMES + 1, 0)
+    ref = synthetic.padded_reference_frame(yuv[0])
+    enc.add_ref_feature_from_frame(ref, True)
+    dec.add_ref_feature_from_frame(ref, False)
+    pr, pb = synthetic.padding_for(H, W)
+    xs = [synthetic.to_model_input([f]) for f in yuv[1:]]
+    for i in range(warmup):
+        qp = QPS[i % len(QPS)]
+        bits, ecp = enc.compress(xs[i % len(xs)], qp, False, pb, pr)
+        dec.decompress(bits, qp, H, W, ecp, False)
+    torch.cuda.synchronize()
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    payloads = []
+    e[0].record(stream)
+    for i in range(frames):
+        qp = QPS[i % len(QPS)]
+        bits, ecp = enc.compress(xs[i % len(xs)], qp, False, pb, pr)
+        payloads.append((bits, qp, ecp))
+    e[1].record(stream)
+    for bits, qp, ecp in payloads:
+        dec.decompress(bits, qp, H, W, ecp, False)
+    e[2].record(stream)
+    torch.cuda.synchronize()
+    te, td = e[0].elapsed_time(e[1]) / frames, e[1].elapsed_time(e[2]) / frames
+    return {"enc_fps": round(1e3 / te, 1), "dec_fps": round(1e3 / td, 1),
+            "enc_ms_per_frame": round(te, 3), "dec_ms_per_frame": round(td, 3),
+            "bytes_per_frame": int(np.mean([p[0].size for p in payloads])), "frames": frames,
+            "reference_published": {"enc_fps_b200": 625.6, "dec_fps_b200": 621.9}}
+
+
 def intra_bench(stream, H, W, reps=10):
     """The intra (DMCI) codec: encode-only and decode-only frames/s at the bench resolution and
     at 256x256 (the reference's CPU-runnable intra case), QP 32."""
@@ -561,6 +605,7 @@ def run_gpu(args):
     roof = roofline_quad(stream)
     intra = None if args.no_intra else intra_bench(stream, H, W)
     htl = None if args.no_htl else htl_bench(stream, H, W)
+    ld = None if args.no_ld else ld_bench(stream, H, W)
     del enc, dec
     torch.cuda.empty_cache()
     batched = batched_streams(args, H, W, args.streams) if args.streams > 0 else None
@@ -586,6 +631,7 @@ def run_gpu(args):
         "reference_published": PUBLISHED,
         "intra": intra,
         "htl": htl,
+        "ld": ld,
         "e2e": {"value": round(e2e, 2), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": kernels_per_step * args.steps,
         "roofline": roof,

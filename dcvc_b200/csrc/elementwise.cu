@@ -737,13 +737,11 @@ __global__ void __launch_bounds__(kDwThreads) dwconv3x3_kernel(const __half* __r
     const int ty = threadIdx.x >> 5;  // tile row
     const int ch = c0 * 8 + 2 * cp;   // first of the pair's two channels
     const bool live = 2 * cp < nv * 8;
-    float wa[9], wb[9];
+    float2 wp[9];  // the pair's two weights per tap
     if (live) {
 #pragma unroll
         for (int k = 0; k < 9; ++k) {
-            const float2 t = __ldg(reinterpret_cast<const float2*>(wt + k * C + ch));
-            wa[k] = t.x;
-            wb[k] = t.y;
+            wp[k] = __ldg(reinterpret_cast<const float2*>(wt + k * C + ch));
         }
     }
     asm volatile("cp.async.wait_group 0;" ::: "memory");
@@ -767,19 +765,19 @@ __global__ void __launch_bounds__(kDwThreads) dwconv3x3_kernel(const __half* __r
         for (int r = 0; r < 3; ++r) {
             win[r][2] = at(ty + r, tx + 2);
         }
-        // FP32 accumulation in the order ky, kx (d3x3_kernel.h:104-166)
-        float a0 = 0.f, a1 = 0.f;
+        // FP32 accumulation in the order ky, kx (d3x3_kernel.h:104-166); one packed FP32 FMA per
+        // tap for the channel pair (each lane rounds as a scalar fmaf would)
+        float2 a = make_float2(0.f, 0.f);
 #pragma unroll
         for (int ky = 0; ky < 3; ++ky) {
 #pragma unroll
             for (int kx = 0; kx < 3; ++kx) {
-                a0 = fmaf(win[ky][kx].x, wa[ky * 3 + kx], a0);
-                a1 = fmaf(win[ky][kx].y, wb[ky * 3 + kx], a1);
+                a = __ffma2_rn(win[ky][kx], wp[ky * 3 + kx], a);
             }
         }
         const int w = w0 + tx;
         if (w < W) {
-            *reinterpret_cast<__half2*>(orow + static_cast<long long>(w) * ldo) = __floats2half2_rn(a0, a1);
+            *reinterpret_cast<__half2*>(orow + static_cast<long long>(w) * ldo) = __floats2half2_rn(a.x, a.y);
         }
 #pragma unroll
         for (int r = 0; r < 3; ++r) {

@@ -394,19 +394,29 @@ __global__ void __launch_bounds__(GemmCfg<BN, EPI>::kThreads, 1)
                     __syncwarp();
 #pragma unroll 1
                     for (int c = 0; c < C::kAccPerBox / 32; ++c) {
+                        const int nc = ncol + c * 32;
+                        // the bias loads are issued before the TMEM load so that their latencies
+                        // overlap (not in the x q epilogues, which have no registers to spare)
+                        constexpr bool kHoist = !epi_has_q(EPI);
+                        const float4* b4 = reinterpret_cast<const float4*>(p.bias + nc);
+                        float4 bb[8];
+                        if constexpr (kHoist) {
+#pragma unroll
+                            for (int j = 0; j < 8; ++j) {
+                                bb[j] = __ldg(b4 + j);
+                            }
+                        }
                         uint32_t r[32];
                         tmem_ld_32x32b_x32(tbase + b * C::kAccPerBox + c * 32, r);
                         tc_wait_ld();
-                        const int nc = ncol + c * 32;
                         float v[32];
-                        const float4* b4 = reinterpret_cast<const float4*>(p.bias + nc);
 #pragma unroll
                         for (int j = 0; j < 8; ++j) {
-                            const float4 bb = __ldg(b4 + j);
-                            v[4 * j + 0] = __uint_as_float(r[4 * j + 0]) + bb.x;
-                            v[4 * j + 1] = __uint_as_float(r[4 * j + 1]) + bb.y;
-                            v[4 * j + 2] = __uint_as_float(r[4 * j + 2]) + bb.z;
-                            v[4 * j + 3] = __uint_as_float(r[4 * j + 3]) + bb.w;
+                            const float4 bj = kHoist ? bb[j] : __ldg(b4 + j);
+                            v[4 * j + 0] = __uint_as_float(r[4 * j + 0]) + bj.x;
+                            v[4 * j + 1] = __uint_as_float(r[4 * j + 1]) + bj.y;
+                            v[4 * j + 2] = __uint_as_float(r[4 * j + 2]) + bj.z;
+                            v[4 * j + 3] = __uint_as_float(r[4 * j + 3]) + bj.w;
                         }
                         if constexpr (EPI == kEpiQuad) {
                             uint32_t o[4];
