@@ -1,6 +1,7 @@
 // extern "C" wrappers of the elementwise, layout and quantisation kernels (include/dcvc_b200.h).
 #include "elementwise.cuh"
 #include "errors.h"
+#include "yuv.cuh"
 
 #include "../../include/dcvc_b200.h"
 
@@ -139,6 +140,22 @@ int dcvc_recover(const int8_t* dec, const uint8_t* cond, const int* block_counts
                  void* stream)
 {
     return wrap(launch_recover(dec, cond, block_counts, n, MH(out), S(stream)), "dcvc_recover");
+}
+
+int dcvc_yuv420_to_input(const void* planes, int frames, int H, int W, void* out, int ldo,
+                         void* stream)
+{
+    return wrap(launch_yuv420_to_input(static_cast<const uint8_t*>(planes), frames, H, W, MH(out),
+                                       ldo, S(stream)),
+                "dcvc_yuv420_to_input");
+}
+
+int dcvc_frames_to_yuv420(const void* const* frames, int nframes, int H, int W, int Wp, int ldp,
+                          void* planes, void* stream)
+{
+    return wrap(launch_frames_to_yuv420(reinterpret_cast<const __half* const*>(frames), nframes, H,
+                                        W, Wp, ldp, static_cast<uint8_t*>(planes), S(stream)),
+                "dcvc_frames_to_yuv420");
 }
 
 }  // extern "C"

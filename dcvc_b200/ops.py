@@ -83,6 +83,8 @@ _sig("dcvc_compact_blocks", [_i])
 _sig("dcvc_compact", [_v, _i, _v, _i, _v, _v, _v, _v])
 _sig("dcvc_recover", [_v, _v, _v, _i, _v, _v])
 _sig("dcvc_scale_index_table", [_v])
+_sig("dcvc_yuv420_to_input", [_v, _i, _i, _i, _v, _i, _v])
+_sig("dcvc_frames_to_yuv420", [ctypes.POINTER(_v), _i, _i, _i, _i, _i, _v, _v])
 
 
 def pad_unshuffle8(x, pad_b, pad_r, out=None):
@@ -218,4 +220,32 @@ def recover(dec, cond, counts):
     out = torch.empty(n, dtype=torch.float16, device=cond.device)
     N.check(N.lib.dcvc_recover(dec.data_ptr(), cond.data_ptr(), counts.data_ptr(), n, out.data_ptr(),
                                _stream()), "recover")
+    return out
+
+
+# ----------------------------------------------------------------------------- YUV 4:2:0 I/O
+
+def yuv420_to_input(planes, frames, H, W, out=None):
+    """planes: uint8 CUDA tensor holding `frames` I420 frames back to back -> the model input
+    [1, 3 * frames, H, W] float16 (channels last), as get_src_frame builds it."""
+    if out is None:
+        out = torch.empty((1, 3 * frames, H, W), dtype=torch.float16, device=planes.device,
+                          memory_format=torch.channels_last)
+    N.check(N.lib.dcvc_yuv420_to_input(planes.data_ptr(), frames, H, W, out.data_ptr(),
+                                       out.stride(3), _stream()), "dcvc_yuv420_to_input")
+    return out
+
+
+def frames_to_yuv420(frames, H, W, out=None):
+    """frames: list of [1, 3, Hp, Wp] float16 channels-last CUDA tensors (reconstructions in
+    [-0.5, 0.5]) -> uint8 CUDA tensor of their I420 planes (cropped to H x W) back to back."""
+    n = len(frames)
+    if out is None:
+        out = torch.empty(n * H * W * 3 // 2, dtype=torch.uint8, device=frames[0].device)
+    for f in frames:
+        if f.stride(1) != 1 or f.stride(3) != 3 or f.shape[1] != 3:
+            raise ValueError("frames must be [1, 3, Hp, Wp] channels-last tensors")
+    ptrs = (_v * n)(*[f.data_ptr() for f in frames])
+    N.check(N.lib.dcvc_frames_to_yuv420(ptrs, n, H, W, frames[0].shape[3], 3, out.data_ptr(),
+                                        _stream()), "dcvc_frames_to_yuv420")
     return out

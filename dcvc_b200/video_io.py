@@ -1,0 +1,238 @@
+"""YUV 4:2:0 file I/O and the end-to-end file round trip of the reference's test harness.
+
+`YUV420Reader` / `YUV420Writer` have the interface of src/utils/video_reader.py:51-99 and
+src/utils/video_writer.py:33-61 (planar I420, 8-bit: Y then U then V per frame).  Their
+`read_raw` / `write_raw` methods move whole frames as bytes, which is what the device path uses:
+the 8-bit planes cross PCIe and `ops.yuv420_to_input` / `ops.frames_to_yuv420` do the
+conversions of get_src_frame (test_video.py:69-123) and of the decoded-frame writer
+(test_video.py:355-362) on the GPU.
+
+`encode_sequence` / `decode_sequence` follow run_one_point_with_stream (test_video.py:167-405):
+an intra frame first (and every `intra_period` frames), then P calls of `frames_per_call` frames
+(8 for the HT-S / HT-L chunk codecs, 1 for the LD codec) with the reference's reset schedule; the
+bitstream is the reference's NAL container (SPS, then one I or P unit per call,
+dcvc_b200.stream_helper).
+"""
+import io
+import os
+
+import numpy as np
+import torch
+
+from . import ops
+from .stream_helper import (NalType, SPSHelper, read_header, read_ip_remaining,
+                            read_sps_remaining, write_ip, write_sps)
+
+
+def frame_bytes(width, height):
+    return width * height * 3 // 2
+
+
+class YUV420Reader:
+    """Planar 8-bit YUV 4:2:0 reader (video_reader.py:51-99)."""
+
+    def __init__(self, src_path, width, height, skip_frame=0):
+        self.eof = False
+        if not src_path.endswith(".yuv"):
+            src_path = src_path + ".yuv"
+        self.src_path = src_path
+        self.y_size = width * height
+        self.y_width = width
+        self.y_height = height
+        self.uv_size = width * height // 2
+        self.uv_width = width // 2
+        self.uv_height = height // 2
+        self.file = open(src_path, "rb")
+        skipped = 0
+        while not self.eof and skipped < skip_frame:
+            y = self.file.read(self.y_size)
+            uv = self.file.read(self.uv_size)
+            if not y or not uv:
+                self.eof = True
+            skipped += 1
+
+    def read_one_frame(self):
+        """(y [1, H, W], uv [2, H/2, W/2]) uint8 arrays, or (None, None) at the end."""
+        if self.eof:
+            return None, None
+        y = self.file.read(self.y_size)
+        uv = self.file.read(self.uv_size)
+        if not y or not uv:
+            self.eof = True
+            return None, None
+        y = np.frombuffer(y, dtype=np.uint8).copy().reshape(1, self.y_height, self.y_width)
+        uv = np.frombuffer(uv, dtype=np.uint8).copy().reshape(2, self.uv_height, self.uv_width)
+        return y, uv
+
+    def read_raw(self, n):
+        """Up to n whole frames as one uint8 array (frames back to back); fewer at the end."""
+        if self.eof:
+            return np.zeros(0, dtype=np.uint8)
+        fb = self.y_size + self.uv_size
+        data = self.file.read(n * fb)
+        k = len(data) // fb
+        if k < n:
+            self.eof = True
+        return np.frombuffer(data[: k * fb], dtype=np.uint8).copy()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, exc_type, exc_val, exc_tb):
+        self.close()
+        return False
+
+    def __del__(self):
+        self.close()
+
+    def close(self):
+        f = getattr(self, "file", None)
+        if f and not f.closed:
+            f.close()
+
+
+class YUV420Writer:
+    """Planar 8-bit YUV 4:2:0 writer (video_writer.py:33-61)."""
+
+    def __init__(self, dst_path, width, height):
+        if not dst_path.endswith(".yuv"):
+            dst_path = dst_path + "/out.yuv"
+        self.dst_path = dst_path
+        self.width = width
+        self.height = height
+        self.file = open(dst_path, "wb")
+
+    def write_one_frame(self, y, uv):
+        self.file.write(np.ascontiguousarray(y, dtype=np.uint8).tobytes())
+        self.file.write(np.ascontiguousarray(uv, dtype=np.uint8).tobytes())
+
+    def write_raw(self, planes):
+        """Whole I420 frames back to back (a uint8 array or tensor)."""
+        if isinstance(planes, torch.Tensor):
+            planes = planes.cpu().numpy()
+        self.file.write(np.ascontiguousarray(planes, dtype=np.uint8).tobytes())
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, exc_type, exc_val, exc_tb):
+        self.close()
+        return False
+
+    def __del__(self):
+        self.close()
+
+    def close(self):
+        f = getattr(self, "file", None)
+        if f and not f.closed:
+            f.close()
+
+
+def padding_size(height, width, p=16):
+    """(padding_r, padding_b) as DMCI.get_padding_size (common_model.py:103-108)."""
+    return (width + p - 1) // p * p - width, (height + p - 1) // p * p - height
+
+
+def _is_intra(frame_idx, intra_period):
+    # test_video.py:207-213
+    intra = frame_idx == 0 or intra_period == 1
+    if intra_period > 1 and frame_idx != 1 and frame_idx % intra_period == 1:
+        intra = True
+    return intra
+
+
+def _upload(raw, device):
+    host = torch.from_numpy(raw).pin_memory()
+    return host.to(device, non_blocking=True)
+
+
+def encode_sequence(src_path, width, height, frame_num, bin_path, i_proxy, p_proxy, qp_i, qp_p,
+                    frames_per_call=8, intra_period=-1, reset_interval=32, device="cuda"):
+    """Codes `frame_num` frames of a YUV 4:2:0 file into the NAL bitstream `bin_path`.
+
+    i_proxy: a DMCIProxy; p_proxy: a DMCHTSProxy / DMCHTLProxy (frames_per_call 8) or DMCLDProxy
+    (frames_per_call 1), both with parameters set.  Returns per-call records
+    (frame index, kind, frames, bytes)."""
+    pad_r, pad_b = padding_size(height, width)
+    fb = frame_bytes(width, height)
+    out = io.BytesIO()
+    sps_helper = SPSHelper()
+    records = []
+    with YUV420Reader(src_path, width, height) as reader:
+        frame_idx = 0
+        while frame_idx < frame_num:
+            intra = _is_intra(frame_idx, intra_period)
+            n = 1 if intra else min(frames_per_call, frame_num - frame_idx)
+            raw = reader.read_raw(n)
+            if raw.size != n * fb:
+                raise EOFError(f"{src_path}: fewer than {frame_num} frames")
+            calls = 1 if intra else frames_per_call
+            if calls > n:  # the last chunk repeats its last frame (test_video.py:101-107)
+                raw = np.concatenate([raw] + [raw[(n - 1) * fb:]] * (calls - n))
+            x = ops.yuv420_to_input(_upload(raw, device), calls, height, width)
+            if intra:
+                qp, reset = qp_i, 0
+                bits, x_hat, ecp = i_proxy.compress(x, qp, pad_b, pad_r)
+                p_proxy.add_ref_feature_from_frame(x_hat, True)
+            else:
+                reset = 1 if reset_interval > 0 and \
+                    (frame_idx + frames_per_call) % reset_interval == 1 else 0
+                qp = qp_p
+                bits, ecp = p_proxy.compress(x, qp, bool(reset), pad_b, pad_r)
+            sps = {"sps_id": -1, "height": height, "width": width}
+            sps_id, sps_new = sps_helper.get_sps_id(sps)
+            sps["sps_id"] = sps_id
+            nb = write_sps(out, sps) if sps_new else 0
+            nb += write_ip(out, intra, sps_id, qp, ecp, reset, bits)
+            records.append((frame_idx, "I" if intra else "P", n, nb))
+            frame_idx += n
+    with open(bin_path, "wb") as f:
+        f.write(out.getbuffer())
+    return records
+
+
+def decode_sequence(bin_path, frame_num, rec_path, i_proxy, p_proxy, frames_per_call=8):
+    """Decodes a bitstream written by encode_sequence and writes the reconstruction as a YUV
+    4:2:0 file (the decoded-frame writer of test_video.py:355-362).  Returns the number of
+    frames written."""
+    with open(bin_path, "rb") as f:
+        buf = io.BytesIO(f.read())
+    sps_helper = SPSHelper()
+    writer = None
+    decoded = 0
+    try:
+        while decoded < frame_num:
+            header = read_header(buf)
+            while header["nal_type"] == NalType.NAL_SPS:
+                sps_helper.add_sps_by_id(read_sps_remaining(buf, header["sps_id"]))
+                header = read_header(buf)
+            sps = sps_helper.get_sps_by_id(header["sps_id"])
+            H, W = sps["height"], sps["width"]
+            if writer is None:
+                writer = YUV420Writer(rec_path, W, H)
+            qp, ec_part, reset, bits = read_ip_remaining(buf)
+            bits = np.frombuffer(bits, dtype=np.uint8)
+            if header["nal_type"] == NalType.NAL_I:
+                x_hat = i_proxy.decompress(bits, qp, H, W, ec_part)
+                p_proxy.add_ref_feature_from_frame(x_hat, False)
+                frames, n = [x_hat], 1
+            else:
+                out = p_proxy.decompress(bits, qp, H, W, ec_part, bool(reset))
+                frames = out if isinstance(out, list) else [out]
+                n = min(frames_per_call, frame_num - decoded)
+            writer.write_raw(ops.frames_to_yuv420(frames[:n], H, W))
+            decoded += n
+    finally:
+        if writer is not None:
+            writer.close()
+    return decoded
+
+
+def write_yuv420(path, frames):
+    """Writes uint8 (y, u, v) plane triples (synthetic.video_chunk_yuv420's frames) to a file."""
+    with open(path, "wb") as f:
+        for y, u, v in frames:
+            f.write(np.ascontiguousarray(y, dtype=np.uint8).tobytes())
+            f.write(np.ascontiguousarray(u, dtype=np.uint8).tobytes())
+            f.write(np.ascontiguousarray(v, dtype=np.uint8).tobytes())
+    return os.path.getsize(path)

@@ -98,6 +98,19 @@ int dcvc_space_to_depth2(const void* x, int H, int W, int C, int ldx, void* out,
 /* 3x3 stride-2 pad-1 patches in (ky, kx, c) order, the A operand of conv_bias with kernel 3
  * (cutlass/conv_kernel.h:22-89). */
 int dcvc_im2col3x3s2(const void* x, int H, int W, int C, int ldx, void* out, void* stream);
+
+/* YUV 4:2:0 planar (I420) I/O on the device.  get_src_frame for YUV input (test_video.py:69-123,
+ * ycbcr420_to_444_np transforms.py:69-80): planes = `frames` (1..8) I420 frames back to back
+ * (uint8, even H and W); out [H, W] pixels with pitch ldo >= 3 frames,
+ * out[p * ldo + 3 f + c] = FP16(FP16(sample / 255) - 0.5), chroma nearest-neighbour up-sampled. */
+int dcvc_yuv420_to_input(const void* planes, int frames, int H, int W, void* out, int ldo,
+                         void* stream);
+/* The decoded-frame writer of test_video.py:355-362 (yuv_444_to_420, transforms.py:83-90): frames
+ * = host array of nframes (1..8) device pointers to FP16 [Hp, Wp, 3] pictures (pixel pitch ldp),
+ * cropped to H x W; planes receives their I420 planes back to back: Y = round(clamp(FP16(
+ * FP16(x + 0.5) * 255), 0, 255)), U / V = trunc of the same on the 2x2 average. */
+int dcvc_frames_to_yuv420(const void* const* frames, int nframes, int H, int W, int Wp, int ldp,
+                          void* planes, void* stream);
 /* replicate_pad / slice (cat_and_pad.cu:53-110). */
 int dcvc_replicate_pad(const void* x, int H, int W, int C, int ldx, int pad_b, int pad_r, void* out,
                        void* stream);
