@@ -576,13 +576,20 @@ def run_gpu(args):
     ms_max = max_over_ranks(ms, "cuda")
     value = FRAMES * args.steps * world / (ms_max / 1e3)
 
-    # ---------------- end to end through the proxy API from pinned host memory
-    x_host = [x.cpu().pin_memory() for x in xs]
+    # ---------------- end to end through the proxy API from pinned host memory: the chunk's
+    # 8-bit YUV 4:2:0 planes go up, are converted to the model input on the device (the FP16
+    # arithmetic of get_src_frame), and the 8 reconstructions come back as YUV 4:2:0 planes (the
+    # decoded-frame writer of the reference harness)
+    from dcvc_b200 import ops
+    planes_host = [torch.from_numpy(np.concatenate(
+        [np.concatenate([y.ravel(), u.ravel(), v.ravel()]) for y, u, v in c])).pin_memory()
+        for c in host_chunks]
+    planes_dev = torch.empty_like(planes_host[0], device="cuda")
     x_dev = torch.empty_like(xs[0])
-    hp, wp = (H + 15) // 16 * 16, (W + 15) // 16 * 16
-    out_host = torch.empty((FRAMES, 3, hp, wp), dtype=torch.float16).pin_memory()
-    h2d = x_host[0].numel() * 2
-    d2h = out_host.numel() * 2
+    out_dev = torch.empty_like(planes_dev)
+    out_host = torch.empty_like(planes_host[0]).pin_memory()
+    h2d = planes_host[0].numel()
+    d2h = out_host.numel()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
@@ -590,10 +597,11 @@ def run_gpu(args):
     windows.append([time.time(), None])
     e0.record(stream)
     for i in range(args.steps):
-        x_dev.copy_(x_host[i % 2], non_blocking=True)
+        planes_dev.copy_(planes_host[i % 2], non_blocking=True)
+        ops.yuv420_to_input(planes_dev, FRAMES, H, W, out=x_dev)
         frames, _ = step(args.warmup + i, x_dev)
-        for f in range(FRAMES):
-            out_host[f].copy_(frames[f][0], non_blocking=True)
+        ops.frames_to_yuv420(frames, H, W, out=out_dev)
+        out_host.copy_(out_dev, non_blocking=True)
     e1.record(stream)
     torch.cuda.synchronize()
     windows[-1][1] = time.time()
@@ -632,7 +640,8 @@ def run_gpu(args):
         "intra": intra,
         "htl": htl,
         "ld": ld,
-        "e2e": {"value": round(e2e, 2), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "e2e": {"value": round(e2e, 2), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "io": "8-bit YUV 4:2:0 planes in and out, converted on the device"},
         "gpu_launches": kernels_per_step * args.steps,
         "roofline": roof,
         "clocks": clk,
