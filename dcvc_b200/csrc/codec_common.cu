@@ -1,5 +1,7 @@
 #include "codec_common.h"
 
+#include "elementwise.cuh"
+
 #include "errors.h"
 
 #include <string>
@@ -29,8 +31,14 @@ int PhaseGraphs::run(int slot, cudaStream_t s, int* err_word,
         return cuda_status(cudaGraphLaunch(g.exec, s), "cudaGraphLaunch");
     }
     Launch L{s, err_word};
-    if (!g.ran_eager) {
+    auto body_and_publish = [&]() {
         body(L);
+        if (err_slot_dev_ != nullptr && err_word != nullptr) {
+            L.note(launch_copy_counted(err_word, err_slot_dev_, sizeof(int), nullptr, 1, nullptr, s));
+        }
+    };
+    if (!g.ran_eager) {
+        body_and_publish();
         g.ran_eager = true;
         g.kernels = L.kernels;
         *kernels += L.kernels;
@@ -41,7 +49,7 @@ int PhaseGraphs::run(int slot, cudaStream_t s, int* err_word,
     if (e != cudaSuccess) {
         return cuda_status(e, "cudaStreamBeginCapture");
     }
-    body(L);
+    body_and_publish();
     e = cudaStreamEndCapture(s, &graph);
     if (L.first != cudaSuccess || e != cudaSuccess) {
         if (graph != nullptr) {
@@ -96,22 +104,60 @@ int load_cdf_tables(const StateDict& sd, RansTables* tables, int z_count, int y_
     return kOk;
 }
 
-int check_device_error_word(int* err_word, const char* where)
+int check_device_error_word(int* err_word, ErrorSlot& slot, const char* where)
 {
-    int code = 0;
-    if (err_word == nullptr) {
+    if (err_word == nullptr || slot.host == nullptr) {
         return kOk;
     }
-    if (cudaMemcpy(&code, err_word, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) {
-        return cuda_status(cudaGetLastError(), where);
-    }
+    const int code = *static_cast<volatile int*>(slot.host);
     if (code != 0) {
         cudaMemset(err_word, 0, sizeof(int));
+        *static_cast<volatile int*>(slot.host) = 0;
         set_last_error(std::string(where) + ": a kernel's bounded wait gave up (device error " +
                        std::to_string(code) + ")");
         return kDeviceTimeout;
     }
     return kOk;
+}
+
+bool ErrorSlot::alloc()
+{
+    void *h = nullptr, *d = nullptr;
+    if (!alloc_mapped(sizeof(int), &h, &d)) {
+        return false;
+    }
+    host = static_cast<int*>(h);
+    dev = static_cast<int*>(d);
+    *host = 0;
+    return true;
+}
+
+void ErrorSlot::release()
+{
+    if (host != nullptr) {
+        cudaFreeHost(host);
+    }
+    host = nullptr;
+    dev = nullptr;
+}
+
+bool alloc_mapped(size_t bytes, void** host, void** dev)
+{
+    *host = nullptr;
+    *dev = nullptr;
+    if (cudaHostAlloc(host, bytes, cudaHostAllocMapped) != cudaSuccess) {
+        cudaGetLastError();
+        *host = nullptr;
+        return false;
+    }
+    if (cudaHostGetDevicePointer(dev, *host, 0) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFreeHost(*host);
+        *host = nullptr;
+        *dev = nullptr;
+        return false;
+    }
+    return true;
 }
 
 }  // namespace dcvc

@@ -23,9 +23,12 @@ public:
     PhaseGraphs& operator=(const PhaseGraphs&) = delete;
     ~PhaseGraphs() { clear(); }
     void clear();
-    // Enqueues phase `slot` on s; adds the phase's kernel count to *kernels.
+    // Enqueues phase `slot` on s; adds the phase's kernel count to *kernels.  Every phase ends by
+    // publishing the device error word into the mapped host slot set with set_error_slot, so
+    // that the host can check it after an event on s without a synchronous copy.
     int run(int slot, cudaStream_t s, int* err_word, const std::function<void(Launch&)>& body,
             int* kernels);
+    void set_error_slot(int* slot_dev) { err_slot_dev_ = slot_dev; }
 
 private:
     struct Slot {
@@ -34,13 +37,28 @@ private:
         int kernels = 0;
     };
     std::vector<Slot> slots_;
+    int* err_slot_dev_ = nullptr;
+};
+
+// A mapped pinned host int that phase graphs copy the device error word into.
+struct ErrorSlot {
+    int* host = nullptr;
+    int* dev = nullptr;
+    bool alloc();
+    void release();
 };
 
 // Loads "bit_estimator_z.{quantized_cdf,cdf_length}" (table set 0) and
 // "gaussian_encoder.{quantized_cdf,cdf_length}" (table set 1) and checks their counts.
 int load_cdf_tables(const StateDict& sd, RansTables* tables, int z_count, int y_count);
 
-// Reads (and clears) the device error word; kDeviceTimeout if a kernel's bounded wait gave up.
-int check_device_error_word(int* err_word, const char* where);
+// Pinned host memory mapped into the device address space (cudaHostAllocMapped): *host for the
+// CPU, *dev for kernels.  Returns false (and leaves both null) when the allocation fails.
+bool alloc_mapped(size_t bytes, void** host, void** dev);
+
+// Checks the error word as the last phase graph published it into `slot` (and clears both the
+// slot and the device word); kDeviceTimeout if a kernel's bounded wait gave up.  The caller must
+// have waited for an event recorded after that phase.
+int check_device_error_word(int* err_word, ErrorSlot& slot, const char* where);
 
 }  // namespace dcvc

@@ -1,7 +1,9 @@
 #include "elementwise.cuh"
+
 #include "common.cuh"
 #include "host_util.h"
 
+#include <algorithm>
 #include <mutex>
 
 namespace dcvc {
@@ -1079,6 +1081,61 @@ cudaError_t launch_dwconv3x3(const __half* x, int H, int W, int C, int ldx, cons
     }
     const dim3 grid((C / 8 + kDwCV - 1) / kDwCV, (H + kDwTH - 1) / kDwTH, (W + kDwTW - 1) / kDwTW);
     launch_pdl(dwconv3x3_kernel, dim3(grid), dim3(kDwThreads), 0, s, x, H, W, C, ldx, w, out, ldo);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------ counted copy
+
+namespace {
+
+constexpr int kCopyThreads = 256;
+
+__global__ void __launch_bounds__(kCopyThreads) copy_counted_kernel(
+    const uint8_t* __restrict__ src, uint8_t* __restrict__ dst, int elem_bytes,
+    const int* __restrict__ count, int max_elems, int* __restrict__ count_out, bool vec)
+{
+    griddep_launch_dependents();
+    griddep_wait();
+    int n = max_elems;
+    if (count != nullptr) {
+        n = min(max(*count, 0), max_elems);
+    }
+    if (count_out != nullptr && blockIdx.x == 0 && threadIdx.x == 0) {
+        *count_out = n;
+    }
+    const long long bytes = static_cast<long long>(n) * elem_bytes;
+    const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+    const long long t0 = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    long long done = 0;
+    if (vec) {
+        const long long nv = bytes / 16;
+        const uint4* s4 = reinterpret_cast<const uint4*>(src);
+        uint4* d4 = reinterpret_cast<uint4*>(dst);
+        for (long long i = t0; i < nv; i += stride) {
+            d4[i] = s4[i];
+        }
+        done = nv * 16;
+    }
+    for (long long i = done + t0; i < bytes; i += stride) {
+        dst[i] = src[i];
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_copy_counted(const void* src, void* dst, int elem_bytes, const int* count,
+                                int max_elems, int* count_out, cudaStream_t s)
+{
+    if (src == nullptr || dst == nullptr || elem_bytes < 1 || elem_bytes > 8 || max_elems < 0) {
+        return cudaErrorInvalidValue;
+    }
+    const bool vec = ((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 15) == 0;
+    const long long bytes = static_cast<long long>(max_elems) * elem_bytes;
+    const long long want = (bytes / 16 + kCopyThreads - 1) / kCopyThreads;
+    const int blocks = static_cast<int>(std::max(1LL, std::min(want, 4LL * num_sms())));
+    launch_pdl(copy_counted_kernel, dim3(blocks), dim3(kCopyThreads), 0, s,
+               static_cast<const uint8_t*>(src), static_cast<uint8_t*>(dst), elem_bytes, count,
+               max_elems, count_out, vec);
     return cudaGetLastError();
 }
 

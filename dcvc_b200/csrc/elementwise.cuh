@@ -124,6 +124,14 @@ int compact_blocks(int n);
 cudaError_t launch_compact(const void* src, int elem_bytes, const uint8_t* cond, int n,
                            int* block_counts, void* dst, int* total, cudaStream_t s);
 
+// Copies n = min(*count, max_elems) elements of elem_bytes each (n = max_elems when count is
+// null) from src to dst, either of which may be mapped pinned host memory, and stores n in
+// *count_out when it is non-null.  The codecs move their symbols, indexes and decoded values
+// between the device and the host with it inside the phase graphs, on the SMs, so that a
+// transfer is never queued behind another phase's kernels.
+cudaError_t launch_copy_counted(const void* src, void* dst, int elem_bytes, const int* count,
+                                int max_elems, int* count_out, cudaStream_t s);
+
 // Allocation-free variant of launch_compact: the block counts live in a file-scope device array
 // (n <= compact_noalloc_max_elements()); see elementwise.cu for the sharing rules.
 int compact_noalloc_max_elements();

@@ -31,6 +31,9 @@ HtlCodec::HtlCodec()
     cudaEventCreateWithFlags(&ev_copy_, cudaEventDisableTiming);
     cudaEventCreateWithFlags(&ev_out_, cudaEventDisableTiming);
     err_word_ = device_error_word();
+    if (err_slot_.alloc()) {
+        graphs_.set_error_slot(err_slot_.dev);
+    }
 }
 
 HtlCodec::~HtlCodec()
@@ -54,6 +57,7 @@ HtlCodec::~HtlCodec()
     cudaEventDestroy(ev_out_);
     cudaStreamDestroy(main_);
     cudaStreamDestroy(copy_);
+    err_slot_.release();
 }
 
 int HtlCodec::set_param(const StateDict& sd, float skip_threshold)
@@ -621,7 +625,7 @@ int HtlCodec::compress(const __half* x, int H, int W, int qp, bool reset, int pa
     if (cudaEventSynchronize(ev_phase_) != cudaSuccess) {
         return cuda_status(cudaGetLastError(), "compress: analysis");
     }
-    st = check_device_error_word(err_word_, "compress");
+    st = check_device_error_word(err_word_, err_slot_, "compress");
     if (st != kOk) {
         return st;
     }
@@ -704,7 +708,7 @@ int HtlCodec::decompress(const uint8_t* bytes, size_t n, int qp, int height, int
         if (st == kOk && cudaEventSynchronize(ev_phase_) != cudaSuccess) {
             st = cuda_status(cudaGetLastError(), "decompress: index building");
         }
-        if (st == kOk) st = check_device_error_word(err_word_, "decompress");
+        if (st == kOk) st = check_device_error_word(err_word_, err_slot_, "decompress");
         int count = 0;
         if (st == kOk) {
             count = *count_host_;

@@ -7,6 +7,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <type_traits>
 
 namespace dcvc {
 
@@ -27,12 +28,13 @@ HtsCodec::HtsCodec()
 {
     cudaGetDevice(&dev_);
     cudaStreamCreateWithFlags(&main_, cudaStreamNonBlocking);
-    cudaStreamCreateWithFlags(&copy_, cudaStreamNonBlocking);
     cudaEventCreateWithFlags(&ev_in_, cudaEventDisableTiming);
     cudaEventCreateWithFlags(&ev_phase_, cudaEventDisableTiming);
-    cudaEventCreateWithFlags(&ev_copy_, cudaEventDisableTiming);
     cudaEventCreateWithFlags(&ev_out_, cudaEventDisableTiming);
     err_word_ = device_error_word();
+    if (err_slot_.alloc()) {
+        graphs_.set_error_slot(err_slot_.dev);
+    }
 }
 
 HtsCodec::~HtsCodec()
@@ -40,9 +42,6 @@ HtsCodec::~HtsCodec()
     cudaSetDevice(dev_);
     if (main_ != nullptr) {
         cudaStreamSynchronize(main_);
-    }
-    if (copy_ != nullptr) {
-        cudaStreamSynchronize(copy_);
     }
     clear_graphs();
     cudaFreeHost(count_host_);
@@ -52,10 +51,9 @@ HtsCodec::~HtsCodec()
     cudaFreeHost(z_host_);
     cudaEventDestroy(ev_in_);
     cudaEventDestroy(ev_phase_);
-    cudaEventDestroy(ev_copy_);
     cudaEventDestroy(ev_out_);
     cudaStreamDestroy(main_);
-    cudaStreamDestroy(copy_);
+    err_slot_.release();
 }
 
 void HtsCodec::clear_graphs() { graphs_.clear(); }
@@ -165,7 +163,6 @@ int HtsCodec::allocate(int Hp, int Wp)
         return kInvalidArgument;
     }
     cudaStreamSynchronize(main_);
-    cudaStreamSynchronize(copy_);
     clear_graphs();
     acts_.clear();
     cudaFreeHost(count_host_);
@@ -178,6 +175,11 @@ int HtsCodec::allocate(int Hp, int Wp)
     idx_host_ = nullptr;
     ydec_host_ = nullptr;
     z_host_ = nullptr;
+    count_hdev_ = nullptr;
+    sym_hdev_ = nullptr;
+    idx_hdev_ = nullptr;
+    ydec_hdev_ = nullptr;
+    z_hdev_ = nullptr;
     Hp_ = Wp_ = 0;
 
     const int H8 = Hp / 8, W8 = Wp / 8;
@@ -250,11 +252,17 @@ int HtsCodec::allocate(int Hp, int Wp)
     count_dev_ = acts_.alloc_n<int>(1);
     ok = ok && z_i8_ && sym_ && sym_c_ && idx_ && idx_c_ && cond_ && y_dec_ && block_counts_ &&
          count_dev_;
-    ok = ok && cudaMallocHost(&count_host_, sizeof(int) * 2) == cudaSuccess;
-    ok = ok && cudaMallocHost(&sym_host_, sizeof(int16_t) * y_num_) == cudaSuccess;
-    ok = ok && cudaMallocHost(&idx_host_, y_num_) == cudaSuccess;
-    ok = ok && cudaMallocHost(&ydec_host_, y_num_) == cudaSuccess;
-    ok = ok && cudaMallocHost(&z_host_, z_num_) == cudaSuccess;
+    auto mapped = [&](size_t bytes, auto** host, auto** dev) {
+        void *h = nullptr, *d = nullptr;
+        ok = ok && alloc_mapped(bytes, &h, &d);
+        *host = static_cast<std::remove_reference_t<decltype(**host)>*>(h);
+        *dev = static_cast<std::remove_reference_t<decltype(**dev)>*>(d);
+    };
+    mapped(sizeof(int) * 2, &count_host_, &count_hdev_);
+    mapped(sizeof(int16_t) * y_num_, &sym_host_, &sym_hdev_);
+    mapped(y_num_, &idx_host_, &idx_hdev_);
+    mapped(y_num_, &ydec_host_, &ydec_hdev_);
+    mapped(z_num_, &z_host_, &z_hdev_);
     if (!ok) {
         cudaGetLastError();
         acts_.clear();
@@ -437,7 +445,9 @@ void HtsCodec::enc_analysis(Launch& L)
     L.note(launch_build_index_enc(y_q_, kChY, scales, ldc, skip_thr_half_, scale_lut_, M16_, kChY,
                                   sym_, cond_, L.s));
     L.note(launch_compact(sym_, 2, cond_, y_num_, block_counts_, sym_c_, count_dev_, L.s), 2);
-    L.note(cudaMemcpyAsync(count_host_, count_dev_, sizeof(int), cudaMemcpyDeviceToHost, L.s), 0);
+    // the symbols, their count and z to the mapped host buffers
+    L.note(launch_copy_counted(sym_c_, sym_hdev_, 2, count_dev_, y_num_, count_hdev_, L.s));
+    L.note(launch_copy_counted(z_i8_, z_hdev_, 1, nullptr, z_num_, nullptr, L.s));
 }
 
 void HtsCodec::enc_update(Launch& L, bool reset)
@@ -464,13 +474,13 @@ void HtsCodec::dec_temporal(Launch& L, bool memory_has_value)
 
 void HtsCodec::dec_hyper(Launch& L)
 {
-    L.note(launch_int8_to_half(z_i8_, z_num_, z_hat_, L.s));
+    L.note(launch_int8_to_half(z_hdev_, z_num_, z_hat_, L.s));  // z as decoded on the host
     hyper_decoder(L);
     prior_fusion(L);
     L.note(launch_build_index_dec(common_ + kChY, 3 * kChY, skip_thr_half_, scale_lut_, M16_, kChY,
                                   idx_, cond_, L.s));
     L.note(launch_compact(idx_, 1, cond_, y_num_, block_counts_, idx_c_, count_dev_, L.s), 2);
-    L.note(cudaMemcpyAsync(count_host_, count_dev_, sizeof(int), cudaMemcpyDeviceToHost, L.s), 0);
+    L.note(launch_copy_counted(idx_c_, idx_hdev_, 1, count_dev_, y_num_, count_hdev_, L.s));
 }
 
 void HtsCodec::dec_context(Launch& L) { feature_extractor(L); }
@@ -480,6 +490,7 @@ void HtsCodec::dec_synthesis(Launch& L)
     const __half* q_dec = common_;
     const __half* means0 = common_ + 2 * kChY;
     const int ldc = 3 * kChY;
+    L.note(launch_copy_counted(ydec_hdev_, y_dec_, 1, count_dev_, y_num_, nullptr, L.s));
     L.note(launch_recover(y_dec_, cond_, block_counts_, y_num_, y_q_, L.s));
     L.note(launch_restore_phase(0, 0, y_q_, kChY, means0, ldc, nullptr, 0, cat_spa_, 2 * kChY,
                                 H16_, W16_, kChY, L.s));
@@ -616,7 +627,7 @@ int HtsCodec::compress(const __half* x, int H, int W, int qp, bool reset, int pa
     if (cudaEventSynchronize(ev_phase_) != cudaSuccess) {
         return cuda_status(cudaGetLastError(), "compress: analysis");
     }
-    st = check_device_error_word(err_word_, "compress");
+    st = check_device_error_word(err_word_, err_slot_, "compress");
     if (st != kOk) {
         return st;
     }
@@ -624,14 +635,6 @@ int HtsCodec::compress(const __half* x, int H, int W, int qp, bool reset, int pa
     if (count < 0 || count > y_num_) {
         set_last_error("compress: symbol count out of range");
         return kInternal;
-    }
-    cudaStreamWaitEvent(copy_, ev_phase_, 0);
-    if (count > 0) {
-        cudaMemcpyAsync(sym_host_, sym_c_, sizeof(int16_t) * count, cudaMemcpyDeviceToHost, copy_);
-    }
-    cudaMemcpyAsync(z_host_, z_i8_, z_num_, cudaMemcpyDeviceToHost, copy_);
-    if (cudaStreamSynchronize(copy_) != cudaSuccess) {
-        return cuda_status(cudaGetLastError(), "compress: symbol copy");
     }
     const int ecp = ec_parallel_for(count);
     RansEncoderSession enc;
@@ -677,9 +680,6 @@ int HtsCodec::decompress(const uint8_t* bytes, size_t n, int qp, int height, int
         st = kCorruptStream;
     }
     if (st == kOk) {
-        cudaMemcpyAsync(z_i8_, z_host_, z_num_, cudaMemcpyHostToDevice, copy_);
-        cudaEventRecord(ev_copy_, copy_);
-        cudaStreamWaitEvent(main_, ev_copy_, 0);
         st = run_phase(kDecHyper, main_);
     }
     if (st == kOk) st = cuda_status(cudaEventRecord(ev_phase_, main_), "decompress");
@@ -689,7 +689,7 @@ int HtsCodec::decompress(const uint8_t* bytes, size_t n, int qp, int height, int
             st = cuda_status(cudaGetLastError(), "decompress: hyper prior");
         }
     }
-    if (st == kOk) st = check_device_error_word(err_word_, "decompress");
+    if (st == kOk) st = check_device_error_word(err_word_, err_slot_, "decompress");
     int count = 0;
     if (st == kOk) {
         count = *count_host_;
@@ -698,24 +698,12 @@ int HtsCodec::decompress(const uint8_t* bytes, size_t n, int qp, int height, int
             st = kInternal;
         }
     }
-    if (st == kOk && count > 0) {
-        cudaStreamWaitEvent(copy_, ev_phase_, 0);
-        cudaMemcpyAsync(idx_host_, idx_c_, count, cudaMemcpyDeviceToHost, copy_);
-        if (cudaStreamSynchronize(copy_) != cudaSuccess) {
-            st = cuda_status(cudaGetLastError(), "decompress: index copy");
-        }
-    }
     // y on the CPU while the feature extractor runs (dmc_hts_proxy.cpp:805-823)
     if (st == kOk && !dec.decode_y(tables_, idx_host_, count, ydec_host_, &err)) {
         set_last_error("decompress: " + err);
         st = kCorruptStream;
     }
     if (st == kOk) {
-        if (count > 0) {
-            cudaMemcpyAsync(y_dec_, ydec_host_, count, cudaMemcpyHostToDevice, copy_);
-        }
-        cudaEventRecord(ev_copy_, copy_);
-        cudaStreamWaitEvent(main_, ev_copy_, 0);
         st = run_phase(kDecSynthesis, main_);
     }
     if (st == kOk) {

@@ -31,6 +31,9 @@ IntraCodec::IntraCodec()
     cudaEventCreateWithFlags(&ev_copy_, cudaEventDisableTiming);
     cudaEventCreateWithFlags(&ev_out_, cudaEventDisableTiming);
     err_word_ = device_error_word();
+    if (err_slot_.alloc()) {
+        graphs_.set_error_slot(err_slot_.dev);
+    }
 }
 
 IntraCodec::~IntraCodec()
@@ -54,6 +57,7 @@ IntraCodec::~IntraCodec()
     cudaEventDestroy(ev_out_);
     cudaStreamDestroy(main_);
     cudaStreamDestroy(copy_);
+    err_slot_.release();
 }
 
 int IntraCodec::set_param(const StateDict& sd, float skip_threshold)
@@ -495,7 +499,7 @@ int IntraCodec::compress(const __half* x, int H, int W, int qp, int pad_b, int p
     if (cudaEventSynchronize(ev_phase_) != cudaSuccess) {
         return cuda_status(cudaGetLastError(), "compress: analysis");
     }
-    st = check_device_error_word(err_word_, "compress");
+    st = check_device_error_word(err_word_, err_slot_, "compress");
     if (st != kOk) {
         return st;
     }
@@ -581,7 +585,7 @@ int IntraCodec::decompress(const uint8_t* bytes, size_t n, int qp, int height, i
         if (st == kOk && cudaEventSynchronize(ev_phase_) != cudaSuccess) {
             st = cuda_status(cudaGetLastError(), "decompress: index building");
         }
-        if (st == kOk) st = check_device_error_word(err_word_, "decompress");
+        if (st == kOk) st = check_device_error_word(err_word_, err_slot_, "decompress");
         int count = 0;
         if (st == kOk) {
             count = *count_host_;

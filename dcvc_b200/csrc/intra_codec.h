@@ -126,6 +126,7 @@ private:
     cudaStream_t copy_ = nullptr;
     cudaEvent_t ev_in_ = nullptr, ev_phase_ = nullptr, ev_copy_ = nullptr, ev_out_ = nullptr;
     int* err_word_ = nullptr;
+    ErrorSlot err_slot_;  // the error word as the phase graphs publish it
     int last_count_ = 0;
     int last_kernels_ = 0;
     int dev_ = 0;

@@ -7,6 +7,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <type_traits>
 
 namespace dcvc {
 
@@ -25,12 +26,13 @@ LdCodec::LdCodec()
 {
     cudaGetDevice(&dev_);
     cudaStreamCreateWithFlags(&main_, cudaStreamNonBlocking);
-    cudaStreamCreateWithFlags(&copy_, cudaStreamNonBlocking);
     cudaEventCreateWithFlags(&ev_in_, cudaEventDisableTiming);
     cudaEventCreateWithFlags(&ev_phase_, cudaEventDisableTiming);
-    cudaEventCreateWithFlags(&ev_copy_, cudaEventDisableTiming);
     cudaEventCreateWithFlags(&ev_out_, cudaEventDisableTiming);
     err_word_ = device_error_word();
+    if (err_slot_.alloc()) {
+        graphs_.set_error_slot(err_slot_.dev);
+    }
 }
 
 LdCodec::~LdCodec()
@@ -38,9 +40,6 @@ LdCodec::~LdCodec()
     cudaSetDevice(dev_);
     if (main_ != nullptr) {
         cudaStreamSynchronize(main_);
-    }
-    if (copy_ != nullptr) {
-        cudaStreamSynchronize(copy_);
     }
     graphs_.clear();
     cudaFreeHost(count_host_);
@@ -50,10 +49,9 @@ LdCodec::~LdCodec()
     cudaFreeHost(z_host_);
     cudaEventDestroy(ev_in_);
     cudaEventDestroy(ev_phase_);
-    cudaEventDestroy(ev_copy_);
     cudaEventDestroy(ev_out_);
     cudaStreamDestroy(main_);
-    cudaStreamDestroy(copy_);
+    err_slot_.release();
 }
 
 int LdCodec::set_param(const StateDict& sd, float skip_threshold)
@@ -149,7 +147,6 @@ int LdCodec::allocate(int Hp, int Wp)
         return kInvalidArgument;
     }
     cudaStreamSynchronize(main_);
-    cudaStreamSynchronize(copy_);
     graphs_.clear();
     acts_.clear();
     cudaFreeHost(count_host_);
@@ -162,6 +159,11 @@ int LdCodec::allocate(int Hp, int Wp)
     idx_host_ = nullptr;
     ydec_host_ = nullptr;
     z_host_ = nullptr;
+    count_hdev_ = nullptr;
+    sym_hdev_ = nullptr;
+    idx_hdev_ = nullptr;
+    ydec_hdev_ = nullptr;
+    z_hdev_ = nullptr;
     Hp_ = Wp_ = 0;
 
     H8_ = Hp / 8;
@@ -226,11 +228,17 @@ int LdCodec::allocate(int Hp, int Wp)
     count_dev_ = acts_.alloc_n<int>(1);
     ok = ok && z_i8_ && sym_ && sym_c_ && idx_ && idx_c_ && cond_ && y_dec_ && block_counts_ &&
          count_dev_;
-    ok = ok && cudaMallocHost(&count_host_, sizeof(int)) == cudaSuccess;
-    ok = ok && cudaMallocHost(&sym_host_, sizeof(int16_t) * y_num_) == cudaSuccess;
-    ok = ok && cudaMallocHost(&idx_host_, y_num_) == cudaSuccess;
-    ok = ok && cudaMallocHost(&ydec_host_, y_num_) == cudaSuccess;
-    ok = ok && cudaMallocHost(&z_host_, z_num_) == cudaSuccess;
+    auto mapped = [&](size_t bytes, auto** host, auto** dev) {
+        void *h = nullptr, *d = nullptr;
+        ok = ok && alloc_mapped(bytes, &h, &d);
+        *host = static_cast<std::remove_reference_t<decltype(**host)>*>(h);
+        *dev = static_cast<std::remove_reference_t<decltype(**dev)>*>(d);
+    };
+    mapped(sizeof(int) * 2, &count_host_, &count_hdev_);
+    mapped(sizeof(int16_t) * y_num_, &sym_host_, &sym_hdev_);
+    mapped(y_num_, &idx_host_, &idx_hdev_);
+    mapped(y_num_, &ydec_host_, &ydec_hdev_);
+    mapped(z_num_, &z_host_, &z_hdev_);
     if (!ok) {
         cudaGetLastError();
         acts_.clear();
@@ -391,7 +399,9 @@ void LdCodec::enc_analysis(Launch& L)
     L.note(launch_build_index_enc(y_q_, kChY, scales, C4, skip_thr_half_, scale_lut_, M16_, kChY,
                                   sym_, cond_, L.s));
     L.note(launch_compact(sym_, 2, cond_, y_num_, block_counts_, sym_c_, count_dev_, L.s), 2);
-    L.note(cudaMemcpyAsync(count_host_, count_dev_, sizeof(int), cudaMemcpyDeviceToHost, L.s), 0);
+    // the symbols, their count and z to the mapped host buffers
+    L.note(launch_copy_counted(sym_c_, sym_hdev_, 2, count_dev_, y_num_, count_hdev_, L.s));
+    L.note(launch_copy_counted(z_i8_, z_hdev_, 1, nullptr, z_num_, nullptr, L.s));
 }
 
 void LdCodec::enc_update(Launch& L, bool reset)
@@ -419,17 +429,18 @@ void LdCodec::dec_temporal(Launch& L, bool memory_has_value)
 
 void LdCodec::dec_hyper(Launch& L)
 {
-    L.note(launch_int8_to_half(z_i8_, z_num_, z_hat_, L.s));
+    L.note(launch_int8_to_half(z_hdev_, z_num_, z_hat_, L.s));  // z as decoded on the host
     entropy_params(L);
     L.note(launch_build_index_dec(cat_sp_ + 2 * kChY, 4 * kChY, skip_thr_half_, scale_lut_, M16_,
                                   kChY, idx_, cond_, L.s));
     L.note(launch_compact(idx_, 1, cond_, y_num_, block_counts_, idx_c_, count_dev_, L.s), 2);
-    L.note(cudaMemcpyAsync(count_host_, count_dev_, sizeof(int), cudaMemcpyDeviceToHost, L.s), 0);
+    L.note(launch_copy_counted(idx_c_, idx_hdev_, 1, count_dev_, y_num_, count_hdev_, L.s));
 }
 
 void LdCodec::dec_synthesis(Launch& L)
 {
     const int C4 = 4 * kChY;
+    L.note(launch_copy_counted(ydec_hdev_, y_dec_, 1, count_dev_, y_num_, nullptr, L.s));
     L.note(launch_recover(y_dec_, cond_, block_counts_, y_num_, y_q_, L.s));
     L.note(launch_restore_phase(0, 0, y_q_, kChY, cat_sp_ + 3 * kChY, C4, nullptr, 0, cat_sp_, C4,
                                 H16_, W16_, kChY, L.s, 2));
@@ -562,7 +573,7 @@ int LdCodec::compress(const __half* x, int H, int W, int qp, bool reset, int pad
     if (cudaEventSynchronize(ev_phase_) != cudaSuccess) {
         return cuda_status(cudaGetLastError(), "compress: analysis");
     }
-    st = check_device_error_word(err_word_, "compress");
+    st = check_device_error_word(err_word_, err_slot_, "compress");
     if (st != kOk) {
         return st;
     }
@@ -570,13 +581,6 @@ int LdCodec::compress(const __half* x, int H, int W, int qp, bool reset, int pad
     if (count < 0 || count > y_num_) {
         set_last_error("compress: symbol count out of range");
         return kInternal;
-    }
-    if (count > 0) {
-        cudaMemcpyAsync(sym_host_, sym_c_, sizeof(int16_t) * count, cudaMemcpyDeviceToHost, copy_);
-    }
-    cudaMemcpyAsync(z_host_, z_i8_, z_num_, cudaMemcpyDeviceToHost, copy_);
-    if (cudaStreamSynchronize(copy_) != cudaSuccess) {
-        return cuda_status(cudaGetLastError(), "compress: symbol copy");
     }
     const int ecp = ec_parallel_for(count);
     RansEncoderSession enc;
@@ -610,7 +614,6 @@ int LdCodec::decompress(const uint8_t* bytes, size_t n, int qp, int height, int 
     last_kernels_ = 0;
     cudaEventRecord(ev_in_, caller);
     cudaStreamWaitEvent(main_, ev_in_, 0);
-    cudaStreamWaitEvent(copy_, ev_in_, 0);
     set_qp(qp, main_);
     int st = run_phase(kDecTemporal + (memory_has_value_ ? 1 : 0), main_);
     RansDecoderSession dec;
@@ -621,9 +624,6 @@ int LdCodec::decompress(const uint8_t* bytes, size_t n, int qp, int height, int 
         st = kCorruptStream;
     }
     if (st == kOk) {
-        cudaMemcpyAsync(z_i8_, z_host_, z_num_, cudaMemcpyHostToDevice, copy_);
-        cudaEventRecord(ev_copy_, copy_);
-        cudaStreamWaitEvent(main_, ev_copy_, 0);
         st = run_phase(kDecHyper, main_);
     }
     if (st == kOk) st = cuda_status(cudaEventRecord(ev_phase_, main_), "decompress");
@@ -631,7 +631,7 @@ int LdCodec::decompress(const uint8_t* bytes, size_t n, int qp, int height, int 
     if (st == kOk && cudaEventSynchronize(ev_phase_) != cudaSuccess) {
         st = cuda_status(cudaGetLastError(), "decompress: hyper prior");
     }
-    if (st == kOk) st = check_device_error_word(err_word_, "decompress");
+    if (st == kOk) st = check_device_error_word(err_word_, err_slot_, "decompress");
     int count = 0;
     if (st == kOk) {
         count = *count_host_;
@@ -640,22 +640,11 @@ int LdCodec::decompress(const uint8_t* bytes, size_t n, int qp, int height, int 
             st = kInternal;
         }
     }
-    if (st == kOk && count > 0) {
-        cudaMemcpyAsync(idx_host_, idx_c_, count, cudaMemcpyDeviceToHost, copy_);
-        if (cudaStreamSynchronize(copy_) != cudaSuccess) {
-            st = cuda_status(cudaGetLastError(), "decompress: index copy");
-        }
-    }
     if (st == kOk && !dec.decode_y(tables_, idx_host_, count, ydec_host_, &err)) {
         set_last_error("decompress: " + err);
         st = kCorruptStream;
     }
     if (st == kOk) {
-        if (count > 0) {
-            cudaMemcpyAsync(y_dec_, ydec_host_, count, cudaMemcpyHostToDevice, copy_);
-        }
-        cudaEventRecord(ev_copy_, copy_);
-        cudaStreamWaitEvent(main_, ev_copy_, 0);
         st = run_phase(kDecSynthesis, main_);
     }
     if (st == kOk) {

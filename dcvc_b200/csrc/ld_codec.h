@@ -127,13 +127,20 @@ private:
     uint8_t* idx_host_ = nullptr;
     int8_t* ydec_host_ = nullptr;
     int8_t* z_host_ = nullptr;
+    // device addresses of the mapped host buffers above: the phase graphs move symbols, indexes,
+    // decoded values and their counts through them (launch_copy_counted)
+    int* count_hdev_ = nullptr;
+    int16_t* sym_hdev_ = nullptr;
+    uint8_t* idx_hdev_ = nullptr;
+    int8_t* ydec_hdev_ = nullptr;
+    int8_t* z_hdev_ = nullptr;
     bool memory_has_value_ = false;
 
     PhaseGraphs graphs_{kPhaseSlots};
     cudaStream_t main_ = nullptr;
-    cudaStream_t copy_ = nullptr;
-    cudaEvent_t ev_in_ = nullptr, ev_phase_ = nullptr, ev_copy_ = nullptr, ev_out_ = nullptr;
+    cudaEvent_t ev_in_ = nullptr, ev_phase_ = nullptr, ev_out_ = nullptr;
     int* err_word_ = nullptr;
+    ErrorSlot err_slot_;  // the error word as the phase graphs publish it
     int last_count_ = 0;
     int last_kernels_ = 0;
     int dev_ = 0;
