@@ -403,9 +403,13 @@ def htl_bench(stream, H, W, chunks=8, warmup=3):
             "reference_published": {"enc_fps_b200": 811.7, "dec_fps_b200": 551.6}}
 
 
-def ld_bench(stream, H, W, frames=32, warmup=4):
+def ld_bench(stream, H, W, frames=32, warmup=4, reset_interval=8):
     """The low-delay model (DMCLDProxy): encode-only and decode-only frames/s at 1080p, one frame
-    per call, QPs cycling as in the main workload; the reference publishes these for B200."""
+    per call, QPs cycling as in the main workload; the reference publishes these for B200.  The
+    temporal memory is reset with the test harness's rule (test_video.py:232-235,
+    (frame_idx + 1) % reset_interval == 1) every 8 frames: the random-init LD recurrence grows its
+    latents frame after frame (the bitrate rises 6x over 20 frames), and the reset keeps it at the
+    rate of the first frames."""
     from dcvc_b200 import synthetic
     from dcvc_b200.entropy_tables import add_cdf_to_state_dict
     from dcvc_b200.inference_extensions_cuda import DMCLDProxy
@@ -422,27 +426,32 @@ def ld_bench(stream, H, W, frames=32, warmup=4):
     dec.add_ref_feature_from_frame(ref, False)
     pr, pb = synthetic.padding_for(H, W)
     xs = [synthetic.to_model_input([f]) for f in yuv[1:]]
+
+    def reset_at(i):  # frame_idx = i + 1 after the intra frame
+        return (i + 2) % reset_interval == 1
+
     for i in range(warmup):
         qp = QPS[i % len(QPS)]
-        bits, ecp = enc.compress(xs[i % len(xs)], qp, False, pb, pr)
-        dec.decompress(bits, qp, H, W, ecp, False)
+        bits, ecp = enc.compress(xs[i % len(xs)], qp, reset_at(i), pb, pr)
+        dec.decompress(bits, qp, H, W, ecp, reset_at(i))
     torch.cuda.synchronize()
     e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
     payloads = []
     e[0].record(stream)
-    for i in range(frames):
+    for i in range(warmup, warmup + frames):
         qp = QPS[i % len(QPS)]
-        bits, ecp = enc.compress(xs[i % len(xs)], qp, False, pb, pr)
-        payloads.append((bits, qp, ecp))
+        bits, ecp = enc.compress(xs[i % len(xs)], qp, reset_at(i), pb, pr)
+        payloads.append((bits, qp, ecp, reset_at(i)))
     e[1].record(stream)
-    for bits, qp, ecp in payloads:
-        dec.decompress(bits, qp, H, W, ecp, False)
+    for bits, qp, ecp, reset in payloads:
+        dec.decompress(bits, qp, H, W, ecp, reset)
     e[2].record(stream)
     torch.cuda.synchronize()
     te, td = e[0].elapsed_time(e[1]) / frames, e[1].elapsed_time(e[2]) / frames
     return {"enc_fps": round(1e3 / te, 1), "dec_fps": round(1e3 / td, 1),
             "enc_ms_per_frame": round(te, 3), "dec_ms_per_frame": round(td, 3),
             "bytes_per_frame": int(np.mean([p[0].size for p in payloads])), "frames": frames,
+            "reset_interval": reset_interval,
             "reference_published": {"enc_fps_b200": 625.6, "dec_fps_b200": 621.9}}
 
 

@@ -1,6 +1,7 @@
 // extern "C" entry points of the host rANS coder (declared in include/dcvc_b200.h).
 #include "errors.h"
 #include "rans_coder.h"
+#include "rans_gpu.cuh"
 
 #include "../../include/dcvc_b200.h"
 
@@ -21,6 +22,11 @@ struct RansHandle {
 };
 
 RansHandle* as_handle(void* h) { return static_cast<RansHandle*>(h); }
+
+struct GpuRansHandle {
+    RansGpuTables tables;
+    void* storage = nullptr;
+};
 
 int fail(int status, const std::string& msg)
 {
@@ -160,5 +166,74 @@ int dcvc_rans_decode_y(void* h, const uint8_t* idx, int n, int8_t* out)
 }
 
 int dcvc_ec_parallel_for(int symbol_count) { return ec_parallel_for(symbol_count); }
+
+int dcvc_rans_gpu_create(void* rans_handle, void** gpu_handle)
+{
+    if (rans_handle == nullptr || gpu_handle == nullptr) {
+        return fail(kInvalidArgument, "dcvc_rans_gpu_create: null argument");
+    }
+    RansHandle* r = as_handle(rans_handle);
+    if (!r->tables.ready()) {
+        return fail(kNotReady, "dcvc_rans_gpu_create: both CDF table sets must be set first");
+    }
+    GpuRansHandle* g = nullptr;
+    try {
+        g = new GpuRansHandle();
+    } catch (const std::exception& e) {
+        return fail(kOutOfMemory, std::string("dcvc_rans_gpu_create: ") + e.what());
+    }
+    const cudaError_t e = rans_gpu_upload(r->tables, &g->tables, &g->storage);
+    if (e != cudaSuccess) {
+        delete g;
+        return cuda_status(e, "dcvc_rans_gpu_create");
+    }
+    *gpu_handle = g;
+    return kOk;
+}
+
+int dcvc_rans_gpu_destroy(void* gpu_handle)
+{
+    GpuRansHandle* g = static_cast<GpuRansHandle*>(gpu_handle);
+    if (g != nullptr) {
+        cudaFree(g->storage);
+        delete g;
+    }
+    return kOk;
+}
+
+size_t dcvc_rans_gpu_scratch_bytes(int n_y, int n_z, int ecp)
+{
+    return rans_gpu_scratch_bytes(n_y, n_z, ecp);
+}
+
+int dcvc_rans_gpu_encode(void* gpu_handle, const dcvc_rans_gpu_enc_job* jobs, int njobs,
+                         void* stream)
+{
+    if (gpu_handle == nullptr) {
+        return fail(kInvalidArgument, "dcvc_rans_gpu_encode: null handle");
+    }
+    const cudaError_t e = launch_rans_gpu_encode(static_cast<GpuRansHandle*>(gpu_handle)->tables,
+                                                 jobs, njobs, static_cast<cudaStream_t>(stream));
+    if (e == cudaErrorInvalidValue) {
+        return fail(kInvalidArgument, "dcvc_rans_gpu_encode: bad job (1..64 jobs, ec_parallel "
+                                      "1..8, z tables in range, non-null buffers)");
+    }
+    return cuda_status(e, "dcvc_rans_gpu_encode");
+}
+
+int dcvc_rans_gpu_decode(void* gpu_handle, const dcvc_rans_gpu_dec_job* jobs, int njobs,
+                         void* stream)
+{
+    if (gpu_handle == nullptr) {
+        return fail(kInvalidArgument, "dcvc_rans_gpu_decode: null handle");
+    }
+    const cudaError_t e = launch_rans_gpu_decode(static_cast<GpuRansHandle*>(gpu_handle)->tables,
+                                                 jobs, njobs, static_cast<cudaStream_t>(stream));
+    if (e == cudaErrorInvalidValue) {
+        return fail(kInvalidArgument, "dcvc_rans_gpu_decode: bad job (1..64 jobs, ec_parallel "
+                                      "1..8, z tables in range, non-null buffers)");
+    }
+    return cuda_status(e, "dcvc_rans_gpu_decode");
+}
 
 }  // extern "C"

@@ -20,6 +20,7 @@ struct Writer {
     size_t pos = 0;
     uint32_t x = kRansL;
     bool overflow = false;
+    bool zero_freq = false;  // a symbol with zero probability in its table (cannot be coded)
 
     void init(size_t cap)
     {
@@ -27,6 +28,7 @@ struct Writer {
         pos = cap;
         x = kRansL;
         overflow = false;
+        zero_freq = false;
     }
     inline void byte(uint8_t b)
     {
@@ -38,6 +40,10 @@ struct Writer {
     }
     inline void put(uint32_t start, uint32_t freq)
     {
+        if (freq == 0) {
+            zero_freq = true;
+            return;
+        }
         const uint32_t x_max = freq << kRenormShift;
         while (x >= x_max) {
             byte(static_cast<uint8_t>(x));
@@ -327,6 +333,10 @@ bool RansEncoderSession::finish(const RansTables& tables, std::vector<uint8_t>* 
         }
         if (w[i].overflow) {
             *err = "rANS encode: sub-stream buffer overflow";
+            return false;
+        }
+        if (w[i].zero_freq) {
+            *err = "rANS encode: a symbol has zero probability in its table";
             return false;
         }
     }

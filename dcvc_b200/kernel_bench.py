@@ -1,7 +1,7 @@
 """Micro-benchmark of the codec's kernels at their 1080p shapes (CUDA events on the launching
 stream), also the small fixed case used for ncu captures.
 
-    python -m dcvc_b200.kernel_bench [--case quad|wsilu|res|bias2048|dwconv|all] [--reps N]
+    python -m dcvc_b200.kernel_bench [--case quad|wsilu|res|bias2048|dwconv|rans|all] [--reps N]
                                      [--sets S] [--bn 0|64|128|256]
 
 Consecutive launches cycle through S independent operand sets (default: enough sets for 300 MB),
@@ -80,6 +80,77 @@ def run(name, reps=20, warmup=5, sets=0, bn=0):
             "gbs": round(byts / sec / 1e9, 1)}
 
 
+def rans(reps=5):
+    """rANS coding of one 1080p payload (y symbols of an HT-S chunk at a mid rate plus its z) on
+    the GPU (one warp per payload, one thread per sub-stream) and on the host threads, and of a
+    batch of 32 such payloads (independent streams) in one GPU launch.  Same bytes either way."""
+    import time
+
+    import numpy as np
+
+    from . import MLCodec_extensions_cpp as M
+    from .entropy_tables import gaussian_tables
+    from .rans_gpu import GpuRansCoder
+    qy, ly = gaussian_tables()
+    qz = np.tile(qy[:1], (64 * 128, 1)).astype(np.int32)
+    lz = np.tile(ly[:1], 64 * 128).astype(np.int32)
+    rng = np.random.default_rng(3)
+    ny, nz = 300000, 128 * 17 * 30
+    q = np.clip(np.round(rng.laplace(0, 1.2, ny)), -128, 127).astype(np.int64)
+    y = ((q << 8) + rng.integers(8, 40, ny)).astype(np.int16)
+    z = np.clip(np.round(rng.laplace(0, 1.0, nz)), -64, 63).astype(np.int8)
+    ecp = M.ec_parallel_for(ny)
+    g = GpuRansCoder(qz, lz, qy, ly)
+    yd, zd = torch.from_numpy(y).cuda(), torch.from_numpy(z).cuda()
+    job = {"y": yd, "z": zd, "z_offset": 0, "z_ch": 128, "ecp": ecp}
+    out = {"case": "rans", "symbols": ny + nz, "ec_parallel": ecp}
+    for name, jobs in (("gpu_1", [job]), ("gpu_32", [job] * 32)):
+        g.encode(jobs)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            outs, st = g.encode(jobs)
+        torch.cuda.synchronize()
+        te = (time.perf_counter() - t0) / reps
+        djobs = [{"data": outs[0], "ecp": ecp, "n_z": nz, "z_offset": 0, "z_ch": 128,
+                  "y_idx": (yd & 0xff).to(torch.uint8)}] * len(jobs)
+        g.decode(djobs)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            g.decode(djobs)
+        torch.cuda.synchronize()
+        td = (time.perf_counter() - t0) / reps
+        out[name] = {"payloads": len(jobs), "enc_ms": round(te * 1e3, 3), "dec_ms": round(td * 1e3, 3)}
+    enc = M.RansEncoder()
+    enc.set_cdf(qz, lz, 0)
+    enc.set_cdf(qy, ly, 1)
+    enc.set_entropy_coder_parallel(ecp)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        enc.reset()
+        enc.encode_y(y)
+        enc.encode_z(z, 0, 128)
+        enc.flush()
+    te = (time.perf_counter() - t0) / reps
+    ref = enc.get_encoded_stream()
+    dec = M.RansDecoder()
+    dec.set_cdf(qz, lz, 0)
+    dec.set_cdf(qy, ly, 1)
+    dec.set_entropy_coder_parallel(ecp)
+    idx = (y & 0xff).astype(np.uint8)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        dec.set_stream(ref)
+        dec.decode_z(nz, 0, 128)
+        dec.decode_y(idx)
+    td = (time.perf_counter() - t0) / reps
+    out["cpu_1"] = {"payloads": 1, "enc_ms": round(te * 1e3, 3), "dec_ms": round(td * 1e3, 3)}
+    out["bytes"] = int(ref.size)
+    out["identical"] = bool(outs[0].cpu().numpy().tobytes() == ref.tobytes())
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--case", default="all")
@@ -89,6 +160,9 @@ def main():
     args = ap.parse_args()
     cases = ["quad", "wsilu", "res", "bias2048", "dwconv"] if args.case == "all" else [args.case]
     for c in cases:
+        if c == "rans":
+            print(json.dumps(rans()), flush=True)
+            continue
         print(json.dumps(run(c, args.reps, sets=args.sets, bn=args.bn)), flush=True)
 
 

@@ -200,6 +200,49 @@ int dcvc_rans_decode_begin(void* handle, const uint8_t* data, size_t size, int e
 int dcvc_rans_decode_z(void* handle, int n, int cdf_offset, int ch, int8_t* out);
 int dcvc_rans_decode_y(void* handle, const uint8_t* idx, int n, int8_t* out);
 
+/* The same coder on the GPU (no reference counterpart: the reference codes on CPU threads,
+ * py_rans.cpp:96-102, 305-312).  Bytes are identical with dcvc_rans_* for the same symbols and
+ * ec_parallel; the container fixes the parallelism at one thread per sub-stream, so a launch codes
+ * up to 64 payloads (independent streams) with one warp each.  All pointers in a job are device
+ * pointers; status receives 0 or 1 (table index out of range), 2 (buffer overflow), 3 (bad
+ * container header), 4 (truncated or corrupt sub-stream), 5 (a symbol with zero probability in
+ * its table). */
+typedef struct {
+    const int16_t* y;   /* y symbols, (value << 8) + table index */
+    int n_y;
+    const int8_t* z;    /* z symbols, table (i % z_ch) + z_offset */
+    int n_z;
+    int z_offset;
+    int z_ch;
+    int ecp;            /* ec_parallel, 1..8 */
+    uint8_t* scratch;   /* dcvc_rans_gpu_scratch_bytes(n_y, n_z, ecp) bytes */
+    uint8_t* out;       /* the payload (container) */
+    int out_cap;
+    int* out_size;
+    int* status;
+} dcvc_rans_gpu_enc_job;
+typedef struct {
+    const uint8_t* data; /* the payload */
+    int size;
+    int ecp;
+    int n_z;
+    int z_offset;
+    int z_ch;
+    int8_t* z_out;
+    const uint8_t* y_idx; /* y table index per y symbol */
+    int n_y;
+    int8_t* y_out;
+    int* status;
+} dcvc_rans_gpu_dec_job;
+/* A device copy of the tables of a dcvc_rans handle (both table sets must be set). */
+int dcvc_rans_gpu_create(void* rans_handle, void** gpu_handle);
+int dcvc_rans_gpu_destroy(void* gpu_handle);
+size_t dcvc_rans_gpu_scratch_bytes(int n_y, int n_z, int ecp);
+int dcvc_rans_gpu_encode(void* gpu_handle, const dcvc_rans_gpu_enc_job* jobs, int njobs,
+                         void* stream);
+int dcvc_rans_gpu_decode(void* gpu_handle, const dcvc_rans_gpu_dec_job* jobs, int njobs,
+                         void* stream);
+
 /* ------------------------------------------------------------------ HT-S chunk codec */
 
 /* One handle = one video stream (its temporal context lives on the device inside the handle),
