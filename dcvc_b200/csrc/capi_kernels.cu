@@ -1,6 +1,7 @@
 // extern "C" kernel-level entry points (declared in include/dcvc_b200.h).
 #include "errors.h"
 #include "elementwise.cuh"
+#include "ffn_sm100.cuh"
 #include "gemm_sm100.cuh"
 #include "quant_tables.h"
 
@@ -78,6 +79,29 @@ int dcvc_conv1x1(int dtype, int epilogue, int M, int N, int K, const void* a, in
         return kInvalidArgument;
     }
     return cuda_status(e, "dcvc_conv1x1");
+}
+
+int dcvc_conv_ffn(int M, int C, int cffn, const void* x, int ldx, const void* w1, const float* b1,
+                  const void* w2, const float* b2, const void* qscale, void* out, int ldo,
+                  void* stream)
+{
+    FfnParams p{};
+    p.M = M;
+    p.C = C;
+    p.cffn = cffn;
+    p.b1 = b1;
+    p.b2 = b2;
+    p.qscale = qscale;
+    p.out = out;
+    p.ldo = ldo;
+    p.err = device_error_word();
+    cudaError_t e = ffn_sm100(x, ldx, w1, w2, p, static_cast<cudaStream_t>(stream));
+    if (e == cudaErrorInvalidValue) {
+        set_last_error("dcvc_conv_ffn: C must be a multiple of 256 and cffn 128 or 256, pitches "
+                       "multiples of 8 elements, pointers 16-byte aligned");
+        return kInvalidArgument;
+    }
+    return cuda_status(e, "dcvc_conv_ffn");
 }
 
 int dcvc_dwconv3x3(const void* x, int H, int W, int C, int ldx, const float* w, void* out, int ldo,

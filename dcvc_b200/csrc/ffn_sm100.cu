@@ -1,0 +1,533 @@
+// Fused ConvFFN of a DepthConvBlock (layers.py:115-125, layers_proxy.cpp:95-101) on tcgen05:
+//
+//   q   = sum_{k<4} WSiLU(x . W1[4c+k]^T + b1[4c+k])      (conv1x1_bias_wsilu_chunk_add)
+//   out = (q . W2^T + b2 + x) [* qscale]                   (conv1x1_bias_shortcut[_with_quant])
+//
+// in one persistent kernel.  Per 128-row tile the quad items (256 ffn.0 columns each) write their
+// 64 quad outputs straight into shared memory, laid out as one 128-byte-swizzled K block of the
+// second GEMM's A operand; the ffn.2 items then read that block with tcgen05.mma and finish with
+// the residual epilogue.  The quad output never goes to global memory and the block's two GEMM
+// launches become one.  The arithmetic is that of the two separate GEMMs (gemm_sm100.cu): the
+// same FP32 accumulation order, the quad output rounded to FP16 before the second GEMM, the same
+// epilogues, so the result is bit-identical.
+#include "ffn_sm100.cuh"
+
+#include "host_util.h"
+
+#include <cstring>
+#include <mutex>
+
+namespace dcvc {
+
+namespace {
+
+constexpr int kBM = 128;
+constexpr int kBK = 64;
+constexpr int kBN1 = 256;        // ffn.0 columns per quad item
+constexpr int kBN2 = 256;        // ffn.2 columns per output item
+constexpr int kEpiWarps = 8;     // two per TMEM lane quadrant, each owning half the columns
+constexpr int kThreads = 64 + 32 * kEpiWarps;
+constexpr long long kWaitLimit = 2000000000LL;  // ~1 s at 2 GHz
+constexpr int kSmemLimit = 232448;
+
+template <int QB>
+struct FfnCfg {
+    static constexpr int kABytes = kBM * kBK * 2;          // 16 KB: one K block of A (or of q)
+    static constexpr int kBBytes = kBN1 * kBK * 2;         // 32 KB: one K block of W1 or W2 rows
+    static constexpr int kStageBytes = kABytes + kBBytes;
+    static constexpr int kQBytes = QB * kABytes;           // q: QB K blocks
+    static constexpr int kEpiBytes = kEpiWarps * 8192;     // two residual / output boxes per warp
+    static constexpr int kBarBytes = 512;
+    static constexpr int kStagesFit =
+        (kSmemLimit - 1024 - kQBytes - kEpiBytes - kBarBytes) / kStageBytes;
+    static constexpr int kStages = kStagesFit > 4 ? 4 : kStagesFit;
+    static constexpr int kQOffset = kStages * kStageBytes;
+    static constexpr int kEpiOffset = kQOffset + kQBytes;
+    static constexpr int kBarOffset = kEpiOffset + kEpiBytes;
+    static constexpr int kBytes = kBarOffset + kBarBytes + 1024;
+    static constexpr int kTmemCols = 512;                  // two 256-column accumulators
+    static_assert(kStages >= 2, "shared memory too small for two pipeline stages");
+    static_assert(kBytes <= kSmemLimit, "shared memory budget exceeded");
+};
+
+// Byte offset of 16-byte chunk j of row r in a 128-byte-swizzled tile (the layout TMA writes for
+// SWIZZLE_128B and tcgen05 descriptors read).
+__device__ __forceinline__ int sw128_off(int r, int j) { return r * 128 + ((j ^ (r & 7)) << 4); }
+
+__device__ __forceinline__ uint32_t pack_h2(float a, float b)
+{
+    __half2 h = __floats2half2_rn(a, b);
+    return *reinterpret_cast<uint32_t*>(&h);
+}
+
+__device__ __forceinline__ float2 unpack_h2(uint32_t u)
+{
+    __half2 h = *reinterpret_cast<__half2*>(&u);
+    return __half22float2(h);
+}
+
+template <int QB, bool HASQ>
+__global__ void __launch_bounds__(kThreads, 1)
+    ffn_sm100_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmW1,
+                     const __grid_constant__ CUtensorMap tmW2, const __grid_constant__ CUtensorMap tmR,
+                     const __grid_constant__ CUtensorMap tmO, const FfnParams p)
+{
+    using C = FfnCfg<QB>;
+    constexpr int kStages = C::kStages;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem =
+        reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t* qbuf = smem + C::kQOffset;
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + C::kBarOffset);
+    uint64_t* empty = full + kStages;
+    uint64_t* tfull = empty + kStages;
+    uint64_t* tempty = tfull + 2;
+    uint64_t* qfull = tempty + 2;    // all quad items of a tile have written q
+    uint64_t* qempty = qfull + 1;    // the ffn.2 MMAs of a tile have read q
+    uint64_t* drain = qempty + 1;
+    uint64_t* resbar = drain + 1;    // [kEpiWarps][2]
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(resbar + 2 * kEpiWarps);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int num_m = (p.M + kBM - 1) / kBM;
+    const int nq = QB;                // quad items per tile = K blocks of q (64 outputs each)
+    const int nr = p.C / kBN2;        // output items per tile
+    const int kx = p.C / kBK;         // K blocks of x
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&tfull[b], 1);
+            mbar_init(&tempty[b], kEpiWarps);
+        }
+        mbar_init(qfull, kEpiWarps);
+        mbar_init(qempty, 1);
+        mbar_init(drain, 1);
+        for (int w = 0; w < 2 * kEpiWarps; ++w) {
+            mbar_init(&resbar[w], 1);
+        }
+        *abort_flag = 0;
+        fence_mbar_init();
+    }
+    if (warp == 0 && lane == 0) {
+        tma_prefetch_desc(&tmX);
+        tma_prefetch_desc(&tmW1);
+        tma_prefetch_desc(&tmW2);
+    }
+    if (warp == 1) {
+        tmem_alloc(tmem_slot, C::kTmemCols);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+    griddep_launch_dependents();
+    griddep_wait();
+
+    if (warp == 0) {
+        // ------------------------------------------------------------ TMA producer
+        if (lane == 0) {
+            int stage = 0;
+            uint32_t phase = 0;
+            int issued = 0;
+            for (int tile = blockIdx.x; tile < num_m && !*abort_flag; tile += gridDim.x) {
+                const int m0 = tile * kBM;
+                for (int it = 0; it < nq + nr && !*abort_flag; ++it) {
+                    const bool quad = it < nq;
+                    const int kbs = quad ? kx : nq;
+                    for (int kb = 0; kb < kbs; ++kb) {
+                        if (!mbar_wait_bounded(&empty[stage], phase ^ 1, kWaitLimit)) {
+                            *abort_flag = 1;
+                            report_error(p.err, kErrGemmProducerTimeout);
+                            break;
+                        }
+                        uint8_t* sa = smem + stage * C::kStageBytes;
+                        if (quad) {
+                            mbar_arrive_expect_tx(&full[stage], C::kStageBytes);
+                            tma_load_2d(sa, &tmX, &full[stage], kb * kBK, m0);
+                            tma_load_2d(sa + C::kABytes, &tmW1, &full[stage], kb * kBK, it * kBN1);
+                        } else {
+                            mbar_arrive_expect_tx(&full[stage], C::kBBytes);
+                            tma_load_2d(sa + C::kABytes, &tmW2, &full[stage], kb * kBK,
+                                        (it - nq) * kBN2);
+                        }
+                        ++issued;
+                        if (++stage == kStages) {
+                            stage = 0;
+                            phase ^= 1;
+                        }
+                    }
+                }
+            }
+            if (*abort_flag) {
+                // Let the copies this thread issued land before the CTA winds down.
+                int n = issued < kStages ? issued : kStages;
+                for (int i = 0; i < n; ++i) {
+                    if (--stage < 0) {
+                        stage = kStages - 1;
+                        phase ^= 1;
+                    }
+                    mbar_wait_bounded(&full[stage], phase, kWaitLimit / 16);
+                }
+            }
+        }
+    } else if (warp == 1) {
+        // ------------------------------------------------------------ MMA issuer
+        if (lane == 0) {
+            const uint32_t idesc = make_idesc_f16(kBM, kBN1, 0);
+            int stage = 0;
+            uint32_t phase = 0;
+            int acc = 0;
+            uint32_t acc_phase = 0;
+            bool issued_any = false;
+            int k = 0;
+            for (int tile = blockIdx.x; tile < num_m && !*abort_flag; tile += gridDim.x, ++k) {
+                for (int it = 0; it < nq + nr && !*abort_flag; ++it) {
+                    const bool quad = it < nq;
+                    if (it == nq) {
+                        // q of this tile is complete in shared memory
+                        if (!mbar_wait_bounded(qfull, k & 1, kWaitLimit)) {
+                            *abort_flag = 1;
+                            report_error(p.err, kErrGemmMmaTimeout);
+                            break;
+                        }
+                        tc_fence_after();
+                    }
+                    if (!mbar_wait_bounded(&tempty[acc], acc_phase ^ 1, kWaitLimit)) {
+                        *abort_flag = 1;
+                        report_error(p.err, kErrGemmMmaTimeout);
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t d = tmem_base + static_cast<uint32_t>(acc * kBN1);
+                    const int kbs = quad ? kx : nq;
+                    for (int kb = 0; kb < kbs; ++kb) {
+                        if (!mbar_wait_bounded(&full[stage], phase, kWaitLimit)) {
+                            *abort_flag = 1;
+                            report_error(p.err, kErrGemmMmaTimeout);
+                            break;
+                        }
+                        tc_fence_after();
+                        const uint8_t* sa = smem + stage * C::kStageBytes;
+                        const uint8_t* a = quad ? sa : qbuf + kb * C::kABytes;
+                        const uint64_t adesc = make_sw128_kmajor_desc(smem_u32(a));
+                        const uint64_t bdesc = make_sw128_kmajor_desc(smem_u32(sa + C::kABytes));
+#pragma unroll
+                        for (int kk = 0; kk < kBK / 16; ++kk) {
+                            tc_mma_f16(d, adesc + 2 * kk, bdesc + 2 * kk, idesc, (kb | kk) != 0 ? 1u : 0u);
+                        }
+                        issued_any = true;
+                        tc_commit(&empty[stage]);
+                        if (++stage == kStages) {
+                            stage = 0;
+                            phase ^= 1;
+                        }
+                    }
+                    if (*abort_flag) {
+                        break;
+                    }
+                    tc_commit(&tfull[acc]);
+                    acc ^= 1;
+                    if (acc == 0) {
+                        acc_phase ^= 1;
+                    }
+                }
+                if (*abort_flag) {
+                    break;
+                }
+                tc_commit(qempty);  // q may be overwritten once this tile's ffn.2 MMAs complete
+            }
+            if (*abort_flag && issued_any) {
+                tc_commit(drain);
+                mbar_wait_bounded(drain, 0, kWaitLimit / 16);
+            }
+        }
+    } else {
+        // ------------------------------------------------------------ epilogue warps
+        const int ew = warp - 2;
+        const int quad_lanes = warp & 3;          // TMEM lane quadrant this warp may access
+        const int half = ew >> 2;                 // which half of the item's 256 columns
+        uint8_t* wbuf = smem + C::kEpiOffset + ew * 8192;  // box b at wbuf + 4096 b
+        uint64_t* rbar = &resbar[2 * ew];
+        uint32_t res_phase = 0;
+        bool res_pending = false;
+        int acc = 0;
+        uint32_t acc_phase = 0;
+        if (lane == 0) {
+            tma_prefetch_desc(&tmO);
+            tma_prefetch_desc(&tmR);
+        }
+        int k = 0;
+        for (int tile = blockIdx.x; tile < num_m && !*abort_flag; tile += gridDim.x, ++k) {
+            const int m0 = tile * kBM;
+            const int row0 = m0 + quad_lanes * 32;   // first row owned by this warp
+            const bool rows_live = row0 < p.M;
+            const int r = quad_lanes * 32 + lane;    // this lane's row inside the tile
+            for (int it = 0; it < nq + nr && !*abort_flag; ++it) {
+                const bool quad = it < nq;
+                if (quad && it == 0 && k > 0) {
+                    // the previous tile's ffn.2 MMAs must have read q before it is overwritten
+                    if (!mbar_wait_bounded(qempty, (k - 1) & 1, kWaitLimit)) {
+                        *abort_flag = 1;
+                        report_error(p.err, kErrGemmEpilogueTimeout);
+                        break;
+                    }
+                }
+                const int ncol0 = (it - nq) * kBN2 + half * (kBN2 / 2);
+                if (!quad && rows_live && lane == 0) {
+                    // the residual (x) of both boxes, in flight while the accumulator finishes
+                    bulk_wait_read0();  // the previous item's stores have read the buffers
+                    for (int b = 0; b < 2; ++b) {
+                        mbar_arrive_expect_tx(&rbar[b], 4096);
+                        tma_load_2d(wbuf + 4096 * b, &tmR, &rbar[b], ncol0 + b * 64, row0);
+                    }
+                    res_pending = true;
+                }
+                if (!mbar_wait_bounded(&tfull[acc], acc_phase, kWaitLimit)) {
+                    *abort_flag = 1;
+                    report_error(p.err, kErrGemmEpilogueTimeout);
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t tbase = tmem_base + (static_cast<uint32_t>(quad_lanes * 32) << 16) +
+                                       acc * kBN1 + half * (kBN1 / 2);
+                if (quad) {
+                    // 128 accumulator columns -> 32 quad outputs of this row, written as four
+                    // 16-byte chunks of K block `it` of q
+                    uint8_t* qblk = qbuf + it * C::kABytes;
+#pragma unroll 1
+                    for (int c = 0; c < 4; ++c) {
+                        const int nc = it * kBN1 + half * (kBN1 / 2) + c * 32;
+                        const float4* b4 = reinterpret_cast<const float4*>(p.b1 + nc);
+                        float4 bb[8];
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) {
+                            bb[j] = __ldg(b4 + j);
+                        }
+                        uint32_t rr[32];
+                        tmem_ld_32x32b_x32(tbase + c * 32, rr);
+                        tc_wait_ld();
+                        float v[32];
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) {
+                            v[4 * j + 0] = __uint_as_float(rr[4 * j + 0]) + bb[j].x;
+                            v[4 * j + 1] = __uint_as_float(rr[4 * j + 1]) + bb[j].y;
+                            v[4 * j + 2] = __uint_as_float(rr[4 * j + 2]) + bb[j].z;
+                            v[4 * j + 3] = __uint_as_float(rr[4 * j + 3]) + bb[j].w;
+                        }
+                        uint32_t o[4];
+#pragma unroll
+                        for (int i = 0; i < 4; ++i) {
+                            const float s0 = wsilu(v[8 * i + 0]) + wsilu(v[8 * i + 1]) +
+                                             wsilu(v[8 * i + 2]) + wsilu(v[8 * i + 3]);
+                            const float s1 = wsilu(v[8 * i + 4]) + wsilu(v[8 * i + 5]) +
+                                             wsilu(v[8 * i + 6]) + wsilu(v[8 * i + 7]);
+                            o[i] = pack_h2(s0, s1);
+                        }
+                        *reinterpret_cast<uint4*>(qblk + sw128_off(r, half * 4 + c)) =
+                            make_uint4(o[0], o[1], o[2], o[3]);
+                    }
+                    tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) {
+                        mbar_arrive(&tempty[acc]);
+                    }
+                    if (it == nq - 1) {
+                        // q complete for this warp's rows: visible to the tensor cores
+                        fence_proxy_async_smem();
+                        __syncwarp();
+                        if (lane == 0) {
+                            mbar_arrive(qfull);
+                        }
+                    }
+                } else {
+                    // ffn.2 output: 128 columns per warp in two 64-column boxes; the result is
+                    // written over the box's residual and stored from there
+#pragma unroll 1
+                    for (int b = 0; b < 2; ++b) {
+                        const int ncol = ncol0 + b * 64;
+                        uint8_t* box = wbuf + 4096 * b;
+                        if (rows_live) {
+                            if (!mbar_wait_bounded(&rbar[b], res_phase, kWaitLimit)) {
+                                *abort_flag = 1;
+                                report_error(p.err, kErrGemmEpilogueTimeout);
+                            }
+                        }
+                        __syncwarp();
+#pragma unroll 1
+                        for (int c = 0; c < 2; ++c) {
+                            const int nc = ncol + c * 32;
+                            const float4* b4 = reinterpret_cast<const float4*>(p.b2 + nc);
+                            float4 bb[8];
+                            if constexpr (!HASQ) {
+#pragma unroll
+                                for (int j = 0; j < 8; ++j) {
+                                    bb[j] = __ldg(b4 + j);
+                                }
+                            }
+                            uint32_t rr[32];
+                            tmem_ld_32x32b_x32(tbase + b * 64 + c * 32, rr);
+                            tc_wait_ld();
+                            float v[32];
+#pragma unroll
+                            for (int j = 0; j < 8; ++j) {
+                                const float4 bj = HASQ ? __ldg(b4 + j) : bb[j];
+                                v[4 * j + 0] = __uint_as_float(rr[4 * j + 0]) + bj.x;
+                                v[4 * j + 1] = __uint_as_float(rr[4 * j + 1]) + bj.y;
+                                v[4 * j + 2] = __uint_as_float(rr[4 * j + 2]) + bj.z;
+                                v[4 * j + 3] = __uint_as_float(rr[4 * j + 3]) + bj.w;
+                            }
+#pragma unroll
+                            for (int j = 0; j < 4; ++j) {
+                                const uint4 u = *reinterpret_cast<const uint4*>(
+                                    box + sw128_off(lane, c * 4 + j));
+                                const float2 a = unpack_h2(u.x), bq = unpack_h2(u.y),
+                                             cc = unpack_h2(u.z), dd = unpack_h2(u.w);
+                                v[8 * j + 0] += a.x;
+                                v[8 * j + 1] += a.y;
+                                v[8 * j + 2] += bq.x;
+                                v[8 * j + 3] += bq.y;
+                                v[8 * j + 4] += cc.x;
+                                v[8 * j + 5] += cc.y;
+                                v[8 * j + 6] += dd.x;
+                                v[8 * j + 7] += dd.y;
+                            }
+                            if constexpr (HASQ) {
+                                const uint4* qs = reinterpret_cast<const uint4*>(
+                                    reinterpret_cast<const __half*>(p.qscale) + nc);
+#pragma unroll
+                                for (int j = 0; j < 4; ++j) {
+                                    const uint4 u = __ldg(qs + j);
+                                    const float2 a = unpack_h2(u.x), bq = unpack_h2(u.y),
+                                                 cc = unpack_h2(u.z), dd = unpack_h2(u.w);
+                                    v[8 * j + 0] *= a.x;
+                                    v[8 * j + 1] *= a.y;
+                                    v[8 * j + 2] *= bq.x;
+                                    v[8 * j + 3] *= bq.y;
+                                    v[8 * j + 4] *= cc.x;
+                                    v[8 * j + 5] *= cc.y;
+                                    v[8 * j + 6] *= dd.x;
+                                    v[8 * j + 7] *= dd.y;
+                                }
+                            }
+#pragma unroll
+                            for (int j = 0; j < 4; ++j) {
+                                *reinterpret_cast<uint4*>(box + sw128_off(lane, c * 4 + j)) =
+                                    make_uint4(pack_h2(v[8 * j + 0], v[8 * j + 1]),
+                                               pack_h2(v[8 * j + 2], v[8 * j + 3]),
+                                               pack_h2(v[8 * j + 4], v[8 * j + 5]),
+                                               pack_h2(v[8 * j + 6], v[8 * j + 7]));
+                            }
+                        }
+                        fence_proxy_async_smem();
+                        __syncwarp();
+                        if (lane == 0 && rows_live) {
+                            tma_store_2d(&tmO, box, ncol, row0);
+                            bulk_commit();
+                        }
+                        __syncwarp();
+                    }
+                    if (rows_live) {
+                        res_phase ^= 1;
+                        res_pending = false;
+                    }
+                    tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) {
+                        mbar_arrive(&tempty[acc]);
+                    }
+                }
+                acc ^= 1;
+                if (acc == 0) {
+                    acc_phase ^= 1;
+                }
+            }
+        }
+        if (lane == 0) {
+            if (res_pending) {
+                // after an abort, let this warp's residual loads land before the CTA winds down
+                mbar_wait_bounded(&rbar[0], res_phase, kWaitLimit / 16);
+                mbar_wait_bounded(&rbar[1], res_phase, kWaitLimit / 16);
+            }
+            bulk_wait_read0();
+        }
+        __syncwarp();
+    }
+
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc(tmem_base, C::kTmemCols);
+    }
+}
+
+template <int QB, bool HASQ>
+cudaError_t launch_ffn(const CUtensorMap (&m)[5], const FfnParams& p, cudaStream_t stream)
+{
+    using C = FfnCfg<QB>;
+    auto kernel = ffn_sm100_kernel<QB, HASQ>;
+    static std::once_flag once;
+    static cudaError_t attr_err = cudaSuccess;
+    std::call_once(once, [&] {
+        attr_err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, C::kBytes);
+    });
+    if (attr_err != cudaSuccess) {
+        return attr_err;
+    }
+    const int num_m = (p.M + kBM - 1) / kBM;
+    const int grid = num_m < num_sms() ? num_m : num_sms();
+    return launch_pdl(kernel, dim3(grid), dim3(kThreads), C::kBytes, stream, m[0], m[1], m[2],
+                      m[3], m[4], p);
+}
+
+}  // namespace
+
+bool ffn_sm100_supported(int C, int cffn, int n1)
+{
+    return C > 0 && C % kBN2 == 0 && (cffn == 128 || cffn == 256) && n1 == 4 * cffn;
+}
+
+bool ffn_sm100_preferred(int C, int cffn, int n1)
+{
+    // With cffn = 256 the on-chip quad tile (64 KB) leaves room for two operand stages only and
+    // the fused kernel is slower than the two GEMMs (64 us against 30 + 22 us for a 512-channel
+    // block at 1080p); with cffn = 128 it is faster (the LD codec gains 8-10 % per frame).
+    return ffn_sm100_supported(C, cffn, n1) && cffn == 128;
+}
+
+cudaError_t ffn_sm100(const void* x, int ldx, const void* w1, const void* w2, const FfnParams& p,
+                      cudaStream_t stream)
+{
+    if (p.M <= 0 || !ffn_sm100_supported(p.C, p.cffn, 4 * p.cffn) || ldx % 8 != 0 ||
+        p.ldo % 8 != 0 || p.b1 == nullptr || p.b2 == nullptr || p.out == nullptr ||
+        (reinterpret_cast<uintptr_t>(x) & 15) != 0 || (reinterpret_cast<uintptr_t>(w1) & 15) != 0 ||
+        (reinterpret_cast<uintptr_t>(w2) & 15) != 0 || (reinterpret_cast<uintptr_t>(p.out) & 15) != 0) {
+        return cudaErrorInvalidValue;
+    }
+    const CUtensorMapDataType dt = CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
+    CUtensorMap m[5];
+    std::memset(m, 0, sizeof(m));
+    const uint64_t xrow = static_cast<uint64_t>(ldx) * 2;
+    const int n1 = 4 * p.cffn;
+    if (!make_tmap_2d(&m[0], dt, x, p.C, p.M, xrow, kBK, kBM, 128) ||
+        !make_tmap_2d(&m[1], dt, w1, p.C, n1, static_cast<uint64_t>(p.C) * 2, kBK, kBN1, 128) ||
+        !make_tmap_2d(&m[2], dt, w2, p.cffn, p.C, static_cast<uint64_t>(p.cffn) * 2, kBK, kBN2, 128) ||
+        !make_tmap_2d(&m[3], dt, x, p.C, p.M, xrow, 64, 32, 128) ||
+        !make_tmap_2d(&m[4], dt, p.out, p.C, p.M, static_cast<uint64_t>(p.ldo) * 2, 64, 32, 128)) {
+        return cudaErrorInvalidValue;
+    }
+    const bool q = p.qscale != nullptr;
+    if (p.cffn == 128) {
+        return q ? launch_ffn<2, true>(m, p, stream) : launch_ffn<2, false>(m, p, stream);
+    }
+    return q ? launch_ffn<4, true>(m, p, stream) : launch_ffn<4, false>(m, p, stream);
+}
+
+}  // namespace dcvc

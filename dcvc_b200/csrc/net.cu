@@ -1,6 +1,7 @@
 #include "net.h"
 
 #include "elementwise.cuh"
+#include "ffn_sm100.cuh"
 #include "gemm_sm100.cuh"
 
 namespace dcvc {
@@ -321,6 +322,12 @@ void run_dcb(Launch& L, const Dcb& d, const __half* x, int ldx, int H, int W, __
     gemm(L, d.dc1, kEpiBiasWsilu, xin, ldin, M, s.t1, d.cdc);
     L.note(launch_dwconv3x3(s.t1, H, W, d.cdc, d.cdc, d.dw, s.t2, d.cdc, L.s));
     gemm(L, d.dc2, kEpiBiasRes, s.t2, d.cdc, M, s.t3, d.C, xin, ldin);
+    if (!d.shortcut && ffn_sm100_preferred(d.C, d.cffn, d.ffn1.cout)) {
+        // the ConvFFN as one kernel, the quad output kept on chip (ffn_sm100.cu)
+        FfnParams fp{M, d.C, d.cffn, d.ffn1.b, d.ffn2.b, q, out, ldo, L.err_word};
+        L.note(ffn_sm100(s.t3, d.C, d.ffn1.w, d.ffn2.w, fp, L.s));
+        return;
+    }
     gemm(L, d.ffn1, kEpiQuad, s.t3, d.C, M, s.t4, d.cffn);
     if (d.shortcut) {
         // conv1x1_bias_shortcut2 (layers_proxy.cpp:89-91): ffn + ffn input + block input

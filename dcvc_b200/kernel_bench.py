@@ -1,7 +1,7 @@
 """Micro-benchmark of the codec's kernels at their 1080p shapes (CUDA events on the launching
 stream), also the small fixed case used for ncu captures.
 
-    python -m dcvc_b200.kernel_bench [--case quad|wsilu|res|bias2048|dwconv|rans|all] [--reps N]
+    python -m dcvc_b200.kernel_bench [--case quad|wsilu|res|bias2048|dwconv|ffn|rans|all] [--reps N]
                                      [--sets S] [--bn 0|64|128|256]
 
 Consecutive launches cycle through S independent operand sets (default: enough sets for 300 MB),
@@ -27,6 +27,15 @@ def _case(name, g, bn=0):
     def rnd(*s, scale=1.0):
         return (torch.randn(*s, device="cuda", generator=g) * scale).half()
 
+    if name == "ffn":
+        # the fused ConvFFN of a 512-channel dcb2 block (quad GEMM + residual GEMM in one kernel)
+        x = rnd(M8, 512)
+        w1, w2 = rnd(1024, 512, scale=512 ** -0.5), rnd(512, 256, scale=256 ** -0.5)
+        b1 = torch.zeros(1024, device="cuda")
+        b2 = torch.zeros(512, device="cuda")
+        out = torch.empty_like(x)
+        fn = lambda: ops.conv_ffn(x, w1, b1, w2, b2, out=out)  # noqa: E731
+        return fn, 2.0 * M8 * (1024 * 512 + 512 * 256), (2 * x.numel() + w1.numel() + w2.numel()) * 2
     if name == "dwconv":
         x = rnd(M8, 256)
         w = torch.randn(9, 256, device="cuda", generator=g)
@@ -158,7 +167,7 @@ def main():
     ap.add_argument("--sets", type=int, default=0)
     ap.add_argument("--bn", type=int, default=0, help="GEMM N tile (0 = the library's choice)")
     args = ap.parse_args()
-    cases = ["quad", "wsilu", "res", "bias2048", "dwconv"] if args.case == "all" else [args.case]
+    cases = ["quad", "wsilu", "res", "bias2048", "dwconv", "ffn"] if args.case == "all" else [args.case]
     for c in cases:
         if c == "rans":
             print(json.dumps(rans()), flush=True)

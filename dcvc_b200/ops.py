@@ -44,6 +44,20 @@ def conv1x1(a, w, bias=None, epilogue=N.EPI_BIAS, res=None, res2=None, qscale=No
     return out
 
 
+def conv_ffn(x, w1, b1, w2, b2, qscale=None, out=None):
+    """Fused ConvFFN: (quad(x . w1^T + b1) . w2^T + b2 + x) [* qscale] for x [M, C] fp16;
+    w1 [4 cffn, C], w2 [C, cffn] fp16, b1 / b2 fp32."""
+    assert x.dim() == 2 and x.stride(1) == 1 and w1.is_contiguous() and w2.is_contiguous()
+    M, C = x.shape
+    cffn = w2.shape[1]
+    if out is None:
+        out = torch.empty((M, C), dtype=x.dtype, device=x.device)
+    N.check(N.lib.dcvc_conv_ffn(M, C, cffn, x.data_ptr(), x.stride(0), w1.data_ptr(),
+                                b1.data_ptr(), w2.data_ptr(), b2.data_ptr(), _ptr(qscale),
+                                out.data_ptr(), out.stride(0), _stream()), "dcvc_conv_ffn")
+    return out
+
+
 def dwconv3x3(x, H, W, w, out=None):
     """Depthwise 3x3 (pad 1, no bias) over an [H*W, C] NHWC tensor; w is fp32 [9, C]."""
     C = x.shape[1]
