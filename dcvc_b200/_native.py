@@ -61,7 +61,7 @@ _proto("dcvc_conv1x1", c_int,
 
 
 _proto("dcvc_conv_ffn", c_int, [c_int, c_int, c_int, c_vp, c_int, c_vp, c_vp, c_vp, c_vp, c_vp,
-                               c_vp, c_int, c_vp])
+                               c_vp, c_int, c_int, c_vp])
 _proto("dcvc_dwconv3x3", c_int, [c_vp, c_int, c_int, c_int, c_int, c_vp, c_vp, c_int, c_vp])
 
 

@@ -83,7 +83,7 @@ int dcvc_conv1x1(int dtype, int epilogue, int M, int N, int K, const void* a, in
 
 int dcvc_conv_ffn(int M, int C, int cffn, const void* x, int ldx, const void* w1, const float* b1,
                   const void* w2, const float* b2, const void* qscale, void* out, int ldo,
-                  void* stream)
+                  int block_n, void* stream)
 {
     FfnParams p{};
     p.M = M;
@@ -95,10 +95,11 @@ int dcvc_conv_ffn(int M, int C, int cffn, const void* x, int ldx, const void* w1
     p.out = out;
     p.ldo = ldo;
     p.err = device_error_word();
+    p.block_n = block_n;
     cudaError_t e = ffn_sm100(x, ldx, w1, w2, p, static_cast<cudaStream_t>(stream));
     if (e == cudaErrorInvalidValue) {
-        set_last_error("dcvc_conv_ffn: C must be a multiple of 256 and cffn 128 or 256, pitches "
-                       "multiples of 8 elements, pointers 16-byte aligned");
+        set_last_error("dcvc_conv_ffn: C must be a multiple of 256 and cffn 128 or 256, block_n "
+                       "0, 128 or 256, pitches multiples of 8 elements, pointers 16-byte aligned");
         return kInvalidArgument;
     }
     return cuda_status(e, "dcvc_conv_ffn");

@@ -23,20 +23,22 @@ namespace {
 
 constexpr int kBM = 128;
 constexpr int kBK = 64;
-constexpr int kBN1 = 256;        // ffn.0 columns per quad item
-constexpr int kBN2 = 256;        // ffn.2 columns per output item
 constexpr int kEpiWarps = 8;     // two per TMEM lane quadrant, each owning half the columns
 constexpr int kThreads = 64 + 32 * kEpiWarps;
 constexpr long long kWaitLimit = 2000000000LL;  // ~1 s at 2 GHz
 constexpr int kSmemLimit = 232448;
 
-template <int QB>
+// QB: K blocks of q (cffn / 64); BN: accumulator columns per item (256 or 128), the same for the
+// quad items (BN ffn.0 columns -> BN / 4 quad outputs) and the output items (BN ffn.2 columns).
+template <int QB, int BN>
 struct FfnCfg {
     static constexpr int kABytes = kBM * kBK * 2;          // 16 KB: one K block of A (or of q)
-    static constexpr int kBBytes = kBN1 * kBK * 2;         // 32 KB: one K block of W1 or W2 rows
+    static constexpr int kBBytes = BN * kBK * 2;           // one K block of BN W1 or W2 rows
     static constexpr int kStageBytes = kABytes + kBBytes;
     static constexpr int kQBytes = QB * kABytes;           // q: QB K blocks
-    static constexpr int kEpiBytes = kEpiWarps * 8192;     // two residual / output boxes per warp
+    static constexpr int kCols = BN / 2;                   // accumulator columns per epilogue warp
+    static constexpr int kBoxes = kCols / 64;              // 64-column output boxes per warp
+    static constexpr int kEpiBytes = kEpiWarps * kBoxes * 4096;  // residual / output boxes
     static constexpr int kBarBytes = 512;
     static constexpr int kStagesFit =
         (kSmemLimit - 1024 - kQBytes - kEpiBytes - kBarBytes) / kStageBytes;
@@ -45,7 +47,7 @@ struct FfnCfg {
     static constexpr int kEpiOffset = kQOffset + kQBytes;
     static constexpr int kBarOffset = kEpiOffset + kEpiBytes;
     static constexpr int kBytes = kBarOffset + kBarBytes + 1024;
-    static constexpr int kTmemCols = 512;                  // two 256-column accumulators
+    static constexpr int kTmemCols = 2 * BN;               // two accumulators
     static_assert(kStages >= 2, "shared memory too small for two pipeline stages");
     static_assert(kBytes <= kSmemLimit, "shared memory budget exceeded");
 };
@@ -66,13 +68,13 @@ __device__ __forceinline__ float2 unpack_h2(uint32_t u)
     return __half22float2(h);
 }
 
-template <int QB, bool HASQ>
+template <int QB, int BN, bool HASQ>
 __global__ void __launch_bounds__(kThreads, 1)
     ffn_sm100_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmW1,
                      const __grid_constant__ CUtensorMap tmW2, const __grid_constant__ CUtensorMap tmR,
                      const __grid_constant__ CUtensorMap tmO, const FfnParams p)
 {
-    using C = FfnCfg<QB>;
+    using C = FfnCfg<QB, BN>;
     constexpr int kStages = C::kStages;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem =
@@ -85,15 +87,15 @@ __global__ void __launch_bounds__(kThreads, 1)
     uint64_t* qfull = tempty + 2;    // all quad items of a tile have written q
     uint64_t* qempty = qfull + 1;    // the ffn.2 MMAs of a tile have read q
     uint64_t* drain = qempty + 1;
-    uint64_t* resbar = drain + 1;    // [kEpiWarps][2]
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(resbar + 2 * kEpiWarps);
+    uint64_t* resbar = drain + 1;    // [kEpiWarps][C::kBoxes]
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(resbar + C::kBoxes * kEpiWarps);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     const int num_m = (p.M + kBM - 1) / kBM;
-    const int nq = QB;                // quad items per tile = K blocks of q (64 outputs each)
-    const int nr = p.C / kBN2;        // output items per tile
+    const int nq = 4 * QB * kBK / BN; // quad items per tile (BN / 4 quad outputs each)
+    const int nr = p.C / BN;          // output items per tile
     const int kx = p.C / kBK;         // K blocks of x
 
     if (threadIdx.x == 0) {
@@ -108,7 +110,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         mbar_init(qfull, kEpiWarps);
         mbar_init(qempty, 1);
         mbar_init(drain, 1);
-        for (int w = 0; w < 2 * kEpiWarps; ++w) {
+        for (int w = 0; w < C::kBoxes * kEpiWarps; ++w) {
             mbar_init(&resbar[w], 1);
         }
         *abort_flag = 0;
@@ -140,7 +142,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 const int m0 = tile * kBM;
                 for (int it = 0; it < nq + nr && !*abort_flag; ++it) {
                     const bool quad = it < nq;
-                    const int kbs = quad ? kx : nq;
+                    const int kbs = quad ? kx : QB;
                     for (int kb = 0; kb < kbs; ++kb) {
                         if (!mbar_wait_bounded(&empty[stage], phase ^ 1, kWaitLimit)) {
                             *abort_flag = 1;
@@ -151,11 +153,11 @@ __global__ void __launch_bounds__(kThreads, 1)
                         if (quad) {
                             mbar_arrive_expect_tx(&full[stage], C::kStageBytes);
                             tma_load_2d(sa, &tmX, &full[stage], kb * kBK, m0);
-                            tma_load_2d(sa + C::kABytes, &tmW1, &full[stage], kb * kBK, it * kBN1);
+                            tma_load_2d(sa + C::kABytes, &tmW1, &full[stage], kb * kBK, it * BN);
                         } else {
                             mbar_arrive_expect_tx(&full[stage], C::kBBytes);
                             tma_load_2d(sa + C::kABytes, &tmW2, &full[stage], kb * kBK,
-                                        (it - nq) * kBN2);
+                                        (it - nq) * BN);
                         }
                         ++issued;
                         if (++stage == kStages) {
@@ -180,7 +182,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     } else if (warp == 1) {
         // ------------------------------------------------------------ MMA issuer
         if (lane == 0) {
-            const uint32_t idesc = make_idesc_f16(kBM, kBN1, 0);
+            const uint32_t idesc = make_idesc_f16(kBM, BN, 0);
             int stage = 0;
             uint32_t phase = 0;
             int acc = 0;
@@ -205,8 +207,8 @@ __global__ void __launch_bounds__(kThreads, 1)
                         break;
                     }
                     tc_fence_after();
-                    const uint32_t d = tmem_base + static_cast<uint32_t>(acc * kBN1);
-                    const int kbs = quad ? kx : nq;
+                    const uint32_t d = tmem_base + static_cast<uint32_t>(acc * BN);
+                    const int kbs = quad ? kx : QB;
                     for (int kb = 0; kb < kbs; ++kb) {
                         if (!mbar_wait_bounded(&full[stage], phase, kWaitLimit)) {
                             *abort_flag = 1;
@@ -253,8 +255,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         const int ew = warp - 2;
         const int quad_lanes = warp & 3;          // TMEM lane quadrant this warp may access
         const int half = ew >> 2;                 // which half of the item's 256 columns
-        uint8_t* wbuf = smem + C::kEpiOffset + ew * 8192;  // box b at wbuf + 4096 b
-        uint64_t* rbar = &resbar[2 * ew];
+        uint8_t* wbuf = smem + C::kEpiOffset + ew * C::kBoxes * 4096;  // box b at wbuf + 4096 b
+        uint64_t* rbar = &resbar[C::kBoxes * ew];
         uint32_t res_phase = 0;
         bool res_pending = false;
         int acc = 0;
@@ -279,11 +281,11 @@ __global__ void __launch_bounds__(kThreads, 1)
                         break;
                     }
                 }
-                const int ncol0 = (it - nq) * kBN2 + half * (kBN2 / 2);
+                const int ncol0 = (it - nq) * BN + half * C::kCols;
                 if (!quad && rows_live && lane == 0) {
                     // the residual (x) of both boxes, in flight while the accumulator finishes
                     bulk_wait_read0();  // the previous item's stores have read the buffers
-                    for (int b = 0; b < 2; ++b) {
+                    for (int b = 0; b < C::kBoxes; ++b) {
                         mbar_arrive_expect_tx(&rbar[b], 4096);
                         tma_load_2d(wbuf + 4096 * b, &tmR, &rbar[b], ncol0 + b * 64, row0);
                     }
@@ -296,14 +298,16 @@ __global__ void __launch_bounds__(kThreads, 1)
                 }
                 tc_fence_after();
                 const uint32_t tbase = tmem_base + (static_cast<uint32_t>(quad_lanes * 32) << 16) +
-                                       acc * kBN1 + half * (kBN1 / 2);
+                                       acc * BN + half * C::kCols;
                 if (quad) {
-                    // 128 accumulator columns -> 32 quad outputs of this row, written as four
-                    // 16-byte chunks of K block `it` of q
-                    uint8_t* qblk = qbuf + it * C::kABytes;
+                    // kCols accumulator columns -> kCols / 4 quad outputs of this row, written as
+                    // 16-byte chunks (8 outputs) into q: quad output j lives in K block j / 64,
+                    // chunk (j % 64) / 8
+                    const int q0 = (it * BN + half * C::kCols) / 4;  // first quad output
+                    uint8_t* qblk = qbuf + (q0 / 64) * C::kABytes;
 #pragma unroll 1
-                    for (int c = 0; c < 4; ++c) {
-                        const int nc = it * kBN1 + half * (kBN1 / 2) + c * 32;
+                    for (int c = 0; c < C::kCols / 32; ++c) {
+                        const int nc = it * BN + half * C::kCols + c * 32;
                         const float4* b4 = reinterpret_cast<const float4*>(p.b1 + nc);
                         float4 bb[8];
 #pragma unroll
@@ -330,7 +334,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                                              wsilu(v[8 * i + 6]) + wsilu(v[8 * i + 7]);
                             o[i] = pack_h2(s0, s1);
                         }
-                        *reinterpret_cast<uint4*>(qblk + sw128_off(r, half * 4 + c)) =
+                        *reinterpret_cast<uint4*>(qblk + sw128_off(r, (q0 % 64) / 8 + c)) =
                             make_uint4(o[0], o[1], o[2], o[3]);
                     }
                     tc_fence_before();
@@ -350,7 +354,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                     // ffn.2 output: 128 columns per warp in two 64-column boxes; the result is
                     // written over the box's residual and stored from there
 #pragma unroll 1
-                    for (int b = 0; b < 2; ++b) {
+                    for (int b = 0; b < C::kBoxes; ++b) {
                         const int ncol = ncol0 + b * 64;
                         uint8_t* box = wbuf + 4096 * b;
                         if (rows_live) {
@@ -452,8 +456,9 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (lane == 0) {
             if (res_pending) {
                 // after an abort, let this warp's residual loads land before the CTA winds down
-                mbar_wait_bounded(&rbar[0], res_phase, kWaitLimit / 16);
-                mbar_wait_bounded(&rbar[1], res_phase, kWaitLimit / 16);
+                for (int b = 0; b < C::kBoxes; ++b) {
+                    mbar_wait_bounded(&rbar[b], res_phase, kWaitLimit / 16);
+                }
             }
             bulk_wait_read0();
         }
@@ -468,11 +473,11 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
 }
 
-template <int QB, bool HASQ>
+template <int QB, int BN, bool HASQ>
 cudaError_t launch_ffn(const CUtensorMap (&m)[5], const FfnParams& p, cudaStream_t stream)
 {
-    using C = FfnCfg<QB>;
-    auto kernel = ffn_sm100_kernel<QB, HASQ>;
+    using C = FfnCfg<QB, BN>;
+    auto kernel = ffn_sm100_kernel<QB, BN, HASQ>;
     static std::once_flag once;
     static cudaError_t attr_err = cudaSuccess;
     std::call_once(once, [&] {
@@ -491,14 +496,16 @@ cudaError_t launch_ffn(const CUtensorMap (&m)[5], const FfnParams& p, cudaStream
 
 bool ffn_sm100_supported(int C, int cffn, int n1)
 {
-    return C > 0 && C % kBN2 == 0 && (cffn == 128 || cffn == 256) && n1 == 4 * cffn;
+    return C > 0 && C % 256 == 0 && (cffn == 128 || cffn == 256) && n1 == 4 * cffn;
 }
 
 bool ffn_sm100_preferred(int C, int cffn, int n1)
 {
-    // With cffn = 256 the on-chip quad tile (64 KB) leaves room for two operand stages only and
-    // the fused kernel is slower than the two GEMMs (64 us against 30 + 22 us for a 512-channel
-    // block at 1080p); with cffn = 128 it is faster (the LD codec gains 8-10 % per frame).
+    // With cffn = 256 the fused kernel is slower than the two GEMMs (65 us against 33 + 22 us for
+    // a 512-channel block at 1080p): each tile's output items wait for all of its quad items, and
+    // with two accumulators the next tile's quad items wait for the output epilogues, so the
+    // tensor pipe idles; the 64 KB q tile also leaves two operand stages.  With cffn = 128 it is
+    // faster (the LD codec gains 8-10 % per frame).
     return ffn_sm100_supported(C, cffn, n1) && cffn == 128;
 }
 
@@ -516,18 +523,31 @@ cudaError_t ffn_sm100(const void* x, int ldx, const void* w1, const void* w2, co
     std::memset(m, 0, sizeof(m));
     const uint64_t xrow = static_cast<uint64_t>(ldx) * 2;
     const int n1 = 4 * p.cffn;
+    // item width: 256 measured faster than 128 for both q widths (a 512-channel block at 1080p:
+    // 65 against 71 us; the four operand stages that 128 allows do not make up for the q
+    // dependency, which serialises a tile's output items behind all of its quad items)
+    const int bn = p.block_n != 0 ? p.block_n : 256;
+    if (bn != 128 && bn != 256) {
+        return cudaErrorInvalidValue;
+    }
     if (!make_tmap_2d(&m[0], dt, x, p.C, p.M, xrow, kBK, kBM, 128) ||
-        !make_tmap_2d(&m[1], dt, w1, p.C, n1, static_cast<uint64_t>(p.C) * 2, kBK, kBN1, 128) ||
-        !make_tmap_2d(&m[2], dt, w2, p.cffn, p.C, static_cast<uint64_t>(p.cffn) * 2, kBK, kBN2, 128) ||
+        !make_tmap_2d(&m[1], dt, w1, p.C, n1, static_cast<uint64_t>(p.C) * 2, kBK, bn, 128) ||
+        !make_tmap_2d(&m[2], dt, w2, p.cffn, p.C, static_cast<uint64_t>(p.cffn) * 2, kBK, bn, 128) ||
         !make_tmap_2d(&m[3], dt, x, p.C, p.M, xrow, 64, 32, 128) ||
         !make_tmap_2d(&m[4], dt, p.out, p.C, p.M, static_cast<uint64_t>(p.ldo) * 2, 64, 32, 128)) {
         return cudaErrorInvalidValue;
     }
     const bool q = p.qscale != nullptr;
     if (p.cffn == 128) {
-        return q ? launch_ffn<2, true>(m, p, stream) : launch_ffn<2, false>(m, p, stream);
+        if (bn == 256) {
+            return q ? launch_ffn<2, 256, true>(m, p, stream) : launch_ffn<2, 256, false>(m, p, stream);
+        }
+        return q ? launch_ffn<2, 128, true>(m, p, stream) : launch_ffn<2, 128, false>(m, p, stream);
     }
-    return q ? launch_ffn<4, true>(m, p, stream) : launch_ffn<4, false>(m, p, stream);
+    if (bn == 256) {
+        return q ? launch_ffn<4, 256, true>(m, p, stream) : launch_ffn<4, 256, false>(m, p, stream);
+    }
+    return q ? launch_ffn<4, 128, true>(m, p, stream) : launch_ffn<4, 128, false>(m, p, stream);
 }
 
 }  // namespace dcvc

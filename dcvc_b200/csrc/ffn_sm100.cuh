@@ -18,6 +18,7 @@ struct FfnParams {
     void* out;           // [M, C] rows, pitch ldo
     int ldo;
     int* err;            // device error word
+    int block_n;         // accumulator columns per item, 128 or 256 (0: the library's choice)
 };
 
 // Whether ffn_sm100 handles a block with these channel counts (n1 = ffn.0 output channels), and

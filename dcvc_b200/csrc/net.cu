@@ -324,7 +324,7 @@ void run_dcb(Launch& L, const Dcb& d, const __half* x, int ldx, int H, int W, __
     gemm(L, d.dc2, kEpiBiasRes, s.t2, d.cdc, M, s.t3, d.C, xin, ldin);
     if (!d.shortcut && ffn_sm100_preferred(d.C, d.cffn, d.ffn1.cout)) {
         // the ConvFFN as one kernel, the quad output kept on chip (ffn_sm100.cu)
-        FfnParams fp{M, d.C, d.cffn, d.ffn1.b, d.ffn2.b, q, out, ldo, L.err_word};
+        FfnParams fp{M, d.C, d.cffn, d.ffn1.b, d.ffn2.b, q, out, ldo, L.err_word, 0};
         L.note(ffn_sm100(s.t3, d.C, d.ffn1.w, d.ffn2.w, fp, L.s));
         return;
     }

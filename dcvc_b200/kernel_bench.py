@@ -34,7 +34,7 @@ def _case(name, g, bn=0):
         b1 = torch.zeros(1024, device="cuda")
         b2 = torch.zeros(512, device="cuda")
         out = torch.empty_like(x)
-        fn = lambda: ops.conv_ffn(x, w1, b1, w2, b2, out=out)  # noqa: E731
+        fn = lambda: ops.conv_ffn(x, w1, b1, w2, b2, out=out, block_n=bn)  # noqa: E731
         return fn, 2.0 * M8 * (1024 * 512 + 512 * 256), (2 * x.numel() + w1.numel() + w2.numel()) * 2
     if name == "dwconv":
         x = rnd(M8, 256)

@@ -44,7 +44,7 @@ def conv1x1(a, w, bias=None, epilogue=N.EPI_BIAS, res=None, res2=None, qscale=No
     return out
 
 
-def conv_ffn(x, w1, b1, w2, b2, qscale=None, out=None):
+def conv_ffn(x, w1, b1, w2, b2, qscale=None, out=None, block_n=0):
     """Fused ConvFFN: (quad(x . w1^T + b1) . w2^T + b2 + x) [* qscale] for x [M, C] fp16;
     w1 [4 cffn, C], w2 [C, cffn] fp16, b1 / b2 fp32."""
     assert x.dim() == 2 and x.stride(1) == 1 and w1.is_contiguous() and w2.is_contiguous()
@@ -54,7 +54,8 @@ def conv_ffn(x, w1, b1, w2, b2, qscale=None, out=None):
         out = torch.empty((M, C), dtype=x.dtype, device=x.device)
     N.check(N.lib.dcvc_conv_ffn(M, C, cffn, x.data_ptr(), x.stride(0), w1.data_ptr(),
                                 b1.data_ptr(), w2.data_ptr(), b2.data_ptr(), _ptr(qscale),
-                                out.data_ptr(), out.stride(0), _stream()), "dcvc_conv_ffn")
+                                out.data_ptr(), out.stride(0), block_n, _stream()),
+            "dcvc_conv_ffn")
     return out
 
 

@@ -83,11 +83,12 @@ int dcvc_conv1x1(int dtype, int epilogue, int M, int N, int K, const void* a, in
  * conv1x1_bias_wsilu_chunk_add quad GEMM followed by conv1x1_bias_shortcut[_with_quant]):
  * out = (quad(x . w1^T + b1) . w2^T + b2 + x) [* qscale], with the quad output kept on chip.
  * x, out [M, C] FP16 (pitches ldx, ldo), w1 [4 cffn, C] (rows 4c+k), w2 [C, cffn], b1 / b2 FP32,
- * qscale [C] FP16 or NULL.  C a multiple of 256, cffn 128 or 256.  Bit-identical with the two
- * dcvc_conv1x1 calls (DCVC_EPI_QUAD, then DCVC_EPI_BIAS_RES / _RES_Q). */
+ * qscale [C] FP16 or NULL.  C a multiple of 256, cffn 128 or 256; block_n = accumulator columns
+ * per work item, 128 or 256 (0 = choose).  Bit-identical with the two dcvc_conv1x1 calls
+ * (DCVC_EPI_QUAD, then DCVC_EPI_BIAS_RES / _RES_Q). */
 int dcvc_conv_ffn(int M, int C, int cffn, const void* x, int ldx, const void* w1, const float* b1,
                   const void* w2, const float* b2, const void* qscale, void* out, int ldo,
-                  void* stream);
+                  int block_n, void* stream);
 
 /* Depthwise 3x3, pad 1, no bias, FP32 accumulation: x, out [H*W, C] FP16 (pitches ldx, ldo),
  * w FP32 [9][C] tap-major.  Replaces d3x3 (src/layers/extensions/inference/cutlass/

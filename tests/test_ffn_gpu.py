@@ -18,10 +18,11 @@ def _weights(C, cffn, g):
     return w1, b1, w2, b2
 
 
+@pytest.mark.parametrize("bn", [0, 128, 256])
 @pytest.mark.parametrize("M,C,cffn,with_q,pitch", [
     (32640, 512, 256, False, 0), (1000, 512, 256, True, 0), (8160, 256, 128, False, 0),
     (777, 256, 128, True, 0), (4096, 768, 256, False, 0), (2000, 256, 128, False, 512)])
-def test_fused_matches_two_gemms(M, C, cffn, with_q, pitch):
+def test_fused_matches_two_gemms(M, C, cffn, with_q, pitch, bn):
     g = torch.Generator(device="cuda").manual_seed(M + C + cffn)
     x = torch.randn(M, C, device="cuda", generator=g).half()
     w1, b1, w2, b2 = _weights(C, cffn, g)
@@ -31,10 +32,10 @@ def test_fused_matches_two_gemms(M, C, cffn, with_q, pitch):
     ref = ops.conv1x1(quad, w2, b2, epi, res=x, qscale=q)
     if pitch:
         buf = torch.full((M, pitch), float("nan"), device="cuda", dtype=torch.float16)
-        out = ops.conv_ffn(x, w1, b1, w2, b2, qscale=q, out=buf[:, 64:64 + C])
+        out = ops.conv_ffn(x, w1, b1, w2, b2, qscale=q, out=buf[:, 64:64 + C], block_n=bn)
         assert torch.isnan(buf[:, :64]).all() and torch.isnan(buf[:, 64 + C:]).all()
     else:
-        out = ops.conv_ffn(x, w1, b1, w2, b2, qscale=q)
+        out = ops.conv_ffn(x, w1, b1, w2, b2, qscale=q, block_n=bn)
     torch.cuda.synchronize()
     assert N.device_error() == 0
     assert torch.equal(out.view(torch.int16), ref.view(torch.int16))
