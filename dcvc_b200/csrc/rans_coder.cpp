@@ -2,7 +2,13 @@
 
 #include <algorithm>
 #include <cstring>
+#include <memory>
+#include <condition_variable>
+#include <functional>
+#include <mutex>
 #include <thread>
+
+#include <unistd.h>
 
 namespace dcvc {
 
@@ -14,18 +20,22 @@ constexpr int kRenormShift = 23 - kScaleBits + 8;  // 15
 constexpr uint32_t kBypassMax = 3;                 // 2-bit bypass digits
 constexpr uint32_t kBypassXMax = (1u << (kScaleBits - 2)) << kRenormShift;
 
-// Sub-stream writer: bytes are produced back to front.
+// Sub-stream writer: bytes are produced back to front.  Each coding thread works on a Writer of
+// its own stack (moved out when done): writers side by side in one array would share cache lines
+// that every symbol updates.
 struct Writer {
-    std::vector<uint8_t> buf;
+    std::unique_ptr<uint8_t[]> buf;  // not zero-filled: every byte handed out is written
+    size_t cap = 0;
     size_t pos = 0;
     uint32_t x = kRansL;
     bool overflow = false;
     bool zero_freq = false;  // a symbol with zero probability in its table (cannot be coded)
 
-    void init(size_t cap)
+    void init(size_t n)
     {
-        buf.assign(cap, 0);
-        pos = cap;
+        buf.reset(new uint8_t[n]);
+        cap = n;
+        pos = n;
         x = kRansL;
         overflow = false;
         zero_freq = false;
@@ -38,18 +48,19 @@ struct Writer {
         }
         buf[--pos] = b;
     }
-    inline void put(uint32_t start, uint32_t freq)
+    inline void put(const RansEncSym& e)
     {
-        if (freq == 0) {
+        if (e.x_max == 0) {
             zero_freq = true;
             return;
         }
-        const uint32_t x_max = freq << kRenormShift;
-        while (x >= x_max) {
+        while (x >= e.x_max) {
             byte(static_cast<uint8_t>(x));
             x >>= 8;
         }
-        x = ((x / freq) << kScaleBits) + (x % freq) + start;
+        const uint32_t q =
+            static_cast<uint32_t>((static_cast<uint64_t>(x) * e.rcp) >> 32) >> e.shift;
+        x += e.bias + q * e.cmpl;
     }
     inline void bits(uint32_t v)
     {
@@ -59,7 +70,7 @@ struct Writer {
         }
         x = (x << 2) | v;
     }
-    inline void symbol(int32_t s, int32_t maxv, const uint32_t* enc)
+    inline void symbol(int32_t s, int32_t maxv, const RansEncSym* enc)
     {
         int32_t v = (s < 0 ? -s : s) * 2 - (s > 0);
         if (v >= maxv) {
@@ -84,8 +95,7 @@ struct Writer {
             }
             v = maxv;
         }
-        const uint32_t e = enc[v];
-        put(e & 0xffff, e >> 16);
+        put(enc[v]);
     }
     void flush()
     {
@@ -93,8 +103,8 @@ struct Writer {
             byte(static_cast<uint8_t>(x >> (8 * k)));
         }
     }
-    const uint8_t* data() const { return buf.data() + pos; }
-    int size() const { return static_cast<int>(buf.size() - pos); }
+    const uint8_t* data() const { return buf.get() + pos; }
+    int size() const { return static_cast<int>(cap - pos); }
 };
 
 inline void split(int n, int parts, int i, int* begin, int* end)
@@ -120,6 +130,70 @@ int shared_tail(const uint8_t* a, int na, const uint8_t* b, int nb)
     return k;
 }
 
+// Persistent workers for the sub-stream tasks of one calling thread (a codec stream's host
+// thread): spawning threads on every call cost as much as coding a small payload.  Workers are
+// created on first use, one per extra sub-stream, and joined when the calling thread exits; a
+// forked child gets a pool of its own.
+class WorkerPool {
+public:
+    ~WorkerPool()
+    {
+        {
+            std::lock_guard<std::mutex> lk(m_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto& t : th_) {
+            t.join();
+        }
+    }
+    void run(int n, const std::function<void(int)>& f)
+    {
+        while (static_cast<int>(th_.size()) < n - 1) {
+            th_.emplace_back([this] { work(); });
+        }
+        {
+            std::lock_guard<std::mutex> lk(m_);
+            fn_ = &f;
+            next_ = 1;
+            n_ = n;
+            left_ = n - 1;
+        }
+        cv_.notify_all();
+        f(0);
+        std::unique_lock<std::mutex> lk(m_);
+        done_.wait(lk, [this] { return left_ == 0; });
+        fn_ = nullptr;
+    }
+
+private:
+    void work()
+    {
+        std::unique_lock<std::mutex> lk(m_);
+        for (;;) {
+            cv_.wait(lk, [this] { return stop_ || next_ < n_; });
+            if (stop_) {
+                return;
+            }
+            const int i = next_++;
+            const std::function<void(int)>* f = fn_;
+            lk.unlock();
+            (*f)(i);
+            lk.lock();
+            if (--left_ == 0) {
+                done_.notify_one();
+            }
+        }
+    }
+
+    std::mutex m_;
+    std::condition_variable cv_, done_;
+    std::vector<std::thread> th_;
+    const std::function<void(int)>* fn_ = nullptr;
+    int next_ = 0, n_ = 0, left_ = 0;
+    bool stop_ = false;
+};
+
 template <typename F>
 void run_parallel(int n, F&& f)
 {
@@ -127,15 +201,15 @@ void run_parallel(int n, F&& f)
         f(0);
         return;
     }
-    std::vector<std::thread> th;
-    th.reserve(n - 1);
-    for (int i = 1; i < n; ++i) {
-        th.emplace_back([&f, i] { f(i); });
+    thread_local std::unique_ptr<WorkerPool> pool;
+    thread_local pid_t owner = 0;
+    if (pool == nullptr || owner != getpid()) {
+        (void)pool.release();  // a pool inherited through fork() has no threads: leave it
+        pool.reset(new WorkerPool());
+        owner = getpid();
     }
-    f(0);
-    for (auto& t : th) {
-        t.join();
-    }
+    const std::function<void(int)> fn = std::forward<F>(f);
+    pool->run(n, fn);
 }
 
 }  // namespace
@@ -211,6 +285,7 @@ bool RansTables::set(int index, const int32_t* cdf, const int32_t* lengths, int 
     t.cdf.assign(cdf, cdf + static_cast<size_t>(count) * stride);
     t.max_value.resize(count);
     t.enc.assign(static_cast<size_t>(count) * stride, 0);
+    t.esym.assign(static_cast<size_t>(count) * stride, RansEncSym{});
     for (int i = 0; i < count; ++i) {
         const int len = lengths[i];
         if (len < 3 || len > stride) {
@@ -223,6 +298,23 @@ bool RansTables::set(int index, const int32_t* cdf, const int32_t* lengths, int 
             const uint32_t start = static_cast<uint16_t>(c[j]);
             const uint32_t freq = static_cast<uint16_t>(c[j + 1] - c[j]);
             t.enc[static_cast<size_t>(i) * stride + j] = start | (freq << 16);
+            RansEncSym& es = t.esym[static_cast<size_t>(i) * stride + j];
+            es.x_max = freq << kRenormShift;
+            es.cmpl = static_cast<uint16_t>((1u << kScaleBits) - freq);
+            if (freq < 2) {
+                // q = x - 1 from the multiply-high, made up for by the bias
+                es.rcp = ~0u;
+                es.shift = 0;
+                es.bias = start + (1u << kScaleBits) - 1;
+            } else {
+                uint32_t sh = 0;
+                while (freq > (1u << sh)) {
+                    ++sh;
+                }
+                es.rcp = static_cast<uint32_t>(((uint64_t{1} << (sh + 31)) + freq - 1) / freq);
+                es.shift = static_cast<uint16_t>(sh - 1);
+                es.bias = start;
+            }
         }
     }
     t_[index] = std::move(t);
@@ -300,7 +392,8 @@ bool RansEncoderSession::finish(const RansTables& tables, std::vector<uint8_t>* 
     Writer w[kMaxEcParallel];
     bool bad_index[kMaxEcParallel] = {false};
     run_parallel(ecp, [&](int i) {
-        w[i].init(cap[i] + 16);
+        Writer lw;
+        lw.init(cap[i] + 16);
         for (const Segment& sg : segs_) {
             int b, e;
             split(sg.n, ecp, i, &b, &e);
@@ -313,18 +406,19 @@ bool RansEncoderSession::finish(const RansTables& tables, std::vector<uint8_t>* 
                         return;
                     }
                     const int32_t s = static_cast<int8_t>(c >> 8);
-                    w[i].symbol(s, ty.max_value[idx],
-                                ty.enc.data() + static_cast<size_t>(idx) * ty.stride);
+                    lw.symbol(s, ty.max_value[idx],
+                              ty.esym.data() + static_cast<size_t>(idx) * ty.stride);
                 }
             } else {
                 for (int k = e - 1; k >= b; --k) {
                     const int t = (k % sg.ch) + sg.cdf_offset;
-                    w[i].symbol(sg.z[k], tz.max_value[t],
-                                tz.enc.data() + static_cast<size_t>(t) * tz.stride);
+                    lw.symbol(sg.z[k], tz.max_value[t],
+                              tz.esym.data() + static_cast<size_t>(t) * tz.stride);
                 }
             }
         }
-        w[i].flush();
+        lw.flush();
+        w[i] = std::move(lw);
     });
     for (int i = 0; i < ecp; ++i) {
         if (bad_index[i]) {
@@ -509,7 +603,7 @@ bool RansDecoderSession::decode_z(const RansTables& tables, int n, int cdf_offse
         return false;
     }
     run_parallel(ecp_, [&](int i) {
-        Reader& r = r_[i];
+        Reader r = r_[i];  // a copy on this thread's stack (see Writer)
         int b, e;
         split(n, ecp_, i, &b, &e);
         for (int k = b; k < e; ++k) {
@@ -518,6 +612,7 @@ bool RansDecoderSession::decode_z(const RansTables& tables, int n, int cdf_offse
                                tz.cdf.data() + static_cast<size_t>(t) * tz.stride, tz.max_value[t],
                                tz.stride - 1);
         }
+        r_[i] = r;
     });
     for (int i = 0; i < ecp_; ++i) {
         if (r_[i].overrun) {
@@ -538,19 +633,20 @@ bool RansDecoderSession::decode_y(const RansTables& tables, const uint8_t* idx, 
     }
     bool bad[kMaxEcParallel] = {false};
     run_parallel(ecp_, [&](int i) {
-        Reader& r = r_[i];
+        Reader r = r_[i];  // a copy on this thread's stack (see Writer)
         int b, e;
         split(n, ecp_, i, &b, &e);
         for (int k = b; k < e; ++k) {
             const int t = idx[k];
             if (t >= ty.count) {
                 bad[i] = true;
-                return;
+                break;
             }
             out[k] = rd_symbol(r.x, r.p, r.end, r.overrun,
                                ty.cdf.data() + static_cast<size_t>(t) * ty.stride, ty.max_value[t],
                                ty.stride - 1);
         }
+        r_[i] = r;
     });
     for (int i = 0; i < ecp_; ++i) {
         if (bad[i]) {

@@ -25,12 +25,24 @@ int ec_parallel_for(int symbol_count);
 // empty vector if the pmf cannot be made valid.
 std::vector<uint32_t> pmf_to_quantized_cdf(const float* pmf, int n);
 
+// Encoder form of one symbol: the state update x -> ((x / freq) << 16) + x % freq + start written
+// as x + bias + q * cmpl with q = x / freq from a multiply-high by a rounded-up reciprocal and a
+// shift (exact for the encoder's x < 2^31; the published method of Giesen's ryg_rans).
+struct RansEncSym {
+    uint32_t x_max;  // freq << 15: renormalise while x >= x_max (0: zero frequency)
+    uint32_t rcp;
+    uint32_t bias;
+    uint16_t cmpl;   // (1 << 16) - freq
+    uint16_t shift;
+};
+
 struct RansTable {
     int count = 0;   // number of tables
     int stride = 0;  // int32 entries per table
     std::vector<int32_t> cdf;       // [count * stride]
     std::vector<int32_t> max_value; // cdf_length - 2
     std::vector<uint32_t> enc;      // [count * stride]: start | (freq << 16)
+    std::vector<RansEncSym> esym;   // [count * stride]
 };
 
 // The two table sets of a coder: index 0 = z (bit estimator), index 1 = y (Gaussian).
