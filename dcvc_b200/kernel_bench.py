@@ -1,7 +1,7 @@
 """Micro-benchmark of the codec's kernels at their 1080p shapes (CUDA events on the launching
 stream), also the small fixed case used for ncu captures.
 
-    python -m dcvc_b200.kernel_bench [--case quad|wsilu|res|bias2048|dwconv|ffn|rans|all] [--reps N]
+    python -m dcvc_b200.kernel_bench [--case quad|wsilu|res|bias2048|dwconv|ffn|ffn_ld|rans|all] [--reps N]
                                      [--sets S] [--bn 0|64|128|256]
 
 Consecutive launches cycle through S independent operand sets (default: enough sets for 300 MB),
@@ -27,15 +27,18 @@ def _case(name, g, bn=0):
     def rnd(*s, scale=1.0):
         return (torch.randn(*s, device="cuda", generator=g) * scale).half()
 
-    if name == "ffn":
-        # the fused ConvFFN of a 512-channel dcb2 block (quad GEMM + residual GEMM in one kernel)
-        x = rnd(M8, 512)
-        w1, w2 = rnd(1024, 512, scale=512 ** -0.5), rnd(512, 256, scale=256 ** -0.5)
-        b1 = torch.zeros(1024, device="cuda")
-        b2 = torch.zeros(512, device="cuda")
+    if name in ("ffn", "ffn_ld"):
+        # the fused ConvFFN (quad GEMM + residual GEMM in one kernel) of a 512-channel dcb2 block
+        # ("ffn") or of a 256-channel one, the LD codec's ("ffn_ld")
+        C = 512 if name == "ffn" else 256
+        cf = C // 2
+        x = rnd(M8, C)
+        w1, w2 = rnd(4 * cf, C, scale=C ** -0.5), rnd(C, cf, scale=cf ** -0.5)
+        b1 = torch.zeros(4 * cf, device="cuda")
+        b2 = torch.zeros(C, device="cuda")
         out = torch.empty_like(x)
         fn = lambda: ops.conv_ffn(x, w1, b1, w2, b2, out=out, block_n=bn)  # noqa: E731
-        return fn, 2.0 * M8 * (1024 * 512 + 512 * 256), (2 * x.numel() + w1.numel() + w2.numel()) * 2
+        return fn, 2.0 * M8 * (4 * cf * C + C * cf), (2 * x.numel() + w1.numel() + w2.numel()) * 2
     if name == "dwconv":
         x = rnd(M8, 256)
         w = torch.randn(9, 256, device="cuda", generator=g)
