@@ -35,16 +35,16 @@ struct FfnCfg {
     static constexpr int kABytes = kBM * kBK * 2;          // 16 KB: one K block of A (or of q)
     static constexpr int kBBytes = BN * kBK * 2;           // one K block of BN W1 or W2 rows
     static constexpr int kStageBytes = kABytes + kBBytes;
-    static constexpr int kQBytes = QB * kABytes;           // q: QB K blocks
+    static constexpr int kQBytes = QB * kABytes;           // one q buffer: QB K blocks
     static constexpr int kCols = BN / 2;                   // accumulator columns per epilogue warp
     static constexpr int kBoxes = kCols / 64;              // 64-column output boxes per warp
     static constexpr int kEpiBytes = kEpiWarps * kBoxes * 4096;  // residual / output boxes
     static constexpr int kBarBytes = 512;
     static constexpr int kStagesFit =
-        (kSmemLimit - 1024 - kQBytes - kEpiBytes - kBarBytes) / kStageBytes;
+        (kSmemLimit - 1024 - 2 * kQBytes - kEpiBytes - kBarBytes) / kStageBytes;
     static constexpr int kStages = kStagesFit > 4 ? 4 : kStagesFit;
     static constexpr int kQOffset = kStages * kStageBytes;
-    static constexpr int kEpiOffset = kQOffset + kQBytes;
+    static constexpr int kEpiOffset = kQOffset + 2 * kQBytes;
     static constexpr int kBarOffset = kEpiOffset + kEpiBytes;
     static constexpr int kBytes = kBarOffset + kBarBytes + 1024;
     static constexpr int kTmemCols = 2 * BN;               // two accumulators
@@ -84,9 +84,9 @@ __global__ void __launch_bounds__(kThreads, 1)
     uint64_t* empty = full + kStages;
     uint64_t* tfull = empty + kStages;
     uint64_t* tempty = tfull + 2;
-    uint64_t* qfull = tempty + 2;    // all quad items of a tile have written q
-    uint64_t* qempty = qfull + 1;    // the ffn.2 MMAs of a tile have read q
-    uint64_t* drain = qempty + 1;
+    uint64_t* qfull = tempty + 2;    // [2]: all quad items of a tile have written its q buffer
+    uint64_t* qempty = qfull + 2;    // [2]: the ffn.2 MMAs of a tile have read its q buffer
+    uint64_t* drain = qempty + 2;
     uint64_t* resbar = drain + 1;    // [kEpiWarps][C::kBoxes]
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(resbar + C::kBoxes * kEpiWarps);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
@@ -97,6 +97,11 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int nq = 4 * QB * kBK / BN; // quad items per tile (BN / 4 quad outputs each)
     const int nr = p.C / BN;          // output items per tile
     const int kx = p.C / kBK;         // K blocks of x
+    // This CTA's tiles are blockIdx.x + j * gridDim.x, j < ntiles.  Work runs in rounds: round j
+    // holds the quad items of tile j (while j < ntiles), then the output items of tile j - 1
+    // (from j = 1), so a tile's output items overlap the next tile's quad items; tile j uses q
+    // buffer j % 2.  The three roles walk the same rounds.
+    const int ntiles = blockIdx.x < num_m ? (num_m - 1 - blockIdx.x) / gridDim.x + 1 : 0;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < kStages; ++s) {
@@ -107,8 +112,10 @@ __global__ void __launch_bounds__(kThreads, 1)
             mbar_init(&tfull[b], 1);
             mbar_init(&tempty[b], kEpiWarps);
         }
-        mbar_init(qfull, kEpiWarps);
-        mbar_init(qempty, 1);
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&qfull[b], kEpiWarps);
+            mbar_init(&qempty[b], 1);
+        }
         mbar_init(drain, 1);
         for (int w = 0; w < C::kBoxes * kEpiWarps; ++w) {
             mbar_init(&resbar[w], 1);
@@ -138,10 +145,13 @@ __global__ void __launch_bounds__(kThreads, 1)
             int stage = 0;
             uint32_t phase = 0;
             int issued = 0;
-            for (int tile = blockIdx.x; tile < num_m && !*abort_flag; tile += gridDim.x) {
-                const int m0 = tile * kBM;
+            for (int j = 0; j <= ntiles && !*abort_flag; ++j) {
                 for (int it = 0; it < nq + nr && !*abort_flag; ++it) {
                     const bool quad = it < nq;
+                    if (quad ? j == ntiles : j == 0) {
+                        continue;
+                    }
+                    const int m0 = (blockIdx.x + j * gridDim.x) * kBM;  // quad items only
                     const int kbs = quad ? kx : QB;
                     for (int kb = 0; kb < kbs; ++kb) {
                         if (!mbar_wait_bounded(&empty[stage], phase ^ 1, kWaitLimit)) {
@@ -188,13 +198,17 @@ __global__ void __launch_bounds__(kThreads, 1)
             int acc = 0;
             uint32_t acc_phase = 0;
             bool issued_any = false;
-            int k = 0;
-            for (int tile = blockIdx.x; tile < num_m && !*abort_flag; tile += gridDim.x, ++k) {
+            for (int j = 0; j <= ntiles && !*abort_flag; ++j) {
                 for (int it = 0; it < nq + nr && !*abort_flag; ++it) {
                     const bool quad = it < nq;
+                    if (quad ? j == ntiles : j == 0) {
+                        continue;
+                    }
+                    const int jt = quad ? j : j - 1;  // the item's tile
+                    const uint8_t* qb = qbuf + (jt & 1) * C::kQBytes;
                     if (it == nq) {
-                        // q of this tile is complete in shared memory
-                        if (!mbar_wait_bounded(qfull, k & 1, kWaitLimit)) {
+                        // q of tile jt is complete in shared memory
+                        if (!mbar_wait_bounded(&qfull[jt & 1], (jt >> 1) & 1, kWaitLimit)) {
                             *abort_flag = 1;
                             report_error(p.err, kErrGemmMmaTimeout);
                             break;
@@ -217,7 +231,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                         }
                         tc_fence_after();
                         const uint8_t* sa = smem + stage * C::kStageBytes;
-                        const uint8_t* a = quad ? sa : qbuf + kb * C::kABytes;
+                        const uint8_t* a = quad ? sa : qb + kb * C::kABytes;
                         const uint64_t adesc = make_sw128_kmajor_desc(smem_u32(a));
                         const uint64_t bdesc = make_sw128_kmajor_desc(smem_u32(sa + C::kABytes));
 #pragma unroll
@@ -243,7 +257,10 @@ __global__ void __launch_bounds__(kThreads, 1)
                 if (*abort_flag) {
                     break;
                 }
-                tc_commit(qempty);  // q may be overwritten once this tile's ffn.2 MMAs complete
+                if (j >= 1) {
+                    // tile j - 1's q buffer may be reused once its ffn.2 MMAs complete
+                    tc_commit(&qempty[(j - 1) & 1]);
+                }
             }
             if (*abort_flag && issued_any) {
                 tc_commit(drain);
@@ -265,17 +282,20 @@ __global__ void __launch_bounds__(kThreads, 1)
             tma_prefetch_desc(&tmO);
             tma_prefetch_desc(&tmR);
         }
-        int k = 0;
-        for (int tile = blockIdx.x; tile < num_m && !*abort_flag; tile += gridDim.x, ++k) {
-            const int m0 = tile * kBM;
-            const int row0 = m0 + quad_lanes * 32;   // first row owned by this warp
-            const bool rows_live = row0 < p.M;
-            const int r = quad_lanes * 32 + lane;    // this lane's row inside the tile
+        const int r = quad_lanes * 32 + lane;        // this lane's row inside a tile
+        for (int j = 0; j <= ntiles && !*abort_flag; ++j) {
             for (int it = 0; it < nq + nr && !*abort_flag; ++it) {
                 const bool quad = it < nq;
-                if (quad && it == 0 && k > 0) {
-                    // the previous tile's ffn.2 MMAs must have read q before it is overwritten
-                    if (!mbar_wait_bounded(qempty, (k - 1) & 1, kWaitLimit)) {
+                if (quad ? j == ntiles : j == 0) {
+                    continue;
+                }
+                const int jt = quad ? j : j - 1;        // the item's tile
+                const int row0 = (blockIdx.x + jt * gridDim.x) * kBM + quad_lanes * 32;
+                const bool rows_live = row0 < p.M;
+                uint8_t* qb = qbuf + (jt & 1) * C::kQBytes;
+                if (quad && it == 0 && jt >= 2) {
+                    // tile jt - 2's ffn.2 MMAs must have read this q buffer before it is reused
+                    if (!mbar_wait_bounded(&qempty[jt & 1], ((jt >> 1) - 1) & 1, kWaitLimit)) {
                         *abort_flag = 1;
                         report_error(p.err, kErrGemmEpilogueTimeout);
                         break;
@@ -304,7 +324,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                     // 16-byte chunks (8 outputs) into q: quad output j lives in K block j / 64,
                     // chunk (j % 64) / 8
                     const int q0 = (it * BN + half * C::kCols) / 4;  // first quad output
-                    uint8_t* qblk = qbuf + (q0 / 64) * C::kABytes;
+                    uint8_t* qblk = qb + (q0 / 64) * C::kABytes;
 #pragma unroll 1
                     for (int c = 0; c < C::kCols / 32; ++c) {
                         const int nc = it * BN + half * C::kCols + c * 32;
@@ -347,7 +367,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                         fence_proxy_async_smem();
                         __syncwarp();
                         if (lane == 0) {
-                            mbar_arrive(qfull);
+                            mbar_arrive(&qfull[jt & 1]);
                         }
                     }
                 } else {
@@ -501,11 +521,10 @@ bool ffn_sm100_supported(int C, int cffn, int n1)
 
 bool ffn_sm100_preferred(int C, int cffn, int n1)
 {
-    // With cffn = 256 the fused kernel is slower than the two GEMMs (65 us against 33 + 22 us for
-    // a 512-channel block at 1080p): each tile's output items wait for all of its quad items, and
-    // with two accumulators the next tile's quad items wait for the output epilogues, so the
-    // tensor pipe idles; the 64 KB q tile also leaves two operand stages.  With cffn = 128 it is
-    // faster (the LD codec gains 8-10 % per frame).
+    // With cffn = 256 the fused kernel is slower than the two GEMMs (88 us against 33 + 22 us for
+    // a 512-channel block at 1080p): two 64 KB q buffers leave two 32 KB operand stages, and the
+    // pipeline starves.  With cffn = 128 it is faster (a 256-channel block at 1080p: 22.5 us; the
+    // LD codec gains 8-10 % per frame).
     return ffn_sm100_supported(C, cffn, n1) && cffn == 128;
 }
 
@@ -523,11 +542,9 @@ cudaError_t ffn_sm100(const void* x, int ldx, const void* w1, const void* w2, co
     std::memset(m, 0, sizeof(m));
     const uint64_t xrow = static_cast<uint64_t>(ldx) * 2;
     const int n1 = 4 * p.cffn;
-    // item width: 256 measured faster than 128 for both q widths (a 512-channel block at 1080p:
-    // 65 against 71 us; the four operand stages that 128 allows do not make up for the q
-    // dependency, which serialises a tile's output items behind all of its quad items)
-    const int bn = p.block_n != 0 ? p.block_n : 256;
-    if (bn != 128 && bn != 256) {
+    // item width: 256 for q 128 wide; q 256 wide (two 64 KB q buffers) leaves room for 128 only
+    const int bn = p.block_n != 0 ? p.block_n : (p.cffn == 128 ? 256 : 128);
+    if ((bn != 128 && bn != 256) || (p.cffn == 256 && bn != 128)) {
         return cudaErrorInvalidValue;
     }
     if (!make_tmap_2d(&m[0], dt, x, p.C, p.M, xrow, kBK, kBM, 128) ||
@@ -543,9 +560,6 @@ cudaError_t ffn_sm100(const void* x, int ldx, const void* w1, const void* w2, co
             return q ? launch_ffn<2, 256, true>(m, p, stream) : launch_ffn<2, 256, false>(m, p, stream);
         }
         return q ? launch_ffn<2, 128, true>(m, p, stream) : launch_ffn<2, 128, false>(m, p, stream);
-    }
-    if (bn == 256) {
-        return q ? launch_ffn<4, 256, true>(m, p, stream) : launch_ffn<4, 256, false>(m, p, stream);
     }
     return q ? launch_ffn<4, 128, true>(m, p, stream) : launch_ffn<4, 128, false>(m, p, stream);
 }
