@@ -48,7 +48,10 @@ def _case(name, g, bn=0):
     shapes = {"quad": (M8, 1024, 512, N.EPI_QUAD), "wsilu": (M8, 256, 512, N.EPI_BIAS_WSILU),
               "res": (M8, 512, 256, N.EPI_BIAS_RES), "bias2048": (M8, 512, 2048, N.EPI_BIAS),
               # launch and ramp cost: one tile, and the residual GEMM at a quarter of the pixels
-              "tiny": (128, 256, 64, N.EPI_BIAS), "res_quarter": (M8 // 4, 512, 256, N.EPI_BIAS_RES)}
+              "tiny": (128, 256, 64, N.EPI_BIAS), "res_quarter": (M8 // 4, 512, 256, N.EPI_BIAS_RES),
+              # the y-level (M / 4) dc.0 and quad GEMMs of a 512-channel block
+              "wsilu_quarter": (M8 // 4, 256, 512, N.EPI_BIAS_WSILU),
+              "quad_quarter": (M8 // 4, 1024, 512, N.EPI_QUAD)}
     M, Nn, K, epi = shapes[name]
     a = rnd(M, K)
     w = rnd(Nn, K, scale=K ** -0.5)
