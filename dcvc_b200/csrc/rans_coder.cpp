@@ -410,10 +410,14 @@ bool RansEncoderSession::finish(const RansTables& tables, std::vector<uint8_t>* 
                               ty.esym.data() + static_cast<size_t>(idx) * ty.stride);
                 }
             } else {
+                // table (k % ch) + cdf_offset, the channel stepped down with k (no division per
+                // symbol)
+                int chn = e > b ? (e - 1) % sg.ch : 0;
                 for (int k = e - 1; k >= b; --k) {
-                    const int t = (k % sg.ch) + sg.cdf_offset;
+                    const int t = chn + sg.cdf_offset;
                     lw.symbol(sg.z[k], tz.max_value[t],
                               tz.esym.data() + static_cast<size_t>(t) * tz.stride);
+                    chn = chn == 0 ? sg.ch - 1 : chn - 1;
                 }
             }
         }
@@ -606,11 +610,13 @@ bool RansDecoderSession::decode_z(const RansTables& tables, int n, int cdf_offse
         Reader r = r_[i];  // a copy on this thread's stack (see Writer)
         int b, e;
         split(n, ecp_, i, &b, &e);
+        int chn = b % ch;  // table (k % ch) + cdf_offset, the channel stepped with k
         for (int k = b; k < e; ++k) {
-            const int t = (k % ch) + cdf_offset;
+            const int t = chn + cdf_offset;
             out[k] = rd_symbol(r.x, r.p, r.end, r.overrun,
                                tz.cdf.data() + static_cast<size_t>(t) * tz.stride, tz.max_value[t],
                                tz.stride - 1);
+            chn = chn + 1 == ch ? 0 : chn + 1;
         }
         r_[i] = r;
     });
