@@ -54,6 +54,15 @@ def parse_args():
     ap.add_argument("--no-ld", action="store_true", help="skip the low-delay (LD) measurement")
     ap.add_argument("--streams", type=int, default=4,
                     help="concurrent streams of the batched form (0 skips it)")
+    ap.add_argument("--serve-seconds", type=float, default=4.0,
+                    help="seconds of Poisson arrivals per offered load of the serving form "
+                         "(0 skips it)")
+    ap.add_argument("--serve-loads", default="60,120,240",
+                    help="offered loads of the serving form, chunks/s")
+    ap.add_argument("--serve-streams", type=int, default=24,
+                    help="streams of the serving form (half encoders, half decoders)")
+    ap.add_argument("--serve-slots", type=int, default=8,
+                    help="requests in flight at once in the serving form")
     return ap.parse_args()
 
 
@@ -332,6 +341,124 @@ def batched_streams(args, H, W, n_streams):
     return {"streams": n_streams, "value": round(FRAMES * args.steps * n_streams / (ms / 1e3), 2),
             "unit": UNIT, "ms": round(ms, 2), "chunks": args.steps * n_streams,
             "note": "concurrent independent 1080p streams on one GPU (plain FP16 kernels)"}
+
+
+SERVE_SIZES = ((240, 416), (480, 832), (720, 1280), (1080, 1920), (2160, 3840))
+SERVE_WEIGHTS = (0.10, 0.20, 0.30, 0.30, 0.10)
+SERVE_BUDGET = 150e9
+
+
+def serving_bench(args):
+    """The serving form: Poisson arrivals of chunk encode and decode requests (50/50) at each
+    offered load, over a fixed set of streams whose resolutions are drawn with the weights
+    10/20/30/30/10 % over 416x240 .. 3840x2160 (seed 3), QP uniform over 0..63, through the
+    continuous-batching ChunkServer (per-stream temporal context resident in HBM, admission by
+    a 150 GB budget, host rANS of one request overlapping the GPU work of the others).
+
+    Encode requests carry the chunk's 8-bit I420 planes from pinned host memory and return the
+    payload bytes; decode requests carry payload bytes and return the I420 planes in pinned host
+    memory, so every request is end to end.  A stream codes groups of two chunks, re-seeding its
+    temporal context at each group start, so decoders replay the two pre-encoded payloads of
+    their group.  Latency = completion - scheduled arrival (host clock, as a client sees it)."""
+    from dcvc_b200 import synthetic
+    from dcvc_b200.entropy_tables import add_cdf_to_state_dict
+    from dcvc_b200.model_spec import calibrated_hts_state_dict
+    from dcvc_b200.serving import (ChunkServer, HtsSessionFactory, StreamSpec, latency_summary,
+                                   pack_i420, poisson_arrivals)
+    rng = np.random.default_rng(3)
+    n_enc = args.serve_streams // 2
+    n_dec = args.serve_streams - n_enc
+    pick = rng.choice(len(SERVE_SIZES), size=args.serve_streams, p=SERVE_WEIGHTS)
+    sizes = [SERVE_SIZES[i] for i in pick]
+    used = sorted(set(sizes))
+    content = {s: [pack_i420(synthetic.video_chunk_yuv420(2, s[0], s[1], FRAMES, FRAMES * k))
+                   for k in range(2)] for s in used}
+    refs = {s: synthetic.padded_reference_frame(synthetic.video_chunk_yuv420(2, s[0], s[1], 1, 0)[0])
+            for s in used}
+    sd = add_cdf_to_state_dict(calibrated_hts_state_dict(0))
+    sd = {k: (v.half().cuda() if v.is_floating_point() else v) for k, v in sd.items()}
+    torch.cuda.synchronize()
+    f = HtsSessionFactory(sd, SKIP_THRES, refs, gop=2, copy_output=False)
+    srv = ChunkServer(f.open, f.estimate_bytes, slots=args.serve_slots, hbm_budget=SERVE_BUDGET,
+                      on_worker_start=f.worker_start)
+    try:
+        enc_ids = [f"enc{i}" for i in range(n_enc)]
+        dec_ids = [f"dec{i}" for i in range(n_dec)]
+        spec = {}
+        for i, sid in enumerate(enc_ids + dec_ids):
+            spec[sid] = StreamSpec("enc" if sid.startswith("enc") else "dec", *sizes[i])
+        # decoders' payloads: one group of two chunks per decoder at its own QPs
+        dec_qps = {sid: [int(q) for q in rng.integers(0, 64, size=2)] for sid in dec_ids}
+        payloads = {}
+        for sid in dec_ids:
+            pre = "pre-" + sid
+            srv.open_stream(pre, StreamSpec("enc", spec[sid].height, spec[sid].width))
+            s = (spec[sid].height, spec[sid].width)
+            rs = [srv.submit(pre, dec_qps[sid][k], content[s][k]) for k in range(2)]
+            payloads[sid] = [r.wait(600) for r in rs]
+            srv.close_stream(pre)
+        # open the streams and run one group each (sessions created, graphs captured)
+        for sid in enc_ids + dec_ids:
+            srv.open_stream(sid, spec[sid])
+        warm = []
+        for sid in enc_ids + dec_ids:
+            for k in range(2):
+                if sid in payloads:
+                    warm.append(srv.submit(sid, dec_qps[sid][k], payloads[sid][k]))
+                else:
+                    s = (spec[sid].height, spec[sid].width)
+                    warm.append(srv.submit(sid, int(rng.integers(0, 64)), content[s][k]))
+        for r in warm:
+            r.wait(600)
+        nxt = {sid: 2 for sid in enc_ids + dec_ids}
+        loads = []
+        for rate in [float(x) for x in args.serve_loads.split(",") if x]:
+            plan = []
+            for t in poisson_arrivals(rate, args.serve_seconds, rng):
+                if rng.random() < 0.5:
+                    sid = enc_ids[int(rng.integers(0, n_enc))]
+                    s = (spec[sid].height, spec[sid].width)
+                    plan.append((t, sid, int(rng.integers(0, 64)), content[s][nxt[sid] % 2]))
+                else:
+                    sid = dec_ids[int(rng.integers(0, n_dec))]
+                    k = nxt[sid] % 2
+                    plan.append((t, sid, dec_qps[sid][k], payloads[sid][k]))
+                nxt[sid] += 1
+            reqs = []
+            t0 = time.perf_counter()
+            for t, sid, qp, payload in plan:
+                delay = t0 + t - time.perf_counter()
+                if delay > 0:
+                    time.sleep(delay)
+                reqs.append(srv.submit(sid, qp, payload, arrival=t0 + t))
+            errors = []
+            for r in reqs:
+                try:
+                    r.wait(600)
+                except TimeoutError:
+                    raise
+                except Exception as e:  # counted as failed in the summary; the first is shown
+                    errors.append(f"{type(e).__name__}: {e}")
+            summ = latency_summary(reqs, t0)
+            if errors:
+                summ["first_error"] = errors[0][:200]
+            ok = [r for r in reqs if r.error is None]
+            px = sum(spec[r.stream_id].height * spec[r.stream_id].width for r in ok)
+            span = max(r.done for r in reqs) - t0
+            summ.update({"offered_chunks_per_s": rate, "requests": len(reqs),
+                         "frames_per_s": round(len(ok) * FRAMES / span, 1),
+                         "frames_1080p_equiv_per_s": round(px * FRAMES / (1920 * 1080) / span, 1)})
+            loads.append(summ)
+        streams_by_size = {f"{w}x{h}": sum(1 for s in sizes if s == (h, w)) for h, w in used}
+        return {"loads": loads, "streams": args.serve_streams, "streams_by_size": streams_by_size,
+                "slots": args.serve_slots, "seconds_per_load": args.serve_seconds,
+                "hbm_budget_gb": SERVE_BUDGET / 1e9, "peak_held_gb": round(srv.peak_held / 1e9, 2),
+                "max_sessions": srv.max_sessions, "failed": srv.failed,
+                "note": "Poisson arrivals, 50/50 encode/decode, resolutions 10/20/30/30/10 % over "
+                        "416x240..3840x2160, QP U[0,63]; end to end (I420 planes host<->device); "
+                        "latency on the host clock from scheduled arrival to result"}
+    finally:
+        srv.shutdown()
 
 
 def split_enc_dec(enc, dec, xs, args, pb, pr, H, W, stream):
@@ -650,6 +777,10 @@ def run_gpu(args):
     del enc, dec
     torch.cuda.empty_cache()
     batched = batched_streams(args, H, W, args.streams) if args.streams > 0 else None
+    torch.cuda.empty_cache()
+    # a one-GPU measurement: under torchrun the ranks skip it
+    serving = serving_bench(args) if args.serve_seconds > 0 and world == 1 else None
+    torch.cuda.empty_cache()
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(H, W)
@@ -669,6 +800,7 @@ def run_gpu(args):
         "bytes_per_chunk": {"mean": int(np.mean(nbytes)), "min": int(min(nbytes)), "max": int(max(nbytes))},
         "enc_decomposed_fps": split,
         "batched": batched,
+        "serving": serving,
         "reference_published": PUBLISHED,
         "intra": intra,
         "htl": htl,

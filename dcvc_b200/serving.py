@@ -1,0 +1,466 @@
+"""Continuous-batching chunk server: chunk encode / decode requests of many video streams of mixed
+resolution and QP share one GPU.
+
+The reference serves one stream per proxy with one call in flight (a proxy is not re-entrant and
+keeps the stream's temporal context inside it, dmc_hts_proxy.h:215-355; the harness walks the
+chunks of a sequence one after another, test_video.py:300-345).  This module keeps that contract
+per stream and serves many streams at once:
+
+* every stream owns a session (a codec proxy holding its temporal context in device memory, plus
+  a CUDA stream); the requests of one stream run in arrival order, one at a time;
+* `slots` worker threads run the head requests of different streams concurrently, so the kernels
+  of one chunk fill the launch gaps, tails and host entropy-coding waits of the others; a request
+  that arrives while others are on the GPU starts as soon as a slot frees, not after a batch;
+* a stream's session is created when its first request is admitted, and only while the device
+  bytes held by all sessions plus the new session's estimate fit the HBM budget; streams waiting
+  for memory are admitted strictly in arrival order, and `close_stream` returns a session's
+  memory after its last request;
+* every request records its arrival, start and completion times (`time.perf_counter`), from
+  which `latency_summary` gives throughput and p50 / p99 latency.
+
+The scheduler (`ChunkServer`) knows nothing of CUDA: a session factory supplies sessions with
+`run(request)`, `device_bytes` and `close()`.  `HtsSessionFactory` is the HT-S one (enc or dec
+role per stream, YUV 4:2:0 planes in and out through host pinned memory).
+"""
+import collections
+import threading
+import time
+from dataclasses import dataclass
+
+import numpy as np
+
+FRAMES = 8  # frames per chunk of the HT-S video model
+
+
+@dataclass(frozen=True)
+class StreamSpec:
+    """One video stream: `kind` "enc" (requests carry I420 planes, results are bytes) or "dec"
+    (requests carry (bytes, ec_parallel), results are I420 planes) at `height` x `width`."""
+    kind: str
+    height: int
+    width: int
+
+    def __post_init__(self):
+        if self.kind not in ("enc", "dec"):
+            raise ValueError(f"stream kind must be 'enc' or 'dec', not {self.kind!r}")
+        if self.height <= 0 or self.width <= 0 or self.height % 2 or self.width % 2:
+            raise ValueError(f"bad stream size {self.height}x{self.width} (positive and even)")
+
+
+class Request:
+    """One chunk request.  `wait()` returns the result or raises the error it failed with."""
+
+    __slots__ = ("stream_id", "qp", "payload", "seq", "arrival", "start", "done", "result",
+                 "error", "_event")
+
+    def __init__(self, stream_id, qp, payload, seq, arrival):
+        self.stream_id = stream_id
+        self.qp = int(qp)
+        self.payload = payload
+        self.seq = seq            # index of this request within its stream
+        self.arrival = arrival
+        self.start = None
+        self.done = None
+        self.result = None
+        self.error = None
+        self._event = threading.Event()
+
+    def finished(self):
+        return self._event.is_set()
+
+    def wait(self, timeout=None):
+        if not self._event.wait(timeout):
+            raise TimeoutError(f"request {self.seq} of stream {self.stream_id} still pending")
+        if self.error is not None:
+            raise self.error
+        return self.result
+
+    @property
+    def latency(self):
+        return None if self.done is None else self.done - self.arrival
+
+    def _finish(self, result=None, error=None):
+        self.done = time.perf_counter()
+        self.result = result
+        self.error = error
+        self._event.set()
+
+
+class _Stream:
+    __slots__ = ("spec", "session", "pending", "running", "closing", "reserved", "opening",
+                 "submitted", "failed_open")
+
+    def __init__(self, spec):
+        self.spec = spec
+        self.session = None
+        self.pending = collections.deque()
+        self.running = False
+        self.closing = False
+        self.reserved = 0      # bytes counted against the budget for this stream
+        self.opening = False
+        self.submitted = 0
+        self.failed_open = None
+
+
+class ChunkServer:
+    """Request loop over per-stream sessions (see the module docstring).
+
+    open_session(stream_id, spec) -> session      called on a worker thread
+    estimate_bytes(spec) -> int                   device bytes a new session will hold
+    """
+
+    def __init__(self, open_session, estimate_bytes, slots=8, hbm_budget=150e9,
+                 on_worker_start=None):
+        if slots < 1:
+            raise ValueError("slots must be >= 1")
+        self._open_session = open_session
+        self._estimate = estimate_bytes
+        self.hbm_budget = int(hbm_budget)
+        self._cv = threading.Condition()
+        self._streams = {}
+        self._admit_queue = collections.deque()  # streams waiting for a session, in order
+        self._held = 0
+        self.peak_held = 0
+        self.max_sessions = 0
+        self.completed = 0
+        self.failed = 0
+        self._stop = False
+        self._on_worker_start = on_worker_start
+        self._workers = [threading.Thread(target=self._worker, name=f"chunk-slot-{i}", daemon=True)
+                         for i in range(slots)]
+        for t in self._workers:
+            t.start()
+
+    # ------------------------------------------------------------------ client side
+    def open_stream(self, stream_id, spec):
+        est = int(self._estimate(spec))
+        if est > self.hbm_budget:
+            raise ValueError(f"stream {stream_id}: a {spec.height}x{spec.width} session needs "
+                             f"~{est} device bytes, more than the {self.hbm_budget}-byte budget")
+        with self._cv:
+            if self._stop:
+                raise RuntimeError("server is shut down")
+            if stream_id in self._streams:
+                raise ValueError(f"stream {stream_id} is already open")
+            self._streams[stream_id] = _Stream(spec)
+
+    def submit(self, stream_id, qp, payload, arrival=None):
+        """Queues one chunk request of an open stream; `arrival` (perf_counter seconds) defaults
+        to now.  Returns the Request."""
+        with self._cv:
+            st = self._streams.get(stream_id)
+            if st is None or st.closing:
+                raise ValueError(f"stream {stream_id} is not open")
+            if self._stop:
+                raise RuntimeError("server is shut down")
+            req = Request(stream_id, qp, payload, st.submitted,
+                          time.perf_counter() if arrival is None else arrival)
+            st.submitted += 1
+            if st.failed_open is not None:
+                self.failed += 1
+                req._finish(error=st.failed_open)
+                return req
+            st.pending.append(req)
+            if st.session is None and not st.opening and stream_id not in self._admit_queue:
+                self._admit_queue.append(stream_id)
+            self._cv.notify()
+            return req
+
+    def close_stream(self, stream_id):
+        """The stream's session is released after its queued requests have run."""
+        with self._cv:
+            st = self._streams.get(stream_id)
+            if st is None:
+                return
+            st.closing = True
+            self._maybe_release(stream_id, st)
+            self._cv.notify_all()
+
+    def shutdown(self, wait=True):
+        """Runs the queued requests, then stops the workers; every stream is closed (idle
+        sessions are released at once, which also lets streams waiting for memory in)."""
+        with self._cv:
+            self._stop = True
+            for sid in list(self._streams):
+                st = self._streams[sid]
+                st.closing = True
+                self._maybe_release(sid, st)
+            self._cv.notify_all()
+        if wait:
+            for t in self._workers:
+                t.join()
+            with self._cv:
+                for sid in list(self._streams):
+                    st = self._streams[sid]
+                    st.closing = True
+                    self._maybe_release(sid, st)
+
+    def held_bytes(self):
+        with self._cv:
+            return self._held
+
+    def sessions(self):
+        with self._cv:
+            return sum(1 for s in self._streams.values() if s.session is not None)
+
+    # ------------------------------------------------------------------ scheduling
+    def _admissible(self, sid):
+        """Admission in arrival order: only the first waiting stream may take memory."""
+        if not self._admit_queue or self._admit_queue[0] != sid:
+            return False
+        st = self._streams[sid]
+        return self._held + int(self._estimate(st.spec)) <= self.hbm_budget
+
+    def _pick(self):
+        """The runnable stream whose head request arrived first, or None."""
+        best, best_t = None, None
+        for sid, st in self._streams.items():
+            if st.running or st.opening or not st.pending:
+                continue
+            if st.session is None and not self._admissible(sid):
+                continue
+            t = st.pending[0].arrival
+            if best is None or t < best_t:
+                best, best_t = sid, t
+        return best
+
+    def _idle(self):
+        return all(not st.pending and not st.running and not st.opening
+                   for st in self._streams.values())
+
+    def _maybe_release(self, sid, st):
+        if st.closing and not st.pending and not st.running and not st.opening:
+            if st.session is not None:
+                try:
+                    st.session.close()
+                finally:
+                    st.session = None
+            self._held -= st.reserved
+            st.reserved = 0
+            self._streams.pop(sid, None)
+            if sid in self._admit_queue:
+                self._admit_queue.remove(sid)
+
+    def _worker(self):
+        if self._on_worker_start is not None:
+            self._on_worker_start()
+        while True:
+            with self._cv:
+                while True:
+                    sid = self._pick()
+                    if sid is not None:
+                        break
+                    if self._stop and self._idle():
+                        self._cv.notify_all()
+                        return
+                    self._cv.wait(0.05)
+                st = self._streams[sid]
+                need_open = st.session is None
+                if need_open:
+                    self._admit_queue.popleft()
+                    st.reserved = int(self._estimate(st.spec))
+                    self._held += st.reserved
+                    self.peak_held = max(self.peak_held, self._held)
+                    st.opening = True
+                else:
+                    req = st.pending.popleft()
+                    st.running = True
+            if need_open:
+                self._open(sid, st)
+                continue
+            req.start = time.perf_counter()
+            try:
+                result = st.session.run(req)
+                err = None
+            except Exception as e:  # reported through the request
+                result, err = None, e
+            req._finish(result, err)
+            with self._cv:
+                st.running = False
+                if err is None:
+                    self.completed += 1
+                else:
+                    self.failed += 1
+                self._maybe_release(sid, st)
+                self._cv.notify_all()
+
+    def _open(self, sid, st):
+        try:
+            session = self._open_session(sid, st.spec)
+            err = None
+        except Exception as e:
+            session, err = None, e
+        with self._cv:
+            st.opening = False
+            if err is not None:
+                # the stream's queued requests fail with the error; its memory is returned
+                st.failed_open = err
+                self._held -= st.reserved
+                st.reserved = 0
+                while st.pending:
+                    self.failed += 1
+                    st.pending.popleft()._finish(error=err)
+            else:
+                st.session = session
+                actual = int(getattr(session, "device_bytes", st.reserved))
+                self._held += actual - st.reserved
+                st.reserved = actual
+                self.peak_held = max(self.peak_held, self._held)
+                self.max_sessions = max(self.max_sessions, sum(
+                    1 for s in self._streams.values() if s.session is not None))
+            self._maybe_release(sid, st)
+            self._cv.notify_all()
+
+
+def latency_summary(requests, t0=None):
+    """Throughput and latency percentiles of finished requests (seconds -> ms)."""
+    done = [r for r in requests if r.done is not None and r.error is None]
+    if not done:
+        return {"completed": 0, "failed": sum(1 for r in requests if r.error is not None)}
+    lat = np.array([r.latency for r in done]) * 1e3
+    start = min(r.arrival for r in requests) if t0 is None else t0
+    end = max(r.done for r in done)
+    return {"completed": len(done),
+            "failed": sum(1 for r in requests if r.error is not None),
+            "chunks_per_s": round(len(done) / (end - start), 2),
+            "p50_ms": round(float(np.percentile(lat, 50)), 2),
+            "p99_ms": round(float(np.percentile(lat, 99)), 2),
+            "max_ms": round(float(lat.max()), 2)}
+
+
+def pack_i420(frames, pin=True):
+    """List of (y, u, v) uint8 planes -> one uint8 host tensor of the frames' I420 planes back to
+    back (the layout of an 8-bit .yuv file), pinned for an asynchronous upload."""
+    import torch
+    t = torch.from_numpy(np.concatenate(
+        [np.concatenate([y.ravel(), u.ravel(), v.ravel()]) for y, u, v in frames]))
+    return t.pin_memory() if pin else t
+
+
+def poisson_arrivals(rate, seconds, rng):
+    """Arrival offsets (seconds) of a Poisson process of `rate` per second over `seconds`."""
+    out, t = [], 0.0
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t >= seconds:
+            return out
+        out.append(t)
+
+
+class HtsSessionFactory:
+    """Sessions of the HT-S chunk codec (DMCHTSProxy) for `ChunkServer`.
+
+    Each session holds its own proxy (weights, activation arena, temporal context) and CUDA
+    stream.  A stream is coded in groups of `gop` chunks: the first chunk of every group re-seeds
+    the temporal context from the stream's reference frame (the reconstruction of an intra
+    frame in the reference's sequence loop, test_video.py:300-320), so a decoder that sees the
+    same group of payloads reproduces the encoder's reconstructions.  Encode requests carry the
+    chunk's I420 planes in host memory (pinned for an asynchronous copy); decode requests carry
+    (bytes, ec_parallel) and return the I420 planes in host memory (a fresh copy when
+    `copy_output`, else the session's pinned buffer, valid until the stream's next request).
+    """
+
+    def __init__(self, state_dict, skip_threshold, ref_frames, gop=2, copy_output=True,
+                 device=None):
+        import torch
+        self._torch = torch
+        self._sd = state_dict
+        self._skip = skip_threshold
+        self._refs = ref_frames  # (H, W) -> [1, 3, Hp, Wp] float16 device frame
+        self.gop = int(gop)
+        self.copy_output = copy_output
+        self.device = torch.cuda.current_device() if device is None else device
+        # the sessions read the state dict and reference frames from their own CUDA streams
+        torch.cuda.current_stream().synchronize()
+        self._lock = threading.Lock()
+        self._measured = {}  # (kind, H, W) -> device bytes of an opened session
+
+    def worker_start(self):
+        self._torch.cuda.set_device(self.device)
+
+    def estimate_bytes(self, spec):
+        """Bytes a session at spec's size will hold: a measured session of the same kind and size;
+        else the tightest upper bound from measured sessions of that kind (a session's bytes are
+        a fixed part plus a part proportional to the padded pixels, so b * max(1, px_new / px)
+        bounds them); else 3.5 KB per padded pixel + 0.5 GB."""
+        hp, wp = (spec.height + 15) // 16 * 16, (spec.width + 15) // 16 * 16
+        with self._lock:
+            key = (spec.kind, spec.height, spec.width)
+            if key in self._measured:
+                return self._measured[key]
+            best = None
+            for (k, h, w), b in self._measured.items():
+                px = ((h + 15) // 16 * 16) * ((w + 15) // 16 * 16)
+                est = int(b * max(1.0, (hp * wp) / px))
+                if k == spec.kind and (best is None or est < best):
+                    best = est
+        if best is not None:
+            return best
+        return int(3.5e3 * hp * wp + 0.5e9)
+
+    def open(self, stream_id, spec):
+        s = _HtsSession(self, spec)
+        with self._lock:
+            self._measured[(spec.kind, spec.height, spec.width)] = max(
+                s.device_bytes, self._measured.get((spec.kind, spec.height, spec.width), 0))
+        return s
+
+
+class _HtsSession:
+    def __init__(self, factory, spec):
+        import torch
+        from . import ops
+        from .inference_extensions_cuda import DMCHTSProxy
+        from .synthetic import padding_for
+        self._torch, self._ops = torch, ops
+        self.spec = spec
+        self.gop = factory.gop
+        self.copy_output = factory.copy_output
+        H, W = spec.height, spec.width
+        self.pr, self.pb = padding_for(H, W)
+        self.ref = factory._refs[(H, W)]
+        self.stream = torch.cuda.Stream()
+        self.count = 0
+        n = FRAMES * H * W * 3 // 2
+        with torch.cuda.stream(self.stream):
+            self.codec = DMCHTSProxy()
+            self.codec.set_param(factory._sd, factory._skip)
+            self.planes = torch.empty(n, dtype=torch.uint8, device="cuda")
+            extra = n
+            if spec.kind == "enc":
+                self.x = torch.empty((1, 3 * FRAMES, H, W), dtype=torch.float16, device="cuda",
+                                     memory_format=torch.channels_last)
+                extra += self.x.numel() * 2
+            else:
+                self.host_out = torch.empty(n, dtype=torch.uint8).pin_memory()
+            self._seed()
+        self.stream.synchronize()
+        self.device_bytes = self.codec.stats()[2] + extra
+
+    def _seed(self):
+        self.codec.add_ref_feature_from_frame(self.ref, self.spec.kind == "enc")
+
+    def run(self, req):
+        torch = self._torch
+        H, W = self.spec.height, self.spec.width
+        with torch.cuda.stream(self.stream):
+            if self.count % self.gop == 0 and self.count > 0:
+                self._seed()
+            self.count += 1
+            if self.spec.kind == "enc":
+                planes = req.payload
+                if planes.numel() != self.planes.numel():
+                    raise ValueError("encode payload is not 8 I420 frames of the stream's size")
+                self.planes.copy_(planes, non_blocking=True)
+                self._ops.yuv420_to_input(self.planes, FRAMES, H, W, out=self.x)
+                return self.codec.compress(self.x, req.qp, False, self.pb, self.pr)
+            bits, ecp = req.payload
+            frames = self.codec.decompress(bits, req.qp, H, W, ecp, False)
+            self._ops.frames_to_yuv420(frames, H, W, out=self.planes)
+            self.host_out.copy_(self.planes, non_blocking=True)
+            self.stream.synchronize()
+            return self.host_out.numpy().copy() if self.copy_output else self.host_out
+
+    def close(self):
+        self.stream.synchronize()
+        self.codec = None
