@@ -411,10 +411,11 @@ def serving_bench(args):
         for r in warm:
             r.wait(600)
         nxt = {sid: 2 for sid in enc_ids + dec_ids}
-        loads = []
-        for rate in [float(x) for x in args.serve_loads.split(",") if x]:
+
+        def draw(times):
+            """(arrival offset, stream, qp, payload) per arrival: encode or decode 50/50."""
             plan = []
-            for t in poisson_arrivals(rate, args.serve_seconds, rng):
+            for t in times:
                 if rng.random() < 0.5:
                     sid = enc_ids[int(rng.integers(0, n_enc))]
                     s = (spec[sid].height, spec[sid].width)
@@ -424,6 +425,9 @@ def serving_bench(args):
                     k = nxt[sid] % 2
                     plan.append((t, sid, dec_qps[sid][k], payloads[sid][k]))
                 nxt[sid] += 1
+            return plan
+
+        def run_plan(plan):
             reqs = []
             t0 = time.perf_counter()
             for t, sid, qp, payload in plan:
@@ -445,18 +449,38 @@ def serving_bench(args):
             ok = [r for r in reqs if r.error is None]
             px = sum(spec[r.stream_id].height * spec[r.stream_id].width for r in ok)
             span = max(r.done for r in reqs) - t0
-            summ.update({"offered_chunks_per_s": rate, "requests": len(reqs),
+            summ.update({"requests": len(reqs),
                          "frames_per_s": round(len(ok) * FRAMES / span, 1),
                          "frames_1080p_equiv_per_s": round(px * FRAMES / (1920 * 1080) / span, 1)})
+            return summ
+
+        loads = []
+        for rate in [float(x) for x in args.serve_loads.split(",") if x]:
+            summ = run_plan(draw(poisson_arrivals(rate, args.serve_seconds, rng)))
+            summ["offered_chunks_per_s"] = rate
             loads.append(summ)
+        # saturation: the same mix with every request queued at once, one request in flight (the
+        # plain one-request-at-a-time form) against `slots` in flight
+        n_sat = max(64, int(120 * args.serve_seconds))
+        saturation = {}
+        for limit in (1, args.serve_slots):
+            srv.set_in_flight_limit(limit)
+            # arrival offsets 1 us apart keep the service order first-come first-served
+            saturation[f"in_flight_{limit}"] = run_plan(draw([i * 1e-6 for i in range(n_sat)]))
+        srv.set_in_flight_limit(args.serve_slots)
+        a = saturation[f"in_flight_{args.serve_slots}"]["frames_1080p_equiv_per_s"]
+        b = saturation["in_flight_1"]["frames_1080p_equiv_per_s"]
+        saturation["speedup"] = round(a / b, 3) if b else None
         streams_by_size = {f"{w}x{h}": sum(1 for s in sizes if s == (h, w)) for h, w in used}
-        return {"loads": loads, "streams": args.serve_streams, "streams_by_size": streams_by_size,
+        return {"loads": loads, "saturation": saturation, "streams": args.serve_streams,
+                "streams_by_size": streams_by_size,
                 "slots": args.serve_slots, "seconds_per_load": args.serve_seconds,
                 "hbm_budget_gb": SERVE_BUDGET / 1e9, "peak_held_gb": round(srv.peak_held / 1e9, 2),
                 "max_sessions": srv.max_sessions, "failed": srv.failed,
                 "note": "Poisson arrivals, 50/50 encode/decode, resolutions 10/20/30/30/10 % over "
                         "416x240..3840x2160, QP U[0,63]; end to end (I420 planes host<->device); "
-                        "latency on the host clock from scheduled arrival to result"}
+                        "latency on the host clock from scheduled arrival to result; a request "
+                        "codes OR decodes its chunk, so its frames count once"}
     finally:
         srv.shutdown()
 

@@ -125,6 +125,8 @@ class ChunkServer:
         self.completed = 0
         self.failed = 0
         self._stop = False
+        self._limit = slots      # requests in flight at most (<= slots)
+        self._in_flight = 0
         self._on_worker_start = on_worker_start
         self._workers = [threading.Thread(target=self._worker, name=f"chunk-slot-{i}", daemon=True)
                          for i in range(slots)]
@@ -195,6 +197,16 @@ class ChunkServer:
                     st.closing = True
                     self._maybe_release(sid, st)
 
+    def set_in_flight_limit(self, n):
+        """Caps the requests in flight at n (1 .. slots); 1 serves one request at a time, as the
+        reference's proxies do."""
+        n = int(n)
+        if not 1 <= n <= len(self._workers):
+            raise ValueError(f"in-flight limit must be in 1..{len(self._workers)}")
+        with self._cv:
+            self._limit = n
+            self._cv.notify_all()
+
     def held_bytes(self):
         with self._cv:
             return self._held
@@ -213,6 +225,8 @@ class ChunkServer:
 
     def _pick(self):
         """The runnable stream whose head request arrived first, or None."""
+        if self._in_flight >= self._limit:
+            return None
         best, best_t = None, None
         for sid, st in self._streams.items():
             if st.running or st.opening or not st.pending:
@@ -265,6 +279,7 @@ class ChunkServer:
                 else:
                     req = st.pending.popleft()
                     st.running = True
+                self._in_flight += 1
             if need_open:
                 self._open(sid, st)
                 continue
@@ -277,6 +292,7 @@ class ChunkServer:
             req._finish(result, err)
             with self._cv:
                 st.running = False
+                self._in_flight -= 1
                 if err is None:
                     self.completed += 1
                 else:
@@ -292,6 +308,7 @@ class ChunkServer:
             session, err = None, e
         with self._cv:
             st.opening = False
+            self._in_flight -= 1
             if err is not None:
                 # the stream's queued requests fail with the error; its memory is returned
                 st.failed_open = err

@@ -197,3 +197,25 @@ def test_latency_summary_and_arrivals():
     arr = poisson_arrivals(200.0, 5.0, rng)
     assert all(0 < a < 5.0 for a in arr) and arr == sorted(arr)
     assert 850 < len(arr) < 1150
+
+
+def test_in_flight_limit():
+    f = FakeFactory(work=0.005)
+    srv = _server(f, slots=4)
+    for sid in range(4):
+        srv.open_stream(sid, StreamSpec("enc", 8, 8))
+    for r in [srv.submit(sid, 0, None) for sid in range(4)]:
+        r.wait(10)  # sessions open
+    srv.set_in_flight_limit(1)
+    f.max_concurrent = 0
+    for r in [srv.submit(sid, 0, None) for _ in range(3) for sid in range(4)]:
+        r.wait(10)
+    assert f.max_concurrent == 1
+    srv.set_in_flight_limit(4)
+    f.max_concurrent = 0
+    for r in [srv.submit(sid, 0, None) for _ in range(3) for sid in range(4)]:
+        r.wait(10)
+    assert f.max_concurrent == 4
+    with pytest.raises(ValueError):
+        srv.set_in_flight_limit(5)
+    srv.shutdown()
