@@ -409,23 +409,28 @@ __global__ void __launch_bounds__(GemmCfg<BN, EPI>::kThreads, 1)
                         uint32_t r[32];
                         tmem_ld_32x32b_x32(tbase + b * C::kAccPerBox + c * 32, r);
                         tc_wait_ld();
-                        float v[32];
+                        // Column pairs in packed f32x2 arithmetic: every operation rounds each
+                        // lane to nearest on its own, in the same order as the scalar form, so
+                        // the outputs are bitwise unchanged and the FP32 instructions halve.
+                        float2 v[16];
 #pragma unroll
                         for (int j = 0; j < 8; ++j) {
                             const float4 bj = kHoist ? bb[j] : __ldg(b4 + j);
-                            v[4 * j + 0] = __uint_as_float(r[4 * j + 0]) + bj.x;
-                            v[4 * j + 1] = __uint_as_float(r[4 * j + 1]) + bj.y;
-                            v[4 * j + 2] = __uint_as_float(r[4 * j + 2]) + bj.z;
-                            v[4 * j + 3] = __uint_as_float(r[4 * j + 3]) + bj.w;
+                            v[2 * j] = __fadd2_rn(
+                                make_float2(__uint_as_float(r[4 * j + 0]), __uint_as_float(r[4 * j + 1])),
+                                make_float2(bj.x, bj.y));
+                            v[2 * j + 1] = __fadd2_rn(
+                                make_float2(__uint_as_float(r[4 * j + 2]), __uint_as_float(r[4 * j + 3])),
+                                make_float2(bj.z, bj.w));
                         }
                         if constexpr (EPI == kEpiQuad) {
                             uint32_t o[4];
 #pragma unroll
                             for (int i = 0; i < 4; ++i) {
-                                const float s0 = wsilu(v[8 * i + 0]) + wsilu(v[8 * i + 1]) +
-                                                 wsilu(v[8 * i + 2]) + wsilu(v[8 * i + 3]);
-                                const float s1 = wsilu(v[8 * i + 4]) + wsilu(v[8 * i + 5]) +
-                                                 wsilu(v[8 * i + 6]) + wsilu(v[8 * i + 7]);
+                                const float2 w0 = wsilu2(v[4 * i + 0]), w1 = wsilu2(v[4 * i + 1]);
+                                const float2 w2 = wsilu2(v[4 * i + 2]), w3 = wsilu2(v[4 * i + 3]);
+                                const float s0 = w0.x + w0.y + w1.x + w1.y;
+                                const float s1 = w2.x + w2.y + w3.x + w3.y;
                                 o[i] = P::pack(s0, s1);
                             }
                             *reinterpret_cast<uint4*>(out_buf + stage_off<C::kRowBytes>(lane, c)) =
@@ -434,8 +439,8 @@ __global__ void __launch_bounds__(GemmCfg<BN, EPI>::kThreads, 1)
                         }
                         if constexpr (EPI == kEpiBiasWsilu) {
 #pragma unroll
-                            for (int j = 0; j < 32; ++j) {
-                                v[j] = wsilu(v[j]);
+                            for (int j = 0; j < 16; ++j) {
+                                v[j] = wsilu2(v[j]);
                             }
                         }
                         if constexpr (epi_has_res(EPI)) {
@@ -443,16 +448,10 @@ __global__ void __launch_bounds__(GemmCfg<BN, EPI>::kThreads, 1)
                             for (int j = 0; j < 4; ++j) {
                                 const uint4 u = *reinterpret_cast<const uint4*>(
                                     res_buf + stage_off<C::kRowBytes>(lane, c * 4 + j));
-                                const float2 a = P::unpack(u.x), bq = P::unpack(u.y),
-                                             cc = P::unpack(u.z), d = P::unpack(u.w);
-                                v[8 * j + 0] += a.x;
-                                v[8 * j + 1] += a.y;
-                                v[8 * j + 2] += bq.x;
-                                v[8 * j + 3] += bq.y;
-                                v[8 * j + 4] += cc.x;
-                                v[8 * j + 5] += cc.y;
-                                v[8 * j + 6] += d.x;
-                                v[8 * j + 7] += d.y;
+                                v[4 * j + 0] = __fadd2_rn(v[4 * j + 0], P::unpack(u.x));
+                                v[4 * j + 1] = __fadd2_rn(v[4 * j + 1], P::unpack(u.y));
+                                v[4 * j + 2] = __fadd2_rn(v[4 * j + 2], P::unpack(u.z));
+                                v[4 * j + 3] = __fadd2_rn(v[4 * j + 3], P::unpack(u.w));
                             }
                         }
                         if constexpr (EPI == kEpiBiasRes2) {
@@ -460,16 +459,10 @@ __global__ void __launch_bounds__(GemmCfg<BN, EPI>::kThreads, 1)
                             for (int j = 0; j < 4; ++j) {
                                 const uint4 u = *reinterpret_cast<const uint4*>(
                                     res2_buf + stage_off<C::kRowBytes>(lane, c * 4 + j));
-                                const float2 a = P::unpack(u.x), bq = P::unpack(u.y),
-                                             cc = P::unpack(u.z), d = P::unpack(u.w);
-                                v[8 * j + 0] += a.x;
-                                v[8 * j + 1] += a.y;
-                                v[8 * j + 2] += bq.x;
-                                v[8 * j + 3] += bq.y;
-                                v[8 * j + 4] += cc.x;
-                                v[8 * j + 5] += cc.y;
-                                v[8 * j + 6] += d.x;
-                                v[8 * j + 7] += d.y;
+                                v[4 * j + 0] = __fadd2_rn(v[4 * j + 0], P::unpack(u.x));
+                                v[4 * j + 1] = __fadd2_rn(v[4 * j + 1], P::unpack(u.y));
+                                v[4 * j + 2] = __fadd2_rn(v[4 * j + 2], P::unpack(u.z));
+                                v[4 * j + 3] = __fadd2_rn(v[4 * j + 3], P::unpack(u.w));
                             }
                         }
                         if constexpr (epi_has_q(EPI)) {
@@ -478,25 +471,19 @@ __global__ void __launch_bounds__(GemmCfg<BN, EPI>::kThreads, 1)
 #pragma unroll
                             for (int j = 0; j < 4; ++j) {
                                 const uint4 u = __ldg(qs + j);
-                                const float2 a = P::unpack(u.x), bq = P::unpack(u.y),
-                                             cc = P::unpack(u.z), d = P::unpack(u.w);
-                                v[8 * j + 0] *= a.x;
-                                v[8 * j + 1] *= a.y;
-                                v[8 * j + 2] *= bq.x;
-                                v[8 * j + 3] *= bq.y;
-                                v[8 * j + 4] *= cc.x;
-                                v[8 * j + 5] *= cc.y;
-                                v[8 * j + 6] *= d.x;
-                                v[8 * j + 7] *= d.y;
+                                v[4 * j + 0] = __fmul2_rn(v[4 * j + 0], P::unpack(u.x));
+                                v[4 * j + 1] = __fmul2_rn(v[4 * j + 1], P::unpack(u.y));
+                                v[4 * j + 2] = __fmul2_rn(v[4 * j + 2], P::unpack(u.z));
+                                v[4 * j + 3] = __fmul2_rn(v[4 * j + 3], P::unpack(u.w));
                             }
                         }
 #pragma unroll
                         for (int j = 0; j < 4; ++j) {
                             *reinterpret_cast<uint4*>(out_buf + stage_off<C::kRowBytes>(lane, c * 4 + j)) =
-                                make_uint4(P::pack(v[8 * j + 0], v[8 * j + 1]),
-                                           P::pack(v[8 * j + 2], v[8 * j + 3]),
-                                           P::pack(v[8 * j + 4], v[8 * j + 5]),
-                                           P::pack(v[8 * j + 6], v[8 * j + 7]));
+                                make_uint4(P::pack(v[4 * j + 0].x, v[4 * j + 0].y),
+                                           P::pack(v[4 * j + 1].x, v[4 * j + 1].y),
+                                           P::pack(v[4 * j + 2].x, v[4 * j + 2].y),
+                                           P::pack(v[4 * j + 3].x, v[4 * j + 3].y));
                         }
                     }
                     fence_proxy_async_smem();
