@@ -200,7 +200,7 @@ def test_latency_summary_and_arrivals():
 
 
 def test_in_flight_limit():
-    f = FakeFactory(work=0.005)
+    f = FakeFactory(work=0.02)
     srv = _server(f, slots=4)
     for sid in range(4):
         srv.open_stream(sid, StreamSpec("enc", 8, 8))
