@@ -219,3 +219,30 @@ def test_in_flight_limit():
     with pytest.raises(ValueError):
         srv.set_in_flight_limit(5)
     srv.shutdown()
+
+
+def test_hts_estimate_bounds_session_bytes():
+    """HtsSessionFactory.estimate_bytes: exact for a measured size, an upper bound from the
+    tightest measured session of the same kind otherwise (a session holds a fixed part plus a part
+    proportional to its padded pixels), and a generous default before any measurement."""
+    from dcvc_b200.serving import HtsSessionFactory
+    f = HtsSessionFactory.__new__(HtsSessionFactory)  # no CUDA needed for the estimate
+    f._lock = threading.Lock()
+    f._measured = {}
+    fixed, per_px = 200e6, 600.0
+
+    def true_bytes(h, w):
+        return int(fixed + per_px * ((h + 15) // 16 * 16) * ((w + 15) // 16 * 16))
+
+    spec = StreamSpec("enc", 1080, 1920)
+    assert f.estimate_bytes(spec) >= true_bytes(1080, 1920)  # default before measurements
+    f._measured[("enc", 480, 832)] = true_bytes(480, 832)
+    f._measured[("enc", 2160, 3840)] = true_bytes(2160, 3840)
+    for h, w in [(240, 416), (720, 1280), (1080, 1920), (2160, 3840), (480, 832)]:
+        est = f.estimate_bytes(StreamSpec("enc", h, w))
+        assert est >= true_bytes(h, w), (h, w)
+    assert f.estimate_bytes(StreamSpec("enc", 480, 832)) == true_bytes(480, 832)
+    # the bound comes from the closest larger-or-equal measurement, not the largest one
+    assert f.estimate_bytes(StreamSpec("enc", 240, 416)) == true_bytes(480, 832)
+    # another kind has its own measurements
+    assert f.estimate_bytes(StreamSpec("dec", 480, 832)) >= true_bytes(480, 832)
