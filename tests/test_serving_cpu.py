@@ -246,3 +246,61 @@ def test_hts_estimate_bounds_session_bytes():
     assert f.estimate_bytes(StreamSpec("enc", 240, 416)) == true_bytes(480, 832)
     # another kind has its own measurements
     assert f.estimate_bytes(StreamSpec("dec", 480, 832)) >= true_bytes(480, 832)
+
+
+def test_concurrent_clients_random_work():
+    """Four client threads submit to 16 streams at once with random work times, under a budget
+    that holds 6 sessions, and close each stream after its last request: every request completes
+    in its stream's order, no stream runs two requests at once, and the budget always holds."""
+    rng = np.random.default_rng(7)
+    works = rng.uniform(0.0, 0.004, size=400)
+
+    class RandFactory(FakeFactory):
+        def __init__(self):
+            super().__init__(work=0.0)
+            self.i = 0
+
+        def open(self, sid, spec):
+            s = super().open(sid, spec)
+            f = self
+            base_run = s.run
+
+            def run(req):
+                with f.lock:
+                    f.work = float(works[f.i % len(works)])
+                    f.i += 1
+                return base_run(req)
+            s.run = run
+            return s
+
+    f = RandFactory()
+    srv = _server(f, slots=5, budget=6 * 32 * 32)
+    for sid in range(16):
+        srv.open_stream(sid, StreamSpec("enc", 32, 32))
+    reqs = {sid: [] for sid in range(16)}
+    lock = threading.Lock()
+
+    def client(cid):
+        for k in range(10):
+            for sid in range(cid, 16, 4):
+                r = srv.submit(sid, k, None)
+                with lock:
+                    reqs[sid].append(r)
+        for sid in range(cid, 16, 4):
+            srv.close_stream(sid)
+
+    threads = [threading.Thread(target=client, args=(c,)) for c in range(4)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    for sid in range(16):
+        for k, r in enumerate(reqs[sid]):
+            assert r.wait(20) == (sid, k, k)
+    srv.shutdown()
+    assert not f.overlap_same_stream
+    assert f.max_live_bytes <= 6 * 32 * 32 and srv.peak_held <= srv.hbm_budget
+    for sid in range(16):
+        assert [q for s, q in f.log if s == sid] == list(range(10))
+    assert sorted(f.closed) == list(range(16))
+    assert srv.held_bytes() == 0 and srv.completed == 160
