@@ -60,6 +60,11 @@ _proto("dcvc_conv1x1", c_int,
         c_vp, c_vp, c_int, c_int, c_int, c_int, c_vp])
 
 
+_proto("dcvc_gemm_autotune", c_int, [c_int, c_int, c_int, c_int, c_int, c_int, c_int, c_vp,
+                                    ctypes.POINTER(c_int), ctypes.POINTER(ctypes.c_float)])
+_proto("dcvc_gemm_autotune_enable", c_int, [c_int])
+_proto("dcvc_gemm_tuned", c_int, [c_int, c_int, c_int, c_int, c_int, c_int, ctypes.POINTER(c_int)])
+_proto("dcvc_gemm_tuning_clear", c_int, [])
 _proto("dcvc_conv_ffn", c_int, [c_int, c_int, c_int, c_vp, c_int, c_vp, c_vp, c_vp, c_vp, c_vp,
                                c_vp, c_int, c_int, c_vp])
 _proto("dcvc_dwconv3x3", c_int, [c_vp, c_int, c_int, c_int, c_int, c_vp, c_vp, c_int, c_vp])

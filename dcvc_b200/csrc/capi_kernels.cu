@@ -8,6 +8,11 @@
 #include "../../include/dcvc_b200.h"
 
 namespace dcvc {
+cudaError_t gemm_autotune(int dtype, int epi, const GemmParams& shape, cudaStream_t stream,
+                          int* best_bn, float* best_us);
+void gemm_autotune_set_enabled(bool on);
+int gemm_tuned_bn(int dtype, int epi, int M, int N, int K, int sub_w);
+void gemm_tuning_clear();
 cudaError_t gemm_sm100(int dtype, const void* A, int lda, const void* W, const GemmParams& p,
                        int epi, int bn, cudaStream_t stream);
 }
@@ -79,6 +84,54 @@ int dcvc_conv1x1(int dtype, int epilogue, int M, int N, int K, const void* a, in
         return kInvalidArgument;
     }
     return cuda_status(e, "dcvc_conv1x1");
+}
+
+int dcvc_gemm_autotune(int dtype, int epilogue, int M, int N, int K, int sub_w, int sub_cout,
+                       void* stream, int* block_n, float* us)
+{
+    if (dtype != DCVC_F16 && dtype != DCVC_BF16) {
+        set_last_error("dcvc_gemm_autotune: dtype must be f16 or bf16");
+        return kInvalidArgument;
+    }
+    GemmParams p{};
+    p.M = M;
+    p.N = N;
+    p.K = K;
+    p.sub_w = sub_w;
+    p.sub_cout = sub_cout;
+    p.err = device_error_word();
+    cudaError_t e = gemm_autotune(dtype, epilogue, p, static_cast<cudaStream_t>(stream), block_n, us);
+    if (e == cudaErrorInvalidValue) {
+        set_last_error("dcvc_gemm_autotune: no tile width supports this shape and epilogue");
+        return kInvalidArgument;
+    }
+    if (e == cudaErrorStreamCaptureUnsupported) {
+        set_last_error("dcvc_gemm_autotune: the stream is being captured");
+        return kInvalidArgument;
+    }
+    return cuda_status(e, "dcvc_gemm_autotune");
+}
+
+int dcvc_gemm_autotune_enable(int on)
+{
+    gemm_autotune_set_enabled(on != 0);
+    return kOk;
+}
+
+int dcvc_gemm_tuned(int dtype, int epilogue, int M, int N, int K, int sub_w, int* block_n)
+{
+    if (block_n == nullptr) {
+        set_last_error("dcvc_gemm_tuned: null output");
+        return kInvalidArgument;
+    }
+    *block_n = gemm_tuned_bn(dtype, epilogue, M, N, K, epilogue == kEpiSubpel ? sub_w : 0);
+    return kOk;
+}
+
+int dcvc_gemm_tuning_clear(void)
+{
+    gemm_tuning_clear();
+    return kOk;
 }
 
 int dcvc_conv_ffn(int M, int C, int cffn, const void* x, int ldx, const void* w1, const float* b1,

@@ -584,6 +584,8 @@ cudaError_t dispatch_epi(int epi, const Maps& m, const GemmParams& p, cudaStream
 
 }  // namespace
 
+int gemm_tuned_bn(int dtype, int epi, int M, int N, int K, int sub_w);
+
 int gemm_pick_bn(int M, int N, int epi, int sub_cout)
 {
     if (epi == kEpiQuad) {
@@ -621,7 +623,11 @@ cudaError_t gemm_sm100(int dtype, const void* A, int lda, const void* W, const G
         return cudaErrorInvalidValue;
     }
     if (bn == 0) {
-        bn = gemm_pick_bn(p.M, p.N, epi, p.sub_cout);
+        // a width measured by the autotuner (gemm_tune.cu) for this shape, else the rule
+        bn = gemm_tuned_bn(dtype, epi, p.M, p.N, p.K, epi == kEpiSubpel ? p.sub_w : 0);
+        if (bn == 0) {
+            bn = gemm_pick_bn(p.M, p.N, epi, p.sub_cout);
+        }
     }
     if (bn == 0 || p.N % bn != 0) {
         return cudaErrorInvalidValue;

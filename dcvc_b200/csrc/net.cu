@@ -8,6 +8,7 @@ namespace dcvc {
 
 cudaError_t gemm_sm100(int dtype, const void* A, int lda, const void* W, const GemmParams& p,
                        int epi, int bn, cudaStream_t stream);
+int gemm_bn_for(int dtype, int epi, const GemmParams& p, cudaStream_t stream);
 
 // ------------------------------------------------------------------------------ arena
 
@@ -305,7 +306,10 @@ void gemm(Launch& L, const Lin& lin, int epi, const __half* x, int ldx, int M, _
     p.sub_w = sub_w;
     p.sub_cout = epi == kEpiSubpel ? lin.cout / 4 : 0;
     p.err = L.err_word;
-    L.note(gemm_sm100(0, x, ldx, lin.w, p, epi, 0, L.s));
+    // the autotuned width of this shape (tuned here on first sight when tuning is enabled and
+    // the phase runs eagerly), else the library's rule
+    const int bn = gemm_bn_for(0, epi, p, L.s);
+    L.note(gemm_sm100(0, x, ldx, lin.w, p, epi, bn, L.s));
 }
 
 void run_dcb(Launch& L, const Dcb& d, const __half* x, int ldx, int H, int W, __half* out, int ldo,

@@ -4,6 +4,8 @@ These exist for tests and for callers that compose their own graphs; the codec r
 drives the kernels from C++.  Every wrapper runs the sm_100a kernel through libdcvc_b200.so on
 the current CUDA stream; nothing here falls back to PyTorch math.
 """
+import ctypes
+
 import torch
 
 from . import _native as N
@@ -44,6 +46,32 @@ def conv1x1(a, w, bias=None, epilogue=N.EPI_BIAS, res=None, res2=None, qscale=No
     return out
 
 
+def gemm_autotune(dtype, epilogue, M, Nn, K, sub_w=0, sub_cout=0):
+    """Times every valid N tile width of one conv1x1 shape on the current stream and records the
+    fastest for conv1x1(block_n=0) and the codecs.  Returns (block_n, microseconds per launch)."""
+    bn, us = ctypes.c_int(), ctypes.c_float()
+    N.check(N.lib.dcvc_gemm_autotune(_DT[dtype], epilogue, M, Nn, K, sub_w, sub_cout, _stream(),
+                                     ctypes.byref(bn), ctypes.byref(us)), "dcvc_gemm_autotune")
+    return bn.value, us.value
+
+
+def gemm_autotune_enable(on=True):
+    """Codecs tune each new GEMM shape on the first, eager run of a phase (before capture)."""
+    N.check(N.lib.dcvc_gemm_autotune_enable(1 if on else 0), "dcvc_gemm_autotune_enable")
+
+
+def gemm_tuned(dtype, epilogue, M, Nn, K, sub_w=0):
+    """The recorded tile width of a shape, 0 if it has not been tuned."""
+    bn = ctypes.c_int()
+    N.check(N.lib.dcvc_gemm_tuned(_DT[dtype], epilogue, M, Nn, K, sub_w, ctypes.byref(bn)),
+            "dcvc_gemm_tuned")
+    return bn.value
+
+
+def gemm_tuning_clear():
+    N.check(N.lib.dcvc_gemm_tuning_clear(), "dcvc_gemm_tuning_clear")
+
+
 def conv_ffn(x, w1, b1, w2, b2, qscale=None, out=None, block_n=0):
     """Fused ConvFFN: (quad(x . w1^T + b1) . w2^T + b2 + x) [* qscale] for x [M, C] fp16;
     w1 [4 cffn, C], w2 [C, cffn] fp16, b1 / b2 fp32."""
@@ -77,8 +105,6 @@ def _sig(name, args):
     f.argtypes = args
     return f
 
-
-import ctypes  # noqa: E402
 
 _i, _v, _f = ctypes.c_int, ctypes.c_void_p, ctypes.c_float
 _sig("dcvc_pad_unshuffle8", [_v, _i, _i, _i, _i, _i, _i, _v, _i, _v])

@@ -79,6 +79,24 @@ int dcvc_conv1x1(int dtype, int epilogue, int M, int N, int K, const void* a, in
                  int ldr2, const void* qscale, void* out, int ldo, int sub_w, int sub_cout,
                  int block_n, void* stream);
 
+/* Runtime autotuner of the dcvc_conv1x1 tile width.  Replaces the reference's compile-time
+ * per-shape configuration tables (HINT_MAP_* in src/layers/extensions/inference/cutlass/
+ * conv1x1_bias.cu:8 and its siblings, looked up by launch_cutlass_helper, cutlass_kernel.h:232-250).
+ * dcvc_gemm_autotune times every valid N tile (256, 128, 64) of one shape (M, N, K, epilogue;
+ * sub_w / sub_cout for SUBPEL) on zero-filled scratch operands on `stream`, which must not be
+ * capturing, and records the fastest in a process-wide table; *block_n and *us (either may be
+ * NULL) receive the choice and its time per launch.  dcvc_conv1x1 with block_n = 0 and the
+ * codecs use a recorded width for their shape, else the library's rule.  The tile width changes
+ * no output bit.  dcvc_gemm_autotune_enable(1) (or DCVC_GEMM_AUTOTUNE=1 in the environment) makes
+ * the codecs tune every new shape on the first, eager run of a phase, before its graph is
+ * captured.  dcvc_gemm_tuned reports the recorded width (0 = none); dcvc_gemm_tuning_clear
+ * empties the table. */
+int dcvc_gemm_autotune(int dtype, int epilogue, int M, int N, int K, int sub_w, int sub_cout,
+                       void* stream, int* block_n, float* us);
+int dcvc_gemm_autotune_enable(int on);
+int dcvc_gemm_tuned(int dtype, int epilogue, int M, int N, int K, int sub_w, int* block_n);
+int dcvc_gemm_tuning_clear(void);
+
 /* The ConvFFN half of a DepthConvBlock in one kernel (layers_proxy.cpp:95-101: the
  * conv1x1_bias_wsilu_chunk_add quad GEMM followed by conv1x1_bias_shortcut[_with_quant]):
  * out = (quad(x . w1^T + b1) . w2^T + b2 + x) [* qscale], with the quad output kept on chip.
