@@ -207,6 +207,9 @@ def decode_sequence(bin_path, frame_num, rec_path, i_proxy, p_proxy, frames_per_
                 sps_helper.add_sps_by_id(read_sps_remaining(buf, header["sps_id"]))
                 header = read_header(buf)
             sps = sps_helper.get_sps_by_id(header["sps_id"])
+            if sps is None:
+                raise ValueError(f"frame {decoded} references sps_id {header['sps_id']}, which no "
+                                 "preceding SPS unit defines")
             H, W = sps["height"], sps["width"]
             if writer is None:
                 writer = YUV420Writer(rec_path, W, H)

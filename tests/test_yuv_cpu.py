@@ -57,3 +57,17 @@ def test_padding_size_matches_reference_rule():
     assert padding_size(1080, 1920) == (0, 8)
     assert padding_size(240, 416) == (0, 0)
     assert padding_size(250, 410) == (6, 6)
+
+
+def test_decode_sequence_rejects_an_undefined_sps(tmp_path):
+    """A frame whose sps_id no earlier SPS unit defined is reported before any decoding (the
+    reference's SPSHelper.get_sps_by_id returns None there and the harness fails on it)."""
+    import pytest
+    from dcvc_b200 import stream_helper as S
+    from dcvc_b200.video_io import decode_sequence
+    path = tmp_path / "bad.bin"
+    with open(path, "wb") as f:
+        S.write_sps(f, {"sps_id": 0, "height": 64, "width": 64})
+        S.write_ip(f, True, 3, 20, 1, 0, b"\x00\x01\x02")
+    with pytest.raises(ValueError, match="sps_id 3"):
+        decode_sequence(str(path), 8, str(tmp_path / "rec.yuv"), None, None)
