@@ -38,6 +38,7 @@ _proto("dcvc_rans_decode_begin", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_siz
 _proto("dcvc_rans_decode_z", [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                               ctypes.c_void_p])
 _proto("dcvc_rans_decode_y", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p])
+_proto("dcvc_rans_inject_task_fault", [ctypes.c_int])
 
 
 def pmf_to_quantized_cdf(pmf):
@@ -51,6 +52,12 @@ def pmf_to_quantized_cdf(pmf):
 
 def ec_parallel_for(symbol_count):
     return _lib.dcvc_ec_parallel_for(int(symbol_count))
+
+
+def inject_task_fault(sub_stream):
+    """Failure-path testing: the next coder task of `sub_stream` throws in its worker; the call
+    raises DcvcError (DCVC_INTERNAL) and the coder stays usable.  -1 cancels."""
+    N.check(_lib.dcvc_rans_inject_task_fault(int(sub_stream)), "inject_task_fault")
 
 
 class _Coder:

@@ -120,7 +120,7 @@ int dcvc_rans_encode_finish(void* h, const uint8_t** data, size_t* size)
     std::string err;
     r->enc_open = false;
     if (!r->enc.finish(r->tables, &r->encoded, &err)) {
-        return fail(kInvalidArgument, "dcvc_rans_encode_finish: " + err);
+        return fail(r->enc.fault() ? kInternal : kInvalidArgument, "dcvc_rans_encode_finish: " + err);
     }
     *data = r->encoded.data();
     *size = r->encoded.size();
@@ -134,7 +134,8 @@ int dcvc_rans_decode_begin(void* h, const uint8_t* data, size_t size, int ec_par
     }
     std::string err;
     if (!as_handle(h)->dec.begin(data, static_cast<int>(size), ec_parallel, &err)) {
-        return fail(kCorruptStream, "dcvc_rans_decode_begin: " + err);
+        return fail(as_handle(h)->dec.fault() ? kInternal : kCorruptStream,
+                    "dcvc_rans_decode_begin: " + err);
     }
     return kOk;
 }
@@ -147,7 +148,7 @@ int dcvc_rans_decode_z(void* h, int n, int cdf_offset, int ch, int8_t* out)
     std::string err;
     RansHandle* r = as_handle(h);
     if (!r->dec.decode_z(r->tables, n, cdf_offset, ch, out, &err)) {
-        return fail(kCorruptStream, "dcvc_rans_decode_z: " + err);
+        return fail(r->dec.fault() ? kInternal : kCorruptStream, "dcvc_rans_decode_z: " + err);
     }
     return kOk;
 }
@@ -160,8 +161,14 @@ int dcvc_rans_decode_y(void* h, const uint8_t* idx, int n, int8_t* out)
     std::string err;
     RansHandle* r = as_handle(h);
     if (!r->dec.decode_y(r->tables, idx, n, out, &err)) {
-        return fail(kCorruptStream, "dcvc_rans_decode_y: " + err);
+        return fail(r->dec.fault() ? kInternal : kCorruptStream, "dcvc_rans_decode_y: " + err);
     }
+    return kOk;
+}
+
+int dcvc_rans_inject_task_fault(int sub_stream)
+{
+    rans_inject_task_fault(sub_stream);
     return kOk;
 }
 

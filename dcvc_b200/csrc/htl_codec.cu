@@ -693,7 +693,7 @@ int HtlCodec::decompress(const uint8_t* bytes, size_t n, int qp, int height, int
     if (st == kOk && (!dec.begin(bytes, static_cast<int>(n), ecp, &err) ||
                       !dec.decode_z(tables_, z_num_, qp * kChZ, kChZ, z_host_, &err))) {
         set_last_error("decompress: " + err);
-        st = kCorruptStream;
+        st = dec.fault() ? kInternal : kCorruptStream;
     }
     if (st == kOk) {
         cudaMemcpyAsync(z_i8_, z_host_, z_num_, cudaMemcpyHostToDevice, copy_);
@@ -725,7 +725,7 @@ int HtlCodec::decompress(const uint8_t* bytes, size_t n, int qp, int height, int
         }
         if (st == kOk && !dec.decode_y(tables_, idx_host_, count, ydec_host_, &err)) {
             set_last_error("decompress: " + err);
-            st = kCorruptStream;
+            st = dec.fault() ? kInternal : kCorruptStream;
         }
         if (st == kOk) {
             if (count > 0) {

@@ -677,7 +677,7 @@ int HtsCodec::decompress(const uint8_t* bytes, size_t n, int qp, int height, int
     if (st == kOk && (!dec.begin(bytes, static_cast<int>(n), ecp, &err) ||
                       !dec.decode_z(tables_, z_num_, qp * kChZ, kChZ, z_host_, &err))) {
         set_last_error("decompress: " + err);
-        st = kCorruptStream;
+        st = dec.fault() ? kInternal : kCorruptStream;
     }
     if (st == kOk) {
         st = run_phase(kDecHyper, main_);
@@ -701,7 +701,7 @@ int HtsCodec::decompress(const uint8_t* bytes, size_t n, int qp, int height, int
     // y on the CPU while the feature extractor runs (dmc_hts_proxy.cpp:805-823)
     if (st == kOk && !dec.decode_y(tables_, idx_host_, count, ydec_host_, &err)) {
         set_last_error("decompress: " + err);
-        st = kCorruptStream;
+        st = dec.fault() ? kInternal : kCorruptStream;
     }
     if (st == kOk) {
         st = run_phase(kDecSynthesis, main_);

@@ -1,11 +1,15 @@
 #include "rans_coder.h"
 
 #include <algorithm>
-#include <cstring>
-#include <memory>
+#include <atomic>
 #include <condition_variable>
+#include <cstring>
+#include <exception>
 #include <functional>
+#include <memory>
 #include <mutex>
+#include <stdexcept>
+#include <string>
 #include <thread>
 
 #include <unistd.h>
@@ -130,6 +134,21 @@ int shared_tail(const uint8_t* a, int na, const uint8_t* b, int nb)
     return k;
 }
 
+// Sub-stream index whose next task throws (failure-path tests); -1: none.
+std::atomic<int> g_inject_task{-1};
+
+// Runs task i of a coder call, throwing first when a fault is injected for it.
+template <typename F>
+void run_task(F& f, int i)
+{
+    int want = i;
+    if (g_inject_task.load(std::memory_order_relaxed) == i &&
+        g_inject_task.compare_exchange_strong(want, -1)) {
+        throw std::runtime_error("injected fault in sub-stream task " + std::to_string(i));
+    }
+    f(i);
+}
+
 // Persistent workers for the sub-stream tasks of one calling thread (a codec stream's host
 // thread): spawning threads on every call cost as much as coding a small payload.  Workers are
 // created on first use, one per extra sub-stream, and joined when the calling thread exits; a
@@ -147,6 +166,9 @@ public:
             t.join();
         }
     }
+    // Runs f(0) on the calling thread and f(1 .. n-1) on the workers.  Every task runs to the
+    // end even when one throws; the first exception is rethrown here after all have finished,
+    // so no task outlives the caller's frame and no worker terminates the process.
     void run(int n, const std::function<void(int)>& f)
     {
         while (static_cast<int>(th_.size()) < n - 1) {
@@ -158,12 +180,19 @@ public:
             next_ = 1;
             n_ = n;
             left_ = n - 1;
+            first_error_ = nullptr;
         }
         cv_.notify_all();
-        f(0);
+        call(f, 0);
         std::unique_lock<std::mutex> lk(m_);
         done_.wait(lk, [this] { return left_ == 0; });
         fn_ = nullptr;
+        if (first_error_) {
+            std::exception_ptr e = first_error_;
+            first_error_ = nullptr;
+            lk.unlock();
+            std::rethrow_exception(e);
+        }
     }
 
 private:
@@ -178,10 +207,23 @@ private:
             const int i = next_++;
             const std::function<void(int)>* f = fn_;
             lk.unlock();
-            (*f)(i);
+            call(*f, i);
             lk.lock();
             if (--left_ == 0) {
                 done_.notify_one();
+            }
+        }
+    }
+
+    // one task; an exception is kept (the first of the call) instead of escaping the thread
+    void call(const std::function<void(int)>& f, int i)
+    {
+        try {
+            run_task(f, i);
+        } catch (...) {
+            std::lock_guard<std::mutex> lk(m_);
+            if (!first_error_) {
+                first_error_ = std::current_exception();
             }
         }
     }
@@ -192,13 +234,14 @@ private:
     const std::function<void(int)>* fn_ = nullptr;
     int next_ = 0, n_ = 0, left_ = 0;
     bool stop_ = false;
+    std::exception_ptr first_error_;
 };
 
 template <typename F>
 void run_parallel(int n, F&& f)
 {
     if (n == 1) {
-        f(0);
+        run_task(f, 0);
         return;
     }
     thread_local std::unique_ptr<WorkerPool> pool;
@@ -362,8 +405,34 @@ void RansEncoderSession::add_z(const int8_t* sym, int n, int cdf_offset, int ch,
     }
 }
 
+namespace {
+
+// Converts an exception thrown by a coder call into its false / err form.
+template <typename F>
+bool guarded(bool* fault, std::string* err, F&& body)
+{
+    *fault = false;
+    try {
+        return body();
+    } catch (const std::bad_alloc&) {
+        *err = "rANS: out of host memory";
+    } catch (const std::exception& e) {
+        *err = std::string("rANS: ") + e.what();
+    }
+    *fault = true;
+    return false;
+}
+
+}  // namespace
+
 bool RansEncoderSession::finish(const RansTables& tables, std::vector<uint8_t>* out,
                                 std::string* err)
+{
+    return guarded(&fault_, err, [&] { return finish_tasks(tables, out, err); });
+}
+
+bool RansEncoderSession::finish_tasks(const RansTables& tables, std::vector<uint8_t>* out,
+                                      std::string* err)
 {
     if (!tables.ready()) {
         *err = "rANS encode: tables not set";
@@ -544,6 +613,23 @@ inline int8_t rd_symbol(uint32_t& x, const uint8_t*& p, const uint8_t* end, bool
 
 bool RansDecoderSession::begin(const uint8_t* data, int size, int ecp, std::string* err)
 {
+    return guarded(&fault_, err, [&] { return begin_tasks(data, size, ecp, err); });
+}
+
+bool RansDecoderSession::decode_z(const RansTables& tables, int n, int cdf_offset, int ch,
+                                  int8_t* out, std::string* err)
+{
+    return guarded(&fault_, err, [&] { return decode_z_tasks(tables, n, cdf_offset, ch, out, err); });
+}
+
+bool RansDecoderSession::decode_y(const RansTables& tables, const uint8_t* idx, int n,
+                                  int8_t* out, std::string* err)
+{
+    return guarded(&fault_, err, [&] { return decode_y_tasks(tables, idx, n, out, err); });
+}
+
+bool RansDecoderSession::begin_tasks(const uint8_t* data, int size, int ecp, std::string* err)
+{
     ecp_ = 0;
     if (ecp < 1 || ecp > kMaxEcParallel || size < 0 || (size > 0 && data == nullptr)) {
         *err = "rANS decode: bad arguments";
@@ -597,8 +683,8 @@ bool RansDecoderSession::begin(const uint8_t* data, int size, int ecp, std::stri
     return true;
 }
 
-bool RansDecoderSession::decode_z(const RansTables& tables, int n, int cdf_offset, int ch,
-                                  int8_t* out, std::string* err)
+bool RansDecoderSession::decode_z_tasks(const RansTables& tables, int n, int cdf_offset, int ch,
+                                        int8_t* out, std::string* err)
 {
     const RansTable& tz = tables.z();
     if (ecp_ == 0 || tz.count == 0 || n < 0 || ch < 1 || cdf_offset < 0 ||
@@ -629,8 +715,8 @@ bool RansDecoderSession::decode_z(const RansTables& tables, int n, int cdf_offse
     return true;
 }
 
-bool RansDecoderSession::decode_y(const RansTables& tables, const uint8_t* idx, int n,
-                                  int8_t* out, std::string* err)
+bool RansDecoderSession::decode_y_tasks(const RansTables& tables, const uint8_t* idx, int n,
+                                        int8_t* out, std::string* err)
 {
     const RansTable& ty = tables.y();
     if (ecp_ == 0 || ty.count == 0 || n < 0) {
@@ -665,6 +751,11 @@ bool RansDecoderSession::decode_y(const RansTables& tables, const uint8_t* idx, 
         }
     }
     return true;
+}
+
+void rans_inject_task_fault(int sub_stream)
+{
+    g_inject_task.store(sub_stream >= 0 && sub_stream < kMaxEcParallel ? sub_stream : -1);
 }
 
 }  // namespace dcvc

@@ -69,11 +69,16 @@ public:
     void add_y(const int16_t* sym, int n, bool copy = true);
     // z symbols use table (i % ch) + cdf_offset.
     void add_z(const int8_t* sym, int n, int cdf_offset, int ch, bool copy = true);
-    // Codes all segments and merges the sub-streams into the container.
+    // Codes all segments and merges the sub-streams into the container.  An exception in any
+    // sub-stream task (e.g. a failed allocation) is caught: finish returns false with the
+    // message and fault() is true.
     bool finish(const RansTables& tables, std::vector<uint8_t>* out, std::string* err);
     int ec_parallel() const { return ecp_; }
+    bool fault() const { return fault_; }
 
 private:
+    bool finish_tasks(const RansTables& tables, std::vector<uint8_t>* out, std::string* err);
+    bool fault_ = false;
     struct Segment {
         bool is_y;
         const int16_t* y;
@@ -96,8 +101,16 @@ public:
                   std::string* err);
     bool decode_y(const RansTables& tables, const uint8_t* idx, int n, int8_t* out,
                   std::string* err);
+    // true when the last call failed on an exception in the coder (not on the stream's bytes)
+    bool fault() const { return fault_; }
 
 private:
+    bool begin_tasks(const uint8_t* data, int size, int ec_parallel, std::string* err);
+    bool decode_z_tasks(const RansTables& tables, int n, int cdf_offset, int ch, int8_t* out,
+                        std::string* err);
+    bool decode_y_tasks(const RansTables& tables, const uint8_t* idx, int n, int8_t* out,
+                        std::string* err);
+    bool fault_ = false;
     struct Reader {
         const uint8_t* p = nullptr;
         const uint8_t* end = nullptr;
@@ -108,5 +121,9 @@ private:
     std::vector<uint8_t> parts_[kMaxEcParallel];
     Reader r_[kMaxEcParallel];
 };
+
+// Failure-path testing: the next coder task of sub-stream `sub_stream` (0 .. 7) throws inside
+// its worker, as an allocation failure there would; -1 cancels a pending injection.
+void rans_inject_task_fault(int sub_stream);
 
 }  // namespace dcvc

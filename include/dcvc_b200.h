@@ -204,6 +204,14 @@ int dcvc_pmf_to_quantized_cdf(const float* pmf, int n, uint32_t* cdf_out);
  * (src/layers/extensions/inference/dmc_common.cpp:31-35). */
 int dcvc_ec_parallel_for(int symbol_count);
 
+/* Failure-path testing of the host coder: the next coder task of sub-stream `sub_stream` (0 .. 7)
+ * throws inside its worker thread, as a failed allocation there would.  The call that ran it
+ * (dcvc_rans_encode_finish / dcvc_rans_decode_*, or a codec's compress / decompress) returns
+ * DCVC_INTERNAL with the message, every other task of the call still completes, and the coder
+ * stays usable.  The reference terminates the process in that case (a worker exception,
+ * rans.cpp:209-222 under py_rans.cpp:104-135).  -1 cancels a pending injection. */
+int dcvc_rans_inject_task_fault(int sub_stream);
+
 /* A coder handle owns two CDF table sets (index 0: z / bit estimator, index 1: y / Gaussian),
  * one payload being encoded and one being decoded.  Not thread-safe; one handle per thread.
  * Replaces RansEncoder / RansDecoder (src/cpp/py_rans/py_rans.h:21-76, bind.cpp:14-40); the

@@ -149,3 +149,41 @@ def test_pmf_to_quantized_cdf_matches_reference():
         out = np.zeros(p.size + 1, np.uint32)
         assert lib.oracle_pmf_to_quantized_cdf(_p(p), p.size, _p(out)) == p.size + 1
         assert (out == ref).all()
+
+
+@pytest.mark.parametrize("sub_stream", [0, 3])
+def test_worker_exception_is_reported_and_the_coder_recovers(gold, sub_stream):
+    """A fault injected into one sub-stream task (as a failed allocation in a worker would
+    throw) fails the call with DCVC_INTERNAL instead of terminating the process; the other tasks
+    finish, and the next call on the same coder produces the reference bytes again.  Task 0 runs
+    on the calling thread, task 3 on a worker."""
+    from dcvc_b200 import _native as N
+    qy, ly, qz, lz, cases = gold
+    ny, nz, ecp, qp, y, z, ref = max(cases, key=lambda c: c[2])  # the most sub-streams
+    assert ecp > sub_stream
+    enc, dec = _coders(qy, ly, qz, lz)
+    enc.set_entropy_coder_parallel(ecp)
+    dec.set_entropy_coder_parallel(ecp)
+
+    def encode():
+        enc.reset()
+        enc.encode_y(y)
+        enc.encode_z(z, qp * 128, 128)
+        enc.flush()
+        return enc.get_encoded_stream()
+
+    M.inject_task_fault(sub_stream)
+    with pytest.raises(N.DcvcError, match="injected fault") as ei:
+        encode()
+    assert ei.value.status == 8  # DCVC_INTERNAL
+    assert encode().tobytes() == ref.tobytes()
+
+    dec.set_stream(ref)
+    M.inject_task_fault(sub_stream)
+    with pytest.raises(N.DcvcError, match="injected fault") as ei:
+        dec.decode_z(nz, qp * 128, 128)
+    assert ei.value.status == 8  # DCVC_INTERNAL
+    dec.set_stream(ref)
+    dec.decode_z(nz, qp * 128, 128)
+    assert np.array_equal(dec.get_decoded_tensor(), z)
+    M.inject_task_fault(-1)
