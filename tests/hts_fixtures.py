@@ -1,8 +1,6 @@
 """Shared helpers for the HT-S codec tests: seeded model state and synthetic chunks."""
 import functools
 
-import torch
-
 from dcvc_b200 import synthetic
 from dcvc_b200.entropy_tables import add_cdf_to_state_dict
 from dcvc_b200.model_spec import hts_state_dict, perturbed_hts_state_dict

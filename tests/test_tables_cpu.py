@@ -4,7 +4,6 @@ import os
 
 import numpy as np
 import pytest
-import torch
 
 from dcvc_b200.entropy_tables import bit_estimator_tables, gaussian_tables
 from dcvc_b200.model_spec import hts_state_dict
