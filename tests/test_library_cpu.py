@@ -33,3 +33,24 @@ def test_host_entry_points_without_gpu():
     st = N.lib.dcvc_conv1x1(9, 0, 128, 128, 64, None, 64, None, None, None, 0, None, 0, None,
                             None, 128, 0, 0, 0, None)
     assert st == 1 and b"dtype" in N.lib.dcvc_last_error()
+
+
+def test_tuner_and_fault_hook_entry_points_without_gpu():
+    """The autotuner's host entry points answer without a GPU (an empty table, a status for the
+    tuning call itself), and the coder's fault hook accepts and cancels an injection."""
+    from dcvc_b200 import _native as N
+    from dcvc_b200 import MLCodec_extensions_cpp as M  # noqa: F401  (binds the fault hook)
+    bn = ctypes.c_int(-1)
+    assert N.lib.dcvc_gemm_tuning_clear() == 0
+    assert N.lib.dcvc_gemm_tuned(0, N.EPI_BIAS, 1000, 256, 512, 0, ctypes.byref(bn)) == 0
+    assert bn.value == 0
+    assert N.lib.dcvc_gemm_tuned(0, N.EPI_BIAS, 1000, 256, 512, 0, None) == 1  # null output
+    assert N.lib.dcvc_gemm_autotune(9, N.EPI_BIAS, 1000, 256, 512, 0, 0, None, None, None) == 1
+    # without a device the tuning call fails with a status (no crash, nothing recorded)
+    st = N.lib.dcvc_gemm_autotune(0, N.EPI_BIAS, 1000, 256, 512, 0, 0, None, ctypes.byref(bn), None)
+    assert st != 0
+    assert N.lib.dcvc_gemm_tuned(0, N.EPI_BIAS, 1000, 256, 512, 0, ctypes.byref(bn)) == 0
+    assert bn.value == 0
+    assert N.lib.dcvc_gemm_autotune_enable(0) == 0
+    assert N.lib.dcvc_rans_inject_task_fault(2) == 0
+    assert N.lib.dcvc_rans_inject_task_fault(-1) == 0
