@@ -20,7 +20,8 @@ per stream and serves many streams at once:
 
 The scheduler (`ChunkServer`) knows nothing of CUDA: a session factory supplies sessions with
 `run(request)`, `device_bytes` and `close()`.  `HtsSessionFactory` is the HT-S one (enc or dec
-role per stream, YUV 4:2:0 planes in and out through host pinned memory).
+role per stream, YUV 4:2:0 planes in and out through host pinned memory).  `StreamRouter` spreads
+streams over one server per GPU.
 """
 import collections
 import threading
@@ -329,6 +330,66 @@ class ChunkServer:
             self._cv.notify_all()
 
 
+class StreamRouter:
+    """Routes streams over several chunk servers, one per GPU: video streams are independent (a
+    stream's temporal context chains only its own chunks), so each stream lives on one device
+    and no tensor crosses devices.  A new stream goes to the server with the most budget left
+    after the streams already routed to it (their sessions' estimated bytes), ties broken by
+    fewer streams; its requests then go where it lives."""
+
+    def __init__(self, servers):
+        if not servers:
+            raise ValueError("a router needs at least one server")
+        self.servers = list(servers)
+        self._lock = threading.Lock()
+        self._where = {}                      # stream id -> server index
+        self._load = [0] * len(self.servers)  # estimated bytes of the streams routed there
+        self._count = [0] * len(self.servers)
+        self._est = {}
+
+    def open_stream(self, stream_id, spec):
+        with self._lock:
+            if stream_id in self._where:
+                raise ValueError(f"stream {stream_id} is already open")
+            ests = [int(srv._estimate(spec)) for srv in self.servers]
+            fits = [i for i, srv in enumerate(self.servers) if ests[i] <= srv.hbm_budget]
+            if not fits:
+                raise ValueError(f"stream {stream_id}: no server's budget holds a "
+                                 f"{spec.height}x{spec.width} session")
+            best = min(fits, key=lambda i: (-(self.servers[i].hbm_budget - self._load[i] - ests[i]),
+                                            self._count[i], i))
+            self.servers[best].open_stream(stream_id, spec)
+            self._where[stream_id] = best
+            self._load[best] += ests[best]
+            self._count[best] += 1
+            self._est[stream_id] = ests[best]
+            return best
+
+    def device_of(self, stream_id):
+        with self._lock:
+            return self._where[stream_id]
+
+    def submit(self, stream_id, qp, payload, arrival=None):
+        with self._lock:
+            i = self._where.get(stream_id)
+        if i is None:
+            raise ValueError(f"stream {stream_id} is not open")
+        return self.servers[i].submit(stream_id, qp, payload, arrival)
+
+    def close_stream(self, stream_id):
+        with self._lock:
+            i = self._where.pop(stream_id, None)
+            if i is None:
+                return
+            self._load[i] -= self._est.pop(stream_id)
+            self._count[i] -= 1
+        self.servers[i].close_stream(stream_id)
+
+    def shutdown(self, wait=True):
+        for srv in self.servers:
+            srv.shutdown(wait)
+
+
 def latency_summary(requests, t0=None):
     """Throughput and latency percentiles of finished requests (seconds -> ms)."""
     done = [r for r in requests if r.done is not None and r.error is None]
@@ -381,14 +442,17 @@ class HtsSessionFactory:
                  device=None):
         import torch
         self._torch = torch
-        self._sd = state_dict
+        self.device = torch.cuda.current_device() if device is None else int(device)
+        dev = torch.device("cuda", self.device)
+        # this device's own copies: sessions never read another GPU's memory
+        self._sd = {k: (v.to(dev) if isinstance(v, torch.Tensor) and v.is_cuda else v)
+                    for k, v in state_dict.items()}
         self._skip = skip_threshold
-        self._refs = ref_frames  # (H, W) -> [1, 3, Hp, Wp] float16 device frame
+        self._refs = {k: v.to(dev) for k, v in ref_frames.items()}  # (H, W) -> [1, 3, Hp, Wp]
         self.gop = int(gop)
         self.copy_output = copy_output
-        self.device = torch.cuda.current_device() if device is None else device
         # the sessions read the state dict and reference frames from their own CUDA streams
-        torch.cuda.current_stream().synchronize()
+        torch.cuda.synchronize(dev)
         self._lock = threading.Lock()
         self._measured = {}  # (kind, H, W) -> device bytes of an opened session
 
@@ -436,16 +500,18 @@ class _HtsSession:
         H, W = spec.height, spec.width
         self.pr, self.pb = padding_for(H, W)
         self.ref = factory._refs[(H, W)]
-        self.stream = torch.cuda.Stream()
+        dev = torch.device("cuda", factory.device)
+        torch.cuda.set_device(dev)  # the proxy binds to the current device
+        self.stream = torch.cuda.Stream(device=dev)
         self.count = 0
         n = FRAMES * H * W * 3 // 2
         with torch.cuda.stream(self.stream):
             self.codec = DMCHTSProxy()
             self.codec.set_param(factory._sd, factory._skip)
-            self.planes = torch.empty(n, dtype=torch.uint8, device="cuda")
+            self.planes = torch.empty(n, dtype=torch.uint8, device=dev)
             extra = n
             if spec.kind == "enc":
-                self.x = torch.empty((1, 3 * FRAMES, H, W), dtype=torch.float16, device="cuda",
+                self.x = torch.empty((1, 3 * FRAMES, H, W), dtype=torch.float16, device=dev,
                                      memory_format=torch.channels_last)
                 extra += self.x.numel() * 2
             else:

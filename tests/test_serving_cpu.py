@@ -304,3 +304,33 @@ def test_concurrent_clients_random_work():
         assert [q for s, q in f.log if s == sid] == list(range(10))
     assert sorted(f.closed) == list(range(16))
     assert srv.held_bytes() == 0 and srv.completed == 160
+
+
+def test_router_spreads_streams_by_remaining_budget():
+    """Streams go to the server with the most budget left after the streams routed to it; their
+    requests run there, in order; closing a stream returns its share."""
+    from dcvc_b200.serving import StreamRouter
+    fa, fb = FakeFactory(work=0.001), FakeFactory(work=0.001)
+    a = _server(fa, slots=2, budget=10 * 64 * 64)
+    b = _server(fb, slots=2, budget=6 * 64 * 64)
+    r = StreamRouter([a, b])
+    placed = [r.open_stream(sid, StreamSpec("enc", 64, 64)) for sid in range(8)]
+    # each stream takes 1 unit and goes where more units remain after it (a: 10, b: 6; a tie
+    # goes to the server with fewer streams): a a a a b a b a
+    assert placed == [0, 0, 0, 0, 1, 0, 1, 0]
+    reqs = [r.submit(sid, k, None) for k in range(3) for sid in range(8)]
+    for q in reqs:
+        assert q.wait(10) == (q.stream_id, q.seq, q.qp)
+    for sid in range(8):
+        f = fa if r.device_of(sid) == 0 else fb
+        assert [k for s, k in f.log if s == sid] == [0, 1, 2]
+    r.close_stream(0)  # a: 5 units used, b: 2 -> a new stream leaves 4 on a, 3 on b
+    assert r.open_stream(100, StreamSpec("enc", 64, 64)) == 0
+    with pytest.raises(ValueError):
+        r.open_stream(100, StreamSpec("enc", 64, 64))
+    with pytest.raises(ValueError, match="budget"):
+        r.open_stream(101, StreamSpec("enc", 4096, 4096))
+    with pytest.raises(ValueError):
+        r.submit(999, 0, None)
+    r.shutdown()
+    assert a.held_bytes() == 0 and b.held_bytes() == 0
