@@ -802,8 +802,14 @@ def run_gpu(args):
     torch.cuda.empty_cache()
     batched = batched_streams(args, H, W, args.streams) if args.streams > 0 else None
     torch.cuda.empty_cache()
-    # a one-GPU measurement: under torchrun the ranks skip it
-    serving = serving_bench(args) if args.serve_seconds > 0 and world == 1 else None
+    # a one-GPU measurement: under torchrun the ranks skip it.  A failure here is reported in its
+    # own key rather than losing the line.
+    serving = None
+    if args.serve_seconds > 0 and world == 1:
+        try:
+            serving = serving_bench(args)
+        except Exception as e:  # noqa: BLE001
+            serving = {"error": f"{type(e).__name__}: {e}"[:300]}
     torch.cuda.empty_cache()
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
