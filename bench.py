@@ -810,7 +810,10 @@ def run_gpu(args):
             serving = serving_bench(args)
         except Exception as e:  # noqa: BLE001
             serving = {"error": f"{type(e).__name__}: {e}"[:300]}
-    torch.cuda.empty_cache()
+    try:
+        torch.cuda.empty_cache()
+    except RuntimeError:
+        pass  # a context broken by the failure above; the CPU baseline and the line still follow
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(H, W)
