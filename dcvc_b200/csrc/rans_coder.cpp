@@ -578,16 +578,34 @@ inline int8_t rd_symbol(uint32_t& x, const uint8_t*& p, const uint8_t* end, bool
                         const int32_t* cdf, int32_t maxv, int last)
 {
     const uint32_t cum = x & ((1u << kScaleBits) - 1);
-    int s = 1;
-    while (s < last && static_cast<uint32_t>(cdf[s]) <= cum) {
-        ++s;
+    // s = the last entry j < last with cdf[j] <= cum.  The symbol mapping puts the most probable
+    // value (0) first, so most symbols end at s = 0 on one comparison; the others continue the
+    // linear search from 1.
+    const uint32_t c1 = static_cast<uint32_t>(cdf[1]);
+    int s = 0;
+    if (last > 1 && c1 <= cum) {
+        s = 1;
+        while (s + 1 < last && static_cast<uint32_t>(cdf[s + 1]) <= cum) {
+            ++s;
+        }
     }
-    --s;
     const uint32_t start = static_cast<uint32_t>(cdf[s]);
-    const uint32_t freq = static_cast<uint32_t>(cdf[s + 1] - cdf[s]);
-    x = freq * (x >> kScaleBits) + (x & ((1u << kScaleBits) - 1)) - start;
-    while (x < kRansL && !overrun) {
-        x = (x << 8) | rd_next(p, end, overrun);
+    const uint32_t freq = static_cast<uint32_t>(cdf[s + 1]) - start;
+    x = freq * (x >> kScaleBits) + cum - start;
+    // From a state in [2^23, 2^31) (every state a valid stream produces) at most two bytes bring
+    // x back into that range (x >> 16 >= 2^7 and freq >= 1): while two bytes remain they are read
+    // without per-byte bounds checks; the checked loop finishes anything else (a corrupt initial
+    // state, the stream's end) exactly as byte-at-a-time reading would.
+    if (x < kRansL) {
+        if (!overrun && end - p >= 2) {
+            x = (x << 8) | *p++;
+            if (x < kRansL) {
+                x = (x << 8) | *p++;
+            }
+        }
+        while (x < kRansL && !overrun) {
+            x = (x << 8) | rd_next(p, end, overrun);
+        }
     }
     int32_t v = s;
     if (v == maxv) {
@@ -606,7 +624,9 @@ inline int8_t rd_symbol(uint32_t& x, const uint8_t*& p, const uint8_t* end, bool
         }
         v = raw + maxv;
     }
-    return static_cast<int8_t>((v % 2 == 1) ? (v + 1) / 2 : -(v + 1) / 2);
+    // 0, +1, -1, +2, -2, ... for v = 0, 1, 2, 3, 4, ... (v >= 0), without a branch
+    const int32_t h = (v + 1) >> 1;
+    return static_cast<int8_t>((v & 1) ? h : -h);
 }
 
 }  // namespace
@@ -694,14 +714,16 @@ bool RansDecoderSession::decode_z_tasks(const RansTables& tables, int n, int cdf
     }
     run_parallel(ecp_, [&](int i) {
         Reader r = r_[i];  // a copy on this thread's stack (see Writer)
+        // the table in locals (the int8 output stores may alias anything, see decode_y)
+        const size_t stride = static_cast<size_t>(tz.stride);
+        const int32_t* const cdf = tz.cdf.data() + static_cast<size_t>(cdf_offset) * stride;
+        const int32_t* const maxv = tz.max_value.data() + cdf_offset;
+        const int last = tz.stride - 1;
         int b, e;
         split(n, ecp_, i, &b, &e);
         int chn = b % ch;  // table (k % ch) + cdf_offset, the channel stepped with k
         for (int k = b; k < e; ++k) {
-            const int t = chn + cdf_offset;
-            out[k] = rd_symbol(r.x, r.p, r.end, r.overrun,
-                               tz.cdf.data() + static_cast<size_t>(t) * tz.stride, tz.max_value[t],
-                               tz.stride - 1);
+            out[k] = rd_symbol(r.x, r.p, r.end, r.overrun, cdf + chn * stride, maxv[chn], last);
             chn = chn + 1 == ch ? 0 : chn + 1;
         }
         r_[i] = r;
@@ -726,17 +748,22 @@ bool RansDecoderSession::decode_y_tasks(const RansTables& tables, const uint8_t*
     bool bad[kMaxEcParallel] = {false};
     run_parallel(ecp_, [&](int i) {
         Reader r = r_[i];  // a copy on this thread's stack (see Writer)
+        // the table in locals: the int8 output stores may alias anything, so fields read through
+        // `ty` would be reloaded after every symbol
+        const int32_t* const cdf = ty.cdf.data();
+        const int32_t* const maxv = ty.max_value.data();
+        const size_t stride = static_cast<size_t>(ty.stride);
+        const int count = ty.count;
+        const int last = ty.stride - 1;
         int b, e;
         split(n, ecp_, i, &b, &e);
         for (int k = b; k < e; ++k) {
             const int t = idx[k];
-            if (t >= ty.count) {
+            if (t >= count) {
                 bad[i] = true;
                 break;
             }
-            out[k] = rd_symbol(r.x, r.p, r.end, r.overrun,
-                               ty.cdf.data() + static_cast<size_t>(t) * ty.stride, ty.max_value[t],
-                               ty.stride - 1);
+            out[k] = rd_symbol(r.x, r.p, r.end, r.overrun, cdf + t * stride, maxv[t], last);
         }
         r_[i] = r;
     });
