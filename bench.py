@@ -645,6 +645,21 @@ def intra_bench(stream, H, W, reps=10):
 
 # ----------------------------------------------------------------------------- arms
 
+def _section(fn, *a):
+    """fn(*a), or {"error": ...} when it raises."""
+    try:
+        return fn(*a)
+    except Exception as e:  # noqa: BLE001
+        return {"error": f"{type(e).__name__}: {e}"[:300]}
+
+
+def _empty_cache():
+    try:
+        torch.cuda.empty_cache()
+    except RuntimeError:
+        pass  # a context broken by a failed section; the CPU baseline and the line still follow
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -795,25 +810,20 @@ def run_gpu(args):
     split = split_enc_dec(enc, dec, xs, args, pb, pr, H, W, stream)
     clk = clocks.stop(windows)
     roof = roofline_quad(stream)
-    intra = None if args.no_intra else intra_bench(stream, H, W)
-    htl = None if args.no_htl else htl_bench(stream, H, W)
-    ld = None if args.no_ld else ld_bench(stream, H, W)
+    # The extra measurements below report a failure in their own key instead of losing the line
+    # (and every rank still reaches the closing barrier).
+    intra = None if args.no_intra else _section(intra_bench, stream, H, W)
+    htl = None if args.no_htl else _section(htl_bench, stream, H, W)
+    ld = None if args.no_ld else _section(ld_bench, stream, H, W)
     del enc, dec
-    torch.cuda.empty_cache()
-    batched = batched_streams(args, H, W, args.streams) if args.streams > 0 else None
-    torch.cuda.empty_cache()
-    # a one-GPU measurement: under torchrun the ranks skip it.  A failure here is reported in its
-    # own key rather than losing the line.
+    _empty_cache()
+    batched = _section(batched_streams, args, H, W, args.streams) if args.streams > 0 else None
+    _empty_cache()
+    # a one-GPU measurement: under torchrun the ranks skip it
     serving = None
     if args.serve_seconds > 0 and world == 1:
-        try:
-            serving = serving_bench(args)
-        except Exception as e:  # noqa: BLE001
-            serving = {"error": f"{type(e).__name__}: {e}"[:300]}
-    try:
-        torch.cuda.empty_cache()
-    except RuntimeError:
-        pass  # a context broken by the failure above; the CPU baseline and the line still follow
+        serving = _section(serving_bench, args)
+    _empty_cache()
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(H, W)
