@@ -29,6 +29,7 @@ STATUS_NAMES = {
 F16, BF16 = 0, 1
 EPI_BIAS, EPI_BIAS_WSILU, EPI_BIAS_RES, EPI_BIAS_RES_Q, EPI_BIAS_RES2, EPI_QUAD, EPI_SUBPEL, \
     EPI_BIAS_Q = range(8)
+BLOCK_N_STREAM = -1  # dcvc_conv1x1 block_n: the streaming form of the residual epilogues
 
 
 class DcvcError(RuntimeError):

@@ -120,6 +120,24 @@ int dcvc_hts_buffer(void* handle, const char* name, const void** ptr, int* rows,
     return static_cast<HtsHandle*>(handle)->codec.buffer(name, ptr, rows, cols, ld);
 }
 
+int dcvc_hts_set_precision(void* handle, int precision)
+{
+    if (handle == nullptr) {
+        return fail(kInvalidArgument, "dcvc_hts_set_precision: null handle");
+    }
+    return static_cast<HtsHandle*>(handle)->codec.set_precision(precision);
+}
+
+int dcvc_hts_buffer_dtype(void* handle, const char* name, int* dtype)
+{
+    if (handle == nullptr || name == nullptr || dtype == nullptr) {
+        return fail(kInvalidArgument, "dcvc_hts_buffer_dtype: null argument");
+    }
+    const void* p = nullptr;
+    int rows = 0, cols = 0, ld = 0;
+    return static_cast<HtsHandle*>(handle)->codec.buffer(name, &p, &rows, &cols, &ld, dtype);
+}
+
 int dcvc_hts_stats(void* handle, int* symbols, int* kernels, size_t* device_bytes)
 {
     if (handle == nullptr) {

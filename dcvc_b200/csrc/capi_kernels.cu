@@ -53,6 +53,50 @@ int dcvc_scale_index_table(uint8_t* lut)
     return kOk;
 }
 
+int dcvc_conv1x1_f8(int epilogue, int M, int N, int K, const void* a, int lda, const void* w,
+                    const float* wscale, const float* bias, void* out, int ldo, int block_n,
+                    void* stream)
+{
+    GemmParams p{};
+    p.M = M;
+    p.N = N;
+    p.K = K;
+    p.bias = bias;
+    p.wscale = wscale;
+    p.out = out;
+    p.ldo = ldo;
+    p.err = device_error_word();
+    cudaError_t e = gemm_sm100(kDtypeF8, a, lda, w, p, epilogue, block_n, static_cast<cudaStream_t>(stream));
+    if (e == cudaErrorInvalidValue) {
+        set_last_error("dcvc_conv1x1_f8: unsupported shape, pitch, alignment or epilogue");
+        return kInvalidArgument;
+    }
+    return cuda_status(e, "dcvc_conv1x1_f8");
+}
+
+int dcvc_quantize_fp8(const void* src, int src_dtype, int lds, float inv_scale, void* dst, int ldd,
+                      int M, int C, void* stream)
+{
+    cudaError_t e = launch_quantize_fp8(static_cast<const __half*>(src), src_dtype, lds, inv_scale,
+                                        static_cast<uint8_t*>(dst), ldd, M, C,
+                                        static_cast<cudaStream_t>(stream));
+    if (e == cudaErrorInvalidValue) {
+        set_last_error("dcvc_quantize_fp8: unsupported size, pitch, alignment or dtype");
+        return kInvalidArgument;
+    }
+    return cuda_status(e, "dcvc_quantize_fp8");
+}
+
+int dcvc_scale_index_table_device(uint8_t* lut, void* stream)
+{
+    if (lut == nullptr) {
+        set_last_error("dcvc_scale_index_table_device: null output");
+        return kInvalidArgument;
+    }
+    return cuda_status(scale_index_table_device(lut, static_cast<cudaStream_t>(stream)),
+                       "dcvc_scale_index_table_device");
+}
+
 int dcvc_conv1x1(int dtype, int epilogue, int M, int N, int K, const void* a, int lda,
                  const void* w, const float* bias, const void* res, int ldr, const void* res2,
                  int ldr2, const void* qscale, void* out, int ldo, int sub_w, int sub_cout,

@@ -193,6 +193,19 @@ __device__ __forceinline__ void tc_mma_f16(uint32_t tmem_d, uint64_t adesc, uint
         : "memory");
 }
 
+// The same for 8-bit operands (kind::f8f6f4; the instruction descriptor's A/B format 0 is
+// E4M3): one instruction covers K = 32, i.e. 32 bytes of each K-major row as in the 16-bit form.
+__device__ __forceinline__ void tc_mma_f8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                          uint32_t idesc, uint32_t accumulate)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
 // Arrives on the mbarrier once all previously issued tcgen05 ops of this thread complete.
 __device__ __forceinline__ void tc_commit(uint64_t* bar)
 {

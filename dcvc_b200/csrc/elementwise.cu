@@ -3,6 +3,8 @@
 #include "common.cuh"
 #include "host_util.h"
 
+#include <cuda_fp8.h>
+
 #include <algorithm>
 #include <mutex>
 
@@ -39,6 +41,41 @@ __device__ __forceinline__ void st8(__half* p, const Vec8h& v) { *reinterpret_ca
 
 // ------------------------------------------------------------------------------ layout
 
+// 16-bit activation formats: FP16 (0) or BF16 (1); conversions round to nearest.
+template <int DT>
+struct Act;
+template <>
+struct Act<0> {
+    using T = __half;
+    static __device__ __forceinline__ float2 to2(uint32_t u)
+    {
+        return __half22float2(*reinterpret_cast<const __half2*>(&u));
+    }
+    static __device__ __forceinline__ uint32_t from2(float a, float b)
+    {
+        __half2 h = __floats2half2_rn(a, b);
+        return *reinterpret_cast<uint32_t*>(&h);
+    }
+    static __device__ __forceinline__ float to(uint16_t u) { return __half2float(__ushort_as_half(u)); }
+    static __device__ __forceinline__ uint16_t from(float f) { return __half_as_ushort(__float2half_rn(f)); }
+};
+template <>
+struct Act<1> {
+    using T = __nv_bfloat16;
+    static __device__ __forceinline__ float2 to2(uint32_t u)
+    {
+        return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u));
+    }
+    static __device__ __forceinline__ uint32_t from2(float a, float b)
+    {
+        __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+        return *reinterpret_cast<uint32_t*>(&h);
+    }
+    static __device__ __forceinline__ float to(uint16_t u) { return __bfloat162float(__ushort_as_bfloat16(u)); }
+    static __device__ __forceinline__ uint16_t from(float f) { return __bfloat16_as_ushort(__float2bfloat16_rn(f)); }
+};
+
+template <int ODT>
 __global__ void pad_unshuffle8_kernel(const __half* __restrict__ x, int H, int W, int C, int ldx,
                                       int H8, int W8, __half* __restrict__ out, int ldo)
 {
@@ -61,11 +98,15 @@ __global__ void pad_unshuffle8_kernel(const __half* __restrict__ x, int H, int W
         for (int dx = 0; dx < 8; ++dx) {
             const int sw = min(w8 * 8 + dx, W - 1);
             o.v[dx] = x[(static_cast<long long>(sh) * W + sw) * ldx + c];
+            if constexpr (ODT == 1) {  // the same values as BF16
+                o.v[dx] = __ushort_as_half(Act<1>::from(__half2float(o.v[dx])));
+            }
         }
         st8(out + pix * ldo + c * 64 + dy * 8, o);
     }
 }
 
+template <int IDT>
 __global__ void shuffle8_clamp_kernel(const __half* __restrict__ in, int H8, int W8, int C, int ldi,
                                       __half* __restrict__ out)
 {
@@ -83,8 +124,13 @@ __global__ void shuffle8_clamp_kernel(const __half* __restrict__ in, int H8, int
                             (y & 7) * 8 + (xx & 7);
         for (int c = 0; c < C; ++c) {
             __half v = src[c * 64];
-            v = __hmax(v, lo);
-            v = __hmin(v, hi);
+            if constexpr (IDT == 1) {  // BF16 input: clamp in FP32, one rounding to FP16
+                const float f = Act<1>::to(__half_as_ushort(v));
+                v = __float2half_rn(fminf(fmaxf(f, -0.5f), 0.5f));
+            } else {
+                v = __hmax(v, lo);
+                v = __hmin(v, hi);
+            }
             out[i * C + c] = v;
         }
     }
@@ -206,6 +252,7 @@ __global__ void int8_to_half_kernel(const int8_t* __restrict__ x, int n, __half*
     }
 }
 
+template <int IDT>
 __global__ void mul_channel_kernel(const __half* __restrict__ x, int M, int C, int ldx,
                                    const __half* __restrict__ q, __half* __restrict__ out, int ldo)
 {
@@ -221,7 +268,9 @@ __global__ void mul_channel_kernel(const __half* __restrict__ x, int M, int C, i
         const Vec8h b = ld8(q + v * 8);
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
-            a.v[j] = hmul(a.v[j], b.v[j]);
+            // a BF16 input value is exact in FP32; the product is rounded once to FP16
+            const float av = IDT == 1 ? Act<1>::to(__half_as_ushort(a.v[j])) : h2f(a.v[j]);
+            a.v[j] = f2h(__fmul_rn(av, h2f(b.v[j])));
         }
         st8(out + m * ldo + v * 8, a);
     }
@@ -710,6 +759,7 @@ __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src,
                  : "memory");
 }
 
+template <int DT>
 __global__ void __launch_bounds__(kDwThreads) dwconv3x3_kernel(const __half* __restrict__ x, int H,
                                                                int W, int C, int ldx,
                                                                const float* __restrict__ wt,
@@ -754,8 +804,8 @@ __global__ void __launch_bounds__(kDwThreads) dwconv3x3_kernel(const __half* __r
     if (!live || ha >= H) {
         return;
     }
-    const __half2* t2 = reinterpret_cast<const __half2*>(&tile[0][0][0]);
-    auto at = [&](int r, int c) { return __half22float2(t2[(r * (kDwTW + 2) + c) * (4 * kDwCV) + cp]); };
+    const uint32_t* t2 = reinterpret_cast<const uint32_t*>(&tile[0][0][0]);
+    auto at = [&](int r, int c) { return Act<DT>::to2(t2[(r * (kDwTW + 2) + c) * (4 * kDwCV) + cp]); };
     float2 win[kDwRows + 2][3];  // window rows ty .. ty + kDwRows + 1 (image rows ha - 1 ..)
 #pragma unroll
     for (int r = 0; r < kDwRows + 2; ++r) {
@@ -793,7 +843,7 @@ __global__ void __launch_bounds__(kDwThreads) dwconv3x3_kernel(const __half* __r
 #pragma unroll
             for (int o = 0; o < kDwRows; ++o) {
                 if (ha + o < H) {
-                    *reinterpret_cast<__half2*>(op + o * next_row) = __floats2half2_rn(acc[o].x, acc[o].y);
+                    *reinterpret_cast<uint32_t*>(op + o * next_row) = Act<DT>::from2(acc[o].x, acc[o].y);
                 }
             }
         }
@@ -805,30 +855,127 @@ __global__ void __launch_bounds__(kDwThreads) dwconv3x3_kernel(const __half* __r
     }
 }
 
+// dst[m, c] = src[m, c] converted between the 16-bit activation formats (round to nearest).
+template <int SDT, int DDT>
+__global__ void convert_kernel(const __half* __restrict__ src, int lds, __half* __restrict__ dst,
+                               int ldd, int M, int C)
+{
+    griddep_launch_dependents();
+    griddep_wait();
+    const int vecs = C / 8;
+    const long long total = static_cast<long long>(M) * vecs;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const long long m = i / vecs;
+        const int v = static_cast<int>(i - m * vecs);
+        const uint4 a = *reinterpret_cast<const uint4*>(src + m * lds + v * 8);
+        const float2 f0 = Act<SDT>::to2(a.x), f1 = Act<SDT>::to2(a.y);
+        const float2 f2 = Act<SDT>::to2(a.z), f3 = Act<SDT>::to2(a.w);
+        *reinterpret_cast<uint4*>(dst + m * ldd + v * 8) =
+            make_uint4(Act<DDT>::from2(f0.x, f0.y), Act<DDT>::from2(f1.x, f1.y),
+                       Act<DDT>::from2(f2.x, f2.y), Act<DDT>::from2(f3.x, f3.y));
+    }
+}
+
+// dst[m, c] = E4M3(src[m, c] * inv_scale), saturating to +-448 (NaN stays NaN).
+template <int SDT>
+__global__ void quantize_fp8_kernel(const __half* __restrict__ src, int lds, float inv_scale,
+                                    uint8_t* __restrict__ dst, int ldd, int M, int C)
+{
+    griddep_launch_dependents();
+    griddep_wait();
+    const int vecs = C / 8;
+    const long long total = static_cast<long long>(M) * vecs;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const long long m = i / vecs;
+        const int v = static_cast<int>(i - m * vecs);
+        const uint4 a = *reinterpret_cast<const uint4*>(src + m * lds + v * 8);
+        const uint32_t w[4] = {a.x, a.y, a.z, a.w};
+        uint32_t o[2];
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const float2 f0 = Act<SDT>::to2(w[2 * j]);
+            const float2 f1 = Act<SDT>::to2(w[2 * j + 1]);
+            const __nv_fp8x2_storage_t lo = __nv_cvt_float2_to_fp8x2(
+                make_float2(f0.x * inv_scale, f0.y * inv_scale), __NV_SATFINITE, __NV_E4M3);
+            const __nv_fp8x2_storage_t hi = __nv_cvt_float2_to_fp8x2(
+                make_float2(f1.x * inv_scale, f1.y * inv_scale), __NV_SATFINITE, __NV_E4M3);
+            o[j] = static_cast<uint32_t>(lo) | (static_cast<uint32_t>(hi) << 16);
+        }
+        *reinterpret_cast<uint2*>(dst + m * ldd + v * 8) = make_uint2(o[0], o[1]);
+    }
+}
+
 inline bool al16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
 
 }  // namespace
 
+cudaError_t launch_quantize_fp8(const __half* src, int src_dtype, int lds, float inv_scale,
+                                uint8_t* dst, int ldd, int M, int C, cudaStream_t s)
+{
+    if (M <= 0 || C % 8 || lds % 8 || ldd % 8 || !al16(src) ||
+        (reinterpret_cast<uintptr_t>(dst) & 7) || (src_dtype != 0 && src_dtype != 1)) {
+        return cudaErrorInvalidValue;
+    }
+    const dim3 g(grid_for(static_cast<long long>(M) * (C / 8)));
+    if (src_dtype == 1) {
+        launch_pdl(quantize_fp8_kernel<1>, g, dim3(kThreads), 0, s, src, lds, inv_scale, dst, ldd, M, C);
+    } else {
+        launch_pdl(quantize_fp8_kernel<0>, g, dim3(kThreads), 0, s, src, lds, inv_scale, dst, ldd, M, C);
+    }
+    return cudaGetLastError();
+}
+
 cudaError_t launch_pad_unshuffle8(const __half* x, int H, int W, int C, int ldx, int pad_b,
-                                  int pad_r, __half* out, int ldo, cudaStream_t s)
+                                  int pad_r, __half* out, int ldo, cudaStream_t s, int out_dtype)
 {
     if (H <= 0 || W <= 0 || (H + pad_b) % 8 || (W + pad_r) % 8 || pad_b < 0 || pad_r < 0 ||
-        ldo % 8 || !al16(out)) {
+        ldo % 8 || !al16(out) || (out_dtype != 0 && out_dtype != 1)) {
         return cudaErrorInvalidValue;
     }
     const int H8 = (H + pad_b) / 8, W8 = (W + pad_r) / 8;
-    launch_pdl(pad_unshuffle8_kernel, dim3(grid_for(static_cast<long long>(H8) * W8 * C * 8)), dim3(kThreads), 0, s, 
-        x, H, W, C, ldx, H8, W8, out, ldo);
+    const dim3 g(grid_for(static_cast<long long>(H8) * W8 * C * 8));
+    if (out_dtype == 1) {
+        launch_pdl(pad_unshuffle8_kernel<1>, g, dim3(kThreads), 0, s, x, H, W, C, ldx, H8, W8, out, ldo);
+    } else {
+        launch_pdl(pad_unshuffle8_kernel<0>, g, dim3(kThreads), 0, s, x, H, W, C, ldx, H8, W8, out, ldo);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_convert(const __half* src, int src_dtype, int lds, __half* dst, int dst_dtype,
+                           int ldd, int M, int C, cudaStream_t s)
+{
+    if (M <= 0 || C % 8 || lds % 8 || ldd % 8 || !al16(src) || !al16(dst) ||
+        (src_dtype != 0 && src_dtype != 1) || (dst_dtype != 0 && dst_dtype != 1)) {
+        return cudaErrorInvalidValue;
+    }
+    const dim3 g(grid_for(static_cast<long long>(M) * (C / 8)));
+    if (src_dtype == 0 && dst_dtype == 1) {
+        launch_pdl(convert_kernel<0, 1>, g, dim3(kThreads), 0, s, src, lds, dst, ldd, M, C);
+    } else if (src_dtype == 1 && dst_dtype == 0) {
+        launch_pdl(convert_kernel<1, 0>, g, dim3(kThreads), 0, s, src, lds, dst, ldd, M, C);
+    } else if (src_dtype == 0) {
+        launch_pdl(convert_kernel<0, 0>, g, dim3(kThreads), 0, s, src, lds, dst, ldd, M, C);
+    } else {
+        launch_pdl(convert_kernel<1, 1>, g, dim3(kThreads), 0, s, src, lds, dst, ldd, M, C);
+    }
     return cudaGetLastError();
 }
 
 cudaError_t launch_shuffle8_clamp(const __half* in, int H8, int W8, int C, int ldi, __half* out,
-                                  cudaStream_t s)
+                                  cudaStream_t s, int in_dtype)
 {
-    if (H8 <= 0 || W8 <= 0 || C <= 0) {
+    if (H8 <= 0 || W8 <= 0 || C <= 0 || (in_dtype != 0 && in_dtype != 1)) {
         return cudaErrorInvalidValue;
     }
-    launch_pdl(shuffle8_clamp_kernel, dim3(grid_for(64LL * H8 * W8)), dim3(kThreads), 0, s, in, H8, W8, C, ldi, out);
+    const dim3 g(grid_for(64LL * H8 * W8));
+    if (in_dtype == 1) {
+        launch_pdl(shuffle8_clamp_kernel<1>, g, dim3(kThreads), 0, s, in, H8, W8, C, ldi, out);
+    } else {
+        launch_pdl(shuffle8_clamp_kernel<0>, g, dim3(kThreads), 0, s, in, H8, W8, C, ldi, out);
+    }
     return cudaGetLastError();
 }
 
@@ -905,13 +1052,18 @@ cudaError_t launch_int8_to_half(const int8_t* x, int n, __half* out, cudaStream_
 }
 
 cudaError_t launch_mul_channel(const __half* x, int M, int C, int ldx, const __half* q,
-                               __half* out, int ldo, cudaStream_t s)
+                               __half* out, int ldo, cudaStream_t s, int in_dtype)
 {
-    if (C % 8 || ldx % 8 || ldo % 8 || !al16(x) || !al16(q) || !al16(out)) {
+    if (C % 8 || ldx % 8 || ldo % 8 || !al16(x) || !al16(q) || !al16(out) ||
+        (in_dtype != 0 && in_dtype != 1)) {
         return cudaErrorInvalidValue;
     }
-    launch_pdl(mul_channel_kernel, dim3(grid_for(static_cast<long long>(M) * (C / 8))), dim3(kThreads), 0, s, 
-        x, M, C, ldx, q, out, ldo);
+    const dim3 g(grid_for(static_cast<long long>(M) * (C / 8)));
+    if (in_dtype == 1) {
+        launch_pdl(mul_channel_kernel<1>, g, dim3(kThreads), 0, s, x, M, C, ldx, q, out, ldo);
+    } else {
+        launch_pdl(mul_channel_kernel<0>, g, dim3(kThreads), 0, s, x, M, C, ldx, q, out, ldo);
+    }
     return cudaGetLastError();
 }
 
@@ -1059,10 +1211,28 @@ cudaError_t launch_restore_4x(int phase, int mode, const __half* part, const __h
 
 int compact_blocks(int n) { return (n + kCompactBlock - 1) / kCompactBlock; }
 
+bool compact_args_ok(const void* src, int elem_bytes, const uint8_t* cond, int n, const void* dst,
+                     const int* total, bool needs_block_counts, const int* block_counts)
+{
+    if (n <= 0 || (elem_bytes != 1 && elem_bytes != 2)) {
+        return false;
+    }
+    if (src == nullptr || dst == nullptr || cond == nullptr || total == nullptr ||
+        (needs_block_counts && block_counts == nullptr)) {
+        return false;
+    }
+    // cond is read 8 bytes at a time; 2-byte elements are read and written as int16
+    const uintptr_t c = reinterpret_cast<uintptr_t>(cond);
+    const uintptr_t e = reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst);
+    const uintptr_t t = reinterpret_cast<uintptr_t>(total) |
+                        reinterpret_cast<uintptr_t>(needs_block_counts ? block_counts : nullptr);
+    return (c & 7) == 0 && (elem_bytes == 1 || (e & 1) == 0) && (t & 3) == 0;
+}
+
 cudaError_t launch_compact(const void* src, int elem_bytes, const uint8_t* cond, int n,
                            int* block_counts, void* dst, int* total, cudaStream_t s)
 {
-    if (n <= 0 || (elem_bytes != 1 && elem_bytes != 2) || (reinterpret_cast<uintptr_t>(cond) & 7)) {
+    if (!compact_args_ok(src, elem_bytes, cond, n, dst, total, true, block_counts)) {
         return cudaErrorInvalidValue;
     }
     const int nb = compact_blocks(n);
@@ -1082,7 +1252,9 @@ cudaError_t launch_compact(const void* src, int elem_bytes, const uint8_t* cond,
 cudaError_t launch_recover(const int8_t* dec, const uint8_t* cond, const int* block_counts, int n,
                            __half* out, cudaStream_t s)
 {
-    if (n <= 0 || (reinterpret_cast<uintptr_t>(cond) & 7)) {
+    if (n <= 0 || dec == nullptr || out == nullptr || block_counts == nullptr || cond == nullptr ||
+        (reinterpret_cast<uintptr_t>(cond) & 7) || (reinterpret_cast<uintptr_t>(out) & 1) ||
+        (reinterpret_cast<uintptr_t>(block_counts) & 3)) {
         return cudaErrorInvalidValue;
     }
     launch_pdl(recover_kernel, dim3(compact_blocks(n)), dim3(kCompactThreads), 0, s, dec, cond, block_counts, n, out);
@@ -1090,13 +1262,18 @@ cudaError_t launch_recover(const int8_t* dec, const uint8_t* cond, const int* bl
 }
 
 cudaError_t launch_dwconv3x3(const __half* x, int H, int W, int C, int ldx, const float* w,
-                             __half* out, int ldo, cudaStream_t s)
+                             __half* out, int ldo, cudaStream_t s, int dtype)
 {
-    if (C % 8 || ldx % 8 || ldo % 8 || !al16(x) || !al16(out) || !al16(w)) {
+    if (C % 8 || ldx % 8 || ldo % 8 || !al16(x) || !al16(out) || !al16(w) ||
+        (dtype != 0 && dtype != 1)) {
         return cudaErrorInvalidValue;
     }
     const dim3 grid((C / 8 + kDwCV - 1) / kDwCV, (H + kDwTH - 1) / kDwTH, (W + kDwTW - 1) / kDwTW);
-    launch_pdl(dwconv3x3_kernel, dim3(grid), dim3(kDwThreads), 0, s, x, H, W, C, ldx, w, out, ldo);
+    if (dtype == 1) {
+        launch_pdl(dwconv3x3_kernel<1>, grid, dim3(kDwThreads), 0, s, x, H, W, C, ldx, w, out, ldo);
+    } else {
+        launch_pdl(dwconv3x3_kernel<0>, grid, dim3(kDwThreads), 0, s, x, H, W, C, ldx, w, out, ldo);
+    }
     return cudaGetLastError();
 }
 
@@ -1171,12 +1348,36 @@ static __device__ __align__(256) int g_compact_block_counts[kCompactNoAllocMaxBl
 int compact_noalloc_max_elements() { return kCompactNoAllocMaxBlocks * kCompactBlock; }
 
 // The host cannot use g_compact_block_counts as a device address: its device address is looked
-// up once per device (with that device current) and cached.  The lookup happens on the first call
-// on each device, so that first call must not be made while a stream is being captured.
+// up once per device (with that device current) and cached together with the context it belongs
+// to.  The lookup happens on the first call on each device, so that first call must not be made
+// while a stream is being captured.  If the device's context is destroyed and re-created (an
+// embedding caller's cudaDeviceReset), the next call sees a different current context and looks
+// the address up again instead of using the stale one.
+static void* current_context()
+{
+    using GetCtxFn = int (*)(void**);
+    static GetCtxFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess) {
+            fn = reinterpret_cast<GetCtxFn>(p);
+        }
+    });
+    void* ctx = nullptr;
+    if (fn == nullptr || fn(&ctx) != 0) {
+        return nullptr;
+    }
+    return ctx;
+}
+
 static int* compact_noalloc_scratch(cudaError_t* err)
 {
     static std::mutex mu;
     static int* addr[64] = {nullptr};
+    static void* ctx_of[64] = {nullptr};
     int dev = 0;
     *err = cudaGetDevice(&dev);
     if (*err != cudaSuccess) {
@@ -1187,13 +1388,16 @@ static int* compact_noalloc_scratch(cudaError_t* err)
         return nullptr;
     }
     std::lock_guard<std::mutex> lk(mu);
-    if (addr[dev] == nullptr) {
+    void* ctx = current_context();
+    if (addr[dev] == nullptr || ctx == nullptr || ctx != ctx_of[dev]) {
         void* p = nullptr;
         *err = cudaGetSymbolAddress(&p, g_compact_block_counts);
         if (*err != cudaSuccess) {
             return nullptr;
         }
         addr[dev] = static_cast<int*>(p);
+        // the symbol lookup makes the device's primary context current if none was
+        ctx_of[dev] = ctx != nullptr ? ctx : current_context();
     }
     return addr[dev];
 }
@@ -1201,8 +1405,8 @@ static int* compact_noalloc_scratch(cudaError_t* err)
 cudaError_t launch_compact_noalloc(const void* src, int elem_bytes, const uint8_t* cond, int n,
                                    void* dst, int* total, cudaStream_t s)
 {
-    if (n <= 0 || n > compact_noalloc_max_elements() || (elem_bytes != 1 && elem_bytes != 2) ||
-        (reinterpret_cast<uintptr_t>(cond) & 7)) {
+    if (n > compact_noalloc_max_elements() ||
+        !compact_args_ok(src, elem_bytes, cond, n, dst, total, false, nullptr)) {
         return cudaErrorInvalidValue;
     }
     cudaError_t err = cudaSuccess;

@@ -1,4 +1,6 @@
-// Elementwise, layout and quantisation kernels (NHWC, FP16) and their launchers.
+// Elementwise, layout and quantisation kernels (NHWC, FP16) and their launchers.  The layout and
+// depthwise kernels that the analysis / synthesis transforms use also take BF16 activations
+// (dtype 1; dtype 0 is FP16); the quantisation and entropy-parameter kernels are FP16 only.
 //
 // Arithmetic follows the reference's FP16 kernels op for op (src/layers/extensions/inference/
 // elementwise/stream.cu, cat_and_pad.cu, shuffle.cu): every FP16 op is computed in FP32 and
@@ -23,13 +25,25 @@ __host__ __device__ __forceinline__ int mask_position(int phase, int quarter)
 
 // pad_and_unshuffle_8 (cat_and_pad.cu:7-51) / pixel_unshuffle by 8 (shuffle.cu:134-185):
 // out[h8, w8, c*64 + dy*8 + dx] = x[min(8h8+dy, H-1), min(8w8+dx, W-1), c].
+// out_dtype 1 writes the same values as BF16 (the input is FP16).
 cudaError_t launch_pad_unshuffle8(const __half* x, int H, int W, int C, int ldx, int pad_b,
-                                  int pad_r, __half* out, int ldo, cudaStream_t s);
+                                  int pad_r, __half* out, int ldo, cudaStream_t s,
+                                  int out_dtype = 0);
+
+// dst[m, c] = E4M3(src[m, c] * inv_scale) (bytes), saturating to +-448; src FP16 (0) or BF16 (1);
+// C % 8 == 0, ldd % 8 == 0.  The A operand of the FP8 GEMM form.
+cudaError_t launch_quantize_fp8(const __half* src, int src_dtype, int lds, float inv_scale,
+                                uint8_t* dst, int ldd, int M, int C, cudaStream_t s);
+
+// dst[m, c] = src[m, c] converted between FP16 (0) and BF16 (1), rounded to nearest; C % 8 == 0.
+cudaError_t launch_convert(const __half* src, int src_dtype, int lds, __half* dst, int dst_dtype,
+                           int ldd, int M, int C, cudaStream_t s);
 
 // pixel_shuffle_8 with clamp to [-0.5, 0.5] (shuffle.cu:40-131):
 // out[y, x, c] = clamp(in[y/8, x/8, c*64 + (y%8)*8 + x%8]).  out is [8*H8, 8*W8, C] dense.
+// in_dtype 1: BF16 input, clamped in FP32 and rounded once to the FP16 output.
 cudaError_t launch_shuffle8_clamp(const __half* in, int H8, int W8, int C, int ldi, __half* out,
-                                  cudaStream_t s);
+                                  cudaStream_t s, int in_dtype = 0);
 
 // out[(h, w), (dy*2 + dx)*C + c] = x[2h+dy, 2w+dx, c]   (pixel_unshuffle(2) with the channel
 // order permuted to (dy, dx, c); the stride-2 conv weight is permuted to match).
@@ -61,8 +75,9 @@ cudaError_t launch_round_z(const __half* z, int n, __half* z_hat, int8_t* z_i8, 
 cudaError_t launch_int8_to_half(const int8_t* x, int n, __half* out, cudaStream_t s);
 
 // multiply_with_broadcast (stream.cu:484-546): out[m, c] = x[m, c] * q[c].
+// in_dtype 1: x is BF16 (q and out stay FP16; one rounding of the FP32 product).
 cudaError_t launch_mul_channel(const __half* x, int M, int C, int ldx, const __half* q,
-                               __half* out, int ldo, cudaStream_t s);
+                               __half* out, int ldo, cudaStream_t s, int in_dtype = 0);
 
 // divide_with_clamp_inplace (stream.cu:422-452): y <- y * rcp(max(q, 0.5)), the reciprocal
 // rounded from FP32 1/q.
@@ -121,6 +136,11 @@ cudaError_t launch_restore_4x(int phase, int mode, const __half* part, const __h
 // stream.cu:175-338).  block_counts needs compact_blocks(n) ints; *total (device) receives the
 // number of kept elements.
 int compact_blocks(int n);
+// Host-side validation shared by the compaction launchers (no CUDA call): n > 0, elem_bytes 1 or
+// 2, non-null pointers, cond 8-byte aligned, 2-byte elements 2-byte aligned, counters 4-byte
+// aligned.  block_counts is checked only when the launcher takes one.
+bool compact_args_ok(const void* src, int elem_bytes, const uint8_t* cond, int n, const void* dst,
+                     const int* total, bool needs_block_counts, const int* block_counts);
 cudaError_t launch_compact(const void* src, int elem_bytes, const uint8_t* cond, int n,
                            int* block_counts, void* dst, int* total, cudaStream_t s);
 
@@ -146,6 +166,6 @@ cudaError_t launch_recover(const int8_t* dec, const uint8_t* cond, const int* bl
 // Depthwise 3x3, pad 1, no bias (d3x3, cutlass/d3x3_kernel.h:104-166): FP32 accumulation in the
 // order ky, kx.  w is FP32 [9][C] (tap-major).
 cudaError_t launch_dwconv3x3(const __half* x, int H, int W, int C, int ldx, const float* w,
-                             __half* out, int ldo, cudaStream_t s);
+                             __half* out, int ldo, cudaStream_t s, int dtype = 0);
 
 }  // namespace dcvc

@@ -113,12 +113,15 @@ __device__ __forceinline__ int stage_off(int r, int j)
     }
 }
 
-template <typename T, int BN, int EPI>
+// F8: E4M3 operands (kind::f8f6f4, 128 elements per 128-byte K block) with the accumulator scaled
+// per output channel by p.wscale before the bias; T is then the BF16 output type.
+template <typename T, int BN, int EPI, bool F8 = false>
 __global__ void __launch_bounds__(GemmCfg<BN, EPI>::kThreads, 1)
     gemm_sm100_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                       const __grid_constant__ CUtensorMap tmO, const __grid_constant__ CUtensorMap tmR,
                       const __grid_constant__ CUtensorMap tmR2, const GemmParams p)
 {
+    constexpr int kKElems = F8 ? 128 : kBK;  // K elements per 128-byte K block
     using C = GemmCfg<BN, EPI>;
     constexpr int kStages = C::kStages;
     extern __shared__ uint8_t smem_raw[];
@@ -138,7 +141,7 @@ __global__ void __launch_bounds__(GemmCfg<BN, EPI>::kThreads, 1)
     const int num_m = (p.M + kBM - 1) / kBM;
     const int num_n = p.N / BN;
     const int num_tiles = num_m * num_n;
-    const int kblocks = p.K / kBK;
+    const int kblocks = p.K / kKElems;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < kStages; ++s) {
@@ -189,8 +192,8 @@ __global__ void __launch_bounds__(GemmCfg<BN, EPI>::kThreads, 1)
                     }
                     mbar_arrive_expect_tx(&full[stage], C::kStageBytes);
                     uint8_t* sa = smem + stage * C::kStageBytes;
-                    tma_load_2d(sa, &tmA, &full[stage], kb * kBK, m0);
-                    tma_load_2d(sa + C::kABytes, &tmB, &full[stage], kb * kBK, n0);
+                    tma_load_2d(sa, &tmA, &full[stage], kb * kKElems, m0);
+                    tma_load_2d(sa + C::kABytes, &tmB, &full[stage], kb * kKElems, n0);
                     ++issued;
                     if (++stage == kStages) {
                         stage = 0;
@@ -213,7 +216,8 @@ __global__ void __launch_bounds__(GemmCfg<BN, EPI>::kThreads, 1)
     } else if (warp == 1) {
         // ------------------------------------------------------------ MMA issuer
         if (lane == 0) {
-            const uint32_t idesc = make_idesc_f16(kBM, BN, Pack2<T>::kFormat);
+            // format 0 is F16 for kind::f16 and E4M3 for kind::f8f6f4
+            const uint32_t idesc = make_idesc_f16(kBM, BN, F8 ? 0 : Pack2<T>::kFormat);
             int stage = 0;
             uint32_t phase = 0;
             int acc = 0;
@@ -238,9 +242,14 @@ __global__ void __launch_bounds__(GemmCfg<BN, EPI>::kThreads, 1)
                     const uint64_t adesc = make_sw128_kmajor_desc(smem_u32(sa));
                     const uint64_t bdesc = make_sw128_kmajor_desc(smem_u32(sa + C::kABytes));
 #pragma unroll
-                    for (int k = 0; k < kBK / 16; ++k) {
-                        // +32 bytes per K=16 step inside the swizzle atom (descriptor units of 16 B)
-                        tc_mma_f16(d, adesc + 2 * k, bdesc + 2 * k, idesc, (kb | k) != 0 ? 1u : 0u);
+                    for (int k = 0; k < 4; ++k) {
+                        // +32 bytes per instruction inside the swizzle atom (descriptor units of
+                        // 16 B): K = 16 16-bit or K = 32 8-bit elements
+                        if constexpr (F8) {
+                            tc_mma_f8(d, adesc + 2 * k, bdesc + 2 * k, idesc, (kb | k) != 0 ? 1u : 0u);
+                        } else {
+                            tc_mma_f16(d, adesc + 2 * k, bdesc + 2 * k, idesc, (kb | k) != 0 ? 1u : 0u);
+                        }
                     }
                     issued_any = true;
                     tc_commit(&empty[stage]);
@@ -416,12 +425,17 @@ __global__ void __launch_bounds__(GemmCfg<BN, EPI>::kThreads, 1)
 #pragma unroll
                         for (int j = 0; j < 8; ++j) {
                             const float4 bj = kHoist ? bb[j] : __ldg(b4 + j);
-                            v[2 * j] = __fadd2_rn(
-                                make_float2(__uint_as_float(r[4 * j + 0]), __uint_as_float(r[4 * j + 1])),
-                                make_float2(bj.x, bj.y));
-                            v[2 * j + 1] = __fadd2_rn(
-                                make_float2(__uint_as_float(r[4 * j + 2]), __uint_as_float(r[4 * j + 3])),
-                                make_float2(bj.z, bj.w));
+                            const float2 a0 = make_float2(__uint_as_float(r[4 * j + 0]), __uint_as_float(r[4 * j + 1]));
+                            const float2 a1 = make_float2(__uint_as_float(r[4 * j + 2]), __uint_as_float(r[4 * j + 3]));
+                            if constexpr (F8) {
+                                // dequantise: acc * (activation scale * weight row scale) + bias
+                                const float4 sj = __ldg(reinterpret_cast<const float4*>(p.wscale + nc) + j);
+                                v[2 * j] = __ffma2_rn(a0, make_float2(sj.x, sj.y), make_float2(bj.x, bj.y));
+                                v[2 * j + 1] = __ffma2_rn(a1, make_float2(sj.z, sj.w), make_float2(bj.z, bj.w));
+                            } else {
+                                v[2 * j] = __fadd2_rn(a0, make_float2(bj.x, bj.y));
+                                v[2 * j + 1] = __fadd2_rn(a1, make_float2(bj.z, bj.w));
+                            }
                         }
                         if constexpr (EPI == kEpiQuad) {
                             uint32_t o[4];
@@ -544,11 +558,11 @@ struct Maps {
     CUtensorMap a, b, o, r, r2;
 };
 
-template <typename T, int BN, int EPI>
+template <typename T, int BN, int EPI, bool F8 = false>
 cudaError_t launch_one(const Maps& m, const GemmParams& p, cudaStream_t stream)
 {
     using C = GemmCfg<BN, EPI>;
-    auto kernel = gemm_sm100_kernel<T, BN, EPI>;
+    auto kernel = gemm_sm100_kernel<T, BN, EPI, F8>;
     static std::once_flag once;
     static cudaError_t attr_err = cudaSuccess;
     std::call_once(once, [&] {
@@ -578,6 +592,22 @@ cudaError_t dispatch_epi(int epi, const Maps& m, const GemmParams& p, cudaStream
         return cudaErrorInvalidValue;
     case kEpiSubpel: return launch_one<T, BN, kEpiSubpel>(m, p, s);
     case kEpiBiasQ: return launch_one<T, BN, kEpiBiasQ>(m, p, s);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+// The FP8 form serves the DepthConvBlock GEMMs without a residual.
+template <int BN>
+cudaError_t dispatch_epi_f8(int epi, const Maps& m, const GemmParams& p, cudaStream_t s)
+{
+    switch (epi) {
+    case kEpiBias: return launch_one<__nv_bfloat16, BN, kEpiBias, true>(m, p, s);
+    case kEpiBiasWsilu: return launch_one<__nv_bfloat16, BN, kEpiBiasWsilu, true>(m, p, s);
+    case kEpiQuad:
+        if constexpr (BN == 256) {
+            return launch_one<__nv_bfloat16, BN, kEpiQuad, true>(m, p, s);
+        }
+        return cudaErrorInvalidValue;
     default: return cudaErrorInvalidValue;
     }
 }
@@ -617,9 +647,15 @@ int gemm_pick_bn(int M, int N, int epi, int sub_cout)
 cudaError_t gemm_sm100(int dtype, const void* A, int lda, const void* W, const GemmParams& p,
                        int epi, int bn, cudaStream_t stream)
 {
-    if (p.M <= 0 || p.N <= 0 || p.K <= 0 || p.K % kBK != 0 || lda % 8 != 0 ||
+    const bool f8 = dtype == kDtypeF8;
+    if (dtype < 0 || dtype > kDtypeF8 || p.M <= 0 || p.N <= 0 || p.K <= 0 ||
+        p.K % (f8 ? 128 : kBK) != 0 || lda % (f8 ? 16 : 8) != 0 ||
         (reinterpret_cast<uintptr_t>(A) & 15) != 0 || (reinterpret_cast<uintptr_t>(W) & 15) != 0 ||
         (reinterpret_cast<uintptr_t>(p.out) & 15) != 0 || p.ldo % 8 != 0) {
+        return cudaErrorInvalidValue;
+    }
+    if (f8 && (p.wscale == nullptr || (reinterpret_cast<uintptr_t>(p.wscale) & 15) != 0 ||
+               (epi != kEpiBias && epi != kEpiBiasWsilu && epi != kEpiQuad))) {
         return cudaErrorInvalidValue;
     }
     if (bn == 0) {
@@ -629,7 +665,10 @@ cudaError_t gemm_sm100(int dtype, const void* A, int lda, const void* W, const G
             bn = gemm_pick_bn(p.M, p.N, epi, p.sub_cout);
         }
     }
-    if (bn == 0 || p.N % bn != 0) {
+    if (bn == kBlockNStream) {
+        return gemm_stream_sm100(dtype, A, lda, W, p, epi, stream);
+    }
+    if (bn <= 0 || p.N % bn != 0) {
         return cudaErrorInvalidValue;
     }
     if (epi != kEpiSubpel && p.bias == nullptr) {
@@ -652,12 +691,17 @@ cudaError_t gemm_sm100(int dtype, const void* A, int lda, const void* W, const G
                               p.M % p.sub_w != 0)) {
         return cudaErrorInvalidValue;
     }
+    // operands: 16-bit, or E4M3 bytes (staged as unsigned bytes); outputs/residuals: FP16, or
+    // BF16 for the BF16 and FP8 forms
     const CUtensorMapDataType dt =
         dtype == 0 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+    const CUtensorMapDataType dop = f8 ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : dt;
+    const int esz = f8 ? 1 : 2;
+    const int kbox = f8 ? 128 : kBK;
     Maps m;
     std::memset(&m, 0, sizeof(m));
-    if (!make_tmap_2d(&m.a, dt, A, p.K, p.M, static_cast<uint64_t>(lda) * 2, kBK, kBM, 128) ||
-        !make_tmap_2d(&m.b, dt, W, p.K, p.N, static_cast<uint64_t>(p.K) * 2, kBK, bn, 128)) {
+    if (!make_tmap_2d(&m.a, dop, A, p.K, p.M, static_cast<uint64_t>(lda) * esz, kbox, kBM, 128) ||
+        !make_tmap_2d(&m.b, dop, W, p.K, p.N, static_cast<uint64_t>(p.K) * esz, kbox, bn, 128)) {
         return cudaErrorInvalidValue;
     }
     if (epi != kEpiSubpel) {
@@ -677,7 +721,12 @@ cudaError_t gemm_sm100(int dtype, const void* A, int lda, const void* W, const G
             return cudaErrorInvalidValue;
         }
     }
-    if (dtype == 0) {
+    if (f8) {
+        switch (bn) {
+        case 256: return dispatch_epi_f8<256>(epi, m, p, stream);
+        case 128: return dispatch_epi_f8<128>(epi, m, p, stream);
+        }
+    } else if (dtype == 0) {
         switch (bn) {
         case 256: return dispatch_epi<__half, 256>(epi, m, p, stream);
         case 128: return dispatch_epi<__half, 128>(epi, m, p, stream);

@@ -29,6 +29,10 @@ enum GemmEpilogue : int {
     kEpiBiasQ = 7,        // out = (acc + b) * q[n]
 };
 
+// block_n value selecting the streaming form of the residual epilogues (gemm_stream_sm100.cu):
+// 128-wide channel slices with W resident in shared memory, contiguous row ranges per CTA.
+constexpr int kBlockNStream = -1;
+
 struct GemmParams {
     int M, N, K;
     const float* bias;   // [N] fp32 (may be null for kEpiSubpel)
@@ -42,6 +46,18 @@ struct GemmParams {
     int sub_w;           // kEpiSubpel: width of the input grid (rows are h * sub_w + w)
     int sub_cout;        // kEpiSubpel: output channels per sub-pixel position
     int* err;            // device error word
+    // FP8 form (dtype 2): per-output-channel FP32 factor applied to the accumulator before the
+    // bias, the product of the weight row's and the activation's quantisation scales
+    const float* wscale = nullptr;
 };
+
+// dtype of gemm_sm100 / dcvc_conv1x1 for E4M3 operands with FP32 accumulation and BF16 output.
+constexpr int kDtypeF8 = 2;
+
+// The streaming form: residual epilogues (kEpiBiasRes, kEpiBiasResQ) with K <= 256 and N a
+// multiple of 128.  Bitwise the same outputs as gemm_sm100 at any tile width.
+bool gemm_stream_eligible(int epi, int M, int N, int K);
+cudaError_t gemm_stream_sm100(int dtype, const void* A, int lda, const void* W, const GemmParams& p,
+                              int epi, cudaStream_t stream);
 
 }  // namespace dcvc

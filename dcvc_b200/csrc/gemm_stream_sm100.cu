@@ -1,0 +1,480 @@
+// Streaming form of the residual 1x1-conv GEMMs for sm_100a (conv1x1_bias_shortcut and
+// conv1x1_bias_shortcut_with_quant; def_cutlass.h:10-34), for K <= 256.
+//
+// At K = 256 these GEMMs are bound by HBM: per output pixel they read 2*K bytes of A, 2*N of
+// residual and write 2*N, against N*K MACs.  The tiled persistent kernel (gemm_sm100.cu) streams
+// A and W through the same operand ring and re-reads W for every tile, and its residual ring is
+// one tile deep, so a tile's epilogue waits a full memory latency for its residual.  This form
+// is laid out for streaming instead:
+//   * every CTA owns one 128-wide slice of the output channels and a contiguous range of rows
+//     (a multiple of 32 rows, balanced over the CTAs of its slice), so all CTAs move the same
+//     number of bytes; the last 128-row tile of a range may be partial (its extra rows are
+//     computed and never stored);
+//   * the CTA's W slice (128 x K) is loaded once and stays in shared memory, so the operand ring
+//     carries only A (16 KB per stage, six stages);
+//   * sixteen epilogue warps (four per TMEM lane quadrant, 32 columns each) keep a two-tile-deep
+//     ring of residual boxes in flight, so a tile's residual lands while earlier tiles compute;
+//   * the result is written over the residual in its slot and stored by TMA.
+// One thread issues tcgen05.mma (M = 128, N = 128, K = 16) into a double-buffered FP32 TMEM
+// accumulator.  Per output element the products are summed in the same order as in the tiled
+// kernel and the epilogue applies bias, residual(s) and x q in the same order, so the outputs
+// are bitwise those of gemm_sm100 at any tile width.
+#include "gemm_sm100.cuh"
+#include "host_util.h"
+
+#include <cstring>
+#include <mutex>
+
+namespace dcvc {
+
+namespace {
+
+constexpr int kSBM = 128;                   // rows per MMA tile
+constexpr int kSBN = 128;                   // output channels per CTA
+constexpr int kSBK = 64;                    // one 128-byte swizzle atom of 16-bit elements
+constexpr int kSMaxK = 256;                 // W slice resident: 128 x 256 x 2 B = 64 KB
+constexpr int kSEpiWarps = 16;
+constexpr int kSThreads = 64 + 32 * kSEpiWarps;
+constexpr int kSCols = kSBN / 4;            // accumulator columns per epilogue warp (32)
+constexpr int kSBoxBytes = 32 * kSCols * 2; // 32 rows x 32 columns of 16-bit values: 2 KB
+constexpr int kSResSlots = 2;               // residual ring depth per warp, in tiles
+constexpr int kSStages = 6;
+constexpr int kSABytes = kSBM * kSBK * 2;   // 16 KB
+constexpr long long kSWaitLimit = 2000000000LL;  // ~1 s at 2 GHz; a correct kernel never waits this long
+
+template <int EPI>
+struct StreamCfg {
+    static constexpr int kSlotBytes = kSBoxBytes;
+    static constexpr int kBOffset = 0;                                   // resident W slice
+    static constexpr int kBBytes = kSBN * kSMaxK * 2;                    // 64 KB
+    static constexpr int kAOffset = kBOffset + kBBytes;
+    static constexpr int kEpiOffset = kAOffset + kSStages * kSABytes;    // 96 KB of A stages
+    static constexpr int kEpiBytes = kSEpiWarps * kSResSlots * kSlotBytes;
+    static constexpr int kBarOffset = kEpiOffset + kEpiBytes;
+    static constexpr int kBarBytes = 512;
+    static constexpr int kBytes = kBarOffset + kBarBytes + 1024;
+    static_assert(kBytes <= 232448, "shared memory budget exceeded");
+};
+
+template <typename T>
+struct SPack2;
+template <>
+struct SPack2<__half> {
+    static __device__ __forceinline__ uint32_t pack(float a, float b)
+    {
+        __half2 h = __floats2half2_rn(a, b);
+        return *reinterpret_cast<uint32_t*>(&h);
+    }
+    static __device__ __forceinline__ float2 unpack(uint32_t u)
+    {
+        __half2 h = *reinterpret_cast<__half2*>(&u);
+        return __half22float2(h);
+    }
+    static constexpr int kFormat = 0;
+};
+template <>
+struct SPack2<__nv_bfloat16> {
+    static __device__ __forceinline__ uint32_t pack(float a, float b)
+    {
+        __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+        return *reinterpret_cast<uint32_t*>(&h);
+    }
+    static __device__ __forceinline__ float2 unpack(uint32_t u)
+    {
+        __nv_bfloat162 h = *reinterpret_cast<__nv_bfloat162*>(&u);
+        return __bfloat1622float2(h);
+    }
+    static constexpr int kFormat = 1;
+};
+
+// Byte offset of 16-byte chunk j (0..3) of row r in a 64-byte-row box written with SWIZZLE_64B.
+__device__ __forceinline__ int sw64_off(int r, int j) { return r * 64 + ((j ^ ((r >> 1) & 3)) << 4); }
+
+// Rows [r0, r1) of the CTA `idx` of `G` CTAs sharing one channel slice: 32-row groups split as
+// evenly as possible.
+__device__ __forceinline__ void cta_rows(int M, int idx, int G, int* r0, int* r1)
+{
+    const int groups = (M + 31) / 32;
+    const int g0 = static_cast<int>((static_cast<long long>(groups) * idx) / G);
+    const int g1 = static_cast<int>((static_cast<long long>(groups) * (idx + 1)) / G);
+    *r0 = g0 * 32;
+    *r1 = g1 * 32 < M ? g1 * 32 : M;
+}
+
+template <typename T, int EPI>
+__global__ void __launch_bounds__(kSThreads, 1)
+    gemm_stream_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                       const __grid_constant__ CUtensorMap tmO, const __grid_constant__ CUtensorMap tmR,
+                       const GemmParams p, int ctas_per_slice)
+{
+    using C = StreamCfg<EPI>;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem =
+        reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + C::kBarOffset);
+    uint64_t* empty = full + kSStages;
+    uint64_t* bfull = empty + kSStages;
+    uint64_t* tfull = bfull + 1;
+    uint64_t* tempty = tfull + 2;
+    uint64_t* drain = tempty + 2;
+    uint64_t* resbar = drain + 1;  // [kSEpiWarps][kSResSlots]
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(resbar + kSEpiWarps * kSResSlots);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int slice = blockIdx.x / ctas_per_slice;
+    const int n0 = slice * kSBN;
+    int r0, r1;
+    cta_rows(p.M, blockIdx.x % ctas_per_slice, ctas_per_slice, &r0, &r1);
+    const int ntiles = r1 > r0 ? (r1 - r0 + kSBM - 1) / kSBM : 0;
+    const int kblocks = p.K / kSBK;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kSStages; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(bfull, 1);
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&tfull[b], 1);
+            mbar_init(&tempty[b], kSEpiWarps);
+        }
+        mbar_init(drain, 1);
+        for (int w = 0; w < kSEpiWarps * kSResSlots; ++w) {
+            mbar_init(&resbar[w], 1);
+        }
+        *abort_flag = 0;
+        fence_mbar_init();
+    }
+    if (warp == 0 && lane == 0) {
+        tma_prefetch_desc(&tmA);
+        tma_prefetch_desc(&tmB);
+    }
+    if (warp == 1) {
+        tmem_alloc(tmem_slot, 2 * kSBN);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+    griddep_launch_dependents();
+    griddep_wait();
+
+    if (warp == 0) {
+        // ------------------------------------------------------------ TMA producer
+        if (lane == 0 && ntiles > 0) {
+            // the W slice once: kblocks boxes of 128 rows x 64 K
+            mbar_arrive_expect_tx(bfull, static_cast<uint32_t>(kblocks * kSBN * kSBK * 2));
+            for (int kb = 0; kb < kblocks; ++kb) {
+                tma_load_2d(smem + C::kBOffset + kb * kSBN * 128, &tmB, bfull, kb * kSBK, n0);
+            }
+            int stage = 0;
+            uint32_t phase = 0;
+            int issued = 0;
+            for (int t = 0; t < ntiles && !*abort_flag; ++t) {
+                const int m0 = r0 + t * kSBM;
+                for (int kb = 0; kb < kblocks; ++kb) {
+                    if (!mbar_wait_bounded(&empty[stage], phase ^ 1, kSWaitLimit)) {
+                        *abort_flag = 1;
+                        report_error(p.err, kErrGemmProducerTimeout);
+                        break;
+                    }
+                    mbar_arrive_expect_tx(&full[stage], kSABytes);
+                    tma_load_2d(smem + C::kAOffset + stage * kSABytes, &tmA, &full[stage], kb * kSBK, m0);
+                    ++issued;
+                    if (++stage == kSStages) {
+                        stage = 0;
+                        phase ^= 1;
+                    }
+                }
+            }
+            if (*abort_flag) {
+                // let this thread's copies land before the CTA winds down
+                mbar_wait_bounded(bfull, 0, kSWaitLimit / 16);
+                int n = issued < kSStages ? issued : kSStages;
+                for (int i = 0; i < n; ++i) {
+                    if (--stage < 0) {
+                        stage = kSStages - 1;
+                        phase ^= 1;
+                    }
+                    mbar_wait_bounded(&full[stage], phase, kSWaitLimit / 16);
+                }
+            }
+        }
+    } else if (warp == 1) {
+        // ------------------------------------------------------------ MMA issuer
+        if (lane == 0 && ntiles > 0) {
+            const uint32_t idesc = make_idesc_f16(kSBM, kSBN, SPack2<T>::kFormat);
+            int stage = 0;
+            uint32_t phase = 0;
+            int acc = 0;
+            uint32_t acc_phase = 0;
+            bool issued_any = false;
+            if (!mbar_wait_bounded(bfull, 0, kSWaitLimit)) {
+                *abort_flag = 1;
+                report_error(p.err, kErrGemmMmaTimeout);
+            }
+            tc_fence_after();
+            for (int t = 0; t < ntiles && !*abort_flag; ++t) {
+                if (!mbar_wait_bounded(&tempty[acc], acc_phase ^ 1, kSWaitLimit)) {
+                    *abort_flag = 1;
+                    report_error(p.err, kErrGemmMmaTimeout);
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t d = tmem_base + static_cast<uint32_t>(acc * kSBN);
+                for (int kb = 0; kb < kblocks; ++kb) {
+                    if (!mbar_wait_bounded(&full[stage], phase, kSWaitLimit)) {
+                        *abort_flag = 1;
+                        report_error(p.err, kErrGemmMmaTimeout);
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint64_t adesc =
+                        make_sw128_kmajor_desc(smem_u32(smem + C::kAOffset + stage * kSABytes));
+                    const uint64_t bdesc =
+                        make_sw128_kmajor_desc(smem_u32(smem + C::kBOffset + kb * kSBN * 128));
+#pragma unroll
+                    for (int k = 0; k < kSBK / 16; ++k) {
+                        tc_mma_f16(d, adesc + 2 * k, bdesc + 2 * k, idesc, (kb | k) != 0 ? 1u : 0u);
+                    }
+                    issued_any = true;
+                    tc_commit(&empty[stage]);
+                    if (++stage == kSStages) {
+                        stage = 0;
+                        phase ^= 1;
+                    }
+                }
+                if (*abort_flag) {
+                    break;
+                }
+                tc_commit(&tfull[acc]);
+                acc ^= 1;
+                if (acc == 0) {
+                    acc_phase ^= 1;
+                }
+            }
+            if (*abort_flag && issued_any) {
+                tc_commit(drain);
+                mbar_wait_bounded(drain, 0, kSWaitLimit / 16);
+            }
+        }
+    } else {
+        // ------------------------------------------------------------ epilogue warps
+        using P = SPack2<T>;
+        const int ew = warp - 2;
+        const int quad = warp & 3;        // TMEM lane quadrant this warp may access
+        const int part = ew >> 2;         // which 32 of the CTA's 128 columns
+        const int ncol = n0 + part * kSCols;
+        uint8_t* wbuf = smem + C::kEpiOffset + ew * kSResSlots * C::kSlotBytes;
+        uint64_t* rbar = &resbar[ew * kSResSlots];
+        uint32_t res_phase = 0;
+        uint32_t res_pending = 0;
+        if (lane == 0) {
+            tma_prefetch_desc(&tmO);
+            tma_prefetch_desc(&tmR);
+        }
+        // residual box of this warp for tile t into slot s (rows past the range: nothing)
+        auto issue_res = [&](int t, int s) {
+            if (t >= ntiles) {
+                return;
+            }
+            const int row0 = r0 + t * kSBM + quad * 32;
+            if (row0 >= r1) {
+                return;
+            }
+            mbar_arrive_expect_tx(&rbar[s], kSBoxBytes);
+            tma_load_2d(wbuf + s * C::kSlotBytes, &tmR, &rbar[s], ncol, row0);
+            res_pending |= 1u << s;
+        };
+        if (lane == 0) {
+            for (int s = 0; s < kSResSlots; ++s) {
+                issue_res(s, s);
+            }
+        }
+        // the bias of this warp's 32 columns, fixed for the whole range
+        float4 bb[8];
+        {
+            const float4* b4 = reinterpret_cast<const float4*>(p.bias + ncol);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                bb[j] = __ldg(b4 + j);
+            }
+        }
+        int acc = 0;
+        uint32_t acc_phase = 0;
+        for (int t = 0; t < ntiles && !*abort_flag; ++t) {
+            const int slot = t % kSResSlots;
+            const int row0 = r0 + t * kSBM + quad * 32;
+            const bool rows_live = row0 < r1;
+            uint8_t* buf = wbuf + slot * C::kSlotBytes;
+            if (!mbar_wait_bounded(&tfull[acc], acc_phase, kSWaitLimit)) {
+                *abort_flag = 1;
+                report_error(p.err, kErrGemmEpilogueTimeout);
+                break;
+            }
+            tc_fence_after();
+            if (rows_live) {
+                if (!mbar_wait_bounded(&rbar[slot], (res_phase >> slot) & 1u, kSWaitLimit)) {
+                    *abort_flag = 1;
+                    report_error(p.err, kErrGemmEpilogueTimeout);
+                } else {
+                    res_pending &= ~(1u << slot);
+                }
+                res_phase ^= 1u << slot;
+            }
+            uint32_t r[32];
+            tmem_ld_32x32b_x32(tmem_base + (static_cast<uint32_t>(quad * 32) << 16) + acc * kSBN +
+                                   part * kSCols,
+                               r);
+            tc_wait_ld();
+            // the accumulator buffer is free once its columns are in registers
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) {
+                mbar_arrive(&tempty[acc]);
+            }
+            acc ^= 1;
+            if (acc == 0) {
+                acc_phase ^= 1;
+            }
+            if (rows_live && !*abort_flag) {
+                float2 v[16];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    v[2 * j] = __fadd2_rn(make_float2(__uint_as_float(r[4 * j + 0]), __uint_as_float(r[4 * j + 1])),
+                                          make_float2(bb[j].x, bb[j].y));
+                    v[2 * j + 1] = __fadd2_rn(make_float2(__uint_as_float(r[4 * j + 2]), __uint_as_float(r[4 * j + 3])),
+                                              make_float2(bb[j].z, bb[j].w));
+                }
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const uint4 u = *reinterpret_cast<const uint4*>(buf + sw64_off(lane, j));
+                    v[4 * j + 0] = __fadd2_rn(v[4 * j + 0], P::unpack(u.x));
+                    v[4 * j + 1] = __fadd2_rn(v[4 * j + 1], P::unpack(u.y));
+                    v[4 * j + 2] = __fadd2_rn(v[4 * j + 2], P::unpack(u.z));
+                    v[4 * j + 3] = __fadd2_rn(v[4 * j + 3], P::unpack(u.w));
+                }
+                if constexpr (EPI == kEpiBiasResQ) {
+                    const uint4* qs = reinterpret_cast<const uint4*>(reinterpret_cast<const T*>(p.qscale) + ncol);
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const uint4 u = __ldg(qs + j);
+                        v[4 * j + 0] = __fmul2_rn(v[4 * j + 0], P::unpack(u.x));
+                        v[4 * j + 1] = __fmul2_rn(v[4 * j + 1], P::unpack(u.y));
+                        v[4 * j + 2] = __fmul2_rn(v[4 * j + 2], P::unpack(u.z));
+                        v[4 * j + 3] = __fmul2_rn(v[4 * j + 3], P::unpack(u.w));
+                    }
+                }
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    *reinterpret_cast<uint4*>(buf + sw64_off(lane, j)) =
+                        make_uint4(P::pack(v[4 * j + 0].x, v[4 * j + 0].y), P::pack(v[4 * j + 1].x, v[4 * j + 1].y),
+                                   P::pack(v[4 * j + 2].x, v[4 * j + 2].y), P::pack(v[4 * j + 3].x, v[4 * j + 3].y));
+                }
+                fence_proxy_async_smem();
+            }
+            __syncwarp();
+            if (lane == 0) {
+                if (rows_live && !*abort_flag) {
+                    tma_store_2d(&tmO, buf, ncol, row0);
+                    bulk_commit();
+                }
+                if (!*abort_flag) {
+                    bulk_wait_read0();  // the store has read the slot: refill it
+                    issue_res(t + kSResSlots, slot);
+                }
+            }
+            __syncwarp();
+        }
+        if (lane == 0) {
+            // after an abort, let this warp's residual loads land before the CTA winds down
+            for (int s = 0; s < kSResSlots; ++s) {
+                if (res_pending & (1u << s)) {
+                    mbar_wait_bounded(&rbar[s], (res_phase >> s) & 1u, kSWaitLimit / 16);
+                }
+            }
+            bulk_wait_read0();
+        }
+        __syncwarp();
+    }
+
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc(tmem_base, 2 * kSBN);
+    }
+}
+
+template <typename T, int EPI>
+cudaError_t launch_stream(const CUtensorMap* maps, const GemmParams& p, cudaStream_t stream)
+{
+    using C = StreamCfg<EPI>;
+    auto kernel = gemm_stream_kernel<T, EPI>;
+    static std::once_flag once;
+    static cudaError_t attr_err = cudaSuccess;
+    std::call_once(once, [&] {
+        attr_err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, C::kBytes);
+    });
+    if (attr_err != cudaSuccess) {
+        return attr_err;
+    }
+    const int slices = p.N / kSBN;
+    // CTAs per channel slice: the SMs shared out, but no more than one per 32-row group
+    int per = num_sms() / slices;
+    const int groups = (p.M + 31) / 32;
+    per = per < groups ? per : groups;
+    per = per < 1 ? 1 : per;
+    return launch_pdl(kernel, dim3(slices * per), dim3(kSThreads), C::kBytes, stream, maps[0], maps[1],
+                      maps[2], maps[3], p, per);
+}
+
+}  // namespace
+
+bool gemm_stream_eligible(int epi, int M, int N, int K)
+{
+    return (epi == kEpiBiasRes || epi == kEpiBiasResQ) && M > 0 &&
+           N % kSBN == 0 && K % kSBK == 0 && K <= kSMaxK && N / kSBN <= num_sms();
+}
+
+// Host launcher of the streaming form; same operands and checks as gemm_sm100 (A [M, K] with
+// pitch lda, W [N, K] dense, outputs/residuals with their pitches).
+cudaError_t gemm_stream_sm100(int dtype, const void* A, int lda, const void* W, const GemmParams& p,
+                              int epi, cudaStream_t stream)
+{
+    if (!gemm_stream_eligible(epi, p.M, p.N, p.K) || lda % 8 != 0 || p.ldo % 8 != 0 ||
+        (reinterpret_cast<uintptr_t>(A) & 15) != 0 || (reinterpret_cast<uintptr_t>(W) & 15) != 0 ||
+        (reinterpret_cast<uintptr_t>(p.out) & 15) != 0 || p.bias == nullptr || p.res == nullptr ||
+        p.ldr % 8 != 0 || (reinterpret_cast<uintptr_t>(p.res) & 15) != 0) {
+        return cudaErrorInvalidValue;
+    }
+    if (epi == kEpiBiasResQ && p.qscale == nullptr) {
+        return cudaErrorInvalidValue;
+    }
+    const CUtensorMapDataType dt = dtype == 0 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+    CUtensorMap maps[4];
+    std::memset(maps, 0, sizeof(maps));
+    if (!make_tmap_2d(&maps[0], dt, A, p.K, p.M, static_cast<uint64_t>(lda) * 2, kSBK, kSBM, 128) ||
+        !make_tmap_2d(&maps[1], dt, W, p.K, p.N, static_cast<uint64_t>(p.K) * 2, kSBK, kSBN, 128) ||
+        !make_tmap_2d(&maps[2], dt, p.out, p.N, p.M, static_cast<uint64_t>(p.ldo) * 2, kSCols, 32, 64) ||
+        !make_tmap_2d(&maps[3], dt, p.res, p.N, p.M, static_cast<uint64_t>(p.ldr) * 2, kSCols, 32, 64)) {
+        return cudaErrorInvalidValue;
+    }
+    if (dtype == 0) {
+        switch (epi) {
+        case kEpiBiasRes: return launch_stream<__half, kEpiBiasRes>(maps, p, stream);
+        case kEpiBiasResQ: return launch_stream<__half, kEpiBiasResQ>(maps, p, stream);
+        }
+    } else {
+        switch (epi) {
+        case kEpiBiasRes: return launch_stream<__nv_bfloat16, kEpiBiasRes>(maps, p, stream);
+        case kEpiBiasResQ: return launch_stream<__nv_bfloat16, kEpiBiasResQ>(maps, p, stream);
+        }
+    }
+    return cudaErrorInvalidValue;
+}
+
+}  // namespace dcvc

@@ -32,13 +32,26 @@ cudaError_t gemm_sm100(int dtype, const void* A, int lda, const void* W, const G
 
 namespace {
 
+// A tuned width belongs to one device: a process that runs codecs on several GPUs (one chunk
+// server per device) tunes and looks up per device ordinal.
 struct TuneKey {
-    int dtype, epi, M, N, K, sub_w;
+    int dev, dtype, epi, M, N, K, sub_w;
     bool operator<(const TuneKey& o) const
     {
-        return std::tie(dtype, epi, M, N, K, sub_w) < std::tie(o.dtype, o.epi, o.M, o.N, o.K, o.sub_w);
+        return std::tie(dev, dtype, epi, M, N, K, sub_w) <
+               std::tie(o.dev, o.dtype, o.epi, o.M, o.N, o.K, o.sub_w);
     }
 };
+
+int current_device()
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return -1;
+    }
+    return dev;
+}
 
 struct TuneEntry {
     int bn;
@@ -97,8 +110,9 @@ int gemm_tuned_bn(int dtype, int epi, int M, int N, int K, int sub_w)
     if (g_tuned_count.load(std::memory_order_acquire) == 0) {
         return 0;
     }
+    const int dev = current_device();
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    auto it = g_tuned.find(TuneKey{dtype, epi, M, N, K, sub_w});
+    auto it = g_tuned.find(TuneKey{dev, dtype, epi, M, N, K, sub_w});
     return it == g_tuned.end() ? 0 : it->second.bn;
 }
 
@@ -128,7 +142,7 @@ cudaError_t gemm_autotune(int dtype, int epi, const GemmParams& shape, cudaStrea
     if (M <= 0 || N <= 0 || K <= 0) {
         return cudaErrorInvalidValue;
     }
-    int cands[3];
+    int cands[4];
     int nc = 0;
     for (int bn : {256, 128, 64}) {
         if (N % bn != 0 || (epi == kEpiQuad && bn != 256) ||
@@ -136,6 +150,9 @@ cudaError_t gemm_autotune(int dtype, int epi, const GemmParams& shape, cudaStrea
             continue;
         }
         cands[nc++] = bn;
+    }
+    if (gemm_stream_eligible(epi, M, N, K)) {
+        cands[nc++] = kBlockNStream;  // the streaming form of the residual epilogues
     }
     if (nc == 0) {
         return cudaErrorInvalidValue;
@@ -223,7 +240,8 @@ cudaError_t gemm_autotune(int dtype, int epi, const GemmParams& shape, cudaStrea
     }
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
-        g_tuned[TuneKey{dtype, epi, M, N, K, epi == kEpiSubpel ? shape.sub_w : 0}] = TuneEntry{best, best_t};
+        g_tuned[TuneKey{current_device(), dtype, epi, M, N, K, epi == kEpiSubpel ? shape.sub_w : 0}] =
+            TuneEntry{best, best_t};
         g_tuned_count.store(g_tuned.size(), std::memory_order_release);
     }
     if (best_bn != nullptr) {

@@ -65,7 +65,10 @@ bool make_tmap_2d(CUtensorMap* map, CUtensorMapDataType dtype, const void* base,
     case 0: sw = CU_TENSOR_MAP_SWIZZLE_NONE; break;
     default: return false;
     }
-    if (box_inner * 2 > static_cast<uint32_t>(swizzle_bytes == 0 ? 256 : swizzle_bytes)) {
+    const uint32_t esz = dtype == CU_TENSOR_MAP_DATA_TYPE_UINT8 ? 1u
+                         : (dtype == CU_TENSOR_MAP_DATA_TYPE_FLOAT32 || dtype == CU_TENSOR_MAP_DATA_TYPE_INT32) ? 4u
+                                                                                                              : 2u;
+    if (box_inner * esz > static_cast<uint32_t>(swizzle_bytes == 0 ? 256 : swizzle_bytes)) {
         return false;  // the inner box extent must fit the swizzle span
     }
     cuuint64_t dims[2] = {inner, outer};

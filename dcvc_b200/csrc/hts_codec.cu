@@ -58,6 +58,16 @@ HtsCodec::~HtsCodec()
 
 void HtsCodec::clear_graphs() { graphs_.clear(); }
 
+int HtsCodec::set_precision(int precision)
+{
+    if (precision != kPrecisionF16 && precision != kPrecisionBF16 && precision != kPrecisionFP8) {
+        set_last_error("set_precision: precision must be 0 (FP16), 1 (BF16) or 2 (FP8)");
+        return kInvalidArgument;
+    }
+    precision_ = precision;
+    return kOk;
+}
+
 int HtsCodec::set_param(const StateDict& sd, float skip_threshold)
 {
     if (main_ != nullptr) {
@@ -67,18 +77,27 @@ int HtsCodec::set_param(const StateDict& sd, float skip_threshold)
     ready_ = false;
     weights_.clear();
     ParamBuilder B(sd, weights_);
+    // the analysis / synthesis transforms in the precision form's format, the entropy-parameter
+    // path in FP16; q_encoder / q_decoder scale outputs of the transforms, q_feature the input
+    // of the temporal prior
+    const int act = precision_ == kPrecisionF16 ? 0 : 1;
+    const bool f8 = precision_ == kPrecisionFP8;
+    act_ = act;
+    fp8_ = f8;
     int r = 0, c = 0;
-    q_enc_tab_ = B.half_rows("q_encoder", &r, &c);
+    q_enc_tab_ = act ? B.bf16_rows("q_encoder", &r, &c) : B.half_rows("q_encoder", &r, &c);
     if (B.ok() && (r != kQpNum || c != kChD)) {
         set_last_error("set_param: q_encoder must be [64, 512]");
         return kInvalidArgument;
     }
-    q_dec_tab_ = B.half_rows("q_decoder", &r, &c);
+    q_dec_tab_ = act ? B.bf16_rows("q_decoder", &r, &c) : B.half_rows("q_decoder", &r, &c);
     q_feat_tab_ = B.half_rows("q_feature", &r, &c);
+    B.set_dtype(act, f8);
     for (int i = 0; i < 6; ++i) {
         encoder_[i] = B.dcb(num("encoder.conv1.", i));
     }
     enc_down_ = B.conv3x3s2("encoder.down.");
+    B.set_dtype(0);
     hyper_enc0_ = B.dcb("hyper_encoder.conv.0.");
     hyper_enc1_ = B.down("hyper_encoder.conv.1.");
     hyper_enc2_ = B.down("hyper_encoder.conv.2.");
@@ -94,6 +113,7 @@ int HtsCodec::set_param(const StateDict& sd, float skip_threshold)
     prior_fusion_out_ = B.lin("y_prior_fusion.conv.3.");
     reduction_ = B.lin("y_spatial_prior_reduction.");
     spatial_prior_out_ = B.lin("y_spatial_prior.conv.3.");
+    B.set_dtype(act, f8);
     dec_up_lin_ = B.subpel("decoder.up.");
     for (int i = 0; i < 7; ++i) {
         decoder_[i] = B.dcb(num("decoder.conv1.", i));
@@ -114,6 +134,7 @@ int HtsCodec::set_param(const StateDict& sd, float skip_threshold)
         }
         rh_head_[i] = B.lin(num("recon_head.conv2.", i, ".3."));
     }
+    B.set_dtype(0);
     if (!B.ok()) {
         set_last_error("set_param: " + B.error());
         weights_.clear();
@@ -139,12 +160,12 @@ int HtsCodec::set_param(const StateDict& sd, float skip_threshold)
         weights_.clear();
         return kInvalidArgument;
     }
-    std::vector<uint8_t> lut(65536);
-    scale_index_table(lut.data());
+    // the scale -> CDF index table, evaluated on the device as the reference's FP16
+    // scale_to_index computes it
     scale_lut_ = weights_.alloc_n<uint8_t>(65536);
-    if (scale_lut_ == nullptr ||
-        cudaMemcpy(scale_lut_, lut.data(), 65536, cudaMemcpyHostToDevice) != cudaSuccess) {
-        set_last_error("set_param: could not upload the scale-index table");
+    if (scale_lut_ == nullptr || scale_index_table_device(scale_lut_, 0) != cudaSuccess ||
+        cudaStreamSynchronize(0) != cudaSuccess) {
+        set_last_error("set_param: could not build the scale-index table");
         return kOutOfMemory;
     }
     skip_threshold_ = skip_threshold;
@@ -229,6 +250,8 @@ int HtsCodec::allocate(int Hp, int Wp)
     lvl32_a_ = H(M32 * kChY);
     lvl64_a_ = H(M64 * kChZ);
     head_ = H(M8 * kChSrcIntra);
+    y_act_ = act_ ? H(M16 * kChY) : nullptr;
+    yhat_act_ = act_ ? H(M16 * kChY) : nullptr;
     q_enc_ = H(kChD);
     q_dec_ = H(kChD);
     q_feat_ = H(kChD);
@@ -241,6 +264,8 @@ int HtsCodec::allocate(int Hp, int Wp)
     scratch_.t2 = H(S);
     scratch_.t3 = H(S);
     scratch_.t4 = H(S);
+    scratch_.t5 = fp8_ ? acts_.alloc_n<uint8_t>(M8 * kChD) : nullptr;
+    ok = ok && (!fp8_ || scratch_.t5 != nullptr);
     z_i8_ = acts_.alloc_n<int8_t>(z_num_);
     sym_ = acts_.alloc_n<int16_t>(y_num_);
     sym_c_ = acts_.alloc_n<int16_t>(y_num_);
@@ -327,7 +352,7 @@ void HtsCodec::feature_extractor(Launch& L)
 void HtsCodec::temporal_prior(Launch& L)
 {
     // temporal_params = RBWS2(memory * q_feature) -> cat_pf[256:768]
-    L.note(launch_mul_channel(cat_fam_, M8_, kChM, 1024, q_feat_, temporal_in_, kChM, L.s));
+    L.note(launch_mul_channel(cat_fam_, M8_, kChM, 1024, q_feat_, temporal_in_, kChM, L.s, act_));
     L.note(launch_space_to_depth2(temporal_in_, H8_, W8_, kChM, kChM, s2d_, L.s));
     gemm(L, temporal_.down, kEpiBias, s2d_, 4 * kChM, M16_, lvl16_a_, 2 * kChY);
     run_dcb(L, temporal_.dcb, lvl16_a_, 2 * kChY, H16_, W16_, cat_pf_ + kChY, 3 * kChY, scratch_);
@@ -370,8 +395,15 @@ void HtsCodec::spatial_prior(Launch& L, int k)
 void HtsCodec::decoder(Launch& L)
 {
     // up: y_hat (cat_spa[0:256]) -> cat_enc[1024:1536]; DCBs on cat_enc[1024:2048]
-    gemm(L, dec_up_lin_, kEpiSubpel, cat_spa_, 2 * kChY, M16_, cat_enc_ + 1024, 2048, nullptr, 0,
-         nullptr, W16_);
+    const __half* yh = cat_spa_;
+    int ldyh = 2 * kChY;
+    if (act_) {  // the BF16 form: y_hat (FP16, exact symbols + means) converted once
+        L.note(launch_convert(cat_spa_, 0, 2 * kChY, yhat_act_, 1, kChY, M16_, kChY, L.s));
+        yh = yhat_act_;
+        ldyh = kChY;
+    }
+    gemm(L, dec_up_lin_, kEpiSubpel, yh, ldyh, M16_, cat_enc_ + 1024, 2048, nullptr, 0, nullptr,
+         W16_);
     run_dcb(L, decoder_[0], cat_enc_ + 1024, 2048, H8_, W8_, lvl8_a_, kChD, scratch_);
     for (int i = 1; i < 6; ++i) {
         run_dcb(L, decoder_[i], lvl8_a_, kChD, H8_, W8_, lvl8_a_, kChD, scratch_);
@@ -393,7 +425,7 @@ void HtsCodec::recon_head(Launch& L, bool all_frames)
         __half* out = (i == kFrames - 1) ? feature_i_ : head_;
         gemm(L, rh_head_[i], kEpiBias, lvl8_a_, kChRecon, M8_, out, kChSrcIntra);
         if (all_frames) {
-            L.note(launch_shuffle8_clamp(out, H8_, W8_, 3, kChSrcIntra, x_hat_[i], L.s));
+            L.note(launch_shuffle8_clamp(out, H8_, W8_, 3, kChSrcIntra, x_hat_[i], L.s, act_));
         }
     }
 }
@@ -410,7 +442,12 @@ void HtsCodec::enc_analysis(Launch& L)
     }
     run_dcb(L, encoder_[5], lvl8_a_, kChD, H8_, W8_, lvl8_a_, kChD, scratch_, q_enc_);
     L.note(launch_im2col3x3s2(lvl8_a_, H8_, W8_, kChD, kChD, col_, L.s));
-    gemm(L, enc_down_, kEpiBias, col_, 9 * kChD, M16_, y_, kChY);
+    if (act_) {  // the BF16 form: y to FP16 for the entropy-parameter path
+        gemm(L, enc_down_, kEpiBias, col_, 9 * kChD, M16_, y_act_, kChY);
+        L.note(launch_convert(y_act_, 1, kChY, y_, 0, kChY, M16_, kChY, L.s));
+    } else {
+        gemm(L, enc_down_, kEpiBias, col_, 9 * kChD, M16_, y_, kChY);
+    }
     if (y_pad_ != y_) {
         L.note(launch_replicate_pad(y_, H16_, W16_, kChY, kChY, H16p_ - H16_, W16p_ - W16_, y_pad_, L.s));
     }
@@ -528,7 +565,7 @@ int HtsCodec::run_phase(int slot, cudaStream_t s)
 }
 
 int HtsCodec::buffer(const std::string& name, const void** ptr, int* rows, int* cols,
-                     int* ld) const
+                     int* ld, int* dtype) const
 {
     if (Hp_ == 0) {
         set_last_error("buffer: no resolution allocated yet");
@@ -537,16 +574,16 @@ int HtsCodec::buffer(const std::string& name, const void** ptr, int* rows, int* 
     struct Entry {
         const char* n;
         const __half* p;
-        int rows, cols, ld;
+        int rows, cols, ld, dtype;
     };
     const Entry e[] = {
-        {"y_hat", cat_spa_, M16_, kChY, 2 * kChY},
-        {"y_q", y_q_, M16_, kChY, kChY},
-        {"memory", cat_fam_, M8_, kChM, 1024},
-        {"feature_p", cat_fam_ + kChM, M8_, kChD, 1024},
-        {"ctx", cat_enc_ + kChSrc, M8_, kChD, 2048},
-        {"common", common_, M16_, 3 * kChY, 3 * kChY},
-        {"feature_i", feature_i_, M8_, kChSrcIntra, kChSrcIntra},
+        {"y_hat", cat_spa_, M16_, kChY, 2 * kChY, 0},
+        {"y_q", y_q_, M16_, kChY, kChY, 0},
+        {"memory", cat_fam_, M8_, kChM, 1024, act_},
+        {"feature_p", cat_fam_ + kChM, M8_, kChD, 1024, act_},
+        {"ctx", cat_enc_ + kChSrc, M8_, kChD, 2048, act_},
+        {"common", common_, M16_, 3 * kChY, 3 * kChY, 0},
+        {"feature_i", feature_i_, M8_, kChSrcIntra, kChSrcIntra, act_},
     };
     for (const Entry& x : e) {
         if (name == x.n) {
@@ -554,6 +591,9 @@ int HtsCodec::buffer(const std::string& name, const void** ptr, int* rows, int* 
             *rows = x.rows;
             *cols = x.cols;
             *ld = x.ld;
+            if (dtype != nullptr) {
+                *dtype = x.dtype;
+            }
             return kOk;
         }
     }
@@ -582,7 +622,7 @@ int HtsCodec::add_ref_feature(const __half* frame, int Hp, int Wp, bool apply_ad
     cudaEventRecord(ev_in_, caller);
     cudaStreamWaitEvent(main_, ev_in_, 0);
     Launch L{main_, err_word_};
-    L.note(launch_pad_unshuffle8(frame, Hp, Wp, 3, 3, 0, 0, feature_i_, kChSrcIntra, main_));
+    L.note(launch_pad_unshuffle8(frame, Hp, Wp, 3, 3, 0, 0, feature_i_, kChSrcIntra, main_, act_));
     if (apply_adaptor) {
         feature_adaptor_i(L, feature_i_);
         feature_extractor(L);
@@ -612,7 +652,7 @@ int HtsCodec::compress(const __half* x, int H, int W, int qp, bool reset, int pa
     cudaStreamWaitEvent(main_, ev_in_, 0);
     set_qp(qp, main_);
     Launch L{main_, err_word_};
-    L.note(launch_pad_unshuffle8(x, H, W, 24, 24, pad_b, pad_r, cat_enc_, 2048, main_));
+    L.note(launch_pad_unshuffle8(x, H, W, 24, 24, pad_b, pad_r, cat_enc_, 2048, main_, act_));
     last_kernels_ += L.kernels;
     int st = cuda_status(L.first, "compress: pad_and_unshuffle_8");
     if (st == kOk) st = run_phase(kEncAnalysis, main_);

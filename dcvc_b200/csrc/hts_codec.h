@@ -21,8 +21,21 @@ public:
     static constexpr int kChY = 256, kChZ = 128, kChD = 512, kChM = 512, kChRecon = 256;
     static constexpr int kQpNum = 64;
 
+    // Activation format of the analysis and synthesis transforms (encoder, decoder, recon head,
+    // feature adaptors and extractor): FP16 as the reference, or BF16.  The entropy-parameter
+    // path (hyper encoder / decoder, temporal prior, prior fusion, spatial prior, quantisation
+    // and indexes) runs in FP16 in every form, with the same kernels on the encoder and the
+    // decoder side, so symbols and CDF indexes round-trip exactly in both.
+    // kPrecisionFP8 is the BF16 form with the DepthConvBlocks' quad GEMMs (ffn.0, the largest
+    // GEMM of every block) on E4M3 operands with per-output-channel scales.
+    enum Precision : int { kPrecisionF16 = 0, kPrecisionBF16 = 1, kPrecisionFP8 = 2 };
+
     HtsCodec();
     ~HtsCodec();
+
+    // Selects the precision form; takes effect at the next set_param.
+    int set_precision(int precision);
+    int precision() const { return precision_; }
 
     // set_param (dmc_hts_proxy.cpp:712-762): weights + CDF tables + skip threshold.
     int set_param(const StateDict& sd, float skip_threshold);
@@ -39,8 +52,11 @@ public:
                    bool reset, cudaStream_t s, const __half** frames);
 
     // Read-only view of an internal buffer for inspection and tests: "y_hat", "y_q", "memory",
-    // "ctx", "feature_p", "common", "feature_i".  rows x cols FP16 with pitch ld.
-    int buffer(const std::string& name, const void** ptr, int* rows, int* cols, int* ld) const;
+    // "ctx", "feature_p", "common", "feature_i".  rows x cols 16-bit values with pitch ld, in the
+    // format *dtype (0 FP16, 1 BF16: "memory", "ctx", "feature_p" and "feature_i" follow the
+    // precision form, the others are FP16).
+    int buffer(const std::string& name, const void** ptr, int* rows, int* cols, int* ld,
+               int* dtype = nullptr) const;
 
     // Statistics of the last call, for reporting.
     int last_symbol_count() const { return last_count_; }
@@ -86,6 +102,9 @@ private:
     // ---------------------------------------------------------------- parameters
     DeviceArena weights_;
     bool ready_ = false;
+    int precision_ = kPrecisionF16;  // requested form
+    int act_ = 0;                    // activation format of the transforms as set up (0 / 1)
+    bool fp8_ = false;               // FP8 quad GEMMs in the transforms (as set up)
     float skip_threshold_ = 0.f;
     __half skip_thr_half_;
     const __half* q_enc_tab_ = nullptr;   // [64][512]
@@ -127,6 +146,7 @@ private:
     __half *z_ = nullptr, *z_hat_ = nullptr, *col_ = nullptr, *s2d_ = nullptr;
     __half *lvl8_a_ = nullptr, *lvl8_b_ = nullptr, *lvl16_a_ = nullptr, *lvl32_a_ = nullptr;
     __half *lvl64_a_ = nullptr, *head_ = nullptr;
+    __half *y_act_ = nullptr, *yhat_act_ = nullptr;  // y and y_hat in the BF16 form's format
     __half *q_enc_ = nullptr, *q_dec_ = nullptr, *q_feat_ = nullptr;  // active QP rows
     __half* x_hat_[kFrames] = {nullptr};
     int8_t* z_i8_ = nullptr;

@@ -124,12 +124,12 @@ int LdCodec::set_param(const StateDict& sd, float skip_threshold)
         weights_.clear();
         return kInvalidArgument;
     }
-    std::vector<uint8_t> lut(65536);
-    scale_index_table(lut.data());
+    // the scale -> CDF index table, evaluated on the device as the reference's FP16
+    // scale_to_index computes it
     scale_lut_ = weights_.alloc_n<uint8_t>(65536);
-    if (scale_lut_ == nullptr ||
-        cudaMemcpy(scale_lut_, lut.data(), 65536, cudaMemcpyHostToDevice) != cudaSuccess) {
-        set_last_error("set_param: could not upload the scale-index table");
+    if (scale_lut_ == nullptr || scale_index_table_device(scale_lut_, 0) != cudaSuccess ||
+        cudaStreamSynchronize(0) != cudaSuccess) {
+        set_last_error("set_param: could not build the scale-index table");
         return kOutOfMemory;
     }
     skip_thr_half_ = __float2half_rn(skip_threshold);

@@ -1,5 +1,9 @@
 #include "net.h"
 
+#include <cuda_fp8.h>
+
+#include <cmath>
+
 #include "elementwise.cuh"
 #include "ffn_sm100.cuh"
 #include "gemm_sm100.cuh"
@@ -64,6 +68,34 @@ const __half* ParamBuilder::upload_half(const std::vector<float>& v)
     return d;
 }
 
+const __half* ParamBuilder::upload_act(const std::vector<float>& v, int dtype)
+{
+    if (dtype == 0) {
+        return upload_half(v);
+    }
+    std::vector<__nv_bfloat16> h(v.size());
+    for (size_t i = 0; i < v.size(); ++i) {
+        h[i] = __float2bfloat16_rn(v[i]);
+    }
+    __nv_bfloat16* d = arena_.alloc_n<__nv_bfloat16>(v.size());
+    if (d == nullptr || cudaMemcpy(d, h.data(), h.size() * 2, cudaMemcpyHostToDevice) != cudaSuccess) {
+        fail("device allocation/copy of parameters failed");
+        return nullptr;
+    }
+    return reinterpret_cast<const __half*>(d);
+}
+
+const __half* ParamBuilder::bf16_rows(const std::string& name, int* rows, int* cols)
+{
+    const HostTensor* t = get(name, 2);
+    if (t == nullptr) {
+        return nullptr;
+    }
+    *rows = static_cast<int>(t->shape[0]);
+    *cols = static_cast<int>(t->numel() / t->shape[0]);
+    return upload_act(t->data, 1);
+}
+
 const float* ParamBuilder::upload_float(const std::vector<float>& v)
 {
     float* d = arena_.alloc_n<float>(v.size());
@@ -99,7 +131,8 @@ Lin ParamBuilder::lin(const std::string& prefix, bool bias)
         fail("'" + prefix + "weight' is not a 1x1 convolution");
         return l;
     }
-    l.w = upload_half(w->data);
+    l.dtype = dtype_;
+    l.w = upload_act(w->data, dtype_);
     if (bias) {
         const HostTensor* b = get(prefix + "bias");
         if (b != nullptr) {
@@ -113,6 +146,7 @@ Dcb ParamBuilder::dcb(const std::string& p, bool shortcut)
 {
     Dcb d;
     d.shortcut = shortcut;
+    d.dtype = dtype_;
     if (has(p + "adaptor.weight")) {
         d.adaptor = true;
         d.ad = lin(p + "adaptor.");
@@ -150,9 +184,38 @@ Dcb ParamBuilder::dcb(const std::string& p, bool shortcut)
     }
     d.dc2.cin = d.cdc;
     d.dc2.cout = d.C;
-    d.dc2.w = upload_half(w3->data);
+    d.dc2.dtype = dtype_;
+    d.dc2.w = upload_act(w3->data, dtype_);
     d.dc2.b = upload_float(fb);
     d.ffn1 = lin(p + "ffn.0.");
+    if (fp8_ && ok()) {
+        // E4M3 rows with per-row scales max|w| / 448 (the FP8 form's quad GEMM)
+        const HostTensor* w1 = get(p + "ffn.0.weight", 2);
+        if (w1 != nullptr) {
+            const int rows = static_cast<int>(w1->shape[0]);
+            const int cols = static_cast<int>(w1->numel() / rows);
+            std::vector<uint8_t> q(w1->data.size());
+            std::vector<float> ws(rows);
+            for (int r = 0; r < rows; ++r) {
+                float mx = 0.f;
+                for (int c = 0; c < cols; ++c) {
+                    mx = std::max(mx, std::fabs(w1->data[static_cast<size_t>(r) * cols + c]));
+                }
+                const float sc = mx > 0.f ? mx / 448.f : 1.f;
+                for (int c = 0; c < cols; ++c) {
+                    q[static_cast<size_t>(r) * cols + c] = static_cast<uint8_t>(__nv_cvt_float_to_fp8(
+                        w1->data[static_cast<size_t>(r) * cols + c] / sc, __NV_SATFINITE, __NV_E4M3));
+                }
+                ws[r] = sc * kFp8ActScale;
+            }
+            uint8_t* dq = arena_.alloc_n<uint8_t>(q.size());
+            if (dq == nullptr || cudaMemcpy(dq, q.data(), q.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+                fail("device allocation/copy of parameters failed");
+            }
+            d.ffn1_w8 = dq;
+            d.ffn1_ws = upload_float(ws);
+        }
+    }
     d.ffn2 = lin(p + "ffn.2.");
     d.cffn = d.ffn2.cin;
     d.cin = d.adaptor ? d.ad.cin : d.C;
@@ -186,7 +249,8 @@ DownBlock ParamBuilder::down(const std::string& p, bool shortcut)
     }
     b.down.cin = k4;
     b.down.cout = cout;
-    b.down.w = upload_half(pw);
+    b.down.dtype = dtype_;
+    b.down.w = upload_act(pw, dtype_);
     b.down.b = upload_float(bias->data);
     b.dcb = dcb(p + "conv.", shortcut);
     return b;
@@ -236,7 +300,8 @@ Lin ParamBuilder::subpel(const std::string& p)
     }
     b.cin = kin;
     b.cout = n4;
-    b.w = upload_half(pw);
+    b.dtype = dtype_;
+    b.w = upload_act(pw, dtype_);
     if (has(p + "conv.0.bias")) {
         const HostTensor* bias = get(p + "conv.0.bias");
         if (bias == nullptr || bias->numel() != n4) {
@@ -280,7 +345,8 @@ Lin ParamBuilder::conv3x3s2(const std::string& p)
     }
     l.cin = 9 * cin;
     l.cout = cout;
-    l.w = upload_half(pw);
+    l.dtype = dtype_;
+    l.w = upload_act(pw, dtype_);
     l.b = upload_float(b->data);
     return l;
 }
@@ -308,8 +374,8 @@ void gemm(Launch& L, const Lin& lin, int epi, const __half* x, int ldx, int M, _
     p.err = L.err_word;
     // the autotuned width of this shape (tuned here on first sight when tuning is enabled and
     // the phase runs eagerly), else the library's rule
-    const int bn = gemm_bn_for(0, epi, p, L.s);
-    L.note(gemm_sm100(0, x, ldx, lin.w, p, epi, bn, L.s));
+    const int bn = gemm_bn_for(lin.dtype, epi, p, L.s);
+    L.note(gemm_sm100(lin.dtype, x, ldx, lin.w, p, epi, bn, L.s));
 }
 
 void run_dcb(Launch& L, const Dcb& d, const __half* x, int ldx, int H, int W, __half* out, int ldo,
@@ -324,15 +390,30 @@ void run_dcb(Launch& L, const Dcb& d, const __half* x, int ldx, int H, int W, __
         ldin = d.C;
     }
     gemm(L, d.dc1, kEpiBiasWsilu, xin, ldin, M, s.t1, d.cdc);
-    L.note(launch_dwconv3x3(s.t1, H, W, d.cdc, d.cdc, d.dw, s.t2, d.cdc, L.s));
+    L.note(launch_dwconv3x3(s.t1, H, W, d.cdc, d.cdc, d.dw, s.t2, d.cdc, L.s, d.dtype));
     gemm(L, d.dc2, kEpiBiasRes, s.t2, d.cdc, M, s.t3, d.C, xin, ldin);
-    if (!d.shortcut && ffn_sm100_preferred(d.C, d.cffn, d.ffn1.cout)) {
+    if (!d.shortcut && d.dtype == 0 && ffn_sm100_preferred(d.C, d.cffn, d.ffn1.cout)) {
         // the ConvFFN as one kernel, the quad output kept on chip (ffn_sm100.cu)
         FfnParams fp{M, d.C, d.cffn, d.ffn1.b, d.ffn2.b, q, out, ldo, L.err_word, 0};
         L.note(ffn_sm100(s.t3, d.C, d.ffn1.w, d.ffn2.w, fp, L.s));
         return;
     }
-    gemm(L, d.ffn1, kEpiQuad, s.t3, d.C, M, s.t4, d.cffn);
+    if (d.ffn1_w8 != nullptr && s.t5 != nullptr) {
+        // the FP8 form: E4M3 copy of the dc output, quad GEMM on kind::f8f6f4
+        L.note(launch_quantize_fp8(s.t3, d.dtype, d.C, 1.0f / kFp8ActScale, s.t5, d.C, M, d.C, L.s));
+        GemmParams p{};
+        p.M = M;
+        p.N = d.ffn1.cout;
+        p.K = d.ffn1.cin;
+        p.bias = d.ffn1.b;
+        p.wscale = d.ffn1_ws;
+        p.out = s.t4;
+        p.ldo = d.cffn;
+        p.err = L.err_word;
+        L.note(gemm_sm100(kDtypeF8, s.t5, d.C, d.ffn1_w8, p, kEpiQuad, 0, L.s));
+    } else {
+        gemm(L, d.ffn1, kEpiQuad, s.t3, d.C, M, s.t4, d.cffn);
+    }
     if (d.shortcut) {
         // conv1x1_bias_shortcut2 (layers_proxy.cpp:89-91): ffn + ffn input + block input
         gemm(L, d.ffn2, kEpiBiasRes2, s.t4, d.cffn, M, out, ldo, s.t3, d.C, nullptr, 0, xin, ldin);

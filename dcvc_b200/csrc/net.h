@@ -47,11 +47,13 @@ struct HostTensor {
 };
 using StateDict = std::map<std::string, HostTensor>;
 
-// 1x1 convolution: w [cout, cin] (FP16, K-major), b [cout] (FP32, may be null).
+// 1x1 convolution: w [cout, cin] (K-major, in the activation format `dtype`: 0 FP16, 1 BF16),
+// b [cout] (FP32, may be null).  The layer reads and writes activations of its own format.
 struct Lin {
     const __half* w = nullptr;
     const float* b = nullptr;
     int cin = 0, cout = 0;
+    int dtype = 0;
 };
 
 // DepthConvBlock (layers.py:128-159; layers_proxy.cpp:71-206).
@@ -65,7 +67,16 @@ struct Dcb {
     Lin ffn2;
     int C = 0, cdc = 0, cffn = 0, cin = 0;
     bool shortcut = false;      // out += block input (layers.py:155-158)
+    int dtype = 0;              // activation format of the whole block (0 FP16, 1 BF16)
+    // FP8 form (BF16 blocks only): ffn.0 (the quad GEMM) on E4M3 operands.  ffn1_w8 [4*cffn, C]
+    // E4M3 rows quantised with their own scale, ffn1_ws = row scale * kFp8ActScale.
+    const uint8_t* ffn1_w8 = nullptr;
+    const float* ffn1_ws = nullptr;
 };
+
+// Quantisation scale of the activations fed to the FP8 GEMMs: x_q = E4M3(x / kFp8ActScale).
+// DepthConvBlock intermediates of the calibrated models stay well inside E4M3's range (+-448).
+constexpr float kFp8ActScale = 1.0f;
 
 // ResidualBlockWithStride2: pixel_unshuffle(2) + 1x1 (K permuted to (dy, dx, c)) + DCB (with the
 // block shortcut when the model keeps the reference's default, layers.py:176-188).
@@ -86,6 +97,16 @@ class ParamBuilder {
 public:
     ParamBuilder(const StateDict& sd, DeviceArena& arena) : sd_(sd), arena_(arena) {}
     bool has(const std::string& name) const { return sd_.count(name) != 0; }
+    // activation format of the layers built from here on (0 FP16, 1 BF16); half_rows tables
+    // stay FP16.  fp8 (with dtype 1): DepthConvBlocks also get E4M3 copies of their ffn.0
+    // weights for the FP8 quad GEMM.
+    void set_dtype(int dtype, bool fp8 = false)
+    {
+        dtype_ = dtype;
+        fp8_ = fp8 && dtype == 1;
+    }
+    // a [rows, cols] table of the state dict as BF16 (per-channel factors of BF16 layers)
+    const __half* bf16_rows(const std::string& name, int* rows, int* cols);
     Lin lin(const std::string& prefix, bool bias = true);
     Dcb dcb(const std::string& prefix, bool shortcut = false);
     DownBlock down(const std::string& prefix, bool shortcut = false);
@@ -101,6 +122,7 @@ public:
 private:
     const HostTensor* get(const std::string& name, size_t ndim_min = 1);
     const __half* upload_half(const std::vector<float>& v);
+    const __half* upload_act(const std::vector<float>& v, int dtype);  // FP16 or BF16 bits
     const float* upload_float(const std::vector<float>& v);
     void fail(const std::string& m)
     {
@@ -110,6 +132,8 @@ private:
     const StateDict& sd_;
     DeviceArena& arena_;
     std::string err_;
+    int dtype_ = 0;
+    bool fp8_ = false;
 };
 
 // Per-level scratch for DCB execution.
@@ -119,6 +143,7 @@ struct Scratch {
     __half* t2 = nullptr;  // depthwise output
     __half* t3 = nullptr;  // dc output (+ residual)
     __half* t4 = nullptr;  // ffn chunk-add output
+    uint8_t* t5 = nullptr; // E4M3 copy of t3 (FP8 form only)
 };
 
 struct Launch {

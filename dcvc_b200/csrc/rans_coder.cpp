@@ -622,11 +622,14 @@ inline int8_t rd_symbol(uint32_t& x, const uint8_t*& p, const uint8_t* end, bool
                 raw |= d << (2 * j);
             }
         }
-        v = raw + maxv;
+        v = static_cast<int32_t>(static_cast<uint32_t>(raw) + static_cast<uint32_t>(maxv));
     }
-    // 0, +1, -1, +2, -2, ... for v = 0, 1, 2, 3, 4, ... (v >= 0), without a branch
-    const int32_t h = (v + 1) >> 1;
-    return static_cast<int8_t>((v & 1) ? h : -h);
+    // 0, +1, -1, +2, -2, ... for v = 0, 1, 2, 3, 4, ...: the reference's expression (rans.cpp,
+    // decode_one_symbol), kept for every v.  A corrupt stream with 16 bypass digits can set bit 31
+    // of raw, and for such negative v only this form gives the reference's (and the GPU
+    // decoder's) symbol; it is evaluated in 64 bits so that no input overflows.
+    const int64_t w = v;
+    return static_cast<int8_t>((w % 2 == 1) ? (w + 1) / 2 : -(w + 1) / 2);
 }
 
 }  // namespace

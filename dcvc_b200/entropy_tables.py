@@ -2,15 +2,15 @@
 
 Restates GaussianEncoder.update and BitEstimator.update (src/models/entropy_models.py:114-217)
 with the same FP32 torch operations in the same order, and quantises each pmf with this
-package's pmf_to_quantized_cdf (the C++ port of py_rans.cpp:35-94).  The resulting int32 tables
-equal the reference model's `gaussian_encoder` / `bit_estimator_z` CDF info bit for bit.
+package's pmf_to_quantized_cdf (the C++ port of py_rans.cpp:35-94) unless the caller passes
+another quantiser with the same contract (list of floats -> list of ints).  The resulting int32
+tables equal the reference model's `gaussian_encoder` / `bit_estimator_z` CDF info bit for bit.
+The native library is loaded only when the default quantiser is used.
 """
 import math
 
 import torch
 import torch.nn.functional as F
-
-from .MLCodec_extensions_cpp import pmf_to_quantized_cdf
 
 MAX_ENTROPY_CODING_VALUE = 8
 SCALE_MIN, SCALE_MAX, SCALE_LEVEL = 0.11, 16.0, 128
@@ -28,17 +28,23 @@ def _reorder_prob(prob):
     return out
 
 
-def _pmf_to_cdf(pmf, tail_mass, pmf_length, max_length):
+def _default_quantizer():
+    from .MLCodec_extensions_cpp import pmf_to_quantized_cdf
+    return pmf_to_quantized_cdf
+
+
+def _pmf_to_cdf(pmf, tail_mass, pmf_length, max_length, quantize=None):
+    quantize = quantize or _default_quantizer()
     cdf = torch.zeros((len(pmf_length), max_length + 2), dtype=torch.int32)
     for i, p in enumerate(pmf):
         prob = torch.cat((p[: pmf_length[i]], tail_mass[i]), dim=0)
-        q = pmf_to_quantized_cdf(_reorder_prob(prob).tolist())
+        q = quantize(_reorder_prob(prob).tolist())
         q = torch.IntTensor(q)
         cdf[i, : q.size(0)] = q
     return cdf
 
 
-def gaussian_tables():
+def gaussian_tables(quantize=None):
     """(quantized_cdf [128, 19] int32, cdf_length [128] int32) of the Gaussian scale tables."""
     scale_table = torch.exp(torch.linspace(math.log(SCALE_MIN), math.log(SCALE_MAX), SCALE_LEVEL))
     zeros = torch.zeros_like(scale_table)
@@ -56,7 +62,7 @@ def gaussian_tables():
     lower = dist.cdf(samples - 0.5)
     pmf = upper - lower
     tail_mass = 2 * lower[:, :1]
-    cdf = _pmf_to_cdf(pmf, tail_mass, pmf_length, max_length)
+    cdf = _pmf_to_cdf(pmf, tail_mass, pmf_length, max_length, quantize)
     return cdf.numpy(), (pmf_length + 2).reshape(-1).int().numpy()
 
 
@@ -70,7 +76,7 @@ def _bit_estimator_prob(x, h, b, a):
 
 
 @torch.inference_mode()
-def bit_estimator_tables(h, b, a):
+def bit_estimator_tables(h, b, a, quantize=None):
     """(quantized_cdf [qp_num * ch, 19], cdf_length [qp_num * ch]) from the bit estimator
     parameters h, b [qp, ch, 4] and a [qp, ch, 3] (FP32, as BitEstimator.update runs them)."""
     h, b, a = h.float().cpu(), b.float().cpu(), a.float().cpu()
@@ -96,15 +102,15 @@ def bit_estimator_tables(h, b, a):
     pmf = pmf.reshape([-1, max_length])
     tail_mass = tail_mass.reshape([-1, 1])
     pmf_length = pmf_length.reshape([-1])
-    cdf = _pmf_to_cdf(pmf, tail_mass, pmf_length, max_length)
+    cdf = _pmf_to_cdf(pmf, tail_mass, pmf_length, max_length, quantize)
     return cdf.numpy(), (pmf_length + 2).reshape(-1).int().numpy()
 
 
-def add_cdf_to_state_dict(state_dict):
+def add_cdf_to_state_dict(state_dict, quantize=None):
     """Adds the four CDF entries the proxies read (common_model.py:64-70)."""
-    qy, ly = gaussian_tables()
+    qy, ly = gaussian_tables(quantize)
     qz, lz = bit_estimator_tables(state_dict["bit_estimator_z.h"], state_dict["bit_estimator_z.b"],
-                                  state_dict["bit_estimator_z.a"])
+                                  state_dict["bit_estimator_z.a"], quantize)
     out = dict(state_dict)
     out["gaussian_encoder.quantized_cdf"] = torch.from_numpy(qy)
     out["gaussian_encoder.cdf_length"] = torch.from_numpy(ly)

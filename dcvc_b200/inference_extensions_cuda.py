@@ -41,6 +41,8 @@ for _k in ("hts", "htl", "ld"):
                                   ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)])
     _proto(f"dcvc_{_k}_stats", [_vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                  ctypes.POINTER(ctypes.c_size_t)])
+_proto("dcvc_hts_set_precision", [_vp, ctypes.c_int])
+_proto("dcvc_hts_buffer_dtype", [_vp, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int)])
 _proto("dcvc_intra_create", [ctypes.POINTER(_vp)])
 _proto("dcvc_intra_destroy", [_vp])
 _proto("dcvc_intra_set_param", [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_char_p),
@@ -139,15 +141,18 @@ class _Proxy:
             (ctypes.c_int * n)(*dtypes), (ctypes.c_int * n)(*on_dev), float(skip_threshold)),
             "set_param")
 
+    def _buffer_dtype(self, name):
+        return torch.float16
+
     def buffer(self, name):
-        """Copy of an internal device buffer as a [rows, cols] float16 tensor (see
-        dcvc_hts_buffer / dcvc_intra_buffer)."""
+        """Copy of an internal device buffer as a [rows, cols] float16 (or, in the HT-S codec's
+        BF16 form, bfloat16) tensor (see dcvc_hts_buffer / dcvc_intra_buffer)."""
         ptr, r, c, ld = _vp(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         N.check(self._fn("buffer")(self._h, name.encode(), ctypes.byref(ptr), ctypes.byref(r),
                                    ctypes.byref(c), ctypes.byref(ld)), "buffer")
-        full = torch.as_tensor(_DeviceView(ptr.value, (r.value, ld.value)), device="cuda")
+        full = torch.as_tensor(_DeviceView(ptr.value, (r.value, ld.value), "<i2"), device="cuda")
         torch.cuda.synchronize()
-        return full[:, : c.value].clone()
+        return full[:, : c.value].clone().view(self._buffer_dtype(name))
 
     def stats(self):
         """(symbols coded by the last call, kernels it enqueued, device bytes held)."""
@@ -159,9 +164,33 @@ class _Proxy:
 
 class DMCHTSProxy(_Proxy):
     """Chunk codec of the HT-S video model (dmc_hts_proxy.h:215-355).  One instance per stream;
-    not re-entrant."""
+    not re-entrant.
+
+    precision: "fp16" (the reference's form, default), "bf16" — the activation format of the
+    analysis and synthesis transforms — or "fp8" (the BF16 form with the transforms' quad GEMMs
+    on E4M3 operands), see dcvc_hts_set_precision; an extension, the reference's constructor
+    takes no arguments.  Inputs and reconstructions stay float16 in every form."""
 
     _kind = "hts"
+    _PRECISIONS = {"fp16": 0, "bf16": 1, "fp8": 2}
+
+    def __init__(self, precision="fp16"):
+        super().__init__()
+        if precision not in self._PRECISIONS:
+            raise ValueError(f"precision must be one of {sorted(self._PRECISIONS)}")
+        if self._kind == "hts":
+            N.check(_lib.dcvc_hts_set_precision(self._h, self._PRECISIONS[precision]),
+                    "set_precision")
+        elif precision != "fp16":
+            raise ValueError(f"{type(self).__name__} runs in the fp16 form only")
+        self.precision = precision
+
+    def _buffer_dtype(self, name):
+        if self._kind != "hts":
+            return torch.float16
+        dt = ctypes.c_int()
+        N.check(_lib.dcvc_hts_buffer_dtype(self._h, name.encode(), ctypes.byref(dt)), "buffer")
+        return torch.bfloat16 if dt.value == 1 else torch.float16
 
     def add_ref_feature_from_frame(self, frame, apply_adaptor=True):
         frame = _channels_last_data(frame, "frame")

@@ -46,6 +46,34 @@ def conv1x1(a, w, bias=None, epilogue=N.EPI_BIAS, res=None, res2=None, qscale=No
     return out
 
 
+def quantize_fp8(x, inv_scale, out=None):
+    """E4M3 bytes of x * inv_scale (x: [M, C] float16 / bfloat16, row pitch x.stride(0)),
+    saturating at +-448; returned as a torch.float8_e4m3fn tensor."""
+    M, C = x.shape
+    if out is None:
+        out = torch.empty((M, C), dtype=torch.float8_e4m3fn, device=x.device)
+    N.check(N.lib.dcvc_quantize_fp8(x.data_ptr(), _DT[x.dtype], x.stride(0), ctypes.c_float(inv_scale),
+                                    out.data_ptr(), out.stride(0), M, C, _stream()),
+            "dcvc_quantize_fp8")
+    return out
+
+
+def conv1x1_f8(a, w, wscale, bias, epilogue=N.EPI_BIAS, out=None, block_n=0):
+    """The FP8 GEMM form: a [M, K] and w [N, K] float8_e4m3fn, wscale [N] fp32 (activation scale
+    times weight-row scale), bias [N] fp32; returns bfloat16 epilogue(acc * wscale + bias)
+    ([M, N/4] for the QUAD epilogue)."""
+    assert a.dim() == 2 and a.stride(1) == 1 and w.is_contiguous()
+    M, K = a.shape
+    Nn = w.shape[0]
+    if out is None:
+        out = torch.empty((M, Nn // 4 if epilogue == N.EPI_QUAD else Nn), dtype=torch.bfloat16,
+                          device=a.device)
+    N.check(N.lib.dcvc_conv1x1_f8(epilogue, M, Nn, K, a.data_ptr(), a.stride(0), w.data_ptr(),
+                                  wscale.data_ptr(), bias.data_ptr(), out.data_ptr(), out.stride(0),
+                                  block_n, _stream()), "dcvc_conv1x1_f8")
+    return out
+
+
 def gemm_autotune(dtype, epilogue, M, Nn, K, sub_w=0, sub_cout=0):
     """Times every valid N tile width of one conv1x1 shape on the current stream and records the
     fastest for conv1x1(block_n=0) and the codecs.  Returns (block_n, microseconds per launch)."""
@@ -124,6 +152,9 @@ _sig("dcvc_compact_blocks", [_i])
 _sig("dcvc_compact", [_v, _i, _v, _i, _v, _v, _v, _v])
 _sig("dcvc_recover", [_v, _v, _v, _i, _v, _v])
 _sig("dcvc_scale_index_table", [_v])
+_sig("dcvc_scale_index_table_device", [_v, _v])
+_sig("dcvc_quantize_fp8", [_v, _i, _i, ctypes.c_float, _v, _i, _i, _i, _v])
+_sig("dcvc_conv1x1_f8", [_i, _i, _i, _i, _v, _i, _v, _v, _v, _v, _i, _i, _v])
 _sig("dcvc_yuv420_to_input", [_v, _i, _i, _i, _v, _i, _v])
 _sig("dcvc_frames_to_yuv420", [ctypes.POINTER(_v), _i, _i, _i, _i, _i, _v, _v])
 
@@ -226,9 +257,18 @@ def restore_phase(phase, mode, y_q, means, q_dec, y_hat, H, W):
 
 
 def scale_index_table(device="cuda"):
+    """The host-computed table (CPU restatement, double-precision logarithm)."""
     lut = torch.empty(65536, dtype=torch.uint8)
     N.check(N.lib.dcvc_scale_index_table(lut.data_ptr()), "scale_index_table")
     return lut.to(device)
+
+
+def scale_index_table_device():
+    """The table the codecs use: the reference's FP16 scale_to_index evaluated on the device."""
+    lut = torch.empty(65536, dtype=torch.uint8, device="cuda")
+    N.check(N.lib.dcvc_scale_index_table_device(lut.data_ptr(), _stream()),
+            "scale_index_table_device")
+    return lut
 
 
 def build_index(encode, y_q, scales, thr, lut):

@@ -28,52 +28,64 @@ def frame_bytes(width, height):
     return width * height * 3 // 2
 
 
+class _I420File:
+    """Frame geometry of a planar 8-bit I420 file: frame k occupies bytes
+    [k * frame, (k + 1) * frame), luma plane first, then the two chroma planes."""
+
+    def __init__(self, width, height):
+        self.width, self.height = width, height
+        self.luma = width * height
+        self.frame = frame_bytes(width, height)
+
+    def split(self, buf):
+        """One frame's bytes -> (y [1, H, W], uv [2, H/2, W/2]) views of a private array."""
+        a = np.frombuffer(buf, dtype=np.uint8).copy()
+        y = a[: self.luma].reshape(1, self.height, self.width)
+        uv = a[self.luma: self.frame].reshape(2, self.height // 2, self.width // 2)
+        return y, uv
+
+
 class YUV420Reader:
-    """Planar 8-bit YUV 4:2:0 reader (video_reader.py:51-99)."""
+    """Reads frames of a planar 8-bit YUV 4:2:0 file by position.
+
+    The constructor and `read_one_frame` keep the interface of the reference's reader
+    (src/utils/video_reader.py:50-99): a path without the ".yuv" suffix gets it appended,
+    `skip_frame` frames are passed over, and `read_one_frame` returns (y [1, H, W],
+    uv [2, H/2, W/2]) or (None, None) once the file has no whole frame left.  Internally the
+    reader keeps only a frame cursor and reads each request with one positioned read
+    (`os.pread`) of whole frames, so `read_raw` can hand many frames to the device path in one
+    buffer."""
 
     def __init__(self, src_path, width, height, skip_frame=0):
-        self.eof = False
-        if not src_path.endswith(".yuv"):
-            src_path = src_path + ".yuv"
-        self.src_path = src_path
-        self.y_size = width * height
-        self.y_width = width
-        self.y_height = height
-        self.uv_size = width * height // 2
-        self.uv_width = width // 2
-        self.uv_height = height // 2
-        self.file = open(src_path, "rb")
-        skipped = 0
-        while not self.eof and skipped < skip_frame:
-            y = self.file.read(self.y_size)
-            uv = self.file.read(self.uv_size)
-            if not y or not uv:
-                self.eof = True
-            skipped += 1
+        self.src_path = src_path if src_path.endswith(".yuv") else src_path + ".yuv"
+        self.geom = _I420File(width, height)
+        self._fd = os.open(self.src_path, os.O_RDONLY)
+        self._frames_in_file = os.fstat(self._fd).st_size // self.geom.frame
+        self.cursor = max(0, int(skip_frame))
+        self.eof = self.cursor >= self._frames_in_file
+
+    def _take(self, n):
+        k = max(0, min(n, self._frames_in_file - self.cursor))
+        data = os.pread(self._fd, k * self.geom.frame, self.cursor * self.geom.frame) if k else b""
+        self.cursor += k
+        self.eof = k < n
+        return data, k
 
     def read_one_frame(self):
         """(y [1, H, W], uv [2, H/2, W/2]) uint8 arrays, or (None, None) at the end."""
         if self.eof:
             return None, None
-        y = self.file.read(self.y_size)
-        uv = self.file.read(self.uv_size)
-        if not y or not uv:
-            self.eof = True
+        data, k = self._take(1)
+        if k == 0:
             return None, None
-        y = np.frombuffer(y, dtype=np.uint8).copy().reshape(1, self.y_height, self.y_width)
-        uv = np.frombuffer(uv, dtype=np.uint8).copy().reshape(2, self.uv_height, self.uv_width)
-        return y, uv
+        return self.geom.split(data)
 
     def read_raw(self, n):
         """Up to n whole frames as one uint8 array (frames back to back); fewer at the end."""
         if self.eof:
             return np.zeros(0, dtype=np.uint8)
-        fb = self.y_size + self.uv_size
-        data = self.file.read(n * fb)
-        k = len(data) // fb
-        if k < n:
-            self.eof = True
-        return np.frombuffer(data[: k * fb], dtype=np.uint8).copy()
+        data, _ = self._take(n)
+        return np.frombuffer(data, dtype=np.uint8).copy()
 
     def __enter__(self):
         return self
@@ -86,31 +98,43 @@ class YUV420Reader:
         self.close()
 
     def close(self):
-        f = getattr(self, "file", None)
-        if f and not f.closed:
-            f.close()
+        fd = getattr(self, "_fd", None)
+        if fd is not None:
+            os.close(fd)
+            self._fd = None
 
 
 class YUV420Writer:
-    """Planar 8-bit YUV 4:2:0 writer (video_writer.py:33-61)."""
+    """Appends planar 8-bit YUV 4:2:0 frames to a file.
+
+    Path rule of the reference's writer (src/utils/video_writer.py:33-61): a destination that
+    does not end in ".yuv" names a directory, and the frames go to "out.yuv" inside it.  Frames
+    are accumulated as byte chunks and appended with one `os.write` per call."""
 
     def __init__(self, dst_path, width, height):
-        if not dst_path.endswith(".yuv"):
-            dst_path = dst_path + "/out.yuv"
-        self.dst_path = dst_path
-        self.width = width
-        self.height = height
-        self.file = open(dst_path, "wb")
+        self.dst_path = dst_path if dst_path.endswith(".yuv") else os.path.join(dst_path, "out.yuv")
+        self.geom = _I420File(width, height)
+        self._fd = os.open(self.dst_path, os.O_WRONLY | os.O_CREAT | os.O_TRUNC, 0o644)
+
+    def _append(self, *arrays):
+        payload = b"".join(np.ascontiguousarray(a, dtype=np.uint8).tobytes() for a in arrays)
+        view = memoryview(payload)
+        while view:
+            view = view[os.write(self._fd, view):]
 
     def write_one_frame(self, y, uv):
-        self.file.write(np.ascontiguousarray(y, dtype=np.uint8).tobytes())
-        self.file.write(np.ascontiguousarray(uv, dtype=np.uint8).tobytes())
+        if np.size(y) + np.size(uv) != self.geom.frame:
+            raise ValueError(f"frame of {np.size(y) + np.size(uv)} bytes, expected "
+                             f"{self.geom.frame} for {self.geom.width}x{self.geom.height}")
+        self._append(y, uv)
 
     def write_raw(self, planes):
         """Whole I420 frames back to back (a uint8 array or tensor)."""
         if isinstance(planes, torch.Tensor):
             planes = planes.cpu().numpy()
-        self.file.write(np.ascontiguousarray(planes, dtype=np.uint8).tobytes())
+        if np.size(planes) % self.geom.frame:
+            raise ValueError("write_raw takes whole frames")
+        self._append(planes)
 
     def __enter__(self):
         return self
@@ -123,9 +147,10 @@ class YUV420Writer:
         self.close()
 
     def close(self):
-        f = getattr(self, "file", None)
-        if f and not f.closed:
-            f.close()
+        fd = getattr(self, "_fd", None)
+        if fd is not None:
+            os.close(fd)
+            self._fd = None
 
 
 def padding_size(height, width, p=16):

@@ -41,6 +41,14 @@ extern "C" {
 #define DCVC_I32 3
 #define DCVC_I64 4
 
+/* precision forms of the HT-S codec (dcvc_hts_set_precision) */
+#define DCVC_PRECISION_F16 0
+#define DCVC_PRECISION_BF16 1
+#define DCVC_PRECISION_FP8 2
+
+/* block_n of dcvc_conv1x1 selecting the streaming form of the residual epilogues */
+#define DCVC_BLOCK_N_STREAM (-1)
+
 /* 1x1-conv GEMM epilogues (dcvc_conv1x1) */
 #define DCVC_EPI_BIAS 0        /* conv1x1_bias                       */
 #define DCVC_EPI_BIAS_WSILU 1  /* conv1x1_bias_wsilu                 */
@@ -73,11 +81,28 @@ int dcvc_device_error(int* code, int clear);
  *   qscale : per-output-channel multiplier [N], activation dtype (BIAS_RES_Q, BIAS_Q)
  *   out    : [M, N] rows (QUAD: [M, N/4]; SUBPEL: [(2H)(2W), sub_cout]) with pitch ldo
  *   sub_w, sub_cout : SUBPEL input width and output channels (N = 4 * sub_cout)
- *   block_n: N tile (0 = choose); K must be a multiple of 64, lda/ldr/ldo multiples of 8. */
+ *   block_n: N tile 256 / 128 / 64 of the tiled kernel, DCVC_BLOCK_N_STREAM for the streaming
+ *            form of BIAS_RES / BIAS_RES_Q (K <= 256, N a multiple of 128: W slice resident in
+ *            shared memory, contiguous row ranges per CTA), 0 = choose; every choice gives the
+ *            same output bits.  K must be a multiple of 64, lda/ldr/ldo multiples of 8. */
 int dcvc_conv1x1(int dtype, int epilogue, int M, int N, int K, const void* a, int lda,
                  const void* w, const float* bias, const void* res, int ldr, const void* res2,
                  int ldr2, const void* qscale, void* out, int ldo, int sub_w, int sub_cout,
                  int block_n, void* stream);
+/* The FP8 form of dcvc_conv1x1 for the epilogues BIAS, BIAS_WSILU and QUAD: a [M, K] and
+ * w [N, K] are E4M3 bytes (lda a multiple of 16, K of 128), the tcgen05 MMA is kind::f8f6f4
+ * with FP32 accumulation, and the epilogue computes acc * wscale[n] + bias[n] (wscale: FP32
+ * per output channel, the product of the activation's and the weight row's quantisation
+ * scales) before the activation; out is BF16.  No counterpart in the reference (its GEMMs are
+ * FP16, cutlass/conv1x1_kernel.h:37-41). */
+int dcvc_conv1x1_f8(int epilogue, int M, int N, int K, const void* a, int lda, const void* w,
+                    const float* wscale, const float* bias, void* out, int ldo, int block_n,
+                    void* stream);
+/* dst[m, c] = E4M3(src[m, c] * inv_scale), saturating at +-448: src FP16 or BF16 (src_dtype
+ * DCVC_F16 / DCVC_BF16) with pitch lds, dst bytes with pitch ldd (C and both pitches multiples
+ * of 8).  The A operand of dcvc_conv1x1_f8; no counterpart in the reference. */
+int dcvc_quantize_fp8(const void* src, int src_dtype, int lds, float inv_scale, void* dst, int ldd,
+                      int M, int C, void* stream);
 
 /* Runtime autotuner of the dcvc_conv1x1 tile width.  Replaces the reference's compile-time
  * per-shape configuration tables (HINT_MAP_* in src/layers/extensions/inference/cutlass/
@@ -191,8 +216,15 @@ int dcvc_recover(const int8_t* dec, const uint8_t* cond, const int* block_counts
 
 /* The 65536-entry table mapping the FP16 bits of a Gaussian scale to its CDF table index, as
  * scale_to_index evaluates it in FP16 (src/layers/extensions/inference/elementwise/
- * stream.cu:77-87 with the constants of def_const.h:6-12); used by the index kernels. */
+ * stream.cu:77-87 with the constants of def_const.h:6-12), computed on the host with the
+ * logarithm in double precision (a CPU restatement; needs no GPU). */
 int dcvc_scale_index_table(uint8_t* lut);
+/* The same table evaluated on the device exactly as the reference's kernel does in its
+ * fast-math build (float max/min, the fast-math logarithm, FP16 roundings of the difference and
+ * the product, round-down to uint8): lut is a device buffer of 65536 bytes.  The codecs use this
+ * table.  Replaces the scale_to_index helper of stream.cu:77-87 (with to_uint8,
+ * common_cu.h:181-184). */
+int dcvc_scale_index_table_device(uint8_t* lut, void* stream);
 
 /* ------------------------------------------------------------------ rANS coder (host) */
 
@@ -313,13 +345,26 @@ int dcvc_hts_compress(void* handle, const void* x, int height, int width, int qp
  * not decode. */
 int dcvc_hts_decompress(void* handle, const uint8_t* bytes, size_t nbytes, int qp, int height,
                         int width, int ec_parallel, int reset, void* stream, void** frames);
-/* Read-only view of a per-stream device buffer (FP16 rows x cols, pitch ld): "y_hat", "y_q",
- * "memory", "ctx", "feature_p", "common", "feature_i".  For inspection and tests; no
- * counterpart in the reference. */
+/* Read-only view of a per-stream device buffer (16-bit rows x cols, pitch ld; FP16 unless
+ * dcvc_hts_buffer_dtype says BF16): "y_hat", "y_q", "memory", "ctx", "feature_p", "common",
+ * "feature_i".  For inspection and tests; no counterpart in the reference. */
 int dcvc_hts_buffer(void* handle, const char* name, const void** ptr, int* rows, int* cols,
                     int* ld);
 /* symbols coded by the last call, kernels it enqueued, device bytes held by the handle */
 int dcvc_hts_stats(void* handle, int* symbols, int* kernels, size_t* device_bytes);
+/* Precision form of the analysis and synthesis transforms (encoder, decoder, recon head, feature
+ * adaptors and extractor): DCVC_PRECISION_F16 (the reference's form, the default) or
+ * DCVC_PRECISION_BF16 (BF16 activations and weights, FP32 accumulation) or DCVC_PRECISION_FP8 (the
+ * BF16 form with every transform DepthConvBlock's quad GEMM, ffn.0, on E4M3 operands: weight rows
+ * quantised with per-output-channel FP32 scales, activations by dcvc_quantize_fp8, FP32
+ * accumulation, dcvc_conv1x1_f8).  The entropy-parameter
+ * path stays FP16 with the same kernels on both sides, so symbols and CDF indexes round-trip
+ * exactly in every form.  Takes effect at the next dcvc_hts_set_param; encoder and decoder
+ * handles must use the same form.  No counterpart in the reference (FP16 only there,
+ * test_video.py:25-27). */
+int dcvc_hts_set_precision(void* handle, int precision);
+/* The 16-bit format (DCVC_F16 or DCVC_BF16) of a buffer named as in dcvc_hts_buffer. */
+int dcvc_hts_buffer_dtype(void* handle, const char* name, int* dtype);
 
 /* ------------------------------------------------------------------ HT-L chunk codec */
 

@@ -198,10 +198,18 @@ static int8_t dec_symbol(dec_t* d, const int32_t* cdf, int32_t maxv)
             nbp += b;
         }
         int32_t raw = 0;
-        for (int j = 0; j < nbp; j++) raw |= (int32_t)dec_bits(d) << (j * BYPASS_BITS);
-        v = raw + maxv;
+        /* digits past the 16th would shift past bit 31 (undefined in the reference's C++, which
+         * a valid stream never reaches: |v| <= 256); they are read and dropped */
+        for (int j = 0; j < nbp; j++) {
+            uint32_t digit = dec_bits(d);
+            if (j < 16) raw = (int32_t)((uint32_t)raw | (digit << (j * BYPASS_BITS)));
+        }
+        v = (int32_t)((uint32_t)raw + (uint32_t)maxv);
     }
-    return (int8_t)((v % 2 == 1) ? (v + 1) / 2 : -(v + 1) / 2);
+    {
+        int64_t w = v;
+        return (int8_t)((w % 2 == 1) ? (w + 1) / 2 : -(w + 1) / 2);
+    }
 }
 
 /* ---------------------------------------------------------------- container */

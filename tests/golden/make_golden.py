@@ -1,9 +1,9 @@
 """Generates the golden fixtures under tests/golden/ from the reference itself.
 
-Run here, where the reference sources exist (default /root/reference) and oracle/_ref has been
+Run here, where the reference sources exist (the reference checkout given by --ref or the DCVC_REFERENCE environment variable) and oracle/_ref has been
 built by `make -C oracle`:
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py [--ref <reference checkout>]
 
 Outputs (all small, committed):
   rans_golden.npz     symbols and the reference coder's bytes for ec_parallel 1..8 and edge cases
@@ -106,8 +106,11 @@ def fingerprint(sd):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("DCVC_REFERENCE"),
+                    help="reference checkout (default: $DCVC_REFERENCE)")
     args = ap.parse_args()
+    if not args.ref:
+        ap.error("give --ref or set DCVC_REFERENCE to the reference checkout")
     sys.path.insert(0, args.ref)
     sys.path.insert(0, os.path.join(ROOT, "oracle", "_ref"))
     import torch

@@ -1,9 +1,9 @@
 """Generates the intra-model golden fixtures under tests/golden/ from the reference itself.
 
-Run here, where the reference sources exist (default /root/reference) and oracle/_ref has been
+Run here, where the reference sources exist (the reference checkout given by --ref or the DCVC_REFERENCE environment variable) and oracle/_ref has been
 built by `make -C oracle`:
 
-    python tests/golden/make_intra_golden.py [--ref /root/reference]
+    python tests/golden/make_intra_golden.py [--ref <reference checkout>]
 
 Outputs (small, committed):
   weights_intra_seed0.json    fingerprints of the reference DMCI() state dict for torch.manual_seed(0)
@@ -76,8 +76,11 @@ def make_segments(qy, ly, qz, lz):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("DCVC_REFERENCE"),
+                    help="reference checkout (default: $DCVC_REFERENCE)")
     args = ap.parse_args()
+    if not args.ref:
+        ap.error("give --ref or set DCVC_REFERENCE to the reference checkout")
     sys.path.insert(0, args.ref)
     import torch
     from src.models.image_model import DMCI

@@ -1,8 +1,8 @@
 """Generates the LD-model golden fixtures under tests/golden/ from the reference itself.
 
-Run here, where the reference sources exist (default /root/reference):
+Run here, where the reference sources exist (the reference checkout given by --ref or the DCVC_REFERENCE environment variable):
 
-    python tests/golden/make_ld_golden.py [--ref /root/reference]
+    python tests/golden/make_ld_golden.py [--ref <reference checkout>]
 
 Outputs (small, committed):
   weights_ld_seed0.json   fingerprints of the reference video_model_ld.DMC() state dict for
@@ -44,8 +44,11 @@ def ld_module_inputs():
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("DCVC_REFERENCE"),
+                    help="reference checkout (default: $DCVC_REFERENCE)")
     args = ap.parse_args()
+    if not args.ref:
+        ap.error("give --ref or set DCVC_REFERENCE to the reference checkout")
     sys.path.insert(0, args.ref)
     import torch
     from src.models.video_model_ld import DMC

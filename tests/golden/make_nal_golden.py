@@ -24,7 +24,10 @@ def payload(i, n):
     return np.random.default_rng(7700 + i).integers(0, 256, n).astype(np.uint8).tobytes()
 
 
-def main(ref="/root/reference"):
+def main(ref=None):
+    ref = ref or os.environ.get("DCVC_REFERENCE")
+    if not ref:
+        raise SystemExit("set DCVC_REFERENCE to the reference checkout")
     sys.path.insert(0, ref)
     from src.utils import stream_helper as S
     f = io.BytesIO()

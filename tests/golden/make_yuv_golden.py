@@ -1,8 +1,8 @@
 """Generates tests/golden/yuv_golden.npz from the reference's own YUV conversions.
 
-Run here, where the reference sources exist (default /root/reference):
+Run here, where the reference sources exist (the reference checkout given by --ref or the DCVC_REFERENCE environment variable):
 
-    python tests/golden/make_yuv_golden.py [--ref /root/reference]
+    python tests/golden/make_yuv_golden.py [--ref <reference checkout>]
 
 The model input is built as get_src_frame does (test_video.py:69-123): ycbcr420_to_444_np on
 the uint8 planes, torch.from_numpy, .half(), / 255.0, - 0.5.  The reconstruction planes are built
@@ -22,8 +22,11 @@ HP, WP = 32, 32           # padded reconstruction size
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("DCVC_REFERENCE"),
+                    help="reference checkout (default: $DCVC_REFERENCE)")
     args = ap.parse_args()
+    if not args.ref:
+        ap.error("give --ref or set DCVC_REFERENCE to the reference checkout")
     sys.path.insert(0, args.ref)
     import torch
     from src.utils.transforms import ycbcr420_to_444_np, yuv_444_to_420

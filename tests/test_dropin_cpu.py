@@ -1,7 +1,8 @@
 """The drop-in modules under the reference's names: the reference's own entropy models, run with
 dcvc_b200's MLCodec_extensions_cpp, build the same CDF tables and code the same bytes as with the
-reference's compiled module.  Runs only where the reference sources are available (this checks
-the boundary from the reference's side; it is skipped elsewhere)."""
+reference's compiled module.  Runs only where the reference checkout is named by the
+DCVC_REFERENCE environment variable (this checks the boundary from the reference's side; it is
+skipped elsewhere)."""
 import os
 import sys
 
@@ -9,8 +10,8 @@ import numpy as np
 import pytest
 import torch
 
-REF = "/root/reference"
-pytestmark = pytest.mark.skipif(not os.path.isdir(os.path.join(REF, "src")),
+REF = os.environ.get("DCVC_REFERENCE", "")
+pytestmark = pytest.mark.skipif(not REF or not os.path.isdir(os.path.join(REF, "src")),
                                 reason="reference sources not available")
 
 

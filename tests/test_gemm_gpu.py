@@ -98,3 +98,82 @@ def test_subpel(H, W, Cin, Cout):
     ref = _ref(N.EPI_SUBPEL, x, w, None, sub_w=W, sub_cout=Cout)
     err = (out.float() - ref).abs()
     assert bool((err <= 2e-2 + 1e-2 * ref.abs()).all()), float(err.max())
+
+
+STREAM_CASES = [
+    # (epilogue name, M, N, K, dtype): dc.3 / ffn.2 at 1080p, y-level shapes, ragged and tiny M
+    ("EPI_BIAS_RES", 32640, 512, 256, torch.float16),
+    ("EPI_BIAS_RES", 8160, 256, 256, torch.float16),
+    ("EPI_BIAS_RES", 8160, 768, 192, torch.float16),
+    ("EPI_BIAS_RES_Q", 32640, 512, 256, torch.float16),
+    ("EPI_BIAS_RES", 4471, 384, 128, torch.float16),
+    ("EPI_BIAS_RES", 37, 128, 64, torch.float16),
+    ("EPI_BIAS_RES", 32640, 512, 256, torch.bfloat16),
+    ("EPI_BIAS_RES_Q", 3000, 256, 256, torch.bfloat16),
+]
+
+
+@pytest.mark.parametrize("name,M,Nn,K,dtype", STREAM_CASES)
+def test_stream_form_matches_tiled_bitwise(name, M, Nn, K, dtype):
+    """The streaming residual GEMM (W slice resident, row ranges per CTA) gives bitwise the
+    tiled kernel's outputs, and both are within the fp32-reference tolerance."""
+    from dcvc_b200 import _native as N, ops
+    epi = getattr(N, name)
+    g = torch.Generator(device="cuda").manual_seed(M + Nn + K)
+    abuf = torch.randn(M, K + 64, device="cuda", generator=g).to(dtype)
+    a = abuf[:, 64:64 + K]
+    w = (torch.randn(Nn, K, device="cuda", generator=g) / K ** 0.5).to(dtype)
+    b = torch.randn(Nn, device="cuda", generator=g) * 0.1
+    rbuf = torch.randn(M, Nn + 128, device="cuda", generator=g).to(dtype)
+    res = rbuf[:, 128:]
+    q = (torch.rand(Nn, device="cuda", generator=g) + 0.5).to(dtype)
+    tiled = ops.conv1x1(a, w, b, epi, res=res, qscale=q, block_n=128 if Nn % 256 else 256)
+    obuf = torch.full((M, Nn + 64), 7.0, device="cuda", dtype=dtype)
+    stream = ops.conv1x1(a, w, b, epi, res=res, qscale=q, out=obuf[:, 64:], block_n=N.BLOCK_N_STREAM)
+    torch.cuda.synchronize()
+    assert N.device_error() == 0
+    assert torch.equal(stream.view(torch.int16), tiled.view(torch.int16))
+    assert bool((obuf[:, :64] == 7.0).all())  # nothing written outside the output view
+    ref = _ref(epi, a, w, b, res, None, q)
+    atol, rtol = TOL[dtype]
+    assert bool(((stream.float() - ref).abs() <= atol + rtol * ref.abs()).all())
+
+
+def test_quantize_fp8_matches_torch_cast():
+    from dcvc_b200 import ops
+    g = torch.Generator(device="cuda").manual_seed(5)
+    for dtype in (torch.float16, torch.bfloat16):
+        xb = (torch.randn(777, 320, device="cuda", generator=g) * 3).to(dtype)
+        x = xb[:, 64:]
+        q = ops.quantize_fp8(x, 1.0 / 0.75)
+        ref = (x.float() * (1.0 / 0.75)).to(torch.float8_e4m3fn)
+        assert torch.equal(q.view(torch.uint8), ref.view(torch.uint8))
+    big = torch.full((8, 8), 6.0e4, device="cuda", dtype=torch.float16)
+    assert float(ops.quantize_fp8(big, 1.0).float().max()) == 448.0  # saturates
+
+
+@pytest.mark.parametrize("name,M,Nn,K,bn", [("EPI_QUAD", 32640, 1024, 512, 256),
+                                             ("EPI_QUAD", 3000, 1024, 256, 256),
+                                             ("EPI_BIAS_WSILU", 5000, 256, 512, 128),
+                                             ("EPI_BIAS", 2047, 512, 384, 256)])
+def test_conv1x1_f8_matches_dequantised_fp32(name, M, Nn, K, bn):
+    """E4M3 operands with per-output-channel scales (kind::f8f6f4, FP32 accumulation) against
+    an fp32 GEMM of the same dequantised operands; BF16 output tolerance."""
+    from dcvc_b200 import _native as N, ops
+    epi = getattr(N, name)
+    g = torch.Generator(device="cuda").manual_seed(M + K)
+    x = torch.randn(M, K, device="cuda", generator=g).to(torch.bfloat16)
+    w = torch.randn(Nn, K, device="cuda", generator=g) / K ** 0.5
+    b = torch.randn(Nn, device="cuda", generator=g) * 0.1
+    a_scale = 0.5
+    w_scale = w.abs().amax(1) / 448.0
+    wq = (w / w_scale[:, None]).to(torch.float8_e4m3fn)
+    aq = ops.quantize_fp8(x, 1.0 / a_scale)
+    out = ops.conv1x1_f8(aq, wq, (w_scale * a_scale).float().contiguous(), b, epi, block_n=bn)
+    torch.cuda.synchronize()
+    assert N.device_error() == 0
+    ad = aq.float() * a_scale
+    wd = wq.float() * w_scale[:, None]
+    ref = _ref(epi, ad, wd, b)
+    err = (out.float() - ref).abs()
+    assert bool((err <= 6e-2 + 2e-2 * ref.abs()).all()), float(err.max())

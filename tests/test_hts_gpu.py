@@ -18,10 +18,21 @@ def _same(a, b):
     return torch.equal(a.view(torch.int16), b.view(torch.int16))
 
 
-@pytest.mark.parametrize("H,W", [(256, 256), (200, 248)])
-def test_round_trip_is_exact(H, W):
+def _proxy(sd, precision):
+    from dcvc_b200.inference_extensions_cuda import DMCHTSProxy
+    p = DMCHTSProxy(precision)
+    p.set_param(sd, 0.15)
+    return p
+
+
+@pytest.mark.parametrize("H,W,precision", [(256, 256, "fp16"), (200, 248, "fp16"),
+                                           (256, 256, "bf16"), (200, 248, "bf16"),
+                                           (200, 248, "fp8")])
+def test_round_trip_is_exact(H, W, precision):
+    """Both precision forms: the BF16 form changes the analysis / synthesis arithmetic, not the
+    exactness of the round trip (reset and padded sizes included)."""
     sd = state_dict()
-    enc, dec = make_proxy(sd), make_proxy(sd)
+    enc, dec = _proxy(sd, precision), _proxy(sd, precision)
     ref = ref_frame(H, W)
     enc.add_ref_feature_from_frame(ref, True)
     dec.add_ref_feature_from_frame(ref, False)  # decoder side defers FA_i (test_video.py:315)
@@ -80,3 +91,29 @@ def test_requires_set_param_and_reference():
     p = DMCHTSProxy()
     with pytest.raises(DcvcError):
         p.compress(chunk(64, 64, 0), 0, False, 0, 0)
+
+
+def test_bf16_form_differs_from_fp16_and_reports_its_buffers():
+    """The BF16 form really runs BF16 transforms: its temporal memory is BF16 (and close to the
+    FP16 form's), its payload differs from the FP16 form's, and a precision outside the two
+    forms is refused."""
+    from dcvc_b200._native import DcvcError  # noqa: F401
+    sd = state_dict()
+    H, W = 128, 192
+    a, b = _proxy(sd, "fp16"), _proxy(sd, "bf16")
+    ref = ref_frame(H, W)
+    a.add_ref_feature_from_frame(ref, True)
+    b.add_ref_feature_from_frame(ref, True)
+    x = chunk(H, W, 0)
+    ba, _ = a.compress(x, 30, False, 0, 0)
+    bb, _ = b.compress(x, 30, False, 0, 0)
+    ma, mb = a.buffer("memory"), b.buffer("memory")
+    assert ma.dtype == torch.float16 and mb.dtype == torch.bfloat16
+    assert b.buffer("common").dtype == torch.float16  # the entropy-parameter path stays FP16
+    rel = float((ma.float() - mb.float()).norm() / ma.float().norm())
+    assert 0 < rel < 0.05, rel
+    assert ba.tobytes() != bb.tobytes()
+    from dcvc_b200.inference_extensions_cuda import DMCHTSProxy
+    with pytest.raises(ValueError):
+        DMCHTSProxy("fp8_unknown")
+

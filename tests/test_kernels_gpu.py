@@ -160,3 +160,29 @@ def test_dwconv3x3(H, W, C):
         groups=C).permute(0, 2, 3, 1).reshape(H * W, C)
     err = (out.float() - ref).abs()
     assert bool((err <= 1e-2 + 1e-2 * ref.abs()).all()), float(err.max())
+
+
+def test_scale_index_table_on_the_device():
+    """The codecs' scale -> CDF index table is evaluated on the device with the reference's own
+    FP16 operation sequence (stream.cu:77-87 in its fast-math build).  It must name one of the
+    128 tables, be monotone in the scale over positive finite scales, and agree with the host's
+    double-precision restatement wherever both are away from a rounding boundary; the entries
+    where the two differ are reported (run with -s)."""
+    from dcvc_b200 import ops
+    dev = ops.scale_index_table_device().cpu().numpy()
+    host = ops.scale_index_table("cpu").numpy()
+    bits = np.arange(65536, dtype=np.uint32).astype(np.uint16)
+    s = bits.view(np.float16).astype(np.float64)
+    pos = np.isfinite(s) & (s > 0)
+    order = np.argsort(s[pos], kind="stable")
+    d = dev[pos][order].astype(np.int32)
+    assert dev.max() <= 127 and (np.diff(d) >= 0).all()
+    coded = pos & (s > np.float64(np.float16(0.15)))
+    diff = np.nonzero(dev != host)[0]
+    diff_coded = np.nonzero((dev != host) & coded)[0]
+    print(f"scale-index table: device vs host differ on {diff.size} of 65536 FP16 scales, "
+          f"{diff_coded.size} of them above the skip threshold", flush=True)
+    for h in diff_coded[:40]:
+        print(f"  scale {s[h]!r} (bits {h:#06x}): device {dev[h]} host {host[h]}")
+    # differences can only sit on rounding boundaries: never more than one table apart
+    assert (np.abs(dev.astype(np.int32) - host.astype(np.int32)) <= 1).all()

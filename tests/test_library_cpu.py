@@ -54,3 +54,38 @@ def test_tuner_and_fault_hook_entry_points_without_gpu():
     assert N.lib.dcvc_gemm_autotune_enable(0) == 0
     assert N.lib.dcvc_rans_inject_task_fault(2) == 0
     assert N.lib.dcvc_rans_inject_task_fault(-1) == 0
+
+
+def test_compaction_entry_points_reject_bad_pointers_without_gpu():
+    """Null or misaligned pointers are refused on the host with DCVC_INVALID_ARGUMENT before any
+    CUDA call, so a ctypes caller gets a status instead of a device memory fault (no GPU here:
+    a launch would fail with a CUDA error, status 2, not 1)."""
+    from dcvc_b200 import _native as N
+    vp, i = ctypes.c_void_p, ctypes.c_int
+    f = N.lib.dcvc_compact
+    f.restype, f.argtypes = i, [vp, i, vp, i, vp, vp, vp, vp]
+    g = N.lib.dcvc_compact_noalloc
+    g.restype, g.argtypes = i, [vp, i, vp, i, vp, vp, vp]
+    r = N.lib.dcvc_recover
+    r.restype, r.argtypes = i, [vp, vp, vp, i, vp, vp]
+    ok = 0x10000  # an aligned stand-in address; never dereferenced because a check fails first
+    cases = [
+        (None, 2, ok, ok, ok, ok),      # null src
+        (ok, 2, None, ok, ok, ok),      # null cond
+        (ok, 2, ok, ok, None, ok),      # null dst
+        (ok, 2, ok, ok, ok, None),      # null total
+        (ok, 2, ok + 4, ok, ok, ok),    # cond not 8-byte aligned
+        (ok + 1, 2, ok, ok, ok, ok),    # 2-byte src misaligned
+        (ok, 2, ok, ok, ok + 1, ok),    # 2-byte dst misaligned
+        (ok, 2, ok, ok, ok, ok + 2),    # total misaligned
+        (ok, 3, ok, ok, ok, ok),        # element size
+    ]
+    for src, eb, cond, counts, dst, total in cases:
+        assert f(src, eb, cond, 1000, counts, dst, total, None) == 1, (src, eb, cond, dst, total)
+        assert b"alignment" in N.lib.dcvc_last_error()
+        assert g(src, eb, cond, 1000, dst, total, None) == 1, (src, eb, cond, dst, total)
+    assert f(ok, 2, ok, 1000, None, ok, ok, None) == 1        # null block counts
+    assert f(ok, 2, ok, 0, ok, ok, ok, None) == 1             # empty input
+    assert r(ok, ok, None, 1000, ok, None) == 1               # recover: null block counts
+    assert r(ok, ok, ok, 1000, ok + 1, None) == 1             # recover: misaligned FP16 output
+    assert r(None, ok, ok, 1000, ok, None) == 1               # recover: null decoded values

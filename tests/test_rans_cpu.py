@@ -187,3 +187,34 @@ def test_worker_exception_is_reported_and_the_coder_recovers(gold, sub_stream):
     dec.decode_z(nz, qp * 128, 128)
     assert np.array_equal(dec.get_decoded_tensor(), z)
     M.inject_task_fault(-1)
+
+
+def test_long_bypass_runs_in_corrupt_payloads_decode_like_the_oracle():
+    """Random payloads decoded under a table whose escape symbol covers all but one code point:
+    nearly every symbol takes the 2-bit bypass path, so runs of 16 digits (which can set bit 31
+    of the escaped value, making it negative) occur.  The product decoder and the C oracle must
+    give the same symbols for every one of them, including the negative-value cases."""
+    lib = oracle_lib()
+    qz = np.zeros((1, 3), np.int32)
+    qz[0] = [0, 1, 65536]
+    lz = np.array([3], np.int32)
+    qy, ly = qz.copy(), lz.copy()
+    enc, dec = _coders(qy, ly, qz, lz)
+    rng = np.random.default_rng(11)
+    n = 40000
+    negative_cases = 0
+    for trial in range(6):
+        data = rng.integers(0, 256, 1 << 20).astype(np.uint8)
+        dec.set_entropy_coder_parallel(1)
+        dec.set_stream(data)
+        dec.decode_z(n, 0, 1)
+        got = dec.get_decoded_tensor().copy()
+        zo = np.zeros(n, np.int8)
+        yo = np.zeros(1, np.int8)
+        idx = np.zeros(1, np.uint8)
+        rc = lib.oracle_decode(_p(qz), _p(lz), qz.shape[1], _p(qy), _p(ly), qy.shape[1],
+                               _p(data), data.size, _p(idx), 0, n, 0, 1, 1, _p(yo), _p(zo))
+        assert rc == 0
+        assert np.array_equal(got, zo), trial
+        negative_cases += int((np.abs(got.astype(np.int32)) > 64).sum())
+    assert negative_cases > 0  # long runs were exercised, not only short escapes

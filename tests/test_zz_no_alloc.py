@@ -5,9 +5,11 @@ process whose device memory is pre-partitioned by its own allocator, or a latenc
 that cannot take cudaMalloc's implicit synchronisation — and so cannot provide the per-call
 block-count buffer that dcvc_compact needs.  Its scratch is a fixed array inside the library.
 Two calls in a row (the second sees the first call's leftover scratch) must give exactly the
-same result as dcvc_compact with a caller buffer; sizes beyond the built-in maximum are refused.
-This file is collected last on purpose."""
+same result as dcvc_compact with a caller buffer and as the CPU oracle's compaction; sizes beyond
+the built-in maximum are refused.  This file is collected last on purpose."""
 import ctypes
+import os
+import sys
 
 import numpy as np
 import pytest
@@ -16,6 +18,8 @@ import torch
 pytestmark = pytest.mark.gpu
 
 MAX_ELEMENTS = 4096 * 8192
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle"))
+import elementwise_oracle  # noqa: E402
 
 
 def _lib():
@@ -56,6 +60,8 @@ def test_no_alloc_compaction_matches_compact_twice():
         k = int(ref_total.item())
         assert int(total.item()) == k == int(cond.sum().item())
         assert torch.equal(dst[:k], ref_dst[:k])
+        want, kw = elementwise_oracle.compact(src.cpu().numpy(), cond.cpu().numpy())
+        assert kw == k and np.array_equal(dst[:k].cpu().numpy(), want)
 
 
 def test_no_alloc_rejects_sizes_beyond_its_scratch():
