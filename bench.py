@@ -178,9 +178,10 @@ def measured_peaks():
         return 6650.0, 1590.0, "fallback"
 
 
-def profiled_traffic():
-    """DRAM bytes per launch of the quad GEMM from the committed ncu summary, or None."""
-    path = os.path.join(ROOT, "profiles", "gemm_quad_1080p.md")
+def profiled_traffic(name):
+    """DRAM bytes per launch of a kernel from its committed ncu summary
+    (profiles/<name>.md, line `traffic_bytes_per_launch: N`), or None."""
+    path = os.path.join(ROOT, "profiles", name + ".md")
     try:
         for line in open(path):
             if line.startswith("traffic_bytes_per_launch:"):
@@ -190,35 +191,67 @@ def profiled_traffic():
     return None
 
 
-def roofline_quad(stream):
-    """Times the dominant kernel (the quad GEMM of the 512-channel blocks at 1080p) on its
-    launching stream with CUDA events and relates it to the measured tensor peak."""
-    from dcvc_b200 import _native as N, ops
-    M, Nn, K = QUAD_SHAPE
-    g = torch.Generator(device="cuda").manual_seed(7)
-    a = torch.randn(M, K, device="cuda", generator=g).half()
-    w = (torch.randn(Nn, K, device="cuda", generator=g) / K ** 0.5).half()
-    b = torch.zeros(Nn, device="cuda")
-    out = torch.empty(M, Nn // 4, device="cuda", dtype=torch.float16)
+def _time_rotating(stream, launches, reps=60):
+    """Average device time of `launches` (callables over independent operand sets, cycled so
+    that consecutive launches read different buffers whose sum exceeds the L2) on `stream`, CUDA
+    events around `reps` launches after a warm-up."""
     with torch.cuda.stream(stream):
-        for _ in range(5):
-            ops.conv1x1(a, w, b, N.EPI_QUAD, out=out)
+        for i in range(2 * len(launches)):
+            launches[i % len(launches)]()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        reps = 50
         e0.record(stream)
-        for _ in range(reps):
-            ops.conv1x1(a, w, b, N.EPI_QUAD, out=out)
+        for i in range(reps):
+            launches[i % len(launches)]()
         e1.record(stream)
     e1.synchronize()
-    sec = e0.elapsed_time(e1) / 1e3 / reps
-    flops = 2.0 * M * Nn * K
-    _, peak_tf, kind = measured_peaks()
-    achieved = flops / sec / 1e12
-    return {"kernel": "gemm_sm100_kernel<half, 256, quad> (ffn.0 + WSiLU chunk-add, M=32640 N=1024 K=512)",
-            "bound": "tensor", "achieved": round(achieved, 1), "peak": peak_tf, "unit": "TFLOP/s",
-            "frac": round(achieved / peak_tf, 3), "peak_kind": f"{kind} bf16 burst",
-            "us_per_launch": round(sec * 1e6, 2), "flops_per_launch": flops,
-            "traffic": profiled_traffic()}
+    return e0.elapsed_time(e1) / 1e3 / reps
+
+
+def roofline(stream):
+    """The two largest kernels of the 1080p chunk, timed standalone on their launching stream
+    with CUDA events at their 1080p shapes and the library's own choice of kernel form:
+    the residual GEMM (dc.3 / ffn.2 of a 512-channel block, M=32640 N=512 K=256 + residual;
+    HBM-bound, the largest share of the chunk in the launch list) and the quad GEMM (ffn.0 +
+    WSiLU chunk-add, M=32640 N=1024 K=512; tensor-bound).  Operand sets rotate through more
+    than the 126 MB L2, so inputs come from HBM.  Returns (dominant, [others])."""
+    from dcvc_b200 import _native as N, ops
+    hbm, peak_tf, kind = measured_peaks()
+    g = torch.Generator(device="cuda").manual_seed(7)
+    M = QUAD_SHAPE[0]
+
+    def rnd(*shape, scale=1.0):
+        return (torch.randn(*shape, device="cuda", generator=g) * scale).half()
+
+    # residual GEMM: three operand sets of 83.5 MB
+    res_launch = []
+    for _ in range(3):
+        a, w = rnd(M, 256), rnd(512, 256, scale=256 ** -0.5)
+        r, o = rnd(M, 512), torch.empty(M, 512, device="cuda", dtype=torch.float16)
+        b = torch.zeros(512, device="cuda")
+        res_launch.append(lambda a=a, w=w, b=b, r=r, o=o: ops.conv1x1(a, w, b, N.EPI_BIAS_RES, res=r, out=o))
+    sec = _time_rotating(stream, res_launch)
+    byts = (M * 256 + 512 * 256 + 2 * M * 512) * 2
+    res = {"kernel": "residual GEMM dc.3 / ffn.2 (M=32640 N=512 K=256 + bias + residual) in the "
+                     "form the library picks for it",
+           "bound": "hbm", "achieved": round(byts / sec / 1e9, 1), "peak": hbm, "unit": "GB/s",
+           "frac": round(byts / sec / 1e9 / hbm, 3), "peak_kind": f"{kind} HBM copy",
+           "us_per_launch": round(sec * 1e6, 2), "bytes_per_launch": byts,
+           "traffic": profiled_traffic("gemm_res_1080p")}
+    # quad GEMM: three operand sets (A 33.4 MB + out 16.7 MB each, plus the 1 MB weights)
+    quad_launch = []
+    for _ in range(3):
+        a, w = rnd(M, 512), rnd(1024, 512, scale=512 ** -0.5)
+        o = torch.empty(M, 256, device="cuda", dtype=torch.float16)
+        b = torch.zeros(1024, device="cuda")
+        quad_launch.append(lambda a=a, w=w, b=b, o=o: ops.conv1x1(a, w, b, N.EPI_QUAD, out=o))
+    sec = _time_rotating(stream, quad_launch)
+    flops = 2.0 * M * 1024 * 512
+    quad = {"kernel": "gemm_sm100_kernel<half, 256, quad> (ffn.0 + WSiLU chunk-add, M=32640 N=1024 K=512)",
+            "bound": "tensor", "achieved": round(flops / sec / 1e12, 1), "peak": peak_tf,
+            "unit": "TFLOP/s", "frac": round(flops / sec / 1e12 / peak_tf, 3),
+            "peak_kind": f"{kind} bf16 burst", "us_per_launch": round(sec * 1e6, 2),
+            "flops_per_launch": flops, "traffic": profiled_traffic("gemm_quad_1080p")}
+    return res, [quad]
 
 
 class ReferenceCpuPath:
@@ -303,6 +336,113 @@ def cpu_baseline(H, W, chunks=2):
     return {"value": round(FRAMES * chunks / sec, 4), "unit": UNIT, "cores": path.threads,
             "kind": "port",
             "sample": f"{chunks} {path.describe()}; {sec:.1f} s timed after one untimed chunk"}
+
+
+def precision_forms(stream, H, W, xs, steps, warmup, forms=("bf16", "fp8")):
+    """The headline workload (one 8-frame chunk compressed and decompressed per step, QPs cycling
+    0/21/42/63, inputs resident) in the other precision forms, device-timed like `value`."""
+    from dcvc_b200 import synthetic
+    from dcvc_b200.entropy_tables import add_cdf_to_state_dict
+    from dcvc_b200.inference_extensions_cuda import DMCHTSProxy
+    from dcvc_b200.model_spec import calibrated_hts_state_dict
+    sd = add_cdf_to_state_dict(calibrated_hts_state_dict(0))
+    sd = {k: (v.half().cuda() if v.is_floating_point() else v) for k, v in sd.items()}
+    pr, pb = synthetic.padding_for(H, W)
+    ref = synthetic.padded_reference_frame(synthetic.video_chunk_yuv420(2, H, W, 1, 0)[0])
+    out = {}
+    for form in forms:
+        enc, dec = DMCHTSProxy(form), DMCHTSProxy(form)
+        enc.set_param(sd, SKIP_THRES)
+        dec.set_param(sd, SKIP_THRES)
+        enc.add_ref_feature_from_frame(ref, True)
+        dec.add_ref_feature_from_frame(ref, False)
+        nbytes = []
+
+        def step(i):
+            qp = QPS[i % len(QPS)]
+            bits, ecp = enc.compress(xs[i % 2], qp, False, pb, pr)
+            dec.decompress(bits, qp, H, W, ecp, False)
+            nbytes.append(bits.size)
+
+        with torch.cuda.stream(stream):
+            for i in range(warmup):
+                step(i)
+            torch.cuda.synchronize()
+            nbytes.clear()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for i in range(steps):
+                step(warmup + i)
+            e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        out[form] = {"value": round(FRAMES * steps / (ms / 1e3), 2), "unit": UNIT,
+                     "ms_per_step": round(ms / steps, 3), "bytes_per_chunk": int(np.mean(nbytes))}
+        del enc, dec
+    return out
+
+
+def parity_vs_fp64_oracle(H, W, forms=("fp16", "bf16", "fp8")):
+    """Error of every precision form against the FP64 oracle (oracle/hts_oracle.py on the host
+    cores) on the benchmark's workload: from one reference frame, the four chunks with QPs
+    0/21/42/63 in order, independent temporal state on each side.  Per QP and form: PSNR delta
+    (mean over the 8 frames, (6Y+U+V)/8), payload-size delta in percent, fraction of quantised
+    latents equal to the oracle's, and whether the decoder reproduced the encoder's symbols
+    exactly."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import hts_oracle
+    from dcvc_b200 import synthetic
+    from dcvc_b200.entropy_tables import add_cdf_to_state_dict
+    from dcvc_b200.inference_extensions_cuda import DMCHTSProxy
+    from dcvc_b200.model_spec import calibrated_hts_state_dict
+    torch.set_num_threads(os.cpu_count() or 1)
+    sd = add_cdf_to_state_dict(calibrated_hts_state_dict(0))
+    sd = {k: (v.half() if v.is_floating_point() else v) for k, v in sd.items()}
+    sd_dev = {k: (v.cuda() if v.is_floating_point() else v) for k, v in sd.items()}
+    pr, pb = synthetic.padding_for(H, W)
+    ref_frame = synthetic.video_chunk_yuv420(2, H, W, 1, 0)[0]
+    chunks = [synthetic.video_chunk_yuv420(2, H, W, FRAMES, FRAMES * k) for k in range(len(QPS))]
+
+    def psnr(xs, frames):
+        return float(np.mean([hts_oracle.psnr_yuv420(xs[i].float().cpu(), *frames[i])[0]
+                              for i in range(len(frames))]))
+
+    t0 = time.perf_counter()
+    oe = hts_oracle.HtsOracle(sd, SKIP_THRES, torch.float64)
+    od = hts_oracle.HtsOracle(sd, SKIP_THRES, torch.float64)
+    ref_cpu = synthetic.padded_reference_frame(ref_frame, device="cpu")
+    oe.add_ref_feature_from_frame(ref_cpu, True)
+    od.add_ref_feature_from_frame(ref_cpu, False)
+    oracle = []
+    for qp, frames in zip(QPS, chunks):
+        r = oe.compress(synthetic.to_model_input(frames, device="cpu"), qp, False, pb, pr)
+        d = od.decompress(r["bit_stream"], qp, H, W, r["ec_parallel"], False)
+        oracle.append((r["bit_stream"].size, psnr(d["x_hat"], frames),
+                       r["y_q"][0].permute(1, 2, 0).reshape(-1, 256).float()))
+    oracle_s = time.perf_counter() - t0
+    out = {"oracle": "FP64 restatement of the HT-S proxy dataflow on the host cores",
+           "oracle_seconds": round(oracle_s, 1), "qps": list(QPS), "forms": {}}
+    for form in forms:
+        enc, dec = DMCHTSProxy(form), DMCHTSProxy(form)
+        enc.set_param(sd_dev, SKIP_THRES)
+        dec.set_param(sd_dev, SKIP_THRES)
+        ref = synthetic.padded_reference_frame(ref_frame)
+        enc.add_ref_feature_from_frame(ref, True)
+        dec.add_ref_feature_from_frame(ref, False)
+        rows = []
+        for (qp, frames), (ob, po, oq) in zip(zip(QPS, chunks), oracle):
+            bits, ecp = enc.compress(synthetic.to_model_input(frames), qp, False, pb, pr)
+            x_hat = dec.decompress(bits, qp, H, W, ecp, False)
+            torch.cuda.synchronize()
+            exact = all(torch.equal(enc.buffer(n).view(torch.int16), dec.buffer(n).view(torch.int16))
+                        for n in ("common", "y_q", "y_hat"))
+            agree = float((enc.buffer("y_q").float().cpu() == oq).float().mean())
+            rows.append({"qp": qp, "dpsnr_db": round(psnr(x_hat, frames) - po, 4),
+                         "dbpp_pct": round(100.0 * (bits.size - ob) / ob, 3),
+                         "latent_agree": round(agree, 5), "round_trip_exact": exact})
+        out["forms"][form] = rows
+        del enc, dec
+    return out
 
 
 def batched_streams(args, H, W, n_streams):
@@ -859,8 +999,10 @@ def run_gpu(args):
 
     # ---------------- encode alone and decode alone (the reference publishes them separately)
     split = split_enc_dec(enc, dec, xs, args, pb, pr, H, W, stream)
+    # ---------------- the same workload in the BF16 and FP8 precision forms
+    forms = _section(precision_forms, stream, H, W, xs, args.steps, args.warmup)
     clk = clocks.stop(windows)
-    roof = roofline_quad(stream)
+    roof, roof_others = roofline(stream)
     # The extra measurements below report a failure in their own key instead of losing the line
     # (and every rank still reaches the closing barrier).
     intra = None if args.no_intra else _section(intra_bench, stream, H, W)
@@ -876,8 +1018,10 @@ def run_gpu(args):
         serving = _section(serving_bench, args)
     _empty_cache()
     cpu = None
+    parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(H, W)
+        parity = _section(parity_vs_fp64_oracle, H, W)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -893,6 +1037,7 @@ def run_gpu(args):
                        "p99": round(float(np.percentile(lat_sorted, 99)), 3)},
         "bytes_per_chunk": {"mean": int(np.mean(nbytes)), "min": int(min(nbytes)), "max": int(max(nbytes))},
         "enc_decomposed_fps": split,
+        "precision_forms": forms,
         "batched": batched,
         "serving": serving,
         "reference_published": PUBLISHED,
@@ -904,8 +1049,10 @@ def run_gpu(args):
                       "stream, double-buffered, inside the timed region"},
         "gpu_launches": kernels_per_step * args.steps,
         "roofline": roof,
+        "roofline_others": roof_others,
         "clocks": clk,
         "cpu_baseline": cpu,
+        "parity": parity,
     }
     print(json.dumps(out), flush=True)
 

@@ -43,6 +43,41 @@ int dcvc_device_error(int* code, int clear)
     return st;
 }
 
+int dcvc_check_device_errors(void* stream)
+{
+    int* w = device_error_word();
+    if (w == nullptr) {
+        set_last_error("dcvc_check_device_errors: no device error word");
+        return kCudaError;
+    }
+    int st = cuda_status(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)),
+                         "dcvc_check_device_errors");
+    if (st != kOk) {
+        return st;
+    }
+    int code = 0;
+    st = cuda_status(cudaMemcpy(&code, w, sizeof(int), cudaMemcpyDeviceToHost), "dcvc_check_device_errors");
+    if (st != kOk) {
+        return st;
+    }
+    if (code != 0) {
+        cudaMemset(w, 0, sizeof(int));
+        set_last_error("a kernel's bounded wait gave up (device error " + std::to_string(code) + ")");
+        return kDeviceTimeout;
+    }
+    return kOk;
+}
+
+int dcvc_gemm_inject_stall(int launches, long long wait_limit_cycles)
+{
+    if (launches > 0 && wait_limit_cycles <= 0) {
+        set_last_error("dcvc_gemm_inject_stall: the wait limit must be positive");
+        return kInvalidArgument;
+    }
+    gemm_inject_stall(launches, wait_limit_cycles);
+    return kOk;
+}
+
 int dcvc_scale_index_table(uint8_t* lut)
 {
     if (lut == nullptr) {

@@ -2,6 +2,7 @@
 #include "gemm_sm100.cuh"
 #include "host_util.h"
 
+#include <atomic>
 #include <cstring>
 #include <mutex>
 
@@ -122,6 +123,8 @@ __global__ void __launch_bounds__(GemmCfg<BN, EPI>::kThreads, 1)
                       const __grid_constant__ CUtensorMap tmR2, const GemmParams p)
 {
     constexpr int kKElems = F8 ? 128 : kBK;  // K elements per 128-byte K block
+    // progress waits give up after `lim` cycles; the drains after an abort keep the full limit
+    const long long lim = p.wait_limit > 0 ? p.wait_limit : kWaitLimit;
     using C = GemmCfg<BN, EPI>;
     constexpr int kStages = C::kStages;
     extern __shared__ uint8_t smem_raw[];
@@ -177,7 +180,7 @@ __global__ void __launch_bounds__(GemmCfg<BN, EPI>::kThreads, 1)
 
     if (warp == 0) {
         // ------------------------------------------------------------ TMA producer
-        if (lane == 0) {
+        if (lane == 0 && !p.stall_test) {
             int stage = 0;
             uint32_t phase = 0;
             int issued = 0;
@@ -185,7 +188,7 @@ __global__ void __launch_bounds__(GemmCfg<BN, EPI>::kThreads, 1)
                 const int m0 = (tile % num_m) * kBM;
                 const int n0 = (tile / num_m) * BN;
                 for (int kb = 0; kb < kblocks; ++kb) {
-                    if (!mbar_wait_bounded(&empty[stage], phase ^ 1, kWaitLimit)) {
+                    if (!mbar_wait_bounded(&empty[stage], phase ^ 1, lim)) {
                         *abort_flag = 1;
                         report_error(p.err, kErrGemmProducerTimeout);
                         break;
@@ -224,7 +227,7 @@ __global__ void __launch_bounds__(GemmCfg<BN, EPI>::kThreads, 1)
             uint32_t acc_phase = 0;
             bool issued_any = false;
             for (int tile = blockIdx.x; tile < num_tiles && !*abort_flag; tile += gridDim.x) {
-                if (!mbar_wait_bounded(&tempty[acc], acc_phase ^ 1, kWaitLimit)) {
+                if (!mbar_wait_bounded(&tempty[acc], acc_phase ^ 1, lim)) {
                     *abort_flag = 1;
                     report_error(p.err, kErrGemmMmaTimeout);
                     break;
@@ -232,7 +235,7 @@ __global__ void __launch_bounds__(GemmCfg<BN, EPI>::kThreads, 1)
                 tc_fence_after();
                 const uint32_t d = tmem_base + static_cast<uint32_t>(acc * BN);
                 for (int kb = 0; kb < kblocks; ++kb) {
-                    if (!mbar_wait_bounded(&full[stage], phase, kWaitLimit)) {
+                    if (!mbar_wait_bounded(&full[stage], phase, lim)) {
                         *abort_flag = 1;
                         report_error(p.err, kErrGemmMmaTimeout);
                         break;
@@ -323,7 +326,7 @@ __global__ void __launch_bounds__(GemmCfg<BN, EPI>::kThreads, 1)
             const int row0 = m0 + quad * 32;        // first row owned by this warp
             const bool rows_live = row0 < p.M;
             const int nacc0 = n0 + half * C::kCols;  // first accumulator column of this warp
-            if (!mbar_wait_bounded(&tfull[acc], acc_phase, kWaitLimit)) {
+            if (!mbar_wait_bounded(&tfull[acc], acc_phase, lim)) {
                 *abort_flag = 1;
                 report_error(p.err, kErrGemmEpilogueTimeout);
                 break;
@@ -386,7 +389,7 @@ __global__ void __launch_bounds__(GemmCfg<BN, EPI>::kThreads, 1)
                     uint8_t* out_buf = epi_has_res(EPI) ? res_slot(slot) : wbuf;
                     if constexpr (epi_has_res(EPI)) {
                         if (rows_live) {
-                            if (!mbar_wait_bounded(&rbar[slot], (res_phase >> slot) & 1u, kWaitLimit)) {
+                            if (!mbar_wait_bounded(&rbar[slot], (res_phase >> slot) & 1u, lim)) {
                                 *abort_flag = 1;
                                 report_error(p.err, kErrGemmEpilogueTimeout);
                             } else {
@@ -642,11 +645,37 @@ int gemm_pick_bn(int M, int N, int epi, int sub_cout)
     return 0;
 }
 
+namespace {
+std::atomic<int> g_stall_launches{0};
+std::atomic<long long> g_stall_limit{0};
+}  // namespace
+
+void gemm_inject_stall(int launches, long long wait_limit_cycles)
+{
+    g_stall_limit.store(wait_limit_cycles);
+    g_stall_launches.store(launches > 0 ? launches : 0);
+}
+
+GemmParams gemm_apply_injection(const GemmParams& p)
+{
+    GemmParams q = p;
+    int n = g_stall_launches.load();
+    while (n > 0 && !g_stall_launches.compare_exchange_weak(n, n - 1)) {
+    }
+    if (n > 0) {
+        q.stall_test = 1;
+        q.wait_limit = g_stall_limit.load();
+    }
+    return q;
+}
+
 // Host launcher.  A: [M, K] with row pitch lda (elements); W: [N, K] dense.  dtype 0 = f16,
-// 1 = bf16.  Returns cudaSuccess or an error (shape/alignment problems -> cudaErrorInvalidValue).
-cudaError_t gemm_sm100(int dtype, const void* A, int lda, const void* W, const GemmParams& p,
+// 1 = bf16, 2 = E4M3 operands with BF16 output.  Returns cudaSuccess or an error
+// (shape/alignment problems -> cudaErrorInvalidValue).
+cudaError_t gemm_sm100(int dtype, const void* A, int lda, const void* W, const GemmParams& p_in,
                        int epi, int bn, cudaStream_t stream)
 {
+    const GemmParams p = gemm_apply_injection(p_in);
     const bool f8 = dtype == kDtypeF8;
     if (dtype < 0 || dtype > kDtypeF8 || p.M <= 0 || p.N <= 0 || p.K <= 0 ||
         p.K % (f8 ? 128 : kBK) != 0 || lda % (f8 ? 16 : 8) != 0 ||

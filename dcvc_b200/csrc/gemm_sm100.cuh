@@ -49,7 +49,19 @@ struct GemmParams {
     // FP8 form (dtype 2): per-output-channel FP32 factor applied to the accumulator before the
     // bias, the product of the weight row's and the activation's quantisation scales
     const float* wscale = nullptr;
+    // Bounded-wait limit of the progress waits in SM clock cycles (0: about one second), and a
+    // failure-detection test switch: the producer issues no loads, so the MMA and epilogue waits
+    // run out, the kernel records DCVC_DEVICE_TIMEOUT in the error word and returns.  Set only
+    // through gemm_inject_stall.
+    long long wait_limit = 0;
+    int stall_test = 0;
 };
+
+// The next `launches` GEMM launches of this process run with stall_test set and the given wait
+// limit (failure-detection tests; launches <= 0 cancels).
+void gemm_inject_stall(int launches, long long wait_limit_cycles);
+// Applies a pending injection to a launch's parameters (used by the GEMM launchers).
+GemmParams gemm_apply_injection(const GemmParams& p);
 
 // dtype of gemm_sm100 / dcvc_conv1x1 for E4M3 operands with FP32 accumulation and BF16 output.
 constexpr int kDtypeF8 = 2;

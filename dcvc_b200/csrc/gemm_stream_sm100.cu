@@ -129,6 +129,8 @@ __global__ void __launch_bounds__(kSThreads, 1)
     cta_rows(p.M, blockIdx.x % ctas_per_slice, ctas_per_slice, &r0, &r1);
     const int ntiles = r1 > r0 ? (r1 - r0 + kSBM - 1) / kSBM : 0;
     const int kblocks = p.K / kSBK;
+    // progress waits give up after `lim` cycles; the drains after an abort keep the full limit
+    const long long lim = p.wait_limit > 0 ? p.wait_limit : kSWaitLimit;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < kSStages; ++s) {
@@ -164,7 +166,7 @@ __global__ void __launch_bounds__(kSThreads, 1)
 
     if (warp == 0) {
         // ------------------------------------------------------------ TMA producer
-        if (lane == 0 && ntiles > 0) {
+        if (lane == 0 && ntiles > 0 && !p.stall_test) {
             // the W slice once: kblocks boxes of 128 rows x 64 K
             mbar_arrive_expect_tx(bfull, static_cast<uint32_t>(kblocks * kSBN * kSBK * 2));
             for (int kb = 0; kb < kblocks; ++kb) {
@@ -176,7 +178,7 @@ __global__ void __launch_bounds__(kSThreads, 1)
             for (int t = 0; t < ntiles && !*abort_flag; ++t) {
                 const int m0 = r0 + t * kSBM;
                 for (int kb = 0; kb < kblocks; ++kb) {
-                    if (!mbar_wait_bounded(&empty[stage], phase ^ 1, kSWaitLimit)) {
+                    if (!mbar_wait_bounded(&empty[stage], phase ^ 1, lim)) {
                         *abort_flag = 1;
                         report_error(p.err, kErrGemmProducerTimeout);
                         break;
@@ -212,13 +214,13 @@ __global__ void __launch_bounds__(kSThreads, 1)
             int acc = 0;
             uint32_t acc_phase = 0;
             bool issued_any = false;
-            if (!mbar_wait_bounded(bfull, 0, kSWaitLimit)) {
+            if (!mbar_wait_bounded(bfull, 0, lim)) {
                 *abort_flag = 1;
                 report_error(p.err, kErrGemmMmaTimeout);
             }
             tc_fence_after();
             for (int t = 0; t < ntiles && !*abort_flag; ++t) {
-                if (!mbar_wait_bounded(&tempty[acc], acc_phase ^ 1, kSWaitLimit)) {
+                if (!mbar_wait_bounded(&tempty[acc], acc_phase ^ 1, lim)) {
                     *abort_flag = 1;
                     report_error(p.err, kErrGemmMmaTimeout);
                     break;
@@ -226,7 +228,7 @@ __global__ void __launch_bounds__(kSThreads, 1)
                 tc_fence_after();
                 const uint32_t d = tmem_base + static_cast<uint32_t>(acc * kSBN);
                 for (int kb = 0; kb < kblocks; ++kb) {
-                    if (!mbar_wait_bounded(&full[stage], phase, kSWaitLimit)) {
+                    if (!mbar_wait_bounded(&full[stage], phase, lim)) {
                         *abort_flag = 1;
                         report_error(p.err, kErrGemmMmaTimeout);
                         break;
@@ -310,14 +312,14 @@ __global__ void __launch_bounds__(kSThreads, 1)
             const int row0 = r0 + t * kSBM + quad * 32;
             const bool rows_live = row0 < r1;
             uint8_t* buf = wbuf + slot * C::kSlotBytes;
-            if (!mbar_wait_bounded(&tfull[acc], acc_phase, kSWaitLimit)) {
+            if (!mbar_wait_bounded(&tfull[acc], acc_phase, lim)) {
                 *abort_flag = 1;
                 report_error(p.err, kErrGemmEpilogueTimeout);
                 break;
             }
             tc_fence_after();
             if (rows_live) {
-                if (!mbar_wait_bounded(&rbar[slot], (res_phase >> slot) & 1u, kSWaitLimit)) {
+                if (!mbar_wait_bounded(&rbar[slot], (res_phase >> slot) & 1u, lim)) {
                     *abort_flag = 1;
                     report_error(p.err, kErrGemmEpilogueTimeout);
                 } else {

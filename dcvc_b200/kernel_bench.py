@@ -1,8 +1,10 @@
 """Micro-benchmark of the codec's kernels at their 1080p shapes (CUDA events on the launching
 stream), also the small fixed case used for ncu captures.
 
-    python -m dcvc_b200.kernel_bench [--case quad|wsilu|res|bias2048|dwconv|ffn|ffn_ld|rans|all] [--reps N]
-                                     [--sets S] [--bn 0|64|128|256]
+    python -m dcvc_b200.kernel_bench [--case quad|quad_f8|wsilu|res|bias2048|dwconv|ffn|ffn_ld|rans|all]
+                                     [--reps N] [--sets S] [--bn 0|64|128|256|-1]
+
+(--bn -1 selects the streaming form of the residual GEMM.)
 
 Consecutive launches cycle through S independent operand sets (default: enough sets for 300 MB),
 so the timed launches read their inputs from HBM rather than from the 126 MB L2, as they do
@@ -39,6 +41,16 @@ def _case(name, g, bn=0):
         out = torch.empty_like(x)
         fn = lambda: ops.conv_ffn(x, w1, b1, w2, b2, out=out, block_n=bn)  # noqa: E731
         return fn, 2.0 * M8 * (4 * cf * C + C * cf), (2 * x.numel() + w1.numel() + w2.numel()) * 2
+    if name == "quad_f8":
+        # ffn.0 of a 512-channel block in the FP8 form: E4M3 operands, per-row scales, BF16 out
+        a = rnd(M8, 512).to(torch.float8_e4m3fn)
+        w = rnd(1024, 512, scale=512 ** -0.5)
+        ws = (w.float().abs().amax(1) / 448.0).contiguous()
+        wq = (w.float() / ws[:, None]).to(torch.float8_e4m3fn)
+        b = torch.zeros(1024, device="cuda")
+        out = torch.empty(M8, 256, device="cuda", dtype=torch.bfloat16)
+        fn = lambda: ops.conv1x1_f8(a, wq, ws, b, N.EPI_QUAD, out=out, block_n=bn)  # noqa: E731
+        return fn, 2.0 * M8 * 1024 * 512, (M8 * 512 + 1024 * 512) + M8 * 256 * 2
     if name == "dwconv":
         x = rnd(M8, 256)
         w = torch.randn(9, 256, device="cuda", generator=g)
@@ -171,7 +183,8 @@ def main():
     ap.add_argument("--case", default="all")
     ap.add_argument("--reps", type=int, default=20)
     ap.add_argument("--sets", type=int, default=0)
-    ap.add_argument("--bn", type=int, default=0, help="GEMM N tile (0 = the library's choice)")
+    ap.add_argument("--bn", type=int, default=0,
+                    help="GEMM N tile (0 = the library's choice, -1 = streaming residual form)")
     args = ap.parse_args()
     cases = ["quad", "wsilu", "res", "bias2048", "dwconv", "ffn"] if args.case == "all" else [args.case]
     for c in cases:

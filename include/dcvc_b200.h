@@ -66,6 +66,16 @@ int dcvc_abi_version(void);
 /* Reads (and optionally clears) the device error word that kernels set when one of their
  * bounded waits gave up.  *code = 0 means no error.  Synchronises the device. */
 int dcvc_device_error(int* code, int clear);
+/* Synchronises `stream`, then returns DCVC_DEVICE_TIMEOUT (and clears the word) if a kernel's
+ * bounded wait gave up, else DCVC_OK.  The reference has no bounded waits (its proxy can wait
+ * for ever, dmc_hts_proxy.cpp:579); no counterpart there. */
+int dcvc_check_device_errors(void* stream);
+/* Failure-detection test hook: the next `launches` GEMM launches (dcvc_conv1x1 and the codecs'
+ * GEMMs) issue no operand loads and give their progress waits a limit of wait_limit_cycles SM
+ * clocks, so the waits run out: the kernel records the timeout in the device error word, drains
+ * only the copies it issued, frees its tensor memory and returns, and the GPU stays usable.
+ * launches <= 0 cancels.  No counterpart in the reference. */
+int dcvc_gemm_inject_stall(int launches, long long wait_limit_cycles);
 
 /* ------------------------------------------------------------------ kernels */
 

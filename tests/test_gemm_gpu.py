@@ -177,3 +177,32 @@ def test_conv1x1_f8_matches_dequantised_fp32(name, M, Nn, K, bn):
     ref = _ref(epi, ad, wd, b)
     err = (out.float() - ref).abs()
     assert bool((err <= 6e-2 + 2e-2 * ref.abs()).all()), float(err.max())
+
+
+@pytest.mark.parametrize("form", ["tiled", "stream"])
+def test_bounded_wait_runs_out_and_the_gpu_keeps_answering(form):
+    """A GEMM whose producer issues no loads (injected) must give up on its waits after the short
+    limit, report DCVC_DEVICE_TIMEOUT through the error word, and leave the context usable: the
+    same GEMM right after it gives the right result.  No trap, no fault, no hang."""
+    import ctypes
+    from dcvc_b200 import _native as N, ops
+    lib = N.lib
+    lib.dcvc_gemm_inject_stall.argtypes = [ctypes.c_int, ctypes.c_longlong]
+    lib.dcvc_check_device_errors.argtypes = [ctypes.c_void_p]
+    g = torch.Generator(device="cuda").manual_seed(9)
+    M, Nn, K = 4096, 512, 256
+    a = torch.randn(M, K, device="cuda", generator=g).half()
+    w = (torch.randn(Nn, K, device="cuda", generator=g) / K ** 0.5).half()
+    b = torch.randn(Nn, device="cuda", generator=g) * 0.1
+    res = torch.randn(M, Nn, device="cuda", generator=g).half()
+    epi, bn = (N.EPI_BIAS, 256) if form == "tiled" else (N.EPI_BIAS_RES, N.BLOCK_N_STREAM)
+    stream = torch.cuda.current_stream().cuda_stream
+    assert lib.dcvc_check_device_errors(stream) == 0
+    assert lib.dcvc_gemm_inject_stall(1, 20000) == 0  # ~10 us at 2 GHz
+    ops.conv1x1(a, w, b, epi, res=res, block_n=bn)
+    assert lib.dcvc_check_device_errors(stream) == 3  # DCVC_DEVICE_TIMEOUT
+    assert b"bounded wait" in lib.dcvc_last_error()
+    out = ops.conv1x1(a, w, b, epi, res=res, block_n=bn)
+    assert lib.dcvc_check_device_errors(stream) == 0
+    ref = _ref(epi, a, w, b, res)
+    assert bool(((out.float() - ref).abs() <= 2e-2 + 1e-2 * ref.abs()).all())
