@@ -52,8 +52,10 @@ def parse_args():
     ap.add_argument("--no-intra", action="store_true", help="skip the intra-codec measurement")
     ap.add_argument("--no-htl", action="store_true", help="skip the HT-L measurement")
     ap.add_argument("--no-ld", action="store_true", help="skip the low-delay (LD) measurement")
-    ap.add_argument("--streams", type=int, default=4,
-                    help="concurrent streams of the batched form (0 skips it)")
+    ap.add_argument("--batch-streams", type=int, default=32,
+                    help="streams of the batching form (0 skips it)")
+    ap.add_argument("--batch-precision", default="bf16", choices=["fp16", "bf16", "fp8"],
+                    help="precision form of the batching form's packed codecs")
     ap.add_argument("--serve-seconds", type=float, default=4.0,
                     help="seconds of Poisson arrivals per offered load of the serving form "
                          "(0 skips it)")
@@ -445,85 +447,136 @@ def parity_vs_fp64_oracle(H, W, forms=("fp16", "bf16", "fp8")):
     return out
 
 
-def batched_streams(args, H, W, n_streams):
-    """The batched form: `n_streams` independent video streams served concurrently on one GPU,
-    each by its own host thread, CUDA stream and encoder/decoder proxy pair (the codec calls
-    release the GIL).  Kernels of different streams fill each other's launch gaps, tails and
-    CPU entropy-coding waits.  Device-timed: every stream waits on one start event and one end
-    event waits on every stream."""
+def batched_form(args):
+    """The batching form: `args.batch_streams` streams (32 by default) of two chunks each, with
+    resolutions drawn from seed 3 uniformly over 416x240 .. 3840x2160 and QPs uniform over 0..63.
+    Batched: the streams of each resolution form one packed batch (DMCHTSProxy.compress_batch /
+    decompress_batch, BF16 form), so every network layer is one launch over all streams of that
+    resolution; the resolution groups run concurrently, one host thread and CUDA stream each.
+    Plain: the same chunks coded one request at a time by single-stream FP16 codecs (the
+    reference's form).  Both encode and decode every chunk; both are device-timed from one start
+    event to one end event.  Reported in frames/s and 1080p-equivalent frames/s (pixels)."""
     import threading
     from dcvc_b200 import synthetic
     from dcvc_b200.entropy_tables import add_cdf_to_state_dict
     from dcvc_b200.inference_extensions_cuda import DMCHTSProxy
     from dcvc_b200.model_spec import calibrated_hts_state_dict
+    rng = np.random.default_rng(3)
+    n = args.batch_streams
+    sizes = [SERVE_SIZES[i] for i in rng.integers(0, len(SERVE_SIZES), size=n)]
+    qps = [[int(q) for q in rng.integers(0, 64, size=2)] for _ in range(n)]
     sd = add_cdf_to_state_dict(calibrated_hts_state_dict(0))
     sd = {k: (v.half().cuda() if v.is_floating_point() else v) for k, v in sd.items()}
-    pr, pb = synthetic.padding_for(H, W)
-    dev = torch.cuda.current_device()
-    workers = []
-    for i in range(n_streams):
-        seed = 100 + i
-        enc, dec = DMCHTSProxy(), DMCHTSProxy()
+    groups = {}
+    for i, s in enumerate(sizes):
+        groups.setdefault(s, []).append(i)
+    refs = [synthetic.padded_reference_frame(synthetic.video_chunk_yuv420(100 + i, *sizes[i], 1, 0)[0])
+            for i in range(n)]
+    xs = [[synthetic.to_model_input(synthetic.video_chunk_yuv420(100 + i, *sizes[i], FRAMES, FRAMES * c))
+           for c in range(2)] for i in range(n)]
+    px = sum(h * w for h, w in sizes) * 2 * FRAMES
+    frames = n * 2 * FRAMES
+
+    def proxies(form):
+        enc, dec = DMCHTSProxy(form), DMCHTSProxy(form)
         enc.set_param(sd, SKIP_THRES)
         dec.set_param(sd, SKIP_THRES)
-        ref = synthetic.padded_reference_frame(synthetic.video_chunk_yuv420(seed, H, W, 1, 0)[0])
-        enc.add_ref_feature_from_frame(ref, True)
-        dec.add_ref_feature_from_frame(ref, False)
-        xs = [synthetic.to_model_input(synthetic.video_chunk_yuv420(seed, H, W, FRAMES, FRAMES * k))
-              for k in range(2)]
-        workers.append({"enc": enc, "dec": dec, "xs": xs, "stream": torch.cuda.Stream(),
-                        "err": None})
-    del sd
-    start_stream = torch.cuda.Stream()
-    start = torch.cuda.Event(enable_timing=True)
-    end = torch.cuda.Event(enable_timing=True)
-    gate = threading.Barrier(n_streams + 1)
+        return enc, dec
 
-    def run(w, first, count, timed):
-        try:
-            torch.cuda.set_device(dev)
-            with torch.cuda.stream(w["stream"]):
-                if timed:
-                    gate.wait()  # the start event has been recorded
-                    w["stream"].wait_event(start)
-                for i in range(first, first + count):
-                    qp = QPS[i % len(QPS)]
-                    bits, ecp = w["enc"].compress(w["xs"][i % 2], qp, False, pb, pr)
-                    w["dec"].decompress(bits, qp, H, W, ecp, False)
-                w["done"] = torch.cuda.Event()
-                w["done"].record(w["stream"])
-        except Exception as e:  # reported by the caller
-            w["err"] = e
-            if timed:
-                gate.abort()
+    # ---- batched: one packed enc/dec pair per resolution group, groups concurrently
+    work = []
+    for (h, w), ids in sorted(groups.items()):
+        enc, dec = proxies(args.batch_precision)
+        work.append({"hw": (h, w), "ids": ids, "enc": enc, "dec": dec, "stream": torch.cuda.Stream(),
+                     "err": None})
 
-    def round_(first, count, timed):
-        threads = [threading.Thread(target=run, args=(w, first, count, timed)) for w in workers]
-        for t in threads:
-            t.start()
-        if timed:
-            start.record(start_stream)
+    def run_group(g, seed_only=False):
+        h, w = g["hw"]
+        pr, pb = synthetic.padding_for(h, w)
+        ids = g["ids"]
+        with torch.cuda.stream(g["stream"]):
+            g["enc"].add_ref_features_from_frames([refs[i] for i in ids], True)
+            g["dec"].add_ref_features_from_frames([refs[i] for i in ids], False)
+            if seed_only:
+                return
+            for c in range(2):
+                q = [qps[i][c] for i in ids]
+                out = g["enc"].compress_batch([xs[i][c] for i in ids], q, False, pb, pr)
+                g["dec"].decompress_batch([b for b, _ in out], q, h, w, [e for _, e in out], False)
+
+    def timed(groups_, fn):
+        start_stream = torch.cuda.Stream()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(start_stream)
+        errors = []
+
+        def body(g):
             try:
-                gate.wait()
-            except threading.BrokenBarrierError:
-                pass
-        for t in threads:
-            t.join()
-        for w in workers:
-            if w["err"] is not None:
-                raise w["err"]
+                g["stream"].wait_event(e0)
+                fn(g)
+            except Exception as ex:  # noqa: BLE001
+                errors.append(f"{type(ex).__name__}: {ex}")
 
-    round_(0, args.warmup, False)
-    torch.cuda.synchronize()
-    round_(args.warmup, args.steps, True)
-    for w in workers:
-        start_stream.wait_event(w["done"])
-    end.record(start_stream)
-    torch.cuda.synchronize()
-    ms = start.elapsed_time(end)
-    return {"streams": n_streams, "value": round(FRAMES * args.steps * n_streams / (ms / 1e3), 2),
-            "unit": UNIT, "ms": round(ms, 2), "chunks": args.steps * n_streams,
-            "note": "concurrent independent 1080p streams on one GPU (plain FP16 kernels)"}
+        th = [threading.Thread(target=body, args=(g,)) for g in groups_]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        for g in groups_:
+            start_stream.wait_stream(g["stream"])
+        e1.record(start_stream)
+        e1.synchronize()
+        if errors:
+            raise RuntimeError(errors[0])
+        return e0.elapsed_time(e1) / 1e3
+
+    for _ in range(2):  # warm-up: sizes the arenas, captures the phase graphs
+        timed(work, run_group)
+    sec_b = timed(work, run_group)
+    launches = sum(g["enc"].stats()[1] + g["dec"].stats()[1] for g in work)
+    for g in work:
+        g["enc"] = g["dec"] = None
+    del work
+    torch.cuda.empty_cache()
+
+    # ---- plain: the same chunks one request at a time, single-stream FP16 codecs
+    plain = {}
+    for hw in sorted(groups):
+        plain[hw] = proxies("fp16")
+
+    def run_plain(g):
+        for i in range(n):
+            h, w = sizes[i]
+            pr, pb = synthetic.padding_for(h, w)
+            enc, dec = plain[(h, w)]
+            enc.add_ref_feature_from_frame(refs[i], True)
+            dec.add_ref_feature_from_frame(refs[i], False)
+            for c in range(2):
+                bits, ecp = enc.compress(xs[i][c], qps[i][c], False, pb, pr)
+                dec.decompress(bits, qps[i][c], h, w, ecp, False)
+
+    one = [{"stream": torch.cuda.Stream()}]
+
+    def plain_body(g):
+        with torch.cuda.stream(g["stream"]):
+            run_plain(g)
+
+    timed(one, plain_body)  # warm-up
+    sec_p = timed(one, plain_body)
+    eq = px / (1920 * 1080)
+    return {"streams": n, "chunks_per_stream": 2, "precision": args.batch_precision,
+            "streams_by_size": {f"{w}x{h}": len(ids) for (h, w), ids in sorted(groups.items())},
+            "batched": {"frames_per_s": round(frames / sec_b, 1),
+                        "frames_1080p_equiv_per_s": round(eq / sec_b, 1),
+                        "seconds": round(sec_b, 4), "launches_last_call": launches},
+            "plain_fp16": {"frames_per_s": round(frames / sec_p, 1),
+                           "frames_1080p_equiv_per_s": round(eq / sec_p, 1),
+                           "seconds": round(sec_p, 4)},
+            "batched_vs_plain": round(sec_p / sec_b, 3),
+            "note": "packed batches per resolution group (one launch per layer over the group's "
+                    "streams), groups concurrent; each stream's bytes equal its single-stream "
+                    "coding (tests/test_batch_gpu.py); random-init weights, synthetic content"}
 
 
 SERVE_SIZES = ((240, 416), (480, 832), (720, 1280), (1080, 1920), (2160, 3840))
@@ -561,7 +614,8 @@ def serving_bench(args):
     sd = add_cdf_to_state_dict(calibrated_hts_state_dict(0))
     sd = {k: (v.half().cuda() if v.is_floating_point() else v) for k, v in sd.items()}
     torch.cuda.synchronize()
-    f = HtsSessionFactory(sd, SKIP_THRES, refs, gop=2, copy_output=False)
+    f = HtsSessionFactory(sd, SKIP_THRES, refs, gop=2, copy_output=False,
+                          max_codecs=args.serve_slots)
     srv = ChunkServer(f.open, f.estimate_bytes, slots=args.serve_slots, hbm_budget=SERVE_BUDGET,
                       on_worker_start=f.worker_start)
     try:
@@ -644,7 +698,7 @@ def serving_bench(args):
             loads.append(summ)
         # saturation: the same mix with every request queued at once, one request in flight (the
         # plain one-request-at-a-time form) against `slots` in flight
-        n_sat = max(64, int(120 * args.serve_seconds))
+        n_sat = min(480, max(64, int(120 * args.serve_seconds)))
         saturation = {}
         for limit in (1, args.serve_slots):
             srv.set_in_flight_limit(limit)
@@ -659,6 +713,12 @@ def serving_bench(args):
                 "streams_by_size": streams_by_size,
                 "slots": args.serve_slots, "seconds_per_load": args.serve_seconds,
                 "hbm_budget_gb": SERVE_BUDGET / 1e9, "peak_held_gb": round(srv.peak_held / 1e9, 2),
+                "peak_codec_pool_gb": round(f.peak_pool_bytes / 1e9, 2),
+                "param_gb": round(f.param_bytes / 1e9, 3),
+                "peak_total_gb": round((srv.peak_held + f.peak_pool_bytes + f.param_bytes) / 1e9, 2),
+                "memory_model": "sessions hold only their temporal context and I420 staging "
+                                "(peak_held_gb); chunks run on a pool of at most `slots` codecs "
+                                "(peak_codec_pool_gb) sharing one parameter set (param_gb)",
                 "max_sessions": srv.max_sessions, "failed": srv.failed,
                 "note": "Poisson arrivals, 50/50 encode/decode, resolutions 10/20/30/30/10 % over "
                         "416x240..3840x2160, QP U[0,63]; end to end (I420 planes host<->device); "
@@ -1010,7 +1070,7 @@ def run_gpu(args):
     ld = None if args.no_ld else _section(ld_bench, stream, H, W)
     del enc, dec
     _empty_cache()
-    batched = _section(batched_streams, args, H, W, args.streams) if args.streams > 0 else None
+    batched = _section(batched_form, args) if args.batch_streams > 0 else None
     _empty_cache()
     # a one-GPU measurement: under torchrun the ranks skip it
     serving = None

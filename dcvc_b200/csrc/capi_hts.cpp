@@ -14,6 +14,9 @@ namespace {
 struct HtsHandle {
     HtsCodec codec;
     std::vector<uint8_t> bytes;
+    std::vector<std::vector<uint8_t>> batch_bytes;  // per stream of the last compress_batch
+    std::vector<const uint8_t*> batch_ptrs;
+    std::vector<size_t> batch_sizes;
 };
 
 int fail(int status, const std::string& msg)
@@ -136,6 +139,99 @@ int dcvc_hts_buffer_dtype(void* handle, const char* name, int* dtype)
     const void* p = nullptr;
     int rows = 0, cols = 0, ld = 0;
     return static_cast<HtsHandle*>(handle)->codec.buffer(name, &p, &rows, &cols, &ld, dtype);
+}
+
+int dcvc_hts_add_ref_features(void* handle, const void* const* frames, int n, int height,
+                              int width, int apply_adaptor, void* stream)
+{
+    if (handle == nullptr || frames == nullptr) {
+        return fail(kInvalidArgument, "dcvc_hts_add_ref_features: null argument");
+    }
+    return static_cast<HtsHandle*>(handle)->codec.add_ref_features(
+        reinterpret_cast<const __half* const*>(frames), n, height, width, apply_adaptor != 0,
+        static_cast<cudaStream_t>(stream));
+}
+
+int dcvc_hts_compress_batch(void* handle, const void* const* xs, int n, int height, int width,
+                            const int* qps, int reset, int pad_b, int pad_r, void* stream,
+                            const uint8_t* const** bytes, const size_t** nbytes, int* ec_parallel)
+{
+    if (handle == nullptr || xs == nullptr || bytes == nullptr || nbytes == nullptr ||
+        ec_parallel == nullptr || n < 1) {
+        return fail(kInvalidArgument, "dcvc_hts_compress_batch: null argument");
+    }
+    HtsHandle* h = static_cast<HtsHandle*>(handle);
+    h->batch_bytes.assign(n, {});
+    int st = h->codec.compress_batch(reinterpret_cast<const __half* const*>(xs), n, height, width,
+                                     qps, reset != 0, pad_b, pad_r,
+                                     static_cast<cudaStream_t>(stream), h->batch_bytes.data(),
+                                     ec_parallel);
+    if (st != kOk) {
+        return st;
+    }
+    h->batch_ptrs.resize(n);
+    h->batch_sizes.resize(n);
+    for (int k = 0; k < n; ++k) {
+        h->batch_ptrs[k] = h->batch_bytes[k].data();
+        h->batch_sizes[k] = h->batch_bytes[k].size();
+    }
+    *bytes = h->batch_ptrs.data();
+    *nbytes = h->batch_sizes.data();
+    return kOk;
+}
+
+int dcvc_hts_decompress_batch(void* handle, const uint8_t* const* bytes, const size_t* nbytes,
+                              const int* qps, const int* ec_parallel, int n, int height, int width,
+                              int reset, void* stream, void** frames)
+{
+    if (handle == nullptr || frames == nullptr) {
+        return fail(kInvalidArgument, "dcvc_hts_decompress_batch: null argument");
+    }
+    const __half* f[HtsCodec::kFrames] = {nullptr};
+    int st = static_cast<HtsHandle*>(handle)->codec.decompress_batch(
+        bytes, nbytes, qps, ec_parallel, n, height, width, reset != 0,
+        static_cast<cudaStream_t>(stream), f);
+    if (st == kOk) {
+        for (int i = 0; i < HtsCodec::kFrames; ++i) {
+            frames[i] = const_cast<__half*>(f[i]);
+        }
+    }
+    return st;
+}
+
+int dcvc_hts_share_params(void* handle, void* source)
+{
+    if (handle == nullptr || source == nullptr) {
+        return fail(kInvalidArgument, "dcvc_hts_share_params: null handle");
+    }
+    return static_cast<HtsHandle*>(handle)->codec.share_params(static_cast<HtsHandle*>(source)->codec);
+}
+
+int dcvc_hts_state_bytes(void* handle, size_t* bytes)
+{
+    if (handle == nullptr || bytes == nullptr) {
+        return fail(kInvalidArgument, "dcvc_hts_state_bytes: null argument");
+    }
+    *bytes = static_cast<HtsHandle*>(handle)->codec.state_bytes();
+    return kOk;
+}
+
+int dcvc_hts_export_state(void* handle, void* dst, void* stream, int* flags)
+{
+    if (handle == nullptr) {
+        return fail(kInvalidArgument, "dcvc_hts_export_state: null handle");
+    }
+    return static_cast<HtsHandle*>(handle)->codec.export_state(dst, static_cast<cudaStream_t>(stream),
+                                                               flags);
+}
+
+int dcvc_hts_import_state(void* handle, const void* src, int flags, void* stream)
+{
+    if (handle == nullptr) {
+        return fail(kInvalidArgument, "dcvc_hts_import_state: null handle");
+    }
+    return static_cast<HtsHandle*>(handle)->codec.import_state(src, flags,
+                                                               static_cast<cudaStream_t>(stream));
 }
 
 int dcvc_hts_stats(void* handle, int* symbols, int* kernels, size_t* device_bytes)

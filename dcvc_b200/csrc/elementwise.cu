@@ -254,7 +254,8 @@ __global__ void int8_to_half_kernel(const int8_t* __restrict__ x, int n, __half*
 
 template <int IDT>
 __global__ void mul_channel_kernel(const __half* __restrict__ x, int M, int C, int ldx,
-                                   const __half* __restrict__ q, __half* __restrict__ out, int ldo)
+                                   const __half* __restrict__ q, __half* __restrict__ out, int ldo,
+                                   int q_rows)
 {
     griddep_launch_dependents();
     griddep_wait();
@@ -265,7 +266,8 @@ __global__ void mul_channel_kernel(const __half* __restrict__ x, int M, int C, i
         const long long m = i / vecs;
         const int v = static_cast<int>(i - m * vecs);
         Vec8h a = ld8(x + m * ldx + v * 8);
-        const Vec8h b = ld8(q + v * 8);
+        // q_rows > 0: stacked images, each with its own row of C factors
+        const Vec8h b = ld8(q + (q_rows > 0 ? (m / q_rows) * C : 0) + v * 8);
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
             // a BF16 input value is exact in FP32; the product is rounded once to FP16
@@ -320,7 +322,7 @@ __global__ void quantize_phase_kernel(int groups, int phase, const __half* __res
                                       const __half* __restrict__ means, int ldm,
                                       const __half* __restrict__ q_dec, int ldd, __half thr,
                                       __half* __restrict__ y_q, int ldq, __half* __restrict__ y_hat,
-                                      int ldh, int H, int W, int C)
+                                      int ldh, int H, int W, int C, int img_h)
 {
     griddep_launch_dependents();
     griddep_wait();
@@ -334,7 +336,8 @@ __global__ void quantize_phase_kernel(int groups, int phase, const __half* __res
         const int v = static_cast<int>(i - m * vecs);
         const int h = static_cast<int>(m / W);
         const int w = static_cast<int>(m - static_cast<long long>(h) * W);
-        const bool on = mask_on(groups, phase, h, w, v, vecs);
+        // stacked images: the mask follows each image's own row parity
+        const bool on = mask_on(groups, phase, h % img_h, w, v, vecs);
         const Vec8h yy = ld8(y + m * ldy + v * 8);
         const Vec8h ss = ld8(scales + m * lds + v * 8);
         const Vec8h mm = ld8(means + m * ldm + v * 8);
@@ -379,7 +382,8 @@ template <int MODE>
 __global__ void restore_phase_kernel(int groups, int phase, const __half* __restrict__ y_q, int ldq,
                                      const __half* __restrict__ means, int ldm,
                                      const __half* __restrict__ q_dec, int ldd,
-                                     __half* __restrict__ y_hat, int ldh, int H, int W, int C)
+                                     __half* __restrict__ y_hat, int ldh, int H, int W, int C,
+                                     int img_h)
 {
     griddep_launch_dependents();
     griddep_wait();
@@ -392,7 +396,7 @@ __global__ void restore_phase_kernel(int groups, int phase, const __half* __rest
         const int v = static_cast<int>(i - m * vecs);
         const int h = static_cast<int>(m / W);
         const int w = static_cast<int>(m - static_cast<long long>(h) * W);
-        const bool on = mask_on(groups, phase, h, w, v, vecs);
+        const bool on = mask_on(groups, phase, h % img_h, w, v, vecs);
         const Vec8h qq = ld8(y_q + m * ldq + v * 8);
         const Vec8h mm = ld8(means + m * ldm + v * 8);
         Vec8h prev, qd, o;
@@ -759,11 +763,14 @@ __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src,
                  : "memory");
 }
 
-template <int DT>
+// CUT: the H rows hold images of img_h rows stacked on top of each other; a tap that reaches
+// into the image above or below reads zero, as the padding of each image alone would.
+template <int DT, bool CUT>
 __global__ void __launch_bounds__(kDwThreads) dwconv3x3_kernel(const __half* __restrict__ x, int H,
                                                                int W, int C, int ldx,
                                                                const float* __restrict__ wt,
-                                                               __half* __restrict__ out, int ldo)
+                                                               __half* __restrict__ out, int ldo,
+                                                               int img_h)
 {
     griddep_launch_dependents();
     griddep_wait();
@@ -806,6 +813,12 @@ __global__ void __launch_bounds__(kDwThreads) dwconv3x3_kernel(const __half* __r
     }
     const uint32_t* t2 = reinterpret_cast<const uint32_t*>(&tile[0][0][0]);
     auto at = [&](int r, int c) { return Act<DT>::to2(t2[(r * (kDwTW + 2) + c) * (4 * kDwCV) + cp]); };
+    bool cut_up[kDwRows], cut_dn[kDwRows];  // the row above / below output row o is another image's
+#pragma unroll
+    for (int o = 0; o < kDwRows; ++o) {
+        cut_up[o] = CUT && (ha + o) % img_h == 0;
+        cut_dn[o] = CUT && (ha + o + 1) % img_h == 0;
+    }
     float2 win[kDwRows + 2][3];  // window rows ty .. ty + kDwRows + 1 (image rows ha - 1 ..)
 #pragma unroll
     for (int r = 0; r < kDwRows + 2; ++r) {
@@ -833,7 +846,11 @@ __global__ void __launch_bounds__(kDwThreads) dwconv3x3_kernel(const __half* __r
             for (int kx = 0; kx < 3; ++kx) {
 #pragma unroll
                 for (int o = 0; o < kDwRows; ++o) {
-                    acc[o] = __ffma2_rn(win[ky + o][kx], wp[ky * 3 + kx], acc[o]);
+                    float2 v = win[ky + o][kx];
+                    if (CUT && ((ky == 0 && cut_up[o]) || (ky == 2 && cut_dn[o]))) {
+                        v = make_float2(0.f, 0.f);
+                    }
+                    acc[o] = __ffma2_rn(v, wp[ky * 3 + kx], acc[o]);
                 }
             }
         }
@@ -1052,7 +1069,7 @@ cudaError_t launch_int8_to_half(const int8_t* x, int n, __half* out, cudaStream_
 }
 
 cudaError_t launch_mul_channel(const __half* x, int M, int C, int ldx, const __half* q,
-                               __half* out, int ldo, cudaStream_t s, int in_dtype)
+                               __half* out, int ldo, cudaStream_t s, int in_dtype, int q_rows)
 {
     if (C % 8 || ldx % 8 || ldo % 8 || !al16(x) || !al16(q) || !al16(out) ||
         (in_dtype != 0 && in_dtype != 1)) {
@@ -1060,9 +1077,9 @@ cudaError_t launch_mul_channel(const __half* x, int M, int C, int ldx, const __h
     }
     const dim3 g(grid_for(static_cast<long long>(M) * (C / 8)));
     if (in_dtype == 1) {
-        launch_pdl(mul_channel_kernel<1>, g, dim3(kThreads), 0, s, x, M, C, ldx, q, out, ldo);
+        launch_pdl(mul_channel_kernel<1>, g, dim3(kThreads), 0, s, x, M, C, ldx, q, out, ldo, q_rows);
     } else {
-        launch_pdl(mul_channel_kernel<0>, g, dim3(kThreads), 0, s, x, M, C, ldx, q, out, ldo);
+        launch_pdl(mul_channel_kernel<0>, g, dim3(kThreads), 0, s, x, M, C, ldx, q, out, ldo, q_rows);
     }
     return cudaGetLastError();
 }
@@ -1082,8 +1099,12 @@ cudaError_t launch_quantize_phase(int phase, int mode, const __half* y, int ldy,
                                   const __half* scales, int lds, const __half* means, int ldm,
                                   const __half* q_dec, int ldd, __half thr, __half* y_q,
                                   int ldq, __half* y_hat, int ldh, int H, int W, int C,
-                                  cudaStream_t s, int groups)
+                                  cudaStream_t s, int groups, int img_h)
 {
+    img_h = img_h > 0 ? img_h : H;
+    if (H % img_h) {
+        return cudaErrorInvalidValue;
+    }
     if ((groups != 2 && groups != 4) || phase < 0 || phase >= groups || C % (8 * groups) || (mode >= 2 && q_dec == nullptr) || mode < 0 ||
         mode > 3) {
         return cudaErrorInvalidValue;
@@ -1091,19 +1112,19 @@ cudaError_t launch_quantize_phase(int phase, int mode, const __half* y, int ldy,
     const int g = grid_for(static_cast<long long>(H) * W * (C / 8));
     if (mode == 3) {
         launch_pdl(quantize_phase_kernel<3>, dim3(g), dim3(kThreads), 0, s, groups, phase, y, ldy, scales,
-                   lds, means, ldm, q_dec, ldd, thr, y_q, ldq, y_hat, ldh, H, W, C);
+                   lds, means, ldm, q_dec, ldd, thr, y_q, ldq, y_hat, ldh, H, W, C, img_h);
     } else if (mode == 0) {
         launch_pdl(quantize_phase_kernel<0>, dim3(g), dim3(kThreads), 0, s, groups, phase, y, ldy, scales, lds, means, ldm,
                                                         q_dec, ldd, thr, y_q, ldq, y_hat, ldh, H,
-                                                        W, C);
+                                                        W, C, img_h);
     } else if (mode == 1) {
         launch_pdl(quantize_phase_kernel<1>, dim3(g), dim3(kThreads), 0, s, groups, phase, y, ldy, scales, lds, means, ldm,
                                                         q_dec, ldd, thr, y_q, ldq, y_hat, ldh, H,
-                                                        W, C);
+                                                        W, C, img_h);
     } else {
         launch_pdl(quantize_phase_kernel<2>, dim3(g), dim3(kThreads), 0, s, groups, phase, y, ldy, scales, lds, means, ldm,
                                                         q_dec, ldd, thr, y_q, ldq, y_hat, ldh, H,
-                                                        W, C);
+                                                        W, C, img_h);
     }
     return cudaGetLastError();
 }
@@ -1111,8 +1132,12 @@ cudaError_t launch_quantize_phase(int phase, int mode, const __half* y, int ldy,
 cudaError_t launch_restore_phase(int phase, int mode, const __half* y_q, int ldq,
                                  const __half* means, int ldm, const __half* q_dec, int ldd,
                                  __half* y_hat, int ldh, int H, int W, int C, cudaStream_t s,
-                                 int groups)
+                                 int groups, int img_h)
 {
+    img_h = img_h > 0 ? img_h : H;
+    if (H % img_h) {
+        return cudaErrorInvalidValue;
+    }
     if ((groups != 2 && groups != 4) || phase < 0 || phase >= groups || C % (8 * groups) || (mode == 2 && q_dec == nullptr) || mode < 0 ||
         mode > 2) {
         return cudaErrorInvalidValue;
@@ -1120,13 +1145,13 @@ cudaError_t launch_restore_phase(int phase, int mode, const __half* y_q, int ldq
     const int g = grid_for(static_cast<long long>(H) * W * (C / 8));
     if (mode == 0) {
         launch_pdl(restore_phase_kernel<0>, dim3(g), dim3(kThreads), 0, s, groups, phase, y_q, ldq, means, ldm, q_dec, ldd,
-                                                       y_hat, ldh, H, W, C);
+                                                       y_hat, ldh, H, W, C, img_h);
     } else if (mode == 1) {
         launch_pdl(restore_phase_kernel<1>, dim3(g), dim3(kThreads), 0, s, groups, phase, y_q, ldq, means, ldm, q_dec, ldd,
-                                                       y_hat, ldh, H, W, C);
+                                                       y_hat, ldh, H, W, C, img_h);
     } else {
         launch_pdl(restore_phase_kernel<2>, dim3(g), dim3(kThreads), 0, s, groups, phase, y_q, ldq, means, ldm, q_dec, ldd,
-                                                       y_hat, ldh, H, W, C);
+                                                       y_hat, ldh, H, W, C, img_h);
     }
     return cudaGetLastError();
 }
@@ -1262,17 +1287,27 @@ cudaError_t launch_recover(const int8_t* dec, const uint8_t* cond, const int* bl
 }
 
 cudaError_t launch_dwconv3x3(const __half* x, int H, int W, int C, int ldx, const float* w,
-                             __half* out, int ldo, cudaStream_t s, int dtype)
+                             __half* out, int ldo, cudaStream_t s, int dtype, int img_h)
 {
+    img_h = img_h > 0 ? img_h : H;
     if (C % 8 || ldx % 8 || ldo % 8 || !al16(x) || !al16(out) || !al16(w) ||
-        (dtype != 0 && dtype != 1)) {
+        (dtype != 0 && dtype != 1) || H % img_h) {
         return cudaErrorInvalidValue;
     }
     const dim3 grid((C / 8 + kDwCV - 1) / kDwCV, (H + kDwTH - 1) / kDwTH, (W + kDwTW - 1) / kDwTW);
+    const bool cut = img_h < H;
     if (dtype == 1) {
-        launch_pdl(dwconv3x3_kernel<1>, grid, dim3(kDwThreads), 0, s, x, H, W, C, ldx, w, out, ldo);
+        if (cut) {
+            launch_pdl(dwconv3x3_kernel<1, true>, grid, dim3(kDwThreads), 0, s, x, H, W, C, ldx, w, out, ldo, img_h);
+        } else {
+            launch_pdl(dwconv3x3_kernel<1, false>, grid, dim3(kDwThreads), 0, s, x, H, W, C, ldx, w, out, ldo, img_h);
+        }
     } else {
-        launch_pdl(dwconv3x3_kernel<0>, grid, dim3(kDwThreads), 0, s, x, H, W, C, ldx, w, out, ldo);
+        if (cut) {
+            launch_pdl(dwconv3x3_kernel<0, true>, grid, dim3(kDwThreads), 0, s, x, H, W, C, ldx, w, out, ldo, img_h);
+        } else {
+            launch_pdl(dwconv3x3_kernel<0, false>, grid, dim3(kDwThreads), 0, s, x, H, W, C, ldx, w, out, ldo, img_h);
+        }
     }
     return cudaGetLastError();
 }

@@ -76,8 +76,10 @@ cudaError_t launch_int8_to_half(const int8_t* x, int n, __half* out, cudaStream_
 
 // multiply_with_broadcast (stream.cu:484-546): out[m, c] = x[m, c] * q[c].
 // in_dtype 1: x is BF16 (q and out stay FP16; one rounding of the FP32 product).
+// q_rows > 0: the M rows are images of q_rows rows each, image k scaled by q row k (q [n, C]).
 cudaError_t launch_mul_channel(const __half* x, int M, int C, int ldx, const __half* q,
-                               __half* out, int ldo, cudaStream_t s, int in_dtype = 0);
+                               __half* out, int ldo, cudaStream_t s, int in_dtype = 0,
+                               int q_rows = 0);
 
 // divide_with_clamp_inplace (stream.cu:422-452): y <- y * rcp(max(q, 0.5)), the reciprocal
 // rounded from FP32 1/q.
@@ -85,7 +87,8 @@ cudaError_t launch_div_clamp(__half* y, int M, int C, int ldy, const __half* q, 
                              cudaStream_t s);
 
 // process_with_mask_no_scale[_add_inplace][_add_and_multiply_inplace] (stream.cu:548-683) for
-// mask phase `phase` on an H x W grid.  mode 0: write y_q / y_hat; 1: accumulate;
+// mask phase `phase` on an H x W grid (img_h > 0: images of img_h rows stacked vertically, each
+// with its own mask rows).  mode 0: write y_q / y_hat; 1: accumulate;
 // 2: accumulate and scale y_hat by max(q_dec, 0.5); 3: accumulate and scale y_hat by q_dec
 // (add_and_multiply_broadcast, stream.cu:8-37: with ldd = 0, q_dec is one row of C scales).
 // groups = 4: the 4-phase masks; groups = 2: the 2-phase checkerboard of the LD model
@@ -94,13 +97,13 @@ cudaError_t launch_quantize_phase(int phase, int mode, const __half* y, int ldy,
                                   const __half* scales, int lds, const __half* means, int ldm,
                                   const __half* q_dec, int ldd, __half thr, __half* y_q,
                                   int ldq, __half* y_hat, int ldh, int H, int W, int C,
-                                  cudaStream_t s, int groups = 4);
+                                  cudaStream_t s, int groups = 4, int img_h = 0);
 
 // restore_y[_and_add_inplace][_and_add_multiply_inplace] (stream.cu:685-760).
 cudaError_t launch_restore_phase(int phase, int mode, const __half* y_q, int ldq,
                                  const __half* means, int ldm, const __half* q_dec, int ldd,
                                  __half* y_hat, int ldh, int H, int W, int C, cudaStream_t s,
-                                 int groups = 4);
+                                 int groups = 4, int img_h = 0);
 
 // build_index_enc (stream.cu:126-173): sym[m*C + c] = (q << 8) + idx, cond = scale > thr, in
 // NHWC symbol order.  idx comes from the 65536-entry table `lut` indexed by the FP16 bits of the
@@ -165,7 +168,8 @@ cudaError_t launch_recover(const int8_t* dec, const uint8_t* cond, const int* bl
 
 // Depthwise 3x3, pad 1, no bias (d3x3, cutlass/d3x3_kernel.h:104-166): FP32 accumulation in the
 // order ky, kx.  w is FP32 [9][C] (tap-major).
+// img_h (0: H): the H rows hold images of img_h rows stacked vertically, each padded on its own.
 cudaError_t launch_dwconv3x3(const __half* x, int H, int W, int C, int ldx, const float* w,
-                             __half* out, int ldo, cudaStream_t s, int dtype = 0);
+                             __half* out, int ldo, cudaStream_t s, int dtype = 0, int img_h = 0);
 
 }  // namespace dcvc

@@ -483,8 +483,11 @@ __global__ void __launch_bounds__(GemmCfg<BN, EPI>::kThreads, 1)
                             }
                         }
                         if constexpr (epi_has_q(EPI)) {
-                            const uint4* qs =
-                                reinterpret_cast<const uint4*>(reinterpret_cast<const T*>(p.qscale) + nc);
+                            // this lane's row picks its image's factors in a packed batch
+                            const int qm = min(row0 + lane, p.M - 1);
+                            const size_t qrow = p.q_rows > 0 ? static_cast<size_t>(qm / p.q_rows) * p.N : 0;
+                            const uint4* qs = reinterpret_cast<const uint4*>(
+                                reinterpret_cast<const T*>(p.qscale) + qrow + nc);
 #pragma unroll
                             for (int j = 0; j < 4; ++j) {
                                 const uint4 u = __ldg(qs + j);

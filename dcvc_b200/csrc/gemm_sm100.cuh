@@ -55,6 +55,9 @@ struct GemmParams {
     // through gemm_inject_stall.
     long long wait_limit = 0;
     int stall_test = 0;
+    // q_rows > 0: the M rows are images of q_rows rows stacked on each other and qscale holds one
+    // row of N factors per image (per-stream QPs of a packed batch); 0: one row for all
+    int q_rows = 0;
 };
 
 // The next `launches` GEMM launches of this process run with stall_test set and the given wait

@@ -7,6 +7,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <thread>
 #include <type_traits>
 
 namespace dcvc {
@@ -31,6 +32,7 @@ HtsCodec::HtsCodec()
     cudaEventCreateWithFlags(&ev_in_, cudaEventDisableTiming);
     cudaEventCreateWithFlags(&ev_phase_, cudaEventDisableTiming);
     cudaEventCreateWithFlags(&ev_out_, cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&ev_state_, cudaEventDisableTiming);
     err_word_ = device_error_word();
     if (err_slot_.alloc()) {
         graphs_.set_error_slot(err_slot_.dev);
@@ -52,6 +54,7 @@ HtsCodec::~HtsCodec()
     cudaEventDestroy(ev_in_);
     cudaEventDestroy(ev_phase_);
     cudaEventDestroy(ev_out_);
+    cudaEventDestroy(ev_state_);
     cudaStreamDestroy(main_);
     err_slot_.release();
 }
@@ -75,8 +78,8 @@ int HtsCodec::set_param(const StateDict& sd, float skip_threshold)
     }
     clear_graphs();
     ready_ = false;
-    weights_.clear();
-    ParamBuilder B(sd, weights_);
+    weights_ = std::make_shared<DeviceArena>();
+    ParamBuilder B(sd, *weights_);
     // the analysis / synthesis transforms in the precision form's format, the entropy-parameter
     // path in FP16; q_encoder / q_decoder scale outputs of the transforms, q_feature the input
     // of the temporal prior
@@ -137,7 +140,7 @@ int HtsCodec::set_param(const StateDict& sd, float skip_threshold)
     B.set_dtype(0);
     if (!B.ok()) {
         set_last_error("set_param: " + B.error());
-        weights_.clear();
+        weights_.reset();
         return kInvalidArgument;
     }
     // structural checks of the HT-S layout (video_model_ht.py:17-23)
@@ -152,17 +155,17 @@ int HtsCodec::set_param(const StateDict& sd, float skip_threshold)
         fe_[0].C == kChD && rh_head_[0].cout == kChSrcIntra && rh_head_[0].cin == kChRecon;
     if (!shapes_ok) {
         set_last_error("set_param: state dict is not an HT-S (DMC, ModelStructure.HTS) model");
-        weights_.clear();
+        weights_.reset();
         return kInvalidArgument;
     }
     // CDF tables (set_param, dmc_hts_proxy.cpp:748-761)
     if (load_cdf_tables(sd, &tables_, kQpNum * kChZ, 128) != kOk) {
-        weights_.clear();
+        weights_.reset();
         return kInvalidArgument;
     }
     // the scale -> CDF index table, evaluated on the device as the reference's FP16
     // scale_to_index computes it
-    scale_lut_ = weights_.alloc_n<uint8_t>(65536);
+    scale_lut_ = weights_->alloc_n<uint8_t>(65536);
     if (scale_lut_ == nullptr || scale_index_table_device(scale_lut_, 0) != cudaSuccess ||
         cudaStreamSynchronize(0) != cudaSuccess) {
         set_last_error("set_param: could not build the scale-index table");
@@ -174,13 +177,17 @@ int HtsCodec::set_param(const StateDict& sd, float skip_threshold)
     return kOk;
 }
 
-int HtsCodec::allocate(int Hp, int Wp)
+int HtsCodec::allocate(int Hp, int Wp, int imgs)
 {
-    if (Hp == Hp_ && Wp == Wp_) {
+    if (Hp == Hp_ && Wp == Wp_ && imgs == imgs_) {
         return kOk;
     }
     if (Hp <= 0 || Wp <= 0 || Hp % 16 || Wp % 16) {
         set_last_error("frame height and width must be positive multiples of 16");
+        return kInvalidArgument;
+    }
+    if (imgs < 1 || imgs > kMaxBatch) {
+        set_last_error("a packed batch holds 1 to " + std::to_string(kMaxBatch) + " streams");
         return kInvalidArgument;
     }
     cudaStreamSynchronize(main_);
@@ -202,6 +209,7 @@ int HtsCodec::allocate(int Hp, int Wp)
     ydec_hdev_ = nullptr;
     z_hdev_ = nullptr;
     Hp_ = Wp_ = 0;
+    imgs_ = 0;
 
     const int H8 = Hp / 8, W8 = Wp / 8;
     const int H16 = H8 / 2, W16 = W8 / 2;
@@ -212,13 +220,24 @@ int HtsCodec::allocate(int Hp, int Wp)
     W16_ = W16;
     H16p_ = H16p;
     W16p_ = W16p;
-    M8_ = H8 * W8;
-    M16_ = H16 * W16;
-    M16p_ = H16p * W16p;
-    M32_ = (H16p / 2) * (W16p / 2);
-    M64_ = (H16p / 4) * (W16p / 4);
-    y_num_ = M16_ * kChY;
-    z_num_ = M64_ * kChZ;
+    // per image, and stacked over the batch's images (row counts of every activation buffer)
+    m8_ = H8 * W8;
+    m16_ = H16 * W16;
+    m16p_ = H16p * W16p;
+    TH8_ = imgs * H8;
+    TH16_ = imgs * H16;
+    TH16p_ = imgs * H16p;
+    TH32_ = imgs * (H16p / 2);
+    TH64_ = imgs * (H16p / 4);
+    M8_ = imgs * H8 * W8;
+    M16_ = imgs * H16 * W16;
+    M16p_ = imgs * H16p * W16p;
+    M32_ = imgs * (H16p / 2) * (W16p / 2);
+    M64_ = imgs * (H16p / 4) * (W16p / 4);
+    ny_ = m16_ * kChY;
+    nz_ = (H16p / 4) * (W16p / 4) * kChZ;
+    y_num_ = imgs * ny_;
+    z_num_ = imgs * nz_;
     const bool pad = (H16p != H16) || (W16p != W16);
 
     bool ok = true;
@@ -252,11 +271,11 @@ int HtsCodec::allocate(int Hp, int Wp)
     head_ = H(M8 * kChSrcIntra);
     y_act_ = act_ ? H(M16 * kChY) : nullptr;
     yhat_act_ = act_ ? H(M16 * kChY) : nullptr;
-    q_enc_ = H(kChD);
-    q_dec_ = H(kChD);
-    q_feat_ = H(kChD);
+    q_enc_ = H(static_cast<size_t>(imgs) * kChD);
+    q_dec_ = H(static_cast<size_t>(imgs) * kChD);
+    q_feat_ = H(static_cast<size_t>(imgs) * kChD);
     for (int i = 0; i < kFrames; ++i) {
-        x_hat_[i] = H(static_cast<size_t>(Hp) * Wp * 3);
+        x_hat_[i] = H(static_cast<size_t>(imgs) * Hp * Wp * 3);
     }
     const size_t S = std::max(M8 * kChD, M16p * 3 * kChY);
     scratch_.t0 = H(S);
@@ -273,8 +292,8 @@ int HtsCodec::allocate(int Hp, int Wp)
     idx_c_ = acts_.alloc_n<uint8_t>(y_num_);
     cond_ = acts_.alloc_n<uint8_t>(y_num_);
     y_dec_ = acts_.alloc_n<int8_t>(y_num_);
-    block_counts_ = acts_.alloc_n<int>(compact_blocks(y_num_));
-    count_dev_ = acts_.alloc_n<int>(1);
+    block_counts_ = acts_.alloc_n<int>(static_cast<size_t>(imgs) * compact_blocks(ny_));
+    count_dev_ = acts_.alloc_n<int>(imgs);
     ok = ok && z_i8_ && sym_ && sym_c_ && idx_ && idx_c_ && cond_ && y_dec_ && block_counts_ &&
          count_dev_;
     auto mapped = [&](size_t bytes, auto** host, auto** dev) {
@@ -283,7 +302,7 @@ int HtsCodec::allocate(int Hp, int Wp)
         *host = static_cast<std::remove_reference_t<decltype(**host)>*>(h);
         *dev = static_cast<std::remove_reference_t<decltype(**dev)>*>(d);
     };
-    mapped(sizeof(int) * 2, &count_host_, &count_hdev_);
+    mapped(sizeof(int) * (imgs + 1), &count_host_, &count_hdev_);
     mapped(sizeof(int16_t) * y_num_, &sym_host_, &sym_hdev_);
     mapped(y_num_, &idx_host_, &idx_hdev_);
     mapped(y_num_, &ydec_host_, &ydec_hdev_);
@@ -304,18 +323,19 @@ int HtsCodec::allocate(int Hp, int Wp)
     }
     Hp_ = Hp;
     Wp_ = Wp;
+    imgs_ = imgs;
     memory_has_value_ = false;
     return kOk;
 }
 
-void HtsCodec::set_qp(int qp, cudaStream_t s)
+void HtsCodec::set_qp(const int* qps, cudaStream_t s)
 {
-    cudaMemcpyAsync(q_enc_, q_enc_tab_ + static_cast<size_t>(qp) * kChD, kChD * 2,
-                    cudaMemcpyDeviceToDevice, s);
-    cudaMemcpyAsync(q_dec_, q_dec_tab_ + static_cast<size_t>(qp) * kChD, kChD * 2,
-                    cudaMemcpyDeviceToDevice, s);
-    cudaMemcpyAsync(q_feat_, q_feat_tab_ + static_cast<size_t>(qp) * kChD, kChD * 2,
-                    cudaMemcpyDeviceToDevice, s);
+    for (int k = 0; k < imgs_; ++k) {
+        const size_t src = static_cast<size_t>(qps[k]) * kChD, dst = static_cast<size_t>(k) * kChD;
+        cudaMemcpyAsync(q_enc_ + dst, q_enc_tab_ + src, kChD * 2, cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(q_dec_ + dst, q_dec_tab_ + src, kChD * 2, cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(q_feat_ + dst, q_feat_tab_ + src, kChD * 2, cudaMemcpyDeviceToDevice, s);
+    }
 }
 
 // ------------------------------------------------------------------------------ network pieces
@@ -323,71 +343,76 @@ void HtsCodec::set_qp(int qp, cudaStream_t s)
 void HtsCodec::feature_adaptor_m(Launch& L)
 {
     // memory = FA_m(cat(memory, feature_p))   (dmc_hts_proxy.cpp:845-851)
-    run_dcb(L, fa_m_[0], cat_fam_, 1024, H8_, W8_, lvl8_a_, kChM, scratch_);
+    run_dcb(L, fa_m_[0], cat_fam_, 1024, TH8_, W8_, lvl8_a_, kChM, scratch_, nullptr, H8_);
     for (int i = 1; i < 5; ++i) {
-        run_dcb(L, fa_m_[i], lvl8_a_, kChM, H8_, W8_, lvl8_a_, kChM, scratch_);
+        run_dcb(L, fa_m_[i], lvl8_a_, kChM, TH8_, W8_, lvl8_a_, kChM, scratch_, nullptr, H8_);
     }
-    run_dcb(L, fa_m_[5], lvl8_a_, kChM, H8_, W8_, cat_fam_, 1024, scratch_);
+    run_dcb(L, fa_m_[5], lvl8_a_, kChM, TH8_, W8_, cat_fam_, 1024, scratch_, nullptr, H8_);
 }
 
 void HtsCodec::feature_adaptor_i(Launch& L, const __half* fi)
 {
-    run_dcb(L, fa_i_[0], fi, kChSrcIntra, H8_, W8_, lvl8_a_, kChM, scratch_);
+    run_dcb(L, fa_i_[0], fi, kChSrcIntra, TH8_, W8_, lvl8_a_, kChM, scratch_, nullptr, H8_);
     for (int i = 1; i < 3; ++i) {
-        run_dcb(L, fa_i_[i], lvl8_a_, kChM, H8_, W8_, lvl8_a_, kChM, scratch_);
+        run_dcb(L, fa_i_[i], lvl8_a_, kChM, TH8_, W8_, lvl8_a_, kChM, scratch_, nullptr, H8_);
     }
-    run_dcb(L, fa_i_[3], lvl8_a_, kChM, H8_, W8_, cat_fam_, 1024, scratch_);
+    run_dcb(L, fa_i_[3], lvl8_a_, kChM, TH8_, W8_, cat_fam_, 1024, scratch_, nullptr, H8_);
 }
 
 void HtsCodec::feature_extractor(Launch& L)
 {
     // ctx = FE(memory); ctx lives in cat_enc[1536:2048]
     __half* ctx = cat_enc_ + kChSrc;
-    run_dcb(L, fe_[0], cat_fam_, 1024, H8_, W8_, ctx, 2048, scratch_);
+    run_dcb(L, fe_[0], cat_fam_, 1024, TH8_, W8_, ctx, 2048, scratch_, nullptr, H8_);
     for (int i = 1; i < 5; ++i) {
-        run_dcb(L, fe_[i], ctx, 2048, H8_, W8_, ctx, 2048, scratch_);
+        run_dcb(L, fe_[i], ctx, 2048, TH8_, W8_, ctx, 2048, scratch_, nullptr, H8_);
     }
 }
 
 void HtsCodec::temporal_prior(Launch& L)
 {
     // temporal_params = RBWS2(memory * q_feature) -> cat_pf[256:768]
-    L.note(launch_mul_channel(cat_fam_, M8_, kChM, 1024, q_feat_, temporal_in_, kChM, L.s, act_));
-    L.note(launch_space_to_depth2(temporal_in_, H8_, W8_, kChM, kChM, s2d_, L.s));
+    L.note(launch_mul_channel(cat_fam_, M8_, kChM, 1024, q_feat_, temporal_in_, kChM, L.s, act_,
+                              imgs_ > 1 ? m8_ : 0));
+    L.note(launch_space_to_depth2(temporal_in_, TH8_, W8_, kChM, kChM, s2d_, L.s));
     gemm(L, temporal_.down, kEpiBias, s2d_, 4 * kChM, M16_, lvl16_a_, 2 * kChY);
-    run_dcb(L, temporal_.dcb, lvl16_a_, 2 * kChY, H16_, W16_, cat_pf_ + kChY, 3 * kChY, scratch_);
+    run_dcb(L, temporal_.dcb, lvl16_a_, 2 * kChY, TH16_, W16_, cat_pf_ + kChY, 3 * kChY, scratch_, nullptr, H16_);
 }
 
 void HtsCodec::hyper_decoder(Launch& L)
 {
     const int H64 = H16p_ / 4, W64 = W16p_ / 4, H32 = H16p_ / 2, W32 = W16p_ / 2;
     gemm(L, hyper_dec0_.up, kEpiSubpel, z_hat_, kChZ, M64_, lvl32_a_, kChY, nullptr, 0, nullptr, W64);
-    run_dcb(L, hyper_dec0_.dcb, lvl32_a_, kChY, H32, W32, lvl32_a_, kChY, scratch_);
+    run_dcb(L, hyper_dec0_.dcb, lvl32_a_, kChY, TH32_, W32, lvl32_a_, kChY, scratch_, nullptr, H32);
     gemm(L, hyper_dec1_.up, kEpiSubpel, lvl32_a_, kChY, M32_, lvl16_a_, kChY, nullptr, 0, nullptr, W32);
-    run_dcb(L, hyper_dec1_.dcb, lvl16_a_, kChY, H16p_, W16p_, lvl16_a_, kChY, scratch_);
+    run_dcb(L, hyper_dec1_.dcb, lvl16_a_, kChY, TH16p_, W16p_, lvl16_a_, kChY, scratch_, nullptr, H16p_);
     if (hyper_pad_ != nullptr) {
-        run_dcb(L, hyper_dec2_, lvl16_a_, kChY, H16p_, W16p_, hyper_pad_, kChY, scratch_);
-        L.note(launch_crop(hyper_pad_, W16p_, kChY, H16_, W16_, kChY, cat_pf_, 3 * kChY, L.s));
+        run_dcb(L, hyper_dec2_, lvl16_a_, kChY, TH16p_, W16p_, hyper_pad_, kChY, scratch_, nullptr, H16p_);
+        for (int k = 0; k < imgs_; ++k) {  // each image's top-left H16 x W16 part
+            L.note(launch_crop(hyper_pad_ + static_cast<size_t>(k) * m16p_ * kChY, W16p_, kChY, H16_,
+                               W16_, kChY, cat_pf_ + static_cast<size_t>(k) * m16_ * 3 * kChY,
+                               3 * kChY, L.s));
+        }
     } else {
-        run_dcb(L, hyper_dec2_, lvl16_a_, kChY, H16_, W16_, cat_pf_, 3 * kChY, scratch_);
+        run_dcb(L, hyper_dec2_, lvl16_a_, kChY, TH16_, W16_, cat_pf_, 3 * kChY, scratch_, nullptr, H16_);
     }
 }
 
 void HtsCodec::prior_fusion(Launch& L)
 {
     const int C = 3 * kChY;
-    run_dcb(L, prior_fusion_[0], cat_pf_, C, H16_, W16_, lvl16_a_, C, scratch_);
-    run_dcb(L, prior_fusion_[1], lvl16_a_, C, H16_, W16_, lvl16_a_, C, scratch_);
-    run_dcb(L, prior_fusion_[2], lvl16_a_, C, H16_, W16_, lvl16_a_, C, scratch_);
+    run_dcb(L, prior_fusion_[0], cat_pf_, C, TH16_, W16_, lvl16_a_, C, scratch_, nullptr, H16_);
+    run_dcb(L, prior_fusion_[1], lvl16_a_, C, TH16_, W16_, lvl16_a_, C, scratch_, nullptr, H16_);
+    run_dcb(L, prior_fusion_[2], lvl16_a_, C, TH16_, W16_, lvl16_a_, C, scratch_, nullptr, H16_);
     gemm(L, prior_fusion_out_, kEpiBias, lvl16_a_, C, M16_, common_, C);
 }
 
 void HtsCodec::spatial_prior(Launch& L, int k)
 {
     const int C = 2 * kChY;
-    run_dcb(L, sp_adaptor_[k], cat_spa_, C, H16_, W16_, lvl16_a_, C, scratch_);
+    run_dcb(L, sp_adaptor_[k], cat_spa_, C, TH16_, W16_, lvl16_a_, C, scratch_, nullptr, H16_);
     for (int i = 0; i < 3; ++i) {
-        run_dcb(L, spatial_prior_[i], lvl16_a_, C, H16_, W16_, lvl16_a_, C, scratch_);
+        run_dcb(L, spatial_prior_[i], lvl16_a_, C, TH16_, W16_, lvl16_a_, C, scratch_, nullptr, H16_);
     }
     gemm(L, spatial_prior_out_, kEpiBias, lvl16_a_, C, M16_, means_, kChY);
 }
@@ -404,11 +429,11 @@ void HtsCodec::decoder(Launch& L)
     }
     gemm(L, dec_up_lin_, kEpiSubpel, yh, ldyh, M16_, cat_enc_ + 1024, 2048, nullptr, 0, nullptr,
          W16_);
-    run_dcb(L, decoder_[0], cat_enc_ + 1024, 2048, H8_, W8_, lvl8_a_, kChD, scratch_);
+    run_dcb(L, decoder_[0], cat_enc_ + 1024, 2048, TH8_, W8_, lvl8_a_, kChD, scratch_, nullptr, H8_);
     for (int i = 1; i < 6; ++i) {
-        run_dcb(L, decoder_[i], lvl8_a_, kChD, H8_, W8_, lvl8_a_, kChD, scratch_);
+        run_dcb(L, decoder_[i], lvl8_a_, kChD, TH8_, W8_, lvl8_a_, kChD, scratch_, nullptr, H8_);
     }
-    run_dcb(L, decoder_[6], lvl8_a_, kChD, H8_, W8_, cat_fam_ + kChM, 1024, scratch_, q_dec_);
+    run_dcb(L, decoder_[6], lvl8_a_, kChD, TH8_, W8_, cat_fam_ + kChM, 1024, scratch_, q_dec_, H8_);
 }
 
 void HtsCodec::recon_head(Launch& L, bool all_frames)
@@ -417,15 +442,15 @@ void HtsCodec::recon_head(Launch& L, bool all_frames)
     const int first = all_frames ? 0 : kFrames - 1;
     for (int i = first; i < kFrames; ++i) {
         if (i % 2 == 0 || !all_frames) {
-            run_dcb(L, rh_common_[i / 2], feature_p, 1024, H8_, W8_, lvl8_b_, kChD, scratch_);
+            run_dcb(L, rh_common_[i / 2], feature_p, 1024, TH8_, W8_, lvl8_b_, kChD, scratch_, nullptr, H8_);
         }
-        run_dcb(L, rh_frame_[i][0], lvl8_b_, kChD, H8_, W8_, lvl8_a_, kChRecon, scratch_);
-        run_dcb(L, rh_frame_[i][1], lvl8_a_, kChRecon, H8_, W8_, lvl8_a_, kChRecon, scratch_);
-        run_dcb(L, rh_frame_[i][2], lvl8_a_, kChRecon, H8_, W8_, lvl8_a_, kChRecon, scratch_);
+        run_dcb(L, rh_frame_[i][0], lvl8_b_, kChD, TH8_, W8_, lvl8_a_, kChRecon, scratch_, nullptr, H8_);
+        run_dcb(L, rh_frame_[i][1], lvl8_a_, kChRecon, TH8_, W8_, lvl8_a_, kChRecon, scratch_, nullptr, H8_);
+        run_dcb(L, rh_frame_[i][2], lvl8_a_, kChRecon, TH8_, W8_, lvl8_a_, kChRecon, scratch_, nullptr, H8_);
         __half* out = (i == kFrames - 1) ? feature_i_ : head_;
         gemm(L, rh_head_[i], kEpiBias, lvl8_a_, kChRecon, M8_, out, kChSrcIntra);
         if (all_frames) {
-            L.note(launch_shuffle8_clamp(out, H8_, W8_, 3, kChSrcIntra, x_hat_[i], L.s, act_));
+            L.note(launch_shuffle8_clamp(out, TH8_, W8_, 3, kChSrcIntra, x_hat_[i], L.s, act_));
         }
     }
 }
@@ -436,12 +461,15 @@ void HtsCodec::enc_analysis(Launch& L)
 {
     const int H32 = H16p_ / 2, W32 = W16p_ / 2, H64 = H16p_ / 4, W64 = W16p_ / 4;
     // encoder (dmc_hts_proxy.cpp:67-78)
-    run_dcb(L, encoder_[0], cat_enc_, 2048, H8_, W8_, lvl8_a_, kChD, scratch_);
+    run_dcb(L, encoder_[0], cat_enc_, 2048, TH8_, W8_, lvl8_a_, kChD, scratch_, nullptr, H8_);
     for (int i = 1; i < 5; ++i) {
-        run_dcb(L, encoder_[i], lvl8_a_, kChD, H8_, W8_, lvl8_a_, kChD, scratch_);
+        run_dcb(L, encoder_[i], lvl8_a_, kChD, TH8_, W8_, lvl8_a_, kChD, scratch_, nullptr, H8_);
     }
-    run_dcb(L, encoder_[5], lvl8_a_, kChD, H8_, W8_, lvl8_a_, kChD, scratch_, q_enc_);
-    L.note(launch_im2col3x3s2(lvl8_a_, H8_, W8_, kChD, kChD, col_, L.s));
+    run_dcb(L, encoder_[5], lvl8_a_, kChD, TH8_, W8_, lvl8_a_, kChD, scratch_, q_enc_, H8_);
+    for (int k = 0; k < imgs_; ++k) {  // each image's patches, zero outside its own border
+        L.note(launch_im2col3x3s2(lvl8_a_ + static_cast<size_t>(k) * m8_ * kChD, H8_, W8_, kChD, kChD,
+                                  col_ + static_cast<size_t>(k) * m16_ * 9 * kChD, L.s));
+    }
     if (act_) {  // the BF16 form: y to FP16 for the entropy-parameter path
         gemm(L, enc_down_, kEpiBias, col_, 9 * kChD, M16_, y_act_, kChY);
         L.note(launch_convert(y_act_, 1, kChY, y_, 0, kChY, M16_, kChY, L.s));
@@ -449,16 +477,20 @@ void HtsCodec::enc_analysis(Launch& L)
         gemm(L, enc_down_, kEpiBias, col_, 9 * kChD, M16_, y_, kChY);
     }
     if (y_pad_ != y_) {
-        L.note(launch_replicate_pad(y_, H16_, W16_, kChY, kChY, H16p_ - H16_, W16p_ - W16_, y_pad_, L.s));
+        for (int k = 0; k < imgs_; ++k) {
+            L.note(launch_replicate_pad(y_ + static_cast<size_t>(k) * m16_ * kChY, H16_, W16_, kChY,
+                                        kChY, H16p_ - H16_, W16p_ - W16_,
+                                        y_pad_ + static_cast<size_t>(k) * m16p_ * kChY, L.s));
+        }
     }
     // hyper encoder
-    run_dcb(L, hyper_enc0_, y_pad_, kChY, H16p_, W16p_, lvl16_a_, kChY, scratch_);
-    L.note(launch_space_to_depth2(lvl16_a_, H16p_, W16p_, kChY, kChY, s2d_, L.s));
+    run_dcb(L, hyper_enc0_, y_pad_, kChY, TH16p_, W16p_, lvl16_a_, kChY, scratch_, nullptr, H16p_);
+    L.note(launch_space_to_depth2(lvl16_a_, TH16p_, W16p_, kChY, kChY, s2d_, L.s));
     gemm(L, hyper_enc1_.down, kEpiBias, s2d_, 4 * kChY, M32_, lvl32_a_, kChY);
-    run_dcb(L, hyper_enc1_.dcb, lvl32_a_, kChY, H32, W32, lvl32_a_, kChY, scratch_);
-    L.note(launch_space_to_depth2(lvl32_a_, H32, W32, kChY, kChY, s2d_, L.s));
+    run_dcb(L, hyper_enc1_.dcb, lvl32_a_, kChY, TH32_, W32, lvl32_a_, kChY, scratch_, nullptr, H32);
+    L.note(launch_space_to_depth2(lvl32_a_, TH32_, W32, kChY, kChY, s2d_, L.s));
     gemm(L, hyper_enc2_.down, kEpiBias, s2d_, 4 * kChY, M64_, lvl64_a_, kChZ);
-    run_dcb(L, hyper_enc2_.dcb, lvl64_a_, kChZ, H64, W64, z_, kChZ, scratch_);
+    run_dcb(L, hyper_enc2_.dcb, lvl64_a_, kChZ, TH64_, W64, z_, kChZ, scratch_, nullptr, H64);
     L.note(launch_round_z(z_, z_num_, z_hat_, z_i8_, L.s));
     temporal_prior(L);
     hyper_decoder(L);
@@ -471,19 +503,26 @@ void HtsCodec::enc_analysis(Launch& L)
     L.note(launch_div_clamp(y_, M16_, kChY, kChY, q_dec, ldc, L.s));
     gemm(L, reduction_, kEpiBias, common_, ldc, M16_, cat_spa_ + kChY, 2 * kChY);
     L.note(launch_quantize_phase(0, 0, y_, kChY, scales, ldc, means0, ldc, nullptr, 0,
-                                 skip_thr_half_, y_q_, kChY, cat_spa_, 2 * kChY, H16_, W16_, kChY,
-                                 L.s));
+                                 skip_thr_half_, y_q_, kChY, cat_spa_, 2 * kChY, TH16_, W16_, kChY,
+                                 L.s, 4, H16_));
     for (int k = 1; k < kMaskPhases; ++k) {
         spatial_prior(L, k - 1);
         L.note(launch_quantize_phase(k, k == kMaskPhases - 1 ? 2 : 1, y_, kChY, scales, ldc,
                                      means_, kChY, q_dec, ldc, skip_thr_half_, y_q_, kChY,
-                                     cat_spa_, 2 * kChY, H16_, W16_, kChY, L.s));
+                                     cat_spa_, 2 * kChY, TH16_, W16_, kChY, L.s, 4, H16_));
     }
     L.note(launch_build_index_enc(y_q_, kChY, scales, ldc, skip_thr_half_, scale_lut_, M16_, kChY,
                                   sym_, cond_, L.s));
-    L.note(launch_compact(sym_, 2, cond_, y_num_, block_counts_, sym_c_, count_dev_, L.s), 2);
-    // the symbols, their count and z to the mapped host buffers
-    L.note(launch_copy_counted(sym_c_, sym_hdev_, 2, count_dev_, y_num_, count_hdev_, L.s));
+    // per image: the coded symbols compacted and copied with their count to the mapped host
+    // buffers (each stream's symbols form its own payload)
+    const int nb = compact_blocks(ny_);
+    for (int k = 0; k < imgs_; ++k) {
+        const size_t o = static_cast<size_t>(k) * ny_;
+        L.note(launch_compact(sym_ + o, 2, cond_ + o, ny_, block_counts_ + static_cast<size_t>(k) * nb,
+                              sym_c_ + o, count_dev_ + k, L.s), 2);
+        L.note(launch_copy_counted(sym_c_ + o, sym_hdev_ + o, 2, count_dev_ + k, ny_, count_hdev_ + k,
+                                   L.s));
+    }
     L.note(launch_copy_counted(z_i8_, z_hdev_, 1, nullptr, z_num_, nullptr, L.s));
 }
 
@@ -516,8 +555,14 @@ void HtsCodec::dec_hyper(Launch& L)
     prior_fusion(L);
     L.note(launch_build_index_dec(common_ + kChY, 3 * kChY, skip_thr_half_, scale_lut_, M16_, kChY,
                                   idx_, cond_, L.s));
-    L.note(launch_compact(idx_, 1, cond_, y_num_, block_counts_, idx_c_, count_dev_, L.s), 2);
-    L.note(launch_copy_counted(idx_c_, idx_hdev_, 1, count_dev_, y_num_, count_hdev_, L.s));
+    const int nb = compact_blocks(ny_);
+    for (int k = 0; k < imgs_; ++k) {
+        const size_t o = static_cast<size_t>(k) * ny_;
+        L.note(launch_compact(idx_ + o, 1, cond_ + o, ny_, block_counts_ + static_cast<size_t>(k) * nb,
+                              idx_c_ + o, count_dev_ + k, L.s), 2);
+        L.note(launch_copy_counted(idx_c_ + o, idx_hdev_ + o, 1, count_dev_ + k, ny_, count_hdev_ + k,
+                                   L.s));
+    }
 }
 
 void HtsCodec::dec_context(Launch& L) { feature_extractor(L); }
@@ -527,15 +572,20 @@ void HtsCodec::dec_synthesis(Launch& L)
     const __half* q_dec = common_;
     const __half* means0 = common_ + 2 * kChY;
     const int ldc = 3 * kChY;
-    L.note(launch_copy_counted(ydec_hdev_, y_dec_, 1, count_dev_, y_num_, nullptr, L.s));
-    L.note(launch_recover(y_dec_, cond_, block_counts_, y_num_, y_q_, L.s));
+    const int nb = compact_blocks(ny_);
+    for (int k = 0; k < imgs_; ++k) {  // each stream's decoded values back into its latents
+        const size_t o = static_cast<size_t>(k) * ny_;
+        L.note(launch_copy_counted(ydec_hdev_ + o, y_dec_ + o, 1, count_dev_ + k, ny_, nullptr, L.s));
+        L.note(launch_recover(y_dec_ + o, cond_ + o, block_counts_ + static_cast<size_t>(k) * nb, ny_,
+                              y_q_ + o, L.s));
+    }
     L.note(launch_restore_phase(0, 0, y_q_, kChY, means0, ldc, nullptr, 0, cat_spa_, 2 * kChY,
-                                H16_, W16_, kChY, L.s));
+                                TH16_, W16_, kChY, L.s, 4, H16_));
     gemm(L, reduction_, kEpiBias, common_, ldc, M16_, cat_spa_ + kChY, 2 * kChY);
     for (int k = 1; k < kMaskPhases; ++k) {
         spatial_prior(L, k - 1);
         L.note(launch_restore_phase(k, k == kMaskPhases - 1 ? 2 : 1, y_q_, kChY, means_, kChY,
-                                    q_dec, ldc, cat_spa_, 2 * kChY, H16_, W16_, kChY, L.s));
+                                    q_dec, ldc, cat_spa_, 2 * kChY, TH16_, W16_, kChY, L.s, 4, H16_));
     }
     decoder(L);
     recon_head(L, true);
@@ -601,20 +651,159 @@ int HtsCodec::buffer(const std::string& name, const void** ptr, int* rows, int* 
     return kInvalidArgument;
 }
 
+// ------------------------------------------------------------------------------ sharing
+
+int HtsCodec::share_params(const HtsCodec& o)
+{
+    if (&o == this) {
+        return kOk;
+    }
+    if (!o.ready_) {
+        set_last_error("share_params: the source codec has no parameters");
+        return kNotReady;
+    }
+    if (o.dev_ != dev_) {
+        set_last_error("share_params: the codecs live on different devices");
+        return kInvalidArgument;
+    }
+    if (main_ != nullptr) {
+        cudaStreamSynchronize(main_);
+    }
+    clear_graphs();
+    if (Hp_ != 0 && (o.act_ != act_ || o.fp8_ != fp8_)) {
+        // the arena's precision-form buffers differ: size it again on the next add_ref_feature
+        acts_.clear();
+        Hp_ = Wp_ = 0;
+    }
+    weights_ = o.weights_;
+    precision_ = o.precision_;
+    act_ = o.act_;
+    fp8_ = o.fp8_;
+    skip_threshold_ = o.skip_threshold_;
+    skip_thr_half_ = o.skip_thr_half_;
+    q_enc_tab_ = o.q_enc_tab_;
+    q_dec_tab_ = o.q_dec_tab_;
+    q_feat_tab_ = o.q_feat_tab_;
+    scale_lut_ = o.scale_lut_;
+    std::copy(std::begin(o.encoder_), std::end(o.encoder_), std::begin(encoder_));
+    enc_down_ = o.enc_down_;
+    hyper_enc0_ = o.hyper_enc0_;
+    hyper_enc1_ = o.hyper_enc1_;
+    hyper_enc2_ = o.hyper_enc2_;
+    hyper_dec0_ = o.hyper_dec0_;
+    hyper_dec1_ = o.hyper_dec1_;
+    hyper_dec2_ = o.hyper_dec2_;
+    temporal_ = o.temporal_;
+    std::copy(std::begin(o.prior_fusion_), std::end(o.prior_fusion_), std::begin(prior_fusion_));
+    prior_fusion_out_ = o.prior_fusion_out_;
+    reduction_ = o.reduction_;
+    std::copy(std::begin(o.sp_adaptor_), std::end(o.sp_adaptor_), std::begin(sp_adaptor_));
+    std::copy(std::begin(o.spatial_prior_), std::end(o.spatial_prior_), std::begin(spatial_prior_));
+    spatial_prior_out_ = o.spatial_prior_out_;
+    dec_up_ = o.dec_up_;
+    dec_up_lin_ = o.dec_up_lin_;
+    std::copy(std::begin(o.decoder_), std::end(o.decoder_), std::begin(decoder_));
+    std::copy(std::begin(o.fa_i_), std::end(o.fa_i_), std::begin(fa_i_));
+    std::copy(std::begin(o.fa_m_), std::end(o.fa_m_), std::begin(fa_m_));
+    std::copy(std::begin(o.fe_), std::end(o.fe_), std::begin(fe_));
+    std::copy(std::begin(o.rh_common_), std::end(o.rh_common_), std::begin(rh_common_));
+    for (int i = 0; i < kFrames; ++i) {
+        std::copy(std::begin(o.rh_frame_[i]), std::end(o.rh_frame_[i]), std::begin(rh_frame_[i]));
+    }
+    std::copy(std::begin(o.rh_head_), std::end(o.rh_head_), std::begin(rh_head_));
+    tables_ = o.tables_;
+    ready_ = true;
+    return kOk;
+}
+
+size_t HtsCodec::state_bytes() const
+{
+    if (Hp_ == 0) {
+        return 0;
+    }
+    return static_cast<size_t>(M8_) * (1024 + kChD + kChSrcIntra) * 2;
+}
+
+int HtsCodec::export_state(void* dst, cudaStream_t caller, int* flags)
+{
+    if (Hp_ == 0 || dst == nullptr || flags == nullptr) {
+        set_last_error("export_state: no resolution allocated yet, or a null argument");
+        return Hp_ == 0 ? kNotReady : kInvalidArgument;
+    }
+    const size_t M8 = M8_;
+    uint8_t* d = static_cast<uint8_t*>(dst);
+    // the copies follow the codec's last call; the codec's next work follows the copies
+    cudaEventRecord(ev_state_, main_);
+    cudaStreamWaitEvent(caller, ev_state_, 0);
+    cudaError_t e = cudaMemcpyAsync(d, cat_fam_, M8 * 1024 * 2, cudaMemcpyDeviceToDevice, caller);
+    d += M8 * 1024 * 2;
+    if (e == cudaSuccess) {
+        e = cudaMemcpy2DAsync(d, kChD * 2, cat_enc_ + kChSrc, 2048 * 2, kChD * 2, M8,
+                              cudaMemcpyDeviceToDevice, caller);
+    }
+    d += M8 * kChD * 2;
+    if (e == cudaSuccess) {
+        e = cudaMemcpyAsync(d, feature_i_, M8 * kChSrcIntra * 2, cudaMemcpyDeviceToDevice, caller);
+    }
+    cudaEventRecord(ev_state_, caller);
+    cudaStreamWaitEvent(main_, ev_state_, 0);
+    *flags = memory_has_value_ ? 1 : 0;
+    return cuda_status(e, "export_state");
+}
+
+int HtsCodec::import_state(const void* src, int flags, cudaStream_t caller)
+{
+    if (Hp_ == 0 || src == nullptr) {
+        set_last_error("import_state: no resolution allocated yet (add_ref_feature first), or a "
+                       "null source");
+        return Hp_ == 0 ? kNotReady : kInvalidArgument;
+    }
+    const size_t M8 = M8_;
+    const uint8_t* s = static_cast<const uint8_t*>(src);
+    cudaEventRecord(ev_state_, main_);
+    cudaStreamWaitEvent(caller, ev_state_, 0);
+    cudaError_t e = cudaMemcpyAsync(cat_fam_, s, M8 * 1024 * 2, cudaMemcpyDeviceToDevice, caller);
+    s += M8 * 1024 * 2;
+    if (e == cudaSuccess) {
+        e = cudaMemcpy2DAsync(cat_enc_ + kChSrc, 2048 * 2, s, kChD * 2, kChD * 2, M8,
+                              cudaMemcpyDeviceToDevice, caller);
+    }
+    s += M8 * kChD * 2;
+    if (e == cudaSuccess) {
+        e = cudaMemcpyAsync(feature_i_, s, M8 * kChSrcIntra * 2, cudaMemcpyDeviceToDevice, caller);
+    }
+    cudaEventRecord(ev_state_, caller);
+    cudaStreamWaitEvent(main_, ev_state_, 0);
+    memory_has_value_ = flags != 0;
+    return cuda_status(e, "import_state");
+}
+
 // ------------------------------------------------------------------------------ public calls
 
 int HtsCodec::add_ref_feature(const __half* frame, int Hp, int Wp, bool apply_adaptor,
                               cudaStream_t caller)
 {
+    return add_ref_features(&frame, 1, Hp, Wp, apply_adaptor, caller);
+}
+
+int HtsCodec::add_ref_features(const __half* const* frames, int n, int Hp, int Wp,
+                               bool apply_adaptor, cudaStream_t caller)
+{
     if (!ready_) {
         set_last_error("add_ref_feature_from_frame: set_param has not been called");
         return kNotReady;
     }
-    if (frame == nullptr) {
+    if (frames == nullptr || n < 1) {
         set_last_error("add_ref_feature_from_frame: null frame");
         return kInvalidArgument;
     }
-    int st = allocate(Hp, Wp);
+    for (int k = 0; k < n; ++k) {
+        if (frames[k] == nullptr) {
+            set_last_error("add_ref_feature_from_frame: null frame");
+            return kInvalidArgument;
+        }
+    }
+    int st = allocate(Hp, Wp, n);
     if (st != kOk) {
         return st;
     }
@@ -622,7 +811,11 @@ int HtsCodec::add_ref_feature(const __half* frame, int Hp, int Wp, bool apply_ad
     cudaEventRecord(ev_in_, caller);
     cudaStreamWaitEvent(main_, ev_in_, 0);
     Launch L{main_, err_word_};
-    L.note(launch_pad_unshuffle8(frame, Hp, Wp, 3, 3, 0, 0, feature_i_, kChSrcIntra, main_, act_));
+    for (int k = 0; k < n; ++k) {
+        L.note(launch_pad_unshuffle8(frames[k], Hp, Wp, 3, 3, 0, 0,
+                                     feature_i_ + static_cast<size_t>(k) * m8_ * kChSrcIntra,
+                                     kChSrcIntra, main_, act_));
+    }
     if (apply_adaptor) {
         feature_adaptor_i(L, feature_i_);
         feature_extractor(L);
@@ -634,25 +827,62 @@ int HtsCodec::add_ref_feature(const __half* frame, int Hp, int Wp, bool apply_ad
     return cuda_status(L.first, "add_ref_feature_from_frame");
 }
 
+namespace {
+
+// Runs fn(k) for k in [0, n): inline for one item, else on one thread per item (the items are
+// independent rANS payloads of a packed batch).
+template <typename F>
+void for_each_stream(int n, F&& fn)
+{
+    if (n == 1) {
+        fn(0);
+        return;
+    }
+    std::vector<std::thread> th;
+    th.reserve(n);
+    for (int k = 0; k < n; ++k) {
+        th.emplace_back([&fn, k] { fn(k); });
+    }
+    for (auto& t : th) {
+        t.join();
+    }
+}
+
+}  // namespace
+
 int HtsCodec::compress(const __half* x, int H, int W, int qp, bool reset, int pad_b, int pad_r,
                        cudaStream_t caller, std::vector<uint8_t>* bytes, int* ec_parallel)
+{
+    return compress_batch(&x, 1, H, W, &qp, reset, pad_b, pad_r, caller, bytes, ec_parallel);
+}
+
+int HtsCodec::compress_batch(const __half* const* xs, int n, int H, int W, const int* qps,
+                             bool reset, int pad_b, int pad_r, cudaStream_t caller,
+                             std::vector<uint8_t>* bytes, int* ec_parallel)
 {
     if (!ready_ || Hp_ == 0) {
         set_last_error("compress: set_param and add_ref_feature_from_frame must come first");
         return kNotReady;
     }
-    if (x == nullptr || qp < 0 || qp >= kQpNum || pad_b < 0 || pad_r < 0 || H + pad_b != Hp_ ||
-        W + pad_r != Wp_) {
-        set_last_error("compress: bad input pointer, qp or size (input + padding must equal the "
-                       "reference frame size)");
+    bool ok = xs != nullptr && qps != nullptr && bytes != nullptr && ec_parallel != nullptr &&
+              n == imgs_ && pad_b >= 0 && pad_r >= 0 && H + pad_b == Hp_ && W + pad_r == Wp_;
+    for (int k = 0; ok && k < n; ++k) {
+        ok = xs[k] != nullptr && qps[k] >= 0 && qps[k] < kQpNum;
+    }
+    if (!ok) {
+        set_last_error("compress: bad input pointer, qp, stream count or size (input + padding "
+                       "must equal the reference frame size, one input per stream of the batch)");
         return kInvalidArgument;
     }
     last_kernels_ = 0;
     cudaEventRecord(ev_in_, caller);
     cudaStreamWaitEvent(main_, ev_in_, 0);
-    set_qp(qp, main_);
+    set_qp(qps, main_);
     Launch L{main_, err_word_};
-    L.note(launch_pad_unshuffle8(x, H, W, 24, 24, pad_b, pad_r, cat_enc_, 2048, main_, act_));
+    for (int k = 0; k < n; ++k) {
+        L.note(launch_pad_unshuffle8(xs[k], H, W, 24, 24, pad_b, pad_r,
+                                     cat_enc_ + static_cast<size_t>(k) * m8_ * 2048, 2048, main_, act_));
+    }
     last_kernels_ += L.kernels;
     int st = cuda_status(L.first, "compress: pad_and_unshuffle_8");
     if (st == kOk) st = run_phase(kEncAnalysis, main_);
@@ -671,53 +901,85 @@ int HtsCodec::compress(const __half* x, int H, int W, int qp, bool reset, int pa
     if (st != kOk) {
         return st;
     }
-    const int count = *count_host_;
-    if (count < 0 || count > y_num_) {
-        set_last_error("compress: symbol count out of range");
-        return kInternal;
+    for (int k = 0; k < n; ++k) {
+        if (count_host_[k] < 0 || count_host_[k] > ny_) {
+            set_last_error("compress: symbol count out of range");
+            return kInternal;
+        }
     }
-    const int ecp = ec_parallel_for(count);
-    RansEncoderSession enc;
-    enc.reset(ecp);
-    enc.add_y(sym_host_, count, false);
-    enc.add_z(z_host_, z_num_, qp * kChZ, kChZ, false);
-    std::string err;
-    if (!enc.finish(tables_, bytes, &err)) {
-        set_last_error("compress: " + err);
-        return kInternal;
+    std::vector<std::string> errs(n);
+    std::vector<char> good(n, 0);
+    for_each_stream(n, [&](int k) {
+        const int count = count_host_[k];
+        const int ecp = ec_parallel_for(count);
+        RansEncoderSession enc;
+        enc.reset(ecp);
+        enc.add_y(sym_host_ + static_cast<size_t>(k) * ny_, count, false);
+        enc.add_z(z_host_ + static_cast<size_t>(k) * nz_, nz_, qps[k] * kChZ, kChZ, false);
+        good[k] = enc.finish(tables_, &bytes[k], &errs[k]) ? 1 : 0;
+        ec_parallel[k] = ecp;
+    });
+    last_count_ = 0;
+    for (int k = 0; k < n; ++k) {
+        if (!good[k]) {
+            set_last_error("compress: " + errs[k]);
+            return kInternal;
+        }
+        last_count_ += count_host_[k];
     }
-    *ec_parallel = ecp;
-    last_count_ = count;
     return kOk;
 }
 
 int HtsCodec::decompress(const uint8_t* bytes, size_t n, int qp, int height, int width, int ecp,
                          bool reset, cudaStream_t caller, const __half** frames)
 {
+    return decompress_batch(&bytes, &n, &qp, &ecp, 1, height, width, reset, caller, frames);
+}
+
+int HtsCodec::decompress_batch(const uint8_t* const* bytes, const size_t* sizes, const int* qps,
+                               const int* ecps, int n, int height, int width, bool reset,
+                               cudaStream_t caller, const __half** frames)
+{
     if (!ready_ || Hp_ == 0) {
         set_last_error("decompress: set_param and add_ref_feature_from_frame must come first");
         return kNotReady;
     }
-    if (qp < 0 || qp >= kQpNum || ecp < 1 || ecp > kMaxEcParallel || n > 0x7fffffff ||
-        (n > 0 && bytes == nullptr) || height <= 0 || width <= 0 ||
-        (height + 63) / 64 != H16p_ / 4 || (width + 63) / 64 != W16p_ / 4 ||
-        ceil_to(height, 16) != Hp_ || ceil_to(width, 16) != Wp_) {
-        set_last_error("decompress: bad qp, ec_parallel, stream or picture size (the size must "
-                       "match the reference frame)");
+    bool ok = bytes != nullptr && sizes != nullptr && qps != nullptr && ecps != nullptr &&
+              frames != nullptr && n == imgs_ && height > 0 && width > 0 &&
+              (height + 63) / 64 == H16p_ / 4 && (width + 63) / 64 == W16p_ / 4 &&
+              ceil_to(height, 16) == Hp_ && ceil_to(width, 16) == Wp_;
+    for (int k = 0; ok && k < n; ++k) {
+        ok = qps[k] >= 0 && qps[k] < kQpNum && ecps[k] >= 1 && ecps[k] <= kMaxEcParallel &&
+             sizes[k] <= 0x7fffffff && (sizes[k] == 0 || bytes[k] != nullptr);
+    }
+    if (!ok) {
+        set_last_error("decompress: bad qp, ec_parallel, stream, stream count or picture size (the "
+                       "size must match the reference frame)");
         return kInvalidArgument;
     }
     last_kernels_ = 0;
     cudaEventRecord(ev_in_, caller);
     cudaStreamWaitEvent(main_, ev_in_, 0);
-    set_qp(qp, main_);
+    set_qp(qps, main_);
     int st = run_phase(kDecTemporal + (memory_has_value_ ? 1 : 0), main_);
     // z on the CPU while the temporal branch runs (dmc_hts_proxy.cpp:794-804)
-    RansDecoderSession dec;
-    std::string err;
-    if (st == kOk && (!dec.begin(bytes, static_cast<int>(n), ecp, &err) ||
-                      !dec.decode_z(tables_, z_num_, qp * kChZ, kChZ, z_host_, &err))) {
-        set_last_error("decompress: " + err);
-        st = dec.fault() ? kInternal : kCorruptStream;
+    std::vector<RansDecoderSession> dec(n);
+    std::vector<std::string> errs(n);
+    std::vector<int> res(n, kOk);
+    if (st == kOk) {
+        for_each_stream(n, [&](int k) {
+            if (!dec[k].begin(bytes[k], static_cast<int>(sizes[k]), ecps[k], &errs[k]) ||
+                !dec[k].decode_z(tables_, nz_, qps[k] * kChZ, kChZ,
+                                 z_host_ + static_cast<size_t>(k) * nz_, &errs[k])) {
+                res[k] = dec[k].fault() ? kInternal : kCorruptStream;
+            }
+        });
+        for (int k = 0; k < n && st == kOk; ++k) {
+            if (res[k] != kOk) {
+                set_last_error("decompress: " + errs[k]);
+                st = res[k];
+            }
+        }
     }
     if (st == kOk) {
         st = run_phase(kDecHyper, main_);
@@ -730,18 +992,26 @@ int HtsCodec::decompress(const uint8_t* bytes, size_t n, int qp, int height, int
         }
     }
     if (st == kOk) st = check_device_error_word(err_word_, err_slot_, "decompress");
-    int count = 0;
-    if (st == kOk) {
-        count = *count_host_;
-        if (count < 0 || count > y_num_) {
+    for (int k = 0; k < n && st == kOk; ++k) {
+        if (count_host_[k] < 0 || count_host_[k] > ny_) {
             set_last_error("decompress: symbol count out of range");
             st = kInternal;
         }
     }
     // y on the CPU while the feature extractor runs (dmc_hts_proxy.cpp:805-823)
-    if (st == kOk && !dec.decode_y(tables_, idx_host_, count, ydec_host_, &err)) {
-        set_last_error("decompress: " + err);
-        st = dec.fault() ? kInternal : kCorruptStream;
+    if (st == kOk) {
+        for_each_stream(n, [&](int k) {
+            const size_t o = static_cast<size_t>(k) * ny_;
+            if (!dec[k].decode_y(tables_, idx_host_ + o, count_host_[k], ydec_host_ + o, &errs[k])) {
+                res[k] = dec[k].fault() ? kInternal : kCorruptStream;
+            }
+        });
+        for (int k = 0; k < n && st == kOk; ++k) {
+            if (res[k] != kOk) {
+                set_last_error("decompress: " + errs[k]);
+                st = res[k];
+            }
+        }
     }
     if (st == kOk) {
         st = run_phase(kDecSynthesis, main_);
@@ -751,7 +1021,10 @@ int HtsCodec::decompress(const uint8_t* bytes, size_t n, int qp, int height, int
         for (int i = 0; i < kFrames; ++i) {
             frames[i] = x_hat_[i];
         }
-        last_count_ = count;
+        last_count_ = 0;
+        for (int k = 0; k < n; ++k) {
+            last_count_ += count_host_[k];
+        }
     }
     cudaEventRecord(ev_out_, main_);
     cudaStreamWaitEvent(caller, ev_out_, 0);

@@ -8,6 +8,7 @@
 
 #include <cuda_runtime.h>
 
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -51,6 +52,25 @@ public:
     int decompress(const uint8_t* bytes, size_t n, int qp, int height, int width, int ecp,
                    bool reset, cudaStream_t s, const __half** frames);
 
+    // Packed batches: n streams of one resolution coded together, every layer of the network one
+    // launch over the n images stacked along the rows (the 1x1 GEMMs see n times the pixels; the
+    // depthwise convolutions and checkerboard masks keep each image's own borders and parity; each
+    // stream has its own QP rows and its own rANS payload, coded on its own host thread).  The
+    // temporal state of all n streams lives in this codec; add_ref_features sizes it for n
+    // streams.  One reset flag covers the batch.  Each stream's payload and reconstruction are
+    // bitwise those of a single-stream codec given the same inputs.  decompress_batch returns 8
+    // frames, each [n * Hp, Wp, 3] with stream k's frame in rows k * Hp ..
+    static constexpr int kMaxBatch = 64;
+    int add_ref_features(const __half* const* frames, int n, int Hp, int Wp, bool apply_adaptor,
+                         cudaStream_t s);
+    int compress_batch(const __half* const* xs, int n, int H, int W, const int* qps, bool reset,
+                       int pad_b, int pad_r, cudaStream_t s, std::vector<uint8_t>* bytes,
+                       int* ec_parallel);
+    int decompress_batch(const uint8_t* const* bytes, const size_t* sizes, const int* qps,
+                         const int* ecps, int n, int height, int width, bool reset, cudaStream_t s,
+                         const __half** frames);
+    int batch_size() const { return imgs_; }
+
     // Read-only view of an internal buffer for inspection and tests: "y_hat", "y_q", "memory",
     // "ctx", "feature_p", "common", "feature_i".  rows x cols 16-bit values with pitch ld, in the
     // format *dtype (0 FP16, 1 BF16: "memory", "ctx", "feature_p" and "feature_i" follow the
@@ -58,9 +78,24 @@ public:
     int buffer(const std::string& name, const void** ptr, int* rows, int* cols, int* ld,
                int* dtype = nullptr) const;
 
+    // Uses the prepared parameters of `other` (same device) instead of a copy of its own: every
+    // parameter device buffer is shared and held until the last codec using it is destroyed or
+    // re-parameterised.  The counterpart of one set_param with the same state dict.
+    int share_params(const HtsCodec& other);
+
+    // The per-stream temporal context (memory and decoded feature, ctx, the I-frame feature and
+    // whether memory holds a value), so that a stream's state can live outside the codec that
+    // codes it: a serving loop keeps one state per stream and runs its chunks on whichever codec
+    // of that resolution is free.  export/import copy device to device on the caller's stream
+    // and order the codec's own stream after the copies; the layout is private to this build.
+    size_t state_bytes() const;
+    int export_state(void* dst, cudaStream_t s, int* flags);
+    int import_state(const void* src, int flags, cudaStream_t s);
+
     // Statistics of the last call, for reporting.
     int last_symbol_count() const { return last_count_; }
-    size_t device_bytes() const { return weights_.bytes() + acts_.bytes(); }
+    size_t device_bytes() const { return (weights_ ? weights_->bytes() : 0) + acts_.bytes(); }
+    size_t activation_bytes() const { return acts_.bytes(); }
     // Number of kernels the last compress/decompress enqueued (graph nodes included).
     int last_kernel_count() const { return last_kernels_; }
 
@@ -75,7 +110,7 @@ private:
         kPhaseSlots = 8,
     };
 
-    int allocate(int Hp, int Wp);
+    int allocate(int Hp, int Wp, int imgs);
     void clear_graphs();
     int run_phase(int slot, cudaStream_t s);
     void record_phase(int slot, Launch& L);
@@ -97,10 +132,10 @@ private:
     void spatial_prior(Launch& L, int k);
     void decoder(Launch& L);
     void recon_head(Launch& L, bool all_frames);
-    void set_qp(int qp, cudaStream_t s);
+    void set_qp(const int* qps, cudaStream_t s);  // one QP per stream of the batch
 
     // ---------------------------------------------------------------- parameters
-    DeviceArena weights_;
+    std::shared_ptr<DeviceArena> weights_;  // shared by codecs that share_params
     bool ready_ = false;
     int precision_ = kPrecisionF16;  // requested form
     int act_ = 0;                    // activation format of the transforms as set up (0 / 1)
@@ -138,8 +173,13 @@ private:
     // ---------------------------------------------------------------- resolution state
     DeviceArena acts_;
     int Hp_ = 0, Wp_ = 0, H8_ = 0, W8_ = 0, H16_ = 0, W16_ = 0, H16p_ = 0, W16p_ = 0;
-    int M8_ = 0, M16_ = 0, M16p_ = 0, M32_ = 0, M64_ = 0;
+    int M8_ = 0, M16_ = 0, M16p_ = 0, M32_ = 0, M64_ = 0;  // rows over all images of the batch
     int y_num_ = 0, z_num_ = 0;
+    // packed batch: images, their rows stacked (TH*), rows of one image (m*), latents of one image
+    int imgs_ = 0;
+    int TH8_ = 0, TH16_ = 0, TH16p_ = 0, TH32_ = 0, TH64_ = 0;
+    int m8_ = 0, m16_ = 0, m16p_ = 0;
+    int ny_ = 0, nz_ = 0;
     __half *cat_enc_ = nullptr, *cat_fam_ = nullptr, *feature_i_ = nullptr, *temporal_in_ = nullptr;
     __half *y_ = nullptr, *y_pad_ = nullptr, *cat_pf_ = nullptr, *hyper_pad_ = nullptr;
     __half *common_ = nullptr, *cat_spa_ = nullptr, *means_ = nullptr, *y_q_ = nullptr;
@@ -174,6 +214,7 @@ private:
     PhaseGraphs graphs_{kPhaseSlots};
     cudaStream_t main_ = nullptr;   // compute stream (graphs run here)
     cudaEvent_t ev_in_ = nullptr, ev_phase_ = nullptr, ev_out_ = nullptr;
+    cudaEvent_t ev_state_ = nullptr;  // state copies on a caller's stream, waited for by main_
     int* err_word_ = nullptr;
     ErrorSlot err_slot_;  // the error word as the phase graphs publish it
     int last_count_ = 0;

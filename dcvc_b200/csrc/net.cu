@@ -355,7 +355,7 @@ Lin ParamBuilder::conv3x3s2(const std::string& p)
 
 void gemm(Launch& L, const Lin& lin, int epi, const __half* x, int ldx, int M, __half* out,
           int ldo, const __half* res, int ldr, const __half* q, int sub_w, const __half* res2,
-          int ldr2)
+          int ldr2, int q_rows)
 {
     GemmParams p{};
     p.M = M;
@@ -371,6 +371,7 @@ void gemm(Launch& L, const Lin& lin, int epi, const __half* x, int ldx, int M, _
     p.ldo = ldo;
     p.sub_w = sub_w;
     p.sub_cout = epi == kEpiSubpel ? lin.cout / 4 : 0;
+    p.q_rows = q != nullptr ? q_rows : 0;
     p.err = L.err_word;
     // the autotuned width of this shape (tuned here on first sight when tuning is enabled and
     // the phase runs eagerly), else the library's rule
@@ -379,8 +380,10 @@ void gemm(Launch& L, const Lin& lin, int epi, const __half* x, int ldx, int M, _
 }
 
 void run_dcb(Launch& L, const Dcb& d, const __half* x, int ldx, int H, int W, __half* out, int ldo,
-             Scratch& s, const __half* q)
+             Scratch& s, const __half* q, int img_h)
 {
+    // per-image factors in a packed batch: one row of q per image of img_h x W pixels
+    const int q_rows = (img_h > 0 && img_h < H) ? img_h * W : 0;
     const int M = H * W;
     const __half* xin = x;
     int ldin = ldx;
@@ -390,9 +393,10 @@ void run_dcb(Launch& L, const Dcb& d, const __half* x, int ldx, int H, int W, __
         ldin = d.C;
     }
     gemm(L, d.dc1, kEpiBiasWsilu, xin, ldin, M, s.t1, d.cdc);
-    L.note(launch_dwconv3x3(s.t1, H, W, d.cdc, d.cdc, d.dw, s.t2, d.cdc, L.s, d.dtype));
+    L.note(launch_dwconv3x3(s.t1, H, W, d.cdc, d.cdc, d.dw, s.t2, d.cdc, L.s, d.dtype, img_h));
     gemm(L, d.dc2, kEpiBiasRes, s.t2, d.cdc, M, s.t3, d.C, xin, ldin);
-    if (!d.shortcut && d.dtype == 0 && ffn_sm100_preferred(d.C, d.cffn, d.ffn1.cout)) {
+    if (!d.shortcut && d.dtype == 0 && (q == nullptr || q_rows == 0) &&
+        ffn_sm100_preferred(d.C, d.cffn, d.ffn1.cout)) {
         // the ConvFFN as one kernel, the quad output kept on chip (ffn_sm100.cu)
         FfnParams fp{M, d.C, d.cffn, d.ffn1.b, d.ffn2.b, q, out, ldo, L.err_word, 0};
         L.note(ffn_sm100(s.t3, d.C, d.ffn1.w, d.ffn2.w, fp, L.s));
@@ -420,7 +424,8 @@ void run_dcb(Launch& L, const Dcb& d, const __half* x, int ldx, int H, int W, __
         return;
     }
     if (q != nullptr) {
-        gemm(L, d.ffn2, kEpiBiasResQ, s.t4, d.cffn, M, out, ldo, s.t3, d.C, q);
+        gemm(L, d.ffn2, kEpiBiasResQ, s.t4, d.cffn, M, out, ldo, s.t3, d.C, q, 0, nullptr, 0,
+             q_rows);
     } else {
         gemm(L, d.ffn2, kEpiBiasRes, s.t4, d.cffn, M, out, ldo, s.t3, d.C);
     }

@@ -158,14 +158,17 @@ struct Launch {
     }
 };
 
-// out[M, cout] (pitch ldo) = epilogue(x[M, cin] (pitch ldx) . lin)
+// out[M, cout] (pitch ldo) = epilogue(x[M, cin] (pitch ldx) . lin).  q_rows > 0: the rows are
+// images of q_rows rows each and q holds one row of factors per image.
 void gemm(Launch& L, const Lin& lin, int epi, const __half* x, int ldx, int M, __half* out,
           int ldo, const __half* res = nullptr, int ldr = 0, const __half* q = nullptr,
-          int sub_w = 0, const __half* res2 = nullptr, int ldr2 = 0);
+          int sub_w = 0, const __half* res2 = nullptr, int ldr2 = 0, int q_rows = 0);
 
 // DepthConvBlockProxy::forward (layers_proxy.cpp:71-101).  `out` may alias `x` unless the block
-// has a shortcut (its last GEMM then reads the block input as a second residual).
+// has a shortcut (its last GEMM then reads the block input as a second residual).  A packed
+// batch passes H = images * img_h rows of stacked images (img_h = 0: one image) and, with a
+// per-image q, one row of factors per image.
 void run_dcb(Launch& L, const Dcb& d, const __half* x, int ldx, int H, int W, __half* out, int ldo,
-             Scratch& s, const __half* q = nullptr);
+             Scratch& s, const __half* q = nullptr, int img_h = 0);
 
 }  // namespace dcvc

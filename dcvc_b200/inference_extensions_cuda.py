@@ -42,6 +42,22 @@ for _k in ("hts", "htl", "ld"):
     _proto(f"dcvc_{_k}_stats", [_vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                  ctypes.POINTER(ctypes.c_size_t)])
 _proto("dcvc_hts_set_precision", [_vp, ctypes.c_int])
+_proto("dcvc_hts_share_params", [_vp, _vp])
+_proto("dcvc_hts_add_ref_features", [_vp, ctypes.POINTER(_vp), ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_int, ctypes.c_int, _vp])
+_proto("dcvc_hts_compress_batch", [_vp, ctypes.POINTER(_vp), ctypes.c_int, ctypes.c_int,
+                                   ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_int,
+                                   ctypes.c_int, ctypes.c_int, _vp,
+                                   ctypes.POINTER(ctypes.POINTER(_vp)),
+                                   ctypes.POINTER(ctypes.POINTER(ctypes.c_size_t)),
+                                   ctypes.POINTER(ctypes.c_int)])
+_proto("dcvc_hts_decompress_batch", [_vp, ctypes.POINTER(_vp), ctypes.POINTER(ctypes.c_size_t),
+                                     ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                     ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp,
+                                     ctypes.POINTER(_vp)])
+_proto("dcvc_hts_state_bytes", [_vp, ctypes.POINTER(ctypes.c_size_t)])
+_proto("dcvc_hts_export_state", [_vp, _vp, _vp, ctypes.POINTER(ctypes.c_int)])
+_proto("dcvc_hts_import_state", [_vp, _vp, ctypes.c_int, _vp])
 _proto("dcvc_hts_buffer_dtype", [_vp, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int)])
 _proto("dcvc_intra_create", [ctypes.POINTER(_vp)])
 _proto("dcvc_intra_destroy", [_vp])
@@ -184,6 +200,96 @@ class DMCHTSProxy(_Proxy):
         elif precision != "fp16":
             raise ValueError(f"{type(self).__name__} runs in the fp16 form only")
         self.precision = precision
+
+    # ---- packed batches: n streams of one resolution per call (HT-S only; an extension)
+    def add_ref_features_from_frames(self, frames, apply_adaptor=True):
+        """Seeds n streams (and sizes the codec for them) from n [1, 3, Hp, Wp] float16 frames."""
+        self._hts_only("add_ref_features_from_frames")
+        frames = [_channels_last_data(f, "frame") for f in frames]
+        n = len(frames)
+        ptrs = (_vp * n)(*[f.data_ptr() for f in frames])
+        N.check(_lib.dcvc_hts_add_ref_features(self._h, ptrs, n, frames[0].shape[2],
+                                               frames[0].shape[3], 1 if apply_adaptor else 0,
+                                               _stream()), "add_ref_features_from_frames")
+
+    def compress_batch(self, xs, qps, reset_feature_memory, padding_b, padding_r):
+        """xs: n [1, 24, H, W] float16 CUDA chunks, qps: n QPs.  Returns n (uint8 array,
+        ec_parallel) pairs, each equal to what a single-stream proxy returns for that stream."""
+        self._hts_only("compress_batch")
+        xs = [_channels_last_data(x, "x") for x in xs]
+        n = len(xs)
+        ptrs = (_vp * n)(*[x.data_ptr() for x in xs])
+        q = (ctypes.c_int * n)(*[int(v) for v in qps])
+        data = ctypes.POINTER(_vp)()
+        sizes = ctypes.POINTER(ctypes.c_size_t)()
+        ecp = (ctypes.c_int * n)()
+        N.check(_lib.dcvc_hts_compress_batch(self._h, ptrs, n, xs[0].shape[2], xs[0].shape[3], q,
+                                             1 if reset_feature_memory else 0, int(padding_b),
+                                             int(padding_r), _stream(), ctypes.byref(data),
+                                             ctypes.byref(sizes), ecp), "compress_batch")
+        out = []
+        for k in range(n):
+            sz = ctypes.c_size_t(sizes[k])
+            out.append((_bytes_out(_vp(data[k]), sz), ecp[k]))
+        return out
+
+    def decompress_batch(self, payloads, qps, height, width, ec_parallels, reset_feature_memory):
+        """n payloads -> 8 [n, 3, Hp, Wp] float16 CUDA tensors (frame i of every stream; stream k
+        is index k), aliasing the proxy's buffers until its next call."""
+        self._hts_only("decompress_batch")
+        bs = [np.ascontiguousarray(np.asarray(b, dtype=np.uint8).reshape(-1)) for b in payloads]
+        n = len(bs)
+        ptrs = (_vp * n)(*[b.ctypes.data for b in bs])
+        sizes = (ctypes.c_size_t * n)(*[b.size for b in bs])
+        q = (ctypes.c_int * n)(*[int(v) for v in qps])
+        e = (ctypes.c_int * n)(*[int(v) for v in ec_parallels])
+        frames = (_vp * FRAMES)()
+        N.check(_lib.dcvc_hts_decompress_batch(self._h, ptrs, sizes, q, e, n, int(height),
+                                               int(width), 1 if reset_feature_memory else 0,
+                                               _stream(), frames), "decompress_batch")
+        hp = (int(height) + 15) // 16 * 16
+        wp = (int(width) + 15) // 16 * 16
+        return [torch.as_tensor(_DeviceView(frames[i], (n, hp, wp, 3)), device="cuda").permute(0, 3, 1, 2)
+                for i in range(FRAMES)]
+
+    # ---- extensions for serving many streams (HT-S only; no counterpart in the reference)
+    def share_params_from(self, other):
+        """Use `other`'s prepared parameters (same device) instead of a set_param of our own."""
+        self._hts_only("share_params_from")
+        N.check(_lib.dcvc_hts_share_params(self._h, other._h), "share_params_from")
+        self.precision = other.precision
+
+    def state_bytes(self):
+        self._hts_only("state_bytes")
+        n = ctypes.c_size_t()
+        N.check(_lib.dcvc_hts_state_bytes(self._h, ctypes.byref(n)), "state_bytes")
+        return n.value
+
+    def export_state(self, out=None):
+        """The stream's temporal context as (uint8 CUDA tensor, flags), copied on the current
+        stream (into `out` when given)."""
+        self._hts_only("export_state")
+        n = self.state_bytes()
+        if out is None:
+            out = torch.empty(n, dtype=torch.uint8, device="cuda")
+        if out.numel() < n or not out.is_cuda:
+            raise ValueError(f"state buffer must be a CUDA uint8 tensor of {n} bytes")
+        flags = ctypes.c_int()
+        N.check(_lib.dcvc_hts_export_state(self._h, out.data_ptr(), _stream(), ctypes.byref(flags)),
+                "export_state")
+        return out, flags.value
+
+    def import_state(self, state, flags):
+        """Replaces the temporal context with one exported at the same resolution and form."""
+        self._hts_only("import_state")
+        if state.numel() < self.state_bytes():
+            raise ValueError("state buffer is smaller than this codec's state")
+        N.check(_lib.dcvc_hts_import_state(self._h, state.data_ptr(), int(flags), _stream()),
+                "import_state")
+
+    def _hts_only(self, what):
+        if self._kind != "hts":
+            raise NotImplementedError(f"{what} is implemented for DMCHTSProxy only")
 
     def _buffer_dtype(self, name):
         if self._kind != "hts":

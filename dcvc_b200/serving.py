@@ -6,8 +6,9 @@ keeps the stream's temporal context inside it, dmc_hts_proxy.h:215-355; the harn
 chunks of a sequence one after another, test_video.py:300-345).  This module keeps that contract
 per stream and serves many streams at once:
 
-* every stream owns a session (a codec proxy holding its temporal context in device memory, plus
-  a CUDA stream); the requests of one stream run in arrival order, one at a time;
+* every stream owns a session (its temporal context in device memory and a CUDA stream; the
+  codecs that run its chunks come from a pool shared by all sessions, see HtsSessionFactory);
+  the requests of one stream run in arrival order, one at a time;
 * `slots` worker threads run the head requests of different streams concurrently, so the kernels
   of one chunk fill the launch gaps, tails and host entropy-coding waits of the others; a request
   that arrives while others are on the GPU starts as soon as a slot frees, not after a batch;
@@ -176,27 +177,32 @@ class ChunkServer:
             if st is None:
                 return
             st.closing = True
-            self._maybe_release(stream_id, st)
+            done = self._maybe_release(stream_id, st)
             self._cv.notify_all()
+        self._close_all([done])
 
     def shutdown(self, wait=True):
         """Runs the queued requests, then stops the workers; every stream is closed (idle
         sessions are released at once, which also lets streams waiting for memory in)."""
+        done = []
         with self._cv:
             self._stop = True
             for sid in list(self._streams):
                 st = self._streams[sid]
                 st.closing = True
-                self._maybe_release(sid, st)
+                done.append(self._maybe_release(sid, st))
             self._cv.notify_all()
+        self._close_all(done)
         if wait:
             for t in self._workers:
                 t.join()
+            done = []
             with self._cv:
                 for sid in list(self._streams):
                     st = self._streams[sid]
                     st.closing = True
-                    self._maybe_release(sid, st)
+                    done.append(self._maybe_release(sid, st))
+            self._close_all(done)
 
     def set_in_flight_limit(self, n):
         """Caps the requests in flight at n (1 .. slots); 1 serves one request at a time, as the
@@ -244,17 +250,24 @@ class ChunkServer:
                    for st in self._streams.values())
 
     def _maybe_release(self, sid, st):
+        """Takes a finished closing stream off the server (call with the lock held).  Returns
+        its session, which the caller closes after releasing the lock: closing waits for the
+        session's GPU work, and no other slot or client should wait behind that."""
         if st.closing and not st.pending and not st.running and not st.opening:
-            if st.session is not None:
-                try:
-                    st.session.close()
-                finally:
-                    st.session = None
+            session, st.session = st.session, None
             self._held -= st.reserved
             st.reserved = 0
             self._streams.pop(sid, None)
             if sid in self._admit_queue:
                 self._admit_queue.remove(sid)
+            return session
+        return None
+
+    @staticmethod
+    def _close_all(sessions):
+        for session in sessions:
+            if session is not None:
+                session.close()
 
     def _worker(self):
         if self._on_worker_start is not None:
@@ -298,8 +311,9 @@ class ChunkServer:
                     self.completed += 1
                 else:
                     self.failed += 1
-                self._maybe_release(sid, st)
+                done = self._maybe_release(sid, st)
                 self._cv.notify_all()
+            self._close_all([done])
 
     def _open(self, sid, st):
         try:
@@ -326,8 +340,9 @@ class ChunkServer:
                 self.peak_held = max(self.peak_held, self._held)
                 self.max_sessions = max(self.max_sessions, sum(
                     1 for s in self._streams.values() if s.session is not None))
-            self._maybe_release(sid, st)
+            done = self._maybe_release(sid, st)
             self._cv.notify_all()
+        self._close_all([done])
 
 
 class StreamRouter:
@@ -428,72 +443,114 @@ def poisson_arrivals(rate, seconds, rng):
 class HtsSessionFactory:
     """Sessions of the HT-S chunk codec (DMCHTSProxy) for `ChunkServer`.
 
-    Each session holds its own proxy (weights, activation arena, temporal context) and CUDA
-    stream.  A stream is coded in groups of `gop` chunks: the first chunk of every group re-seeds
-    the temporal context from the stream's reference frame (the reconstruction of an intra
-    frame in the reference's sequence loop, test_video.py:300-320), so a decoder that sees the
-    same group of payloads reproduces the encoder's reconstructions.  Encode requests carry the
-    chunk's I420 planes in host memory (pinned for an asynchronous copy); decode requests carry
+    A stream's real state is its temporal context (memory and decoded feature, ctx, the I-frame
+    feature: ~113 MB at 1080p), so that is all a session keeps on the device, with its CUDA
+    stream and its I420 staging buffers.  The codecs that run the chunks form a pool shared by
+    every session of this factory: one parameter set per device (the first codec's set_param,
+    the others share_params from it) and per codec one activation arena for one resolution.  A
+    request takes a free codec of its stream's resolution (creating one while the pool holds
+    fewer than `max_codecs`, else re-sizing an idle codec of another resolution), imports the
+    session's state, codes the chunk, exports the state and returns the codec to the pool.  The
+    kernels are deterministic, so a stream's results do not depend on which codec ran them.
+
+    A stream is coded in groups of `gop` chunks: the first chunk of every group re-seeds the
+    temporal context from the stream's reference frame (the reconstruction of an intra frame in
+    the reference's sequence loop, test_video.py:300-320), so a decoder that sees the same group
+    of payloads reproduces the encoder's reconstructions.  Encode requests carry the chunk's I420
+    planes in host memory (pinned for an asynchronous copy); decode requests carry
     (bytes, ec_parallel) and return the I420 planes in host memory (a fresh copy when
     `copy_output`, else the session's pinned buffer, valid until the stream's next request).
     """
 
     def __init__(self, state_dict, skip_threshold, ref_frames, gop=2, copy_output=True,
-                 device=None):
+                 device=None, max_codecs=8, precision="fp16"):
         import torch
+        from .inference_extensions_cuda import DMCHTSProxy
         self._torch = torch
         self.device = torch.cuda.current_device() if device is None else int(device)
         dev = torch.device("cuda", self.device)
-        # this device's own copies: sessions never read another GPU's memory
-        self._sd = {k: (v.to(dev) if isinstance(v, torch.Tensor) and v.is_cuda else v)
-                    for k, v in state_dict.items()}
-        self._skip = skip_threshold
         self._refs = {k: v.to(dev) for k, v in ref_frames.items()}  # (H, W) -> [1, 3, Hp, Wp]
         self.gop = int(gop)
         self.copy_output = copy_output
-        # the sessions read the state dict and reference frames from their own CUDA streams
-        torch.cuda.synchronize(dev)
+        self.max_codecs = int(max_codecs)
+        with torch.cuda.device(dev):
+            # this device's own parameter set: sessions never read another GPU's memory
+            sd = {k: (v.to(dev) if isinstance(v, torch.Tensor) and v.is_cuda else v)
+                  for k, v in state_dict.items()}
+            torch.cuda.synchronize(dev)
+            self._params = DMCHTSProxy(precision)
+            self._params.set_param(sd, skip_threshold)
+        self.param_bytes = self._params.stats()[2]
         self._lock = threading.Lock()
-        self._measured = {}  # (kind, H, W) -> device bytes of an opened session
+        self._free = collections.defaultdict(list)  # (H, W) -> idle codecs
+        self._codecs = 0                            # codecs alive (idle or in use)
+        self._codec_bytes = {}                      # (H, W) -> activation bytes of one codec
+        self.pool_bytes = 0                         # activation bytes of the live codecs
+        self.peak_pool_bytes = 0
 
     def worker_start(self):
         self._torch.cuda.set_device(self.device)
 
+    @staticmethod
+    def state_bytes_for(height, width):
+        hp, wp = (height + 15) // 16 * 16, (width + 15) // 16 * 16
+        return (hp // 8) * (wp // 8) * (1024 + 512 + 192) * 2
+
     def estimate_bytes(self, spec):
-        """Bytes a session at spec's size will hold: a measured session of the same kind and size;
-        else the tightest upper bound from measured sessions of that kind (a session's bytes are
-        a fixed part plus a part proportional to the padded pixels, so b * max(1, px_new / px)
-        bounds them); else 3.5 KB per padded pixel + 0.5 GB."""
-        hp, wp = (spec.height + 15) // 16 * 16, (spec.width + 15) // 16 * 16
-        with self._lock:
-            key = (spec.kind, spec.height, spec.width)
-            if key in self._measured:
-                return self._measured[key]
-            best = None
-            for (k, h, w), b in self._measured.items():
-                px = ((h + 15) // 16 * 16) * ((w + 15) // 16 * 16)
-                est = int(b * max(1.0, (hp * wp) / px))
-                if k == spec.kind and (best is None or est < best):
-                    best = est
-        if best is not None:
-            return best
-        return int(3.5e3 * hp * wp + 0.5e9)
+        """Device bytes a session holds: its temporal context plus its I420 staging (and, for an
+        encoder, its model-input buffer)."""
+        n = FRAMES * spec.height * spec.width * 3 // 2
+        extra = n + (FRAMES * 3 * spec.height * spec.width * 2 if spec.kind == "enc" else 0)
+        return self.state_bytes_for(spec.height, spec.width) + extra
 
     def open(self, stream_id, spec):
-        s = _HtsSession(self, spec)
+        return _HtsSession(self, spec)
+
+    # ---- the codec pool
+    def _acquire(self, H, W, stream):
+        from .inference_extensions_cuda import DMCHTSProxy
+        torch = self._torch
+        key = (H, W)
         with self._lock:
-            self._measured[(spec.kind, spec.height, spec.width)] = max(
-                s.device_bytes, self._measured.get((spec.kind, spec.height, spec.width), 0))
-        return s
+            if self._free[key]:
+                return self._free[key].pop()
+            evict = None
+            if self._codecs >= self.max_codecs:
+                for k, lst in self._free.items():
+                    if lst:
+                        evict = lst.pop()
+                        self.pool_bytes -= self._codec_bytes[k]
+                        break
+                if evict is None:
+                    raise RuntimeError("codec pool exhausted (more requests in flight than codecs)")
+            else:
+                self._codecs += 1
+        codec = evict
+        if codec is None:
+            codec = DMCHTSProxy(self._params.precision)
+            codec.share_params_from(self._params)
+        # size the arena for this resolution (the session's state is imported right after)
+        with torch.cuda.stream(stream):
+            codec.add_ref_feature_from_frame(self._refs[key], False)
+        b = codec.stats()[2] - self.param_bytes
+        with self._lock:
+            self._codec_bytes[key] = b
+            self.pool_bytes += b
+            self.peak_pool_bytes = max(self.peak_pool_bytes, self.pool_bytes)
+        return codec
+
+    def _release(self, H, W, codec):
+        with self._lock:
+            self._free[(H, W)].append(codec)
 
 
 class _HtsSession:
     def __init__(self, factory, spec):
         import torch
         from . import ops
-        from .inference_extensions_cuda import DMCHTSProxy
         from .synthetic import padding_for
         self._torch, self._ops = torch, ops
+        self.factory = factory
         self.spec = spec
         self.gop = factory.gop
         self.copy_output = factory.copy_output
@@ -501,49 +558,51 @@ class _HtsSession:
         self.pr, self.pb = padding_for(H, W)
         self.ref = factory._refs[(H, W)]
         dev = torch.device("cuda", factory.device)
-        torch.cuda.set_device(dev)  # the proxy binds to the current device
+        torch.cuda.set_device(dev)
         self.stream = torch.cuda.Stream(device=dev)
         self.count = 0
         n = FRAMES * H * W * 3 // 2
-        with torch.cuda.stream(self.stream):
-            self.codec = DMCHTSProxy()
-            self.codec.set_param(factory._sd, factory._skip)
-            self.planes = torch.empty(n, dtype=torch.uint8, device=dev)
-            extra = n
-            if spec.kind == "enc":
-                self.x = torch.empty((1, 3 * FRAMES, H, W), dtype=torch.float16, device=dev,
-                                     memory_format=torch.channels_last)
-                extra += self.x.numel() * 2
-            else:
-                self.host_out = torch.empty(n, dtype=torch.uint8).pin_memory()
-            self._seed()
-        self.stream.synchronize()
-        self.device_bytes = self.codec.stats()[2] + extra
-
-    def _seed(self):
-        self.codec.add_ref_feature_from_frame(self.ref, self.spec.kind == "enc")
+        self.state = torch.empty(factory.state_bytes_for(H, W), dtype=torch.uint8, device=dev)
+        self.flags = 0
+        self.planes = torch.empty(n, dtype=torch.uint8, device=dev)
+        if spec.kind == "enc":
+            self.x = torch.empty((1, 3 * FRAMES, H, W), dtype=torch.float16, device=dev,
+                                 memory_format=torch.channels_last)
+        else:
+            self.host_out = torch.empty(n, dtype=torch.uint8).pin_memory()
+        self.device_bytes = factory.estimate_bytes(spec)
 
     def run(self, req):
         torch = self._torch
         H, W = self.spec.height, self.spec.width
-        with torch.cuda.stream(self.stream):
-            if self.count % self.gop == 0 and self.count > 0:
-                self._seed()
-            self.count += 1
-            if self.spec.kind == "enc":
-                planes = req.payload
-                if planes.numel() != self.planes.numel():
-                    raise ValueError("encode payload is not 8 I420 frames of the stream's size")
-                self.planes.copy_(planes, non_blocking=True)
-                self._ops.yuv420_to_input(self.planes, FRAMES, H, W, out=self.x)
-                return self.codec.compress(self.x, req.qp, False, self.pb, self.pr)
-            bits, ecp = req.payload
-            frames = self.codec.decompress(bits, req.qp, H, W, ecp, False)
-            self._ops.frames_to_yuv420(frames, H, W, out=self.planes)
-            self.host_out.copy_(self.planes, non_blocking=True)
-            self.stream.synchronize()
-            return self.host_out.numpy().copy() if self.copy_output else self.host_out
+        codec = self.factory._acquire(H, W, self.stream)
+        try:
+            with torch.cuda.stream(self.stream):
+                if self.count % self.gop == 0:
+                    # a group starts from the reference frame, not from the stored state
+                    codec.add_ref_feature_from_frame(self.ref, self.spec.kind == "enc")
+                else:
+                    codec.import_state(self.state, self.flags)
+                self.count += 1
+                if self.spec.kind == "enc":
+                    planes = req.payload
+                    if planes.numel() != self.planes.numel():
+                        raise ValueError("encode payload is not 8 I420 frames of the stream's size")
+                    self.planes.copy_(planes, non_blocking=True)
+                    self._ops.yuv420_to_input(self.planes, FRAMES, H, W, out=self.x)
+                    result = codec.compress(self.x, req.qp, False, self.pb, self.pr)
+                    _, self.flags = codec.export_state(self.state)
+                    return result
+                bits, ecp = req.payload
+                frames = codec.decompress(bits, req.qp, H, W, ecp, False)
+                self._ops.frames_to_yuv420(frames, H, W, out=self.planes)
+                _, self.flags = codec.export_state(self.state)
+                self.host_out.copy_(self.planes, non_blocking=True)
+                self.stream.synchronize()
+                return self.host_out.numpy().copy() if self.copy_output else self.host_out
+        finally:
+            self.factory._release(H, W, codec)
 
     def close(self):
         self.stream.synchronize()
-        self.codec = None
+        self.state = None

@@ -375,6 +375,40 @@ int dcvc_hts_stats(void* handle, int* symbols, int* kernels, size_t* device_byte
 int dcvc_hts_set_precision(void* handle, int precision);
 /* The 16-bit format (DCVC_F16 or DCVC_BF16) of a buffer named as in dcvc_hts_buffer. */
 int dcvc_hts_buffer_dtype(void* handle, const char* name, int* dtype);
+/* handle takes the prepared parameters of source (set_param done there, same device) without a
+ * copy: both read the same device buffers, which live until the last handle using them is
+ * destroyed or re-parameterised.  The reference keeps one weight copy per proxy
+ * (dmc_hts_proxy.cpp:712-762); no counterpart there. */
+int dcvc_hts_share_params(void* handle, void* source);
+/* Packed batches of n streams of one resolution (1 <= n <= 64): one handle holds the temporal
+ * context of all n streams and runs every layer of the network as one launch over the n images
+ * stacked along the rows; each stream has its own QP and its own payload (its bytes equal a
+ * single-stream handle's on the same inputs).  add_ref_features seeds (and sizes) the n
+ * streams from n frames [Hp, Wp, 3]; compress_batch takes n inputs [H, W, 24] and n QPs and
+ * returns n payloads (pointer and size arrays owned by the handle, valid until its next call)
+ * and n ec_parallel values; decompress_batch takes n payloads and returns 8 frames, each
+ * [n * Hp, Wp, 3] FP16 with stream k in rows k * Hp .. (k + 1) * Hp - 1.  One reset flag covers
+ * the batch.  The reference codes one stream per proxy call (dmc_hts_proxy.cpp:504-710); no
+ * counterpart there. */
+int dcvc_hts_add_ref_features(void* handle, const void* const* frames, int n, int height,
+                              int width, int apply_adaptor, void* stream);
+int dcvc_hts_compress_batch(void* handle, const void* const* xs, int n, int height, int width,
+                            const int* qps, int reset, int pad_b, int pad_r, void* stream,
+                            const uint8_t* const** bytes, const size_t** nbytes, int* ec_parallel);
+int dcvc_hts_decompress_batch(void* handle, const uint8_t* const* bytes, const size_t* nbytes,
+                              const int* qps, const int* ec_parallel, int n, int height, int width,
+                              int reset, void* stream, void** frames);
+/* A stream's temporal context outside the handle: its size in bytes at the handle's current
+ * resolution (0 before the first add_ref_feature), and device-to-device copies of it on
+ * `stream` (export also returns a flags word that import takes back); the handle's own work is
+ * ordered after the copies.  A chunk server keeps one exported state per stream and runs each
+ * chunk on any free handle of that resolution: import, compress or decompress, export.  The
+ * layout is private to this build and valid only between handles of the same resolution and
+ * precision form.  The reference keeps the context inside the proxy (dmc_hts_proxy.h:314-326);
+ * no counterpart there. */
+int dcvc_hts_state_bytes(void* handle, size_t* bytes);
+int dcvc_hts_export_state(void* handle, void* dst, void* stream, int* flags);
+int dcvc_hts_import_state(void* handle, const void* src, int flags, void* stream);
 
 /* ------------------------------------------------------------------ HT-L chunk codec */
 

@@ -221,31 +221,19 @@ def test_in_flight_limit():
     srv.shutdown()
 
 
-def test_hts_estimate_bounds_session_bytes():
-    """HtsSessionFactory.estimate_bytes: exact for a measured size, an upper bound from the
-    tightest measured session of the same kind otherwise (a session holds a fixed part plus a part
-    proportional to its padded pixels), and a generous default before any measurement."""
+def test_hts_session_bytes_are_the_temporal_context_and_staging():
+    """HtsSessionFactory.estimate_bytes: a session holds the stream's temporal context (memory
+    and decoded feature 1024 + ctx 512 + I-frame feature 192 channels at 1/8 resolution, 16-bit)
+    plus its I420 staging (and an encoder's model-input buffer); the codecs' arenas live in the
+    shared pool, not in the sessions."""
     from dcvc_b200.serving import HtsSessionFactory
     f = HtsSessionFactory.__new__(HtsSessionFactory)  # no CUDA needed for the estimate
-    f._lock = threading.Lock()
-    f._measured = {}
-    fixed, per_px = 200e6, 600.0
-
-    def true_bytes(h, w):
-        return int(fixed + per_px * ((h + 15) // 16 * 16) * ((w + 15) // 16 * 16))
-
-    spec = StreamSpec("enc", 1080, 1920)
-    assert f.estimate_bytes(spec) >= true_bytes(1080, 1920)  # default before measurements
-    f._measured[("enc", 480, 832)] = true_bytes(480, 832)
-    f._measured[("enc", 2160, 3840)] = true_bytes(2160, 3840)
-    for h, w in [(240, 416), (720, 1280), (1080, 1920), (2160, 3840), (480, 832)]:
-        est = f.estimate_bytes(StreamSpec("enc", h, w))
-        assert est >= true_bytes(h, w), (h, w)
-    assert f.estimate_bytes(StreamSpec("enc", 480, 832)) == true_bytes(480, 832)
-    # the bound comes from the closest larger-or-equal measurement, not the largest one
-    assert f.estimate_bytes(StreamSpec("enc", 240, 416)) == true_bytes(480, 832)
-    # another kind has its own measurements
-    assert f.estimate_bytes(StreamSpec("dec", 480, 832)) >= true_bytes(480, 832)
+    ctx = HtsSessionFactory.state_bytes_for(1080, 1920)
+    assert ctx == 136 * 240 * 1728 * 2  # ~113 MB at 1080p (padded to 1088)
+    planes = 8 * 1080 * 1920 * 3 // 2
+    assert f.estimate_bytes(StreamSpec("dec", 1080, 1920)) == ctx + planes
+    assert f.estimate_bytes(StreamSpec("enc", 1080, 1920)) == ctx + planes + 8 * 3 * 1080 * 1920 * 2
+    assert HtsSessionFactory.state_bytes_for(2160, 3840) == 270 * 480 * 1728 * 2
 
 
 def test_concurrent_clients_random_work():
