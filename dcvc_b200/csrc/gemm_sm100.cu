@@ -706,6 +706,9 @@ cudaError_t gemm_sm100(int dtype, const void* A, int lda, const void* W, const G
     if (bn == kBlockNStream) {
         return gemm_stream_sm100(dtype, A, lda, W, p, epi, stream);
     }
+    if (p.out8 != nullptr) {
+        return cudaErrorInvalidValue;  // the E4M3 side output exists in the streaming form only
+    }
     if (bn <= 0 || p.N % bn != 0) {
         return cudaErrorInvalidValue;
     }

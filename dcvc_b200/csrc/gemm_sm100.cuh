@@ -58,6 +58,11 @@ struct GemmParams {
     // q_rows > 0: the M rows are images of q_rows rows stacked on each other and qscale holds one
     // row of N factors per image (per-stream QPs of a packed batch); 0: one row for all
     int q_rows = 0;
+    // Streaming residual form only: also store E4M3(round_T(out) * out8_inv_scale) to out8 (bytes,
+    // pitch ldo8), the operand of the FP8 GEMM that reads this output next
+    void* out8 = nullptr;
+    int ldo8 = 0;
+    float out8_inv_scale = 1.f;
 };
 
 // The next `launches` GEMM launches of this process run with stall_test set and the given wait

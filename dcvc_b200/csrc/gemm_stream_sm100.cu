@@ -22,6 +22,8 @@
 #include "gemm_sm100.cuh"
 #include "host_util.h"
 
+#include <cuda_fp8.h>
+
 #include <cstring>
 #include <mutex>
 
@@ -374,11 +376,33 @@ __global__ void __launch_bounds__(kSThreads, 1)
                         v[4 * j + 3] = __fmul2_rn(v[4 * j + 3], P::unpack(u.w));
                     }
                 }
+                uint32_t pk[16];
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    pk[j] = P::pack(v[j].x, v[j].y);
+                }
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     *reinterpret_cast<uint4*>(buf + sw64_off(lane, j)) =
-                        make_uint4(P::pack(v[4 * j + 0].x, v[4 * j + 0].y), P::pack(v[4 * j + 1].x, v[4 * j + 1].y),
-                                   P::pack(v[4 * j + 2].x, v[4 * j + 2].y), P::pack(v[4 * j + 3].x, v[4 * j + 3].y));
+                        make_uint4(pk[4 * j + 0], pk[4 * j + 1], pk[4 * j + 2], pk[4 * j + 3]);
+                }
+                if (p.out8 != nullptr && row0 + lane < p.M) {
+                    // the E4M3 copy of the stored (rounded) values, as a separate quantisation of
+                    // this output would produce it: 32 bytes of this lane's row
+                    uint32_t q8[8];
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        const float2 a = P::unpack(pk[2 * j]), b = P::unpack(pk[2 * j + 1]);
+                        const uint32_t lo = __nv_cvt_float2_to_fp8x2(
+                            make_float2(a.x * p.out8_inv_scale, a.y * p.out8_inv_scale), __NV_SATFINITE, __NV_E4M3);
+                        const uint32_t hi = __nv_cvt_float2_to_fp8x2(
+                            make_float2(b.x * p.out8_inv_scale, b.y * p.out8_inv_scale), __NV_SATFINITE, __NV_E4M3);
+                        q8[j] = lo | (hi << 16);
+                    }
+                    uint4* d8 = reinterpret_cast<uint4*>(static_cast<uint8_t*>(p.out8) +
+                                                         static_cast<size_t>(row0 + lane) * p.ldo8 + ncol);
+                    d8[0] = make_uint4(q8[0], q8[1], q8[2], q8[3]);
+                    d8[1] = make_uint4(q8[4], q8[5], q8[6], q8[7]);
                 }
                 fence_proxy_async_smem();
             }
@@ -458,6 +482,9 @@ cudaError_t gemm_stream_sm100(int dtype, const void* A, int lda, const void* W, 
         return cudaErrorInvalidValue;
     }
     if (epi == kEpiBiasResQ && p.qscale == nullptr) {
+        return cudaErrorInvalidValue;
+    }
+    if (p.out8 != nullptr && (p.ldo8 % 16 != 0 || (reinterpret_cast<uintptr_t>(p.out8) & 15) != 0)) {
         return cudaErrorInvalidValue;
     }
     const CUtensorMapDataType dt = dtype == 0 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;

@@ -394,7 +394,28 @@ void run_dcb(Launch& L, const Dcb& d, const __half* x, int ldx, int H, int W, __
     }
     gemm(L, d.dc1, kEpiBiasWsilu, xin, ldin, M, s.t1, d.cdc);
     L.note(launch_dwconv3x3(s.t1, H, W, d.cdc, d.cdc, d.dw, s.t2, d.cdc, L.s, d.dtype, img_h));
-    gemm(L, d.dc2, kEpiBiasRes, s.t2, d.cdc, M, s.t3, d.C, xin, ldin);
+    // the FP8 form: the streaming residual GEMM also writes the E4M3 operand of the quad GEMM
+    const bool fp8_quad = d.ffn1_w8 != nullptr && s.t5 != nullptr;
+    bool t5_ready = false;
+    if (fp8_quad && gemm_stream_eligible(kEpiBiasRes, M, d.C, d.cdc) && d.C % 16 == 0) {
+        GemmParams p{};
+        p.M = M;
+        p.N = d.C;
+        p.K = d.cdc;
+        p.bias = d.dc2.b;
+        p.res = xin;
+        p.ldr = ldin;
+        p.out = s.t3;
+        p.ldo = d.C;
+        p.out8 = s.t5;
+        p.ldo8 = d.C;
+        p.out8_inv_scale = 1.0f / kFp8ActScale;
+        p.err = L.err_word;
+        L.note(gemm_sm100(d.dc2.dtype, s.t2, d.cdc, d.dc2.w, p, kEpiBiasRes, kBlockNStream, L.s));
+        t5_ready = true;
+    } else {
+        gemm(L, d.dc2, kEpiBiasRes, s.t2, d.cdc, M, s.t3, d.C, xin, ldin);
+    }
     if (!d.shortcut && d.dtype == 0 && (q == nullptr || q_rows == 0) &&
         ffn_sm100_preferred(d.C, d.cffn, d.ffn1.cout)) {
         // the ConvFFN as one kernel, the quad output kept on chip (ffn_sm100.cu)
@@ -404,7 +425,9 @@ void run_dcb(Launch& L, const Dcb& d, const __half* x, int ldx, int H, int W, __
     }
     if (d.ffn1_w8 != nullptr && s.t5 != nullptr) {
         // the FP8 form: E4M3 copy of the dc output, quad GEMM on kind::f8f6f4
-        L.note(launch_quantize_fp8(s.t3, d.dtype, d.C, 1.0f / kFp8ActScale, s.t5, d.C, M, d.C, L.s));
+        if (!t5_ready) {
+            L.note(launch_quantize_fp8(s.t3, d.dtype, d.C, 1.0f / kFp8ActScale, s.t5, d.C, M, d.C, L.s));
+        }
         GemmParams p{};
         p.M = M;
         p.N = d.ffn1.cout;

@@ -1,7 +1,7 @@
 """Micro-benchmark of the codec's kernels at their 1080p shapes (CUDA events on the launching
 stream), also the small fixed case used for ncu captures.
 
-    python -m dcvc_b200.kernel_bench [--case quad|quad_f8|wsilu|res|bias2048|dwconv|ffn|ffn_ld|rans|all]
+    python -m dcvc_b200.kernel_bench [--case quad|quad_f8|wsilu|res|bias2048|dwconv|ffn|ffn_ld|unshuffle|quantize|rans|all]
                                      [--reps N] [--sets S] [--bn 0|64|128|256|-1]
 
 (--bn -1 selects the streaming form of the residual GEMM.)
@@ -51,6 +51,20 @@ def _case(name, g, bn=0):
         out = torch.empty(M8, 256, device="cuda", dtype=torch.bfloat16)
         fn = lambda: ops.conv1x1_f8(a, wq, ws, b, N.EPI_QUAD, out=out, block_n=bn)  # noqa: E731
         return fn, 2.0 * M8 * 1024 * 512, (M8 * 512 + 1024 * 512) + M8 * 256 * 2
+    if name == "unshuffle":
+        # pad_and_unshuffle_8 of one 1080p input chunk: [1080, 1920, 24] -> [136 x 240, 1536]
+        x = rnd(1080, 1920, 24)
+        out = torch.empty(M8, 1536, device="cuda", dtype=torch.float16)
+        fn = lambda: ops.pad_unshuffle8(x, 8, 0, out=out)  # noqa: E731
+        return fn, 0.0, (x.numel() + out.numel()) * 2
+    if name == "quantize":
+        # the last masked quantisation phase at 1080p (y: 68 x 120 x 256, mode 2: accumulate and
+        # scale by max(q_dec, 0.5)); reads y, scales, means, q_dec, y_q, y_hat, writes y_q, y_hat
+        M16 = 68 * 120
+        y, sc, mu, qd = rnd(M16, 256), rnd(M16, 256).abs(), rnd(M16, 256), rnd(M16, 256).abs()
+        yq, yh = torch.zeros_like(y), torch.zeros_like(y)
+        fn = lambda: ops.quantize_phase(3, 2, y, sc, mu, qd, 0.15, yq, yh, 68, 120)  # noqa: E731
+        return fn, 0.0, 8 * y.numel() * 2
     if name == "dwconv":
         x = rnd(M8, 256)
         w = torch.randn(9, 256, device="cuda", generator=g)
