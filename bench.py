@@ -614,8 +614,7 @@ def serving_bench(args):
     sd = add_cdf_to_state_dict(calibrated_hts_state_dict(0))
     sd = {k: (v.half().cuda() if v.is_floating_point() else v) for k, v in sd.items()}
     torch.cuda.synchronize()
-    f = HtsSessionFactory(sd, SKIP_THRES, refs, gop=2, copy_output=False,
-                          max_codecs=args.serve_slots)
+    f = HtsSessionFactory(sd, SKIP_THRES, refs, gop=2, copy_output=False)
     srv = ChunkServer(f.open, f.estimate_bytes, slots=args.serve_slots, hbm_budget=SERVE_BUDGET,
                       on_worker_start=f.worker_start)
     try:
@@ -717,8 +716,10 @@ def serving_bench(args):
                 "param_gb": round(f.param_bytes / 1e9, 3),
                 "peak_total_gb": round((srv.peak_held + f.peak_pool_bytes + f.param_bytes) / 1e9, 2),
                 "memory_model": "sessions hold only their temporal context and I420 staging "
-                                "(peak_held_gb); chunks run on a pool of at most `slots` codecs "
-                                "(peak_codec_pool_gb) sharing one parameter set (param_gb)",
+                                "(peak_held_gb); chunks run on a pool of codecs, as many per "
+                                "resolution as its requests in flight at once "
+                                "(peak_codec_pool_gb), sharing one parameter set (param_gb)",
+                "codecs_created": f.codecs_created, "codecs_evicted": f.codecs_evicted,
                 "max_sessions": srv.max_sessions, "failed": srv.failed,
                 "note": "Poisson arrivals, 50/50 encode/decode, resolutions 10/20/30/30/10 % over "
                         "416x240..3840x2160, QP U[0,63]; end to end (I420 planes host<->device); "

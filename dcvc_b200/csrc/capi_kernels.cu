@@ -68,6 +68,12 @@ int dcvc_check_device_errors(void* stream)
     return kOk;
 }
 
+int dcvc_gemm_stream_form(int enable)
+{
+    gemm_set_stream_form(enable != 0);
+    return kOk;
+}
+
 int dcvc_gemm_inject_stall(int launches, long long wait_limit_cycles)
 {
     if (launches > 0 && wait_limit_cycles <= 0) {

@@ -622,9 +622,16 @@ cudaError_t dispatch_epi_f8(int epi, const Maps& m, const GemmParams& p, cudaStr
 
 int gemm_tuned_bn(int dtype, int epi, int M, int N, int K, int sub_w);
 
+namespace {
+std::atomic<int> g_stream_form{1};
+}  // namespace
+
+void gemm_set_stream_form(bool on) { g_stream_form.store(on ? 1 : 0); }
+
 int gemm_pick_bn(int M, int N, int epi, int sub_cout, int K)
 {
-    if (K > 0 && gemm_stream_eligible(epi, M, N, K)) {
+    if (K > 0 && g_stream_form.load(std::memory_order_relaxed) != 0 &&
+        gemm_stream_eligible(epi, M, N, K)) {
         // residual epilogues at K <= 256: the streaming form (W resident, row ranges per CTA)
         // moves the same bytes in 18.1 us where the tiled kernel takes 21.8 us (dc.3 / ffn.2 at
         // 1080p), with the same output bits

@@ -448,10 +448,11 @@ class HtsSessionFactory:
     stream and its I420 staging buffers.  The codecs that run the chunks form a pool shared by
     every session of this factory: one parameter set per device (the first codec's set_param,
     the others share_params from it) and per codec one activation arena for one resolution.  A
-    request takes a free codec of its stream's resolution (creating one while the pool holds
-    fewer than `max_codecs`, else re-sizing an idle codec of another resolution), imports the
-    session's state, codes the chunk, exports the state and returns the codec to the pool.  The
-    kernels are deterministic, so a stream's results do not depend on which codec ran them.
+    request takes an idle codec of its stream's resolution (or creates one; the pool grows to the
+    number of requests of each resolution in flight at once, and idle codecs of other resolutions
+    are released only beyond `pool_budget` bytes), imports the session's state, codes the chunk,
+    exports the state and returns the codec to the pool.  The kernels are deterministic, so a
+    stream's results do not depend on which codec ran them.
 
     A stream is coded in groups of `gop` chunks: the first chunk of every group re-seeds the
     temporal context from the stream's reference frame (the reconstruction of an intra frame in
@@ -463,7 +464,7 @@ class HtsSessionFactory:
     """
 
     def __init__(self, state_dict, skip_threshold, ref_frames, gop=2, copy_output=True,
-                 device=None, max_codecs=8, precision="fp16"):
+                 device=None, pool_budget=64e9, precision="fp16"):
         import torch
         from .inference_extensions_cuda import DMCHTSProxy
         self._torch = torch
@@ -472,7 +473,7 @@ class HtsSessionFactory:
         self._refs = {k: v.to(dev) for k, v in ref_frames.items()}  # (H, W) -> [1, 3, Hp, Wp]
         self.gop = int(gop)
         self.copy_output = copy_output
-        self.max_codecs = int(max_codecs)
+        self.pool_budget = int(pool_budget)
         with torch.cuda.device(dev):
             # this device's own parameter set: sessions never read another GPU's memory
             sd = {k: (v.to(dev) if isinstance(v, torch.Tensor) and v.is_cuda else v)
@@ -482,11 +483,12 @@ class HtsSessionFactory:
             self._params.set_param(sd, skip_threshold)
         self.param_bytes = self._params.stats()[2]
         self._lock = threading.Lock()
-        self._free = collections.defaultdict(list)  # (H, W) -> idle codecs
-        self._codecs = 0                            # codecs alive (idle or in use)
+        self._free = collections.defaultdict(list)  # (H, W) -> idle codecs, least recent first
         self._codec_bytes = {}                      # (H, W) -> activation bytes of one codec
         self.pool_bytes = 0                         # activation bytes of the live codecs
         self.peak_pool_bytes = 0
+        self.codecs_created = 0
+        self.codecs_evicted = 0
 
     def worker_start(self):
         self._torch.cuda.set_device(self.device)
@@ -508,27 +510,29 @@ class HtsSessionFactory:
 
     # ---- the codec pool
     def _acquire(self, H, W, stream):
+        """An idle codec of this resolution, else a new one (sharing the parameters).  A codec
+        keeps its arena and its captured phase graphs between requests, so the pool grows to
+        the concurrency each resolution sees and stays there; idle codecs of other resolutions
+        are released only when the pool would exceed `pool_budget` bytes."""
         from .inference_extensions_cuda import DMCHTSProxy
         torch = self._torch
         key = (H, W)
+        evicted = []
         with self._lock:
             if self._free[key]:
                 return self._free[key].pop()
-            evict = None
-            if self._codecs >= self.max_codecs:
-                for k, lst in self._free.items():
-                    if lst:
-                        evict = lst.pop()
-                        self.pool_bytes -= self._codec_bytes[k]
-                        break
-                if evict is None:
-                    raise RuntimeError("codec pool exhausted (more requests in flight than codecs)")
-            else:
-                self._codecs += 1
-        codec = evict
-        if codec is None:
-            codec = DMCHTSProxy(self._params.precision)
-            codec.share_params_from(self._params)
+            need = self._codec_bytes.get(key, 0)
+            while self.pool_bytes + need > self.pool_budget:
+                victim = next((k for k, lst in self._free.items() if lst and k != key), None)
+                if victim is None:
+                    break  # everything else is in use: the budget is exceeded for this request
+                evicted.append(self._free[victim].pop(0))
+                self.pool_bytes -= self._codec_bytes[victim]
+                self.codecs_evicted += 1
+            self.codecs_created += 1
+        del evicted  # their arenas are freed with them
+        codec = DMCHTSProxy(self._params.precision)
+        codec.share_params_from(self._params)
         # size the arena for this resolution (the session's state is imported right after)
         with torch.cuda.stream(stream):
             codec.add_ref_feature_from_frame(self._refs[key], False)
