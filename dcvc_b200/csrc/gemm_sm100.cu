@@ -627,6 +627,7 @@ std::atomic<int> g_stream_form{1};
 }  // namespace
 
 void gemm_set_stream_form(bool on) { g_stream_form.store(on ? 1 : 0); }
+bool gemm_stream_form_enabled() { return g_stream_form.load(std::memory_order_relaxed) != 0; }
 
 int gemm_pick_bn(int M, int N, int epi, int sub_cout, int K)
 {

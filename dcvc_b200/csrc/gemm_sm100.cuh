@@ -80,6 +80,7 @@ bool gemm_stream_eligible(int epi, int M, int N, int K);
 // Whether the library's own choice (block_n = 0, no tuned width) may pick the streaming form
 // (default on); explicit block_n values are not affected.
 void gemm_set_stream_form(bool on);
+bool gemm_stream_form_enabled();
 cudaError_t gemm_stream_sm100(int dtype, const void* A, int lda, const void* W, const GemmParams& p,
                               int epi, cudaStream_t stream);
 

@@ -397,7 +397,8 @@ void run_dcb(Launch& L, const Dcb& d, const __half* x, int ldx, int H, int W, __
     // the FP8 form: the streaming residual GEMM also writes the E4M3 operand of the quad GEMM
     const bool fp8_quad = d.ffn1_w8 != nullptr && s.t5 != nullptr;
     bool t5_ready = false;
-    if (fp8_quad && gemm_stream_eligible(kEpiBiasRes, M, d.C, d.cdc) && d.C % 16 == 0) {
+    if (fp8_quad && gemm_stream_form_enabled() && gemm_stream_eligible(kEpiBiasRes, M, d.C, d.cdc) &&
+        d.C % 16 == 0) {
         GemmParams p{};
         p.M = M;
         p.N = d.C;

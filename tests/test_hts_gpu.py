@@ -118,3 +118,28 @@ def test_bf16_form_differs_from_fp16_and_reports_its_buffers():
     with pytest.raises(ValueError):
         DMCHTSProxy("fp8_unknown")
 
+
+
+def test_fp8_operand_fused_in_the_residual_epilogue_is_bitwise_the_separate_quantisation():
+    """In the FP8 form the streaming residual GEMM writes the quad GEMM's E4M3 operand in its
+    epilogue; with the streaming form switched off the same operand comes from the tiled GEMM
+    and a separate quantisation kernel.  Both give the same payload and reconstruction."""
+    from dcvc_b200 import _native as N
+    sd = state_dict()
+    H, W = 128, 192
+    out = {}
+    try:
+        for on in (1, 0):
+            N.lib.dcvc_gemm_stream_form(on)
+            enc, dec = _proxy(sd, "fp8"), _proxy(sd, "fp8")
+            ref = ref_frame(H, W)
+            enc.add_ref_feature_from_frame(ref, True)
+            dec.add_ref_feature_from_frame(ref, False)
+            bits, ecp = enc.compress(chunk(H, W, 0), 33, False, 0, 0)
+            frames = dec.decompress(bits, 33, H, W, ecp, False)
+            torch.cuda.synchronize()
+            out[on] = (bits, [f.clone() for f in frames])
+    finally:
+        N.lib.dcvc_gemm_stream_form(1)
+    assert np.array_equal(out[0][0], out[1][0])
+    assert all(torch.equal(a, b) for a, b in zip(out[0][1], out[1][1]))
