@@ -69,6 +69,10 @@ _proto("dcvc_gemm_tuning_clear", c_int, [])
 _proto("dcvc_conv_ffn", c_int, [c_int, c_int, c_int, c_vp, c_int, c_vp, c_vp, c_vp, c_vp, c_vp,
                                c_vp, c_int, c_int, c_vp])
 _proto("dcvc_dwconv3x3", c_int, [c_vp, c_int, c_int, c_int, c_int, c_vp, c_vp, c_int, c_vp])
+_proto("dcvc_dwconv3x3_ex", c_int, [c_int, c_vp, c_int, c_int, c_int, c_int, c_int, c_vp, c_vp, c_int, c_vp])
+_proto("dcvc_dw3x3_conv1x1_res", c_int, [c_int, c_int, c_int, c_int, c_vp, c_int, c_vp, c_int, c_vp, c_int,
+                                        c_vp, c_vp, c_int, c_vp, c_int, c_vp])
+_proto("dcvc_dw_fusion", c_int, [c_int])
 
 
 def device_error(clear=True):

@@ -74,6 +74,12 @@ int dcvc_gemm_stream_form(int enable)
     return kOk;
 }
 
+int dcvc_dw_fusion(int enable)
+{
+    gemm_set_dw_fusion(enable != 0);
+    return kOk;
+}
+
 int dcvc_gemm_inject_stall(int launches, long long wait_limit_cycles)
 {
     if (launches > 0 && wait_limit_cycles <= 0) {
@@ -257,6 +263,57 @@ int dcvc_dwconv3x3(const void* x, int H, int W, int C, int ldx, const float* w, 
         return kInvalidArgument;
     }
     return cuda_status(e, "dcvc_dwconv3x3");
+}
+
+int dcvc_dwconv3x3_ex(int dtype, const void* x, int H, int W, int img_h, int C, int ldx, const float* w,
+                      void* out, int ldo, void* stream)
+{
+    if ((dtype != DCVC_F16 && dtype != DCVC_BF16) || x == nullptr || w == nullptr || out == nullptr ||
+        H <= 0 || W <= 0 || img_h < 0) {
+        set_last_error("dcvc_dwconv3x3_ex: bad arguments");
+        return kInvalidArgument;
+    }
+    cudaError_t e = launch_dwconv3x3(static_cast<const __half*>(x), H, W, C, ldx, w, static_cast<__half*>(out),
+                                     ldo, static_cast<cudaStream_t>(stream), dtype, img_h);
+    if (e == cudaErrorInvalidValue) {
+        set_last_error("dcvc_dwconv3x3_ex: C, pitches and pointers must be multiples of 8 elements / 16 bytes, "
+                       "img_h must divide H");
+        return kInvalidArgument;
+    }
+    return cuda_status(e, "dcvc_dwconv3x3_ex");
+}
+
+int dcvc_dw3x3_conv1x1_res(int dtype, int H, int W, int img_h, const void* x, int ldx,
+                           const float* dw_weight, int K, const void* w, int N, const float* bias,
+                           const void* res, int ldr, void* out, int ldo, void* stream)
+{
+    if ((dtype != DCVC_F16 && dtype != DCVC_BF16) || x == nullptr || dw_weight == nullptr || w == nullptr ||
+        bias == nullptr || res == nullptr || out == nullptr || H <= 0 || W <= 0 || img_h < 0 ||
+        static_cast<long long>(H) * W > (1LL << 30)) {
+        set_last_error("dcvc_dw3x3_conv1x1_res: bad arguments");
+        return kInvalidArgument;
+    }
+    GemmParams p{};
+    p.M = H * W;
+    p.N = N;
+    p.K = K;
+    p.bias = bias;
+    p.res = res;
+    p.ldr = ldr;
+    p.out = out;
+    p.ldo = ldo;
+    p.err = device_error_word();
+    p.dw_weight = dw_weight;
+    p.dw_h = H;
+    p.dw_w = W;
+    p.dw_img_h = img_h > 0 ? img_h : H;
+    cudaError_t e = gemm_sm100(dtype, x, ldx, w, p, kEpiBiasRes, kBlockNStream, static_cast<cudaStream_t>(stream));
+    if (e == cudaErrorInvalidValue) {
+        set_last_error("dcvc_dw3x3_conv1x1_res: unsupported shape, pitch or alignment (K a multiple of 64 "
+                       "up to 256, N of 128, img_h dividing H)");
+        return kInvalidArgument;
+    }
+    return cuda_status(e, "dcvc_dw3x3_conv1x1_res");
 }
 
 }  // extern "C"

@@ -624,10 +624,13 @@ int gemm_tuned_bn(int dtype, int epi, int M, int N, int K, int sub_w);
 
 namespace {
 std::atomic<int> g_stream_form{1};
+std::atomic<int> g_dw_fusion{0};
 }  // namespace
 
 void gemm_set_stream_form(bool on) { g_stream_form.store(on ? 1 : 0); }
 bool gemm_stream_form_enabled() { return g_stream_form.load(std::memory_order_relaxed) != 0; }
+void gemm_set_dw_fusion(bool on) { g_dw_fusion.store(on ? 1 : 0); }
+bool gemm_dw_fusion_enabled() { return g_dw_fusion.load(std::memory_order_relaxed) != 0; }
 
 int gemm_pick_bn(int M, int N, int epi, int sub_cout, int K)
 {
@@ -714,8 +717,9 @@ cudaError_t gemm_sm100(int dtype, const void* A, int lda, const void* W, const G
     if (bn == kBlockNStream) {
         return gemm_stream_sm100(dtype, A, lda, W, p, epi, stream);
     }
-    if (p.out8 != nullptr) {
-        return cudaErrorInvalidValue;  // the E4M3 side output exists in the streaming form only
+    if (p.out8 != nullptr || p.dw_weight != nullptr) {
+        // the E4M3 side output and the depthwise operand exist in the streaming form only
+        return cudaErrorInvalidValue;
     }
     if (bn <= 0 || p.N % bn != 0) {
         return cudaErrorInvalidValue;

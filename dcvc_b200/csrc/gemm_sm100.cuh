@@ -63,6 +63,13 @@ struct GemmParams {
     void* out8 = nullptr;
     int ldo8 = 0;
     float out8_inv_scale = 1.f;
+    // Streaming residual form only (kEpiBiasRes): A is the depthwise 3x3 convolution (zero
+    // padding, no bias, FP32 sums in the order ky, kx) of the given A over a dw_h x dw_w pixel
+    // grid (dw_h * dw_w = M rows, images of dw_img_h rows stacked), weights [9][K] FP32
+    const float* dw_weight = nullptr;
+    int dw_h = 0;
+    int dw_w = 0;
+    int dw_img_h = 0;
 };
 
 // The next `launches` GEMM launches of this process run with stall_test set and the given wait
@@ -81,6 +88,10 @@ bool gemm_stream_eligible(int epi, int M, int N, int K);
 // (default on); explicit block_n values are not affected.
 void gemm_set_stream_form(bool on);
 bool gemm_stream_form_enabled();
+// Whether the codecs compute the depthwise 3x3 inside the streaming residual GEMM (default off:
+// measured slower than the two launches, see the kernel file).
+void gemm_set_dw_fusion(bool on);
+bool gemm_dw_fusion_enabled();
 cudaError_t gemm_stream_sm100(int dtype, const void* A, int lda, const void* W, const GemmParams& p,
                               int epi, cudaStream_t stream);
 

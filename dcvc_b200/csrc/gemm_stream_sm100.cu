@@ -15,6 +15,18 @@
 //   * sixteen epilogue warps (four per TMEM lane quadrant, 32 columns each) keep a two-tile-deep
 //     ring of residual boxes in flight, so a tile's residual lands while earlier tiles compute;
 //   * the result is written over the residual in its slot and stored by TMA.
+// Depthwise form (p.dw_weight set): A is the depthwise 3x3 convolution of the given input,
+// computed in the kernel (DepthConvBlock: d3x3 followed by conv1x1_bias_shortcut,
+// layers_proxy.cpp:81-82).  Four producer warps compute each 128-row x 64-channel A stage on the
+// CUDA cores from three TMA-staged bands of input rows (the pixel row above, the row itself and
+// the row below, 66 pixels each per 64-pixel half) and write it in the MMA's 128-byte-swizzled
+// operand layout; the depthwise output never goes to memory.  The products are summed in FP32 in
+// the order ky, kx and rounded once to the activation type, as the standalone depthwise kernel
+// does, so A, and every output bit, equal those of the two-launch form.  Measured at 1080p (M =
+// 32640, K = 256, N = 512) it is slower than the two launches (114.7 us against 14.3 + 18.3 us):
+// each of the four channel slices recomputes the depthwise values of its rows, and with two band
+// sets in shared memory the producers wait for every band's L2 latency.  The codecs therefore use
+// it only when asked to (gemm_set_dw_fusion).
 // One thread issues tcgen05.mma (M = 128, N = 128, K = 16) into a double-buffered FP32 TMEM
 // accumulator.  Per output element the products are summed in the same order as in the tiled
 // kernel and the epilogue applies bias, residual(s) and x q in the same order, so the outputs
@@ -36,26 +48,43 @@ constexpr int kSBN = 128;                   // output channels per CTA
 constexpr int kSBK = 64;                    // one 128-byte swizzle atom of 16-bit elements
 constexpr int kSMaxK = 256;                 // W slice resident: 128 x 256 x 2 B = 64 KB
 constexpr int kSEpiWarps = 16;
-constexpr int kSThreads = 64 + 32 * kSEpiWarps;
 constexpr int kSCols = kSBN / 4;            // accumulator columns per epilogue warp (32)
 constexpr int kSBoxBytes = 32 * kSCols * 2; // 32 rows x 32 columns of 16-bit values: 2 KB
 constexpr int kSResSlots = 2;               // residual ring depth per warp, in tiles
 constexpr int kSStages = 6;
 constexpr int kSABytes = kSBM * kSBK * 2;   // 16 KB
 constexpr long long kSWaitLimit = 2000000000LL;  // ~1 s at 2 GHz; a correct kernel never waits this long
+// depthwise form
+constexpr int kDwProdWarps = 4;
+constexpr int kDwStages = 2;                        // A stages: the producers, not the MMA, set the pace
+constexpr int kDwSubPx = 64;                        // output pixels per producer step (half a stage)
+constexpr int kDwPxPerWarp = kDwSubPx / kDwProdWarps;  // 16 consecutive pixels per warp
+constexpr int kDwBandRows = kDwSubPx + 2;           // input pixels per band: one more on each side
+constexpr int kDwBandBytes = kDwBandRows * kSBK * 2;  // 8448
+constexpr int kDwHaloBytes = 3 * kDwBandBytes;      // rows above, at and below: 25344
 
-template <int EPI>
+template <int EPI, bool DW>
 struct StreamCfg {
+    static constexpr int kProdWarps = DW ? kDwProdWarps : 1;
+    static constexpr int kMmaWarp = kProdWarps;
+    static constexpr int kThreads = 32 * (kProdWarps + 1 + kSEpiWarps);
+    static constexpr int kStages = DW ? kDwStages : kSStages;
     static constexpr int kSlotBytes = kSBoxBytes;
     static constexpr int kBOffset = 0;                                   // resident W slice
     static constexpr int kBBytes = kSBN * kSMaxK * 2;                    // 64 KB
     static constexpr int kAOffset = kBOffset + kBBytes;
-    static constexpr int kEpiOffset = kAOffset + kSStages * kSABytes;    // 96 KB of A stages
+    static constexpr int kHaloOffset = kAOffset + kStages * kSABytes;    // two band sets (DW)
+    static constexpr int kHaloBytes = DW ? (2 * kDwHaloBytes + 1023) / 1024 * 1024 : 0;
+    static constexpr int kEpiOffset = kHaloOffset + kHaloBytes;
     static constexpr int kEpiBytes = kSEpiWarps * kSResSlots * kSlotBytes;
     static constexpr int kBarOffset = kEpiOffset + kEpiBytes;
     static constexpr int kBarBytes = 512;
-    static constexpr int kBytes = kBarOffset + kBarBytes + 1024;
+    // DW: each epilogue warp's 32 bias values (registers are short with four producer warps)
+    static constexpr int kBiasOffset = kBarOffset + kBarBytes;
+    static constexpr int kBiasBytes = DW ? kSEpiWarps * kSCols * 4 : 0;
+    static constexpr int kBytes = kBiasOffset + kBiasBytes + 1024;
     static_assert(kBytes <= 232448, "shared memory budget exceeded");
+    static_assert(kEpiOffset % 1024 == 0 && kHaloOffset % 1024 == 0, "TMA destinations stay aligned");
 };
 
 template <typename T>
@@ -103,24 +132,27 @@ __device__ __forceinline__ void cta_rows(int M, int idx, int G, int* r0, int* r1
     *r1 = g1 * 32 < M ? g1 * 32 : M;
 }
 
-template <typename T, int EPI>
-__global__ void __launch_bounds__(kSThreads, 1)
+template <typename T, int EPI, bool DW>
+__global__ void __launch_bounds__(StreamCfg<EPI, DW>::kThreads, 1)
     gemm_stream_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                        const __grid_constant__ CUtensorMap tmO, const __grid_constant__ CUtensorMap tmR,
                        const GemmParams p, int ctas_per_slice)
 {
-    using C = StreamCfg<EPI>;
+    using C = StreamCfg<EPI, DW>;
+    constexpr int kStages = C::kStages;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem =
         reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + C::kBarOffset);
-    uint64_t* empty = full + kSStages;
-    uint64_t* bfull = empty + kSStages;
+    uint64_t* empty = full + kStages;
+    uint64_t* bfull = empty + kStages;
     uint64_t* tfull = bfull + 1;
     uint64_t* tempty = tfull + 2;
     uint64_t* drain = tempty + 2;
     uint64_t* resbar = drain + 1;  // [kSEpiWarps][kSResSlots]
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(resbar + kSEpiWarps * kSResSlots);
+    uint64_t* hfull = resbar + kSEpiWarps * kSResSlots;  // DW: band sets landed / read
+    uint64_t* hempty = hfull + 2;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(hempty + 2);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5;
@@ -135,9 +167,14 @@ __global__ void __launch_bounds__(kSThreads, 1)
     const long long lim = p.wait_limit > 0 ? p.wait_limit : kSWaitLimit;
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s < kSStages; ++s) {
-            mbar_init(&full[s], 1);
+        for (int s = 0; s < kStages; ++s) {
+            // DW: one arrival per producer warp once its rows of the stage are written
+            mbar_init(&full[s], DW ? kDwProdWarps : 1);
             mbar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&hfull[b], 1);
+            mbar_init(&hempty[b], kDwProdWarps);
         }
         mbar_init(bfull, 1);
         for (int b = 0; b < 2; ++b) {
@@ -155,7 +192,7 @@ __global__ void __launch_bounds__(kSThreads, 1)
         tma_prefetch_desc(&tmA);
         tma_prefetch_desc(&tmB);
     }
-    if (warp == 1) {
+    if (warp == C::kMmaWarp) {
         tmem_alloc(tmem_slot, 2 * kSBN);
         tmem_relinquish();
     }
@@ -166,7 +203,163 @@ __global__ void __launch_bounds__(kSThreads, 1)
     griddep_launch_dependents();
     griddep_wait();
 
-    if (warp == 0) {
+    if (DW && warp < C::kProdWarps) {
+        // ------------------------------------------------------------ depthwise producers
+        // Step v fills half `v & 1` (64 rows) of the A stage of unit u = v >> 1 = (tile
+        // u / kblocks, K block u % kblocks) from band set v & 1; each warp computes 16
+        // consecutive pixels, each lane one channel pair, sliding a 3 x 3 window of FP32 pairs.
+        using P = SPack2<T>;
+        const int subs = 2 * ntiles * kblocks;
+        const bool issuer = warp == 0 && lane == 0;
+        uint32_t halo_pending = 0;
+        int halo_last0 = 0, halo_last1 = 0;  // the last step issued into band set 0 / 1
+        auto issue_halo = [&](int v) {
+            const int u = v >> 1;
+            const int t = u / kblocks;
+            const int kb = u - t * kblocks;
+            const int first = r0 + t * kSBM + (v & 1) * kDwSubPx;  // first output pixel
+            uint8_t* hb = smem + C::kHaloOffset + (v & 1) * kDwHaloBytes;
+            mbar_arrive_expect_tx(&hfull[v & 1], kDwHaloBytes);
+            for (int b = 0; b < 3; ++b) {
+                // band b: input pixels first - 1 + (b - 1) * W .. + 65; rows outside the
+                // image (negative or past M) read as zero
+                tma_load_2d(hb + b * kDwBandBytes, &tmA, &hfull[v & 1], kb * kSBK,
+                            first - 1 + (b - 1) * p.dw_w);
+            }
+            halo_pending |= 1u << (v & 1);
+            if (v & 1) {
+                halo_last1 = v;
+            } else {
+                halo_last0 = v;
+            }
+        };
+        if (ntiles > 0 && !p.stall_test) {
+            if (issuer) {
+                mbar_arrive_expect_tx(bfull, static_cast<uint32_t>(kblocks * kSBN * kSBK * 2));
+                for (int kb = 0; kb < kblocks; ++kb) {
+                    tma_load_2d(smem + C::kBOffset + kb * kSBN * 128, &tmB, bfull, kb * kSBK, n0);
+                }
+                issue_halo(0);
+                if (subs > 1) {
+                    issue_halo(1);
+                }
+            }
+            const int W8 = p.dw_w;
+            const int img_h = p.dw_img_h;
+            const float2* wt2 = reinterpret_cast<const float2*>(p.dw_weight);
+            float2 wp[9];
+            for (int v = 0; v < subs; ++v) {
+                if (__any_sync(0xffffffffu, *abort_flag != 0)) {
+                    break;  // one decision for the whole warp
+                }
+                const int u = v >> 1;
+                const int ph = v & 1;
+                const int t = u / kblocks;
+                const int kb = u - t * kblocks;
+                const int s = u % kStages;
+                uint8_t* stage = smem + C::kAOffset + s * kSABytes;
+                // every wait's outcome is made warp-uniform, so the warp leaves the loop together
+                if (ph == 0) {
+                    if (!__all_sync(0xffffffffu, mbar_wait_bounded(&empty[s], ((u / kStages) & 1) ^ 1, lim))) {
+                        *abort_flag = 1;
+                        report_error(p.err, kErrGemmProducerTimeout);
+                        break;
+                    }
+                    // the weights [9][K] of this lane's channel pair in K block kb
+#pragma unroll
+                    for (int k = 0; k < 9; ++k) {
+                        wp[k] = __ldg(wt2 + k * (p.K >> 1) + kb * (kSBK / 2) + lane);
+                    }
+                }
+                if (!__all_sync(0xffffffffu, mbar_wait_bounded(&hfull[v & 1], (v >> 1) & 1, lim))) {
+                    *abort_flag = 1;
+                    report_error(p.err, kErrGemmProducerTimeout);
+                    break;
+                }
+                if (issuer) {
+                    halo_pending &= ~(1u << (v & 1));
+                }
+                const uint32_t* band =
+                    reinterpret_cast<const uint32_t*>(smem + C::kHaloOffset + (v & 1) * kDwHaloBytes);
+                constexpr int kBandWords = kDwBandBytes / 4;
+                const int l0 = warp * kDwPxPerWarp;  // first pixel of this warp within the half
+                const int px0 = r0 + t * kSBM + ph * kDwSubPx + l0;
+                const int h0 = px0 / W8;
+                int w = px0 - h0 * W8;  // column of the current pixel
+                int hm = h0 % img_h;    // its row within its image
+                float2 win[3][3];       // [band][column - 1 .. + 1]
+#pragma unroll
+                for (int b = 0; b < 3; ++b) {
+                    win[b][0] = P::unpack(band[b * kBandWords + l0 * 32 + lane]);
+                    win[b][1] = P::unpack(band[b * kBandWords + (l0 + 1) * 32 + lane]);
+                }
+#pragma unroll
+                for (int j = 0; j < kDwPxPerWarp; ++j) {
+#pragma unroll
+                    for (int b = 0; b < 3; ++b) {
+                        win[b][2] = P::unpack(band[b * kBandWords + (l0 + j + 2) * 32 + lane]);
+                    }
+                    // taps outside the pixel's image are zero, as in the standalone kernel's
+                    // zero-filled halo; FP32 accumulation in the order ky, kx
+                    const bool ok_y[3] = {hm != 0, true, hm != img_h - 1};
+                    const bool ok_x[3] = {w != 0, true, w != W8 - 1};
+                    float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+                    for (int ky = 0; ky < 3; ++ky) {
+#pragma unroll
+                        for (int kx = 0; kx < 3; ++kx) {
+                            const float2 x = (ok_y[ky] && ok_x[kx]) ? win[ky][kx] : make_float2(0.f, 0.f);
+                            acc = __ffma2_rn(x, wp[ky * 3 + kx], acc);
+                        }
+                    }
+                    // row r of the stage, channel pair `lane`: 16-byte chunk lane / 4, swizzled
+                    // with the row as TMA's 128-byte swizzle would place it
+                    const int r = ph * kDwSubPx + l0 + j;
+                    *reinterpret_cast<uint32_t*>(stage + r * 128 + ((((lane >> 2) ^ (r & 7))) << 4) +
+                                                 (lane & 3) * 4) = P::pack(acc.x, acc.y);
+#pragma unroll
+                    for (int b = 0; b < 3; ++b) {
+                        win[b][0] = win[b][1];
+                        win[b][1] = win[b][2];
+                    }
+                    if (++w == W8) {
+                        w = 0;
+                        if (++hm == img_h) {
+                            hm = 0;
+                        }
+                    }
+                }
+                // the stage is read by the tensor cores (async proxy)
+                fence_proxy_async_smem();
+                __syncwarp();
+                if (lane == 0) {
+                    mbar_arrive(&hempty[v & 1]);
+                    if (ph == 1) {
+                        mbar_arrive(&full[s]);
+                    }
+                }
+                if (issuer && v + 2 < subs) {
+                    // the band set is free once every producer warp has read it
+                    if (!mbar_wait_bounded(&hempty[v & 1], (v >> 1) & 1, lim)) {
+                        *abort_flag = 1;
+                        report_error(p.err, kErrGemmProducerTimeout);
+                    } else {
+                        issue_halo(v + 2);
+                    }
+                }
+                __syncwarp();
+            }
+            if (issuer && *abort_flag) {
+                // let this thread's copies land before the CTA winds down
+                mbar_wait_bounded(bfull, 0, kSWaitLimit / 16);
+                for (int b = 0; b < 2; ++b) {
+                    if (halo_pending & (1u << b)) {
+                        mbar_wait_bounded(&hfull[b], ((b ? halo_last1 : halo_last0) >> 1) & 1, kSWaitLimit / 16);
+                    }
+                }
+            }
+        }
+    } else if (!DW && warp == 0) {
         // ------------------------------------------------------------ TMA producer
         if (lane == 0 && ntiles > 0 && !p.stall_test) {
             // the W slice once: kblocks boxes of 128 rows x 64 K
@@ -188,7 +381,7 @@ __global__ void __launch_bounds__(kSThreads, 1)
                     mbar_arrive_expect_tx(&full[stage], kSABytes);
                     tma_load_2d(smem + C::kAOffset + stage * kSABytes, &tmA, &full[stage], kb * kSBK, m0);
                     ++issued;
-                    if (++stage == kSStages) {
+                    if (++stage == kStages) {
                         stage = 0;
                         phase ^= 1;
                     }
@@ -197,17 +390,17 @@ __global__ void __launch_bounds__(kSThreads, 1)
             if (*abort_flag) {
                 // let this thread's copies land before the CTA winds down
                 mbar_wait_bounded(bfull, 0, kSWaitLimit / 16);
-                int n = issued < kSStages ? issued : kSStages;
+                int n = issued < kStages ? issued : kStages;
                 for (int i = 0; i < n; ++i) {
                     if (--stage < 0) {
-                        stage = kSStages - 1;
+                        stage = kStages - 1;
                         phase ^= 1;
                     }
                     mbar_wait_bounded(&full[stage], phase, kSWaitLimit / 16);
                 }
             }
         }
-    } else if (warp == 1) {
+    } else if (warp == C::kMmaWarp) {
         // ------------------------------------------------------------ MMA issuer
         if (lane == 0 && ntiles > 0) {
             const uint32_t idesc = make_idesc_f16(kSBM, kSBN, SPack2<T>::kFormat);
@@ -246,7 +439,7 @@ __global__ void __launch_bounds__(kSThreads, 1)
                     }
                     issued_any = true;
                     tc_commit(&empty[stage]);
-                    if (++stage == kSStages) {
+                    if (++stage == kStages) {
                         stage = 0;
                         phase ^= 1;
                     }
@@ -268,7 +461,7 @@ __global__ void __launch_bounds__(kSThreads, 1)
     } else {
         // ------------------------------------------------------------ epilogue warps
         using P = SPack2<T>;
-        const int ew = warp - 2;
+        const int ew = warp - (C::kMmaWarp + 1);
         const int quad = warp & 3;        // TMEM lane quadrant this warp may access
         const int part = ew >> 2;         // which 32 of the CTA's 128 columns
         const int ncol = n0 + part * kSCols;
@@ -298,9 +491,16 @@ __global__ void __launch_bounds__(kSThreads, 1)
                 issue_res(s, s);
             }
         }
-        // the bias of this warp's 32 columns, fixed for the whole range
-        float4 bb[8];
-        {
+        // the bias of this warp's 32 columns, fixed for the whole range: in registers, or (DW,
+        // where four producer warps leave fewer registers per thread) in shared memory
+        float4 bb[DW ? 1 : 8];
+        const float4* bs4 = nullptr;
+        if constexpr (DW) {
+            float* bs = reinterpret_cast<float*>(smem + C::kBiasOffset) + ew * kSCols;
+            bs[lane] = __ldg(p.bias + ncol + lane);
+            __syncwarp();
+            bs4 = reinterpret_cast<const float4*>(bs);
+        } else {
             const float4* b4 = reinterpret_cast<const float4*>(p.bias + ncol);
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
@@ -348,10 +548,16 @@ __global__ void __launch_bounds__(kSThreads, 1)
                 float2 v[16];
 #pragma unroll
                 for (int j = 0; j < 8; ++j) {
+                    float4 b;
+                    if constexpr (DW) {
+                        b = bs4[j];
+                    } else {
+                        b = bb[j];
+                    }
                     v[2 * j] = __fadd2_rn(make_float2(__uint_as_float(r[4 * j + 0]), __uint_as_float(r[4 * j + 1])),
-                                          make_float2(bb[j].x, bb[j].y));
+                                          make_float2(b.x, b.y));
                     v[2 * j + 1] = __fadd2_rn(make_float2(__uint_as_float(r[4 * j + 2]), __uint_as_float(r[4 * j + 3])),
-                                              make_float2(bb[j].z, bb[j].w));
+                                              make_float2(b.z, b.w));
                 }
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
@@ -433,17 +639,17 @@ __global__ void __launch_bounds__(kSThreads, 1)
 
     tc_fence_before();
     __syncthreads();
-    if (warp == 1) {
+    if (warp == C::kMmaWarp) {
         tc_fence_after();
         tmem_dealloc(tmem_base, 2 * kSBN);
     }
 }
 
-template <typename T, int EPI>
+template <typename T, int EPI, bool DW>
 cudaError_t launch_stream(const CUtensorMap* maps, const GemmParams& p, cudaStream_t stream)
 {
-    using C = StreamCfg<EPI>;
-    auto kernel = gemm_stream_kernel<T, EPI>;
+    using C = StreamCfg<EPI, DW>;
+    auto kernel = gemm_stream_kernel<T, EPI, DW>;
     static std::once_flag once;
     static cudaError_t attr_err = cudaSuccess;
     std::call_once(once, [&] {
@@ -458,7 +664,7 @@ cudaError_t launch_stream(const CUtensorMap* maps, const GemmParams& p, cudaStre
     const int groups = (p.M + 31) / 32;
     per = per < groups ? per : groups;
     per = per < 1 ? 1 : per;
-    return launch_pdl(kernel, dim3(slices * per), dim3(kSThreads), C::kBytes, stream, maps[0], maps[1],
+    return launch_pdl(kernel, dim3(slices * per), dim3(C::kThreads), C::kBytes, stream, maps[0], maps[1],
                       maps[2], maps[3], p, per);
 }
 
@@ -487,24 +693,36 @@ cudaError_t gemm_stream_sm100(int dtype, const void* A, int lda, const void* W, 
     if (p.out8 != nullptr && (p.ldo8 % 16 != 0 || (reinterpret_cast<uintptr_t>(p.out8) & 15) != 0)) {
         return cudaErrorInvalidValue;
     }
+    const bool dw = p.dw_weight != nullptr;
+    if (dw && (epi != kEpiBiasRes || p.dw_w < 1 || p.dw_h < 1 ||
+               static_cast<long long>(p.dw_h) * p.dw_w != p.M || p.dw_img_h < 1 || p.dw_h % p.dw_img_h != 0 ||
+               (reinterpret_cast<uintptr_t>(p.dw_weight) & 15) != 0)) {
+        return cudaErrorInvalidValue;
+    }
     const CUtensorMapDataType dt = dtype == 0 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
     CUtensorMap maps[4];
     std::memset(maps, 0, sizeof(maps));
-    if (!make_tmap_2d(&maps[0], dt, A, p.K, p.M, static_cast<uint64_t>(lda) * 2, kSBK, kSBM, 128) ||
+    // A: 128-row operand boxes, or (depthwise form) unswizzled 66-pixel bands of the input
+    if (!(dw ? make_tmap_2d(&maps[0], dt, A, p.K, p.M, static_cast<uint64_t>(lda) * 2, kSBK, kDwBandRows, 0)
+             : make_tmap_2d(&maps[0], dt, A, p.K, p.M, static_cast<uint64_t>(lda) * 2, kSBK, kSBM, 128)) ||
         !make_tmap_2d(&maps[1], dt, W, p.K, p.N, static_cast<uint64_t>(p.K) * 2, kSBK, kSBN, 128) ||
         !make_tmap_2d(&maps[2], dt, p.out, p.N, p.M, static_cast<uint64_t>(p.ldo) * 2, kSCols, 32, 64) ||
         !make_tmap_2d(&maps[3], dt, p.res, p.N, p.M, static_cast<uint64_t>(p.ldr) * 2, kSCols, 32, 64)) {
         return cudaErrorInvalidValue;
     }
+    if (dw) {
+        return dtype == 0 ? launch_stream<__half, kEpiBiasRes, true>(maps, p, stream)
+                          : launch_stream<__nv_bfloat16, kEpiBiasRes, true>(maps, p, stream);
+    }
     if (dtype == 0) {
         switch (epi) {
-        case kEpiBiasRes: return launch_stream<__half, kEpiBiasRes>(maps, p, stream);
-        case kEpiBiasResQ: return launch_stream<__half, kEpiBiasResQ>(maps, p, stream);
+        case kEpiBiasRes: return launch_stream<__half, kEpiBiasRes, false>(maps, p, stream);
+        case kEpiBiasResQ: return launch_stream<__half, kEpiBiasResQ, false>(maps, p, stream);
         }
     } else {
         switch (epi) {
-        case kEpiBiasRes: return launch_stream<__nv_bfloat16, kEpiBiasRes>(maps, p, stream);
-        case kEpiBiasResQ: return launch_stream<__nv_bfloat16, kEpiBiasResQ>(maps, p, stream);
+        case kEpiBiasRes: return launch_stream<__nv_bfloat16, kEpiBiasRes, false>(maps, p, stream);
+        case kEpiBiasResQ: return launch_stream<__nv_bfloat16, kEpiBiasResQ, false>(maps, p, stream);
         }
     }
     return cudaErrorInvalidValue;

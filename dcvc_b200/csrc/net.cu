@@ -393,12 +393,18 @@ void run_dcb(Launch& L, const Dcb& d, const __half* x, int ldx, int H, int W, __
         ldin = d.C;
     }
     gemm(L, d.dc1, kEpiBiasWsilu, xin, ldin, M, s.t1, d.cdc);
-    L.note(launch_dwconv3x3(s.t1, H, W, d.cdc, d.cdc, d.dw, s.t2, d.cdc, L.s, d.dtype, img_h));
+    // d3x3 + conv1x1_bias_shortcut: one streaming GEMM launch whose operand producer computes the
+    // depthwise 3x3, or two launches
+    const bool stream_dc2 = gemm_stream_form_enabled() && gemm_stream_eligible(kEpiBiasRes, M, d.C, d.cdc);
+    const bool dw_fused = stream_dc2 && gemm_dw_fusion_enabled() && d.dc2.dtype == d.dtype;
+    if (!dw_fused) {
+        L.note(launch_dwconv3x3(s.t1, H, W, d.cdc, d.cdc, d.dw, s.t2, d.cdc, L.s, d.dtype, img_h));
+    }
     // the FP8 form: the streaming residual GEMM also writes the E4M3 operand of the quad GEMM
     const bool fp8_quad = d.ffn1_w8 != nullptr && s.t5 != nullptr;
+    const bool out8 = fp8_quad && stream_dc2 && d.C % 16 == 0;
     bool t5_ready = false;
-    if (fp8_quad && gemm_stream_form_enabled() && gemm_stream_eligible(kEpiBiasRes, M, d.C, d.cdc) &&
-        d.C % 16 == 0) {
+    if (dw_fused || out8) {
         GemmParams p{};
         p.M = M;
         p.N = d.C;
@@ -408,12 +414,21 @@ void run_dcb(Launch& L, const Dcb& d, const __half* x, int ldx, int H, int W, __
         p.ldr = ldin;
         p.out = s.t3;
         p.ldo = d.C;
-        p.out8 = s.t5;
-        p.ldo8 = d.C;
-        p.out8_inv_scale = 1.0f / kFp8ActScale;
         p.err = L.err_word;
-        L.note(gemm_sm100(d.dc2.dtype, s.t2, d.cdc, d.dc2.w, p, kEpiBiasRes, kBlockNStream, L.s));
-        t5_ready = true;
+        if (out8) {
+            p.out8 = s.t5;
+            p.ldo8 = d.C;
+            p.out8_inv_scale = 1.0f / kFp8ActScale;
+            t5_ready = true;
+        }
+        if (dw_fused) {
+            p.dw_weight = d.dw;
+            p.dw_h = H;
+            p.dw_w = W;
+            p.dw_img_h = img_h > 0 ? img_h : H;
+        }
+        L.note(gemm_sm100(d.dc2.dtype, dw_fused ? s.t1 : s.t2, d.cdc, d.dc2.w, p, kEpiBiasRes, kBlockNStream,
+                          L.s));
     } else {
         gemm(L, d.dc2, kEpiBiasRes, s.t2, d.cdc, M, s.t3, d.C, xin, ldin);
     }

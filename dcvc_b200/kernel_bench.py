@@ -1,7 +1,7 @@
 """Micro-benchmark of the codec's kernels at their 1080p shapes (CUDA events on the launching
 stream), also the small fixed case used for ncu captures.
 
-    python -m dcvc_b200.kernel_bench [--case quad|quad_f8|wsilu|res|bias2048|dwconv|ffn|ffn_ld|unshuffle|quantize|rans|all]
+    python -m dcvc_b200.kernel_bench [--case quad|quad_f8|wsilu|res|dwres|dwres_split|bias2048|dwconv|ffn|ffn_ld|unshuffle|quantize|rans|all]
                                      [--reps N] [--sets S] [--bn 0|64|128|256|-1]
 
 (--bn -1 selects the streaming form of the residual GEMM.)
@@ -12,7 +12,9 @@ inside a chunk.
 
 Shapes are those of a 512-channel dcb2 DepthConvBlock at 1920x1088 (M = 136 x 240 = 32640
 pixels): dc.0 (512 -> 256, WSiLU), depthwise 3x3 on 256 channels, dc.3 (256 -> 512 + residual),
-ffn.0 (512 -> 4 x 256, WSiLU chunk-add), and the encoder's 2048 -> 512 adaptor.
+ffn.0 (512 -> 4 x 256, WSiLU chunk-add), and the encoder's 2048 -> 512 adaptor.  `dwres` is the
+depthwise 3x3 and dc.3 in one launch (the depthwise form of the streaming residual GEMM),
+`dwres_split` the same two steps as two launches.
 """
 import argparse
 import json
@@ -65,6 +67,23 @@ def _case(name, g, bn=0):
         yq, yh = torch.zeros_like(y), torch.zeros_like(y)
         fn = lambda: ops.quantize_phase(3, 2, y, sc, mu, qd, 0.15, yq, yh, 68, 120)  # noqa: E731
         return fn, 0.0, 8 * y.numel() * 2
+    if name in ("dwres", "dwres_split"):
+        # depthwise 3x3 on dc.0's 256-channel output, then dc.3 (256 -> 512) + bias + residual
+        x = rnd(M8, 256)
+        dw = torch.randn(9, 256, device="cuda", generator=g)
+        w = rnd(512, 256, scale=256 ** -0.5)
+        b = torch.zeros(512, device="cuda")
+        res = rnd(M8, 512)
+        out = torch.empty(M8, 512, device="cuda", dtype=torch.float16)
+        if name == "dwres":
+            fn = lambda: ops.dw3x3_conv1x1_res(x, 136, 240, dw, w, b, res, out=out)  # noqa: E731
+        else:
+            t = torch.empty_like(x)
+
+            def fn():
+                ops.dwconv3x3(x, 136, 240, dw, t)
+                ops.conv1x1(t, w, b, N.EPI_BIAS_RES, res=res, out=out, block_n=N.BLOCK_N_STREAM)
+        return fn, 2.0 * M8 * 512 * 256, (x.numel() + w.numel() + 2 * res.numel()) * 2 + dw.numel() * 4
     if name == "dwconv":
         x = rnd(M8, 256)
         w = torch.randn(9, 256, device="cuda", generator=g)

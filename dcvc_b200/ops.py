@@ -125,6 +125,30 @@ def dwconv3x3(x, H, W, w, out=None):
     return out
 
 
+def dwconv3x3_ex(x, H, W, w, img_h=0, out=None):
+    """dwconv3x3 for FP16 or BF16 x over images of img_h rows stacked along H (0: one image)."""
+    C = x.shape[1]
+    if out is None:
+        out = torch.empty_like(x)
+    N.check(N.lib.dcvc_dwconv3x3_ex(_DT[x.dtype], x.data_ptr(), H, W, img_h, C, x.stride(0), w.data_ptr(),
+                                    out.data_ptr(), out.stride(0), _stream()), "dcvc_dwconv3x3_ex")
+    return out
+
+
+def dw3x3_conv1x1_res(x, H, W, dw_w, w, bias, res, img_h=0, out=None):
+    """(dwconv3x3_ex(x) . w^T + bias + res) in one launch: x [H*W, K], dw_w fp32 [9, K],
+    w [N, K], bias fp32 [N], res [H*W, N] (row pitches from the tensors)."""
+    M, K = x.shape
+    Nn = w.shape[0]
+    assert M == H * W and w.shape[1] == K and w.is_contiguous() and dw_w.is_contiguous()
+    if out is None:
+        out = torch.empty((M, Nn), dtype=x.dtype, device=x.device)
+    N.check(N.lib.dcvc_dw3x3_conv1x1_res(_DT[x.dtype], H, W, img_h, x.data_ptr(), x.stride(0), dw_w.data_ptr(),
+                                         K, w.data_ptr(), Nn, bias.data_ptr(), res.data_ptr(), res.stride(0),
+                                         out.data_ptr(), out.stride(0), _stream()), "dcvc_dw3x3_conv1x1_res")
+    return out
+
+
 # ----------------------------------------------------------------------------- elementwise
 
 def _sig(name, args):

@@ -152,6 +152,27 @@ int dcvc_conv_ffn(int M, int C, int cffn, const void* x, int ldx, const void* w1
  * d3x3_kernel.h:104-166, d3x3.cu). */
 int dcvc_dwconv3x3(const void* x, int H, int W, int C, int ldx, const float* w, void* out, int ldo,
                    void* stream);
+/* dcvc_dwconv3x3 for FP16 or BF16 (dtype) over images of img_h rows stacked along H (a tap in
+ * the image above or below reads zero; img_h = 0: one image).  No counterpart in the reference
+ * (FP16 only there, one image per launch). */
+int dcvc_dwconv3x3_ex(int dtype, const void* x, int H, int W, int img_h, int C, int ldx, const float* w,
+                      void* out, int ldo, void* stream);
+/* out[M, N] = dw(x)[M, K] . w[N, K]^T + bias + res with M = H * W: the DepthConvBlock's depthwise
+ * 3x3 and the conv1x1_bias_shortcut after it (src/layers/extensions/inference/layers_proxy.cpp:81-82,
+ * d3x3 then conv1x1_bias_shortcut) as one launch of the streaming residual GEMM, whose operand
+ * producer computes the depthwise 3x3 on the CUDA cores; its output never goes to memory.  dw is
+ * dcvc_dwconv3x3_ex (x [H*W, K] pitch ldx, dw_weight FP32 [9][K], images of img_h rows, 0: one)
+ * and the result is bitwise that of dcvc_dwconv3x3_ex followed by dcvc_conv1x1 with
+ * DCVC_EPI_BIAS_RES.  dtype DCVC_F16 or DCVC_BF16; K a multiple of 64 up to 256, N of 128; w, res,
+ * out with pitches K, ldr, ldo.  No counterpart in the reference (two launches there). */
+int dcvc_dw3x3_conv1x1_res(int dtype, int H, int W, int img_h, const void* x, int ldx,
+                           const float* dw_weight, int K, const void* w, int N, const float* bias,
+                           const void* res, int ldr, void* out, int ldo, void* stream);
+/* Whether the codecs run each DepthConvBlock's depthwise 3x3 inside the residual GEMM that follows
+ * it (1; needs the streaming form) or as a launch of its own (0, the default: at 1080p the fused
+ * launch takes 114.7 us against 32.2 us for the two launches).  Output bits are the same either
+ * way.  No counterpart in the reference. */
+int dcvc_dw_fusion(int enable);
 
 /* Layout kernels (FP16, NHWC rows with pitches in elements). */
 /* pad_and_unshuffle_8 / pixel_unshuffle(8) (elementwise/cat_and_pad.cu:7-51, shuffle.cu:134-185):

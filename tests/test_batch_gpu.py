@@ -81,3 +81,27 @@ def test_batch_arguments_are_checked():
         enc.compress_batch([x, x], [1, 64], False, 0, 0)  # qp out of range
     out = enc.compress_batch([x, x], [7, 7], False, 0, 0)
     assert np.array_equal(out[0][0], out[1][0])  # same input, same QP, same reference: same bytes
+
+
+def test_packed_batch_with_and_without_depthwise_fusion():
+    """Stacked images keep their own zero borders in the depthwise form of the residual GEMM
+    too: a packed batch codes to the same bytes with the depthwise 3x3 fused or separate."""
+    from dcvc_b200 import _native as N
+    sd = state_dict()
+    H, W, n = 200, 248, 2
+    pr, pb = synthetic.padding_for(H, W)
+    refs = [synthetic.padded_reference_frame(synthetic.video_chunk_yuv420(4 + k, H, W, 1, 0)[0])
+            for k in range(n)]
+    xs = [synthetic.to_model_input(synthetic.video_chunk_yuv420(4 + k, H, W, 8, 8)) for k in range(n)]
+    out = {}
+    try:
+        for on in (1, 0):
+            N.lib.dcvc_dw_fusion(on)
+            enc = _proxy(sd, "fp16")
+            enc.add_ref_features_from_frames(refs, True)
+            out[on] = enc.compress_batch(xs, [7, 58], False, pb, pr)
+            torch.cuda.synchronize()
+    finally:
+        N.lib.dcvc_dw_fusion(0)
+    for (b0, e0), (b1, e1) in zip(out[0], out[1]):
+        assert e0 == e1 and np.array_equal(b0, b1)

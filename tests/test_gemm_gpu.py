@@ -206,3 +206,77 @@ def test_bounded_wait_runs_out_and_the_gpu_keeps_answering(form):
     assert lib.dcvc_check_device_errors(stream) == 0
     ref = _ref(epi, a, w, b, res)
     assert bool(((out.float() - ref).abs() <= 2e-2 + 1e-2 * ref.abs()).all())
+
+
+DW_CASES = [
+    # (H, W, img_h, K, N, dtype): dc.3 of a 512-channel block at 1080p; y-level; stacked images
+    # with an odd width; a grid narrower than one warp's 16 pixels; one-row images
+    (136, 240, 0, 256, 512, torch.float16),
+    (136, 240, 0, 256, 512, torch.bfloat16),
+    (68, 120, 0, 256, 256, torch.float16),
+    (26, 52, 13, 256, 128, torch.float16),
+    (26, 52, 13, 128, 384, torch.bfloat16),
+    (5, 7, 0, 64, 128, torch.float16),
+    (3, 300, 1, 192, 256, torch.float16),
+]
+
+
+@pytest.mark.parametrize("H,W,img_h,K,Nn,dtype", DW_CASES)
+def test_depthwise_form_is_bitwise_the_two_launches(H, W, img_h, K, Nn, dtype):
+    """The depthwise form of the streaming residual GEMM (the depthwise 3x3 computed by its operand
+    producer) gives bitwise the outputs of the depthwise kernel followed by the residual GEMM, and
+    is within tolerance of an fp32 torch reference of the two steps."""
+    from dcvc_b200 import _native as N, ops
+    M = H * W
+    g = torch.Generator(device="cuda").manual_seed(H * W + K)
+    xbuf = torch.randn(M, K + 64, device="cuda", generator=g).to(dtype)
+    x = xbuf[:, 64:]
+    dw = torch.randn(9, K, device="cuda", generator=g) * 0.3
+    w = (torch.randn(Nn, K, device="cuda", generator=g) / K ** 0.5).to(dtype)
+    b = torch.randn(Nn, device="cuda", generator=g) * 0.1
+    res = torch.randn(M, Nn, device="cuda", generator=g).to(dtype)
+    t = ops.dwconv3x3_ex(x, H, W, dw, img_h=img_h)
+    split = ops.conv1x1(t, w, b, N.EPI_BIAS_RES, res=res, block_n=N.BLOCK_N_STREAM)
+    tiled = ops.conv1x1(t, w, b, N.EPI_BIAS_RES, res=res, block_n=128)
+    obuf = torch.full((M, Nn + 64), 7.0, device="cuda", dtype=dtype)
+    fused = ops.dw3x3_conv1x1_res(x, H, W, dw, w, b, res, img_h=img_h, out=obuf[:, 64:])
+    torch.cuda.synchronize()
+    assert N.device_error() == 0
+    assert torch.equal(fused.view(torch.int16), split.view(torch.int16))
+    assert torch.equal(fused.view(torch.int16), tiled.view(torch.int16))
+    assert bool((obuf[:, :64] == 7.0).all())
+    # fp32 reference: per-image zero-padded depthwise conv, rounded to the activation type
+    ih = img_h if img_h > 0 else H
+    xi = x.float().reshape(H // ih, ih, W, K).permute(0, 3, 1, 2)
+    d = torch.nn.functional.conv2d(xi, dw.t().reshape(K, 1, 3, 3), padding=1, groups=K)
+    d = d.permute(0, 2, 3, 1).reshape(M, K).to(dtype).float()
+    ref = d @ w.float().t() + b + res.float()
+    atol, rtol = TOL[dtype]
+    assert bool(((fused.float() - ref).abs() <= atol + rtol * ref.abs()).all())
+
+
+def test_depthwise_form_bounded_wait_runs_out():
+    """The depthwise form's producers skip their work under the stall injection; the MMA and
+    epilogue waits run out, the launch reports DCVC_DEVICE_TIMEOUT and the next launch is right."""
+    import ctypes
+    from dcvc_b200 import _native as N, ops
+    lib = N.lib
+    lib.dcvc_gemm_inject_stall.argtypes = [ctypes.c_int, ctypes.c_longlong]
+    lib.dcvc_check_device_errors.argtypes = [ctypes.c_void_p]
+    g = torch.Generator(device="cuda").manual_seed(13)
+    H, W, K, Nn = 32, 64, 256, 512
+    x = torch.randn(H * W, K, device="cuda", generator=g).half()
+    dw = torch.randn(9, K, device="cuda", generator=g) * 0.3
+    w = (torch.randn(Nn, K, device="cuda", generator=g) / K ** 0.5).half()
+    b = torch.randn(Nn, device="cuda", generator=g) * 0.1
+    res = torch.randn(H * W, Nn, device="cuda", generator=g).half()
+    stream = torch.cuda.current_stream().cuda_stream
+    assert lib.dcvc_check_device_errors(stream) == 0
+    assert lib.dcvc_gemm_inject_stall(1, 20000) == 0
+    ops.dw3x3_conv1x1_res(x, H, W, dw, w, b, res)
+    assert lib.dcvc_check_device_errors(stream) == 3  # DCVC_DEVICE_TIMEOUT
+    out = ops.dw3x3_conv1x1_res(x, H, W, dw, w, b, res)
+    assert lib.dcvc_check_device_errors(stream) == 0
+    t = ops.dwconv3x3_ex(x, H, W, dw)
+    ref = ops.conv1x1(t, w, b, N.EPI_BIAS_RES, res=res, block_n=N.BLOCK_N_STREAM)
+    assert torch.equal(out.view(torch.int16), ref.view(torch.int16))

@@ -143,3 +143,32 @@ def test_fp8_operand_fused_in_the_residual_epilogue_is_bitwise_the_separate_quan
         N.lib.dcvc_gemm_stream_form(1)
     assert np.array_equal(out[0][0], out[1][0])
     assert all(torch.equal(a, b) for a, b in zip(out[0][1], out[1][1]))
+
+
+@pytest.mark.parametrize("precision", ["fp16", "bf16"])
+def test_depthwise_fused_into_the_residual_gemm_gives_the_same_codec_outputs(precision):
+    """With the depthwise 3x3 computed inside the residual GEMM (opt-in) and as its own launch
+    (the default), the codec gives the same payload and reconstruction."""
+    from dcvc_b200 import _native as N
+    sd = state_dict()
+    H, W = 128, 192
+    out = {}
+    try:
+        for on in (1, 0):
+            N.lib.dcvc_dw_fusion(on)
+            enc, dec = _proxy(sd, precision), _proxy(sd, precision)
+            ref = ref_frame(H, W)
+            enc.add_ref_feature_from_frame(ref, True)
+            dec.add_ref_feature_from_frame(ref, False)
+            res = []
+            for k, qp in enumerate((12, 50)):
+                bits, ecp = enc.compress(chunk(H, W, k), qp, False, 0, 0)
+                frames = dec.decompress(bits, qp, H, W, ecp, False)
+                torch.cuda.synchronize()
+                res.append((bits, [f.clone() for f in frames]))
+            out[on] = res
+    finally:
+        N.lib.dcvc_dw_fusion(0)
+    for (b0, f0), (b1, f1) in zip(out[0], out[1]):
+        assert np.array_equal(b0, b1)
+        assert all(torch.equal(a, b) for a, b in zip(f0, f1))
