@@ -70,7 +70,7 @@ int dcvc_check_device_errors(void* stream)
 
 int dcvc_gemm_stream_form(int enable)
 {
-    gemm_set_stream_form(enable != 0);
+    gemm_set_stream_form(enable);
     return kOk;
 }
 

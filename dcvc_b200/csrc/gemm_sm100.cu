@@ -627,18 +627,20 @@ std::atomic<int> g_stream_form{1};
 std::atomic<int> g_dw_fusion{0};
 }  // namespace
 
-void gemm_set_stream_form(bool on) { g_stream_form.store(on ? 1 : 0); }
+void gemm_set_stream_form(int form) { g_stream_form.store(form < 0 ? 0 : (form > 2 ? 2 : form)); }
 bool gemm_stream_form_enabled() { return g_stream_form.load(std::memory_order_relaxed) != 0; }
 void gemm_set_dw_fusion(bool on) { g_dw_fusion.store(on ? 1 : 0); }
 bool gemm_dw_fusion_enabled() { return g_dw_fusion.load(std::memory_order_relaxed) != 0; }
 
 int gemm_pick_bn(int M, int N, int epi, int sub_cout, int K)
 {
-    if (K > 0 && g_stream_form.load(std::memory_order_relaxed) != 0 &&
-        gemm_stream_eligible(epi, M, N, K)) {
+    const int form = g_stream_form.load(std::memory_order_relaxed);
+    const bool res = epi == kEpiBiasRes || epi == kEpiBiasResQ;
+    if (K > 0 && (res ? form >= 1 : form >= 2) && gemm_stream_eligible(epi, M, N, K)) {
         // residual epilogues at K <= 256: the streaming form (W resident, row ranges per CTA)
         // moves the same bytes in 18.1 us where the tiled kernel takes 21.8 us (dc.3 / ffn.2 at
-        // 1080p), with the same output bits
+        // 1080p), with the same output bits; the bias / WSiLU epilogues at K <= 512 only when
+        // asked for (form 2)
         return kBlockNStream;
     }
     if (epi == kEpiQuad) {

@@ -81,12 +81,14 @@ GemmParams gemm_apply_injection(const GemmParams& p);
 // dtype of gemm_sm100 / dcvc_conv1x1 for E4M3 operands with FP32 accumulation and BF16 output.
 constexpr int kDtypeF8 = 2;
 
-// The streaming form: residual epilogues (kEpiBiasRes, kEpiBiasResQ) with K <= 256 and N a
-// multiple of 128.  Bitwise the same outputs as gemm_sm100 at any tile width.
+// The streaming form: residual epilogues (kEpiBiasRes, kEpiBiasResQ) with K <= 256, bias and
+// WSiLU epilogues with K <= 512, N a multiple of 128.  Bitwise the same outputs as gemm_sm100 at
+// any tile width.
 bool gemm_stream_eligible(int epi, int M, int N, int K);
-// Whether the library's own choice (block_n = 0, no tuned width) may pick the streaming form
-// (default on); explicit block_n values are not affected.
-void gemm_set_stream_form(bool on);
+// Which epilogues the library's own choice (block_n = 0, no tuned width) may give the streaming
+// form: 0 none, 1 the residual epilogues (default), 2 also bias and WSiLU; explicit block_n values
+// are not affected.
+void gemm_set_stream_form(int form);
 bool gemm_stream_form_enabled();
 // Whether the codecs compute the depthwise 3x3 inside the streaming residual GEMM (default off:
 // measured slower than the two launches, see the kernel file).

@@ -46,12 +46,16 @@ namespace {
 constexpr int kSBM = 128;                   // rows per MMA tile
 constexpr int kSBN = 128;                   // output channels per CTA
 constexpr int kSBK = 64;                    // one 128-byte swizzle atom of 16-bit elements
-constexpr int kSMaxK = 256;                 // W slice resident: 128 x 256 x 2 B = 64 KB
+constexpr int kSMaxK = 256;                 // residual epilogues: W slice 128 x 256 x 2 B = 64 KB
+constexpr int kSMaxKPlain = 512;            // bias / WSiLU epilogues: W slice up to 128 KB
 constexpr int kSEpiWarps = 16;
 constexpr int kSCols = kSBN / 4;            // accumulator columns per epilogue warp (32)
 constexpr int kSBoxBytes = 32 * kSCols * 2; // 32 rows x 32 columns of 16-bit values: 2 KB
 constexpr int kSResSlots = 2;               // residual ring depth per warp, in tiles
 constexpr int kSStages = 6;
+constexpr int kSStagesPlain = 4;            // bias / WSiLU: a W slice twice as large leaves four
+
+__host__ __device__ constexpr bool stream_has_res(int epi) { return epi == kEpiBiasRes || epi == kEpiBiasResQ; }
 constexpr int kSABytes = kSBM * kSBK * 2;   // 16 KB
 constexpr long long kSWaitLimit = 2000000000LL;  // ~1 s at 2 GHz; a correct kernel never waits this long
 // depthwise form
@@ -68,15 +72,19 @@ struct StreamCfg {
     static constexpr int kProdWarps = DW ? kDwProdWarps : 1;
     static constexpr int kMmaWarp = kProdWarps;
     static constexpr int kThreads = 32 * (kProdWarps + 1 + kSEpiWarps);
-    static constexpr int kStages = DW ? kDwStages : kSStages;
+    static constexpr bool kRes = stream_has_res(EPI);
+    static constexpr int kStages = DW ? kDwStages : (kRes ? kSStages : kSStagesPlain);
+    // residual epilogues: a ring of residual boxes per warp; others: one output staging box
+    static constexpr int kResSlots = kRes ? kSResSlots : 1;
+    static constexpr int kMaxK = kRes ? kSMaxK : kSMaxKPlain;
     static constexpr int kSlotBytes = kSBoxBytes;
     static constexpr int kBOffset = 0;                                   // resident W slice
-    static constexpr int kBBytes = kSBN * kSMaxK * 2;                    // 64 KB
+    static constexpr int kBBytes = kSBN * kMaxK * 2;                     // 64 / 128 KB
     static constexpr int kAOffset = kBOffset + kBBytes;
     static constexpr int kHaloOffset = kAOffset + kStages * kSABytes;    // two band sets (DW)
     static constexpr int kHaloBytes = DW ? (2 * kDwHaloBytes + 1023) / 1024 * 1024 : 0;
     static constexpr int kEpiOffset = kHaloOffset + kHaloBytes;
-    static constexpr int kEpiBytes = kSEpiWarps * kSResSlots * kSlotBytes;
+    static constexpr int kEpiBytes = kSEpiWarps * kResSlots * kSlotBytes;
     static constexpr int kBarOffset = kEpiOffset + kEpiBytes;
     static constexpr int kBarBytes = 512;
     // DW: each epilogue warp's 32 bias values (registers are short with four producer warps)
@@ -465,7 +473,7 @@ __global__ void __launch_bounds__(StreamCfg<EPI, DW>::kThreads, 1)
         const int quad = warp & 3;        // TMEM lane quadrant this warp may access
         const int part = ew >> 2;         // which 32 of the CTA's 128 columns
         const int ncol = n0 + part * kSCols;
-        uint8_t* wbuf = smem + C::kEpiOffset + ew * kSResSlots * C::kSlotBytes;
+        uint8_t* wbuf = smem + C::kEpiOffset + ew * C::kResSlots * C::kSlotBytes;
         uint64_t* rbar = &resbar[ew * kSResSlots];
         uint32_t res_phase = 0;
         uint32_t res_pending = 0;
@@ -475,7 +483,7 @@ __global__ void __launch_bounds__(StreamCfg<EPI, DW>::kThreads, 1)
         }
         // residual box of this warp for tile t into slot s (rows past the range: nothing)
         auto issue_res = [&](int t, int s) {
-            if (t >= ntiles) {
+            if (!C::kRes || t >= ntiles) {
                 return;
             }
             const int row0 = r0 + t * kSBM + quad * 32;
@@ -487,7 +495,7 @@ __global__ void __launch_bounds__(StreamCfg<EPI, DW>::kThreads, 1)
             res_pending |= 1u << s;
         };
         if (lane == 0) {
-            for (int s = 0; s < kSResSlots; ++s) {
+            for (int s = 0; s < C::kResSlots; ++s) {
                 issue_res(s, s);
             }
         }
@@ -510,7 +518,7 @@ __global__ void __launch_bounds__(StreamCfg<EPI, DW>::kThreads, 1)
         int acc = 0;
         uint32_t acc_phase = 0;
         for (int t = 0; t < ntiles && !*abort_flag; ++t) {
-            const int slot = t % kSResSlots;
+            const int slot = t % C::kResSlots;
             const int row0 = r0 + t * kSBM + quad * 32;
             const bool rows_live = row0 < r1;
             uint8_t* buf = wbuf + slot * C::kSlotBytes;
@@ -520,7 +528,7 @@ __global__ void __launch_bounds__(StreamCfg<EPI, DW>::kThreads, 1)
                 break;
             }
             tc_fence_after();
-            if (rows_live) {
+            if (C::kRes && rows_live) {
                 if (!mbar_wait_bounded(&rbar[slot], (res_phase >> slot) & 1u, lim)) {
                     *abort_flag = 1;
                     report_error(p.err, kErrGemmEpilogueTimeout);
@@ -559,13 +567,21 @@ __global__ void __launch_bounds__(StreamCfg<EPI, DW>::kThreads, 1)
                     v[2 * j + 1] = __fadd2_rn(make_float2(__uint_as_float(r[4 * j + 2]), __uint_as_float(r[4 * j + 3])),
                                               make_float2(b.z, b.w));
                 }
+                if constexpr (C::kRes) {
 #pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const uint4 u = *reinterpret_cast<const uint4*>(buf + sw64_off(lane, j));
-                    v[4 * j + 0] = __fadd2_rn(v[4 * j + 0], P::unpack(u.x));
-                    v[4 * j + 1] = __fadd2_rn(v[4 * j + 1], P::unpack(u.y));
-                    v[4 * j + 2] = __fadd2_rn(v[4 * j + 2], P::unpack(u.z));
-                    v[4 * j + 3] = __fadd2_rn(v[4 * j + 3], P::unpack(u.w));
+                    for (int j = 0; j < 4; ++j) {
+                        const uint4 u = *reinterpret_cast<const uint4*>(buf + sw64_off(lane, j));
+                        v[4 * j + 0] = __fadd2_rn(v[4 * j + 0], P::unpack(u.x));
+                        v[4 * j + 1] = __fadd2_rn(v[4 * j + 1], P::unpack(u.y));
+                        v[4 * j + 2] = __fadd2_rn(v[4 * j + 2], P::unpack(u.z));
+                        v[4 * j + 3] = __fadd2_rn(v[4 * j + 3], P::unpack(u.w));
+                    }
+                }
+                if constexpr (EPI == kEpiBiasWsilu) {
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) {
+                        v[j] = wsilu2(v[j]);
+                    }
                 }
                 if constexpr (EPI == kEpiBiasResQ) {
                     // this lane's row picks its image's factors in a packed batch
@@ -619,15 +635,15 @@ __global__ void __launch_bounds__(StreamCfg<EPI, DW>::kThreads, 1)
                     bulk_commit();
                 }
                 if (!*abort_flag) {
-                    bulk_wait_read0();  // the store has read the slot: refill it
-                    issue_res(t + kSResSlots, slot);
+                    bulk_wait_read0();  // the store has read the slot: refill or reuse it
+                    issue_res(t + C::kResSlots, slot);
                 }
             }
             __syncwarp();
         }
         if (lane == 0) {
             // after an abort, let this warp's residual loads land before the CTA winds down
-            for (int s = 0; s < kSResSlots; ++s) {
+            for (int s = 0; s < C::kResSlots; ++s) {
                 if (res_pending & (1u << s)) {
                     mbar_wait_bounded(&rbar[s], (res_phase >> s) & 1u, kSWaitLimit / 16);
                 }
@@ -672,8 +688,12 @@ cudaError_t launch_stream(const CUtensorMap* maps, const GemmParams& p, cudaStre
 
 bool gemm_stream_eligible(int epi, int M, int N, int K)
 {
-    return (epi == kEpiBiasRes || epi == kEpiBiasResQ) && M > 0 &&
-           N % kSBN == 0 && K % kSBK == 0 && K <= kSMaxK && N / kSBN <= num_sms();
+    const bool res = stream_has_res(epi);
+    if (!res && epi != kEpiBias && epi != kEpiBiasWsilu) {
+        return false;
+    }
+    return M > 0 && N % kSBN == 0 && K % kSBK == 0 && K <= (res ? kSMaxK : kSMaxKPlain) &&
+           N / kSBN <= num_sms();
 }
 
 // Host launcher of the streaming form; same operands and checks as gemm_sm100 (A [M, K] with
@@ -681,11 +701,17 @@ bool gemm_stream_eligible(int epi, int M, int N, int K)
 cudaError_t gemm_stream_sm100(int dtype, const void* A, int lda, const void* W, const GemmParams& p,
                               int epi, cudaStream_t stream)
 {
+    const bool res = stream_has_res(epi);
     if (!gemm_stream_eligible(epi, p.M, p.N, p.K) || lda % 8 != 0 || p.ldo % 8 != 0 ||
         (reinterpret_cast<uintptr_t>(A) & 15) != 0 || (reinterpret_cast<uintptr_t>(W) & 15) != 0 ||
-        (reinterpret_cast<uintptr_t>(p.out) & 15) != 0 || p.bias == nullptr || p.res == nullptr ||
-        p.ldr % 8 != 0 || (reinterpret_cast<uintptr_t>(p.res) & 15) != 0) {
+        (reinterpret_cast<uintptr_t>(p.out) & 15) != 0 || p.bias == nullptr) {
         return cudaErrorInvalidValue;
+    }
+    if (res && (p.res == nullptr || p.ldr % 8 != 0 || (reinterpret_cast<uintptr_t>(p.res) & 15) != 0)) {
+        return cudaErrorInvalidValue;
+    }
+    if (!res && p.out8 != nullptr) {
+        return cudaErrorInvalidValue;  // the E4M3 side output belongs to the residual epilogues
     }
     if (epi == kEpiBiasResQ && p.qscale == nullptr) {
         return cudaErrorInvalidValue;
@@ -707,8 +733,11 @@ cudaError_t gemm_stream_sm100(int dtype, const void* A, int lda, const void* W, 
              : make_tmap_2d(&maps[0], dt, A, p.K, p.M, static_cast<uint64_t>(lda) * 2, kSBK, kSBM, 128)) ||
         !make_tmap_2d(&maps[1], dt, W, p.K, p.N, static_cast<uint64_t>(p.K) * 2, kSBK, kSBN, 128) ||
         !make_tmap_2d(&maps[2], dt, p.out, p.N, p.M, static_cast<uint64_t>(p.ldo) * 2, kSCols, 32, 64) ||
-        !make_tmap_2d(&maps[3], dt, p.res, p.N, p.M, static_cast<uint64_t>(p.ldr) * 2, kSCols, 32, 64)) {
+        (res && !make_tmap_2d(&maps[3], dt, p.res, p.N, p.M, static_cast<uint64_t>(p.ldr) * 2, kSCols, 32, 64))) {
         return cudaErrorInvalidValue;
+    }
+    if (!res) {
+        maps[3] = maps[2];  // no residual: the kernel never reads this map
     }
     if (dw) {
         return dtype == 0 ? launch_stream<__half, kEpiBiasRes, true>(maps, p, stream)
@@ -716,11 +745,15 @@ cudaError_t gemm_stream_sm100(int dtype, const void* A, int lda, const void* W, 
     }
     if (dtype == 0) {
         switch (epi) {
+        case kEpiBias: return launch_stream<__half, kEpiBias, false>(maps, p, stream);
+        case kEpiBiasWsilu: return launch_stream<__half, kEpiBiasWsilu, false>(maps, p, stream);
         case kEpiBiasRes: return launch_stream<__half, kEpiBiasRes, false>(maps, p, stream);
         case kEpiBiasResQ: return launch_stream<__half, kEpiBiasResQ, false>(maps, p, stream);
         }
     } else {
         switch (epi) {
+        case kEpiBias: return launch_stream<__nv_bfloat16, kEpiBias, false>(maps, p, stream);
+        case kEpiBiasWsilu: return launch_stream<__nv_bfloat16, kEpiBiasWsilu, false>(maps, p, stream);
         case kEpiBiasRes: return launch_stream<__nv_bfloat16, kEpiBiasRes, false>(maps, p, stream);
         case kEpiBiasResQ: return launch_stream<__nv_bfloat16, kEpiBiasResQ, false>(maps, p, stream);
         }

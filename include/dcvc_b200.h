@@ -99,9 +99,10 @@ int dcvc_conv1x1(int dtype, int epilogue, int M, int N, int K, const void* a, in
                  const void* w, const float* bias, const void* res, int ldr, const void* res2,
                  int ldr2, const void* qscale, void* out, int ldo, int sub_w, int sub_cout,
                  int block_n, void* stream);
-/* Whether the library's own tile choice (block_n = 0 without a tuned width, and the codecs) may
- * pick the streaming form of the residual epilogues: 1 (the default) or 0.  Output bits are the
- * same either way.  No counterpart in the reference. */
+/* Which GEMMs the library's own tile choice (block_n = 0 without a tuned width, and the codecs)
+ * gives the streaming form: 0 none, 1 the residual epilogues at K <= 256 (the default), 2 also
+ * the bias and WSiLU epilogues at K <= 512.  Output bits are the same either way.  No counterpart
+ * in the reference. */
 int dcvc_gemm_stream_form(int enable);
 /* The FP8 form of dcvc_conv1x1 for the epilogues BIAS, BIAS_WSILU and QUAD: a [M, K] and
  * w [N, K] are E4M3 bytes (lda a multiple of 16, K of 128), the tcgen05 MMA is kind::f8f6f4

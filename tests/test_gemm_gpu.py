@@ -110,13 +110,20 @@ STREAM_CASES = [
     ("EPI_BIAS_RES", 37, 128, 64, torch.float16),
     ("EPI_BIAS_RES", 32640, 512, 256, torch.bfloat16),
     ("EPI_BIAS_RES_Q", 3000, 256, 256, torch.bfloat16),
+    # bias / WSiLU epilogues at K <= 512: dc.0 at 1080p and at the y level, ragged shapes
+    ("EPI_BIAS_WSILU", 32640, 256, 512, torch.float16),
+    ("EPI_BIAS_WSILU", 8160, 256, 512, torch.bfloat16),
+    ("EPI_BIAS_WSILU", 2047, 640, 448, torch.float16),
+    ("EPI_BIAS", 4471, 384, 320, torch.float16),
+    ("EPI_BIAS", 37, 128, 64, torch.bfloat16),
 ]
 
 
 @pytest.mark.parametrize("name,M,Nn,K,dtype", STREAM_CASES)
 def test_stream_form_matches_tiled_bitwise(name, M, Nn, K, dtype):
-    """The streaming residual GEMM (W slice resident, row ranges per CTA) gives bitwise the
-    tiled kernel's outputs, and both are within the fp32-reference tolerance."""
+    """The streaming GEMM (W slice resident, row ranges per CTA) gives bitwise the tiled kernel's
+    outputs for the residual, bias and WSiLU epilogues, and both are within the fp32-reference
+    tolerance."""
     from dcvc_b200 import _native as N, ops
     epi = getattr(N, name)
     g = torch.Generator(device="cuda").manual_seed(M + Nn + K)
