@@ -30,6 +30,7 @@ F16, BF16 = 0, 1
 EPI_BIAS, EPI_BIAS_WSILU, EPI_BIAS_RES, EPI_BIAS_RES_Q, EPI_BIAS_RES2, EPI_QUAD, EPI_SUBPEL, \
     EPI_BIAS_Q = range(8)
 BLOCK_N_STREAM = -1  # dcvc_conv1x1 block_n: the streaming form of the residual epilogues
+BLOCK_N_PAIR = -2  # dcvc_conv1x1 block_n: the CTA-pair form (cta_group::2) of bias / WSiLU / quad
 
 
 class DcvcError(RuntimeError):
@@ -73,6 +74,7 @@ _proto("dcvc_dwconv3x3_ex", c_int, [c_int, c_vp, c_int, c_int, c_int, c_int, c_i
 _proto("dcvc_dw3x3_conv1x1_res", c_int, [c_int, c_int, c_int, c_int, c_vp, c_int, c_vp, c_int, c_vp, c_int,
                                         c_vp, c_vp, c_int, c_vp, c_int, c_vp])
 _proto("dcvc_dw_fusion", c_int, [c_int])
+_proto("dcvc_gemm_pair_form", c_int, [c_int])
 
 
 def device_error(clear=True):

@@ -234,6 +234,25 @@ int dcvc_hts_import_state(void* handle, const void* src, int flags, void* stream
                                                                static_cast<cudaStream_t>(stream));
 }
 
+int dcvc_hts_set_timing(void* handle, int enable)
+{
+    if (handle == nullptr) {
+        return fail(kInvalidArgument, "dcvc_hts_set_timing: null handle");
+    }
+    static_cast<HtsHandle*>(handle)->codec.set_timing(enable != 0);
+    return kOk;
+}
+
+int dcvc_hts_timing(void* handle, float* out, int cap, int* count)
+{
+    if (handle == nullptr || out == nullptr || cap < 0) {
+        return fail(kInvalidArgument, "dcvc_hts_timing: null handle or output");
+    }
+    const int n = static_cast<HtsHandle*>(handle)->codec.timing(out, cap);
+    if (count) *count = n;
+    return kOk;
+}
+
 int dcvc_hts_stats(void* handle, int* symbols, int* kernels, size_t* device_bytes)
 {
     if (handle == nullptr) {

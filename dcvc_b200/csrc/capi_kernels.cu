@@ -74,6 +74,12 @@ int dcvc_gemm_stream_form(int enable)
     return kOk;
 }
 
+int dcvc_gemm_pair_form(int enable)
+{
+    gemm_set_pair_form(enable != 0);
+    return kOk;
+}
+
 int dcvc_dw_fusion(int enable)
 {
     gemm_set_dw_fusion(enable != 0);

@@ -7,11 +7,29 @@
 #include "rans_coder.h"
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
+#include <chrono>
 #include <functional>
 #include <vector>
 
 namespace dcvc {
+
+// An NVTX range over a scope (phase graph launches, host entropy coding), visible to profilers
+// that attach an NVTX tool; without one the calls do nothing.
+class NvtxRange {
+public:
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
+
+using Clock = std::chrono::steady_clock;
+inline float ms_between(Clock::time_point a, Clock::time_point b)
+{
+    return std::chrono::duration<float, std::milli>(b - a).count();
+}
 
 // One CUDA graph per phase slot.  The first run of a slot is eager (it initialises every
 // kernel's attributes and validates the launches), the second is captured into a graph, later

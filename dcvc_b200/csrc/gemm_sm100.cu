@@ -66,7 +66,9 @@ __host__ __device__ constexpr int out_box_cols(int bn, int epi)
     return epi == kEpiQuad ? epi_cols(bn, epi) / 4 : (epi_cols(bn, epi) < 64 ? epi_cols(bn, epi) : 64);
 }
 
-template <int BN, int EPI>
+// PAIR: the CTA is one of a cluster pair computing 256-row tiles with cta_group::2; it stages
+// half of the B tile (BN / 2 rows).
+template <int BN, int EPI, bool PAIR = false>
 struct GemmCfg {
     static constexpr int kEpiWarps = epi_warps(BN, EPI);
     static constexpr int kThreads = 64 + 32 * kEpiWarps;  // producer warp, MMA warp, epilogue warps
@@ -85,7 +87,7 @@ struct GemmCfg {
     static constexpr int kWarpStage = 4096 * (kResBufs == 0 ? 1 : kResBufs * kResSlots);
     static constexpr int kEpiBytes = kEpiWarps * kWarpStage;
     static constexpr int kABytes = kBM * kBK * 2;
-    static constexpr int kBBytes = BN * kBK * 2;
+    static constexpr int kBBytes = (PAIR ? BN / 2 : BN) * kBK * 2;
     static constexpr int kStageBytes = kABytes + kBBytes;
     static constexpr int kBarBytes = 512;
     static constexpr int kStagesFit = (kSmemLimit - 1024 - kEpiBytes - kBarBytes) / kStageBytes;
@@ -116,16 +118,24 @@ __device__ __forceinline__ int stage_off(int r, int j)
 
 // F8: E4M3 operands (kind::f8f6f4, 128 elements per 128-byte K block) with the accumulator scaled
 // per output channel by p.wscale before the bias; T is then the BF16 output type.
-template <typename T, int BN, int EPI, bool F8 = false>
-__global__ void __launch_bounds__(GemmCfg<BN, EPI>::kThreads, 1)
+//
+// PAIR: launched as clusters of two CTAs.  The pair computes 256 x BN tiles: CTA rank r stages rows
+// 128 r .. 128 r + 127 of the A tile and rows (BN / 2) r .. of the B tile, its TMA loads count on
+// the even CTA's full barrier, the even CTA issues tcgen05.mma.cta_group::2 (M = 256) and commits
+// to the empty and accumulator-full barriers of both CTAs, and each CTA's epilogue drains its own
+// 128 accumulator rows and arrives on the even CTA's accumulator-empty barrier.
+template <typename T, int BN, int EPI, bool F8 = false, bool PAIR = false>
+__global__ void __launch_bounds__(GemmCfg<BN, EPI, PAIR>::kThreads, 1)
     gemm_sm100_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                       const __grid_constant__ CUtensorMap tmO, const __grid_constant__ CUtensorMap tmR,
                       const __grid_constant__ CUtensorMap tmR2, const GemmParams p)
 {
+    static_assert(!(PAIR && F8), "the pair form is built for 16-bit operands");
     constexpr int kKElems = F8 ? 128 : kBK;  // K elements per 128-byte K block
     // progress waits give up after `lim` cycles; the drains after an abort keep the full limit
     const long long lim = p.wait_limit > 0 ? p.wait_limit : kWaitLimit;
-    using C = GemmCfg<BN, EPI>;
+    using C = GemmCfg<BN, EPI, PAIR>;
+    constexpr int kTileM = PAIR ? 2 * kBM : kBM;
     constexpr int kStages = C::kStages;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem =
@@ -141,10 +151,15 @@ __global__ void __launch_bounds__(GemmCfg<BN, EPI>::kThreads, 1)
 
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
-    const int num_m = (p.M + kBM - 1) / kBM;
+    const int num_m = (p.M + kTileM - 1) / kTileM;
     const int num_n = p.N / BN;
     const int num_tiles = num_m * num_n;
     const int kblocks = p.K / kKElems;
+    // work units: CTAs, or (PAIR) CTA pairs; rank 0 is the pair's MMA issuer
+    const uint32_t rank = PAIR ? cluster_cta_rank() : 0;
+    const int unit = PAIR ? static_cast<int>(blockIdx.x >> 1) : static_cast<int>(blockIdx.x);
+    const int units = PAIR ? static_cast<int>(gridDim.x >> 1) : static_cast<int>(gridDim.x);
+    const int row_off = PAIR ? static_cast<int>(rank) * kBM : 0;  // this CTA's rows in the tile
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < kStages; ++s) {
@@ -153,7 +168,8 @@ __global__ void __launch_bounds__(GemmCfg<BN, EPI>::kThreads, 1)
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(&tfull[b], 1);
-            mbar_init(&tempty[b], C::kEpiWarps);
+            // PAIR: both CTAs' epilogue warps release the even CTA's accumulator
+            mbar_init(&tempty[b], PAIR ? 2 * C::kEpiWarps : C::kEpiWarps);
         }
         mbar_init(drain, 1);
         for (int w = 0; w < 2 * C::kEpiWarps; ++w) {
@@ -167,11 +183,19 @@ __global__ void __launch_bounds__(GemmCfg<BN, EPI>::kThreads, 1)
         tma_prefetch_desc(&tmB);
     }
     if (warp == 1) {
-        tmem_alloc(tmem_slot, C::kTmemCols);
-        tmem_relinquish();
+        if constexpr (PAIR) {
+            tmem_alloc_pair(tmem_slot, C::kTmemCols);
+            tmem_relinquish_pair();
+        } else {
+            tmem_alloc(tmem_slot, C::kTmemCols);
+            tmem_relinquish();
+        }
     }
     tc_fence_before();
     __syncthreads();
+    if constexpr (PAIR) {
+        cluster_sync();  // the peer's barriers are initialised before any copy or arrive reaches them
+    }
     tc_fence_after();
     const uint32_t tmem_base = *tmem_slot;
     // setup above overlaps the predecessor's tail; its outputs are read only after this
@@ -184,8 +208,8 @@ __global__ void __launch_bounds__(GemmCfg<BN, EPI>::kThreads, 1)
             int stage = 0;
             uint32_t phase = 0;
             int issued = 0;
-            for (int tile = blockIdx.x; tile < num_tiles && !*abort_flag; tile += gridDim.x) {
-                const int m0 = (tile % num_m) * kBM;
+            for (int tile = unit; tile < num_tiles && !*abort_flag; tile += units) {
+                const int m0 = (tile % num_m) * kTileM + row_off;
                 const int n0 = (tile / num_m) * BN;
                 for (int kb = 0; kb < kblocks; ++kb) {
                     if (!mbar_wait_bounded(&empty[stage], phase ^ 1, lim)) {
@@ -193,10 +217,21 @@ __global__ void __launch_bounds__(GemmCfg<BN, EPI>::kThreads, 1)
                         report_error(p.err, kErrGemmProducerTimeout);
                         break;
                     }
-                    mbar_arrive_expect_tx(&full[stage], C::kStageBytes);
                     uint8_t* sa = smem + stage * C::kStageBytes;
-                    tma_load_2d(sa, &tmA, &full[stage], kb * kKElems, m0);
-                    tma_load_2d(sa + C::kABytes, &tmB, &full[stage], kb * kKElems, n0);
+                    if constexpr (PAIR) {
+                        // the even CTA's barrier counts both CTAs' bytes
+                        if (rank == 0) {
+                            mbar_arrive_expect_tx(&full[stage], 2 * C::kStageBytes);
+                        }
+                        const uint32_t fb = cluster_map(&full[stage], 0);
+                        tma_load_2d_pair(sa, &tmA, fb, kb * kKElems, m0);
+                        tma_load_2d_pair(sa + C::kABytes, &tmB, fb, kb * kKElems,
+                                         n0 + static_cast<int>(rank) * (BN / 2));
+                    } else {
+                        mbar_arrive_expect_tx(&full[stage], C::kStageBytes);
+                        tma_load_2d(sa, &tmA, &full[stage], kb * kKElems, m0);
+                        tma_load_2d(sa + C::kABytes, &tmB, &full[stage], kb * kKElems, n0);
+                    }
                     ++issued;
                     if (++stage == kStages) {
                         stage = 0;
@@ -204,8 +239,9 @@ __global__ void __launch_bounds__(GemmCfg<BN, EPI>::kThreads, 1)
                     }
                 }
             }
-            if (*abort_flag) {
-                // Let the copies this thread issued land before the CTA winds down.
+            if (*abort_flag && (!PAIR || rank == 0)) {
+                // Let the copies this thread issued land before the CTA winds down (PAIR: the
+                // even CTA's barriers count the peer's copies too).
                 int n = issued < kStages ? issued : kStages;
                 for (int i = 0; i < n; ++i) {
                     if (--stage < 0) {
@@ -218,15 +254,15 @@ __global__ void __launch_bounds__(GemmCfg<BN, EPI>::kThreads, 1)
         }
     } else if (warp == 1) {
         // ------------------------------------------------------------ MMA issuer
-        if (lane == 0) {
+        if (lane == 0 && (!PAIR || rank == 0)) {
             // format 0 is F16 for kind::f16 and E4M3 for kind::f8f6f4
-            const uint32_t idesc = make_idesc_f16(kBM, BN, F8 ? 0 : Pack2<T>::kFormat);
+            const uint32_t idesc = make_idesc_f16(kTileM, BN, F8 ? 0 : Pack2<T>::kFormat);
             int stage = 0;
             uint32_t phase = 0;
             int acc = 0;
             uint32_t acc_phase = 0;
             bool issued_any = false;
-            for (int tile = blockIdx.x; tile < num_tiles && !*abort_flag; tile += gridDim.x) {
+            for (int tile = unit; tile < num_tiles && !*abort_flag; tile += units) {
                 if (!mbar_wait_bounded(&tempty[acc], acc_phase ^ 1, lim)) {
                     *abort_flag = 1;
                     report_error(p.err, kErrGemmMmaTimeout);
@@ -250,12 +286,18 @@ __global__ void __launch_bounds__(GemmCfg<BN, EPI>::kThreads, 1)
                         // 16 B): K = 16 16-bit or K = 32 8-bit elements
                         if constexpr (F8) {
                             tc_mma_f8(d, adesc + 2 * k, bdesc + 2 * k, idesc, (kb | k) != 0 ? 1u : 0u);
+                        } else if constexpr (PAIR) {
+                            tc_mma_f16_pair(d, adesc + 2 * k, bdesc + 2 * k, idesc, (kb | k) != 0 ? 1u : 0u);
                         } else {
                             tc_mma_f16(d, adesc + 2 * k, bdesc + 2 * k, idesc, (kb | k) != 0 ? 1u : 0u);
                         }
                     }
                     issued_any = true;
-                    tc_commit(&empty[stage]);
+                    if constexpr (PAIR) {
+                        tc_commit_pair_both(&empty[stage]);  // frees the stage in both CTAs
+                    } else {
+                        tc_commit(&empty[stage]);
+                    }
                     if (++stage == kStages) {
                         stage = 0;
                         phase ^= 1;
@@ -264,7 +306,11 @@ __global__ void __launch_bounds__(GemmCfg<BN, EPI>::kThreads, 1)
                 if (*abort_flag) {
                     break;
                 }
-                tc_commit(&tfull[acc]);
+                if constexpr (PAIR) {
+                    tc_commit_pair_both(&tfull[acc]);
+                } else {
+                    tc_commit(&tfull[acc]);
+                }
                 acc ^= 1;
                 if (acc == 0) {
                     acc_phase ^= 1;
@@ -272,7 +318,11 @@ __global__ void __launch_bounds__(GemmCfg<BN, EPI>::kThreads, 1)
             }
             if (*abort_flag && issued_any) {
                 // Drain this thread's outstanding MMAs before the columns are released.
-                tc_commit(drain);
+                if constexpr (PAIR) {
+                    tc_commit_pair_local(drain);
+                } else {
+                    tc_commit(drain);
+                }
                 mbar_wait_bounded(drain, 0, kWaitLimit / 16);
             }
         }
@@ -296,11 +346,11 @@ __global__ void __launch_bounds__(GemmCfg<BN, EPI>::kThreads, 1)
         // Issues the residual load of box `b` of this CTA's `k`-th tile into ring slot `s`
         // (lane 0; nothing for tiles past the end or rows past M).
         auto issue_res = [&](int k, int b, int s) {
-            const int t = blockIdx.x + k * gridDim.x;
+            const int t = unit + k * units;
             if (t >= num_tiles) {
                 return;
             }
-            const int r0 = (t % num_m) * kBM + quad * 32;
+            const int r0 = (t % num_m) * kTileM + row_off + quad * 32;
             if (r0 >= p.M) {
                 return;
             }
@@ -320,8 +370,8 @@ __global__ void __launch_bounds__(GemmCfg<BN, EPI>::kThreads, 1)
             }
         }
         int item = 0;  // (tile, box) sequence number of this warp
-        for (int tile = blockIdx.x, k = 0; tile < num_tiles && !*abort_flag; tile += gridDim.x, ++k) {
-            const int m0 = (tile % num_m) * kBM;
+        for (int tile = unit, k = 0; tile < num_tiles && !*abort_flag; tile += units, ++k) {
+            const int m0 = (tile % num_m) * kTileM + row_off;
             const int n0 = (tile / num_m) * BN;
             const int row0 = m0 + quad * 32;        // first row owned by this warp
             const bool rows_live = row0 < p.M;
@@ -527,7 +577,11 @@ __global__ void __launch_bounds__(GemmCfg<BN, EPI>::kThreads, 1)
             tc_fence_before();
             __syncwarp();
             if (lane == 0) {
-                mbar_arrive(&tempty[acc]);
+                if (PAIR && rank != 0) {
+                    mbar_arrive_remote(cluster_map(&tempty[acc], 0));  // the even CTA's barrier
+                } else {
+                    mbar_arrive(&tempty[acc]);
+                }
             }
             acc ^= 1;
             if (acc == 0) {
@@ -554,9 +608,17 @@ __global__ void __launch_bounds__(GemmCfg<BN, EPI>::kThreads, 1)
 
     tc_fence_before();
     __syncthreads();
+    if constexpr (PAIR) {
+        // both CTAs are done with the pair's accumulators and with each other's barriers
+        cluster_sync();
+    }
     if (warp == 1) {
         tc_fence_after();
-        tmem_dealloc(tmem_base, C::kTmemCols);
+        if constexpr (PAIR) {
+            tmem_dealloc_pair(tmem_base, C::kTmemCols);
+        } else {
+            tmem_dealloc(tmem_base, C::kTmemCols);
+        }
     }
 }
 
@@ -564,11 +626,11 @@ struct Maps {
     CUtensorMap a, b, o, r, r2;
 };
 
-template <typename T, int BN, int EPI, bool F8 = false>
+template <typename T, int BN, int EPI, bool F8 = false, bool PAIR = false>
 cudaError_t launch_one(const Maps& m, const GemmParams& p, cudaStream_t stream)
 {
-    using C = GemmCfg<BN, EPI>;
-    auto kernel = gemm_sm100_kernel<T, BN, EPI, F8>;
+    using C = GemmCfg<BN, EPI, PAIR>;
+    auto kernel = gemm_sm100_kernel<T, BN, EPI, F8, PAIR>;
     static std::once_flag once;
     static cudaError_t attr_err = cudaSuccess;
     std::call_once(once, [&] {
@@ -577,9 +639,18 @@ cudaError_t launch_one(const Maps& m, const GemmParams& p, cudaStream_t stream)
     if (attr_err != cudaSuccess) {
         return attr_err;
     }
-    const int num_tiles = ((p.M + kBM - 1) / kBM) * (p.N / BN);
-    const int grid = num_tiles < num_sms() ? num_tiles : num_sms();
-    return launch_pdl(kernel, dim3(grid), dim3(C::kThreads), C::kBytes, stream, m.a, m.b, m.o, m.r, m.r2, p);
+    if constexpr (PAIR) {
+        // one cluster of two CTAs per pair of SMs, at most one per 256-row tile
+        const int num_tiles = ((p.M + 2 * kBM - 1) / (2 * kBM)) * (p.N / BN);
+        int pairs = num_sms() / 2;
+        pairs = num_tiles < pairs ? num_tiles : pairs;
+        return launch_pdl_cluster(kernel, dim3(2 * pairs), dim3(C::kThreads), C::kBytes, stream, 2, m.a, m.b, m.o,
+                                  m.r, m.r2, p);
+    } else {
+        const int num_tiles = ((p.M + kBM - 1) / kBM) * (p.N / BN);
+        const int grid = num_tiles < num_sms() ? num_tiles : num_sms();
+        return launch_pdl(kernel, dim3(grid), dim3(C::kThreads), C::kBytes, stream, m.a, m.b, m.o, m.r, m.r2, p);
+    }
 }
 
 template <typename T, int BN>
@@ -625,7 +696,10 @@ int gemm_tuned_bn(int dtype, int epi, int M, int N, int K, int sub_w);
 namespace {
 std::atomic<int> g_stream_form{1};
 std::atomic<int> g_dw_fusion{0};
+std::atomic<int> g_pair_form{0};
 }  // namespace
+
+void gemm_set_pair_form(bool on) { g_pair_form.store(on ? 1 : 0); }
 
 void gemm_set_stream_form(int form) { g_stream_form.store(form < 0 ? 0 : (form > 2 ? 2 : form)); }
 bool gemm_stream_form_enabled() { return g_stream_form.load(std::memory_order_relaxed) != 0; }
@@ -644,6 +718,9 @@ int gemm_pick_bn(int M, int N, int epi, int sub_cout, int K)
         return kBlockNStream;
     }
     if (epi == kEpiQuad) {
+        if (N % 256 == 0 && g_pair_form.load(std::memory_order_relaxed) != 0 && num_sms() >= 2) {
+            return kBlockNPair;
+        }
         return N % 256 == 0 ? 256 : 0;  // the quad epilogue sums groups of 4 over BN/2 columns
     }
     int lim = (epi == kEpiSubpel) ? sub_cout : N;
@@ -714,6 +791,9 @@ cudaError_t gemm_sm100(int dtype, const void* A, int lda, const void* W, const G
         bn = gemm_tuned_bn(dtype, epi, p.M, p.N, p.K, epi == kEpiSubpel ? p.sub_w : 0);
         if (bn == 0) {
             bn = gemm_pick_bn(p.M, p.N, epi, p.sub_cout, p.K);
+            if (bn == kBlockNPair && f8) {
+                bn = 256;  // the pair form is built for 16-bit operands
+            }
         }
     }
     if (bn == kBlockNStream) {
@@ -722,6 +802,13 @@ cudaError_t gemm_sm100(int dtype, const void* A, int lda, const void* W, const G
     if (p.out8 != nullptr || p.dw_weight != nullptr) {
         // the E4M3 side output and the depthwise operand exist in the streaming form only
         return cudaErrorInvalidValue;
+    }
+    const bool pair = bn == kBlockNPair;
+    if (pair) {
+        if (f8 || (epi != kEpiBias && epi != kEpiBiasWsilu && epi != kEpiQuad) || num_sms() < 2) {
+            return cudaErrorInvalidValue;
+        }
+        bn = 256;
     }
     if (bn <= 0 || p.N % bn != 0) {
         return cudaErrorInvalidValue;
@@ -756,7 +843,7 @@ cudaError_t gemm_sm100(int dtype, const void* A, int lda, const void* W, const G
     Maps m;
     std::memset(&m, 0, sizeof(m));
     if (!make_tmap_2d(&m.a, dop, A, p.K, p.M, static_cast<uint64_t>(lda) * esz, kbox, kBM, 128) ||
-        !make_tmap_2d(&m.b, dop, W, p.K, p.N, static_cast<uint64_t>(p.K) * esz, kbox, bn, 128)) {
+        !make_tmap_2d(&m.b, dop, W, p.K, p.N, static_cast<uint64_t>(p.K) * esz, kbox, pair ? bn / 2 : bn, 128)) {
         return cudaErrorInvalidValue;
     }
     if (epi != kEpiSubpel) {
@@ -775,6 +862,20 @@ cudaError_t gemm_sm100(int dtype, const void* A, int lda, const void* W, const G
             !make_tmap_2d(&m.r2, dt, p.res2, p.N, p.M, static_cast<uint64_t>(p.ldr2) * 2, ow, 32, sw)) {
             return cudaErrorInvalidValue;
         }
+    }
+    if (pair) {
+        switch (epi) {
+        case kEpiBias:
+            return dtype == 0 ? launch_one<__half, 256, kEpiBias, false, true>(m, p, stream)
+                              : launch_one<__nv_bfloat16, 256, kEpiBias, false, true>(m, p, stream);
+        case kEpiBiasWsilu:
+            return dtype == 0 ? launch_one<__half, 256, kEpiBiasWsilu, false, true>(m, p, stream)
+                              : launch_one<__nv_bfloat16, 256, kEpiBiasWsilu, false, true>(m, p, stream);
+        case kEpiQuad:
+            return dtype == 0 ? launch_one<__half, 256, kEpiQuad, false, true>(m, p, stream)
+                              : launch_one<__nv_bfloat16, 256, kEpiQuad, false, true>(m, p, stream);
+        }
+        return cudaErrorInvalidValue;
     }
     if (f8) {
         switch (bn) {

@@ -32,6 +32,9 @@ enum GemmEpilogue : int {
 // block_n value selecting the streaming form of the residual epilogues (gemm_stream_sm100.cu):
 // 128-wide channel slices with W resident in shared memory, contiguous row ranges per CTA.
 constexpr int kBlockNStream = -1;
+// block_n value selecting the CTA-pair form (cta_group::2, 256 x 256 tiles over two SMs, each
+// staging half of the W tile) of the bias, WSiLU and quad epilogues with 16-bit operands.
+constexpr int kBlockNPair = -2;
 
 struct GemmParams {
     int M, N, K;
@@ -93,6 +96,8 @@ bool gemm_stream_form_enabled();
 // Whether the codecs compute the depthwise 3x3 inside the streaming residual GEMM (default off:
 // measured slower than the two launches, see the kernel file).
 void gemm_set_dw_fusion(bool on);
+// Whether the library's own choice gives the quad GEMM the CTA-pair form (default off).
+void gemm_set_pair_form(bool on);
 bool gemm_dw_fusion_enabled();
 cudaError_t gemm_stream_sm100(int dtype, const void* A, int lda, const void* W, const GemmParams& p,
                               int epi, cudaStream_t stream);

@@ -610,8 +610,57 @@ void HtsCodec::record_phase(int slot, Launch& L)
 
 int HtsCodec::run_phase(int slot, cudaStream_t s)
 {
-    return graphs_.run(slot, s, err_word_, [&](Launch& L) { record_phase(slot, L); },
-                       &last_kernels_);
+    static const char* const kNames[kPhaseSlots] = {"hts enc_analysis", "hts enc_update", "hts enc_update reset",
+                                                    "hts dec_temporal", "hts dec_temporal memory", "hts dec_hyper",
+                                                    "hts dec_context", "hts dec_synthesis"};
+    NvtxRange range(kNames[slot]);
+    if (timing_) {
+        cudaEventRecord(tev_[slot][0], s);
+    }
+    const int st = graphs_.run(slot, s, err_word_, [&](Launch& L) { record_phase(slot, L); }, &last_kernels_);
+    if (timing_) {
+        cudaEventRecord(tev_[slot][1], s);
+        tev_used_[slot] = true;
+    }
+    return st;
+}
+
+void HtsCodec::set_timing(bool on)
+{
+    cudaSetDevice(dev_);
+    if (on && tev_[0][0] == nullptr) {
+        for (auto& e : tev_) {
+            cudaEventCreate(&e[0]);
+            cudaEventCreate(&e[1]);
+        }
+    }
+    timing_ = on && tev_[0][0] != nullptr;
+}
+
+int HtsCodec::timing(float* out, int cap)
+{
+    if (out == nullptr || cap <= 0) {
+        return 0;
+    }
+    float v[kTimingValues];
+    for (int i = 0; i < kPhaseSlots; ++i) {
+        v[i] = -1.f;
+        if (timing_ && tev_used_[i] && cudaEventSynchronize(tev_[i][1]) == cudaSuccess) {
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, tev_[i][0], tev_[i][1]) == cudaSuccess) {
+                v[i] = ms;
+            }
+        }
+    }
+    cudaGetLastError();
+    for (int i = 0; i < 5; ++i) {
+        v[kPhaseSlots + i] = host_ms_[i];
+    }
+    const int n = cap < kTimingValues ? cap : kTimingValues;
+    for (int i = 0; i < n; ++i) {
+        out[i] = v[i];
+    }
+    return n;
 }
 
 int HtsCodec::buffer(const std::string& name, const void** ptr, int* rows, int* cols,
@@ -875,6 +924,7 @@ int HtsCodec::compress_batch(const __half* const* xs, int n, int H, int W, const
         return kInvalidArgument;
     }
     last_kernels_ = 0;
+    begin_timing();
     cudaEventRecord(ev_in_, caller);
     cudaStreamWaitEvent(main_, ev_in_, 0);
     set_qp(qps, main_);
@@ -894,9 +944,13 @@ int HtsCodec::compress_batch(const __half* const* xs, int n, int H, int W, const
         return st;
     }
     // symbols to the host while enc_update runs (worker, dmc_hts_proxy.cpp:778-793)
+    const auto t_wait = Clock::now();
     if (cudaEventSynchronize(ev_phase_) != cudaSuccess) {
         return cuda_status(cudaGetLastError(), "compress: analysis");
     }
+    const auto t_rans = Clock::now();
+    host_ms_[0] = ms_between(t_wait, t_rans);
+    NvtxRange range("hts rANS encode");
     st = check_device_error_word(err_word_, err_slot_, "compress");
     if (st != kOk) {
         return st;
@@ -919,6 +973,7 @@ int HtsCodec::compress_batch(const __half* const* xs, int n, int H, int W, const
         good[k] = enc.finish(tables_, &bytes[k], &errs[k]) ? 1 : 0;
         ec_parallel[k] = ecp;
     });
+    host_ms_[1] = ms_between(t_rans, Clock::now());
     last_count_ = 0;
     for (int k = 0; k < n; ++k) {
         if (!good[k]) {
@@ -958,15 +1013,18 @@ int HtsCodec::decompress_batch(const uint8_t* const* bytes, const size_t* sizes,
         return kInvalidArgument;
     }
     last_kernels_ = 0;
+    begin_timing();
     cudaEventRecord(ev_in_, caller);
     cudaStreamWaitEvent(main_, ev_in_, 0);
     set_qp(qps, main_);
     int st = run_phase(kDecTemporal + (memory_has_value_ ? 1 : 0), main_);
+    auto t0 = Clock::now();
     // z on the CPU while the temporal branch runs (dmc_hts_proxy.cpp:794-804)
     std::vector<RansDecoderSession> dec(n);
     std::vector<std::string> errs(n);
     std::vector<int> res(n, kOk);
     if (st == kOk) {
+        NvtxRange range("hts rANS decode z");
         for_each_stream(n, [&](int k) {
             if (!dec[k].begin(bytes[k], static_cast<int>(sizes[k]), ecps[k], &errs[k]) ||
                 !dec[k].decode_z(tables_, nz_, qps[k] * kChZ, kChZ,
@@ -981,16 +1039,20 @@ int HtsCodec::decompress_batch(const uint8_t* const* bytes, const size_t* sizes,
             }
         }
     }
+    host_ms_[2] = ms_between(t0, Clock::now());
     if (st == kOk) {
         st = run_phase(kDecHyper, main_);
     }
     if (st == kOk) st = cuda_status(cudaEventRecord(ev_phase_, main_), "decompress");
     if (st == kOk) st = run_phase(kDecContext, main_);
+    t0 = Clock::now();
     if (st == kOk) {
         if (cudaEventSynchronize(ev_phase_) != cudaSuccess) {
             st = cuda_status(cudaGetLastError(), "decompress: hyper prior");
         }
     }
+    host_ms_[3] = ms_between(t0, Clock::now());
+    t0 = Clock::now();
     if (st == kOk) st = check_device_error_word(err_word_, err_slot_, "decompress");
     for (int k = 0; k < n && st == kOk; ++k) {
         if (count_host_[k] < 0 || count_host_[k] > ny_) {
@@ -1000,6 +1062,7 @@ int HtsCodec::decompress_batch(const uint8_t* const* bytes, const size_t* sizes,
     }
     // y on the CPU while the feature extractor runs (dmc_hts_proxy.cpp:805-823)
     if (st == kOk) {
+        NvtxRange range("hts rANS decode y");
         for_each_stream(n, [&](int k) {
             const size_t o = static_cast<size_t>(k) * ny_;
             if (!dec[k].decode_y(tables_, idx_host_ + o, count_host_[k], ydec_host_ + o, &errs[k])) {
@@ -1013,6 +1076,7 @@ int HtsCodec::decompress_batch(const uint8_t* const* bytes, const size_t* sizes,
             }
         }
     }
+    host_ms_[4] = ms_between(t0, Clock::now());
     if (st == kOk) {
         st = run_phase(kDecSynthesis, main_);
     }

@@ -98,6 +98,22 @@ public:
     size_t activation_bytes() const { return acts_.bytes(); }
     // Number of kernels the last compress/decompress enqueued (graph nodes included).
     int last_kernel_count() const { return last_kernels_; }
+    // Phase timing of the following calls (off by default): CUDA events around every phase graph
+    // and host clocks around the host's waits and entropy coding.  timing() fills up to `cap`
+    // values (milliseconds; -1 for a phase the last compress / decompress did not run) in the
+    // order of kTimingNames and returns how many it wrote.
+    void set_timing(bool on);
+    int timing(float* out, int cap);
+    static constexpr int kTimingValues = 13;
+    void begin_timing()
+    {
+        for (bool& u : tev_used_) {
+            u = false;
+        }
+        for (float& h : host_ms_) {
+            h = -1.f;
+        }
+    }
 
 private:
     enum Phase {
@@ -215,6 +231,11 @@ private:
     cudaStream_t main_ = nullptr;   // compute stream (graphs run here)
     cudaEvent_t ev_in_ = nullptr, ev_phase_ = nullptr, ev_out_ = nullptr;
     cudaEvent_t ev_state_ = nullptr;  // state copies on a caller's stream, waited for by main_
+    // phase timing (set_timing): events before / after each phase slot, host intervals
+    bool timing_ = false;
+    cudaEvent_t tev_[8][2] = {};
+    bool tev_used_[8] = {};
+    float host_ms_[5] = {-1.f, -1.f, -1.f, -1.f, -1.f};
     int* err_word_ = nullptr;
     ErrorSlot err_slot_;  // the error word as the phase graphs publish it
     int last_count_ = 0;

@@ -59,6 +59,8 @@ _proto("dcvc_hts_state_bytes", [_vp, ctypes.POINTER(ctypes.c_size_t)])
 _proto("dcvc_hts_export_state", [_vp, _vp, _vp, ctypes.POINTER(ctypes.c_int)])
 _proto("dcvc_hts_import_state", [_vp, _vp, ctypes.c_int, _vp])
 _proto("dcvc_hts_buffer_dtype", [_vp, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int)])
+_proto("dcvc_hts_set_timing", [_vp, ctypes.c_int])
+_proto("dcvc_hts_timing", [_vp, ctypes.POINTER(ctypes.c_float), ctypes.c_int, ctypes.POINTER(ctypes.c_int)])
 _proto("dcvc_intra_create", [ctypes.POINTER(_vp)])
 _proto("dcvc_intra_destroy", [_vp])
 _proto("dcvc_intra_set_param", [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_char_p),
@@ -202,6 +204,24 @@ class DMCHTSProxy(_Proxy):
         self.precision = precision
 
     # ---- packed batches: n streams of one resolution per call (HT-S only; an extension)
+    TIMING_NAMES = ("enc_analysis", "enc_update", "enc_update_reset", "dec_temporal",
+                    "dec_temporal_memory", "dec_hyper", "dec_context", "dec_synthesis",
+                    "host_wait_analysis", "host_rans_encode", "host_decode_z", "host_wait_hyper",
+                    "host_decode_y")
+
+    def set_timing(self, enable=True):
+        """Times the phase graphs (CUDA events) and the host's waits and entropy coding of the
+        following calls; timing() returns the last call's values in milliseconds."""
+        N.check(_lib.dcvc_hts_set_timing(self._h, 1 if enable else 0), "set_timing")
+
+    def timing(self):
+        """{name: ms} for the parts the last compress / decompress ran."""
+        out = (ctypes.c_float * len(self.TIMING_NAMES))()
+        n = ctypes.c_int()
+        N.check(_lib.dcvc_hts_timing(self._h, out, len(out), ctypes.byref(n)), "timing")
+        return {k: round(float(out[i]), 4) for i, k in enumerate(self.TIMING_NAMES[:n.value])
+                if out[i] >= 0}
+
     def add_ref_features_from_frames(self, frames, apply_adaptor=True):
         """Seeds n streams (and sizes the codec for them) from n [1, 3, Hp, Wp] float16 frames."""
         self._hts_only("add_ref_features_from_frames")

@@ -48,6 +48,9 @@ extern "C" {
 
 /* block_n of dcvc_conv1x1 selecting the streaming form of the residual epilogues */
 #define DCVC_BLOCK_N_STREAM (-1)
+/* block_n of dcvc_conv1x1 selecting the CTA-pair form of the bias, WSiLU and quad epilogues
+ * (cta_group::2: two SMs share each 256 x 256 tile, each staging half of its W rows; 16-bit) */
+#define DCVC_BLOCK_N_PAIR (-2)
 
 /* 1x1-conv GEMM epilogues (dcvc_conv1x1) */
 #define DCVC_EPI_BIAS 0        /* conv1x1_bias                       */
@@ -104,6 +107,9 @@ int dcvc_conv1x1(int dtype, int epilogue, int M, int N, int K, const void* a, in
  * the bias and WSiLU epilogues at K <= 512.  Output bits are the same either way.  No counterpart
  * in the reference. */
 int dcvc_gemm_stream_form(int enable);
+/* Whether the library's own tile choice (and the codecs) gives the quad GEMM the CTA-pair form
+ * (DCVC_BLOCK_N_PAIR): 1 or 0 (the default).  No counterpart in the reference. */
+int dcvc_gemm_pair_form(int enable);
 /* The FP8 form of dcvc_conv1x1 for the epilogues BIAS, BIAS_WSILU and QUAD: a [M, K] and
  * w [N, K] are E4M3 bytes (lda a multiple of 16, K of 128), the tcgen05 MMA is kind::f8f6f4
  * with FP32 accumulation, and the epilogue computes acc * wscale[n] + bias[n] (wscale: FP32
@@ -388,6 +394,15 @@ int dcvc_hts_buffer(void* handle, const char* name, const void** ptr, int* rows,
                     int* ld);
 /* symbols coded by the last call, kernels it enqueued, device bytes held by the handle */
 int dcvc_hts_stats(void* handle, int* symbols, int* kernels, size_t* device_bytes);
+/* Phase timing (off by default; enabling it adds two events per phase graph).  After a call,
+ * dcvc_hts_timing writes up to `cap` values in milliseconds, -1 for a part the last call did not
+ * run, and their number to *count: the device time of the phase graphs enc_analysis, enc_update,
+ * enc_update (reset), dec_temporal, dec_temporal (memory), dec_hyper, dec_context,
+ * dec_synthesis, then the host's time waiting for enc_analysis, rANS-encoding, decoding z,
+ * waiting for dec_hyper and decoding y.  Every phase graph and host coding step is also an NVTX
+ * range.  No counterpart in the reference. */
+int dcvc_hts_set_timing(void* handle, int enable);
+int dcvc_hts_timing(void* handle, float* out, int cap, int* count);
 /* Precision form of the analysis and synthesis transforms (encoder, decoder, recon head, feature
  * adaptors and extractor): DCVC_PRECISION_F16 (the reference's form, the default) or
  * DCVC_PRECISION_BF16 (BF16 activations and weights, FP32 accumulation) or DCVC_PRECISION_FP8 (the

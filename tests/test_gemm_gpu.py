@@ -287,3 +287,65 @@ def test_depthwise_form_bounded_wait_runs_out():
     t = ops.dwconv3x3_ex(x, H, W, dw)
     ref = ops.conv1x1(t, w, b, N.EPI_BIAS_RES, res=res, block_n=N.BLOCK_N_STREAM)
     assert torch.equal(out.view(torch.int16), ref.view(torch.int16))
+
+
+PAIR_CASES = [
+    # (epilogue name, M, N, K, dtype): the quad GEMM at 1080p and at a ragged M (the last 256-row
+    # tile half empty), dc.0 at the y level, a small bias GEMM, BF16
+    ("EPI_QUAD", 32640, 1024, 512, torch.float16),
+    ("EPI_QUAD", 3000, 1024, 256, torch.float16),
+    ("EPI_BIAS_WSILU", 8160, 256, 512, torch.float16),
+    ("EPI_BIAS", 777, 512, 128, torch.float16),
+    ("EPI_QUAD", 8160, 1024, 512, torch.bfloat16),
+]
+
+
+@pytest.mark.parametrize("name,M,Nn,K,dtype", PAIR_CASES)
+def test_pair_form_matches_tiled(name, M, Nn, K, dtype):
+    """The CTA-pair form (cta_group::2: 256 x 256 tiles over two SMs, each staging half of W)
+    against the one-SM tiled kernel and the fp32 reference.  The products are summed in the same
+    K order; whether the tensor cores round M = 256 tiles exactly as M = 128 tiles is printed."""
+    from dcvc_b200 import _native as N, ops
+    epi = getattr(N, name)
+    g = torch.Generator(device="cuda").manual_seed(M + Nn + K + 1)
+    a = torch.randn(M, K, device="cuda", generator=g).to(dtype)
+    w = (torch.randn(Nn, K, device="cuda", generator=g) / K ** 0.5).to(dtype)
+    b = torch.randn(Nn, device="cuda", generator=g) * 0.1
+    nout = Nn // 4 if epi == N.EPI_QUAD else Nn
+    tiled = ops.conv1x1(a, w, b, epi, block_n=256)
+    obuf = torch.full((M, nout + 64), 7.0, device="cuda", dtype=dtype)
+    pair = ops.conv1x1(a, w, b, epi, out=obuf[:, 64:], block_n=N.BLOCK_N_PAIR)
+    torch.cuda.synchronize()
+    assert N.device_error() == 0
+    assert bool((obuf[:, :64] == 7.0).all())
+    same = torch.equal(pair.view(torch.int16), tiled.view(torch.int16))
+    print(f"pair form {name} {M}x{Nn}x{K} {dtype}: bitwise equal to the tiled kernel: {same}, "
+          f"max |diff| {float((pair.float() - tiled.float()).abs().max()):.3e}")
+    ref = _ref(epi, a, w, b)
+    atol, rtol = TOL[dtype]
+    assert bool(((pair.float() - ref).abs() <= atol + rtol * ref.abs()).all())
+
+
+def test_pair_form_bounded_wait_runs_out():
+    """Under the stall injection neither CTA of a pair loads anything: the even CTA's MMA wait and
+    the odd CTA's epilogue wait run out, the launch reports DCVC_DEVICE_TIMEOUT, both CTAs meet at
+    the final cluster barrier, and the next launch is right."""
+    import ctypes
+    from dcvc_b200 import _native as N, ops
+    lib = N.lib
+    lib.dcvc_gemm_inject_stall.argtypes = [ctypes.c_int, ctypes.c_longlong]
+    lib.dcvc_check_device_errors.argtypes = [ctypes.c_void_p]
+    g = torch.Generator(device="cuda").manual_seed(21)
+    M, Nn, K = 4096, 1024, 256
+    a = torch.randn(M, K, device="cuda", generator=g).half()
+    w = (torch.randn(Nn, K, device="cuda", generator=g) / K ** 0.5).half()
+    b = torch.randn(Nn, device="cuda", generator=g) * 0.1
+    stream = torch.cuda.current_stream().cuda_stream
+    assert lib.dcvc_check_device_errors(stream) == 0
+    assert lib.dcvc_gemm_inject_stall(1, 20000) == 0
+    ops.conv1x1(a, w, b, N.EPI_QUAD, block_n=N.BLOCK_N_PAIR)
+    assert lib.dcvc_check_device_errors(stream) == 3  # DCVC_DEVICE_TIMEOUT
+    out = ops.conv1x1(a, w, b, N.EPI_QUAD, block_n=N.BLOCK_N_PAIR)
+    assert lib.dcvc_check_device_errors(stream) == 0
+    ref = _ref(N.EPI_QUAD, a, w, b)
+    assert bool(((out.float() - ref).abs() <= 2e-2 + 1e-2 * ref.abs()).all())
