@@ -96,7 +96,11 @@ def _case(name, g, bn=0):
               "tiny": (128, 256, 64, N.EPI_BIAS), "res_quarter": (M8 // 4, 512, 256, N.EPI_BIAS_RES),
               # the y-level (M / 4) dc.0 and quad GEMMs of a 512-channel block
               "wsilu_quarter": (M8 // 4, 256, 512, N.EPI_BIAS_WSILU),
-              "quad_quarter": (M8 // 4, 1024, 512, N.EPI_QUAD)}
+              "quad_quarter": (M8 // 4, 1024, 512, N.EPI_QUAD),
+              # the recon head's 256-channel blocks (8 frames x 3 per decoded chunk) and the
+              # y-level residual GEMMs at K = 512
+              "wsilu256": (M8, 256, 256, N.EPI_BIAS_WSILU), "res256": (M8, 256, 256, N.EPI_BIAS_RES),
+              "quad256": (M8, 1024, 256, N.EPI_QUAD), "res512y": (M8 // 4, 512, 512, N.EPI_BIAS_RES)}
     M, Nn, K, epi = shapes[name]
     a = rnd(M, K)
     w = rnd(Nn, K, scale=K ** -0.5)
