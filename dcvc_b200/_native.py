@@ -75,6 +75,7 @@ _proto("dcvc_dw3x3_conv1x1_res", c_int, [c_int, c_int, c_int, c_int, c_vp, c_int
                                         c_vp, c_vp, c_int, c_vp, c_int, c_vp])
 _proto("dcvc_dw_fusion", c_int, [c_int])
 _proto("dcvc_gemm_pair_form", c_int, [c_int])
+_proto("dcvc_hts_recon_branches", c_int, [c_int])
 
 
 def device_error(clear=True):

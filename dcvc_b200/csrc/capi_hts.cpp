@@ -234,6 +234,15 @@ int dcvc_hts_import_state(void* handle, const void* src, int flags, void* stream
                                                                static_cast<cudaStream_t>(stream));
 }
 
+int dcvc_hts_recon_branches(int n)
+{
+    if (n != 1 && n != 2) {
+        return fail(kInvalidArgument, "dcvc_hts_recon_branches: 1 or 2");
+    }
+    HtsCodec::set_recon_branches(n);
+    return kOk;
+}
+
 int dcvc_hts_set_timing(void* handle, int enable)
 {
     if (handle == nullptr) {

@@ -60,6 +60,7 @@ _proto("dcvc_hts_export_state", [_vp, _vp, _vp, ctypes.POINTER(ctypes.c_int)])
 _proto("dcvc_hts_import_state", [_vp, _vp, ctypes.c_int, _vp])
 _proto("dcvc_hts_buffer_dtype", [_vp, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int)])
 _proto("dcvc_hts_set_timing", [_vp, ctypes.c_int])
+_proto("dcvc_hts_recon_branches", [ctypes.c_int])
 _proto("dcvc_hts_timing", [_vp, ctypes.POINTER(ctypes.c_float), ctypes.c_int, ctypes.POINTER(ctypes.c_int)])
 _proto("dcvc_intra_create", [ctypes.POINTER(_vp)])
 _proto("dcvc_intra_destroy", [_vp])

@@ -172,3 +172,31 @@ def test_depthwise_fused_into_the_residual_gemm_gives_the_same_codec_outputs(pre
     for (b0, f0), (b1, f1) in zip(out[0], out[1]):
         assert np.array_equal(b0, b1)
         assert all(torch.equal(a, b) for a, b in zip(f0, f1))
+
+
+def test_recon_head_in_two_branches_gives_the_same_frames():
+    """With the decoded chunk's recon head split into two concurrent branches (frames 4..7 on a
+    second stream, their own scratch buffers) the codec gives the same payloads and frames."""
+    from dcvc_b200 import _native as N
+    sd = state_dict()
+    H, W = 128, 192
+    out = {}
+    try:
+        for n in (2, 1):
+            N.lib.dcvc_hts_recon_branches(n)
+            enc, dec = _proxy(sd, "fp16"), _proxy(sd, "fp16")
+            ref = ref_frame(H, W)
+            enc.add_ref_feature_from_frame(ref, True)
+            dec.add_ref_feature_from_frame(ref, False)
+            res = []
+            for k, qp in enumerate((5, 40, 63)):
+                bits, ecp = enc.compress(chunk(H, W, k), qp, k == 2, 0, 0)
+                frames = dec.decompress(bits, qp, H, W, ecp, k == 2)
+                torch.cuda.synchronize()
+                res.append((bits, [f.clone() for f in frames]))
+            out[n] = res
+    finally:
+        N.lib.dcvc_hts_recon_branches(2)
+    for (b0, f0), (b1, f1) in zip(out[1], out[2]):
+        assert np.array_equal(b0, b1)
+        assert all(torch.equal(a, b) for a, b in zip(f0, f1))
