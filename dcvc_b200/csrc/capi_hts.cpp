@@ -236,8 +236,8 @@ int dcvc_hts_import_state(void* handle, const void* src, int flags, void* stream
 
 int dcvc_hts_recon_branches(int n)
 {
-    if (n != 1 && n != 2) {
-        return fail(kInvalidArgument, "dcvc_hts_recon_branches: 1 or 2");
+    if (n != 1 && n != 2 && n != 4) {
+        return fail(kInvalidArgument, "dcvc_hts_recon_branches: 1, 2 or 4");
     }
     HtsCodec::set_recon_branches(n);
     return kOk;

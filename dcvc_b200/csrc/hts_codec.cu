@@ -30,15 +30,17 @@ std::string num(const char* prefix, int i, const char* suffix = ".")
 
 }  // namespace
 
-void HtsCodec::set_recon_branches(int n) { g_recon_branches.store(n == 2 ? 2 : 1); }
+void HtsCodec::set_recon_branches(int n) { g_recon_branches.store((n == 2 || n == 4) ? n : 1); }
 
 HtsCodec::HtsCodec()
 {
     cudaGetDevice(&dev_);
     cudaStreamCreateWithFlags(&main_, cudaStreamNonBlocking);
-    cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking);
     cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming);
-    cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming);
+    for (int b = 0; b < kMaxReconBranches - 1; ++b) {
+        cudaStreamCreateWithFlags(&side_[b], cudaStreamNonBlocking);
+        cudaEventCreateWithFlags(&ev_join_[b], cudaEventDisableTiming);
+    }
     cudaEventCreateWithFlags(&ev_in_, cudaEventDisableTiming);
     cudaEventCreateWithFlags(&ev_phase_, cudaEventDisableTiming);
     cudaEventCreateWithFlags(&ev_out_, cudaEventDisableTiming);
@@ -66,14 +68,16 @@ HtsCodec::~HtsCodec()
     cudaEventDestroy(ev_out_);
     cudaEventDestroy(ev_state_);
     cudaEventDestroy(ev_fork_);
-    cudaEventDestroy(ev_join_);
+    for (int b = 0; b < kMaxReconBranches - 1; ++b) {
+        cudaEventDestroy(ev_join_[b]);
+        cudaStreamDestroy(side_[b]);
+    }
     for (auto& e : tev_) {
         if (e[0] != nullptr) {
             cudaEventDestroy(e[0]);
             cudaEventDestroy(e[1]);
         }
     }
-    cudaStreamDestroy(side_);
     cudaStreamDestroy(main_);
     err_slot_.release();
 }
@@ -304,18 +308,22 @@ int HtsCodec::allocate(int Hp, int Wp, int imgs)
     scratch_.t4 = H(S);
     scratch_.t5 = fp8_ ? acts_.alloc_n<uint8_t>(M8 * kChD) : nullptr;
     ok = ok && (!fp8_ || scratch_.t5 != nullptr);
-    split_recon_ = g_recon_branches.load() == 2;
-    if (split_recon_) {
-        lvl8_a2_ = H(M8 * kChD);
-        lvl8_b2_ = H(M8 * kChD);
-        head2_ = H(M8 * kChSrcIntra);
-        scratch2_.t0 = H(S);
-        scratch2_.t1 = H(S);
-        scratch2_.t2 = H(S);
-        scratch2_.t3 = H(S);
-        scratch2_.t4 = H(S);
-        scratch2_.t5 = fp8_ ? acts_.alloc_n<uint8_t>(M8 * kChD) : nullptr;
-        ok = ok && (!fp8_ || scratch2_.t5 != nullptr);
+    recon_branches_ = g_recon_branches.load();
+    rb_a_[0] = lvl8_a_;
+    rb_b_[0] = lvl8_b_;
+    rb_head_[0] = head_;
+    rb_scratch_[0] = scratch_;
+    for (int b = 1; b < recon_branches_; ++b) {
+        rb_a_[b] = H(M8 * kChD);
+        rb_b_[b] = H(M8 * kChD);
+        rb_head_[b] = H(M8 * kChSrcIntra);
+        rb_scratch_[b].t0 = H(S);
+        rb_scratch_[b].t1 = H(S);
+        rb_scratch_[b].t2 = H(S);
+        rb_scratch_[b].t3 = H(S);
+        rb_scratch_[b].t4 = H(S);
+        rb_scratch_[b].t5 = fp8_ ? acts_.alloc_n<uint8_t>(M8 * kChD) : nullptr;
+        ok = ok && (!fp8_ || rb_scratch_[b].t5 != nullptr);
     }
     z_i8_ = acts_.alloc_n<int8_t>(z_num_);
     sym_ = acts_.alloc_n<int16_t>(y_num_);
@@ -491,21 +499,28 @@ void HtsCodec::recon_head(Launch& L, bool all_frames)
         frames(L, kFrames - 1, kFrames, lvl8_a_, lvl8_b_, head_, scratch_);
         return;
     }
-    if (!split_recon_) {
+    const int nb = recon_branches_;
+    if (nb <= 1) {
         frames(L, 0, kFrames, lvl8_a_, lvl8_b_, head_, scratch_);
         return;
     }
-    // two branches: frames 4..7 on side_ (forked from and joined back into L.s; inside a graph
-    // capture this makes two parallel chains of the graph), frames 0..3 on L.s
+    // nb branches of kFrames / nb frames (a multiple of the 2 frames sharing a common block):
+    // branch b > 0 on side_[b - 1], forked from and joined back into L.s (inside a graph capture
+    // this makes parallel chains of the graph), branch 0 on L.s
+    const int per = kFrames / nb;
     L.note(cudaEventRecord(ev_fork_, L.s), 0);
-    L.note(cudaStreamWaitEvent(side_, ev_fork_, 0), 0);
-    Launch L2{side_, L.err_word};
-    frames(L2, kFrames / 2, kFrames, lvl8_a2_, lvl8_b2_, head2_, scratch2_);
-    frames(L, 0, kFrames / 2, lvl8_a_, lvl8_b_, head_, scratch_);
-    L2.note(cudaEventRecord(ev_join_, side_), 0);
-    L.note(cudaStreamWaitEvent(L.s, ev_join_, 0), 0);
-    L.note(L2.first, 0);
-    L.kernels += L2.kernels;
+    for (int b = 1; b < nb; ++b) {
+        L.note(cudaStreamWaitEvent(side_[b - 1], ev_fork_, 0), 0);
+        Launch Lb{side_[b - 1], L.err_word};
+        frames(Lb, b * per, (b + 1) * per, rb_a_[b], rb_b_[b], rb_head_[b], rb_scratch_[b]);
+        Lb.note(cudaEventRecord(ev_join_[b - 1], side_[b - 1]), 0);
+        L.note(Lb.first, 0);
+        L.kernels += Lb.kernels;
+    }
+    frames(L, 0, per, lvl8_a_, lvl8_b_, head_, scratch_);
+    for (int b = 1; b < nb; ++b) {
+        L.note(cudaStreamWaitEvent(L.s, ev_join_[b - 1], 0), 0);
+    }
 }
 
 // ------------------------------------------------------------------------------ phases

@@ -104,7 +104,7 @@ public:
     // order of kTimingNames and returns how many it wrote.
     void set_timing(bool on);
     // Process-wide: how many concurrent branches codecs allocated after the call give the 8-frame
-    // recon head of a decoded chunk (1 or 2).
+    // recon head of a decoded chunk (1, 2 or 4).
     static void set_recon_branches(int n);
     int timing(float* out, int cap);
     static constexpr int kTimingValues = 13;
@@ -215,11 +215,12 @@ private:
     int* block_counts_ = nullptr;
     int* count_dev_ = nullptr;
     Scratch scratch_;
-    // the second branch of a decoded chunk's recon head (frames 4..7 on side_, concurrently with
-    // frames 0..3 on main_; allocated when the split is enabled at allocation time)
-    bool split_recon_ = false;
-    __half *lvl8_a2_ = nullptr, *lvl8_b2_ = nullptr, *head2_ = nullptr;
-    Scratch scratch2_;
+    // the further branches of a decoded chunk's recon head (branch b > 0 on side_[b - 1] with
+    // its own buffers, concurrently with branch 0 on main_; allocated at allocation time)
+    static constexpr int kMaxReconBranches = 4;
+    int recon_branches_ = 1;
+    __half *rb_a_[kMaxReconBranches] = {}, *rb_b_[kMaxReconBranches] = {}, *rb_head_[kMaxReconBranches] = {};
+    Scratch rb_scratch_[kMaxReconBranches];
     // pinned host staging
     int* count_host_ = nullptr;
     int16_t* sym_host_ = nullptr;
@@ -237,8 +238,8 @@ private:
 
     PhaseGraphs graphs_{kPhaseSlots};
     cudaStream_t main_ = nullptr;   // compute stream (graphs run here)
-    cudaStream_t side_ = nullptr;   // the recon head's second branch (forked from main_)
-    cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
+    cudaStream_t side_[kMaxReconBranches - 1] = {};  // the recon head's further branches
+    cudaEvent_t ev_fork_ = nullptr, ev_join_[kMaxReconBranches - 1] = {};
     cudaEvent_t ev_in_ = nullptr, ev_phase_ = nullptr, ev_out_ = nullptr;
     cudaEvent_t ev_state_ = nullptr;  // state copies on a caller's stream, waited for by main_
     // phase timing (set_timing): events before / after each phase slot, host intervals

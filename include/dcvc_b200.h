@@ -402,11 +402,11 @@ int dcvc_hts_stats(void* handle, int* symbols, int* kernels, size_t* device_byte
  * waiting for dec_hyper and decoding y.  Every phase graph and host coding step is also an NVTX
  * range.  No counterpart in the reference. */
 int dcvc_hts_set_timing(void* handle, int enable);
-/* How many concurrent branches (1, or 2, the default) the 8-frame recon head of a decoded chunk
- * runs in, for HT-S codecs whose resolution is set after the call: with 2, frames 4..7 run on a
- * second stream (a parallel chain of the phase graph) with their own scratch buffers (about 250
- * MB more at 1080p), and a 1080p chunk codes 1.2 % faster.  Outputs are the same either way.  No
- * counterpart in the reference. */
+/* How many concurrent branches (1, 2 -- the default -- or 4) the 8-frame recon head of a decoded
+ * chunk runs in, for HT-S codecs whose resolution is set after the call: with 2, frames 4..7 run
+ * on a second stream (a parallel chain of the phase graph) with their own scratch buffers (about
+ * 250 MB more at 1080p), and a 1080p chunk codes 1.2 % faster; 4 was measured slower than 2.
+ * Outputs are the same in every case.  No counterpart in the reference. */
 int dcvc_hts_recon_branches(int n);
 int dcvc_hts_timing(void* handle, float* out, int cap, int* count);
 /* Precision form of the analysis and synthesis transforms (encoder, decoder, recon head, feature

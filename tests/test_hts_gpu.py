@@ -175,14 +175,14 @@ def test_depthwise_fused_into_the_residual_gemm_gives_the_same_codec_outputs(pre
 
 
 def test_recon_head_in_two_branches_gives_the_same_frames():
-    """With the decoded chunk's recon head split into two concurrent branches (frames 4..7 on a
-    second stream, their own scratch buffers) the codec gives the same payloads and frames."""
+    """With the decoded chunk's recon head split into two or four concurrent branches (frames on
+    further streams with their own scratch buffers) the codec gives the same payloads and frames."""
     from dcvc_b200 import _native as N
     sd = state_dict()
     H, W = 128, 192
     out = {}
     try:
-        for n in (2, 1):
+        for n in (4, 2, 1):
             N.lib.dcvc_hts_recon_branches(n)
             enc, dec = _proxy(sd, "fp16"), _proxy(sd, "fp16")
             ref = ref_frame(H, W)
@@ -197,6 +197,7 @@ def test_recon_head_in_two_branches_gives_the_same_frames():
             out[n] = res
     finally:
         N.lib.dcvc_hts_recon_branches(2)
-    for (b0, f0), (b1, f1) in zip(out[1], out[2]):
-        assert np.array_equal(b0, b1)
-        assert all(torch.equal(a, b) for a, b in zip(f0, f1))
+    for n in (2, 4):
+        for (b0, f0), (b1, f1) in zip(out[1], out[n]):
+            assert np.array_equal(b0, b1)
+            assert all(torch.equal(a, b) for a, b in zip(f0, f1))
