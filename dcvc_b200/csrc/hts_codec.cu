@@ -308,6 +308,19 @@ int HtsCodec::allocate(int Hp, int Wp, int imgs)
     scratch_.t4 = H(S);
     scratch_.t5 = fp8_ ? acts_.alloc_n<uint8_t>(M8 * kChD) : nullptr;
     ok = ok && (!fp8_ || scratch_.t5 != nullptr);
+    // the temporal prior's side branch (enc_analysis): its DepthConvBlock is 512 channels wide at
+    // the 1/16 scale
+    s2d_t_ = H(M16 * 4 * kChM);
+    lvl16_t_ = H(M16 * 2 * kChY);
+    {
+        const size_t St = M16 * 4 * kChY;
+        scratch_t_.t0 = H(St);
+        scratch_t_.t1 = H(St);
+        scratch_t_.t2 = H(St);
+        scratch_t_.t3 = H(St);
+        scratch_t_.t4 = H(St);
+        scratch_t_.t5 = nullptr;  // the entropy-parameter path stays 16-bit in every form
+    }
     recon_branches_ = g_recon_branches.load();
     rb_a_[0] = lvl8_a_;
     rb_b_[0] = lvl8_b_;
@@ -409,14 +422,14 @@ void HtsCodec::feature_extractor(Launch& L)
     }
 }
 
-void HtsCodec::temporal_prior(Launch& L)
+void HtsCodec::temporal_prior(Launch& L, __half* s2d, __half* lvl16, Scratch& sc)
 {
     // temporal_params = RBWS2(memory * q_feature) -> cat_pf[256:768]
     L.note(launch_mul_channel(cat_fam_, M8_, kChM, 1024, q_feat_, temporal_in_, kChM, L.s, act_,
                               imgs_ > 1 ? m8_ : 0));
-    L.note(launch_space_to_depth2(temporal_in_, TH8_, W8_, kChM, kChM, s2d_, L.s));
-    gemm(L, temporal_.down, kEpiBias, s2d_, 4 * kChM, M16_, lvl16_a_, 2 * kChY);
-    run_dcb(L, temporal_.dcb, lvl16_a_, 2 * kChY, TH16_, W16_, cat_pf_ + kChY, 3 * kChY, scratch_, nullptr, H16_);
+    L.note(launch_space_to_depth2(temporal_in_, TH8_, W8_, kChM, kChM, s2d, L.s));
+    gemm(L, temporal_.down, kEpiBias, s2d, 4 * kChM, M16_, lvl16, 2 * kChY);
+    run_dcb(L, temporal_.dcb, lvl16, 2 * kChY, TH16_, W16_, cat_pf_ + kChY, 3 * kChY, sc, nullptr, H16_);
 }
 
 void HtsCodec::hyper_decoder(Launch& L)
@@ -528,6 +541,17 @@ void HtsCodec::recon_head(Launch& L, bool all_frames)
 void HtsCodec::enc_analysis(Launch& L)
 {
     const int H32 = H16p_ / 2, W32 = W16p_ / 2, H64 = H16p_ / 4, W64 = W16p_ / 4;
+    // the temporal prior depends only on the memory of the last chunk: a side branch of the graph
+    // (its own working buffers) computes it while the encoder and the hyper encoder run
+    L.note(cudaEventRecord(ev_fork_, L.s), 0);
+    L.note(cudaStreamWaitEvent(side_[0], ev_fork_, 0), 0);
+    {
+        Launch Lt{side_[0], L.err_word};
+        temporal_prior(Lt, s2d_t_, lvl16_t_, scratch_t_);
+        Lt.note(cudaEventRecord(ev_join_[0], side_[0]), 0);
+        L.note(Lt.first, 0);
+        L.kernels += Lt.kernels;
+    }
     // encoder (dmc_hts_proxy.cpp:67-78)
     run_dcb(L, encoder_[0], cat_enc_, 2048, TH8_, W8_, lvl8_a_, kChD, scratch_, nullptr, H8_);
     for (int i = 1; i < 5; ++i) {
@@ -560,7 +584,7 @@ void HtsCodec::enc_analysis(Launch& L)
     gemm(L, hyper_enc2_.down, kEpiBias, s2d_, 4 * kChY, M64_, lvl64_a_, kChZ);
     run_dcb(L, hyper_enc2_.dcb, lvl64_a_, kChZ, TH64_, W64, z_, kChZ, scratch_, nullptr, H64);
     L.note(launch_round_z(z_, z_num_, z_hat_, z_i8_, L.s));
-    temporal_prior(L);
+    L.note(cudaStreamWaitEvent(L.s, ev_join_[0], 0), 0);  // the temporal prior branch
     hyper_decoder(L);
     prior_fusion(L);
     // entropy parameters: q_dec | scales | means in common_ (chunk_tensors_3)
@@ -613,7 +637,7 @@ void HtsCodec::dec_temporal(Launch& L, bool memory_has_value)
     } else {
         feature_adaptor_i(L, feature_i_);
     }
-    temporal_prior(L);
+    temporal_prior(L, s2d_, lvl16_a_, scratch_);
 }
 
 void HtsCodec::dec_hyper(Launch& L)

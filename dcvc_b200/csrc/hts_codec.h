@@ -145,7 +145,9 @@ private:
     void feature_adaptor_m(Launch& L);
     void feature_adaptor_i(Launch& L, const __half* feature_i);
     void feature_extractor(Launch& L);
-    void temporal_prior(Launch& L);
+    // temporal prior into cat_pf_[256:768] with the given working buffers (the main ones, or the
+    // side branch's in enc_analysis)
+    void temporal_prior(Launch& L, __half* s2d, __half* lvl16, Scratch& sc);
     void hyper_decoder(Launch& L);
     void prior_fusion(Launch& L);
     void spatial_prior(Launch& L, int k);
@@ -221,6 +223,9 @@ private:
     int recon_branches_ = 1;
     __half *rb_a_[kMaxReconBranches] = {}, *rb_b_[kMaxReconBranches] = {}, *rb_head_[kMaxReconBranches] = {};
     Scratch rb_scratch_[kMaxReconBranches];
+    // enc_analysis runs the temporal prior as a side branch, concurrently with the encoder
+    __half *s2d_t_ = nullptr, *lvl16_t_ = nullptr;
+    Scratch scratch_t_;
     // pinned host staging
     int* count_host_ = nullptr;
     int16_t* sym_host_ = nullptr;
