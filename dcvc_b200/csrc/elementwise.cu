@@ -136,6 +136,53 @@ __global__ void shuffle8_clamp_kernel(const __half* __restrict__ in, int H8, int
     }
 }
 
+// The same for C = 3 (the reconstructions) with vector accesses: one thread per output row and group
+// of 8 output pixels (one input pixel), three 16-byte loads (one per channel, the row's 8 values)
+// and three 16-byte stores of the 8 interleaved pixels; the clamp is the same per element.
+template <int IDT>
+__global__ void shuffle8_clamp3_kernel(const __half* __restrict__ in, int H8, int W8, int ldi,
+                                       __half* __restrict__ out)
+{
+    griddep_launch_dependents();
+    griddep_wait();
+    const long long groups = static_cast<long long>(H8) * 8 * W8;
+    const __half lo = __float2half_rn(-0.5f);
+    const __half hi = __float2half_rn(0.5f);
+    for (long long g = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; g < groups;
+         g += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const int y = static_cast<int>(g / W8);
+        const int w8 = static_cast<int>(g - static_cast<long long>(y) * W8);
+        const __half* src = in + (static_cast<long long>(y >> 3) * W8 + w8) * ldi + (y & 7) * 8;
+        Vec8h u[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            u[c] = ld8(src + c * 64);
+        }
+        Vec8h o[3];
+#pragma unroll
+        for (int dx = 0; dx < 8; ++dx) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                __half v = u[c].v[dx];
+                if constexpr (IDT == 1) {  // BF16 input: clamp in FP32, one rounding to FP16
+                    const float f = Act<1>::to(__half_as_ushort(v));
+                    v = __float2half_rn(fminf(fmaxf(f, -0.5f), 0.5f));
+                } else {
+                    v = __hmax(v, lo);
+                    v = __hmin(v, hi);
+                }
+                const int k = dx * 3 + c;  // pixel dx, channel c of the 24 outputs
+                o[k >> 3].v[k & 7] = v;
+            }
+        }
+        __half* dst = out + (static_cast<long long>(y) * W8 + w8) * 24;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            st8(dst + 8 * j, o[j]);
+        }
+    }
+}
+
 __global__ void space_to_depth2_kernel(const __half* __restrict__ x, int H, int W, int C, int ldx,
                                        __half* __restrict__ out)
 {
@@ -986,6 +1033,15 @@ cudaError_t launch_shuffle8_clamp(const __half* in, int H8, int W8, int C, int l
 {
     if (H8 <= 0 || W8 <= 0 || C <= 0 || (in_dtype != 0 && in_dtype != 1)) {
         return cudaErrorInvalidValue;
+    }
+    if (C == 3 && ldi % 8 == 0 && ldi >= 192 && al16(in) && al16(out)) {
+        const dim3 g3(grid_for(8LL * H8 * W8));
+        if (in_dtype == 1) {
+            launch_pdl(shuffle8_clamp3_kernel<1>, g3, dim3(kThreads), 0, s, in, H8, W8, ldi, out);
+        } else {
+            launch_pdl(shuffle8_clamp3_kernel<0>, g3, dim3(kThreads), 0, s, in, H8, W8, ldi, out);
+        }
+        return cudaGetLastError();
     }
     const dim3 g(grid_for(64LL * H8 * W8));
     if (in_dtype == 1) {

@@ -1,7 +1,7 @@
 """Micro-benchmark of the codec's kernels at their 1080p shapes (CUDA events on the launching
 stream), also the small fixed case used for ncu captures.
 
-    python -m dcvc_b200.kernel_bench [--case quad|quad_f8|wsilu|res|dwres|dwres_split|bias2048|dwconv|ffn|ffn_ld|unshuffle|quantize|rans|all]
+    python -m dcvc_b200.kernel_bench [--case quad|quad_f8|wsilu|res|dwres|dwres_split|bias2048|dwconv|ffn|ffn_ld|unshuffle|shuffle|quantize|rans|all]
                                      [--reps N] [--sets S] [--bn 0|64|128|256|-1]
 
 (--bn -1 selects the streaming form of the residual GEMM.)
@@ -58,6 +58,15 @@ def _case(name, g, bn=0):
         x = rnd(1080, 1920, 24)
         out = torch.empty(M8, 1536, device="cuda", dtype=torch.float16)
         fn = lambda: ops.pad_unshuffle8(x, 8, 0, out=out)  # noqa: E731
+        return fn, 0.0, (x.numel() + out.numel()) * 2
+    if name == "shuffle":
+        # pixel_shuffle(8) + clamp of one reconstructed 1080p frame: [136 x 240, 192] -> [1088, 1920, 3]
+        x = rnd(M8, 192)
+        out = torch.empty(1088, 1920, 3, device="cuda", dtype=torch.float16)
+
+        def fn():
+            N.check(N.lib.dcvc_shuffle8_clamp(x.data_ptr(), 136, 240, 3, 192, out.data_ptr(),
+                                              torch.cuda.current_stream().cuda_stream), "shuffle8_clamp")
         return fn, 0.0, (x.numel() + out.numel()) * 2
     if name == "quantize":
         # the last masked quantisation phase at 1080p (y: 68 x 120 x 256, mode 2: accumulate and

@@ -58,6 +58,9 @@ def test_layout_kernels():
     y = _f16(rng.standard_normal((13 * 15, 192)) * 0.7)
     y[0, :5] = np.nan
     assert _same(ops.shuffle8_clamp(_dev(y), 13, 15), O.shuffle8_clamp(y, 13, 15))
+    # the general kernel: a row pitch that is not a multiple of 8 halves, an unaligned start
+    yp = _dev(np.pad(y, ((0, 0), (1, 0))))[:, 1:]
+    assert _same(ops.shuffle8_clamp(yp, 13, 15), O.shuffle8_clamp(y, 13, 15))
     z = _f16(rng.standard_normal((34 * 60, 256)))
     assert _same(ops.space_to_depth2(_dev(z), 34, 60), O.space_to_depth2(z, 34, 60))
     assert _same(ops.im2col3x3s2(_dev(z), 34, 60), O.im2col3x3s2(z, 34, 60))
