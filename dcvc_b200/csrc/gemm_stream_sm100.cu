@@ -51,8 +51,16 @@ constexpr int kSMaxKPlain = 512;            // bias / WSiLU epilogues: W slice u
 constexpr int kSEpiWarps = 16;
 constexpr int kSCols = kSBN / 4;            // accumulator columns per epilogue warp (32)
 constexpr int kSBoxBytes = 32 * kSCols * 2; // 32 rows x 32 columns of 16-bit values: 2 KB
-constexpr int kSResSlots = 2;               // residual ring depth per warp, in tiles
-constexpr int kSStages = 6;
+// residual ring depth per warp, in tiles, and A stages of the residual epilogues (compile-time
+// overrides exist for tuning builds; the library uses the defaults)
+#ifndef DCVC_STREAM_RES_SLOTS
+#define DCVC_STREAM_RES_SLOTS 2
+#endif
+#ifndef DCVC_STREAM_STAGES
+#define DCVC_STREAM_STAGES 6
+#endif
+constexpr int kSResSlots = DCVC_STREAM_RES_SLOTS;
+constexpr int kSStages = DCVC_STREAM_STAGES;
 constexpr int kSStagesPlain = 4;            // bias / WSiLU: a W slice twice as large leaves four
 
 __host__ __device__ constexpr bool stream_has_res(int epi) { return epi == kEpiBiasRes || epi == kEpiBiasResQ; }
