@@ -241,7 +241,11 @@ __global__ void __launch_bounds__(GemmCfg<BN, EPI, PAIR>::kThreads, 1)
             }
             if (*abort_flag && (!PAIR || rank == 0)) {
                 // Let the copies this thread issued land before the CTA winds down (PAIR: the
-                // even CTA's barriers count the peer's copies too).
+                // even CTA's barriers count the peer's copies too; the odd CTA cannot observe its
+                // own copies, so after an abort it relies on the even CTA's drain, which waits
+                // (bounded) for both CTAs' bytes of each stage it issued, and on the cluster
+                // barrier before either CTA exits.  A stage that only the odd CTA issued before
+                // the abort is not waited for; under the stall injection neither CTA issues any.)
                 int n = issued < kStages ? issued : kStages;
                 for (int i = 0; i < n; ++i) {
                     if (--stage < 0) {
