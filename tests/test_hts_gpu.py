@@ -201,3 +201,27 @@ def test_recon_head_in_two_branches_gives_the_same_frames():
         for (b0, f0), (b1, f1) in zip(out[1], out[n]):
             assert np.array_equal(b0, b1)
             assert all(torch.equal(a, b) for a, b in zip(f0, f1))
+
+
+def test_phase_timing_reports_every_part_of_a_call():
+    """set_timing() makes a codec time its phase graphs and its host steps; after a compress and a
+    decompress, timing() names the parts each call ran with non-negative milliseconds."""
+    sd = state_dict()
+    H, W = 128, 192
+    enc, dec = _proxy(sd, "fp16"), _proxy(sd, "fp16")
+    ref = ref_frame(H, W)
+    enc.add_ref_feature_from_frame(ref, True)
+    dec.add_ref_feature_from_frame(ref, False)
+    enc.set_timing(True)
+    dec.set_timing(True)
+    bits, ecp = enc.compress(chunk(H, W, 0), 30, False, 0, 0)
+    torch.cuda.synchronize()
+    te = enc.timing()
+    dec.decompress(bits, 30, H, W, ecp, False)
+    torch.cuda.synchronize()
+    td = dec.timing()
+    assert {"enc_analysis", "enc_update", "host_wait_analysis", "host_rans_encode"} <= set(te)
+    assert {"dec_temporal", "dec_hyper", "dec_context", "dec_synthesis", "host_decode_z",
+            "host_wait_hyper", "host_decode_y"} <= set(td)
+    assert all(v >= 0 for v in list(te.values()) + list(td.values()))
+    assert te["enc_analysis"] > 0 and td["dec_synthesis"] > 0
